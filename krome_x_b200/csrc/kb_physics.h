@@ -1,0 +1,272 @@
+// Runtime physics the benchmark networks call from their rates and thermal
+// terms, restated for host and device (KB_HD). Each function evaluates the
+// published fit the reference's runtime module evaluates, with the same
+// constants and the same operation order (the CPU checker compiles this
+// file too and must reproduce the reference's numbers bit for bit):
+//
+//   cooling_Atomic     Cen 1992 collisional ionization + excitation
+//                      (reference runtime/core/cooling.hpp:32-68)
+//   cooling_H2         Glover & Abel 2008 low-density colliders, HM79 /
+//                      Glover 2015 LTE limit (cooling.hpp:74-177)
+//   cooling_Continuum  Lenzuni+1996 Planck opacity, Jeans-length escape
+//                      (cooling.hpp:282-303)
+//   dissH2_Martin96    Martin, Schwarz & Mandy 1996 H2 collisional
+//                      dissociation (special_rates.hpp:20-63)
+//   H/He_recombination_on_dust  Weingartner & Draine 2001
+//                      (dust_rates.hpp:37-66)
+//   H2_solomonLW       Solomon-process H2 photodissociation
+//                      (h2_shielding.hpp:84-93)
+//
+// Included inside the network namespace after the generated indices; the
+// KB_HAS_<species> macros select the terms a network has.
+#pragma once
+
+KB_HD inline double cool_sigmoid_(double x, double x0, double s) {
+  return 10.0 / (10.0 + std::exp(-s * (x - x0)));
+}
+
+KB_HD inline double wCool_(double logT, double logTmin, double logTmax) {
+  const double x = (logT - logTmin) / (logTmax - logTmin);
+  const double w = std::pow(10.0, 200.0 * (cool_sigmoid_(x, -0.2, 50.0)
+                            * cool_sigmoid_(-x, -1.2, 50.0) - 1.0));
+  return (w < 1e-199) ? 0.0 : w;
+}
+
+#ifdef KB_HAS_E
+KB_HD inline double cooling_Atomic(double Tgas, const double* n) {
+  const double temp = std::fmax(Tgas, 10.0);
+  const double T5 = temp / 1e5;
+  const double ne = n[IDX_E];
+  (void)T5; (void)ne;
+  double cool = 0.0;
+#ifdef KB_HAS_H
+  cool += 1.27e-21 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+          * std::exp(-1.578091e5 / temp) * ne * n[IDX_H];
+#endif
+#ifdef KB_HAS_He
+  cool += 9.38e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+          * std::exp(-2.853354e5 / temp) * ne * n[IDX_He];
+#endif
+#ifdef KB_HAS_Hej
+  cool += 4.95e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+          * std::exp(-6.31515e5 / temp) * ne * n[IDX_Hej];
+  cool += 5.01e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+          * std::exp(-5.5338e4 / temp) * ne * ne * n[IDX_Hej];
+#endif
+#ifdef KB_HAS_H
+  cool += 7.5e-19 / (1.0 + std::sqrt(T5)) * std::exp(-1.18348e5 / temp)
+          * ne * n[IDX_H];
+#endif
+#ifdef KB_HAS_Hej
+  cool += 9.1e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+          * std::exp(-1.3179e4 / temp) * ne * ne * n[IDX_Hej];
+  cool += 5.54e-17 * std::pow(temp, -0.397) / (1.0 + std::sqrt(T5))
+          * std::exp(-4.73638e5 / temp) * ne * n[IDX_Hej];
+#endif
+  return std::fmax(cool, 0.0);
+}
+#else
+KB_HD inline double cooling_Atomic(double, const double*) { return 0.0; }
+#endif
+
+#ifdef KB_HAS_H2
+KB_HD inline double cooling_H2(double Tgas, const double* n) {
+  const double temp = Tgas;
+  const double T3 = temp * 1e-3;
+  const double logt3 = std::log10(T3);
+  const double logt = std::log10(temp);
+  const double logt32 = logt3 * logt3, logt33 = logt32 * logt3,
+               logt34 = logt33 * logt3, logt35 = logt34 * logt3,
+               logt36 = logt35 * logt3, logt37 = logt36 * logt3,
+               logt38 = logt37 * logt3;
+  const double w14 = wCool_(logt, 1.0, 4.0);
+  const double w24 = wCool_(logt, 2.0, 4.0);
+  (void)w14; (void)w24; (void)logt36; (void)logt37; (void)logt38;
+  double cool = 0.0;
+#ifdef KB_HAS_H
+  double fH2H;
+  if (temp <= 1e2)
+    fH2H = std::pow(10.0, -16.818342 + 37.383713 * logt3
+           + 58.145166 * logt32 + 48.656103 * logt33
+           + 20.159831 * logt34 + 3.8479610 * logt35) * n[IDX_H];
+  else if (temp <= 1e3)
+    fH2H = std::pow(10.0, -24.311209 + 3.5692468 * logt3
+           - 11.332860 * logt32 - 27.850082 * logt33
+           - 21.328264 * logt34 - 4.2519023 * logt35) * n[IDX_H];
+  else if (temp <= 6e3)
+    fH2H = std::pow(10.0, -24.311209 + 4.6450521 * logt3
+           - 3.7209846 * logt32 + 5.9369081 * logt33
+           - 5.5108049 * logt34 + 1.5538288 * logt35) * n[IDX_H];
+  else
+    fH2H = 1.862314467912518e-22 * wCool_(logt, 1.0, std::log10(6e3))
+           * n[IDX_H];
+  cool += fH2H;
+#endif
+#ifdef KB_HAS_Hj
+  double fH2Hp;
+  if (temp > 1e1 && temp <= 1e4)
+    fH2Hp = std::pow(10.0, -22.089523 + 1.5714711 * logt3
+            + 0.015391166 * logt32 - 0.23619985 * logt33
+            - 0.51002221 * logt34 + 0.32168730 * logt35) * n[IDX_Hj];
+  else
+    fH2Hp = 1.182509139382060e-21 * n[IDX_Hj] * w14;
+  cool += fH2Hp;
+#endif
+  cool += w24 * std::pow(10.0, -23.962112 + 2.09433740 * logt3
+          - 0.77151436 * logt32 + 0.43693353 * logt33
+          - 0.14913216 * logt34 - 0.033638326 * logt35) * n[IDX_H2];
+#ifdef KB_HAS_E
+  double fH2e;
+  if (temp <= 5e2)
+    fH2e = std::pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+           + 96.743155 * logt32 + 343.19180 * logt33
+           + 734.71651 * logt34 + 983.67576 * logt35
+           + 801.81247 * logt36 + 364.14446 * logt37
+           + 70.609154 * logt38, 30.0)) * n[IDX_E];
+  else
+    fH2e = std::pow(10.0, -22.921189 + 1.6802758 * logt3
+           + 0.93310622 * logt32 + 4.0406627 * logt33
+           - 4.7274036 * logt34 - 8.8077017 * logt35
+           + 8.9167183 * logt36 + 6.4380698 * logt37
+           - 6.3701156 * logt38) * n[IDX_E];
+  cool += fH2e * w24;
+#endif
+#ifdef KB_HAS_He
+  double fH2He;
+  if (temp > 1e1 && temp <= 1e4)
+    fH2He = std::pow(10.0, -23.689237 + 2.1892372 * logt3
+            - 0.81520438 * logt32 + 0.29036281 * logt33
+            - 0.16596184 * logt34 + 0.19191375 * logt35) * n[IDX_He];
+  else
+    fH2He = 1.002560385050777e-22 * n[IDX_He] * w14;
+  cool += fH2He;
+#endif
+  if (cool <= 0.0) return 0.0;
+  double HDL;
+  if (temp < 2e3) {
+    const double HDLR = 9.5e-22 * std::pow(T3, 3.76)
+                        / (1.0 + 0.12 * std::pow(T3, 2.1))
+                        * std::exp(-std::pow(0.13 / T3, 3.0))
+                        + 3e-24 * std::exp(-0.51 / T3);
+    const double HDLV = 6.7e-19 * std::exp(-5.86 / T3)
+                        + 1.6e-18 * std::exp(-11.7 / T3);
+    HDL = HDLR + HDLV;
+  } else if (temp <= 1e4) {
+    HDL = std::pow(10.0, -20.584225 + 5.0194035 * logt3
+          - 1.5738805 * logt32 - 4.7155769 * logt33
+          + 2.4714161 * logt34 + 5.4710750 * logt35
+          - 3.9467356 * logt36 - 2.2148338 * logt37
+          + 1.8161874 * logt38);
+  } else {
+    const double dump14 = 1.0
+        / (1.0 + std::exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
+    HDL = 5.531333679406485e-19 * dump14;
+  }
+  if (HDL == 0.0) return 0.0;
+  return n[IDX_H2] / (1.0 / HDL + 1.0 / cool);
+}
+#else
+KB_HD inline double cooling_H2(double, const double*) { return 0.0; }
+#endif
+
+// Planck mean opacity (Lenzuni+1996, density-only fit)
+KB_HD inline double kpla_(const double* n) {
+  const double rho = rho_(n);
+  if (rho < 1e-12) return 0.0;
+  const double y = std::log10(std::fmin(rho, 0.5));
+  return std::pow(10.0, 1.000042 * y + 2.14989);
+}
+
+KB_HD inline double cooling_Continuum(double Tgas, const double* n) {
+  const double rho = std::fmax(rho_(n), 1e-40);
+  const double kgas = kpla_(n);
+  const double mu = rho / std::fmax(ntot_(n), 1e-40) / kbc::p_mass;
+  const double lj = std::sqrt(kbc::pi * kbc::boltzmann_erg * Tgas
+                              / rho / kbc::p_mass / kbc::gravity / mu);
+  const double tau = lj * kgas * rho + 1e-40;
+  const double beta = std::fmin(1.0, 1.0 / (tau * tau));
+  return 4.0 * kbc::stefboltz_erg * Tgas * Tgas * Tgas * Tgas
+      * kgas * rho * beta;
+}
+
+#ifdef KB_EXTERN_dissH2_Martin96
+KB_HD inline double dissH2_Martin96(double Tgas_in, const double* n,
+                                    const Params& p) {
+  (void)p;
+  const double Tgas = std::fmin(Tgas_in, 4.5e4);
+  constexpr double m[2][21] = {
+      {-178.4239, -68.42243, 43.20243, -4.633167, 69.70086, 40870.38,
+       -23705.70, 128.8953, -53.91334, 5.315517, -19.73427, 16780.95,
+       -25786.11, 14.82123, -4.890915, 0.4749030, -133.8283, -1.164408,
+       0.8227443, 0.5864073, -2.056313},
+      {-142.7664, 42.70741, -2.027365, -0.2582097, 21.36094, 27535.31,
+       -21467.79, 60.34928, -27.43096, 2.676150, -11.28215, 14254.55,
+       -23125.20, 9.305564, -2.464009, 0.1985955, 743.0600, -1.174242,
+       0.7502286, 0.2358848, 2.937507}};
+  const double n_H = Hnuclei_(n);
+  const double logT = std::log10(Tgas);
+  const double invT = 1.0 / Tgas;
+  const double logT2 = logT * logT;
+  const double logT3 = logT2 * logT;
+  double k_CID = 0.0;
+KB_UNROLL
+  for (int i = 0; i < 2; ++i) {
+    const double* c = m[i];
+    const double logk_h1 = c[0] + c[1] * logT + c[2] * logT2
+        + c[3] * logT3 + c[4] * std::log10(1.0 + c[5] * invT);
+    const double logk_h2 = c[6] * invT;
+    const double logk_l1 = c[7] + c[8] * logT + c[9] * logT2
+        + c[10] * std::log10(1.0 + c[11] * invT);
+    const double logk_l2 = c[12] * invT;
+    const double logn_c1 = c[13] + c[14] * logT + c[15] * logT2
+        + c[16] * invT;
+    const double logn_c2 = c[17] + logn_c1;
+    const double pp = c[18] + c[19] * std::exp(-Tgas / 1.850e3)
+        + c[20] * std::exp(-Tgas / 4.40e2);
+    const double n_c1 = std::pow(10.0, logn_c1);
+    const double n_c2 = std::pow(10.0, logn_c2);
+    const double logk_CID = logk_h1
+        - (logk_h1 - logk_l1) / (1.0 + std::pow(n_H / n_c1, pp))
+        + logk_h2
+        - (logk_h2 - logk_l2) / (1.0 + std::pow(n_H / n_c2, pp));
+    k_CID += std::pow(10.0, logk_CID);
+  }
+  return k_CID;
+}
+#endif
+
+#if defined(KB_EXTERN_H_recombination_on_dust) \
+    || defined(KB_EXTERN_He_recombination_on_dust)
+KB_HD inline double wd01_fit_(double pre, double c1, double p1, double c2,
+                              double q, double p2a, double p2b, double Tgas,
+                              const double* n, const Params& p) {
+  if (n[IDX_E] < 1e-20) return 0.0;
+  const double scale = pre * (p.d2g / 1e-2);
+  const double psi = p.G0 * std::sqrt(Tgas) / n[IDX_E];
+  if (psi <= 0.0) return scale;
+  return scale / (1.0 + c1 * std::pow(psi, p1)
+                  * (1.0 + c2 * std::pow(Tgas, q)
+                     * std::pow(psi, p2a + p2b * std::log(Tgas))));
+}
+#endif
+#ifdef KB_EXTERN_H_recombination_on_dust
+KB_HD inline double H_recombination_on_dust(double Tgas, const double* n,
+                                            const Params& p) {
+  return wd01_fit_(1.225e-13, 8.074e-6, 1.378, 5.087e2, 0.01586, -0.4723,
+                   -1.102e-5, Tgas, n, p);
+}
+#endif
+#ifdef KB_EXTERN_He_recombination_on_dust
+KB_HD inline double He_recombination_on_dust(double Tgas, const double* n,
+                                             const Params& p) {
+  return wd01_fit_(5.572e-14, 3.185e-7, 1.512, 5.115e3, 3.903e-7, -0.4956,
+                   -5.494e-7, Tgas, n, p);
+}
+#endif
+#ifdef KB_EXTERN_H2_solomonLW
+KB_HD inline double H2_solomonLW(double flux_eV, double Tgas, const double* n,
+                                 const Params& p) {
+  (void)Tgas; (void)n; (void)p;
+  return 1.38e9 * flux_eV * kbc::eV_to_erg;
+}
+#endif

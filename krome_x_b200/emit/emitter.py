@@ -1,0 +1,743 @@
+"""Network emitter: writes the per-network device header the B200 kernels
+compile against (``krome_x_b200/networks/net_<key>.h``).
+
+Frontend. The network language is the reference's ``.knet`` format; the
+emitter parses and resolves a network with the reference generator's own
+frontend (``kromex.knet.parse_network`` and the ``kromex.codegen.Codegen``
+resolution: piecewise groups, rate classification, parameters) and renders
+each rate and variable expression with ``Codegen.cexpr``, so every rate is
+the same arithmetic expression as in a reference project (reference:
+kromex/codegen.py:1618-1733). The frontend is needed only when a header is
+(re)generated, on a machine that has the reference tree; the generated
+headers are committed and nothing at build or run time imports it.
+
+Backend (this project's). The header is one host/device (``KB_HD``) scalar
+form of the network, laid out for a warp-per-cell integrator where the
+scalar network math is SIMT-uniform across lanes (every lane of a cell's
+warp evaluates it on its own state: the base state, or a perturbed one in a
+difference-quotient Jacobian column):
+
+* ``rates_fixed`` / ``rates_var``: the rate coefficients of Tgas and the
+  parameters only, and the rest (densities, externs); piecewise groups with
+  the reference's ``outside=asym`` selection (zero below the group, the
+  temperature clamped above it; reference: kromex/codegen.py:8052-8114);
+* ``rhs``: mass-action dn/dt with each species' terms accumulated in
+  reaction order, reactants then products (reference: kromex/codegen.py:
+  4289-4327), so the sums round as the reference's do;
+* ``jac_stoich``: the stoichiometric Jacobian d dn_i / d n_j of the rates
+  held fixed (reference: kromex/codegen.py:8366-8378, 5172-5210);
+* ``thermal_dTdt``: (gamma - 1)(heat - cool)/(kB ntot) with the configured
+  processes in the reference's term order (reference:
+  runtime/core/solve_cell.hpp:305-429), the network-derived terms (H2
+  formation heating, collisional dissociation cooling, recombination
+  cooling, the EXACT adiabatic index) emitted by the rules the reference
+  generator applies (kromex/codegen.py:4900-5000, 6857-6966, 3697-3819).
+"""
+import math
+import os
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent.parent
+OUTDIR = PKG / "networks"
+
+# the benchmark networks and their generation options (the reference
+# Preprocessor's thermal section)
+NETWORKS = {
+    "primordial": dict(network="primordial", cooling=["ATOMIC", "H2"],
+                       heating=["CHEM", "COMPRESS"]),
+    "primordial3": dict(network="primordial3",
+                        cooling=["H2", "CONT", "CHEM"],
+                        heating=["COMPRESS", "CHEM"],
+                        h2_opacity="RIPAMONTI", gamma="EXACT"),
+    "galaxy_ism": dict(network="galaxy_ism", cooling=[], heating=[]),
+}
+
+# H2-chemistry energy ledger of thermal CHEM (reactants, products, eV,
+# thermalized): formation heats by its exothermicity times the HM79
+# thermalized fraction, collisional dissociation cools by 4.48 eV
+# (reference: kromex/codegen.py:4929-4937)
+CHEM_LEDGER = [
+    (["H", "H", "H"], ["H", "H2"], "4.48", True),
+    (["H", "H", "H2"], ["H2", "H2"], "4.48", True),
+    (["H", "H-"], ["H2", "e-"], "3.53", True),
+    (["H", "H2+"], ["H+", "H2"], "1.83", True),
+    (["H", "H2"], ["H", "H", "H"], "-4.48", False),
+    (["H2", "e-"], ["H", "H", "e-"], "-4.48", False),
+    (["H2", "H2"], ["H", "H", "H2"], "-4.48", False),
+]
+
+
+def _reference_root():
+    return Path(os.environ.get("KROME_REFERENCE", "/root/reference"))
+
+
+def _frontend(cfg):
+    """the resolved network: the reference generator's parse + Codegen,
+    configured as a reference project with these options would be"""
+    ref = _reference_root()
+    for p in (str(ref), str(ref / "kromex")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    from kromex import Preprocessor
+    import codegen
+    import knet
+    kp = Preprocessor(network=cfg["network"])
+    kp.thermal.cooling = cfg.get("cooling", [])
+    kp.thermal.heating = cfg.get("heating", [])
+    if cfg.get("h2_opacity"):
+        kp.thermal.h2_opacity = cfg["h2_opacity"]
+    if cfg.get("gamma"):
+        kp.thermal.gamma = cfg["gamma"]
+    _, args = kp._args("/tmp/kb_emit_unused")
+    args.network_file = args.network_pos or args.network
+    net = knet.parse_network(args.network_file)
+    if net.errors:
+        raise RuntimeError("; ".join(net.errors))
+    gen = codegen.Codegen(
+        net, outside=args.outside, secion=args.secondary_ionization.split(","),
+        num2col=args.num2col, metal_cooling=args.metal_cooling.split(","),
+        dust_tables=args.dust_tables, gas_total=args.gas_total,
+        cooling=args.cooling.split(","), heating=args.heating.split(","),
+        cooling_floor=args.cooling_floor, evolve_rad=args.evolve_rad,
+        evolve_Td=args.evolve_Td, shielding=args.shielding, gamma=args.gamma,
+        h2_opacity=args.h2_opacity, photo_induced=args.photo_induced,
+        photoelectric=args.photoelectric, wd01=args.wd01,
+        cmb_pumping=args.cmb_pumping, habing_shield=args.habing_dust_shielding,
+        reactant_multiplicity=args.reactant_multiplicity,
+        screening=args.screening, binding_energies=args.binding_energies,
+        surface_nu=args.surface_nu,
+        surface_competition=not args.no_surface_competition,
+        surface_tunnelling=not args.no_surface_tunnelling,
+        reactive_desorption=args.reactive_desorption,
+        cr_desorption=args.cr_desorption, surface_bins=args.surface_bins,
+        rtol=args.rtol, atol=args.atol, cool_files=[],
+        cool_levels=args.cool_levels, evolve_dust=args.evolve_dust,
+        custom_atol=args.custom_atol, custom_rtol=args.custom_rtol,
+        cool_escape=args.cool_escape, rhs=args.rhs)
+    gen.generate_files()  # completes the resolution (parameters, groups)
+    return net, gen, codegen
+
+
+class Emitter:
+    def __init__(self, key, cfg):
+        self.key = key
+        self.cfg = cfg
+        self.net, self.gen, self.cg = _frontend(cfg)
+        self.species = sorted(self.net.species)
+        self.idx = {s: i for i, s in enumerate(self.species)}
+        self.lines = []
+        self.hoisted = {}
+
+    # -- helpers -----------------------------------------------------------
+
+    def w(self, s=""):
+        self.lines.append(s)
+
+    def cid(self, s):
+        return self.gen.cid(s)
+
+    def cx(self, ast, tvar):
+        g = self.gen
+        g._hoisted = dict(self.hoisted)
+        g._in_ratefn = False
+        s = g.cexpr(ast, tvar)
+        return s.replace("constants::", "kbc::")
+
+    def num(self, v):
+        return self.gen.cnum(v)
+
+    def den(self, sp):
+        return "n[IDX_%s]" % self.cid(sp)
+
+    # -- sections ----------------------------------------------------------
+
+    def emit_head(self):
+        net, gen = self.net, self.gen
+        ns = len(self.species)
+        nr = len(net.reactions)
+        w = self.w
+        w("// Generated by krome_x_b200.emit from the network '%s' -- do not "
+          "edit." % net.name)
+        w("// One host/device (KB_HD) scalar form of the network: species,")
+        w("// parameters, rate coefficients, mass-action rhs, stoichiometric")
+        w("// Jacobian and the thermal equation (see krome_x_b200/emit/")
+        w("// emitter.py for the layout and the reference rules it follows).")
+        w("#pragma once")
+        w('#include "../csrc/kb_common.h"')
+        w("")
+        w("namespace kbnet {")
+        w("")
+        w('constexpr const char* NETWORK_NAME = "%s";' % net.name)
+        w('constexpr const char* NETWORK_KEY = "%s";' % self.key)
+        w("constexpr int NSPEC = %d;" % ns)
+        w("constexpr int NREA = %d;" % nr)
+        for i, s in enumerate(self.species):
+            w("constexpr int IDX_%s = %d;" % (self.cid(s), i))
+        for s in self.species:
+            w("#define KB_HAS_%s 1" % self.cid(s))
+        for f in sorted(net.externs):
+            w("#define KB_EXTERN_%s 1" % f)
+        w("constexpr int IDX_ELECTRON = %d;" % self.idx.get("e-", -1))
+        w("")
+        names = ", ".join('"%s"' % s for s in self.species)
+        w("inline const char* const species_names[NSPEC] = {%s};" % names)
+        sp = net.species
+        mass_amu = [sp[s]["mass_amu"] for s in self.species]
+        # masses in grams as the reference writes them (mass_amu * amu)
+        import constants as kc  # the reference's constant table
+        mass_g = [m * kc.amu for m in mass_amu]
+        charge = [sp[s]["charge"] for s in self.species]
+        nH = [float(self.gen._natoms_H(s)) if hasattr(self.gen, "_natoms_H")
+              else float((sp[s]["composition"] or {}).get("H", 0))
+              for s in self.species]
+        w("KB_HD inline double species_mass_g(int i) {")
+        w("  constexpr double t_[NSPEC] = {%s};"
+          % ", ".join(repr(float(m)) for m in mass_g))
+        w("  return t_[i];")
+        w("}")
+        w("KB_HD inline int species_charge(int i) {")
+        w("  constexpr int t_[NSPEC] = {%s};" % ", ".join(str(c) for c in charge))
+        w("  return t_[i];")
+        w("}")
+        w("KB_HD inline double species_natoms_H(int i) {")
+        w("  constexpr double t_[NSPEC] = {%s};" % ", ".join(repr(x) for x in nH))
+        w("  return t_[i];")
+        w("}")
+        # summing helpers: sequential sums in species order (reference:
+        # generated net_<name>_core.hpp ntot_ / Hnuclei_ / rho_)
+        w("KB_HD inline double ntot_(const double* n) {")
+        w("  double s = 0.0;")
+        w("KB_UNROLL")
+        w("  for (int i = 0; i < NSPEC; ++i) s += n[i];")
+        w("  return s;")
+        w("}")
+        w("KB_HD inline double Hnuclei_(const double* n) {")
+        w("  double s = 0.0;")
+        w("KB_UNROLL")
+        w("  for (int i = 0; i < NSPEC; ++i) s += n[i] * species_natoms_H(i);")
+        w("  return s;")
+        w("}")
+        w("KB_HD inline double rho_(const double* n) {")
+        w("  double s = 0.0;")
+        w("KB_UNROLL")
+        w("  for (int i = 0; i < NSPEC; ++i) s += n[i] * species_mass_g(i);")
+        w("  return s;")
+        w("}")
+        w("")
+        # parameters
+        univ = {nm: (dv, cm) for nm, dv, cm in self.cg.UNIVERSAL_PARAMS}
+        pn = list(gen.pnames)
+        req = set(gen.param_required)
+        dflt = []
+        for s in pn:
+            if s in net.params:
+                dflt.append(float(net.params[s]))
+            else:
+                dv = univ[s][0]
+                dflt.append(None if dv is None else float(dv))
+        w("constexpr int NPAR = %d;" % len(pn))
+        w("struct Params {")
+        for s in pn:
+            w("  double %s;" % s)
+        w("};")
+        w("inline const char* const param_names[NPAR] = {%s};"
+          % ", ".join('"%s"' % s for s in pn))
+        w("// the defaults of a parameter row; NaN marks a REQUIRED parameter")
+        w("inline double param_default(int i) {")
+        w("  const double t_[NPAR] = {%s};" % ", ".join(
+            "NAN" if d is None else repr(d) for d in dflt))
+        w("  return t_[i];")
+        w("}")
+        w("inline const char* const param_required_by[NPAR] = {%s};" % ", ".join(
+            '"%s"' % (gen.param_required_by.get(s, "") if s in req else "")
+            .replace('"', "'") for s in pn))
+        w("KB_HD inline void params_from_row(const double* row, Params& p) {")
+        for i, s in enumerate(pn):
+            w("  p.%s = row[%d];" % (s, i))
+        w("}")
+        w("KB_HD inline int params_missing(const Params& p) {")
+        w("  (void)p;")
+        for i, s in enumerate(pn):
+            if s in req:
+                w("  if (p.%s != p.%s) return %d;" % (s, s, i))
+        w("  return -1;")
+        w("}")
+        self.pnames = pn
+        self.meta = dict(
+            network=net.name, key=self.key, species=list(self.species),
+            mass_g=mass_g, charge=charge, params=pn,
+            defaults=[None if d is None else d for d in dflt],
+            required_by={s: gen.param_required_by.get(s, "") for s in pn
+                         if s in req},
+            nrea=nr, options=self.cfg)
+        w("")
+
+    def emit_physics(self):
+        self.w('#include "../csrc/kb_physics.h"')
+        self.w("")
+
+    def emit_vars(self):
+        net = self.net
+        order = getattr(net, "var_order", None) or list(net.vars)
+        for name in order:
+            ast = net.vars[name]
+            self.w("KB_HD inline double v_%s(double Tgas, const double* n, "
+                   "const Params& p) {" % name)
+            self.w("  (void)Tgas; (void)n; (void)p;")
+            self.w("  return %s;" % self.cx(ast, "Tgas"))
+            self.w("}")
+        self.w("")
+
+    def _rate_body(self, rx, tv):
+        i = rx["id"] - 1
+        return ["k[%d] = %s;  // %s" % (i, self.cx(rx["rate"]["ast"], tv),
+                                         rx["eq"])]
+
+    def hoist(self, rxs, tvar, indent):
+        """the vars the given rates reference, as locals of this scope"""
+        names = sorted({nd["s"] for rx in rxs
+                        for nd in self.gen.deep_walk(rx["rate"]["ast"])
+                        if nd.get("kind") == "var"})
+        self.hoisted = {}
+        for s in names:
+            self.w("%sconst double vh_%s = v_%s(%s, n, p);" % (indent, s, s, tvar))
+            self.w("%s(void)vh_%s;" % (indent, s))
+        self.hoisted = {s: "vh_" + s for s in names}
+
+    def emit_grouped(self, body, select, hoist=True):
+        """statements for the selected expr-rate reactions, singles first,
+        then each piecewise group with the outside=asym selection (zero
+        below the group's range, temperature clamped above it)"""
+        w = self.w
+        singles, groups = [], {}
+        for rx in self.net.reactions:
+            if rx["rate"]["kind"] != "expr" or not select(rx):
+                continue
+            if rx.get("group") is None:
+                singles.append(rx)
+            else:
+                groups.setdefault(rx["group"], []).append(rx)
+        if hoist and singles:
+            self.hoist(singles, "Tgas", "  ")
+        for rx in singles:
+            for ln in body(rx, "Tgas"):
+                w("  " + ln)
+        self.hoisted = {}
+        outside = self.gen.outside
+        for g, pieces in sorted(groups.items()):
+            pieces.sort(key=lambda r: r["trange"])
+            glo, ghi = pieces[0]["trange"][0], pieces[-1]["trange"][1]
+            w("  {  // group %d: %s" % (g, pieces[0]["eq"]))
+            w("    double T = Tgas;")
+            clamp_lo = outside == "clamp"
+            zero_lo = outside in ("zero", "asym") and glo > 0.0
+            clamp_hi = outside in ("clamp", "asym")
+            if clamp_lo and glo > 0.0:
+                w("    if (T < %s) T = %s;" % (self.num(glo), self.num(glo)))
+            if clamp_hi and ghi != math.inf:
+                w("    if (T > %s) T = %s;" % (self.num(ghi), self.num(ghi)))
+            if hoist:
+                self.hoist(pieces, "T", "    ")
+            cond0 = "T >= %s && " % self.num(glo) if zero_lo else ""
+            for j, rx in enumerate(pieces):
+                lo, hi = rx["trange"]
+                last = j == len(pieces) - 1
+                cmp_hi = "<=" if (last and hi != math.inf) else "<"
+                conds = []
+                if j > 0 or zero_lo:
+                    conds.append("T >= %s" % self.num(lo))
+                if hi != math.inf and not (last and clamp_hi):
+                    conds.append("T %s %s" % (cmp_hi, self.num(hi)))
+                cond = " && ".join(conds) if conds else "true"
+                kw = "if" if j == 0 else "else if"
+                w("    %s (%s%s) {" % (kw, cond0 if j == 0 else "", cond))
+                for ln in body(rx, "T"):
+                    w("      " + ln)
+                w("    }")
+                cond0 = ""
+            w("  }")
+            self.hoisted = {}
+
+    def emit_rates(self):
+        gen = self.gen
+        fixed = [rx for rx in self.net.reactions
+                 if rx["rate"]["kind"] == "expr" and gen.rate_is_fixed(rx)]
+        self.nfixed = len(fixed)
+        for part, sel in (("fixed", gen.rate_is_fixed),
+                          ("var", lambda rx: not gen.rate_is_fixed(rx))):
+            self.w("// rate coefficients of Tgas and the parameters only"
+                   if part == "fixed" else
+                   "// rate coefficients that also depend on the densities")
+            self.w("KB_HD inline void rates_%s(double Tgas, const double* n, "
+                   "const Params& p, double* k) {" % part)
+            self.w("  (void)Tgas; (void)n; (void)p; (void)k;")
+            self.emit_grouped(self._rate_body, sel)
+            self.w("}")
+        # which coefficients each part writes
+        fixed_ids = sorted(rx["id"] - 1 for rx in fixed)
+        self.w("constexpr int NREA_FIXED = %d;" % len(fixed_ids))
+        self.w("KB_HD inline bool rate_is_fixed(int r) {")
+        self.w("  switch (r) {")
+        for i in fixed_ids:
+            self.w("    case %d:" % i)
+        if fixed_ids:
+            self.w("      return true;")
+        self.w("    default: return false;")
+        self.w("  }")
+        self.w("}")
+        self.w("")
+
+    def _kin(self, rx):
+        return [r["sp"] for r in rx["reactants"] if r["kinetic"]]
+
+    def emit_rhs(self):
+        w = self.w
+        w("// mass-action dn/dt: per species, the flux terms in reaction "
+          "order")
+        w("KB_HD inline void rhs(const double* n, const double* k, double* dn) {")
+        w("KB_UNROLL")
+        w("  for (int i = 0; i < NSPEC; ++i) dn[i] = 0.0;")
+        w("  double flux;")
+        w("  (void)flux;")
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            fac = ["k[%d]" % i] + [self.den(s) for s in self._kin(rx)]
+            w("  flux = %s;" % "*".join(fac))
+            for r in rx["reactants"]:
+                w("  dn[IDX_%s] -= flux;" % self.cid(r["sp"]))
+            for pr in rx["products"]:
+                w("  dn[IDX_%s] += flux;" % self.cid(pr["sp"]))
+        w("}")
+        w("")
+
+    def emit_jac(self):
+        """d dn_i / d n_j of the mass-action terms at fixed k, into
+        J[i*rs + j*cs] (the species block, zeroed here)"""
+        w = self.w
+        w("KB_HD inline void jac_stoich(const double* n, const double* k, "
+          "double* J, int rs, int cs) {")
+        w("  for (int i = 0; i < NSPEC; ++i)")
+        w("    for (int j = 0; j < NSPEC; ++j) J[i*rs + j*cs] = 0.0;")
+        w("  double d;")
+        w("  (void)d; (void)n; (void)k;")
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            targets = {}
+            for s in self._kin(rx):
+                targets[s] = targets.get(s, 0) + 1
+            for tgt, mult in sorted(targets.items()):
+                rest = ["k[%d]" % i]
+                for s, c in sorted(targets.items()):
+                    rest += [self.den(s)] * (c - 1 if s == tgt else c)
+                coef = ("%d.0*" % mult) if mult > 1 else ""
+                w("  d = %s;" % (coef + "*".join(rest)))
+                col = "IDX_%s" % self.cid(tgt)
+                for r in rx["reactants"]:
+                    w("  J[IDX_%s*rs + %s*cs] -= d;" % (self.cid(r["sp"]), col))
+                for pr in rx["products"]:
+                    w("  J[IDX_%s*rs + %s*cs] += d;" % (self.cid(pr["sp"]), col))
+        w("}")
+        w("")
+
+    # -- thermal -----------------------------------------------------------
+
+    def _recomb_reactions(self):
+        """the electron recombinations X^q+ + e- -> X^(q-1)+ of atomic ions
+        the ATOMIC recombination cooling counts (reference:
+        kromex/codegen.py:6857-6888)"""
+        net, out = self.net, []
+        for rx in net.reactions:
+            if rx["rate"]["kind"] != "expr":
+                continue
+            R, P = rx["reactants"], rx["products"]
+            if len(R) != 2 or len(P) != 1:
+                continue
+            ions = [r["sp"] for r in R if r["sp"] != "e-"]
+            if len(ions) != 1 or len(R) - len(ions) != 1:
+                continue
+            ion, prod = ions[0], P[0]["sp"]
+            si, sp = net.species[ion], net.species[prod]
+            if si["opaque"] or sp["opaque"] or si["phase"] != "gas" \
+                    or sp["phase"] != "gas" or self.gen._natoms(ion) != 1:
+                continue
+            if si["composition"] != sp["composition"] \
+                    or sp["charge"] != si["charge"] - 1 or si["charge"] < 1:
+                continue
+            if any(nd.get("kind") in ("extern", "table")
+                   and "dust" in str(nd.get("f", "")).lower()
+                   or nd.get("s") == "Tdust"
+                   for nd in self.gen.deep_walk(rx["rate"]["ast"])):
+                continue
+            out.append(rx)
+        return out
+
+    def emit_thermal(self):
+        w = self.w
+        th = self.gen.thermal
+        net = self.net
+        # the H2 chemistry ledger (thermal CHEM)
+        chem = []
+        for rx in net.reactions:
+            R = sorted(r["sp"] for r in rx["reactants"])
+            P = sorted(p0["sp"] for p0 in rx["products"])
+            for rr, pp, q, ff in CHEM_LEDGER:
+                if R == rr and P == pp:
+                    chem.append((q, rx, ff))
+                    break
+        heat_terms = [x for x in chem if not x[0].startswith("-")]
+        diss_terms = [x for x in chem if x[0].startswith("-")]
+        if th.get("cool_chem"):
+            w("KB_HD inline double cooling_chem(const double* n, const double* k) {")
+            w("  double c = 0.0;")
+            for q, rx, _ in diss_terms:
+                prod = "*".join(self.den(r["sp"]) for r in rx["reactants"])
+                w("  c += k[%d] * %s * %s;" % (rx["id"] - 1, q[1:], prod))
+            if diss_terms:
+                w("  c *= kbc::eV_to_erg;")
+            w("  return c;")
+            w("}")
+        if th.get("heat_chem"):
+            w("KB_HD inline double heating_chem(double Tgas, const double* n, "
+              "const double* k) {")
+            w("  double h = 0.0;")
+            if heat_terms:
+                w("  const double ev2erg = kbc::eV_to_erg;")
+                w("  const double dd = Hnuclei_(n);")
+                w("  const double ncr = 1.0e6 / std::sqrt(Tgas)")
+                w("      / (1.6 * std::exp(-std::pow(4.0e2 / Tgas, 2.0)) "
+                  "* n[IDX_H] / dd")
+                w("         + 1.4 * std::exp(-1.2e4 / (Tgas + 1.2e3)) "
+                  "* n[IDX_H2] / dd);")
+                w("  const double ffac = 1.0 / (1.0 + ncr / dd);")
+                for q, rx, ff in heat_terms:
+                    prod = "*".join(self.den(r["sp"]) for r in rx["reactants"])
+                    qexpr = "%s*ffac" % q if ff else q
+                    w("  h += k[%d] * (%s) * %s;" % (rx["id"] - 1, qexpr, prod))
+                w("  h *= ev2erg;")
+            w("  return h;")
+            w("}")
+        if th.get("cool_atomic"):
+            rxs = self._recomb_reactions()
+            idx = {rx["id"]: j for j, rx in enumerate(rxs)}
+            nr = max(len(rxs), 1)
+            w("// recombination rates of the ATOMIC cooling and T dk/dT of the")
+            w("// piece active at T (central difference, relative step 1e-4;")
+            w("// 0 where the rate's temperature is clamped)")
+            w("KB_HD inline void recomb_rates_(double Tgas, const double* n, "
+              "const Params& p, double* kr, double* tdk) {")
+            w("  (void)n; (void)p;")
+            w("  const double h = 1e-4;")
+            w("  for (int j = 0; j < %d; ++j) kr[j] = tdk[j] = 0.0;" % len(rxs))
+
+            def body(rx, tv):
+                j = idx[rx["id"]]
+                e = lambda t: self.cx(rx["rate"]["ast"], t)
+                out = ["kr[%d] = %s;" % (j, e(tv))]
+                if tv == "Tgas":
+                    out.append("{ const double Tp_ = Tgas * (1.0 + h), "
+                               "Tm_ = Tgas * (1.0 - h);")
+                else:
+                    out.append("if (%s == Tgas) { const double Tp_ = %s * "
+                               "(1.0 + h), Tm_ = %s * (1.0 - h);"
+                               % (tv, tv, tv))
+                out.append("  tdk[%d] = ((%s) - (%s)) / (2.0 * h); }"
+                           % (j, e("Tp_"), e("Tm_")))
+                return out
+            self.emit_grouped(body, lambda rx: rx["id"] in idx, hoist=False)
+            w("}")
+            w("KB_HD inline double cooling_recomb_(double Tgas, const double* n, "
+              "const Params& p) {")
+            w("  const double T = std::fmin(std::fmax(Tgas, p.Tcmb), 1e9);")
+            w("  double k0[%d], tdk[%d];" % (nr, nr))
+            w("  recomb_rates_(T, n, p, k0, tdk);")
+            w("  double c = 0.0;")
+            for j, rx in enumerate(rxs):
+                ion = [r["sp"] for r in rx["reactants"] if r["sp"] != "e-"][0]
+                w("  c += n[IDX_E] * %s * std::fmax(0.0, 1.5 * k0[%d] + tdk[%d]);"
+                  % (self.den(ion), j, j))
+            w("  return kbc::boltzmann_erg * T * c;")
+            w("}")
+        if th.get("cool_H2"):
+            mode = self.gen.h2_opacity
+            w("KB_HD inline double h2_opacity_(const double* n) {")
+            w("  (void)n;")
+            if mode == "RIPAMONTI":
+                w("  return std::fmin(1.0, std::pow(std::fmax(1.25e-10 * "
+                  "ntot_(n), 1e-40), -0.45));")
+            elif not mode:
+                w("  return 1.0;")
+            else:
+                raise NotImplementedError("h2_opacity %s" % mode)
+            w("}")
+        self.emit_gamma()
+        # dT/dt
+        w("// dTgas/dt at the thermal temperature T (capped to [2.73, 1e9] K by")
+        w("// the caller) with the rates k of the rate temperature")
+        w("KB_HD inline double thermal_dTdt(double T, const double* n, "
+          "const double* k, const Params& p) {")
+        w("  (void)k; (void)p;")
+        w("  double heat = 0.0, cool = 0.0;")
+        heat_order = [("heat_CR", None), ("heat_chem", "heating_chem(T, n, k)"),
+                      ("heat_dH", None),
+                      ("heat_compress", "ntot_(n) * kbc::boltzmann_erg * T / p.tff")]
+        supported = {"heat_chem", "heat_compress"}
+        for f, expr in heat_order:
+            if th.get(f):
+                if f not in supported:
+                    raise NotImplementedError(f)
+                w("  heat += %s;" % expr)
+        for f in ("heat_visc", "heat_photoDust", "heat_netPhotoDust",
+                  "heat_photoAv", "heat_photo", "heat_ZCIE", "heat_nuclear"):
+            if th.get(f):
+                raise NotImplementedError(f)
+        cool_order = [
+            ("cool_atomic", "cooling_Atomic(T, n) + cooling_recomb_(T, n, p)"),
+            ("cool_H2", "cooling_H2(T, n) * h2_opacity_(n)"),
+            ("cool_chem", "cooling_chem(n, k)"),
+            ("cool_cont", "cooling_Continuum(T, n)"),
+        ]
+        for f in ("cool_HD", "cool_mol", "cool_Z", "cool_ZCIE", "cool_Zext",
+                  "cooling_floor", "cool_compton", "cool_CIE", "cool_expansion",
+                  "cool_ff", "cool_dH", "cool_dust", "cool_dustTab",
+                  "cool_dust_bins"):
+            if th.get(f):
+                raise NotImplementedError(f)
+        for f, expr in cool_order:
+            if th.get(f):
+                w("  cool += %s;" % expr)
+        w("  return (gamma_index(T, n, p) - 1.0) * (heat - cool)")
+        w("      / (kbc::boltzmann_erg * ntot_(n));")
+        w("}")
+        w("")
+
+    def emit_gamma(self):
+        """the adiabatic index: CONST (the gamma_ad parameter) or EXACT
+        (reference: kromex/codegen.py:3697-3819)"""
+        w = self.w
+        gen = self.gen
+        mode = gen.gamma
+        if mode == "CONST":
+            w("KB_HD inline double gamma_index(double Tgas, const double* n, "
+              "const Params& p) {")
+            w("  (void)Tgas; (void)n;")
+            w("  return p.gamma_ad;")
+            w("}")
+            return
+        if mode != "EXACT":
+            raise NotImplementedError("gamma %s" % mode)
+        cg = self.cg
+        sp_sorted = self.species
+        mono = [s for s in sp_sorted if gen._natoms(s) == 1]
+        dis = []
+        for s in sp_sorted:
+            if gen._natoms(s) != 2:
+                continue
+            ve, be = cg.GAMMA_VIB_K.get(s), cg.GAMMA_ROT_K.get(s)
+            if ve is None and be is None:
+                continue
+            dis.append((s, ve, be))
+        ves = [ve for _, ve, _ in dis if ve is not None]
+        if any(be is not None for s, _, be in dis if s != "H2"):
+            w("KB_HD inline double gamma_rot_(double Tin, double brot) {")
+            w("  const double ib = brot / std::fmax(Tin, 10.0);")
+            w("  double z = 0.0, e1 = 0.0, e2 = 0.0;")
+            w("KB_UNROLL")
+            w("  for (int j = 0; j <= 10; ++j) {")
+            w("    const double E = j * (j + 1.0) * ib;")
+            w("    const double g = (2.0 * j + 1.0) * std::exp(-E);")
+            w("    z += g; e1 += g * E; e2 += g * E * E;")
+            w("  }")
+            w("  const double m = e1 / z;")
+            w("  return e2 / z - m * m;")
+            w("}")
+        if any(s == "H2" and be is not None for s, _, be in dis):
+            w("KB_HD inline double gamma_rotop_(double Tin, double a) {")
+            w("  const double ib = 85.4 / std::fmax(Tin, 10.0);")
+            w("  double zp = 0.0, p1 = 0.0, p2 = 0.0, zo = 0.0, o1 = 0.0, "
+              "o2 = 0.0;")
+            w("KB_UNROLL")
+            w("  for (int j = 0; j <= 10; j += 2) {")
+            w("    const int j1 = j + 1;")
+            w("    const double Ep = j * (j + 1.0) * ib;")
+            w("    const double Eo = j1 * (j1 + 1.0) * ib;")
+            w("    const double gp = (2.0 * j + 1.0) * std::exp(-Ep);")
+            w("    const double go = 3.0 * (2.0 * j1 + 1.0) * std::exp(-Eo);")
+            w("    zp += gp; p1 += gp * Ep; p2 += gp * Ep * Ep;")
+            w("    zo += go; o1 += go * Eo; o2 += go * Eo * Eo;")
+            w("  }")
+            w("  const double b = 1.0 - a;")
+            w("  const double mp = p1 / zp, mo = o1 / zo;")
+            w("  return b * (p2 / zp - mp * mp) + a * (o2 / zo - mo * mo);")
+            w("}")
+        w("KB_HD inline double gamma_index(double Tgas, const double* n, "
+          "const Params& p) {")
+        w("  (void)Tgas; (void)n; (void)p;")
+        if ves:
+            w("  const double iTv = 1.0 / std::fmax(Tgas, %s);"
+              % self.num(min(ves) * 1e-2))
+        terms = []
+        for s, ve, be in dis:
+            cs = self.cid(s)
+            vpart = "0.0"
+            if ve is not None:
+                w("  const double x_%s = %s * iTv, e_%s = std::exp(x_%s);"
+                  % (cs, self.num(ve), cs, cs))
+                vpart = ("2.0 * x_%s * x_%s * e_%s / ((e_%s - 1.0) * "
+                         "(e_%s - 1.0))" % (cs, cs, cs, cs, cs))
+            rpart = "2.0"
+            if be is not None:
+                rpart = ("2.0 * gamma_rotop_(Tgas, p.opratio / (p.opratio + 1.0))"
+                         if s == "H2"
+                         else "2.0 * gamma_rot_(Tgas, %s)" % self.num(be))
+            w("  const double gi_%s = 0.5 * (3.0 + %s + %s);" % (cs, rpart, vpart))
+            terms.append(cs)
+        w("  const double mosum = %s;"
+          % (" + ".join(self.den(s) for s in mono) or "0.0"))
+        w("  const double ysum = mosum%s;"
+          % "".join(" + n[IDX_%s]" % c for c in terms))
+        w("  const double gsum = 1.5 * mosum%s;"
+          % "".join(" + n[IDX_%s] * gi_%s" % (c, c) for c in terms))
+        w("  return gsum > 0.0 ? 1.0 + ysum / gsum : 5.0 / 3.0;")
+        w("}")
+
+    def emit_tail(self):
+        th = self.gen.thermal
+        any_thermal = any(th.get(f) for f in th if f.startswith(("cool_", "heat_")))
+        self.w("constexpr bool HAS_THERMAL_TERMS = %s;"
+               % ("true" if any_thermal else "false"))
+        self.w("}  // namespace kbnet")
+
+    def run(self):
+        self.emit_head()
+        self.emit_physics()
+        self.emit_vars()
+        self.emit_rates()
+        self.emit_rhs()
+        self.emit_jac()
+        self.emit_thermal()
+        self.emit_tail()
+        return "\n".join(self.lines) + "\n"
+
+
+def emit(key):
+    import json
+    em = Emitter(key, NETWORKS[key])
+    text = em.run()
+    OUTDIR.mkdir(parents=True, exist_ok=True)
+    out = OUTDIR / ("net_%s.h" % key)
+    out.write_text(text)
+    em.meta["nrea_fixed"] = em.nfixed
+    (OUTDIR / ("net_%s.json" % key)).write_text(
+        json.dumps(em.meta, indent=1) + "\n")
+    return out
+
+
+def main(argv):
+    keys = argv or list(NETWORKS)
+    for k in keys:
+        print("wrote", emit(k))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

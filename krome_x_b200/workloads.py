@@ -1,0 +1,134 @@
+"""Seeded synthetic batches of the benchmark workloads.
+
+No dataset is involved: every batch is drawn with ``numpy.random.
+default_rng(seed)`` from the distributions the benchmark names, laid out as
+``krome_solve_cells`` takes them (``n[ncell, nspec]`` cell-major, species in
+the network's code-point order, ``Tgas[ncell]``, ``dt[ncell]``,
+``par[ncell, npar]``).
+
+* ``primordial``   (configs 0 and 2) n_H log-uniform in [1, 1e6] cm^-3,
+  Tgas log-uniform in [10, 1e4] K, H : H+ : e- : He = 1e4 : 1 : 1 : 775 with
+  H = n_H, every other species 1e-20 n_H; dt = 3.15e10 s; tff the free-fall
+  time of the cell (reference runtime/core/query.hpp:176-182).
+* ``primordial3``  (config 1) n_H log-uniform in [1, 1e14], Tgas in
+  [50, 5000] K, x_H2 in [1e-6, 0.5], x_e = x_H+ in [1e-8, 1e-2] (all
+  log-uniform), He/H = 0.0775, H = n_H - 2 n_H2 - n_H+; trace species
+  1e-20 n_H. The hydro loop: per call tff = t_ff(n), every density x 1.01,
+  dt = 0.01 tff (the reference's collapse driver,
+  examples/tests/collapse/test.cpp:47-63).
+* ``galaxy_ism``   (config 4) n_H log-uniform in [1e-2, 1e4], Tgas in
+  [10, 1e6] K, crate in [1e-17, 1e-16], G0 in [0.3, 3], d2g in
+  [0.003, 0.03] (log-uniform, one decade around the typical values);
+  H2 1e-6 n_H, H+ = e- = 1e-4 n_H, He 0.0775 n_H; dt = 3.15e11 s.
+"""
+import numpy as np
+
+GRAVITY = 6.6743e-08
+PI = 3.141592653589793
+
+
+def loguniform(rng, lo, hi, size):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size))
+
+
+def free_fall_time(n, mass_g):
+    """sqrt(3 pi / (32 G rho)) per cell (rho = sum n_i m_i, sequential)"""
+    rho = np.zeros(n.shape[0])
+    for i in range(n.shape[1]):
+        rho = rho + n[:, i] * mass_g[i]
+    return np.sqrt(3.0 * PI / (32.0 * GRAVITY * np.maximum(rho, 1e-40)))
+
+
+def _index(species):
+    return {s: i for i, s in enumerate(species)}
+
+
+def primordial(ncell, info, seed=0):
+    species, mass_g, param_names = info["species"], info["mass_g"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1.0, 1e6, ncell)
+    T = loguniform(rng, 10.0, 1e4, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    n[:, ix["H"]] = nH
+    n[:, ix["H+"]] = nH * 1e-4
+    n[:, ix["e-"]] = nH * 1e-4
+    n[:, ix["He"]] = nH * 0.0775
+    dt = np.full(ncell, 3.15e10)
+    par = _default_rows(ncell, info)
+    par[:, param_names.index("tff")] = free_fall_time(n, mass_g)
+    return n, T, dt, par
+
+
+def primordial3(ncell, info, seed=0):
+    species, mass_g, param_names = info["species"], info["mass_g"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1.0, 1e14, ncell)
+    T = loguniform(rng, 50.0, 5000.0, ncell)
+    xH2 = loguniform(rng, 1e-6, 0.5, ncell)
+    xe = loguniform(rng, 1e-8, 1e-2, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    n[:, ix["H2"]] = xH2 * nH
+    n[:, ix["H+"]] = xe * nH
+    n[:, ix["e-"]] = xe * nH
+    n[:, ix["He"]] = 0.0775 * nH
+    n[:, ix["H"]] = nH - 2.0 * n[:, ix["H2"]] - n[:, ix["H+"]]
+    par = _default_rows(ncell, info)
+    tff = free_fall_time(n, mass_g)
+    par[:, param_names.index("tff")] = tff
+    dt = 0.01 * tff
+    return n, T, dt, par
+
+
+def hydro_step(n, par, mass_g, param_names):
+    """one call of the collapse loop, in place: tff of the current state,
+    densities x 1.01, dt = 0.01 tff (returned)"""
+    tff = free_fall_time(n, mass_g)
+    par[:, param_names.index("tff")] = tff
+    n *= 1.01
+    return 0.01 * tff
+
+
+def galaxy_ism(ncell, info, seed=0):
+    species, mass_g, param_names = info["species"], info["mass_g"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1e-2, 1e4, ncell)
+    T = loguniform(rng, 10.0, 1e6, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    n[:, ix["H"]] = nH
+    n[:, ix["H2"]] = 1e-6 * nH
+    n[:, ix["H+"]] = 1e-4 * nH
+    n[:, ix["e-"]] = 1e-4 * nH
+    n[:, ix["He"]] = 0.0775 * nH
+    par = _default_rows(ncell, info)
+    par[:, param_names.index("crate")] = loguniform(rng, 1e-17, 1e-16, ncell)
+    par[:, param_names.index("G0")] = loguniform(rng, 0.3, 3.0, ncell)
+    par[:, param_names.index("d2g")] = loguniform(rng, 0.003, 0.03, ncell)
+    dt = np.full(ncell, 3.15e11)
+    return n, T, dt, par
+
+
+def _default_rows(ncell, info):
+    """every cell's parameter row at the network defaults (NaN: required)"""
+    return np.repeat(np.asarray(info["defaults"], dtype=float)[None, :],
+                     ncell, axis=0)
+
+
+def hydro_step_info(n, par, info):
+    return hydro_step(n, par, info["mass_g"], info["params"])
+
+
+GENERATORS = {"primordial": primordial, "primordial3": primordial3,
+              "galaxy_ism": galaxy_ism}
+
+# the solve options of each workload (krome_opts keys)
+OPTIONS = {
+    "primordial": dict(evolve_T=1, jac=1, linsol=1, rtol=1e-6, atol_n=1e-20,
+                       atol_T=1e-6),
+    "primordial3": dict(evolve_T=1, jac=0, linsol=0, rtol=1e-6,
+                        atol_n=1e-20, atol_T=1e-6),
+    "galaxy_ism": dict(evolve_T=1, jac=0, linsol=0, rtol=1e-6,
+                       atol_n=1e-20, atol_T=1e-6),
+}

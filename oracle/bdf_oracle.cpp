@@ -1,0 +1,1137 @@
+// CPU ORACLE -- test infrastructure only (the checker, never the product).
+//
+// A serial restatement, in plain C++, of the reference's per-cell stiff
+// solve: the CVODE 7.9 BDF port (reference runtime/core/cvode/
+// bdf_cell.hpp) driven by the per-cell problem of runtime/core/
+// solve_cell.hpp (state layout, rhs with the thermal equation, the JAC_FD
+// and hybrid JAC_ANALYTIC Jacobians, the restart wrapper, the post-solve
+// rules) and the batch rules of runtime/core/solve_cells.hpp. The network
+// math comes from the generated header selected by KB_NET_HEADER (the same
+// scalar form the GPU kernels compile). Every function keeps the
+// reference's operation order, so on the same inputs this file reproduces
+// the reference's strict build (oracle/_ref/libkrome_<net>_strict.so) bit
+// for bit; tests/test_oracle_pin.py checks exactly that.
+//
+// Built by oracle/build.py into oracle/_build/liboracle_<net>.so; only
+// tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include KB_NET_HEADER
+
+using namespace kbnet;
+
+namespace {
+
+// ---- flags (reference runtime/krome.hpp:95-145, bdf_cell.hpp:108-123) ----
+enum : int {
+  SUCCESS = 0, TOO_MUCH_WORK = -1, TOO_MUCH_ACC = -2, ERR_FAILURE = -3,
+  CONV_FAILURE = -4, LSETUP_FAIL = -6, LSOLVE_FAIL = -7, RHSFUNC_FAIL = -8,
+  FIRST_RHSFUNC_ERR = -9, REPTD_RHSFUNC_ERR = -10, UNREC_RHSFUNC_ERR = -11,
+  NLS_FAIL = -16, ILL_INPUT = -22, TOO_CLOSE = -27,
+  FLAG_PARAM_UNSET = -105, FLAG_NONPOSITIVE_T = -110
+};
+// internal flags (bdf_cell.hpp:227-239)
+enum : int {
+  DO_ERROR_TEST = 2, PREDICT_AGAIN = 3, TRY_AGAIN = 5, FIRST_CALL = 6,
+  PREV_CONV_FAIL = 7, PREV_ERR_FAIL = 9, RHSFUNC_RECVR = 10,
+  NLS_CONTINUE = 901, NLS_CONV_RECVR = 902, LS_LUFACT_FAIL = 1
+};
+enum : int { NO_FAILURES = 0, FAIL_BAD_J = 1, FAIL_OTHER = 2 };
+
+// CVODE constants (bdf_cell.hpp:242-272)
+constexpr int QMAX = 5, L_MAX = 6;
+constexpr double HLB_FACTOR = 100.0, HUB_FACTOR = 0.1, H_BIAS = 0.5;
+constexpr int MAX_ITERS = 4;
+constexpr double CORTES = 0.1, ETA_MIN_FX = 0.0, ETA_MAX_FX = 1.5,
+                 ETA_MAX_FS = 10000.0, ETA_MAX_ES = 10.0, ETA_MAX_GS = 10.0,
+                 ETA_MIN = 0.1, ETA_MAX_EF = 0.2, ETA_MIN_EF = 0.1,
+                 ETA_CF = 0.25;
+constexpr long SMALL_NST = 10;
+constexpr int SMALL_NEF = 2;
+constexpr double ONEPSM = 1.000001, ADDON = 1e-6, BIAS1 = 6.0, BIAS2 = 6.0,
+                 BIAS3 = 10.0;
+constexpr int LONG_WAIT = 10, MXNEF1 = 3;
+constexpr long MSBP = 20, MSBJ = 51;
+constexpr double DGMAX_LSETUP = 0.3, DGMAX_JBAD = 0.2, MIN_INC_MULT = 1000.0;
+constexpr int NLS_MAXCOR = 3;
+constexpr double CRDOWN = 0.3, RDIV = 2.0;
+constexpr double UROUND = DBL_EPSILON;
+
+inline double smax_(double a, double b) { return a > b ? a : b; }
+inline double smin_(double a, double b) { return a < b ? a : b; }
+inline double ssqrt_(double x) { return x <= 0.0 ? 0.0 : std::sqrt(x); }
+inline double spowi_(double base, int e) {
+  double prod = 1.0;
+  const int ex = e < 0 ? -e : e;
+  for (int i = 1; i <= ex; i++) prod *= base;
+  if (e < 0) prod = 1.0 / prod;
+  return prod;
+}
+
+// ---- serial N_Vector operations with N_VLinearSum's special cases -------
+// (bdf_cell.hpp:296-400)
+void axpy_(int N, double a, const double* x, double* y) {
+  if (a == 1.0) { for (int i = 0; i < N; i++) y[i] += x[i]; return; }
+  if (a == -1.0) { for (int i = 0; i < N; i++) y[i] -= x[i]; return; }
+  for (int i = 0; i < N; i++) y[i] += a * x[i];
+}
+void lin_sum_(int N, double a, const double* x, double b, const double* y,
+              double* z) {
+  if (b == 1.0 && z == y) { axpy_(N, a, x, z); return; }
+  if (a == 1.0 && z == x) { axpy_(N, b, y, z); return; }
+  if (a == 1.0 && b == 1.0) {
+    for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
+    return;
+  }
+  bool test;
+  if ((test = (a == 1.0 && b == -1.0)) || (a == -1.0 && b == 1.0)) {
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
+    return;
+  }
+  if ((test = (a == 1.0)) || b == 1.0) {
+    const double c = test ? b : a;
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
+    return;
+  }
+  if ((test = (a == -1.0)) || b == -1.0) {
+    const double c = test ? b : a;
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
+    return;
+  }
+  if (a == b) { for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]); return; }
+  if (a == -b) { for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]); return; }
+  for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
+}
+void scale_(int N, double c, const double* x, double* z) {
+  for (int i = 0; i < N; i++) z[i] = c * x[i];
+}
+double wrms_(int N, const double* x, const double* w) {
+  double sum = 0.0;
+  for (int i = 0; i < N; i++) {
+    const double p = x[i] * w[i];
+    sum += p * p;
+  }
+  return ssqrt_(sum / N);
+}
+double max_norm_(int N, const double* x) {
+  double mx = 0.0;
+  for (int i = 0; i < N; i++)
+    if (std::fabs(x[i]) > mx) mx = std::fabs(x[i]);
+  return mx;
+}
+
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457)
+int getrf_(double* a, int n, int* p) {
+  for (int k = 0; k < n; k++) {
+    double* col_k = a + (long)k * n;
+    int l = k;
+    for (int i = k + 1; i < n; i++)
+      if (std::fabs(col_k[i]) > std::fabs(col_k[l])) l = i;
+    p[k] = l;
+    if (col_k[l] == 0.0) return k + 1;
+    if (l != k)
+      for (int i = 0; i < n; i++) {
+        double* ci = a + (long)i * n;
+        const double t = ci[l];
+        ci[l] = ci[k];
+        ci[k] = t;
+      }
+    const double mult = 1.0 / col_k[k];
+    for (int i = k + 1; i < n; i++) col_k[i] *= mult;
+    for (int j = k + 1; j < n; j++) {
+      double* col_j = a + (long)j * n;
+      const double a_kj = col_j[k];
+      if (a_kj != 0.0)
+        for (int i = k + 1; i < n; i++) col_j[i] -= a_kj * col_k[i];
+    }
+  }
+  return 0;
+}
+void getrs_(const double* a, int n, const int* p, double* b) {
+  for (int k = 0; k < n; k++) {
+    const int pk = p[k];
+    if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
+  }
+  for (int k = 0; k < n - 1; k++) {
+    const double* col_k = a + (long)k * n;
+    for (int i = k + 1; i < n; i++) b[i] -= col_k[i] * b[k];
+  }
+  for (int k = n - 1; k > 0; k--) {
+    const double* col_k = a + (long)k * n;
+    b[k] /= col_k[k];
+    for (int i = 0; i < k; i++) b[i] -= col_k[i] * b[k];
+  }
+  b[0] /= a[0];
+}
+
+// ---- the per-cell problem (solve_cell.hpp:438-813, 883-1132) ------------
+struct Problem {
+  Params p;
+  double Tfix = 0.0;
+  int NEQ = NSPEC;
+  int iT = -1;
+  bool hit_T0 = false;
+  bool kfix_on = false;   // fixed Tgas: rates_fixed once per solve
+  double kfix[NREA + 1];
+  bool kT_on = false;     // evolved Tgas: rates_fixed cached per Tgas
+  bool kT_ok = false;
+  double kT_T = 0.0;
+  double kT[NREA + 1];
+  double k[NREA + 1];
+  double k0[NREA + 1], kp[NREA + 1];
+  double fm[NSPEC + 1];
+
+  double state_T(const double* y) const {
+    const double T = iT >= 0 ? y[iT] : Tfix;
+    return std::fmin(std::fmax(T, p.Tcmb), 1e9);
+  }
+  static double thermal_T(double T) { return std::fmin(std::fmax(T, 2.73), 1e9); }
+
+  void eval_rates(double T, const double* y, double* kk) {
+    if (kfix_on) {
+      for (int i = 0; i < NREA; ++i) kk[i] = kfix[i];
+      rates_var(T, y, p, kk);
+    } else if (kT_on) {
+      if (!kT_ok || T != kT_T) {
+        for (int i = 0; i < NREA; ++i) kT[i] = 0.0;
+        rates_fixed(T, y, p, kT);
+        kT_T = T;
+        kT_ok = true;
+      }
+      for (int i = 0; i < NREA; ++i) kk[i] = kT[i];
+      rates_var(T, y, p, kk);
+    } else {
+      for (int i = 0; i < NREA; ++i) kk[i] = 0.0;
+      rates_fixed(T, y, p, kk);
+      rates_var(T, y, p, kk);
+    }
+  }
+  double aux(const double* y, const double* kk) {
+    const double T = thermal_T(iT >= 0 ? y[iT] : Tfix);
+    return thermal_dTdt(T, y, kk, p);
+  }
+  void full_rhs(const double* y, double* f) {
+    const double T = state_T(y);
+    eval_rates(T, y, k);
+    rhs(y, k, f);
+    if (iT >= 0) f[iT] = aux(y, k);
+  }
+  // the integrator's view: T <= 0 or a non-finite f is recoverable
+  int rhs_cb(const double* y, double* f) {
+    if (iT >= 0 && !(y[iT] > 0.0)) { hit_T0 = true; return 1; }
+    full_rhs(y, f);
+    for (int i = 0; i < NEQ; ++i)
+      if (!std::isfinite(f[i])) return 1;
+    return 0;
+  }
+  // fd_step_n_ (solve_cell.hpp:729-733)
+  static double fd_step_n(const double* y, int j) {
+    double s = 0.0;
+    for (int i = 0; i < NSPEC; ++i) s += std::fabs(y[i]);
+    return std::fmax(std::fmax(1e-7 * std::fabs(y[j]), 1e-9 * s), 1e-30);
+  }
+  // JAC_ANALYTIC: stoichiometric block + central-difference Tgas column +
+  // difference-quotient thermal row (jac_assemble_, solve_cell.hpp:883-1118);
+  // J column-major NEQ x NEQ, zeroed by the caller
+  int jac_cb(const double* y, double* J, double* yp, double* fp) {
+    const int N = NEQ;
+    const double T = state_T(y);
+    eval_rates(T, y, k0);
+    jac_stoich(y, k0, J, 1, N);
+    if (iT < 0) return 0;
+    for (int i = 0; i < N; ++i) yp[i] = y[i];
+    {
+      const int col = iT;
+      const double h = std::fmax(1e-6 * std::fabs(y[col]), 1e-8);
+      yp[col] = y[col] + h;
+      full_rhs(yp, fp);
+      yp[col] = y[col] - h;
+      full_rhs(yp, fm);
+      yp[col] = y[col];
+      for (int i = 0; i < N; ++i)
+        J[i + (long)col * N] = (fp[i] - fm[i]) / (2.0 * h);
+    }
+    eval_rates(T, y, k0);
+    const double f0 = aux(y, k0);
+    for (int j = 0; j < NSPEC; ++j) {
+      const double h = fd_step_n(y, j);
+      yp[j] = y[j] + h;
+      eval_rates(T, yp, kp);
+      const double f1 = aux(yp, kp);
+      yp[j] = y[j];
+      J[iT + (long)j * N] = (f1 - f0) / h;
+    }
+    return 0;
+  }
+};
+
+struct Stats {
+  long nst = 0, nfe = 0, nfeDQ = 0, nje = 0, nsetups = 0, nni = 0, nnf = 0,
+       ncfn = 0, netf = 0;
+  void add(const Stats& s) {
+    nst += s.nst; nfe += s.nfe; nfeDQ += s.nfeDQ; nje += s.nje;
+    nsetups += s.nsetups; nni += s.nni; nnf += s.nnf; ncfn += s.ncfn;
+    netf += s.netf;
+  }
+};
+
+struct BdfOpts {
+  double rtol = 1e-4;
+  const double* atol = nullptr;
+  long max_steps = 500;
+  int max_err_fails = 7, max_conv_fails = 10;
+  double h0 = 0.0;
+  bool dq_jac = false;
+  int inv_row = -1, inv_n = 0;
+};
+
+// one cell's CVODE BDF (bdf_cell.hpp:490-1501), unit stride, dense LU
+class Cvode {
+ public:
+  Stats st;
+  Cvode(Problem& prob, int n, const BdfOpts& opts)
+      : P(prob), N(n), o(opts), work((L_MAX + 9) * n + 2 * n * n), piv(n) {
+    double* w = work.data();
+    for (int j = 0; j < L_MAX; j++, w += N) zn[j] = w;
+    ewt = w; w += N;
+    y = w; w += N;
+    acor = w; w += N;
+    tempv = w; w += N;
+    ftemp = w; w += N;
+    delta = w; w += N;
+    vtemp1 = w; w += N;
+    vtemp2 = w; w += N;
+    vtemp3 = w; w += N;
+    A = w; w += (long)N * N;
+    savedJ = w;
+    mxstep = o.max_steps == 0 ? 500 : o.max_steps;
+    double mn = o.atol[0];
+    for (int i = 1; i < N; i++)
+      if (o.atol[i] < mn) mn = o.atol[i];
+    atolmin0 = mn == 0.0;
+  }
+
+  void reinit(double t0, const double* y0, double h_init) {
+    tn = t0;
+    for (int i = 0; i < N; i++) zn[0][i] = y0[i];
+    q = 1; L = 2; qwait = L;
+    etamax = ETA_MAX_FS;
+    qu = 0; hu = 0.0; tolsf = 1.0;
+    st = Stats();
+    nstlp = 0; nscon = 0; h0u = 0.0; next_h = 0.0; next_q = 0;
+    hin = h_init;
+    nstlj = 0;
+    acnrmcur = false; nls_jcur = false; jcur = false;
+    saved_tq5 = 0.0;
+    for (int i = 0; i <= L_MAX; i++) tau[i] = 0.0;
+    eta = 1.0;
+  }
+
+  int solve(double tout, double* yout, double* tret) {
+    int istate = SUCCESS;
+    *tret = tn;
+    {
+      const double tdist = std::fabs(tout - tn);
+      const double tround = UROUND * smax_(std::fabs(tn), std::fabs(tout));
+      if (tdist == 0.0 || tdist < 2.0 * tround) return TOO_CLOSE;
+      if (ewt_set(zn[0], ewt) != 0) return ILL_INPUT;
+      const int retval = P.rhs_cb(zn[0], zn[1]);
+      st.nfe++;
+      if (retval < 0) return RHSFUNC_FAIL;
+      if (retval > 0) return FIRST_RHSFUNC_ERR;
+      h = hin;
+      if (h != 0.0 && (tout - tn) * h < 0.0) return ILL_INPUT;
+      if (h == 0.0) {
+        const int hflag = hin_(tout);
+        if (hflag != SUCCESS) return hflag;
+      }
+      // hmax_inv = 0, hmin = 0 (CVODE defaults)
+      hscale = h;
+      h0u = h;
+      hprime = h;
+      scale_(N, h, zn[1], zn[1]);
+    }
+    long nstloc = 0;
+    for (;;) {
+      next_h = h;
+      next_q = q;
+      if (st.nst > 0 && ewt_set(zn[0], ewt) != 0) {
+        istate = ILL_INPUT; *tret = tn; copy_(zn[0], yout); break;
+      }
+      if (mxstep > 0 && nstloc >= mxstep) {
+        istate = TOO_MUCH_WORK; *tret = tn; copy_(zn[0], yout); break;
+      }
+      const double nrm = wrms_(N, zn[0], ewt);
+      tolsf = UROUND * nrm;
+      if (tolsf > 1.0) {
+        istate = TOO_MUCH_ACC; *tret = tn; copy_(zn[0], yout);
+        tolsf *= 2.0;
+        break;
+      }
+      tolsf = 1.0;
+      const int kflag = step_();
+      if (kflag != SUCCESS) {
+        istate = kflag; *tret = tn; copy_(zn[0], yout); break;
+      }
+      nstloc++;
+      if ((tn - tout) * h >= 0.0) {
+        istate = SUCCESS;
+        *tret = tout;
+        get_dky_(tout, yout);
+        next_q = qprime;
+        next_h = hprime;
+        break;
+      }
+    }
+    return istate;
+  }
+  double current_step() const { return next_h; }
+
+ private:
+  Problem& P;
+  const int N;
+  const BdfOpts o;
+  std::vector<double> work;
+  std::vector<int> piv;
+  long mxstep;
+  bool atolmin0;
+  double* zn[L_MAX];
+  double *ewt, *y, *acor, *tempv, *ftemp, *delta, *vtemp1, *vtemp2, *vtemp3;
+  double *A, *savedJ;
+  double tn = 0.0, h = 0.0, hin = 0.0, hprime = 0.0, hscale = 0.0, h0u = 0.0;
+  double next_h = 0.0, hu = 0.0, eta = 1.0, etamax = 0.0, etaq = 0.0;
+  double etaqm1 = 0.0, etaqp1 = 0.0, tolsf = 1.0, saved_tq5 = 0.0;
+  double tau[L_MAX + 1] = {}, tq[6] = {}, l[L_MAX] = {};
+  double rl1 = 0.0, gamma = 0.0, gammap = 0.0, gamrat = 0.0;
+  double crate = 0.0, delp = 0.0, delnrm = 0.0, acnrm = 0.0;
+  int q = 1, qprime = 1, next_q = 0, qu = 0, L = 2, qwait = 2;
+  long nscon = 0, nstlp = 0, nstlj = 0;
+  int convfail = 0;
+  bool acnrmcur = false, jcur = false, nls_jcur = false;
+
+  void copy_(const double* x, double* z) const {
+    for (int i = 0; i < N; i++) z[i] = x[i];
+  }
+  // cvEwtSetSV (bdf_cell.hpp:689-713)
+  int ewt_set(const double* ycur, double* weight) {
+    for (int i = 0; i < N; i++) weight[i] = std::fabs(ycur[i]);
+    for (int i = 0; i < N; i++) weight[i] = (o.rtol * weight[i]) + o.atol[i];
+    if (atolmin0) {
+      double mn = weight[0];
+      for (int i = 1; i < N; i++)
+        if (weight[i] < mn) mn = weight[i];
+      if (mn <= 0.0) return -1;
+    }
+    for (int i = 0; i < N; i++) weight[i] = 1.0 / weight[i];
+    return 0;
+  }
+  // cvHin, cvUpperBoundH0, cvYddNorm (bdf_cell.hpp:717-794)
+  int hin_(double tout) {
+    const double tdiff = tout - tn;
+    const int sign = (tdiff > 0.0) ? 1 : -1;
+    const double tdist = std::fabs(tdiff);
+    const double tround = UROUND * smax_(std::fabs(tn), std::fabs(tout));
+    const double hlb = HLB_FACTOR * tround;
+    const double hub = upper_bound_h0_(tdist);
+    double hg = ssqrt_(hlb * hub);
+    if (hub < hlb) {
+      h = sign == -1 ? -hg : hg;
+      return SUCCESS;
+    }
+    double hs = hg, hnew = hg, yddnrm = 0.0;
+    for (int count1 = 1; count1 <= MAX_ITERS; count1++) {
+      bool hgOK = false;
+      for (int count2 = 1; count2 <= MAX_ITERS; count2++) {
+        const double hgs = hg * sign;
+        const int retval = ydd_norm_(hgs, &yddnrm);
+        if (retval < 0) return RHSFUNC_FAIL;
+        if (retval == SUCCESS) { hgOK = true; break; }
+        hg *= 0.2;
+      }
+      if (!hgOK) {
+        if (count1 <= 2) return REPTD_RHSFUNC_ERR;
+        hnew = hs;
+        break;
+      }
+      hs = hg;
+      hnew = (yddnrm * hub * hub > 2.0) ? ssqrt_(2.0 / yddnrm)
+                                         : ssqrt_(hg * hub);
+      if (count1 == MAX_ITERS) break;
+      const double hrat = hnew / hg;
+      if ((hrat > 0.5) && (hrat < 2.0)) break;
+      if ((count1 > 1) && (hrat > 2.0)) { hnew = hg; break; }
+      hg = hnew;
+    }
+    double h0 = H_BIAS * hnew;
+    if (h0 < hlb) h0 = hlb;
+    if (h0 > hub) h0 = hub;
+    if (sign == -1) h0 = -h0;
+    h = h0;
+    return SUCCESS;
+  }
+  double upper_bound_h0_(double tdist) {
+    double* temp1 = tempv;
+    double* temp2 = acor;
+    for (int i = 0; i < N; i++) temp2[i] = std::fabs(zn[0][i]);
+    ewt_set(zn[0], temp1);
+    for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
+    lin_sum_(N, HUB_FACTOR, temp2, 1.0, temp1, temp1);
+    for (int i = 0; i < N; i++) temp2[i] = std::fabs(zn[1][i]);
+    for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
+    const double hub_inv = max_norm_(N, temp1);
+    double hub = HUB_FACTOR * tdist;
+    if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
+    return hub;
+  }
+  int ydd_norm_(double hg, double* yddnrm) {
+    lin_sum_(N, hg, zn[1], 1.0, zn[0], y);
+    const int retval = P.rhs_cb(y, tempv);
+    st.nfe++;
+    if (retval < 0) return RHSFUNC_FAIL;
+    if (retval > 0) return RHSFUNC_RECVR;
+    lin_sum_(N, 1.0 / hg, tempv, -1.0 / hg, zn[1], tempv);
+    *yddnrm = wrms_(N, tempv, ewt);
+    return SUCCESS;
+  }
+  // cvStep (bdf_cell.hpp:798-822)
+  int step_() {
+    int ncf = 0, nef = 0;
+    double dsm = 0.0;
+    if (st.nst > 0 && hprime != h) adjust_params_();
+    const double saved_t = tn;
+    int nflag = FIRST_CALL;
+    for (;;) {
+      predict_();
+      set_();
+      nflag = nls_(nflag);
+      const int kflag = handle_nflag_(&nflag, saved_t, &ncf);
+      if (kflag == PREDICT_AGAIN) continue;
+      if (kflag != DO_ERROR_TEST) return kflag;
+      const int eflag = do_error_test_(&nflag, saved_t, &nef, &dsm);
+      if (eflag == TRY_AGAIN) continue;
+      if (eflag != SUCCESS) return eflag;
+      break;
+    }
+    complete_step_();
+    prepare_next_step_(dsm);
+    etamax = (st.nst <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
+    scale_(N, tq[2], acor, acor);
+    return SUCCESS;
+  }
+  void adjust_params_() {
+    if (qprime != q) {
+      adjust_order_(qprime - q);
+      q = qprime;
+      L = q + 1;
+      qwait = L;
+    }
+    rescale_();
+  }
+  void adjust_order_(int deltaq) {
+    if ((q == 2) && (deltaq != 1)) return;
+    if (deltaq == 1) increase_bdf_();
+    else if (deltaq == -1) decrease_bdf_();
+  }
+  void increase_bdf_() {
+    for (int i = 0; i <= QMAX; i++) l[i] = 0.0;
+    double alpha1, prod, xiold, alpha0;
+    l[2] = alpha1 = prod = xiold = 1.0;
+    alpha0 = -1.0;
+    double hsum = hscale;
+    if (q > 1)
+      for (int j = 1; j < q; j++) {
+        hsum += tau[j + 1];
+        const double xi = hsum / hscale;
+        prod *= xi;
+        alpha0 -= 1.0 / (j + 1);
+        alpha1 += 1.0 / xi;
+        for (int i = j + 2; i >= 2; i--) l[i] = l[i] * xiold + l[i - 1];
+        xiold = xi;
+      }
+    const double A1 = (-alpha0 - alpha1) / prod;
+    scale_(N, A1, zn[QMAX], zn[L]);
+    if (q > 1)
+      for (int j = 2; j <= q; j++) axpy_(N, l[j], zn[L], zn[j]);
+  }
+  void decrease_bdf_() {
+    for (int i = 0; i <= QMAX; i++) l[i] = 0.0;
+    l[2] = 1.0;
+    double hsum = 0.0;
+    for (int j = 1; j <= q - 2; j++) {
+      hsum += tau[j];
+      const double xi = hsum / hscale;
+      for (int i = j + 2; i >= 2; i--) l[i] = l[i] * xi + l[i - 1];
+    }
+    if (q > 2)
+      for (int j = 2; j < q; j++) axpy_(N, -l[j], zn[q], zn[j]);
+  }
+  void rescale_() {
+    double c = eta;
+    for (int j = 1; j <= q; j++) {
+      scale_(N, c, zn[j], zn[j]);
+      c = eta * c;
+    }
+    h = hscale * eta;
+    next_h = h;
+    hscale = h;
+    nscon = 0;
+  }
+  void predict_() {
+    tn += h;
+    for (int k = 1; k <= q; k++)
+      for (int j = q; j >= k; j--) axpy_(N, 1.0, zn[j], zn[j - 1]);
+  }
+  void restore_(double saved_t) {
+    tn = saved_t;
+    for (int k = 1; k <= q; k++)
+      for (int j = q; j >= k; j--) axpy_(N, -1.0, zn[j], zn[j - 1]);
+  }
+  // cvSet, cvSetBDF, cvSetTqBDF (bdf_cell.hpp:903-954)
+  void set_() {
+    double xi_inv, xistar_inv, alpha0, alpha0_hat;
+    l[0] = l[1] = xi_inv = xistar_inv = 1.0;
+    for (int i = 2; i <= q; i++) l[i] = 0.0;
+    alpha0 = alpha0_hat = -1.0;
+    double hsum = h;
+    if (q > 1) {
+      for (int j = 2; j < q; j++) {
+        hsum += tau[j - 1];
+        xi_inv = h / hsum;
+        alpha0 -= 1.0 / j;
+        for (int i = j; i >= 1; i--) l[i] += l[i - 1] * xi_inv;
+      }
+      alpha0 -= 1.0 / q;
+      xistar_inv = -l[1] - alpha0;
+      hsum += tau[q - 1];
+      xi_inv = h / hsum;
+      alpha0_hat = -l[1] - xi_inv;
+      for (int i = q; i >= 1; i--) l[i] += l[i - 1] * xistar_inv;
+    }
+    set_tq_bdf_(hsum, alpha0, alpha0_hat, xi_inv, xistar_inv);
+    rl1 = 1.0 / l[1];
+    gamma = h * rl1;
+    if (st.nst == 0) gammap = gamma;
+    gamrat = (st.nst > 0) ? gamma / gammap : 1.0;
+  }
+  void set_tq_bdf_(double hsum, double alpha0, double alpha0_hat,
+                   double xi_inv, double xistar_inv) {
+    const double A1 = 1.0 - alpha0_hat + alpha0;
+    const double A2 = 1.0 + q * A1;
+    tq[2] = std::fabs(A1 / (alpha0 * A2));
+    tq[5] = std::fabs(A2 * xistar_inv / (l[q] * xi_inv));
+    if (qwait == 1) {
+      if (q > 1) {
+        const double C = xistar_inv / l[q];
+        const double A3 = alpha0 + 1.0 / q;
+        const double A4 = alpha0_hat + xi_inv;
+        const double Cpinv = (1.0 - A4 + A3) / A3;
+        tq[1] = std::fabs(C * Cpinv);
+      } else {
+        tq[1] = 1.0;
+      }
+      hsum += tau[q];
+      xi_inv = h / hsum;
+      const double A5 = alpha0 - (1.0 / (q + 1));
+      const double A6 = alpha0_hat - xi_inv;
+      const double Cppinv = (1.0 - A6 + A5) / A2;
+      tq[3] = std::fabs(Cppinv / (xi_inv * (q + 2) * A5));
+    }
+    tq[4] = CORTES / tq[2];
+  }
+  // the charge invariant of the Newton correction (bdf_cell.hpp:1266-1287)
+  double inv_dot_(const double* x) const {
+    double s = 0.0;
+    for (int i = 0; i < o.inv_n; i++)
+      if (species_charge(i) != 0) s += species_charge(i) * x[i];
+    return s;
+  }
+  void inv_set_(double* x, double target) const {
+    const int r = o.inv_row;
+    double s = 0.0, sa = 0.0;
+    for (int i = 0; i < o.inv_n; i++)
+      if (i != r && species_charge(i) != 0) {
+        s += species_charge(i) * x[i];
+        sa += std::fabs(species_charge(i) * (zn[0][i] + acor[i]));
+      }
+    const double yr = zn[0][r] + acor[r];
+    const double xr = (target - s) / species_charge(r);
+    if (std::fabs(species_charge(r) * yr) >= 1e-6 * sa && yr + xr >= 0.0)
+      x[r] = xr;
+  }
+  // cvNls + the Newton module (bdf_cell.hpp:958-1048)
+  int nls_(int nflag) {
+    convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL))
+                   ? NO_FAILURES : FAIL_OTHER;
+    bool callSetup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL)
+                     || (st.nst == 0) || (st.nst >= nstlp + MSBP)
+                     || (std::fabs(gamrat - 1.0) > DGMAX_LSETUP);
+    for (int i = 0; i < N; i++) acor[i] = 0.0;
+    const double tol = tq[4];
+    bool jbad = false;
+    long niters = 0, nconvfails = 0;
+    int retval;
+    for (;;) {
+      int curiter = 0;
+      retval = residual_();
+      if (retval != SUCCESS) break;
+      if (callSetup) {
+        retval = nls_lsetup_(jbad, &nls_jcur);
+        if (retval != SUCCESS) break;
+      }
+      for (;;) {
+        niters++;
+        const bool inv = o.dq_jac && o.inv_row >= 0;
+        const double cg = inv ? inv_dot_(delta) : 0.0;
+        scale_(N, -1.0, delta, delta);
+        retval = lsolve_(delta);
+        if (retval != SUCCESS) break;
+        if (inv) inv_set_(delta, -cg);
+        lin_sum_(N, 1.0, acor, 1.0, delta, acor);
+        retval = conv_test_(curiter, tol);
+        curiter++;
+        if (retval == SUCCESS) { nls_jcur = false; break; }
+        if (retval != NLS_CONTINUE) break;
+        if (curiter >= NLS_MAXCOR) { retval = NLS_CONV_RECVR; break; }
+        retval = residual_();
+        if (retval != SUCCESS) break;
+      }
+      if (retval == SUCCESS) break;
+      if ((retval > 0) && !nls_jcur) {
+        nconvfails++;
+        callSetup = true;
+        jbad = true;
+        for (int i = 0; i < N; i++) acor[i] = 0.0;
+        continue;
+      }
+      break;
+    }
+    if (retval != SUCCESS) nconvfails++;
+    st.nni += niters;
+    st.nnf += nconvfails;
+    if (retval != SUCCESS) return retval;
+    lin_sum_(N, 1.0, zn[0], 1.0, acor, y);
+    if (!acnrmcur) acnrm = wrms_(N, acor, ewt);
+    jcur = false;
+    return SUCCESS;
+  }
+  int residual_() {
+    lin_sum_(N, 1.0, zn[0], 1.0, acor, y);
+    const int retval = P.rhs_cb(y, ftemp);
+    st.nfe++;
+    if (retval < 0) return RHSFUNC_FAIL;
+    if (retval > 0) return RHSFUNC_RECVR;
+    lin_sum_(N, rl1, zn[1], 1.0, acor, delta);
+    lin_sum_(N, -gamma, ftemp, 1.0, delta, delta);
+    return SUCCESS;
+  }
+  int conv_test_(int m, double tol) {
+    delnrm = wrms_(N, delta, ewt);
+    if (m > 0) crate = smax_(CRDOWN * crate, delnrm / delp);
+    const double dcon = delnrm * smin_(1.0, crate) / tol;
+    if (dcon <= 1.0) {
+      acnrm = (m == 0) ? delnrm : wrms_(N, acor, ewt);
+      acnrmcur = true;
+      return SUCCESS;
+    }
+    if ((m >= 1) && (delnrm > RDIV * delp)) return NLS_CONV_RECVR;
+    delp = delnrm;
+    return NLS_CONTINUE;
+  }
+  int nls_lsetup_(bool jbad, bool* jcur_out) {
+    if (jbad) convfail = FAIL_BAD_J;
+    const int retval = ls_setup_();
+    st.nsetups++;
+    *jcur_out = jcur;
+    gamrat = 1.0;
+    gammap = gamma;
+    crate = 1.0;
+    delnrm = 0.0;
+    nstlp = st.nst;
+    if (retval < 0) return LSETUP_FAIL;
+    if (retval > 0) return NLS_CONV_RECVR;
+    return SUCCESS;
+  }
+  // cvLsSetup + A = I - gamma J + dense LU (bdf_cell.hpp:1069-1130)
+  int ls_setup_() {
+    const long NN = (long)N * N;
+    const double dgamma = std::fabs((gamma / gammap) - 1.0);
+    const bool jbad_ls = (st.nst == 0) || (st.nst >= nstlj + MSBJ)
+                         || ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
+                         || (convfail == FAIL_OTHER);
+    int retval = 0;
+    if (!jbad_ls) {
+      jcur = false;
+    } else {
+      jcur = true;
+      if (!o.dq_jac)
+        for (long k = 0; k < NN; k++) savedJ[k] = 0.0;
+      const int jr = o.dq_jac ? dq_jac_(tn, y, ftemp, savedJ, vtemp1)
+                              : P.jac_cb(y, savedJ, vtemp1, vtemp2);
+      if (jr < 0) retval = -1;
+      else if (jr > 0) retval = 1;
+    }
+    if (retval == 0) {
+      const double c = -gamma;
+      for (int j = 0; j < N; j++) {
+        for (int i = 0; i < N; i++) {
+          const long k = i + (long)j * N;
+          A[k] = savedJ[k] * c;
+        }
+        A[j + (long)j * N] += 1.0;
+      }
+    }
+    if (jcur) {
+      st.nje++;
+      nstlj = st.nst;
+    }
+    if (retval != 0) return retval;
+    return getrf_(A, N, piv.data()) > 0 ? LS_LUFACT_FAIL : 0;
+  }
+  int lsolve_(double* b) {
+    getrs_(A, N, piv.data(), b);
+    if (gamrat != 1.0) scale_(N, 2.0 / (1.0 + gamrat), b, b);
+    return SUCCESS;
+  }
+  // cvLsDenseDQJac (bdf_cell.hpp:1290-1311)
+  int dq_jac_(double t, double* yv, const double* fy, double* Jac,
+              double* tmp1) {
+    (void)t;
+    double* ftmp = tmp1;
+    const double srur = ssqrt_(UROUND);
+    const double fnorm = wrms_(N, fy, ewt);
+    const double minInc = (fnorm != 0.0)
+        ? (MIN_INC_MULT * std::fabs(h) * UROUND * (double)N * fnorm) : 1.0;
+    int retval = 0;
+    for (int j = 0; j < N; j++) {
+      const double yjsaved = yv[j];
+      const double inc = smax_(srur * std::fabs(yjsaved), minInc / ewt[j]);
+      yv[j] += inc;
+      retval = P.rhs_cb(yv, ftmp);
+      st.nfeDQ++;
+      if (retval != 0) break;
+      yv[j] = yjsaved;
+      const double inc_inv = 1.0 / inc;
+      lin_sum_(N, inc_inv, ftmp, -inc_inv, fy, Jac + (long)j * N);
+    }
+    return retval;
+  }
+  int handle_nflag_(int* nflagPtr, double saved_t, int* ncfPtr) {
+    const int nflag = *nflagPtr;
+    if (nflag == SUCCESS) return DO_ERROR_TEST;
+    st.ncfn++;
+    restore_(saved_t);
+    if (nflag < 0) {
+      if (nflag == LSETUP_FAIL) return LSETUP_FAIL;
+      if (nflag == LSOLVE_FAIL) return LSOLVE_FAIL;
+      if (nflag == RHSFUNC_FAIL) return RHSFUNC_FAIL;
+      return NLS_FAIL;
+    }
+    (*ncfPtr)++;
+    etamax = 1.0;
+    if ((std::fabs(h) <= 0.0 * ONEPSM) || (*ncfPtr == o.max_conv_fails)) {
+      if (nflag == NLS_CONV_RECVR) return CONV_FAILURE;
+      if (nflag == RHSFUNC_RECVR) return REPTD_RHSFUNC_ERR;
+    }
+    eta = smax_(ETA_CF, 0.0 / std::fabs(h));
+    *nflagPtr = PREV_CONV_FAIL;
+    rescale_();
+    return PREDICT_AGAIN;
+  }
+  int do_error_test_(int* nflagPtr, double saved_t, int* nefPtr,
+                     double* dsmPtr) {
+    const double dsm = acnrm * tq[2];
+    *dsmPtr = dsm;
+    if (dsm <= 1.0) return SUCCESS;
+    (*nefPtr)++;
+    st.netf++;
+    *nflagPtr = PREV_ERR_FAIL;
+    restore_(saved_t);
+    if ((std::fabs(h) <= 0.0 * ONEPSM) || (*nefPtr == o.max_err_fails))
+      return ERR_FAILURE;
+    etamax = 1.0;
+    if (*nefPtr <= MXNEF1) {
+      eta = 1.0 / (std::pow(BIAS2 * dsm, 1.0 / L) + ADDON);
+      eta = smax_(ETA_MIN_EF, smax_(eta, 0.0 / std::fabs(h)));
+      if (*nefPtr >= SMALL_NEF) eta = smin_(eta, ETA_MAX_EF);
+      rescale_();
+      return TRY_AGAIN;
+    }
+    if (q > 1) {
+      eta = smax_(ETA_MIN_EF, 0.0 / std::fabs(h));
+      adjust_order_(-1);
+      L = q;
+      q--;
+      qwait = L;
+      rescale_();
+      return TRY_AGAIN;
+    }
+    eta = smax_(ETA_MIN_EF, 0.0 / std::fabs(h));
+    h *= eta;
+    next_h = h;
+    hscale = h;
+    qwait = LONG_WAIT;
+    nscon = 0;
+    const int retval = P.rhs_cb(zn[0], tempv);
+    st.nfe++;
+    if (retval < 0) return RHSFUNC_FAIL;
+    if (retval > 0) return UNREC_RHSFUNC_ERR;
+    scale_(N, h, tempv, zn[1]);
+    return TRY_AGAIN;
+  }
+  void complete_step_() {
+    st.nst++;
+    nscon++;
+    hu = h;
+    qu = q;
+    for (int i = q; i >= 2; i--) tau[i] = tau[i - 1];
+    if ((q == 1) && (st.nst > 1)) tau[2] = tau[1];
+    tau[1] = h;
+    for (int j = 0; j <= q; j++) axpy_(N, l[j], acor, zn[j]);
+    qwait--;
+    if ((qwait == 1) && (q != QMAX)) {
+      copy_(acor, zn[QMAX]);
+      saved_tq5 = tq[5];
+    }
+  }
+  void prepare_next_step_(double dsm) {
+    if (etamax == 1.0) {
+      qwait = qwait > 2 ? qwait : 2;
+      qprime = q;
+      hprime = h;
+      eta = 1.0;
+      return;
+    }
+    etaq = 1.0 / (std::pow(BIAS2 * dsm, 1.0 / L) + ADDON);
+    if (qwait != 0) {
+      eta = etaq;
+      qprime = q;
+      set_eta_();
+    } else {
+      qwait = 2;
+      etaqm1 = compute_etaqm1_();
+      etaqp1 = compute_etaqp1_();
+      choose_eta_();
+      set_eta_();
+    }
+  }
+  void set_eta_() {
+    if ((eta > ETA_MIN_FX) && (eta < ETA_MAX_FX)) {
+      eta = 1.0;
+      hprime = h;
+      return;
+    }
+    if (eta >= ETA_MAX_FX) {
+      eta = smin_(eta, etamax);
+      eta /= smax_(1.0, std::fabs(h) * 0.0 * eta);
+    } else {
+      eta = smax_(eta, ETA_MIN);
+      eta = smax_(eta, 0.0 / std::fabs(h));
+    }
+    hprime = h * eta;
+    if (qprime < q) nscon = 0;
+  }
+  double compute_etaqm1_() {
+    etaqm1 = 0.0;
+    if (q > 1) {
+      const double ddn = wrms_(N, zn[q], ewt) * tq[1];
+      etaqm1 = 1.0 / (std::pow(BIAS1 * ddn, 1.0 / q) + ADDON);
+    }
+    return etaqm1;
+  }
+  double compute_etaqp1_() {
+    etaqp1 = 0.0;
+    if (q != QMAX) {
+      if (saved_tq5 == 0.0) return etaqp1;
+      const double cquot = (tq[5] / saved_tq5) * spowi_(h / tau[2], L);
+      lin_sum_(N, -cquot, zn[QMAX], 1.0, acor, tempv);
+      const double dup = wrms_(N, tempv, ewt) * tq[3];
+      etaqp1 = 1.0 / (std::pow(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
+    }
+    return etaqp1;
+  }
+  void choose_eta_() {
+    const double etam = smax_(etaqm1, smax_(etaq, etaqp1));
+    if ((etam > ETA_MIN_FX) && (etam < ETA_MAX_FX)) {
+      eta = 1.0;
+      qprime = q;
+      return;
+    }
+    if (etam == etaq) {
+      eta = etaq;
+      qprime = q;
+    } else if (etam == etaqm1) {
+      eta = etaqm1;
+      qprime = q - 1;
+    } else {
+      eta = etaqp1;
+      qprime = q + 1;
+      copy_(acor, zn[QMAX]);
+    }
+  }
+  void get_dky_(double t, double* dky) {
+    const double s = (t - tn) / h;
+    for (int j = q; j >= 0; j--) {
+      double c = 1.0;
+      for (int i = 0; i < j; i++) c *= s;
+      if (j == q) scale_(N, c, zn[j], dky);
+      else axpy_(N, c, zn[j], dky);
+    }
+  }
+};
+
+}  // namespace
+
+// the solve options of one call (the krome_opts keys the hot path reads;
+// reference runtime/krome.hpp:187-254)
+struct oracle_opts {
+  int evolve_T;
+  int jac;      // 0 auto, 1 analytic, 2 difference quotients
+  double rtol, atol_n, atol_T;
+  long max_steps;
+  int max_err_fails, max_conv_fails, max_restarts;
+  int clip_negative;
+};
+
+// per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf, restarts
+constexpr int ORACLE_NSTAT = 9;
+
+#define ORACLE_API __attribute__((visibility("default")))
+
+extern "C" {
+
+ORACLE_API int oracle_nspec(void) { return NSPEC; }
+ORACLE_API int oracle_npar(void) { return NPAR; }
+ORACLE_API const char* oracle_network(void) { return NETWORK_KEY; }
+
+// one cell (solve_cell.hpp:2094-2203 with integrate_ 1662-1705 and the
+// restart wrapper bdf_cell.hpp:1513-1547); n, Tgas in/out
+ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, double dt,
+                     const oracle_opts* so, long* stats) {
+  Problem c;
+  params_from_row(par, c.p);
+  if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
+  c.Tfix = *Tgas;
+  c.NEQ = NSPEC;
+  if (so->evolve_T) c.iT = c.NEQ++;
+  const int N = c.NEQ;
+  std::vector<double> y(N), avec(N);
+  for (int i = 0; i < NSPEC; ++i) y[i] = n[i];
+  if (c.iT >= 0) y[c.iT] = *Tgas;
+  if (NREA_FIXED > 0) {
+    if (c.iT < 0) {
+      for (int i = 0; i <= NREA; ++i) c.kfix[i] = 0.0;
+      rates_fixed(c.state_T(n), n, c.p, c.kfix);
+      c.kfix_on = true;
+    } else {
+      c.kT_on = true;
+      c.kT_ok = false;
+    }
+  }
+  for (int i = 0; i < NSPEC; ++i) avec[i] = so->atol_n;
+  if (c.iT >= 0) avec[c.iT] = so->atol_T;
+  const int jac = so->jac != 0 ? so->jac : (so->evolve_T ? 2 : 1);
+  BdfOpts bo;
+  bo.rtol = so->rtol;
+  bo.atol = avec.data();
+  bo.max_steps = so->max_steps;
+  bo.max_err_fails = so->max_err_fails;
+  bo.max_conv_fails = so->max_conv_fails;
+  bo.dq_jac = jac == 2;
+  if (IDX_ELECTRON >= 0) {  // charge_newton_ (solve_cell.hpp:1631-1642)
+    bo.inv_row = IDX_ELECTRON;
+    bo.inv_n = NSPEC;
+  }
+  Stats bs;
+  int restarts = 0;
+  int flag;
+  {
+    Cvode cv(c, N, bo);
+    cv.reinit(0.0, y.data(), bo.h0);
+    double t = 0.0;
+    for (;;) {
+      const int f = cv.solve(dt, y.data(), &t);
+      bs.add(cv.st);
+      if (f >= 0) { flag = 0; break; }
+      const bool restartable = f == ERR_FAILURE || f == CONV_FAILURE
+                               || f == REPTD_RHSFUNC_ERR;
+      if (!restartable || restarts >= so->max_restarts) { flag = f; break; }
+      ++restarts;
+      const double hcur = cv.current_step();
+      cv.reinit(t, y.data(), hcur > 0.0 ? 0.1 * hcur : 0.0);
+    }
+  }
+  if (stats != nullptr) {
+    const long s[ORACLE_NSTAT] = {bs.nst, bs.nfe, bs.nfeDQ, bs.nje,
+                                  bs.nsetups, bs.nni, bs.nnf, bs.netf,
+                                  (long)restarts};
+    for (int i = 0; i < ORACLE_NSTAT; ++i) stats[i] = s[i];
+  }
+  if (flag == 0 && c.iT >= 0 && !(y[c.iT] > 0.0 && std::isfinite(y[c.iT])))
+    flag = FLAG_NONPOSITIVE_T;
+  if (c.hit_T0 && (flag == REPTD_RHSFUNC_ERR || flag == RHSFUNC_FAIL
+                   || flag == UNREC_RHSFUNC_ERR || flag == FIRST_RHSFUNC_ERR))
+    flag = FLAG_NONPOSITIVE_T;
+  if (flag == 0) {
+    for (int i = 0; i < NSPEC; ++i) {
+      n[i] = y[i];
+      if (so->clip_negative && n[i] < 0.0) n[i] = 0.0;
+    }
+    if (c.iT >= 0) *Tgas = y[c.iT];
+  }
+  return flag;
+}
+
+// many cells (solve_cells.hpp:47-161): the required-parameter rule over
+// every cell first, then each cell with dt > 0; the returned flag is the
+// lowest-index failing cell's. par: one row (par_stride 0) or rows.
+ORACLE_API int oracle_solve_cells(int ncell, double* n, double* Tgas, const double* dt,
+                       const double* par, int par_stride, int* flags,
+                       const oracle_opts* so, long* stats, int nthreads) {
+  if (ncell < 0 || n == nullptr || Tgas == nullptr || dt == nullptr
+      || so == nullptr)
+    return -1;
+  if (par_stride != 0 && par_stride != NPAR) return -1;
+  std::vector<double> dflt(NPAR);
+  for (int i = 0; i < NPAR; ++i) dflt[i] = param_default(i);
+  const double* P = par != nullptr ? par : dflt.data();
+  const int ps = par != nullptr ? par_stride : 0;
+  bool missing = false;
+  for (int c = 0; c < ncell; ++c) {
+    Params pc;
+    params_from_row(P + (long)c * ps, pc);
+    const bool m = params_missing(pc) >= 0;
+    if (flags != nullptr) flags[c] = m ? FLAG_PARAM_UNSET : 0;
+    missing |= m;
+  }
+  if (missing) return FLAG_PARAM_UNSET;
+  std::vector<int> fl(ncell > 0 ? ncell : 1, 0);
+  (void)nthreads;
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int c = 0; c < ncell; ++c) {
+    long* sc = stats != nullptr ? stats + (long)c * ORACLE_NSTAT : nullptr;
+    if (dt[c] > 0.0) {
+      fl[c] = oracle_solve_one(n + (long)c * NSPEC, Tgas + c,
+                               P + (long)c * ps, dt[c], so, sc);
+    } else {
+      fl[c] = 0;
+      if (sc != nullptr)
+        for (int i = 0; i < ORACLE_NSTAT; ++i) sc[i] = 0;
+    }
+  }
+  int first = 0;
+  for (int c = 0; c < ncell; ++c) {
+    if (flags != nullptr) flags[c] = fl[c];
+    if (first == 0) first = fl[c];
+  }
+  return first;
+}
+
+}  // extern "C"

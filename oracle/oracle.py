@@ -1,0 +1,126 @@
+"""ctypes access to the CPU oracle and to the reference's own libraries.
+
+Test infrastructure only (the checker): tests/, ``__graft_entry__.smoke()``
+and bench.py's CPU-baseline leg use it; the product never does.
+
+* ``Oracle(net)``     the restatement (oracle/_build/liboracle_<net>.so,
+                      built on demand from oracle/bdf_oracle.cpp).
+* ``Reference(net)``  the reference's generated ``krome_solve_cells``
+                      compiled from its own sources (oracle/_ref/, made by
+                      oracle/build_ref.py where the reference tree exists);
+                      ``strict=True`` the bit-for-bit pin build.
+"""
+import ctypes
+import os
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_long)
+NSTAT = 9
+STAT_NAMES = ("nst", "nfe", "nfeDQ", "nje", "nsetups", "nni", "nnf", "netf",
+              "restarts")
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("evolve_T", ctypes.c_int), ("jac", ctypes.c_int),
+                ("rtol", ctypes.c_double), ("atol_n", ctypes.c_double),
+                ("atol_T", ctypes.c_double), ("max_steps", ctypes.c_long),
+                ("max_err_fails", ctypes.c_int),
+                ("max_conv_fails", ctypes.c_int),
+                ("max_restarts", ctypes.c_int),
+                ("clip_negative", ctypes.c_int)]
+
+
+def _ptr(a, t=_D):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+class Oracle:
+    def __init__(self, net):
+        import sys
+        sys.path.insert(0, str(HERE))
+        import build as _b  # oracle/build.py
+        self.lib = ctypes.CDLL(str(_b.build(net)))
+        self.lib.oracle_solve_cells.restype = ctypes.c_int
+        self.lib.oracle_solve_cells.argtypes = [
+            ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _I,
+            ctypes.POINTER(_Opts), _L, ctypes.c_int]
+        self.nspec = self.lib.oracle_nspec()
+        self.npar = self.lib.oracle_npar()
+
+    def solve(self, n, T, dt, par, evolve_T=1, jac=0, rtol=1e-6, atol_n=1e-20,
+              atol_T=1e-6, max_steps=100000, max_err_fails=7,
+              max_conv_fails=10, max_restarts=5, clip_negative=1,
+              threads=None, **_):
+        n = np.array(n, dtype=float, order="C", copy=True)
+        T = np.array(T, dtype=float, order="C", copy=True)
+        dt = np.ascontiguousarray(dt, dtype=float)
+        par = np.ascontiguousarray(par, dtype=float)
+        ncell = n.shape[0]
+        stride = 0 if par.ndim == 1 else self.npar
+        flags = np.zeros(ncell, dtype=np.intc)
+        stats = np.zeros((ncell, NSTAT), dtype=np.int64)
+        o = _Opts(int(evolve_T), int(jac), rtol, atol_n, atol_T,
+                  int(max_steps), max_err_fails, max_conv_fails,
+                  max_restarts, int(clip_negative))
+        nt = threads or os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ret = self.lib.oracle_solve_cells(
+            ncell, _ptr(n), _ptr(T), _ptr(dt), _ptr(par), stride,
+            _ptr(flags, _I), ctypes.byref(o), _ptr(stats, _L), nt)
+        self.seconds = time.perf_counter() - t0
+        return dict(n=n, T=T, flags=flags, stats=stats, ret=ret)
+
+
+class Reference:
+    """the reference's krome_solve_cells (its generated C ABI)"""
+
+    def __init__(self, net, strict=False):
+        name = "libkrome_%s%s.so" % (net, "_strict" if strict else "")
+        path = HERE / "_ref" / name
+        if not path.exists():
+            raise FileNotFoundError(
+                "%s missing: run oracle/build_ref.py where the reference "
+                "tree is available" % path)
+        lib = self.lib = ctypes.CDLL(str(path))
+        lib.krome_opts_new.restype = ctypes.c_void_p
+        lib.krome_opts_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                       ctypes.c_double]
+        lib.krome_opts_set.restype = ctypes.c_int
+        lib.krome_opts_free.argtypes = [ctypes.c_void_p]
+        lib.krome_solve_cells.restype = ctypes.c_int
+        lib.krome_solve_cells.argtypes = [ctypes.c_int, _D, _D, _D, _D,
+                                          ctypes.c_int, ctypes.c_void_p, _I,
+                                          ctypes.c_void_p]
+        lib.krome_npar.restype = ctypes.c_int
+        self.npar = lib.krome_npar()
+
+    def solve(self, n, T, dt, par, **opts):
+        n = np.array(n, dtype=float, order="C", copy=True)
+        T = np.array(T, dtype=float, order="C", copy=True)
+        dt = np.ascontiguousarray(dt, dtype=float)
+        par = np.ascontiguousarray(par, dtype=float)
+        ncell = n.shape[0]
+        stride = 0 if par.ndim == 1 else self.npar
+        flags = np.zeros(ncell, dtype=np.intc)
+        h = self.lib.krome_opts_new()
+        opts = dict(opts)
+        opts.setdefault("error_report", 0)
+        opts.setdefault("path", 1)
+        for k, v in opts.items():
+            if k in ("threads",):
+                continue
+            if self.lib.krome_opts_set(h, k.encode(), float(v)) != 0:
+                raise KeyError(k)
+        t0 = time.perf_counter()
+        ret = self.lib.krome_solve_cells(ncell, _ptr(n), _ptr(T), _ptr(dt),
+                                         _ptr(par), stride, None,
+                                         _ptr(flags, _I), h)
+        self.seconds = time.perf_counter() - t0
+        self.lib.krome_opts_free(h)
+        return dict(n=n, T=T, flags=flags, ret=ret)
