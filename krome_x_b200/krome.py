@@ -1,0 +1,317 @@
+"""Python binding of libkrome_b200_<net>.so (ctypes), mirroring the
+reference's generated binding (runtime/interfaces/python/krome.py): the
+same ``Network`` / ``Options`` / ``Result`` / ``KromeError`` names, the same
+``solve(n, Tgas, dt, par, opts)`` semantics (new arrays returned, inputs
+never modified, a REQUIRED parameter left unset raises before the call,
+``check=True`` raises on a failed cell), plus ``solve_batch`` (strict
+shapes: ``n[N, nspec]``, ``Tgas[N]``, ``dt[N]``, ``par`` one row or
+``[N, npar]``) and ``solve_device`` for arrays already in GPU memory
+(torch CUDA tensors or raw device pointers).
+
+    from krome_x_b200 import krome
+    net = krome.load("primordial")
+    opts = net.options(evolve_T=True, rtol=1e-6, jac="analytic")
+    res = net.solve_batch(n, Tgas, dt, par, opts=opts)
+
+There is no CPU fallback: the library computes on the GPU or fails.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import netinfo
+
+__all__ = ["load", "Network", "Options", "Result", "KromeError"]
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_long)
+_ENUMS = {"jac": ("auto", "analytic", "fd"),
+          "linsol": ("auto", "dense", "lapack", "sparse"),
+          "path": ("auto", "percell", "device"),
+          "kernel": ("plain", "persistent")}
+STAT_NAMES = ("nst", "nfe", "nfeDQ", "nje", "nsetups", "nni", "nnf", "netf",
+              "restarts")
+LIBDIR = Path(__file__).resolve().parent / "lib"
+
+
+class KromeError(RuntimeError):
+    """a rejected argument or option, or a failed solve."""
+
+
+def load(network):
+    """the Network of a generated network key (e.g. "primordial") or of a
+    library path"""
+    return Network(network)
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+class Result:
+    """solve() output: new arrays n, Tgas, the per-cell flags, the returned
+    flag ierr and (solve_batch with stats=True) per-cell counters"""
+
+    def __init__(self, n, Tgas, flags, ierr, stats=None):
+        self.n, self.Tgas, self.flags, self.ierr = n, Tgas, flags, ierr
+        self.stats = stats
+
+    def __repr__(self):
+        return "<krome_b200 Result ierr=%d>" % self.ierr
+
+
+class Options:
+    """an options handle (krome_opts), set by key as in the reference"""
+
+    def __init__(self, net, **values):
+        self._net = net
+        self._lib = net._lib
+        self._h = ctypes.c_void_p(self._lib.krome_opts_new())
+        for k, v in values.items():
+            self[k] = v
+
+    def __setitem__(self, key, value):
+        if key in _ENUMS and isinstance(value, str):
+            value = _ENUMS[key].index(value)
+        if isinstance(value, bool):
+            value = int(value)
+        if self._lib.krome_opts_set(self._h, key.encode(), float(value)) != 0:
+            raise KromeError("bad option %s = %r" % (key, value))
+
+    def __getitem__(self, key):
+        v = ctypes.c_double()
+        if self._lib.krome_opts_get(self._h, key.encode(), ctypes.byref(v)) != 0:
+            raise KromeError("unknown option %s" % key)
+        return v.value
+
+    def set(self, **values):
+        for k, v in values.items():
+            self[k] = v
+        return self
+
+    def __del__(self):
+        try:
+            self._lib.krome_opts_free(self._h)
+        except Exception:
+            pass
+
+
+class Network:
+    """one generated network, compiled into libkrome_b200_<net>.so"""
+
+    def __init__(self, network):
+        p = Path(network)
+        if p.suffix == ".so":
+            path = p
+            key = p.stem[len("libkrome_b200_"):]
+        else:
+            key = str(network)
+            path = LIBDIR / ("libkrome_b200_%s.so" % key)
+        if not path.exists():
+            raise KromeError("library %s not found: build it with "
+                             "python -m krome_x_b200.build %s" % (path, key))
+        self.key = key
+        self.path = path
+        lib = self._lib = ctypes.CDLL(str(path))
+        proto = {
+            "krome_network_name": (ctypes.c_char_p, []),
+            "krome_version": (ctypes.c_char_p, []),
+            "krome_nspec": (ctypes.c_int, []),
+            "krome_nrea": (ctypes.c_int, []),
+            "krome_npar": (ctypes.c_int, []),
+            "krome_species_name": (ctypes.c_char_p, [ctypes.c_int]),
+            "krome_species_index": (ctypes.c_int, [ctypes.c_char_p]),
+            "krome_param_name": (ctypes.c_char_p, [ctypes.c_int]),
+            "krome_param_index": (ctypes.c_int, [ctypes.c_char_p]),
+            "krome_param_required_by": (ctypes.c_char_p, [ctypes.c_int]),
+            "krome_params_default": (None, [_D]),
+            "krome_flag_message": (ctypes.c_char_p, [ctypes.c_int]),
+            "krome_opts_new": (ctypes.c_void_p, []),
+            "krome_opts_free": (None, [ctypes.c_void_p]),
+            "krome_opts_set": (ctypes.c_int, [ctypes.c_void_p,
+                                              ctypes.c_char_p,
+                                              ctypes.c_double]),
+            "krome_opts_get": (ctypes.c_int, [ctypes.c_void_p,
+                                              ctypes.c_char_p, _D]),
+            "krome_solve_cells": (ctypes.c_int, [
+                ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_void_p,
+                _I, ctypes.c_void_p]),
+            "krome_b200_solve_batch": (ctypes.c_int, [
+                ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _I, _L,
+                ctypes.c_void_p]),
+            "krome_b200_solve_device": (ctypes.c_int, [
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p]),
+            "krome_has_device": (ctypes.c_int, []),
+            "krome_b200_nstat": (ctypes.c_int, []),
+        }
+        for name, (res, args) in proto.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        self.name = lib.krome_network_name().decode()
+        self.version = lib.krome_version().decode()
+        self.nspec = lib.krome_nspec()
+        self.nrea = lib.krome_nrea()
+        self.npar = lib.krome_npar()
+        self.species = tuple(lib.krome_species_name(i).decode()
+                             for i in range(self.nspec))
+        self.params = tuple(lib.krome_param_name(i).decode()
+                            for i in range(self.npar))
+        self.required = {s: lib.krome_param_required_by(i).decode()
+                         for i, s in enumerate(self.params)
+                         if lib.krome_param_required_by(i).decode()}
+        self._pidx = {s: i for i, s in enumerate(self.params)}
+        self.info = netinfo.load(key) if (netinfo.NETDIR / (
+            "net_%s.json" % key)).exists() else None
+        self._opts = None
+
+    def __repr__(self):
+        return "<krome_b200 Network %s: %d species, %d reactions>" % (
+            self.name, self.nspec, self.nrea)
+
+    # -- description ------------------------------------------------------
+
+    def idx(self, name):
+        i = self._lib.krome_species_index(name.encode())
+        if i < 0:
+            raise KromeError("unknown species %r" % name)
+        return i
+
+    def params_default(self):
+        row = np.zeros(self.npar)
+        self._lib.krome_params_default(_dptr(row))
+        return row
+
+    def param_rows(self, ncell, **values):
+        rows = np.repeat(self.params_default()[None, :], ncell, axis=0)
+        for k, v in values.items():
+            if k not in self._pidx:
+                raise KromeError("unknown parameter %r" % k)
+            rows[:, self._pidx[k]] = np.broadcast_to(np.asarray(v, float),
+                                                     (ncell,))
+        return rows
+
+    def flag_message(self, flag):
+        return self._lib.krome_flag_message(int(flag)).decode()
+
+    def options(self, **values):
+        return Options(self, **values)
+
+    @property
+    def has_device(self):
+        return bool(self._lib.krome_has_device())
+
+    # -- solves -------------------------------------------------------------
+
+    def _options(self, opts):
+        if opts is not None:
+            return opts
+        if self._opts is None:
+            self._opts = Options(self)
+        return self._opts
+
+    def _params(self, par, ncell):
+        stride, P = 0, None
+        if isinstance(par, dict):
+            P = self.param_rows(ncell, **par)
+            stride = self.npar
+        elif par is not None:
+            P = np.ascontiguousarray(par, dtype=float)
+            if P.shape == (self.npar,):
+                stride = 0
+            elif P.shape == (ncell, self.npar):
+                stride = self.npar
+            else:
+                raise KromeError("par must have shape (%d,) or (%d, %d), got "
+                                 "%s" % (self.npar, ncell, self.npar, P.shape))
+        rows = (self.params_default()[None, :] if P is None
+                else P.reshape(-1, self.npar))
+        unset = [s for s in self.required
+                 if np.isnan(rows[:, self._pidx[s]]).any()]
+        if unset:
+            raise KromeError("required parameter(s) not set: %s" % "; ".join(
+                "%s (for %s)" % (s, self.required[s]) for s in unset))
+        return P, stride
+
+    def _run(self, n, T, dtv, P, stride, opts, check, stats):
+        ncell = n.shape[0]
+        flags = np.zeros(ncell, dtype=np.intc)
+        st = np.zeros((ncell, len(STAT_NAMES)), dtype=np.int64) if stats else None
+        ierr = self._lib.krome_b200_solve_batch(
+            ncell, _dptr(n), _dptr(T), _dptr(dtv), _dptr(P), stride,
+            flags.ctypes.data_as(_I), None if st is None else st.ctypes.data_as(_L),
+            opts._h)
+        if check and ierr != 0:
+            bad = np.flatnonzero(flags)
+            raise KromeError("krome_solve_cells returned %d: %s (failed cells: "
+                             "%s); pass check=False to get the result anyway"
+                             % (ierr, self.flag_message(ierr),
+                                bad[:20].tolist() or "n/a"))
+        return flags, ierr, st
+
+    def solve(self, n, Tgas, dt, par=None, opts=None, check=True,
+              stats=False):
+        """integrate every cell over its own dt [s] (reference
+        runtime/interfaces/python/krome.py:458-507): n[nspec] or
+        n[ncell, nspec], Tgas and dt scalars or per cell, par None / a dict
+        / one row / rows. Returns a Result with new arrays."""
+        n = np.array(n, dtype=float, order="C", copy=True)
+        if n.ndim == 0 or n.ndim > 2 or n.shape[-1] != self.nspec:
+            raise KromeError("n must have shape (%d,) or (ncell, %d), got %s"
+                             % (self.nspec, self.nspec, n.shape))
+        single = n.ndim == 1
+        n = n.reshape(-1, self.nspec)
+        ncell = n.shape[0]
+        T = np.array(np.broadcast_to(np.asarray(Tgas, dtype=float), (ncell,)),
+                     order="C", copy=True)
+        dtv = np.array(np.broadcast_to(np.asarray(dt, dtype=float), (ncell,)),
+                       order="C", copy=True)
+        opts = self._options(opts)
+        P, stride = self._params(par, ncell)
+        flags, ierr, st = self._run(n, T, dtv, P, stride, opts, check, stats)
+        if single:
+            return Result(n[0], T[0], flags[0], ierr,
+                          None if st is None else st[0])
+        return Result(n, T, flags, ierr, st)
+
+    def solve_batch(self, n, Tgas, dt, par=None, opts=None, check=True,
+                    stats=False):
+        """the batched entry point: n[N, nspec], Tgas[N], dt[N] exactly
+        (no scalar broadcast), par None / dict / one row / [N, npar]"""
+        n = np.asarray(n, dtype=float)
+        if n.ndim != 2 or n.shape[1] != self.nspec:
+            raise KromeError("solve_batch: n must be (N, %d), got %s"
+                             % (self.nspec, n.shape))
+        N = n.shape[0]
+        for name, v in (("Tgas", Tgas), ("dt", dt)):
+            if np.shape(v) != (N,):
+                raise KromeError("solve_batch: %s must be (%d,), got %s"
+                                 % (name, N, np.shape(v)))
+        return self.solve(n, Tgas, dt, par=par, opts=opts, check=check,
+                          stats=stats)
+
+    def solve_device(self, n, Tgas, dt, par, flags, opts=None, stats=None,
+                     cursor=None, stream=0):
+        """device-resident solve: every argument a CUDA array (torch tensor
+        or an int device pointer): n[N, nspec] and Tgas[N] updated in place,
+        dt[N], par one row or [N, npar], flags[N] int32; cursor one uint32
+        (the work queue of the persistent kernel); asynchronous on stream"""
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        N = int(n.shape[0])
+        npar_el = int(par.numel()) if hasattr(par, "numel") else self.npar
+        stride = 0 if npar_el == self.npar else self.npar
+        opts = self._options(opts)
+        r = self._lib.krome_b200_solve_device(
+            N, ptr(n), ptr(Tgas), ptr(dt), ptr(par), stride, ptr(flags),
+            ptr(stats), ptr(cursor), opts._h, ctypes.c_void_p(stream))
+        if r != 0:
+            raise KromeError("krome_b200_solve_device returned %d: %s"
+                             % (r, self.flag_message(r)))
+        return r
