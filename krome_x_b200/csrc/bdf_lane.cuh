@@ -1,0 +1,881 @@
+// Lane-per-cell CVODE BDF integrator for sm_100a: each lane of a warp
+// integrates its own cell, and the warp serves the lanes' right-hand-side
+// and Jacobian requests together.
+//
+// Why this layout. The network math (rate coefficients with their exp /
+// log / pow, the thermal terms) dominates the solve and is scalar per
+// cell. With one warp per cell (bdf_warp.cuh) every lane evaluates the
+// same state, so a warp instruction does one cell's work; here a warp
+// instruction evaluates 32 cells. The integrator's control flow differs
+// between cells (Newton iteration counts, Jacobian refreshes, failed
+// attempts, cells that finish early), so it is written as a per-lane
+// resumable state machine that stops at every rhs or Jacobian request:
+//
+//   loop:  1. every lane advances its own CVODE logic (cheap, O(N) and
+//             O(N^2) vector work in its private memory) to its next
+//             request; a lane whose cell is done writes it back and takes
+//             the next cell (a fixed one, or the next one of the device
+//             work queue in the persistent kernel), so lanes never wait
+//             for the slowest cell of their warp;
+//          2. Jacobian requests are served one requesting cell at a time
+//             by the whole warp: lane j evaluates the rhs perturbed in
+//             component j (the difference-quotient columns, or the hybrid
+//             analytic Jacobian's thermal-row and Tgas-column terms), the
+//             columns meet in shared memory;
+//          3. all lanes with an rhs request evaluate it in one SIMT pass.
+//
+// The algorithm and every decision are CVODE's as the reference ports it
+// (runtime/core/cvode/bdf_cell.hpp:490-1547: cvHin, cvStep, the modified
+// Newton iteration, cvLsSetup's reuse heuristics, the dense LU with
+// partial pivoting, the error test, the step and order selection, the
+// restart wrapper) around the reference's per-cell problem
+// (runtime/core/solve_cell.hpp:750-813, 883-1118, 1631-1642, 2094-2203).
+// Every loop is bounded as in bdf_warp.cuh (max_steps, the per-step
+// failure limits, max_restarts; the queue loop by the number of cells).
+#pragma once
+
+namespace kbl {
+
+using namespace kbnet;
+using kbw::SolveOpts;
+using kbw::NSTAT;
+using namespace kbw;  // flags and CVODE constants
+
+enum : int { REQ_NONE = 0, REQ_RHS = 1, REQ_JAC = 2, REQ_DONE = 3 };
+
+// resume points of the state machine
+enum : int {
+  PC_NEW = 0, PC_FIRST_RHS, PC_HIN_RHS, PC_RES_OUTER, PC_RES_INNER,
+  PC_JAC, PC_ERRTEST_RHS, PC_IDLE
+};
+
+template <int N>
+struct LaneCell {
+  // ---- the cell ----
+  int cell;        // the cell being integrated, -1 when idle
+  int pc;
+  double dt;
+  double Tfix;
+  Params p;
+  bool hitT0;
+  int restarts;
+  long tot[NSTAT];
+  // ---- vectors ----
+  double zn[L_MAX][N];
+  double ewt[N], y[N], acor[N], tempv[N], ftemp[N], delta[N];
+  double yreq[N], freq[N];   // the pending rhs request and its result
+  int rhs_ret;
+  double savedJ[N * N];      // column-major (element (i, j) at i + j N)
+  double A[N * N];
+  int piv[N];
+  double atol[N];
+  // ---- CVodeMem ----
+  long st[NSTAT];
+  long mxstep, nstloc;
+  bool atolmin0;
+  double tn, h, hin, hprime, hscale, next_h, hu, eta, etamax, etaq;
+  double etaqm1, etaqp1, tolsf, saved_tq5;
+  double tau[L_MAX + 1], tq[6], l[L_MAX];
+  double rl1, gamma, gammap, gamrat, crate, delp, delnrm, acnrm;
+  int q, qprime, next_q, qu, L, qwait;
+  long nscon, nstlp, nstlj;
+  int convfail;
+  bool acnrmcur, jcur, nls_jcur;
+  // ---- loop state kept across requests ----
+  double tret;
+  // cvHin
+  int hin_count1, hin_count2, hin_sign;
+  double hin_hg, hin_hs, hin_hnew, hin_hlb, hin_hub, hin_hgs;
+  // cvStep
+  int ncf, nef, nflag;
+  double saved_t, dsm;
+  // Newton
+  bool callSetup, jbad;
+  long niters, nconvfails;
+  int curiter, nls_ret;
+  double tol;
+  // ls_setup
+  int ls_retval;
+};
+
+// ---- vector operations (bdf_cell.hpp:296-400), private arrays ----
+template <int N>
+__device__ __forceinline__ void axpy_(double a, const double* x, double* y) {
+  if (a == 1.0) {
+    KB_UNROLL for (int i = 0; i < N; i++) y[i] += x[i];
+  } else if (a == -1.0) {
+    KB_UNROLL for (int i = 0; i < N; i++) y[i] -= x[i];
+  } else {
+    KB_UNROLL for (int i = 0; i < N; i++) y[i] += a * x[i];
+  }
+}
+template <int N>
+__device__ __forceinline__ void lin_sum_(double a, const double* x, double b,
+                                         const double* y, double* z) {
+  if (b == 1.0 && z == y) { axpy_<N>(a, x, z); return; }
+  if (a == 1.0 && z == x) { axpy_<N>(b, y, z); return; }
+  if (a == 1.0 && b == 1.0) {
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
+    return;
+  }
+  bool test;
+  if ((test = (a == 1.0 && b == -1.0)) || (a == -1.0 && b == 1.0)) {
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
+    return;
+  }
+  if ((test = (a == 1.0)) || b == 1.0) {
+    const double c = test ? b : a;
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
+    return;
+  }
+  if ((test = (a == -1.0)) || b == -1.0) {
+    const double c = test ? b : a;
+    const double* v1 = test ? y : x;
+    const double* v2 = test ? x : y;
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
+    return;
+  }
+  if (a == b) {
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
+    return;
+  }
+  if (a == -b) {
+    KB_UNROLL for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
+    return;
+  }
+  KB_UNROLL for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
+}
+template <int N>
+__device__ __forceinline__ void scale_(double c, const double* x, double* z) {
+  KB_UNROLL for (int i = 0; i < N; i++) z[i] = c * x[i];
+}
+template <int N>
+__device__ __forceinline__ double wrms_(const double* x, const double* w) {
+  double sum = 0.0;
+  KB_UNROLL for (int i = 0; i < N; i++) {
+    const double pv = x[i] * w[i];
+    sum += pv * pv;
+  }
+  return ssqrt_(sum / N);
+}
+
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457)
+template <int N>
+__device__ int getrf_(double* a, int* p) {
+  for (int k = 0; k < N; k++) {
+    double* col_k = a + k * N;
+    int l = k;
+    for (int i = k + 1; i < N; i++)
+      if (fabs(col_k[i]) > fabs(col_k[l])) l = i;
+    p[k] = l;
+    if (col_k[l] == 0.0) return k + 1;
+    if (l != k)
+      for (int i = 0; i < N; i++) {
+        double* ci = a + i * N;
+        const double t = ci[l];
+        ci[l] = ci[k];
+        ci[k] = t;
+      }
+    const double mult = 1.0 / col_k[k];
+    for (int i = k + 1; i < N; i++) col_k[i] *= mult;
+    for (int j = k + 1; j < N; j++) {
+      double* col_j = a + j * N;
+      const double a_kj = col_j[k];
+      if (a_kj != 0.0)
+        for (int i = k + 1; i < N; i++) col_j[i] -= a_kj * col_k[i];
+    }
+  }
+  return 0;
+}
+template <int N>
+__device__ void getrs_(const double* a, const int* p, double* b) {
+  for (int k = 0; k < N; k++) {
+    const int pk = p[k];
+    if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
+  }
+  for (int k = 0; k < N - 1; k++) {
+    const double* col_k = a + k * N;
+    const double bk = b[k];
+    for (int i = k + 1; i < N; i++) b[i] -= col_k[i] * bk;
+  }
+  for (int k = N - 1; k > 0; k--) {
+    const double* col_k = a + k * N;
+    b[k] /= col_k[k];
+    const double bk = b[k];
+    for (int i = 0; i < k; i++) b[i] -= col_k[i] * bk;
+  }
+  b[0] /= a[0];
+}
+
+template <int N, bool EVT>
+struct Machine {
+  LaneCell<N>& s;
+  const SolveOpts& o;
+  __device__ Machine(LaneCell<N>& s_, const SolveOpts& o_) : s(s_), o(o_) {}
+
+  __device__ int ewt_set(const double* ycur, double* w) {
+    KB_UNROLL for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
+    KB_UNROLL for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
+    if (s.atolmin0) {
+      double mn = w[0];
+      KB_UNROLL for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
+      if (mn <= 0.0) return -1;
+    }
+    KB_UNROLL for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
+    return 0;
+  }
+
+  __device__ void reinit(double t0, const double* y0, double h_init) {
+    s.tn = t0;
+    KB_UNROLL for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
+    s.q = 1; s.L = 2; s.qwait = s.L;
+    s.etamax = ETA_MAX_FS;
+    s.qu = 0; s.hu = 0.0; s.tolsf = 1.0;
+    for (int i = 0; i < NSTAT; ++i) s.st[i] = 0;
+    s.nstlp = 0; s.nscon = 0; s.next_h = 0.0; s.next_q = 0;
+    s.hin = h_init;
+    s.nstlj = 0;
+    s.acnrmcur = false; s.nls_jcur = false; s.jcur = false;
+    s.saved_tq5 = 0.0;
+    for (int i = 0; i <= L_MAX; i++) s.tau[i] = 0.0;
+    s.eta = 1.0;
+  }
+
+  __device__ __forceinline__ void request_rhs(const double* yv, int pc) {
+    KB_UNROLL for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
+    s.pc = pc;
+  }
+
+  // ---- step helpers (bdf_cell.hpp:825-954, 1386-1500) ----
+  __device__ void rescale_() {
+    double c = s.eta;
+    for (int j = 1; j <= s.q; j++) {
+      scale_<N>(c, s.zn[j], s.zn[j]);
+      c = s.eta * c;
+    }
+    s.h = s.hscale * s.eta;
+    s.next_h = s.h;
+    s.hscale = s.h;
+    s.nscon = 0;
+  }
+  __device__ void increase_bdf_() {
+    for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
+    double alpha1, prod, xiold, alpha0;
+    s.l[2] = alpha1 = prod = xiold = 1.0;
+    alpha0 = -1.0;
+    double hsum = s.hscale;
+    if (s.q > 1)
+      for (int j = 1; j < s.q; j++) {
+        hsum += s.tau[j + 1];
+        const double xi = hsum / s.hscale;
+        prod *= xi;
+        alpha0 -= 1.0 / (j + 1);
+        alpha1 += 1.0 / xi;
+        for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xiold + s.l[i - 1];
+        xiold = xi;
+      }
+    const double A1 = (-alpha0 - alpha1) / prod;
+    scale_<N>(A1, s.zn[QMAX], s.zn[s.L]);
+    if (s.q > 1)
+      for (int j = 2; j <= s.q; j++) axpy_<N>(s.l[j], s.zn[s.L], s.zn[j]);
+  }
+  __device__ void decrease_bdf_() {
+    for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
+    s.l[2] = 1.0;
+    double hsum = 0.0;
+    for (int j = 1; j <= s.q - 2; j++) {
+      hsum += s.tau[j];
+      const double xi = hsum / s.hscale;
+      for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xi + s.l[i - 1];
+    }
+    if (s.q > 2)
+      for (int j = 2; j < s.q; j++) axpy_<N>(-s.l[j], s.zn[s.q], s.zn[j]);
+  }
+  __device__ void adjust_order_(int deltaq) {
+    if ((s.q == 2) && (deltaq != 1)) return;
+    if (deltaq == 1) increase_bdf_();
+    else if (deltaq == -1) decrease_bdf_();
+  }
+  __device__ void predict_() {
+    s.tn += s.h;
+    for (int k = 1; k <= s.q; k++)
+      for (int j = s.q; j >= k; j--) axpy_<N>(1.0, s.zn[j], s.zn[j - 1]);
+  }
+  __device__ void restore_(double saved_t) {
+    s.tn = saved_t;
+    for (int k = 1; k <= s.q; k++)
+      for (int j = s.q; j >= k; j--) axpy_<N>(-1.0, s.zn[j], s.zn[j - 1]);
+  }
+  __device__ void set_() {
+    double xi_inv, xistar_inv, alpha0, alpha0_hat;
+    s.l[0] = s.l[1] = xi_inv = xistar_inv = 1.0;
+    for (int i = 2; i <= s.q; i++) s.l[i] = 0.0;
+    alpha0 = alpha0_hat = -1.0;
+    double hsum = s.h;
+    const int q = s.q;
+    if (q > 1) {
+      for (int j = 2; j < q; j++) {
+        hsum += s.tau[j - 1];
+        xi_inv = s.h / hsum;
+        alpha0 -= 1.0 / j;
+        for (int i = j; i >= 1; i--) s.l[i] += s.l[i - 1] * xi_inv;
+      }
+      alpha0 -= 1.0 / q;
+      xistar_inv = -s.l[1] - alpha0;
+      hsum += s.tau[q - 1];
+      xi_inv = s.h / hsum;
+      alpha0_hat = -s.l[1] - xi_inv;
+      for (int i = q; i >= 1; i--) s.l[i] += s.l[i - 1] * xistar_inv;
+    }
+    const double A1 = 1.0 - alpha0_hat + alpha0;
+    const double A2 = 1.0 + q * A1;
+    s.tq[2] = fabs(A1 / (alpha0 * A2));
+    s.tq[5] = fabs(A2 * xistar_inv / (s.l[q] * xi_inv));
+    if (s.qwait == 1) {
+      if (q > 1) {
+        const double C = xistar_inv / s.l[q];
+        const double A3 = alpha0 + 1.0 / q;
+        const double A4 = alpha0_hat + xi_inv;
+        const double Cpinv = (1.0 - A4 + A3) / A3;
+        s.tq[1] = fabs(C * Cpinv);
+      } else {
+        s.tq[1] = 1.0;
+      }
+      hsum += s.tau[q];
+      const double xi2 = s.h / hsum;
+      const double A5 = alpha0 - (1.0 / (q + 1));
+      const double A6 = alpha0_hat - xi2;
+      const double Cppinv = (1.0 - A6 + A5) / A2;
+      s.tq[3] = fabs(Cppinv / (xi2 * (q + 2) * A5));
+    }
+    s.tq[4] = CORTES / s.tq[2];
+    s.rl1 = 1.0 / s.l[1];
+    s.gamma = s.h * s.rl1;
+    if (s.st[ST_NST] == 0) s.gammap = s.gamma;
+    s.gamrat = (s.st[ST_NST] > 0) ? s.gamma / s.gammap : 1.0;
+  }
+  __device__ void complete_step_() {
+    s.st[ST_NST]++;
+    s.nscon++;
+    s.hu = s.h;
+    s.qu = s.q;
+    for (int i = s.q; i >= 2; i--) s.tau[i] = s.tau[i - 1];
+    if ((s.q == 1) && (s.st[ST_NST] > 1)) s.tau[2] = s.tau[1];
+    s.tau[1] = s.h;
+    for (int j = 0; j <= s.q; j++) axpy_<N>(s.l[j], s.acor, s.zn[j]);
+    s.qwait--;
+    if ((s.qwait == 1) && (s.q != QMAX)) {
+      KB_UNROLL for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      s.saved_tq5 = s.tq[5];
+    }
+  }
+  __device__ void set_eta_() {
+    if ((s.eta > ETA_MIN_FX) && (s.eta < ETA_MAX_FX)) {
+      s.eta = 1.0;
+      s.hprime = s.h;
+      return;
+    }
+    if (s.eta >= ETA_MAX_FX) s.eta = smin_(s.eta, s.etamax);
+    else s.eta = smax_(s.eta, ETA_MIN);
+    s.hprime = s.h * s.eta;
+    if (s.qprime < s.q) s.nscon = 0;
+  }
+  __device__ void prepare_next_step_(double dsm) {
+    if (s.etamax == 1.0) {
+      s.qwait = s.qwait > 2 ? s.qwait : 2;
+      s.qprime = s.q;
+      s.hprime = s.h;
+      s.eta = 1.0;
+      return;
+    }
+    s.etaq = 1.0 / (pow(BIAS2 * dsm, 1.0 / s.L) + ADDON);
+    if (s.qwait != 0) {
+      s.eta = s.etaq;
+      s.qprime = s.q;
+      set_eta_();
+      return;
+    }
+    s.qwait = 2;
+    s.etaqm1 = 0.0;
+    if (s.q > 1) {
+      const double ddn = wrms_<N>(s.zn[s.q], s.ewt) * s.tq[1];
+      s.etaqm1 = 1.0 / (pow(BIAS1 * ddn, 1.0 / s.q) + ADDON);
+    }
+    s.etaqp1 = 0.0;
+    if (s.q != QMAX && s.saved_tq5 != 0.0) {
+      const double rr = s.h / s.tau[2];
+      double prod = 1.0;
+      for (int i = 1; i <= s.L; i++) prod *= rr;
+      const double cquot = (s.tq[5] / s.saved_tq5) * prod;
+      lin_sum_<N>(-cquot, s.zn[QMAX], 1.0, s.acor, s.tempv);
+      const double dup = wrms_<N>(s.tempv, s.ewt) * s.tq[3];
+      s.etaqp1 = 1.0 / (pow(BIAS3 * dup, 1.0 / (s.L + 1)) + ADDON);
+    }
+    const double etam = smax_(s.etaqm1, smax_(s.etaq, s.etaqp1));
+    if ((etam > ETA_MIN_FX) && (etam < ETA_MAX_FX)) {
+      s.eta = 1.0;
+      s.qprime = s.q;
+    } else if (etam == s.etaq) {
+      s.eta = s.etaq;
+      s.qprime = s.q;
+    } else if (etam == s.etaqm1) {
+      s.eta = s.etaqm1;
+      s.qprime = s.q - 1;
+    } else {
+      s.eta = s.etaqp1;
+      s.qprime = s.q + 1;
+      KB_UNROLL for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+    }
+    set_eta_();
+  }
+  __device__ void get_dky_(double t, double* dky) {
+    const double sv = (t - s.tn) / s.h;
+    for (int j = s.q; j >= 0; j--) {
+      double c = 1.0;
+      for (int i = 0; i < j; i++) c *= sv;
+      if (j == s.q) scale_<N>(c, s.zn[j], dky);
+      else axpy_<N>(c, s.zn[j], dky);
+    }
+  }
+  // the charge invariant of a DQ-Jacobian Newton correction
+  // (bdf_cell.hpp:1266-1287)
+  __device__ double inv_dot_(const double* x) const {
+    double sum = 0.0;
+    KB_UNROLL for (int i = 0; i < NSPEC; i++)
+      if (species_charge(i) != 0) sum += species_charge(i) * x[i];
+    return sum;
+  }
+  __device__ void inv_set_(double* x, double target) const {
+    const int r = IDX_ELECTRON;
+    double sum = 0.0, sa = 0.0;
+    KB_UNROLL for (int i = 0; i < NSPEC; i++)
+      if (i != r && species_charge(i) != 0) {
+        sum += species_charge(i) * x[i];
+        sa += fabs(species_charge(i) * (s.zn[0][i] + s.acor[i]));
+      }
+    const double yr = s.zn[0][r] + s.acor[r];
+    const double cr = (double)species_charge(r);
+    const double xr = (target - sum) / cr;
+    if (fabs(cr * yr) >= 1e-6 * sa && yr + xr >= 0.0) x[r] = xr;
+  }
+  // the Newton matrix after a (re)evaluated or reused J: A = I - gamma J
+  // and its LU (the tail of cvLsSetup, bdf_cell.hpp:1097-1130)
+  __device__ int ls_finish_() {
+    int retval = s.ls_retval;
+    if (retval == 0) {
+      const double c = -s.gamma;
+      for (int j = 0; j < N; j++) {
+        for (int i = 0; i < N; i++) {
+          const int k = i + j * N;
+          s.A[k] = s.savedJ[k] * c;
+        }
+        s.A[j + j * N] += 1.0;
+      }
+    }
+    if (s.jcur) {
+      s.st[ST_NJE]++;
+      s.nstlj = s.st[ST_NST];
+    }
+    if (retval != 0) return retval;
+    return getrf_<N>(s.A, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
+  }
+  // cvNlsLSetup's bookkeeping around ls_setup (bdf_cell.hpp:1051-1065)
+  __device__ int lsetup_done_(int retval) {
+    s.st[ST_NSETUPS]++;
+    s.nls_jcur = s.jcur;
+    s.gamrat = 1.0;
+    s.gammap = s.gamma;
+    s.crate = 1.0;
+    s.delnrm = 0.0;
+    s.nstlp = s.st[ST_NST];
+    if (retval < 0) return LSETUP_FAIL;
+    if (retval > 0) return NLS_CONV_RECVR;
+    return SUCCESS;
+  }
+
+  // ---- the state machine: advance to the next request ----
+  // returns REQ_RHS (s.yreq set), REQ_JAC, or REQ_DONE (the cell's flag
+  // in *flag_out)
+  __device__ int advance(int* flag_out) {
+    int retval;
+    switch (s.pc) {
+      case PC_NEW: goto L_new;
+      case PC_FIRST_RHS: goto L_first_rhs;
+      case PC_HIN_RHS: goto L_hin_rhs;
+      case PC_RES_OUTER: goto L_res_outer;
+      case PC_RES_INNER: goto L_res_inner;
+      case PC_JAC: goto L_jac;
+      case PC_ERRTEST_RHS: goto L_errtest_rhs;
+      default: return REQ_NONE;
+    }
+
+  L_new:  // a fresh cell (reinit done by the caller), or a restart
+  L_solve: {
+      // CVode(dt) first-call block (bdf_cell.hpp:570-593)
+      s.tret = s.tn;
+      const double tout = s.dt;
+      const double tdist = fabs(tout - s.tn);
+      const double tround = UROUND * smax_(fabs(s.tn), fabs(tout));
+      if (tdist == 0.0 || tdist < 2.0 * tround) { retval = TOO_CLOSE; goto L_solve_end; }
+      if (ewt_set(s.zn[0], s.ewt) != 0) { retval = ILL_INPUT; goto L_solve_end; }
+      request_rhs(s.zn[0], PC_FIRST_RHS);
+      return REQ_RHS;
+    }
+  L_first_rhs: {
+      KB_UNROLL for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
+      s.st[ST_NFE]++;
+      if (s.rhs_ret > 0) { retval = FIRST_RHSFUNC_ERR; goto L_solve_end; }
+      s.h = s.hin;
+      const double tout = s.dt;
+      if (s.h != 0.0 && (tout - s.tn) * s.h < 0.0) { retval = ILL_INPUT; goto L_solve_end; }
+      if (s.h != 0.0) goto L_after_hin;
+      // cvHin (bdf_cell.hpp:717-794)
+      const double tdiff = tout - s.tn;
+      s.hin_sign = (tdiff > 0.0) ? 1 : -1;
+      const double tdist = fabs(tdiff);
+      const double tround = UROUND * smax_(fabs(s.tn), fabs(tout));
+      s.hin_hlb = HLB_FACTOR * tround;
+      {  // cvUpperBoundH0
+        double* temp1 = s.tempv;
+        double* temp2 = s.acor;
+        KB_UNROLL for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[0][i]);
+        ewt_set(s.zn[0], temp1);
+        KB_UNROLL for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
+        lin_sum_<N>(HUB_FACTOR, temp2, 1.0, temp1, temp1);
+        KB_UNROLL for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[1][i]);
+        KB_UNROLL for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
+        double hub_inv = 0.0;
+        KB_UNROLL for (int i = 0; i < N; i++)
+          if (fabs(temp1[i]) > hub_inv) hub_inv = fabs(temp1[i]);
+        double hub = HUB_FACTOR * tdist;
+        if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
+        s.hin_hub = hub;
+      }
+      s.hin_hg = ssqrt_(s.hin_hlb * s.hin_hub);
+      if (s.hin_hub < s.hin_hlb) {
+        s.h = s.hin_sign == -1 ? -s.hin_hg : s.hin_hg;
+        goto L_after_hin;
+      }
+      s.hin_hs = s.hin_hg;
+      s.hin_hnew = s.hin_hg;
+      s.hin_count1 = 1;
+    }
+  L_hin_c1: {
+      s.hin_count2 = 1;
+    }
+  L_hin_c2: {
+      s.hin_hgs = s.hin_hg * s.hin_sign;
+      lin_sum_<N>(s.hin_hgs, s.zn[1], 1.0, s.zn[0], s.y);
+      request_rhs(s.y, PC_HIN_RHS);
+      return REQ_RHS;
+    }
+  L_hin_rhs: {
+      KB_UNROLL for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      s.st[ST_NFE]++;
+      bool hgOK = false;
+      double yddnrm = 0.0;
+      if (s.rhs_ret == 0) {
+        lin_sum_<N>(1.0 / s.hin_hgs, s.tempv, -1.0 / s.hin_hgs, s.zn[1], s.tempv);
+        yddnrm = wrms_<N>(s.tempv, s.ewt);
+        hgOK = true;
+      } else {
+        s.hin_hg *= 0.2;
+        if (++s.hin_count2 <= MAX_ITERS) goto L_hin_c2;
+      }
+      if (!hgOK) {
+        if (s.hin_count1 <= 2) { retval = REPTD_RHSFUNC_ERR; goto L_solve_end; }
+        s.hin_hnew = s.hin_hs;
+        goto L_hin_done;
+      }
+      s.hin_hs = s.hin_hg;
+      const double hub = s.hin_hub;
+      s.hin_hnew = (yddnrm * hub * hub > 2.0) ? ssqrt_(2.0 / yddnrm)
+                                              : ssqrt_(s.hin_hg * hub);
+      if (s.hin_count1 == MAX_ITERS) goto L_hin_done;
+      const double hrat = s.hin_hnew / s.hin_hg;
+      if ((hrat > 0.5) && (hrat < 2.0)) goto L_hin_done;
+      if ((s.hin_count1 > 1) && (hrat > 2.0)) {
+        s.hin_hnew = s.hin_hg;
+        goto L_hin_done;
+      }
+      s.hin_hg = s.hin_hnew;
+      s.hin_count1++;
+      goto L_hin_c1;
+    }
+  L_hin_done: {
+      double h0 = H_BIAS * s.hin_hnew;
+      if (h0 < s.hin_hlb) h0 = s.hin_hlb;
+      if (h0 > s.hin_hub) h0 = s.hin_hub;
+      if (s.hin_sign == -1) h0 = -h0;
+      s.h = h0;
+    }
+  L_after_hin: {
+      s.hscale = s.h;
+      s.hprime = s.h;
+      scale_<N>(s.h, s.zn[1], s.zn[1]);
+      s.nstloc = 0;
+    }
+  L_step_loop: {
+      // the CVode main loop (bdf_cell.hpp:595-636)
+      s.next_h = s.h;
+      s.next_q = s.q;
+      if (s.st[ST_NST] > 0 && ewt_set(s.zn[0], s.ewt) != 0) {
+        retval = ILL_INPUT; s.tret = s.tn; goto L_solve_end;
+      }
+      if (s.mxstep > 0 && s.nstloc >= s.mxstep) {
+        retval = TOO_MUCH_WORK; s.tret = s.tn; goto L_solve_end;
+      }
+      const double nrm = wrms_<N>(s.zn[0], s.ewt);
+      s.tolsf = UROUND * nrm;
+      if (s.tolsf > 1.0) {
+        retval = TOO_MUCH_ACC; s.tret = s.tn; s.tolsf *= 2.0;
+        goto L_solve_end;
+      }
+      s.tolsf = 1.0;
+      // cvStep (bdf_cell.hpp:798-822)
+      s.ncf = 0;
+      s.nef = 0;
+      s.dsm = 0.0;
+      if (s.st[ST_NST] > 0 && s.hprime != s.h) {
+        if (s.qprime != s.q) {
+          adjust_order_(s.qprime - s.q);
+          s.q = s.qprime;
+          s.L = s.q + 1;
+          s.qwait = s.L;
+        }
+        rescale_();
+      }
+      s.saved_t = s.tn;
+      s.nflag = FIRST_CALL;
+    }
+  L_attempt: {
+      predict_();
+      set_();
+      // cvNls (bdf_cell.hpp:958-1019)
+      s.convfail = ((s.nflag == FIRST_CALL) || (s.nflag == PREV_ERR_FAIL))
+                       ? NO_FAILURES : FAIL_OTHER;
+      s.callSetup = (s.nflag == PREV_CONV_FAIL) || (s.nflag == PREV_ERR_FAIL)
+                    || (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlp + MSBP)
+                    || (fabs(s.gamrat - 1.0) > DGMAX_LSETUP);
+      KB_UNROLL for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+      s.tol = s.tq[4];
+      s.jbad = false;
+      s.niters = 0;
+      s.nconvfails = 0;
+    }
+  L_nls_outer: {
+      s.curiter = 0;
+      lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
+      request_rhs(s.y, PC_RES_OUTER);
+      return REQ_RHS;
+    }
+  L_res_outer: {
+      retval = residual_done_();
+      if (retval != SUCCESS) goto L_nls_after_outer;
+      if (!s.callSetup) goto L_newton_iter;
+      // cvNlsLSetup -> cvLsSetup (bdf_cell.hpp:1051-1096)
+      if (s.jbad) s.convfail = FAIL_BAD_J;
+      {
+        const double dgamma = fabs((s.gamma / s.gammap) - 1.0);
+        const bool jbad_ls = (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlj + MSBJ)
+            || ((s.convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
+            || (s.convfail == FAIL_OTHER);
+        s.ls_retval = 0;
+        if (!jbad_ls) {
+          s.jcur = false;
+        } else {
+          s.jcur = true;
+          s.pc = PC_JAC;
+          return REQ_JAC;  // savedJ from the warp (ls_retval set there)
+        }
+      }
+    }
+  L_jac: {
+      retval = lsetup_done_(ls_finish_());
+      if (retval != SUCCESS) goto L_nls_after_outer;
+    }
+  L_newton_iter: {
+      s.niters++;
+      const bool inv = (o.jac == 2) && IDX_ELECTRON >= 0;
+      const double cg = inv ? inv_dot_(s.delta) : 0.0;
+      scale_<N>(-1.0, s.delta, s.delta);
+      getrs_<N>(s.A, s.piv, s.delta);
+      if (s.gamrat != 1.0) scale_<N>(2.0 / (1.0 + s.gamrat), s.delta, s.delta);
+      if (inv) inv_set_(s.delta, -cg);
+      lin_sum_<N>(1.0, s.acor, 1.0, s.delta, s.acor);
+      // cvNlsConvTest (bdf_cell.hpp:1035-1048)
+      const int m = s.curiter;
+      s.delnrm = wrms_<N>(s.delta, s.ewt);
+      if (m > 0) s.crate = smax_(CRDOWN * s.crate, s.delnrm / s.delp);
+      const double dcon = s.delnrm * smin_(1.0, s.crate) / s.tol;
+      if (dcon <= 1.0) {
+        s.acnrm = (m == 0) ? s.delnrm : wrms_<N>(s.acor, s.ewt);
+        s.acnrmcur = true;
+        retval = SUCCESS;
+      } else if ((m >= 1) && (s.delnrm > RDIV * s.delp)) {
+        retval = NLS_CONV_RECVR;
+      } else {
+        s.delp = s.delnrm;
+        retval = NLS_CONTINUE;
+      }
+      s.curiter++;
+      if (retval == SUCCESS) { s.nls_jcur = false; goto L_nls_after_outer; }
+      if (retval != NLS_CONTINUE) goto L_nls_after_outer;
+      if (s.curiter >= NLS_MAXCOR) { retval = NLS_CONV_RECVR; goto L_nls_after_outer; }
+      lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
+      request_rhs(s.y, PC_RES_INNER);
+      return REQ_RHS;
+    }
+  L_res_inner: {
+      retval = residual_done_();
+      if (retval != SUCCESS) goto L_nls_after_outer;
+      goto L_newton_iter;
+    }
+  L_nls_after_outer: {
+      if (retval == SUCCESS) goto L_nls_end;
+      if ((retval > 0) && !s.nls_jcur) {
+        s.nconvfails++;
+        s.callSetup = true;
+        s.jbad = true;
+        KB_UNROLL for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+        goto L_nls_outer;
+      }
+    }
+  L_nls_end: {
+      if (retval != SUCCESS) s.nconvfails++;
+      s.st[ST_NNI] += s.niters;
+      s.st[ST_NNF] += s.nconvfails;
+      if (retval == SUCCESS) {
+        lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
+        if (!s.acnrmcur) s.acnrm = wrms_<N>(s.acor, s.ewt);
+        s.jcur = false;
+      }
+      s.nflag = retval;
+      // cvHandleNFlag (bdf_cell.hpp:1315-1337)
+      if (s.nflag != SUCCESS) {
+        restore_(s.saved_t);
+        if (s.nflag < 0) {
+          retval = (s.nflag == LSETUP_FAIL || s.nflag == LSOLVE_FAIL
+                    || s.nflag == RHSFUNC_FAIL) ? s.nflag : NLS_FAIL;
+          goto L_step_fail;
+        }
+        s.ncf++;
+        s.etamax = 1.0;
+        if ((fabs(s.h) <= 0.0) || (s.ncf == o.max_conv_fails)) {
+          if (s.nflag == NLS_CONV_RECVR) { retval = CONV_FAILURE; goto L_step_fail; }
+          if (s.nflag == RHSFUNC_RECVR) { retval = REPTD_RHSFUNC_ERR; goto L_step_fail; }
+        }
+        s.eta = smax_(ETA_CF, 0.0 / fabs(s.h));
+        s.nflag = PREV_CONV_FAIL;
+        rescale_();
+        goto L_attempt;
+      }
+      // cvDoErrorTest (bdf_cell.hpp:1339-1381)
+      const double dsm = s.acnrm * s.tq[2];
+      s.dsm = dsm;
+      if (dsm <= 1.0) goto L_step_ok;
+      s.nef++;
+      s.st[ST_NETF]++;
+      s.nflag = PREV_ERR_FAIL;
+      restore_(s.saved_t);
+      if ((fabs(s.h) <= 0.0) || (s.nef == o.max_err_fails)) {
+        retval = ERR_FAILURE;
+        goto L_step_fail;
+      }
+      s.etamax = 1.0;
+      if (s.nef <= MXNEF1) {
+        s.eta = 1.0 / (pow(BIAS2 * dsm, 1.0 / s.L) + ADDON);
+        s.eta = smax_(ETA_MIN_EF, smax_(s.eta, 0.0 / fabs(s.h)));
+        if (s.nef >= SMALL_NEF) s.eta = smin_(s.eta, ETA_MAX_EF);
+        rescale_();
+        goto L_attempt;
+      }
+      if (s.q > 1) {
+        s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
+        adjust_order_(-1);
+        s.L = s.q;
+        s.q--;
+        s.qwait = s.L;
+        rescale_();
+        goto L_attempt;
+      }
+      s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
+      s.h *= s.eta;
+      s.next_h = s.h;
+      s.hscale = s.h;
+      s.qwait = LONG_WAIT;
+      s.nscon = 0;
+      request_rhs(s.zn[0], PC_ERRTEST_RHS);
+      return REQ_RHS;
+    }
+  L_errtest_rhs: {
+      KB_UNROLL for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      s.st[ST_NFE]++;
+      if (s.rhs_ret > 0) { retval = UNREC_RHSFUNC_ERR; goto L_step_fail; }
+      scale_<N>(s.h, s.tempv, s.zn[1]);
+      goto L_attempt;
+    }
+  L_step_ok: {
+      complete_step_();
+      prepare_next_step_(s.dsm);
+      s.etamax = (s.st[ST_NST] <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
+      scale_<N>(s.tq[2], s.acor, s.acor);
+      s.nstloc++;
+      if ((s.tn - s.dt) * s.h >= 0.0) {
+        s.tret = s.dt;
+        get_dky_(s.dt, s.y);  // y(tout) into y
+        s.next_q = s.qprime;
+        s.next_h = s.hprime;
+        retval = SUCCESS;
+        goto L_solve_end;
+      }
+      goto L_step_loop;
+    }
+  L_step_fail: {
+      s.tret = s.tn;
+      goto L_solve_end;
+    }
+  L_solve_end: {
+      // the restart wrapper (bdf_cell.hpp:1536-1546). y holds y(tout) on
+      // success; on failure the last accepted state, which is zn[0] (also
+      // when the failure precedes the first step: zn[0] is then the state
+      // of the last reinit, the reference's untouched yout)
+      if (retval < 0) {
+        KB_UNROLL for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
+      }
+      for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
+      if (retval >= 0) {
+        *flag_out = 0;
+        s.pc = PC_IDLE;
+        return REQ_DONE;
+      }
+      const bool restartable = retval == ERR_FAILURE || retval == CONV_FAILURE
+                               || retval == REPTD_RHSFUNC_ERR;
+      if (!restartable || s.restarts >= o.max_restarts) {
+        *flag_out = retval;
+        s.pc = PC_IDLE;
+        return REQ_DONE;
+      }
+      ++s.restarts;
+      const double hcur = s.next_h;
+      reinit(s.tret, s.y, hcur > 0.0 ? 0.1 * hcur : 0.0);
+      goto L_solve;
+    }
+  }
+
+  // cvNlsResidual's tail after its rhs (bdf_cell.hpp:1022-1032)
+  __device__ int residual_done_() {
+    KB_UNROLL for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
+    s.st[ST_NFE]++;
+    if (s.rhs_ret > 0) return RHSFUNC_RECVR;
+    lin_sum_<N>(s.rl1, s.zn[1], 1.0, s.acor, s.delta);
+    lin_sum_<N>(-s.gamma, s.ftemp, 1.0, s.delta, s.delta);
+    return SUCCESS;
+  }
+};
+
+}  // namespace kbl

@@ -28,6 +28,7 @@
 
 #include KB_NET_HEADER
 #include "bdf_warp.cuh"
+#include "bdf_lane.cuh"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
 
@@ -103,6 +104,264 @@ kb_cells_persistent(int ncell, double* n, double* T, const double* dt,
   }
 }
 
+// ---- lane-per-cell kernels (bdf_lane.cuh) ----
+
+template <bool EVT>
+struct LaneGeo {
+  static constexpr int N = kbnet::NSPEC + (EVT ? 1 : 0);
+  // per-warp shared memory: the Jacobian being assembled (column-major)
+  // and two rhs vectors (the hybrid Jacobian's Tgas column)
+  static constexpr int SMEM_DOUBLES = N * N + 2 * N;
+};
+
+// the warp serves lane `src`'s Jacobian request: lane j < N evaluates the
+// rhs perturbed in component j (the difference-quotient column j,
+// bdf_cell.hpp:1290-1311), or the hybrid analytic Jacobian's terms
+// (solve_cell.hpp:883-1118: lane j < NSPEC the thermal row's species j,
+// lane NSPEC the base state, lanes NSPEC+1 / NSPEC+2 the Tgas column at
+// T + h / T - h; lane src the stoichiometric block); the result lands in
+// lane src's savedJ
+template <bool EVT>
+__device__ void serve_jac(kbl::LaneCell<LaneGeo<EVT>::N>& s, int src,
+                          const SolveOpts& so, double* sJ) {
+  constexpr int N = LaneGeo<EVT>::N;
+  using namespace kbnet;
+  const unsigned FULLM = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  double yf[N], fy[N], f[N], k[NREA + 1];
+  KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = __shfl_sync(FULLM, s.y[i], src);
+  Params p;
+  {
+    double row[NPAR];
+    const double* ps = reinterpret_cast<const double*>(&s.p);
+    KB_UNROLL for (int i = 0; i < NPAR; ++i) row[i] = __shfl_sync(FULLM, ps[i], src);
+    params_from_row(row, p);
+  }
+  const double Tfix = __shfl_sync(FULLM, s.Tfix, src);
+  bool hit = false;
+  int ret = 0;
+  long ndq = 0;
+  if (so.jac == 2) {
+    KB_UNROLL for (int i = 0; i < N; ++i) fy[i] = __shfl_sync(FULLM, s.ftemp[i], src);
+    double ewtf[N];
+    KB_UNROLL for (int i = 0; i < N; ++i) ewtf[i] = __shfl_sync(FULLM, s.ewt[i], src);
+    const double h = __shfl_sync(FULLM, s.h, src);
+    const double srur = kbw::ssqrt_(kbw::UROUND);
+    double sum = 0.0;
+    KB_UNROLL for (int i = 0; i < N; ++i) {
+      const double pv = fy[i] * ewtf[i];
+      sum += pv * pv;
+    }
+    const double fnorm = kbw::ssqrt_(sum / N);
+    const double minInc = (fnorm != 0.0)
+        ? (kbw::MIN_INC_MULT * fabs(h) * kbw::UROUND * (double)N * fnorm) : 1.0;
+    const int j = lane < N ? lane : 0;
+    const double yj = kbw::pick<N>(yf, j);
+    const double ewj = kbw::pick<N>(ewtf, j);
+    const double inc = kbw::smax_(srur * fabs(yj), minInc / ewj);
+    KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = (i == lane) ? yf[i] + inc : yf[i];
+    int r = kbw::rhs_check<N, EVT>(yf, f, p, Tfix, k, hit);
+    if (lane >= N) { r = 0; hit = false; }
+    const unsigned bad = __ballot_sync(FULLM, r != 0);
+    const int first_bad = bad ? __ffs(bad) - 1 : N;
+    ndq = bad ? first_bad + 1 : N;
+    ret = bad ? 1 : 0;
+    hit = __any_sync(FULLM, hit && lane <= first_bad);
+    if (lane < N && lane < first_bad) {
+      const double inc_inv = 1.0 / inc;
+      KB_UNROLL for (int i = 0; i < N; ++i) sJ[i + lane * N] = inc_inv * (f[i] - fy[i]);
+    }
+  } else {
+    const double T = EVT ? fmin(fmax(yf[N - 1], p.Tcmb), 1e9)
+                         : fmin(fmax(Tfix, p.Tcmb), 1e9);
+    if (lane == 0) {
+      KB_UNROLL for (int i = 0; i <= NREA; ++i) k[i] = 0.0;
+      rates_fixed(T, yf, p, k);
+      rates_var(T, yf, p, k);
+      jac_stoich(yf, k, sJ, 1, N);  // column-major: (i, j) at i + j N
+    }
+    if (EVT) {
+      constexpr int iT = N - 1;
+      double sumabs = 0.0;
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) sumabs += fabs(yf[i]);
+      const double hT = fmax(1e-6 * fabs(yf[iT]), 1e-8);
+      const double yjl = kbw::pick<N>(yf, lane < N ? lane : 0);
+      const double hj = lane < NSPEC
+          ? fmax(fmax(1e-7 * fabs(yjl), 1e-9 * sumabs), 1e-30) : 1.0;
+      KB_UNROLL for (int i = 0; i < N; ++i) {
+        double v = yf[i];
+        if (lane < NSPEC && i == lane) v = yf[i] + hj;
+        if (lane == NSPEC + 1 && i == iT) v = yf[iT] + hT;
+        if (lane == NSPEC + 2 && i == iT) v = yf[iT] - hT;
+        yf[i] = v;
+      }
+      const double Tl = (lane == NSPEC + 1 || lane == NSPEC + 2)
+                            ? fmin(fmax(yf[iT], p.Tcmb), 1e9) : T;
+      KB_UNROLL for (int i = 0; i <= NREA; ++i) k[i] = 0.0;
+      rates_fixed(Tl, yf, p, k);
+      rates_var(Tl, yf, p, k);
+      rhs(yf, k, f);
+      const double Tth = fmin(fmax(yf[iT], 2.73), 1e9);
+      f[iT] = thermal_dTdt(Tth, yf, k, p);
+      double* sv = sJ + N * N;
+      __syncwarp();
+      if (lane == NSPEC + 1) { KB_UNROLL for (int i = 0; i < N; ++i) sv[i] = f[i]; }
+      if (lane == NSPEC + 2) { KB_UNROLL for (int i = 0; i < N; ++i) sv[N + i] = f[i]; }
+      __syncwarp();
+      if (lane < N) sJ[lane + iT * N] = (sv[lane] - sv[N + lane]) / (2.0 * hT);
+      const double f0 = __shfl_sync(FULLM, f[iT], NSPEC);
+      if (lane < NSPEC) sJ[iT + lane * N] = (f[iT] - f0) / hj;
+    }
+  }
+  __syncwarp();
+  if (lane == src) {
+    for (int i = 0; i < N * N; ++i) s.savedJ[i] = sJ[i];
+    s.ls_retval = ret;
+    s.st[kbw::ST_NFEDQ] += ndq;
+    s.hitT0 = s.hitT0 || hit;
+  }
+  __syncwarp();
+}
+
+// start cell c on this lane: false when the cell needs no integration
+// (its flag is written here)
+template <bool EVT>
+__device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
+                           kbl::Machine<LaneGeo<EVT>::N, EVT>& m, int c,
+                           const double* n, const double* T, const double* dt,
+                           const double* par, int pstride, int* flags,
+                           long* stats, const SolveOpts& so) {
+  constexpr int N = LaneGeo<EVT>::N;
+  using namespace kbnet;
+  const double dtc = dt[c];
+  int skip_flag = 1;
+  if (so.fail_every > 0 && (c + 1) % so.fail_every == 0) skip_flag = kbw::TOO_MUCH_WORK;
+  else if (!(dtc > 0.0)) skip_flag = 0;
+  if (skip_flag != 1) {
+    if (flags != nullptr) flags[c] = skip_flag;
+    if (stats != nullptr)
+      for (int i = 0; i < NSTAT; ++i) stats[(long)c * NSTAT + i] = 0;
+    return false;
+  }
+  params_from_row(par + (long)c * pstride, s.p);
+  if (params_missing(s.p) >= 0) {
+    if (flags != nullptr) flags[c] = kbw::FLAG_PARAM_UNSET;
+    return false;
+  }
+  s.cell = c;
+  s.dt = dtc;
+  s.Tfix = T[c];
+  s.hitT0 = false;
+  s.restarts = 0;
+  for (int i = 0; i < NSTAT; ++i) s.tot[i] = 0;
+  double y0[N];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) y0[i] = n[(long)c * NSPEC + i];
+  if (EVT) y0[N - 1] = T[c];
+  KB_UNROLL for (int i = 0; i < N; ++i) s.atol[i] = i < NSPEC ? so.atol_n : so.atol_T;
+  s.atolmin0 = (so.atol_n == 0.0) || (EVT && so.atol_T == 0.0);
+  s.mxstep = so.max_steps == 0 ? 500
+             : (so.max_steps < 0 ? KB_MAX_STEPS_CAP : so.max_steps);
+  m.reinit(0.0, y0, 0.0);
+  s.pc = kbl::PC_NEW;
+  return true;
+}
+
+// the post-solve rules of solve() (solve_cell.hpp:2156-2176) and the
+// write-back of a finished cell
+template <bool EVT>
+__device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
+                            double* n, double* T, int* flags, long* stats,
+                            const SolveOpts& so) {
+  constexpr int N = LaneGeo<EVT>::N;
+  using namespace kbnet;
+  const int c = s.cell;
+  s.tot[kbw::ST_RESTARTS] = s.restarts;
+  if (stats != nullptr)
+    for (int i = 0; i < NSTAT; ++i) stats[(long)c * NSTAT + i] = s.tot[i];
+  const double Tend = s.y[N - 1];
+  if (flag == 0 && EVT && !(Tend > 0.0 && isfinite(Tend)))
+    flag = kbw::FLAG_NONPOSITIVE_T;
+  if (s.hitT0 && (flag == kbw::REPTD_RHSFUNC_ERR || flag == kbw::RHSFUNC_FAIL
+                  || flag == kbw::UNREC_RHSFUNC_ERR
+                  || flag == kbw::FIRST_RHSFUNC_ERR))
+    flag = kbw::FLAG_NONPOSITIVE_T;
+  if (flag == 0) {
+    KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
+      double v = s.y[i];
+      if (so.clip_negative && v < 0.0) v = 0.0;
+      n[(long)c * NSPEC + i] = v;
+    }
+    if (EVT) T[c] = Tend;
+  }
+  if (flags != nullptr) flags[c] = flag;
+  s.cell = -1;
+}
+
+// one warp = 32 cells in flight. persistent == 0: each lane integrates the
+// cell of its global thread index; persistent == 1: lanes pull cells from
+// the device work queue (`cursor`) until it is exhausted
+template <bool EVT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+kb_lane_cells(int ncell, double* n, double* T, const double* dt,
+              const double* par, int pstride, int* flags, long* stats,
+              SolveOpts so, unsigned* cursor, int persistent) {
+  constexpr int N = LaneGeo<EVT>::N;
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5;
+  double* sJ = smem + warp * LaneGeo<EVT>::SMEM_DOUBLES;
+  kbl::LaneCell<N> s;
+  kbl::Machine<N, EVT> m(s, so);
+  s.cell = -1;
+  s.pc = kbl::PC_IDLE;
+  bool static_taken = false;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  bool exhausted = false;
+  for (;;) {
+    int req = kbl::REQ_NONE;
+    // 1. advance this lane to its next request, taking new cells as the
+    //    current one finishes
+    while (!exhausted) {
+      if (s.cell < 0) {
+        int c;
+        if (persistent) {
+          c = (int)atomicAdd(cursor, 1u);
+        } else {
+          c = static_taken ? ncell : gtid;
+          static_taken = true;
+        }
+        if (c >= ncell) { exhausted = true; break; }
+        if (!lane_start<EVT>(s, m, c, n, T, dt, par, pstride, flags, stats, so))
+          continue;
+      }
+      int flag = 0;
+      req = m.advance(&flag);
+      if (req == kbl::REQ_DONE) {
+        lane_finish<EVT>(s, flag, n, T, flags, stats, so);
+        req = kbl::REQ_NONE;
+        continue;
+      }
+      break;
+    }
+    if (__all_sync(0xffffffffu, exhausted)) break;
+    // 2. the warp serves the Jacobian requests, one cell at a time
+    unsigned jm = __ballot_sync(0xffffffffu, req == kbl::REQ_JAC);
+    while (jm) {
+      const int src = __ffs(jm) - 1;
+      jm &= jm - 1;
+      serve_jac<EVT>(s, src, so, sJ);
+    }
+    // 3. the rhs requests, in one SIMT pass
+    if (req == kbl::REQ_RHS) {
+      double yf[N], f[N], k[kbnet::NREA + 1];
+      KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = s.yreq[i];
+      bool hit = false;
+      s.rhs_ret = kbw::rhs_check<N, EVT>(yf, f, s.p, s.Tfix, k, hit);
+      if (hit) s.hitT0 = true;
+      KB_UNROLL for (int i = 0; i < N; ++i) s.freq[i] = f[i];
+    }
+  }
+}
+
 // ---- options (krome_opts keys, reference krome.cpp:198-300) ----
 }  // namespace
 
@@ -118,6 +377,7 @@ struct krome_opts {
   long long device_memory = 0;
   // this library's keys
   int kernel = 1;          // 0 plain, 1 persistent work queue
+  int layout = 1;          // 0 one warp per cell, 1 one lane per cell
   int queue_chunk = 1;     // cells per queue pop
   int blocks_per_sm = 0;   // persistent grid: 0 = occupancy limit
   int fail_every = 0;      // fault injection (tests)
@@ -187,6 +447,30 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    int* flags, long* stats, unsigned* cursor,
                    cudaStream_t stream) {
   const SolveOpts so = to_solve_opts(h);
+  if (h.layout == 1) {  // lane per cell
+    const size_t lsmem =
+        sizeof(double) * kWarpsPerBlock * LaneGeo<EVT>::SMEM_DOUBLES;
+    const int threads = kWarpsPerBlock * 32;
+    long blocks;
+    if (h.kernel == 0) {
+      blocks = ((long)ncell + threads - 1) / threads;
+    } else {
+      int per_sm = h.blocks_per_sm;
+      if (per_sm <= 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, kb_lane_cells<EVT>, threads, lsmem);
+        if (per_sm <= 0) per_sm = 1;
+      }
+      blocks = (long)num_sms() * per_sm;
+      const long need = ((long)ncell + threads - 1) / threads;
+      if (blocks > need) blocks = need > 0 ? need : 1;
+      cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(unsigned), stream);
+      if (e != cudaSuccess) return e;
+    }
+    kb_lane_cells<EVT><<<(int)blocks, threads, lsmem, stream>>>(
+        ncell, n, T, dt, par, pstride, flags, stats, so, cursor, h.kernel);
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(double) * kWarpsPerBlock * Geo<EVT>::SMEM_DOUBLES;
   if (h.kernel == 0) {
     const int blocks = (ncell + kWarpsPerBlock - 1) / kWarpsPerBlock;
@@ -325,6 +609,7 @@ int* int_key(krome_opts* h, const char* k) {
       {"jac", offsetof(krome_opts, jac)},
       {"linsol", offsetof(krome_opts, linsol)},
       {"kernel", offsetof(krome_opts, kernel)},
+      {"layout", offsetof(krome_opts, layout)},
       {"queue_chunk", offsetof(krome_opts, queue_chunk)},
       {"blocks_per_sm", offsetof(krome_opts, blocks_per_sm)},
       {"fail_every", offsetof(krome_opts, fail_every)},
@@ -374,6 +659,7 @@ KB_API int krome_opts_set(krome_opts* h, const char* key, double v) {
   if (!std::strcmp(key, "path") && (x < 0 || x > 2)) return -1;
   if (!std::strcmp(key, "conserve") && (x < 0 || x > 3)) return -1;
   if (!std::strcmp(key, "kernel") && (x < 0 || x > 1)) return -1;
+  if (!std::strcmp(key, "layout") && (x < 0 || x > 1)) return -1;
   if ((!std::strcmp(key, "max_err_fails") || !std::strcmp(key, "max_conv_fails")
        || !std::strcmp(key, "max_restarts") || !std::strcmp(key, "queue_chunk")
        || !std::strcmp(key, "fail_every") || !std::strcmp(key, "blocks_per_sm"))
@@ -430,7 +716,7 @@ KB_API int krome_b200_solve_device(int ncell, double* n, double* Tgas,
       || flags == nullptr)
     return -1;
   if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
-  if (h->kernel == 1 && cursor == nullptr) return -1;
+  if (cursor == nullptr && (h->kernel == 1)) return -1;
   if (const int u = unsupported(*h)) return u;
   const cudaError_t e = launch_any(*h, ncell, n, Tgas, dt, par, par_stride,
                                    flags, stats, cursor,
