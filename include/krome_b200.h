@@ -1,0 +1,143 @@
+/* libkrome_b200_<net>.so -- the drop-in C ABI of the per-cell chemistry and
+ * gas-temperature solve, computed on a B200 (sm_100a).
+ *
+ * One library per generated network (krome_x_b200/networks/net_<net>.h),
+ * as the reference builds one libkrome per generated project. The entry
+ * points below keep the reference's names, argument meanings, array
+ * layouts and return flags; each cites the reference declaration it
+ * replaces (runtime/interfaces/C/krome.h in the reference tree). The
+ * krome_b200_* entry points are additions of this library.
+ *
+ * Layouts (as the reference): n[ncell][nspec] cell-major, species in the
+ * network's code-point order; Tgas, dt [ncell]; par one row broadcast to
+ * every cell (par_stride 0) or rows [ncell][npar] (par_stride npar).
+ * Flags: 0 success; CVODE's -1 ... -27 for a failed integration (the cell
+ * left untouched); -105 a REQUIRED parameter unset in some row (nothing
+ * integrated); -110 the integration ended at Tgas <= 0; -104 a
+ * configuration this library does not run (LAPACK or sparse linsol,
+ * conservation) or no usable GPU; -111 the device buffers could not be
+ * allocated; -1 bad arguments. There is no CPU fallback.
+ */
+#ifndef KROME_B200_H
+#define KROME_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct krome_opts krome_opts;
+
+/* ---- network description (reference krome.h:96-114) ---- */
+/* krome.h:96 */
+const char* krome_flag_message(int flag);
+/* krome.h:99 */
+const char* krome_version(void);
+/* krome.h:101 */
+const char* krome_network_name(void);
+/* krome.h:102-104 */
+int krome_nspec(void);
+int krome_nrea(void);
+int krome_npar(void);
+/* krome.h:105-108 */
+const char* krome_species_name(int i);
+int krome_species_index(const char* name);
+const char* krome_param_name(int i);
+int krome_param_index(const char* name);
+/* krome.h:111: one row of npar defaults; a REQUIRED parameter is NaN */
+void krome_params_default(double* par);
+/* krome.h:114 */
+const char* krome_param_required_by(int i);
+
+/* ---- options (reference krome.h:170-173, keys krome.cpp:198-260) ----
+ * Keys as the reference: evolve_T, jac (0 auto, 1 analytic, 2 fd), linsol
+ * (0 auto, 1 dense; 2 lapack and 3 sparse return -104 from a solve),
+ * rtol, atol_n, atol_T, atol_u, max_steps, max_err_fails, max_conv_fails,
+ * max_restarts, clip_negative, error_report, renormalize_x, conserve,
+ * path, device_cache, device_memory, min_device, min_interleave. This
+ * library's keys: layout (0 one warp per cell, 1 one lane per cell),
+ * kernel (0 plain, 1 persistent work queue), lane_minb (2, 3, 4: the
+ * lane kernel's register budget), queue_chunk, blocks_per_sm, fail_every
+ * (fault injection: every k-th cell reports -1 untouched). Unknown key or
+ * bad value: -1. */
+krome_opts* krome_opts_new(void);
+void krome_opts_free(krome_opts* h);
+int krome_opts_set(krome_opts* h, const char* key, double value);
+int krome_opts_get(const krome_opts* h, const char* key, double* value);
+
+/* ---- the solve (reference krome.h:291-294, krome.cpp:396-438) ----
+ * Host arrays, updated in place; extra (the reference's krome_cells of
+ * photon / dust rows) must be NULL for these networks; flags[ncell] may
+ * be NULL. Returns 0 or the lowest-index failing cell's flag. */
+int krome_solve_cells(int ncell, double* n, double* Tgas, const double* dt,
+                      const double* par, int par_stride, const void* extra,
+                      int* flags, const krome_opts* h);
+
+/* krome_get_rates (reference krome.h:387-389): k[ncell][nrea] at each
+ * cell's rate temperature clamp(Tgas, Tcmb, 1e9); Phi and h unused */
+int krome_get_rates(int ncell, const double* n, const double* Tgas,
+                    const double* par, int par_stride, const double* Phi,
+                    const void* h, double* k);
+
+/* krome_has_device (reference krome.h:193): 1 when a CUDA device is
+ * visible */
+int krome_has_device(void);
+
+/* ---- additions of this library ---- */
+
+/* the number of per-cell counters, and the equations of a cell */
+int krome_b200_nstat(void);
+int krome_b200_neq(int evolve_T);
+
+/* krome_solve_cells with per-cell counters: stats[ncell][nstat] (nst, nfe,
+ * nfeDQ, nje, nsetups, nni, nnf, netf, restarts; may be NULL). The
+ * batched entry point the Python binding's solve / solve_batch use. */
+int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
+                           const double* dt, const double* par,
+                           int par_stride, int* flags, long* stats,
+                           const krome_opts* h);
+
+/* device-resident solve (the role of the reference's
+ * krome_solve_cells_device, krome.h:339-344, cell-major layout): every
+ * pointer is device memory, n and Tgas updated in place, flags[ncell]
+ * (required), stats optional, cursor one unsigned (the persistent
+ * kernel's work queue; reset by the call). Asynchronous on `stream` (a
+ * cudaStream_t, NULL the legacy stream); no host synchronization, so it
+ * can be captured in a CUDA graph. The required-parameter rule is checked
+ * per cell on the device (-105 in that cell's flag). Returns 0 after a
+ * successful launch, -1 bad arguments, -104 launch failure. */
+int krome_b200_solve_device(int ncell, double* n, double* Tgas,
+                            const double* dt, const double* par,
+                            int par_stride, int* flags, long* stats,
+                            unsigned* cursor, const krome_opts* h,
+                            void* stream);
+
+/* one step of the reference's collapse driver on device arrays
+ * (examples/tests/collapse/test.cpp:47-63): tff = the free-fall time of
+ * each cell's current densities written into parameter tff_index, every
+ * density x factor, dt = dtfrac tff, then krome_b200_solve_device.
+ * par must be per-cell rows (par_stride npar). Asynchronous on stream. */
+int krome_b200_hydro_step(int ncell, double* n, double* Tgas, double* dt,
+                          double* par, int par_stride, int tff_index,
+                          double factor, double dtfrac, int* flags,
+                          long* stats, unsigned* cursor, const krome_opts* h,
+                          void* stream);
+
+/* krome_b200_hydro_step captured once as a CUDA graph on `stream` (a
+ * non-default stream) and replayed with krome_b200_graph_launch; the arrays
+ * stay bound to the graph. new returns NULL on failure. */
+void* krome_b200_graph_new(int ncell, double* n, double* Tgas, double* dt,
+                           double* par, int par_stride, int tff_index,
+                           double factor, double dtfrac, int* flags,
+                           long* stats, unsigned* cursor, const krome_opts* h,
+                           void* stream);
+int krome_b200_graph_launch(void* graph, void* stream);
+void krome_b200_graph_free(void* graph);
+
+/* the FP64 pipe's peak of this GPU, measured with register-resident DFMA
+ * chains over the whole device [TFLOP/s] (the roofline's denominator) */
+int krome_b200_fp64_peak(double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KROME_B200_H */

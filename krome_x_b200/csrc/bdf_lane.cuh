@@ -102,11 +102,11 @@ struct LaneCell {
 template <int N>
 __device__ __forceinline__ void axpy_(double a, const double* x, double* y) {
   if (a == 1.0) {
-    KB_UNROLL for (int i = 0; i < N; i++) y[i] += x[i];
+    for (int i = 0; i < N; i++) y[i] += x[i];
   } else if (a == -1.0) {
-    KB_UNROLL for (int i = 0; i < N; i++) y[i] -= x[i];
+    for (int i = 0; i < N; i++) y[i] -= x[i];
   } else {
-    KB_UNROLL for (int i = 0; i < N; i++) y[i] += a * x[i];
+    for (int i = 0; i < N; i++) y[i] += a * x[i];
   }
 }
 template <int N>
@@ -115,48 +115,48 @@ __device__ __forceinline__ void lin_sum_(double a, const double* x, double b,
   if (b == 1.0 && z == y) { axpy_<N>(a, x, z); return; }
   if (a == 1.0 && z == x) { axpy_<N>(b, y, z); return; }
   if (a == 1.0 && b == 1.0) {
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
+    for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
     return;
   }
   bool test;
   if ((test = (a == 1.0 && b == -1.0)) || (a == -1.0 && b == 1.0)) {
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
+    for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
     return;
   }
   if ((test = (a == 1.0)) || b == 1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
+    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
     return;
   }
   if ((test = (a == -1.0)) || b == -1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
+    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
     return;
   }
   if (a == b) {
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
+    for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
     return;
   }
   if (a == -b) {
-    KB_UNROLL for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
+    for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
     return;
   }
-  KB_UNROLL for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
+  for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
 }
 template <int N>
 __device__ __forceinline__ void scale_(double c, const double* x, double* z) {
-  KB_UNROLL for (int i = 0; i < N; i++) z[i] = c * x[i];
+  for (int i = 0; i < N; i++) z[i] = c * x[i];
 }
 template <int N>
 __device__ __forceinline__ double wrms_(const double* x, const double* w) {
   double sum = 0.0;
-  KB_UNROLL for (int i = 0; i < N; i++) {
+  for (int i = 0; i < N; i++) {
     const double pv = x[i] * w[i];
     sum += pv * pv;
   }
@@ -218,20 +218,20 @@ struct Machine {
   __device__ Machine(LaneCell<N>& s_, const SolveOpts& o_) : s(s_), o(o_) {}
 
   __device__ int ewt_set(const double* ycur, double* w) {
-    KB_UNROLL for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
-    KB_UNROLL for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
+    for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
+    for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
     if (s.atolmin0) {
       double mn = w[0];
-      KB_UNROLL for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
+      for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
       if (mn <= 0.0) return -1;
     }
-    KB_UNROLL for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
+    for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
     return 0;
   }
 
   __device__ void reinit(double t0, const double* y0, double h_init) {
     s.tn = t0;
-    KB_UNROLL for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
+    for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
     s.q = 1; s.L = 2; s.qwait = s.L;
     s.etamax = ETA_MAX_FS;
     s.qu = 0; s.hu = 0.0; s.tolsf = 1.0;
@@ -246,7 +246,7 @@ struct Machine {
   }
 
   __device__ __forceinline__ void request_rhs(const double* yv, int pc) {
-    KB_UNROLL for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
+    for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
     s.pc = pc;
   }
 
@@ -369,7 +369,7 @@ struct Machine {
     for (int j = 0; j <= s.q; j++) axpy_<N>(s.l[j], s.acor, s.zn[j]);
     s.qwait--;
     if ((s.qwait == 1) && (s.q != QMAX)) {
-      KB_UNROLL for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
       s.saved_tq5 = s.tq[5];
     }
   }
@@ -428,7 +428,7 @@ struct Machine {
     } else {
       s.eta = s.etaqp1;
       s.qprime = s.q + 1;
-      KB_UNROLL for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
     }
     set_eta_();
   }
@@ -445,14 +445,14 @@ struct Machine {
   // (bdf_cell.hpp:1266-1287)
   __device__ double inv_dot_(const double* x) const {
     double sum = 0.0;
-    KB_UNROLL for (int i = 0; i < NSPEC; i++)
+    for (int i = 0; i < NSPEC; i++)
       if (species_charge(i) != 0) sum += species_charge(i) * x[i];
     return sum;
   }
   __device__ void inv_set_(double* x, double target) const {
     const int r = IDX_ELECTRON;
     double sum = 0.0, sa = 0.0;
-    KB_UNROLL for (int i = 0; i < NSPEC; i++)
+    for (int i = 0; i < NSPEC; i++)
       if (i != r && species_charge(i) != 0) {
         sum += species_charge(i) * x[i];
         sa += fabs(species_charge(i) * (s.zn[0][i] + s.acor[i]));
@@ -526,7 +526,7 @@ struct Machine {
       return REQ_RHS;
     }
   L_first_rhs: {
-      KB_UNROLL for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
+      for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
       s.st[ST_NFE]++;
       if (s.rhs_ret > 0) { retval = FIRST_RHSFUNC_ERR; goto L_solve_end; }
       s.h = s.hin;
@@ -542,14 +542,14 @@ struct Machine {
       {  // cvUpperBoundH0
         double* temp1 = s.tempv;
         double* temp2 = s.acor;
-        KB_UNROLL for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[0][i]);
+        for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[0][i]);
         ewt_set(s.zn[0], temp1);
-        KB_UNROLL for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
+        for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
         lin_sum_<N>(HUB_FACTOR, temp2, 1.0, temp1, temp1);
-        KB_UNROLL for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[1][i]);
-        KB_UNROLL for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
+        for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[1][i]);
+        for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
         double hub_inv = 0.0;
-        KB_UNROLL for (int i = 0; i < N; i++)
+        for (int i = 0; i < N; i++)
           if (fabs(temp1[i]) > hub_inv) hub_inv = fabs(temp1[i]);
         double hub = HUB_FACTOR * tdist;
         if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
@@ -574,7 +574,7 @@ struct Machine {
       return REQ_RHS;
     }
   L_hin_rhs: {
-      KB_UNROLL for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
       s.st[ST_NFE]++;
       bool hgOK = false;
       double yddnrm = 0.0;
@@ -661,7 +661,7 @@ struct Machine {
       s.callSetup = (s.nflag == PREV_CONV_FAIL) || (s.nflag == PREV_ERR_FAIL)
                     || (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlp + MSBP)
                     || (fabs(s.gamrat - 1.0) > DGMAX_LSETUP);
-      KB_UNROLL for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+      for (int i = 0; i < N; i++) s.acor[i] = 0.0;
       s.tol = s.tq[4];
       s.jbad = false;
       s.niters = 0;
@@ -741,7 +741,7 @@ struct Machine {
         s.nconvfails++;
         s.callSetup = true;
         s.jbad = true;
-        KB_UNROLL for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+        for (int i = 0; i < N; i++) s.acor[i] = 0.0;
         goto L_nls_outer;
       }
     }
@@ -813,7 +813,7 @@ struct Machine {
       return REQ_RHS;
     }
   L_errtest_rhs: {
-      KB_UNROLL for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
       s.st[ST_NFE]++;
       if (s.rhs_ret > 0) { retval = UNREC_RHSFUNC_ERR; goto L_step_fail; }
       scale_<N>(s.h, s.tempv, s.zn[1]);
@@ -845,7 +845,7 @@ struct Machine {
       // when the failure precedes the first step: zn[0] is then the state
       // of the last reinit, the reference's untouched yout)
       if (retval < 0) {
-        KB_UNROLL for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
+        for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
       }
       for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
       if (retval >= 0) {
@@ -869,7 +869,7 @@ struct Machine {
 
   // cvNlsResidual's tail after its rhs (bdf_cell.hpp:1022-1032)
   __device__ int residual_done_() {
-    KB_UNROLL for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
+    for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
     s.st[ST_NFE]++;
     if (s.rhs_ret > 0) return RHSFUNC_RECVR;
     lin_sum_<N>(s.rl1, s.zn[1], 1.0, s.acor, s.delta);

@@ -109,119 +109,18 @@ kb_cells_persistent(int ncell, double* n, double* T, const double* dt,
 template <bool EVT>
 struct LaneGeo {
   static constexpr int N = kbnet::NSPEC + (EVT ? 1 : 0);
-  // per-warp shared memory: the Jacobian being assembled (column-major)
-  // and two rhs vectors (the hybrid Jacobian's Tgas column)
-  static constexpr int SMEM_DOUBLES = N * N + 2 * N;
+  // lanes one Jacobian request occupies: the N difference-quotient
+  // columns, or the hybrid analytic Jacobian's NSPEC species + base +
+  // Tgas +/- h states
+  static constexpr int JLANES_DQ = N;
+  static constexpr int JLANES_AN = EVT ? kbnet::NSPEC + 3 : 1;
+  static constexpr int ROLE_BASE = EVT ? kbnet::NSPEC : 0;
+  // per-warp shared memory: the Jacobians being assembled (column-major,
+  // one N x N block per request of a pass) and the Tgas +/- h rhs
+  // vectors of the hybrid Jacobian
+  static constexpr int MAXJ = 32 / (JLANES_DQ < JLANES_AN ? JLANES_DQ : JLANES_AN);
+  static constexpr int SMEM_DOUBLES = MAXJ * (N * N + 2 * N);
 };
-
-// the warp serves lane `src`'s Jacobian request: lane j < N evaluates the
-// rhs perturbed in component j (the difference-quotient column j,
-// bdf_cell.hpp:1290-1311), or the hybrid analytic Jacobian's terms
-// (solve_cell.hpp:883-1118: lane j < NSPEC the thermal row's species j,
-// lane NSPEC the base state, lanes NSPEC+1 / NSPEC+2 the Tgas column at
-// T + h / T - h; lane src the stoichiometric block); the result lands in
-// lane src's savedJ
-template <bool EVT>
-__device__ void serve_jac(kbl::LaneCell<LaneGeo<EVT>::N>& s, int src,
-                          const SolveOpts& so, double* sJ) {
-  constexpr int N = LaneGeo<EVT>::N;
-  using namespace kbnet;
-  const unsigned FULLM = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  double yf[N], fy[N], f[N], k[NREA + 1];
-  KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = __shfl_sync(FULLM, s.y[i], src);
-  Params p;
-  {
-    double row[NPAR];
-    const double* ps = reinterpret_cast<const double*>(&s.p);
-    KB_UNROLL for (int i = 0; i < NPAR; ++i) row[i] = __shfl_sync(FULLM, ps[i], src);
-    params_from_row(row, p);
-  }
-  const double Tfix = __shfl_sync(FULLM, s.Tfix, src);
-  bool hit = false;
-  int ret = 0;
-  long ndq = 0;
-  if (so.jac == 2) {
-    KB_UNROLL for (int i = 0; i < N; ++i) fy[i] = __shfl_sync(FULLM, s.ftemp[i], src);
-    double ewtf[N];
-    KB_UNROLL for (int i = 0; i < N; ++i) ewtf[i] = __shfl_sync(FULLM, s.ewt[i], src);
-    const double h = __shfl_sync(FULLM, s.h, src);
-    const double srur = kbw::ssqrt_(kbw::UROUND);
-    double sum = 0.0;
-    KB_UNROLL for (int i = 0; i < N; ++i) {
-      const double pv = fy[i] * ewtf[i];
-      sum += pv * pv;
-    }
-    const double fnorm = kbw::ssqrt_(sum / N);
-    const double minInc = (fnorm != 0.0)
-        ? (kbw::MIN_INC_MULT * fabs(h) * kbw::UROUND * (double)N * fnorm) : 1.0;
-    const int j = lane < N ? lane : 0;
-    const double yj = kbw::pick<N>(yf, j);
-    const double ewj = kbw::pick<N>(ewtf, j);
-    const double inc = kbw::smax_(srur * fabs(yj), minInc / ewj);
-    KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = (i == lane) ? yf[i] + inc : yf[i];
-    int r = kbw::rhs_check<N, EVT>(yf, f, p, Tfix, k, hit);
-    if (lane >= N) { r = 0; hit = false; }
-    const unsigned bad = __ballot_sync(FULLM, r != 0);
-    const int first_bad = bad ? __ffs(bad) - 1 : N;
-    ndq = bad ? first_bad + 1 : N;
-    ret = bad ? 1 : 0;
-    hit = __any_sync(FULLM, hit && lane <= first_bad);
-    if (lane < N && lane < first_bad) {
-      const double inc_inv = 1.0 / inc;
-      KB_UNROLL for (int i = 0; i < N; ++i) sJ[i + lane * N] = inc_inv * (f[i] - fy[i]);
-    }
-  } else {
-    const double T = EVT ? fmin(fmax(yf[N - 1], p.Tcmb), 1e9)
-                         : fmin(fmax(Tfix, p.Tcmb), 1e9);
-    if (lane == 0) {
-      KB_UNROLL for (int i = 0; i <= NREA; ++i) k[i] = 0.0;
-      rates_fixed(T, yf, p, k);
-      rates_var(T, yf, p, k);
-      jac_stoich(yf, k, sJ, 1, N);  // column-major: (i, j) at i + j N
-    }
-    if (EVT) {
-      constexpr int iT = N - 1;
-      double sumabs = 0.0;
-      KB_UNROLL for (int i = 0; i < NSPEC; ++i) sumabs += fabs(yf[i]);
-      const double hT = fmax(1e-6 * fabs(yf[iT]), 1e-8);
-      const double yjl = kbw::pick<N>(yf, lane < N ? lane : 0);
-      const double hj = lane < NSPEC
-          ? fmax(fmax(1e-7 * fabs(yjl), 1e-9 * sumabs), 1e-30) : 1.0;
-      KB_UNROLL for (int i = 0; i < N; ++i) {
-        double v = yf[i];
-        if (lane < NSPEC && i == lane) v = yf[i] + hj;
-        if (lane == NSPEC + 1 && i == iT) v = yf[iT] + hT;
-        if (lane == NSPEC + 2 && i == iT) v = yf[iT] - hT;
-        yf[i] = v;
-      }
-      const double Tl = (lane == NSPEC + 1 || lane == NSPEC + 2)
-                            ? fmin(fmax(yf[iT], p.Tcmb), 1e9) : T;
-      KB_UNROLL for (int i = 0; i <= NREA; ++i) k[i] = 0.0;
-      rates_fixed(Tl, yf, p, k);
-      rates_var(Tl, yf, p, k);
-      rhs(yf, k, f);
-      const double Tth = fmin(fmax(yf[iT], 2.73), 1e9);
-      f[iT] = thermal_dTdt(Tth, yf, k, p);
-      double* sv = sJ + N * N;
-      __syncwarp();
-      if (lane == NSPEC + 1) { KB_UNROLL for (int i = 0; i < N; ++i) sv[i] = f[i]; }
-      if (lane == NSPEC + 2) { KB_UNROLL for (int i = 0; i < N; ++i) sv[N + i] = f[i]; }
-      __syncwarp();
-      if (lane < N) sJ[lane + iT * N] = (sv[lane] - sv[N + lane]) / (2.0 * hT);
-      const double f0 = __shfl_sync(FULLM, f[iT], NSPEC);
-      if (lane < NSPEC) sJ[iT + lane * N] = (f[iT] - f0) / hj;
-    }
-  }
-  __syncwarp();
-  if (lane == src) {
-    for (int i = 0; i < N * N; ++i) s.savedJ[i] = sJ[i];
-    s.ls_retval = ret;
-    s.st[kbw::ST_NFEDQ] += ndq;
-    s.hitT0 = s.hitT0 || hit;
-  }
-  __syncwarp();
-}
 
 // start cell c on this lane: false when the cell needs no integration
 // (its flag is written here)
@@ -299,16 +198,26 @@ __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
 
 // one warp = 32 cells in flight. persistent == 0: each lane integrates the
 // cell of its global thread index; persistent == 1: lanes pull cells from
-// the device work queue (`cursor`) until it is exhausted
-template <bool EVT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// the device work queue (`cursor`) until it is exhausted.
+//
+// Each round: (1) every lane advances its cell to its next request;
+// (2) the warp evaluates the requests with ONE rhs call site: pass 0 the
+// lanes' own rhs requests, then one pass per group of Jacobian requests,
+// where request r of the pass occupies lanes [r*JL, (r+1)*JL) (JL the lanes
+// one Jacobian needs) and lane r*JL + j evaluates its column / term j; the
+// assembled Jacobians go through shared memory to the requesting lanes.
+template <bool EVT, int MINB>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
 kb_lane_cells(int ncell, double* n, double* T, const double* dt,
               const double* par, int pstride, int* flags, long* stats,
               SolveOpts so, unsigned* cursor, int persistent) {
   constexpr int N = LaneGeo<EVT>::N;
+  using namespace kbnet;
+  constexpr unsigned FULLM = 0xffffffffu;
   extern __shared__ double smem[];
   const int warp = threadIdx.x >> 5;
-  double* sJ = smem + warp * LaneGeo<EVT>::SMEM_DOUBLES;
+  const int lane = threadIdx.x & 31;
+  double* sw = smem + warp * LaneGeo<EVT>::SMEM_DOUBLES;
   kbl::LaneCell<N> s;
   kbl::Machine<N, EVT> m(s, so);
   s.cell = -1;
@@ -316,10 +225,11 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
   bool static_taken = false;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   bool exhausted = false;
+  const bool dq = so.jac == 2;
+  const int JL = dq ? LaneGeo<EVT>::JLANES_DQ : LaneGeo<EVT>::JLANES_AN;
+  const int per_pass = 32 / JL;
   for (;;) {
     int req = kbl::REQ_NONE;
-    // 1. advance this lane to its next request, taking new cells as the
-    //    current one finishes
     while (!exhausted) {
       if (s.cell < 0) {
         int c;
@@ -342,22 +252,164 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
       }
       break;
     }
-    if (__all_sync(0xffffffffu, exhausted)) break;
-    // 2. the warp serves the Jacobian requests, one cell at a time
-    unsigned jm = __ballot_sync(0xffffffffu, req == kbl::REQ_JAC);
-    while (jm) {
-      const int src = __ffs(jm) - 1;
-      jm &= jm - 1;
-      serve_jac<EVT>(s, src, so, sJ);
-    }
-    // 3. the rhs requests, in one SIMT pass
-    if (req == kbl::REQ_RHS) {
-      double yf[N], f[N], k[kbnet::NREA + 1];
-      KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = s.yreq[i];
+    if (__all_sync(FULLM, exhausted)) break;
+    const unsigned jm = __ballot_sync(FULLM, req == kbl::REQ_JAC);
+    const int nj = __popc(jm);
+    const int npass = 1 + (nj + per_pass - 1) / per_pass;
+    unsigned jrest = jm;
+    for (int pass = 0; pass < npass; ++pass) {
+      // ---- this lane's task ----
+      bool active;
+      int src = lane, role = 0;
+      unsigned passm = 0;  // the requesting lanes served in this pass
+      if (pass == 0) {
+        active = req == kbl::REQ_RHS;
+      } else {
+        for (int r = 0; r < per_pass && jrest; ++r) {
+          const unsigned b = jrest & (~jrest + 1u);
+          passm |= b;
+          jrest &= jrest - 1u;
+        }
+        const int grp = lane / JL;
+        role = lane - grp * JL;
+        // the grp-th set bit of passm
+        unsigned t = passm;
+        for (int r = 0; r < grp && t; ++r) t &= t - 1u;
+        active = grp < per_pass && t != 0u;
+        src = active ? __ffs(t) - 1 : lane;
+      }
+      // ---- the state to evaluate ----
+      double yf[N], f[N], k[NREA + 1];
+      Params p;
+      double Tfix, inc = 1.0, hT = 1.0;
+      if (pass == 0) {
+        KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = s.yreq[i];
+        p = s.p;
+        Tfix = s.Tfix;
+      } else {
+        KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = __shfl_sync(FULLM, s.y[i], src);
+        {
+          double row[NPAR];
+          const double* ps = reinterpret_cast<const double*>(&s.p);
+          KB_UNROLL for (int i = 0; i < NPAR; ++i) row[i] = __shfl_sync(FULLM, ps[i], src);
+          params_from_row(row, p);
+        }
+        Tfix = __shfl_sync(FULLM, s.Tfix, src);
+        if (dq) {
+          // CVODE's increment of column `role` (bdf_cell.hpp:1294-1301)
+          double sum = 0.0, yj = 0.0, ewj = 1.0;
+          KB_UNROLL for (int i = 0; i < N; ++i) {
+            const double fyi = __shfl_sync(FULLM, s.ftemp[i], src);
+            const double ewi = __shfl_sync(FULLM, s.ewt[i], src);
+            const double pv = fyi * ewi;
+            sum += pv * pv;
+            if (i == role) { yj = yf[i]; ewj = ewi; }
+          }
+          const double h = __shfl_sync(FULLM, s.h, src);
+          const double fnorm = kbw::ssqrt_(sum / N);
+          const double minInc = (fnorm != 0.0)
+              ? (kbw::MIN_INC_MULT * fabs(h) * kbw::UROUND * (double)N * fnorm) : 1.0;
+          inc = kbw::smax_(kbw::ssqrt_(kbw::UROUND) * fabs(yj), minInc / ewj);
+          KB_UNROLL for (int i = 0; i < N; ++i) if (i == role) yf[i] += inc;
+        } else if (EVT) {
+          // hybrid analytic Jacobian terms (solve_cell.hpp:1053-1099)
+          constexpr int iT = N - 1;
+          double sumabs = 0.0, yj = 0.0;
+          KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
+            sumabs += fabs(yf[i]);
+            if (i == role) yj = yf[i];
+          }
+          hT = fmax(1e-6 * fabs(yf[iT]), 1e-8);
+          inc = role < NSPEC ? fmax(fmax(1e-7 * fabs(yj), 1e-9 * sumabs), 1e-30) : 1.0;
+          KB_UNROLL for (int i = 0; i < NSPEC; ++i) if (i == role) yf[i] += inc;
+          if (role == NSPEC + 1) yf[iT] += hT;
+          if (role == NSPEC + 2) yf[iT] -= hT;
+        }
+      }
+      // ---- the one rhs evaluation of this round and pass ----
+      // (the hybrid Jacobian's species terms keep the base rate
+      // temperature: their perturbation leaves Tgas alone)
       bool hit = false;
-      s.rhs_ret = kbw::rhs_check<N, EVT>(yf, f, s.p, s.Tfix, k, hit);
-      if (hit) s.hitT0 = true;
-      KB_UNROLL for (int i = 0; i < N; ++i) s.freq[i] = f[i];
+      int r = 0;
+      if (active) {
+        kbw::full_rhs<N, EVT>(yf, f, p, Tfix, k);
+        // the integrator's checks (rhs_host_, solve_cell.hpp:794-813): a
+        // trial Tgas <= 0 or a non-finite f is a recoverable failure; the
+        // hybrid Jacobian's terms are plain full_rhs_ evaluations
+        if (pass == 0 || dq) {
+          if (EVT && !(yf[N - 1] > 0.0)) {
+            hit = true;
+            r = 1;
+          } else {
+            bool ok = true;
+            KB_UNROLL for (int i = 0; i < N; ++i) ok = ok && isfinite(f[i]);
+            r = ok ? 0 : 1;
+          }
+        }
+        // the hybrid Jacobian's base-state lane: the stoichiometric block
+        // with the rates of the base state (jacobian_split)
+        if (pass > 0 && !dq && role == LaneGeo<EVT>::ROLE_BASE)
+          jac_stoich(yf, k, sw + (lane / JL) * (N * N + 2 * N), 1, N);
+      }
+      // ---- results ----
+      if (pass == 0) {
+        if (active) {
+          KB_UNROLL for (int i = 0; i < N; ++i) s.freq[i] = f[i];
+          s.rhs_ret = r;
+          if (hit) s.hitT0 = true;
+        }
+        continue;
+      }
+      const int grp = lane / JL;
+      double* blk = sw + (active ? grp : 0) * (N * N + 2 * N);
+      const unsigned bad = __ballot_sync(FULLM, active && r != 0);
+      const unsigned gmask = (JL >= 32) ? FULLM
+          : (((1u << JL) - 1u) << (active ? grp * JL : 0));
+      const unsigned gbad = active ? (bad & gmask) : 0u;
+      const int first_bad = gbad ? (__ffs(gbad) - 1 - grp * JL) : N;
+      (void)gmask;
+      const unsigned hitm = __ballot_sync(FULLM, active && hit && role <= first_bad);
+      if (dq) {
+        const bool store = active && role < N && role < first_bad;
+        const double inc_inv = 1.0 / inc;
+        KB_UNROLL for (int i = 0; i < N; ++i) {
+          const double fyi = __shfl_sync(FULLM, s.ftemp[i], src);
+          if (store) blk[i + role * N] = inc_inv * (f[i] - fyi);
+        }
+      } else if (EVT) {
+        constexpr int iT = N - 1;
+        double* sv = blk + N * N;
+        if (active && role == NSPEC + 1) { KB_UNROLL for (int i = 0; i < N; ++i) sv[i] = f[i]; }
+        if (active && role == NSPEC + 2) { KB_UNROLL for (int i = 0; i < N; ++i) sv[N + i] = f[i]; }
+        // the base state's thermal row value (role NSPEC of the group)
+        const double f0 = __shfl_sync(FULLM, f[iT], (active ? grp * JL : 0)
+                                                     + LaneGeo<EVT>::ROLE_BASE);
+        if (active && role < NSPEC) blk[iT + role * N] = (f[iT] - f0) / inc;
+        __syncwarp();
+        if (active && role < N) blk[role + iT * N] = (sv[role] - sv[N + role]) / (2.0 * hT);
+      }
+      __syncwarp();
+      // the requesting lane: its stoichiometric block (analytic), then the
+      // assembled Jacobian into its savedJ
+      if ((passm >> lane) & 1u) {
+        int g = 0;
+        for (unsigned t = passm & ((1u << lane) - 1u); t; t &= t - 1u) ++g;
+        double* myblk = sw + g * (N * N + 2 * N);
+        const int base = g * JL;
+        const unsigned mbad = bad & (((JL >= 32) ? FULLM : ((1u << JL) - 1u)) << base);
+        const int fb = mbad ? (__ffs(mbad) - 1 - base) : N;
+        if (!dq) {
+          for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
+          s.ls_retval = 0;
+        } else {
+          for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
+          s.ls_retval = mbad ? 1 : 0;
+          s.st[kbw::ST_NFEDQ] += mbad ? fb + 1 : N;
+        }
+        if (hitm & (((JL >= 32) ? FULLM : ((1u << JL) - 1u)) << base))
+          s.hitT0 = true;
+      }
+      __syncwarp();
     }
   }
 }
@@ -378,6 +430,8 @@ struct krome_opts {
   // this library's keys
   int kernel = 1;          // 0 plain, 1 persistent work queue
   int layout = 1;          // 0 one warp per cell, 1 one lane per cell
+  int lane_minb = 3;       // lane kernel: resident blocks per SM it is
+                           // compiled for (2, 3, 4: the register budget)
   int queue_chunk = 1;     // cells per queue pop
   int blocks_per_sm = 0;   // persistent grid: 0 = occupancy limit
   int fail_every = 0;      // fault injection (tests)
@@ -451,14 +505,18 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
     const size_t lsmem =
         sizeof(double) * kWarpsPerBlock * LaneGeo<EVT>::SMEM_DOUBLES;
     const int threads = kWarpsPerBlock * 32;
+    // register budget of the kernel: 2, 3 or 4 resident blocks per SM
+    auto kern = h.lane_minb == 2 ? kb_lane_cells<EVT, 2>
+              : h.lane_minb == 4 ? kb_lane_cells<EVT, 4>
+                                 : kb_lane_cells<EVT, 3>;
     long blocks;
     if (h.kernel == 0) {
       blocks = ((long)ncell + threads - 1) / threads;
     } else {
       int per_sm = h.blocks_per_sm;
       if (per_sm <= 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, kb_lane_cells<EVT>, threads, lsmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads,
+                                                      lsmem);
         if (per_sm <= 0) per_sm = 1;
       }
       blocks = (long)num_sms() * per_sm;
@@ -467,7 +525,7 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
       cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(unsigned), stream);
       if (e != cudaSuccess) return e;
     }
-    kb_lane_cells<EVT><<<(int)blocks, threads, lsmem, stream>>>(
+    kern<<<(int)blocks, threads, lsmem, stream>>>(
         ncell, n, T, dt, par, pstride, flags, stats, so, cursor, h.kernel);
     return cudaGetLastError();
   }
@@ -610,6 +668,7 @@ int* int_key(krome_opts* h, const char* k) {
       {"linsol", offsetof(krome_opts, linsol)},
       {"kernel", offsetof(krome_opts, kernel)},
       {"layout", offsetof(krome_opts, layout)},
+      {"lane_minb", offsetof(krome_opts, lane_minb)},
       {"queue_chunk", offsetof(krome_opts, queue_chunk)},
       {"blocks_per_sm", offsetof(krome_opts, blocks_per_sm)},
       {"fail_every", offsetof(krome_opts, fail_every)},
@@ -660,6 +719,7 @@ KB_API int krome_opts_set(krome_opts* h, const char* key, double v) {
   if (!std::strcmp(key, "conserve") && (x < 0 || x > 3)) return -1;
   if (!std::strcmp(key, "kernel") && (x < 0 || x > 1)) return -1;
   if (!std::strcmp(key, "layout") && (x < 0 || x > 1)) return -1;
+  if (!std::strcmp(key, "lane_minb") && (x < 2 || x > 4)) return -1;
   if ((!std::strcmp(key, "max_err_fails") || !std::strcmp(key, "max_conv_fails")
        || !std::strcmp(key, "max_restarts") || !std::strcmp(key, "queue_chunk")
        || !std::strcmp(key, "fail_every") || !std::strcmp(key, "blocks_per_sm"))
@@ -798,6 +858,197 @@ KB_API int krome_solve_cells(int ncell, double* n, double* Tgas,
   (void)extra;  // no photon bins or dust bins in these networks
   return krome_b200_solve_batch(ncell, n, Tgas, dt, par, par_stride, flags,
                                 nullptr, h);
+}
+
+namespace {
+// the rate coefficients of each cell at its rate temperature clamp(Tgas,
+// Tcmb, 1e9) (the reference's krome_get_rates query, krome.h:387-389)
+__global__ void kb_rates(int ncell, const double* n, const double* T,
+                         const double* par, int pstride, double* k) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  using namespace kbnet;
+  double nv[NSPEC], kk[NREA + 1];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) nv[i] = n[(long)c * NSPEC + i];
+  Params p;
+  params_from_row(par + (long)c * pstride, p);
+  const double Tr = fmin(fmax(T[c], p.Tcmb), 1e9);
+  KB_UNROLL for (int i = 0; i <= NREA; ++i) kk[i] = 0.0;
+  rates_fixed(Tr, nv, p, kk);
+  rates_var(Tr, nv, p, kk);
+  KB_UNROLL for (int i = 0; i < NREA; ++i) k[(long)c * NREA + i] = kk[i];
+}
+}  // namespace
+
+// krome_get_rates (reference krome.h:387-389): k[ncell][nrea], host arrays;
+// the photo rates (no photon bins here) are 0. Phi and h are unused.
+KB_API int krome_get_rates(int ncell, const double* n, const double* Tgas,
+                           const double* par, int par_stride,
+                           const double* Phi, const void* h, double* k) {
+  (void)Phi; (void)h;
+  if (ncell < 0 || n == nullptr || Tgas == nullptr || k == nullptr) return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+  if (ncell == 0) return 0;
+  std::vector<double> dflt(kbnet::NPAR);
+  krome_params_default(dflt.data());
+  const double* P = par != nullptr ? par : dflt.data();
+  const int ps = par != nullptr ? par_stride : 0;
+  for (int c = 0; c < ncell; ++c)
+    if (row_missing(P + (long)c * ps)) return -105;
+  const size_t nb = sizeof(double) * (size_t)ncell * kbnet::NSPEC;
+  const size_t tb = sizeof(double) * (size_t)ncell;
+  const size_t pb = sizeof(double) * (ps ? (size_t)ncell * ps : (size_t)kbnet::NPAR);
+  const size_t kb = sizeof(double) * (size_t)ncell * kbnet::NREA;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (g_buf.ensure(al(nb) + al(tb) + al(pb) + al(kb)) != cudaSuccess) return -111;
+  char* b = static_cast<char*>(g_buf.p);
+  double* dn = reinterpret_cast<double*>(b); b += al(nb);
+  double* dT = reinterpret_cast<double*>(b); b += al(tb);
+  double* dp = reinterpret_cast<double*>(b); b += al(pb);
+  double* dk = reinterpret_cast<double*>(b);
+  cudaError_t e = cudaMemcpy(dn, n, nb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dT, Tgas, tb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dp, P, pb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    kb_rates<<<(ncell + 127) / 128, 128>>>(ncell, dn, dT, dp, ps, dk);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(k, dk, kb, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? 0 : -104;
+}
+
+// ---------------------------------------------------------------------------
+// the hydro loop of the collapse driver, on the device
+
+namespace {
+// one compression step of the reference's collapse driver
+// (examples/tests/collapse/test.cpp:47-63): tff = sqrt(3 pi / (32 G rho))
+// of the current state (rho = sum n_i m_i in species order, the reference's
+// rho_), the parameter tff of the cell set to it, every density x factor,
+// dt = dtfrac tff
+__global__ void kb_compress(int ncell, double* n, double* par, int pstride,
+                            int tff_index, double* dt, double factor,
+                            double dtfrac) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  using namespace kbnet;
+  double* nc = n + (long)c * NSPEC;
+  double v[NSPEC];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) v[i] = nc[i];
+  const double rho = rho_(v);
+  const double tff = sqrt(3.0 * kbc::pi / (32.0 * kbc::gravity * fmax(rho, 1e-40)));
+  if (pstride > 0) par[(long)c * pstride + tff_index] = tff;
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) nc[i] = v[i] * factor;
+  dt[c] = dtfrac * tff;
+}
+
+struct HydroGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+}  // namespace
+
+// one device-resident hydro step: compression (kb_compress) then the solve,
+// on `stream`, asynchronously (nothing allocated, no host synchronization)
+KB_API int krome_b200_hydro_step(int ncell, double* n, double* Tgas,
+                                 double* dt, double* par, int par_stride,
+                                 int tff_index, double factor, double dtfrac,
+                                 int* flags, long* stats, unsigned* cursor,
+                                 const krome_opts* h, void* stream) {
+  if (h == nullptr || ncell < 0 || par_stride != kbnet::NPAR
+      || tff_index < 0 || tff_index >= kbnet::NPAR)
+    return -1;
+  if (ncell == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  kb_compress<<<(ncell + 127) / 128, 128, 0, s>>>(
+      ncell, n, par, par_stride, tff_index, dt, factor, dtfrac);
+  if (cudaGetLastError() != cudaSuccess) return -104;
+  return krome_b200_solve_device(ncell, n, Tgas, dt, par, par_stride, flags,
+                                 stats, cursor, h, stream);
+}
+
+// the hydro step captured once as a CUDA graph (compression, work-queue
+// reset, solve) and replayed by krome_b200_graph_launch; the arrays stay
+// bound to the graph. Returns a handle or NULL.
+KB_API void* krome_b200_graph_new(int ncell, double* n, double* Tgas,
+                                  double* dt, double* par, int par_stride,
+                                  int tff_index, double factor, double dtfrac,
+                                  int* flags, long* stats, unsigned* cursor,
+                                  const krome_opts* h, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto* g = new HydroGraph();
+  // occupancy queries are made before the capture
+  (void)num_sms();
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    delete g;
+    return nullptr;
+  }
+  const int r = krome_b200_hydro_step(ncell, n, Tgas, dt, par, par_stride,
+                                      tff_index, factor, dtfrac, flags, stats,
+                                      cursor, h, stream);
+  const cudaError_t e = cudaStreamEndCapture(s, &g->graph);
+  if (r != 0 || e != cudaSuccess
+      || cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) {
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return nullptr;
+  }
+  return g;
+}
+
+KB_API int krome_b200_graph_launch(void* handle, void* stream) {
+  auto* g = static_cast<HydroGraph*>(handle);
+  if (g == nullptr) return -1;
+  return cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream))
+             == cudaSuccess ? 0 : -104;
+}
+
+KB_API void krome_b200_graph_free(void* handle) {
+  auto* g = static_cast<HydroGraph*>(handle);
+  if (g == nullptr) return;
+  cudaGraphExecDestroy(g->exec);
+  cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+// the FP64 pipe's peak, measured: independent DFMA chains in registers,
+// the whole GPU, timed with events. Writes TFLOP/s (2 flops per DFMA).
+namespace {
+__global__ void kb_dfma_chains(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
+  double x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b);
+    x3 = fma(x3, a, b); x4 = fma(x4, a, b); x5 = fma(x5, a, b);
+    x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  const double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+}  // namespace
+
+KB_API int krome_b200_fp64_peak(double* tflops) {
+  if (tflops == nullptr) return -1;
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return -104;
+  const int blocks = num_sms() * 8, threads = 256, iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  kb_dfma_chains<<<blocks, threads>>>(out, 256, 0.999999, 1e-7);
+  cudaEventRecord(e0);
+  kb_dfma_chains<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(e1);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess || ms <= 0.0f) return -104;
+  *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
+  return 0;
 }
 
 KB_API int krome_has_device(void) {

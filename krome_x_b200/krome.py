@@ -148,6 +148,25 @@ class Network:
                 ctypes.c_void_p, ctypes.c_void_p]),
             "krome_has_device": (ctypes.c_int, []),
             "krome_b200_nstat": (ctypes.c_int, []),
+            "krome_get_rates": (ctypes.c_int, [
+                ctypes.c_int, _D, _D, _D, ctypes.c_int, _D, ctypes.c_void_p,
+                _D]),
+            "krome_b200_hydro_step": (ctypes.c_int, [
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p]),
+            "krome_b200_graph_new": (ctypes.c_void_p, [
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p]),
+            "krome_b200_graph_launch": (ctypes.c_int, [ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
+            "krome_b200_graph_free": (None, [ctypes.c_void_p]),
+            "krome_b200_fp64_peak": (ctypes.c_int, [_D]),
         }
         for name, (res, args) in proto.items():
             fn = getattr(lib, name)
@@ -315,3 +334,71 @@ class Network:
             raise KromeError("krome_b200_solve_device returned %d: %s"
                              % (r, self.flag_message(r)))
         return r
+
+    def rates(self, n, Tgas, par=None):
+        """the rate coefficients k[ncell, nrea] at each cell's rate
+        temperature (krome_get_rates, computed on the GPU)"""
+        n = np.ascontiguousarray(np.atleast_2d(n), dtype=float)
+        ncell = n.shape[0]
+        T = np.ascontiguousarray(np.broadcast_to(np.asarray(Tgas, float),
+                                                 (ncell,)))
+        P, stride = self._params(par, ncell)
+        k = np.zeros((ncell, self.nrea))
+        r = self._lib.krome_get_rates(ncell, _dptr(n), _dptr(T), _dptr(P),
+                                      stride, None, None, _dptr(k))
+        if r != 0:
+            raise KromeError("krome_get_rates returned %d" % r)
+        return k
+
+    def fp64_peak(self):
+        """the measured FP64 peak of the GPU [TFLOP/s]"""
+        v = ctypes.c_double()
+        if self._lib.krome_b200_fp64_peak(ctypes.byref(v)) != 0:
+            raise KromeError("no GPU for the FP64 peak measurement")
+        return v.value
+
+    def hydro_graph(self, n, Tgas, dt, par, flags, opts, stats=None,
+                    cursor=None, factor=1.01, dtfrac=0.01, stream=None):
+        """a HydroGraph: one collapse-driver step (tff, densities x factor,
+        dt = dtfrac tff, then the solve) captured as a CUDA graph on the
+        device arrays (torch CUDA tensors), replayed by .launch()"""
+        return HydroGraph(self, n, Tgas, dt, par, flags, opts, stats, cursor,
+                          factor, dtfrac, stream)
+
+
+class HydroGraph:
+    """the captured hydro step (krome_b200_graph_new / _launch / _free)"""
+
+    def __init__(self, net, n, Tgas, dt, par, flags, opts, stats, cursor,
+                 factor, dtfrac, stream):
+        import torch
+        self.net = net
+        self.stream = stream or torch.cuda.Stream()
+        self.cursor = cursor if cursor is not None else torch.zeros(
+            1, dtype=torch.int32, device=n.device)
+        self._keep = (n, Tgas, dt, par, flags, stats, opts)
+        ptr = lambda x: None if x is None else x.data_ptr()
+        self._h = net._lib.krome_b200_graph_new(
+            int(n.shape[0]), ptr(n), ptr(Tgas), ptr(dt), ptr(par),
+            net.npar, net.params.index("tff"), factor, dtfrac, ptr(flags),
+            ptr(stats), ptr(self.cursor), opts._h,
+            ctypes.c_void_p(self.stream.cuda_stream))
+        if not self._h:
+            raise KromeError("CUDA graph capture of the hydro step failed")
+
+    def launch(self):
+        r = self.net._lib.krome_b200_graph_launch(
+            ctypes.c_void_p(self._h), ctypes.c_void_p(self.stream.cuda_stream))
+        if r != 0:
+            raise KromeError("graph launch failed (%d)" % r)
+
+    def free(self):
+        if self._h:
+            self.net._lib.krome_b200_graph_free(ctypes.c_void_p(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -1007,6 +1007,17 @@ constexpr int ORACLE_NSTAT = 9;
 
 extern "C" {
 
+// the rate coefficients at (T, n) with the parameter row par: the
+// reference's rates() (zero, rates_fixed, rates_var)
+ORACLE_API void oracle_rates(double T, const double* n, const double* par,
+                             double* k) {
+  Params p;
+  params_from_row(par, p);
+  for (int i = 0; i < NREA; ++i) k[i] = 0.0;
+  rates_fixed(T, n, p, k);
+  rates_var(T, n, p, k);
+}
+ORACLE_API int oracle_nrea(void) { return NREA; }
 ORACLE_API int oracle_nspec(void) { return NSPEC; }
 ORACLE_API int oracle_npar(void) { return NPAR; }
 ORACLE_API const char* oracle_network(void) { return NETWORK_KEY; }

@@ -124,3 +124,19 @@ class Reference:
         self.seconds = time.perf_counter() - t0
         self.lib.krome_opts_free(h)
         return dict(n=n, T=T, flags=flags, ret=ret)
+
+
+def _ref_worker(args):
+    net, strict, n, T, dt, par, opts = args
+    out = Reference(net, strict=strict).solve(n, T, dt, par, **opts)
+    return out
+
+
+def reference_solve(net, n, T, dt, par, strict=False, **opts):
+    """Reference(net).solve in a spawned child process: the reference's
+    generated tables are function-local statics, which GCC emits as
+    process-wide unique symbols, so two networks' libraries must never share
+    a process"""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1) as pool:
+        return pool.map(_ref_worker, [(net, strict, n, T, dt, par, opts)])[0]

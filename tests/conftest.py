@@ -1,0 +1,56 @@
+"""Shared fixtures of the test suite.
+
+Markers: ``gpu`` for tests that need a CUDA device (run on the B200 host with
+``pytest -m gpu``); everything else runs on the CPU (``-m "not gpu"``).
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+NETWORKS = ("primordial", "primordial3", "galaxy_ism")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def golden(key):
+    return np.load(ROOT / "tests" / "golden" / ("%s.npz" % key))
+
+
+def parity(a_n, a_T, a_flags, b_n, b_T, b_flags, rtol, atol=1e-20):
+    """the parity metric of the benchmark: over the cells where both
+    solves succeed, the relative error of every abundance above atol/rtol
+    (the rtol-dominated ones) and of Tgas must be <= 10 rtol; returns the
+    fraction of such cells that pass, the CVODE-weighted error
+    |a - b| / (rtol |b| + atol) of the others (max), and the flag
+    agreement"""
+    ok = (a_flags == 0) & (b_flags == 0)
+    na, nb = a_n[ok], b_n[ok]
+    big = np.abs(nb) > atol / rtol
+    with np.errstate(all="ignore"):
+        rel = np.where(big, np.abs(na - nb) / np.abs(nb), 0.0)
+        wgt = np.where(big, 0.0, np.abs(na - nb) / (rtol * np.abs(nb) + atol))
+    relT = np.abs(a_T[ok] - b_T[ok]) / np.abs(b_T[ok])
+    cell_ok = (rel.max(axis=1) <= 10 * rtol) & (relT <= 10 * rtol)
+    return dict(cells=int(ok.sum()),
+                frac=float(cell_ok.mean()) if ok.any() else 1.0,
+                max_rel=float(rel.max()) if ok.any() else 0.0,
+                max_relT=float(relT.max()) if ok.any() else 0.0,
+                max_weighted_trace=float(wgt.max()) if ok.any() else 0.0,
+                flags_equal=float(np.mean(a_flags == b_flags)))
+
+
+@pytest.fixture(scope="session")
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,61 @@
+"""Generate the golden fixtures of the parity tests from the reference.
+
+Run where the reference tree and oracle/_ref (oracle/build_ref.py) exist:
+``python tests/golden/make_golden.py``. For each benchmark network it writes
+``tests/golden/<net>.npz`` with
+
+* ``k_T, k_n, k_idx, k_ref``: the reference's own golden rate vectors -- the
+  K_REF table the reference generator writes into each project's
+  krome_check.cpp (rate coefficients at three temperatures, computed by its
+  independent network interpreter, kromex/netcheck.py), with the probe
+  parameters of that check (every parameter 1.3e-17, Tdust 10 K);
+* ``n, T, dt, par`` / ``n_out, T_out, flags``: 64 seeded cells of the
+  benchmark workload solved by the reference's strict build
+  (oracle/_ref/libkrome_<net>_strict.so, krome_solve_cells) with the
+  workload's options, each network in its own process (the generated
+  libraries must not share one).
+"""
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+from krome_x_b200 import netinfo, workloads  # noqa: E402
+from oracle import reference_solve  # noqa: E402
+
+NCELL = 64
+
+
+def _array(text, name):
+    m = re.search(r"%s\[[^\]]*\](?:\[[^\]]*\])?\s*=\s*(\{.*?\});" % name, text,
+                  re.S)
+    body = m.group(1).replace("{", "[").replace("}", "]")
+    return np.array(eval(body), dtype=float)
+
+
+def main():
+    for key in ("primordial", "primordial3", "galaxy_ism"):
+        info = netinfo.load(key)
+        chk = (ROOT / "oracle" / "_ref" / "gen" / key / "krome_check.cpp").read_text()
+        k_T = _array(chk, "T_REF")
+        k_n = _array(chk, "N_REF")
+        k_idx = _array(chk, "I_REF").astype(np.int32)
+        k_ref = _array(chk, "K_REF")
+        n, T, dt, par = workloads.GENERATORS[key](NCELL, info, seed=11)
+        opts = dict(workloads.OPTIONS[key])
+        out = reference_solve(key, n, T, dt, par, strict=True, **opts)
+        np.savez_compressed(HERE / ("%s.npz" % key), k_T=k_T, k_n=k_n,
+                            k_idx=k_idx, k_ref=k_ref, n=n, T=T, dt=dt, par=par,
+                            n_out=out["n"], T_out=out["T"], flags=out["flags"],
+                            ret=out["ret"])
+        print(key, "flags", np.unique(out["flags"]), "->", HERE / ("%s.npz" % key))
+
+
+if __name__ == "__main__":
+    main()
