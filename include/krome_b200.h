@@ -133,6 +133,25 @@ void* krome_b200_graph_new(int ncell, double* n, double* Tgas, double* dt,
 int krome_b200_graph_launch(void* graph, void* stream);
 void krome_b200_graph_free(void* graph);
 
+/* krome_solve_cells for callers that cannot let the library allocate device
+ * memory -- a code that gives the whole GPU to its own memory pool, or a
+ * time step that must not pay cudaMalloc's device-wide synchronization.
+ * No counterpart in the reference (its device path allocates per call).
+ * Same arguments, layouts, flags and failed-cell rule as krome_solve_cells
+ * (flags may be NULL); the call's device copies go through one array
+ * compiled into the library, 16 MiB of device memory per GPU held until
+ * the process exits, instead of an allocation: it fits about
+ * 16 MiB / (8 (nspec + 2 + npar) + 4) bytes-per-cell cells (per-cell
+ * parameter rows), and a larger call returns -111 (FLAG_DEVICE_MEMORY)
+ * with nothing touched. The first call on a device looks up the array's
+ * device address (once per device); make it before any stream capture.
+ * All calls share the array: the entry point serialises its own calls,
+ * and calls that overlapped on the GPU would race. */
+int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
+                                   const double* dt, const double* par,
+                                   int par_stride, int* flags,
+                                   const krome_opts* h);
+
 /* the FP64 pipe's peak of this GPU, measured with register-resident DFMA
  * chains over the whole device [TFLOP/s] (the roofline's denominator) */
 int krome_b200_fp64_peak(double* tflops);

@@ -1051,6 +1051,134 @@ KB_API int krome_b200_fp64_peak(double* tflops) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// krome_solve_cells without device allocation
+//
+// Some callers cannot let a library call cudaMalloc: a hydro code that hands
+// the whole GPU to its own memory pool at start-up (so a foreign allocation
+// fails or fragments its pool), or a time step that must not pay
+// cudaMalloc's implicit device-wide synchronization. For them this entry
+// point stages the call's device copies in one fixed array compiled into
+// the library instead of allocating: KB_NOALLOC_BYTES (16 MiB) of device
+// memory that every GPU loading the library holds until the process exits.
+// It holds, 256-byte aligned, the persistent kernel's work-queue cursor and
+// the cells' n, Tgas, dt, parameter rows and flags; a call whose cells do not
+// fit returns FLAG_DEVICE_MEMORY (-111) before touching anything.
+//
+// Host code never uses the array's name as an address (on the host it names
+// a stand-in, not device memory): the first call on each device, with that
+// device current, asks cudaGetSymbolAddress for the device address and
+// keeps it. Make that first call before any stream capture. All calls share
+// the one array and it keeps the previous call's contents; the cursor is
+// zeroed by every launch and every cell's flag is written by the kernel.
+// Calls that overlapped on the GPU would race on the array: the entry point
+// serialises its own calls (a mutex held until the results are back on the
+// host).
+
+#define KB_NOALLOC_BYTES (16u << 20)
+static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// the device address of the scratch array on the current device
+// (once per device), or nullptr
+void* noalloc_scratch() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices)
+    return nullptr;
+  if (g_noalloc_ptr[d] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, kb_noalloc_scratch) != cudaSuccess)
+      return nullptr;
+    g_noalloc_ptr[d] = p;
+  }
+  return g_noalloc_ptr[d];
+}
+}  // namespace
+
+KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
+                                          const double* dt, const double* par,
+                                          int par_stride, int* flags,
+                                          const krome_opts* h) {
+  if (h == nullptr || ncell < 0 || n == nullptr || Tgas == nullptr
+      || dt == nullptr)
+    return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR)
+    return -1;
+  if (ncell == 0) return 0;
+  double dflt[kbnet::NPAR];
+  for (int i = 0; i < kbnet::NPAR; ++i) dflt[i] = kbnet::param_default(i);
+  const double* P = par != nullptr ? par : dflt;
+  const int ps = par != nullptr ? par_stride : 0;
+  bool missing = false;
+  for (int c = 0; c < ncell; ++c) {
+    const bool m = row_missing(P + (long)c * ps);
+    if (flags != nullptr) flags[c] = m ? -105 : 0;
+    missing |= m;
+  }
+  if (missing) return -105;
+  if (const int u = unsupported(*h)) {
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = u;
+    return u;
+  }
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t nb = sizeof(double) * (size_t)ncell * kbnet::NSPEC;
+  const size_t tb = sizeof(double) * (size_t)ncell;
+  const size_t pb = sizeof(double) * (ps ? (size_t)ncell * ps : (size_t)kbnet::NPAR);
+  const size_t fb = sizeof(int) * (size_t)ncell;
+  const size_t need = 256 + al(nb) + 2 * al(tb) + al(pb) + al(fb);
+  if (need > KB_NOALLOC_BYTES) {
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = -111;
+    return -111;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  char* b = static_cast<char*>(noalloc_scratch());
+  if (b == nullptr) return -104;
+  unsigned* dcur = reinterpret_cast<unsigned*>(b); b += 256;
+  double* dn = reinterpret_cast<double*>(b); b += al(nb);
+  double* dT = reinterpret_cast<double*>(b); b += al(tb);
+  double* ddt = reinterpret_cast<double*>(b); b += al(tb);
+  double* dp = reinterpret_cast<double*>(b); b += al(pb);
+  int* dfl = reinterpret_cast<int*>(b);
+  cudaStream_t s = 0;
+  cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, Tgas, tb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ddt, dt, tb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, P, pb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = launch_any(*h, ncell, dn, dT, ddt, dp, ps, dfl, nullptr, dcur, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(n, dn, nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Tgas, dT, tb, cudaMemcpyDeviceToHost, s);
+  if (flags != nullptr && e == cudaSuccess)
+    e = cudaMemcpyAsync(flags, dfl, fb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return -104;
+  }
+  if (flags != nullptr) {
+    for (int c = 0; c < ncell; ++c)
+      if (flags[c] != 0) return flags[c];
+    return 0;
+  }
+  // no flags array: the lowest failing cell's flag, read in fixed chunks
+  int chunk[1024];
+  for (int c0 = 0; c0 < ncell; c0 += 1024) {
+    const int m = ncell - c0 < 1024 ? ncell - c0 : 1024;
+    if (cudaMemcpy(chunk, dfl + c0, sizeof(int) * m, cudaMemcpyDeviceToHost)
+        != cudaSuccess)
+      return -104;
+    for (int i = 0; i < m; ++i)
+      if (chunk[i] != 0) return chunk[i];
+  }
+  return 0;
+}
+
 KB_API int krome_has_device(void) {
   int count = 0;
   return cudaGetDeviceCount(&count) == cudaSuccess && count > 0 ? 1 : 0;
