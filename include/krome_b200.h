@@ -57,8 +57,11 @@ const char* krome_param_required_by(int i);
  * library's keys: layout (0 one warp per cell, 1 one lane per cell),
  * kernel (0 plain, 1 persistent work queue), lane_minb (2, 3, 4: the
  * lane kernel's register budget), queue_chunk, blocks_per_sm, fail_every
- * (fault injection: every k-th cell reports -1 untouched). Unknown key or
- * bad value: -1. */
+ * (fault injection: every k-th cell reports -1 untouched), lu32 (the Newton
+ * matrix factored in FP32 with residuals, rhs, history and error test in
+ * FP64; after a Newton failure the matrix is refactored in FP64 until the
+ * next accepted step; lane layout only, else -104). Unknown key or bad
+ * value: -1. */
 krome_opts* krome_opts_new(void);
 void krome_opts_free(krome_opts* h);
 int krome_opts_set(krome_opts* h, const char* key, double value);
@@ -89,7 +92,8 @@ int krome_b200_nstat(void);
 int krome_b200_neq(int evolve_T);
 
 /* krome_solve_cells with per-cell counters: stats[ncell][nstat] (nst, nfe,
- * nfeDQ, nje, nsetups, nni, nnf, netf, restarts; may be NULL). The
+ * nfeDQ, nje, nsetups, nni, nnf, netf, restarts, nlu64 = the FP64 refactors
+ * of the lu32 form; may be NULL). The
  * batched entry point the Python binding's solve / solve_batch use. */
 int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
                            const double* dt, const double* par,
@@ -151,6 +155,13 @@ int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
                                    const double* dt, const double* par,
                                    int par_stride, int* flags,
                                    const krome_opts* h);
+
+/* the network rhs evaluated alone, one thread per cell, reps times per
+ * cell, at full SIMT width (host arrays of the evolve_T state): rhs
+ * evaluations per second -- the rhs-throughput bound of the solve */
+int krome_b200_rhs_throughput(int ncell, const double* n, const double* Tgas,
+                              const double* par, int par_stride, int reps,
+                              double* rhs_per_s);
 
 /* the FP64 pipe's peak of this GPU, measured with register-resident DFMA
  * chains over the whole device [TFLOP/s] (the roofline's denominator) */

@@ -8,20 +8,25 @@
 // same state, so a warp instruction does one cell's work; here a warp
 // instruction evaluates 32 cells. The integrator's control flow differs
 // between cells (Newton iteration counts, Jacobian refreshes, failed
-// attempts, cells that finish early), so it is written as a per-lane
-// resumable state machine that stops at every rhs or Jacobian request:
+// attempts, cells that finish early), so each lane keeps its place in
+// CVODE as a phase and stops at every rhs or Jacobian request:
 //
-//   loop:  1. every lane advances its own CVODE logic (cheap, O(N) and
-//             O(N^2) vector work in its private memory) to its next
-//             request; a lane whose cell is done writes it back and takes
-//             the next cell (a fixed one, or the next one of the device
-//             work queue in the persistent kernel), so lanes never wait
-//             for the slowest cell of their warp;
-//          2. Jacobian requests are served one requesting cell at a time
-//             by the whole warp: lane j evaluates the rhs perturbed in
-//             component j (the difference-quotient columns, or the hybrid
-//             analytic Jacobian's thermal-row and Tgas-column terms), the
-//             columns meet in shared memory;
+//   loop:  1. one sweep runs the phase handlers in a fixed order, each a
+//             structured block over the lanes in that phase (cheap O(N) and
+//             O(N^2) vector work in the lane's private memory); a lane
+//             passes through as many handlers as its cell needs, and the
+//             order follows CVODE's flow, so every lane reaches its next
+//             request within the sweep. Lanes in the same phase execute a
+//             handler together and reconverge after it. A lane whose cell
+//             is done writes it back and takes the next cell (a fixed one,
+//             or the next one of the device work queue in the persistent
+//             kernel), so lanes never wait for the slowest cell of their
+//             warp;
+//          2. Jacobian requests are served by the whole warp: lane j of a
+//             request's group evaluates the rhs perturbed in component j
+//             (the difference-quotient columns, or the hybrid analytic
+//             Jacobian's thermal-row and Tgas-column terms), the columns
+//             meet in shared memory;
 //          3. all lanes with an rhs request evaluate it in one SIMT pass.
 //
 // The algorithm and every decision are CVODE's as the reference ports it
@@ -41,19 +46,41 @@ using kbw::SolveOpts;
 using kbw::NSTAT;
 using namespace kbw;  // flags and CVODE constants
 
-enum : int { REQ_NONE = 0, REQ_RHS = 1, REQ_JAC = 2, REQ_DONE = 3 };
+// what a lane waits for at the end of a sweep
+enum : int { WAIT_NONE = 0, WAIT_RHS = 1, WAIT_JAC = 2 };
 
-// resume points of the state machine
+// the phases, in the order one sweep runs their handlers
 enum : int {
-  PC_NEW = 0, PC_FIRST_RHS, PC_HIN_RHS, PC_RES_OUTER, PC_RES_INNER,
-  PC_JAC, PC_ERRTEST_RHS, PC_IDLE
+  PH_RES_OUTER = 0,  // consume the rhs of a Newton pass's first residual
+  PH_RES_INNER,      // consume the rhs of a later Newton residual
+  PH_SETUP,          // cvLsSetup: reuse J or ask the warp for it
+  PH_LSFINISH,       // A = I - gamma J, its LU, cvNlsLSetup's bookkeeping
+  PH_NEWTON,         // one Newton iteration and its convergence test
+  PH_NLS_AFTER,      // a failed Newton pass: retry with a fresh J?
+  PH_NLS_END,        // cvNls' tail, cvHandleNFlag, cvDoErrorTest
+  PH_ERRTEST_RHS,    // consume the rhs of the order-1 restart of a step
+  PH_STEP_OK,        // cvCompleteStep, cvPrepareNextStep, tout reached?
+  PH_SOLVE_END,      // the restart wrapper
+  PH_SOLVE,          // CVode's first-call block
+  PH_FIRST_RHS,      // consume f(t0, y0)
+  PH_HIN_START,      // cvHin's bounds
+  PH_HIN_RHS,        // consume cvYddNorm's rhs
+  PH_HIN_REQ,        // cvYddNorm: request the rhs at t0 + hg
+  PH_AFTER_HIN,      // the first step size is known
+  PH_STEP,           // the CVode loop top and cvStep's prologue
+  PH_ATTEMPT,        // predict, cvSet, cvNls' set-up
+  PH_NLS_OUTER,      // request the rhs of a Newton pass's first residual
+  PH_DONE,           // the cell is finished (flag set): take the next one
+  PH_IDLE            // no cell left for this lane
 };
 
 template <int N>
 struct LaneCell {
   // ---- the cell ----
-  int cell;        // the cell being integrated, -1 when idle
-  int pc;
+  int cell;        // the cell being integrated, -1 when none
+  int ph, wait;    // the phase, and the request the lane waits on
+  int retval;      // the result carried into the next phase
+  int flag;        // the finished cell's flag (PH_DONE)
   double dt;
   double Tfix;
   Params p;
@@ -66,8 +93,13 @@ struct LaneCell {
   double yreq[N], freq[N];   // the pending rhs request and its result
   int rhs_ret;
   double savedJ[N * N];      // column-major (element (i, j) at i + j N)
-  double A[N * N];
+  union {                    // the Newton matrix's factors
+    double A[N * N];
+    float A32[N * N];        // the FP32 form (SolveOpts::lu32)
+  };
   int piv[N];
+  bool lu64;                 // lu32: factor in FP64 until the next step
+  bool fact32;               // the current factors are A32's
   double atol[N];
   // ---- CVodeMem ----
   long st[NSTAT];
@@ -92,123 +124,146 @@ struct LaneCell {
   // Newton
   bool callSetup, jbad;
   long niters, nconvfails;
-  int curiter, nls_ret;
+  int curiter;
   double tol;
   // ls_setup
   int ls_retval;
 };
 
+// Code size. The control code of the sweep runs on a few lanes at a time
+// and is not where the time goes, but every instruction of it competes with
+// the rhs for the instruction cache; these switches keep it compact: the
+// vector loops rolled (KBL_LOOP), the vector and step helpers out of line
+// (KBL_HELPER, KBL_VEC), the sweep one function (KBL_SWEEP).
+#ifndef KBL_LOOP
+#define KBL_LOOP
+#endif
+#ifndef KBL_VEC
+#define KBL_VEC __forceinline__
+#endif
+#ifndef KBL_HELPER
+#define KBL_HELPER
+#endif
+#ifndef KBL_SWEEP
+#define KBL_SWEEP
+#endif
+
 // ---- vector operations (bdf_cell.hpp:296-400), private arrays ----
 template <int N>
-__device__ __forceinline__ void axpy_(double a, const double* x, double* y) {
+__device__ KBL_VEC void axpy_(double a, const double* x, double* y) {
   if (a == 1.0) {
-    for (int i = 0; i < N; i++) y[i] += x[i];
+    KBL_LOOP for (int i = 0; i < N; i++) y[i] += x[i];
   } else if (a == -1.0) {
-    for (int i = 0; i < N; i++) y[i] -= x[i];
+    KBL_LOOP for (int i = 0; i < N; i++) y[i] -= x[i];
   } else {
-    for (int i = 0; i < N; i++) y[i] += a * x[i];
+    KBL_LOOP for (int i = 0; i < N; i++) y[i] += a * x[i];
   }
 }
 template <int N>
-__device__ __forceinline__ void lin_sum_(double a, const double* x, double b,
+__device__ KBL_VEC void lin_sum_(double a, const double* x, double b,
                                          const double* y, double* z) {
   if (b == 1.0 && z == y) { axpy_<N>(a, x, z); return; }
   if (a == 1.0 && z == x) { axpy_<N>(b, y, z); return; }
   if (a == 1.0 && b == 1.0) {
-    for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
     return;
   }
   bool test;
   if ((test = (a == 1.0 && b == -1.0)) || (a == -1.0 && b == 1.0)) {
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
     return;
   }
   if ((test = (a == 1.0)) || b == 1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
     return;
   }
   if ((test = (a == -1.0)) || b == -1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
     return;
   }
   if (a == b) {
-    for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
     return;
   }
   if (a == -b) {
-    for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
+    KBL_LOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
     return;
   }
-  for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
+  KBL_LOOP for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
 }
 template <int N>
-__device__ __forceinline__ void scale_(double c, const double* x, double* z) {
-  for (int i = 0; i < N; i++) z[i] = c * x[i];
+__device__ KBL_VEC void scale_(double c, const double* x, double* z) {
+  KBL_LOOP for (int i = 0; i < N; i++) z[i] = c * x[i];
 }
 template <int N>
-__device__ __forceinline__ double wrms_(const double* x, const double* w) {
+__device__ KBL_VEC double wrms_(const double* x, const double* w) {
   double sum = 0.0;
-  for (int i = 0; i < N; i++) {
+  KBL_LOOP for (int i = 0; i < N; i++) {
     const double pv = x[i] * w[i];
     sum += pv * pv;
   }
   return ssqrt_(sum / N);
 }
 
-// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457)
-template <int N>
-__device__ int getrf_(double* a, int* p) {
-  for (int k = 0; k < N; k++) {
-    double* col_k = a + k * N;
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457). R is
+// the factors' type: double, or float for the FP32 Newton-matrix form (the
+// factorisation's arithmetic in float; the solve's right-hand side and its
+// accumulation stay double)
+template <int N, class R>
+__device__ KBL_HELPER int getrf_(R* a, int* p) {
+  KBL_LOOP for (int k = 0; k < N; k++) {
+    R* col_k = a + k * N;
     int l = k;
-    for (int i = k + 1; i < N; i++)
+    KBL_LOOP for (int i = k + 1; i < N; i++)
       if (fabs(col_k[i]) > fabs(col_k[l])) l = i;
     p[k] = l;
-    if (col_k[l] == 0.0) return k + 1;
-    if (l != k)
-      for (int i = 0; i < N; i++) {
-        double* ci = a + i * N;
-        const double t = ci[l];
+    if (col_k[l] == R(0)) return k + 1;
+    if (l != k) {
+      KBL_LOOP for (int i = 0; i < N; i++) {
+        R* ci = a + i * N;
+        const R t = ci[l];
         ci[l] = ci[k];
         ci[k] = t;
       }
-    const double mult = 1.0 / col_k[k];
-    for (int i = k + 1; i < N; i++) col_k[i] *= mult;
-    for (int j = k + 1; j < N; j++) {
-      double* col_j = a + j * N;
-      const double a_kj = col_j[k];
-      if (a_kj != 0.0)
-        for (int i = k + 1; i < N; i++) col_j[i] -= a_kj * col_k[i];
+    }
+    const R mult = R(1) / col_k[k];
+    KBL_LOOP for (int i = k + 1; i < N; i++) col_k[i] *= mult;
+    KBL_LOOP for (int j = k + 1; j < N; j++) {
+      R* col_j = a + j * N;
+      const R a_kj = col_j[k];
+      if (a_kj != R(0)) {
+        KBL_LOOP for (int i = k + 1; i < N; i++) col_j[i] -= a_kj * col_k[i];
+      }
     }
   }
   return 0;
 }
-template <int N>
-__device__ void getrs_(const double* a, const int* p, double* b) {
-  for (int k = 0; k < N; k++) {
+template <int N, class R>
+__device__ KBL_HELPER void getrs_(const R* a, const int* p, double* b) {
+  KBL_LOOP for (int k = 0; k < N; k++) {
     const int pk = p[k];
     if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
   }
-  for (int k = 0; k < N - 1; k++) {
-    const double* col_k = a + k * N;
+  KBL_LOOP for (int k = 0; k < N - 1; k++) {
+    const R* col_k = a + k * N;
     const double bk = b[k];
-    for (int i = k + 1; i < N; i++) b[i] -= col_k[i] * bk;
+    KBL_LOOP for (int i = k + 1; i < N; i++) b[i] -= (double)col_k[i] * bk;
   }
-  for (int k = N - 1; k > 0; k--) {
-    const double* col_k = a + k * N;
-    b[k] /= col_k[k];
+  KBL_LOOP for (int k = N - 1; k > 0; k--) {
+    const R* col_k = a + k * N;
+    b[k] /= (double)col_k[k];
     const double bk = b[k];
-    for (int i = 0; i < k; i++) b[i] -= col_k[i] * bk;
+    KBL_LOOP for (int i = 0; i < k; i++) b[i] -= (double)col_k[i] * bk;
   }
-  b[0] /= a[0];
+  b[0] /= (double)a[0];
 }
 
 template <int N, bool EVT>
@@ -217,7 +272,7 @@ struct Machine {
   const SolveOpts& o;
   __device__ Machine(LaneCell<N>& s_, const SolveOpts& o_) : s(s_), o(o_) {}
 
-  __device__ int ewt_set(const double* ycur, double* w) {
+  __device__ KBL_HELPER int ewt_set(const double* ycur, double* w) {
     for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
     for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
     if (s.atolmin0) {
@@ -229,7 +284,7 @@ struct Machine {
     return 0;
   }
 
-  __device__ void reinit(double t0, const double* y0, double h_init) {
+  __device__ KBL_HELPER void reinit(double t0, const double* y0, double h_init) {
     s.tn = t0;
     for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
     s.q = 1; s.L = 2; s.qwait = s.L;
@@ -240,18 +295,26 @@ struct Machine {
     s.hin = h_init;
     s.nstlj = 0;
     s.acnrmcur = false; s.nls_jcur = false; s.jcur = false;
+    s.lu64 = false; s.fact32 = false;
     s.saved_tq5 = 0.0;
     for (int i = 0; i <= L_MAX; i++) s.tau[i] = 0.0;
     s.eta = 1.0;
   }
 
-  __device__ __forceinline__ void request_rhs(const double* yv, int pc) {
+  __device__ __forceinline__ void request_rhs(const double* yv, int ph) {
     for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
-    s.pc = pc;
+    s.ph = ph;
+    s.wait = WAIT_RHS;
+  }
+  // a failed CVode call: to the restart wrapper at the current time
+  __device__ __forceinline__ void fail_solve(int retval) {
+    s.tret = s.tn;
+    s.retval = retval;
+    s.ph = PH_SOLVE_END;
   }
 
   // ---- step helpers (bdf_cell.hpp:825-954, 1386-1500) ----
-  __device__ void rescale_() {
+  __device__ KBL_HELPER void rescale_() {
     double c = s.eta;
     for (int j = 1; j <= s.q; j++) {
       scale_<N>(c, s.zn[j], s.zn[j]);
@@ -262,7 +325,7 @@ struct Machine {
     s.hscale = s.h;
     s.nscon = 0;
   }
-  __device__ void increase_bdf_() {
+  __device__ KBL_HELPER void increase_bdf_() {
     for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
     double alpha1, prod, xiold, alpha0;
     s.l[2] = alpha1 = prod = xiold = 1.0;
@@ -283,7 +346,7 @@ struct Machine {
     if (s.q > 1)
       for (int j = 2; j <= s.q; j++) axpy_<N>(s.l[j], s.zn[s.L], s.zn[j]);
   }
-  __device__ void decrease_bdf_() {
+  __device__ KBL_HELPER void decrease_bdf_() {
     for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
     s.l[2] = 1.0;
     double hsum = 0.0;
@@ -295,22 +358,22 @@ struct Machine {
     if (s.q > 2)
       for (int j = 2; j < s.q; j++) axpy_<N>(-s.l[j], s.zn[s.q], s.zn[j]);
   }
-  __device__ void adjust_order_(int deltaq) {
+  __device__ KBL_HELPER void adjust_order_(int deltaq) {
     if ((s.q == 2) && (deltaq != 1)) return;
     if (deltaq == 1) increase_bdf_();
     else if (deltaq == -1) decrease_bdf_();
   }
-  __device__ void predict_() {
+  __device__ KBL_HELPER void predict_() {
     s.tn += s.h;
     for (int k = 1; k <= s.q; k++)
       for (int j = s.q; j >= k; j--) axpy_<N>(1.0, s.zn[j], s.zn[j - 1]);
   }
-  __device__ void restore_(double saved_t) {
+  __device__ KBL_HELPER void restore_(double saved_t) {
     s.tn = saved_t;
     for (int k = 1; k <= s.q; k++)
       for (int j = s.q; j >= k; j--) axpy_<N>(-1.0, s.zn[j], s.zn[j - 1]);
   }
-  __device__ void set_() {
+  __device__ KBL_HELPER void set_() {
     double xi_inv, xistar_inv, alpha0, alpha0_hat;
     s.l[0] = s.l[1] = xi_inv = xistar_inv = 1.0;
     for (int i = 2; i <= s.q; i++) s.l[i] = 0.0;
@@ -358,7 +421,8 @@ struct Machine {
     if (s.st[ST_NST] == 0) s.gammap = s.gamma;
     s.gamrat = (s.st[ST_NST] > 0) ? s.gamma / s.gammap : 1.0;
   }
-  __device__ void complete_step_() {
+  __device__ KBL_HELPER void complete_step_() {
+    s.lu64 = false;
     s.st[ST_NST]++;
     s.nscon++;
     s.hu = s.h;
@@ -373,7 +437,7 @@ struct Machine {
       s.saved_tq5 = s.tq[5];
     }
   }
-  __device__ void set_eta_() {
+  __device__ KBL_HELPER void set_eta_() {
     if ((s.eta > ETA_MIN_FX) && (s.eta < ETA_MAX_FX)) {
       s.eta = 1.0;
       s.hprime = s.h;
@@ -384,7 +448,7 @@ struct Machine {
     s.hprime = s.h * s.eta;
     if (s.qprime < s.q) s.nscon = 0;
   }
-  __device__ void prepare_next_step_(double dsm) {
+  __device__ KBL_HELPER void prepare_next_step_(double dsm) {
     if (s.etamax == 1.0) {
       s.qwait = s.qwait > 2 ? s.qwait : 2;
       s.qprime = s.q;
@@ -432,7 +496,7 @@ struct Machine {
     }
     set_eta_();
   }
-  __device__ void get_dky_(double t, double* dky) {
+  __device__ KBL_HELPER void get_dky_(double t, double* dky) {
     const double sv = (t - s.tn) / s.h;
     for (int j = s.q; j >= 0; j--) {
       double c = 1.0;
@@ -442,17 +506,18 @@ struct Machine {
     }
   }
   // the charge invariant of a DQ-Jacobian Newton correction
-  // (bdf_cell.hpp:1266-1287)
+  // (bdf_cell.hpp:1266-1287); the species loops are unrolled so that the
+  // charges are constants
   __device__ double inv_dot_(const double* x) const {
     double sum = 0.0;
-    for (int i = 0; i < NSPEC; i++)
+    KB_UNROLL for (int i = 0; i < NSPEC; i++)
       if (species_charge(i) != 0) sum += species_charge(i) * x[i];
     return sum;
   }
   __device__ void inv_set_(double* x, double target) const {
-    const int r = IDX_ELECTRON;
+    const int r = IDX_ELECTRON < 0 ? 0 : IDX_ELECTRON;
     double sum = 0.0, sa = 0.0;
-    for (int i = 0; i < NSPEC; i++)
+    KB_UNROLL for (int i = 0; i < NSPEC; i++)
       if (i != r && species_charge(i) != 0) {
         sum += species_charge(i) * x[i];
         sa += fabs(species_charge(i) * (s.zn[0][i] + s.acor[i]));
@@ -464,24 +529,34 @@ struct Machine {
   }
   // the Newton matrix after a (re)evaluated or reused J: A = I - gamma J
   // and its LU (the tail of cvLsSetup, bdf_cell.hpp:1097-1130)
-  __device__ int ls_finish_() {
-    int retval = s.ls_retval;
-    if (retval == 0) {
-      const double c = -s.gamma;
-      for (int j = 0; j < N; j++) {
-        for (int i = 0; i < N; i++) {
-          const int k = i + j * N;
-          s.A[k] = s.savedJ[k] * c;
-        }
-        s.A[j + j * N] += 1.0;
-      }
-    }
+  __device__ KBL_HELPER int ls_finish_() {
+    const int retval = s.ls_retval;
     if (s.jcur) {
       s.st[ST_NJE]++;
       s.nstlj = s.st[ST_NST];
     }
     if (retval != 0) return retval;
-    return getrf_<N>(s.A, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
+    const double c = -s.gamma;
+    s.fact32 = o.lu32 && !s.lu64;
+    if (s.fact32) {
+      for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++) {
+          const int k = i + j * N;
+          double a = s.savedJ[k] * c;
+          if (i == j) a += 1.0;
+          s.A32[k] = (float)a;
+        }
+      return getrf_<N, float>(s.A32, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
+    }
+    for (int j = 0; j < N; j++) {
+      for (int i = 0; i < N; i++) {
+        const int k = i + j * N;
+        s.A[k] = s.savedJ[k] * c;
+      }
+      s.A[j + j * N] += 1.0;
+    }
+    if (o.lu32) s.st[ST_NLU64]++;
+    return getrf_<N, double>(s.A, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
   }
   // cvNlsLSetup's bookkeeping around ls_setup (bdf_cell.hpp:1051-1065)
   __device__ int lsetup_done_(int retval) {
@@ -497,43 +572,261 @@ struct Machine {
     return SUCCESS;
   }
 
-  // ---- the state machine: advance to the next request ----
-  // returns REQ_RHS (s.yreq set), REQ_JAC, or REQ_DONE (the cell's flag
-  // in *flag_out)
-  __device__ int advance(int* flag_out) {
-    int retval;
-    switch (s.pc) {
-      case PC_NEW: goto L_new;
-      case PC_FIRST_RHS: goto L_first_rhs;
-      case PC_HIN_RHS: goto L_hin_rhs;
-      case PC_RES_OUTER: goto L_res_outer;
-      case PC_RES_INNER: goto L_res_inner;
-      case PC_JAC: goto L_jac;
-      case PC_ERRTEST_RHS: goto L_errtest_rhs;
-      default: return REQ_NONE;
+  // ---- one sweep of the phase handlers ----
+  // Each handler acts on the lanes in its phase and may move them on to a
+  // later handler; a lane leaves the sweep waiting for an rhs or a
+  // Jacobian, in PH_DONE, or (after an early failure of a CVode call,
+  // rare) in PH_SOLVE_END, which the next sweep takes up.
+  __device__ KBL_SWEEP void sweep() {
+    if (s.wait != WAIT_NONE) return;
+    // ---- cvNlsResidual's tail (bdf_cell.hpp:1022-1032) ----
+    // (a failure of a pass's first residual or of its lsetup ends the
+    // Newton solve without the retry, bdf_cell.hpp:972-977)
+    if (s.ph == PH_RES_OUTER) {
+      const int r = residual_done_();
+      if (r != SUCCESS) { s.retval = r; s.ph = PH_NLS_END; }
+      else s.ph = s.callSetup ? PH_SETUP : PH_NEWTON;
     }
-
-  L_new:  // a fresh cell (reinit done by the caller), or a restart
-  L_solve: {
-      // CVode(dt) first-call block (bdf_cell.hpp:570-593)
+    if (s.ph == PH_RES_INNER) {
+      const int r = residual_done_();
+      if (r != SUCCESS) { s.retval = r; s.ph = PH_NLS_AFTER; }
+      else s.ph = PH_NEWTON;
+    }
+    // ---- cvNlsLSetup -> cvLsSetup (bdf_cell.hpp:1051-1096) ----
+    if (s.ph == PH_SETUP) {
+      if (s.jbad) s.convfail = FAIL_BAD_J;
+      const double dgamma = fabs((s.gamma / s.gammap) - 1.0);
+      const bool jbad_ls = (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlj + MSBJ)
+          || ((s.convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
+          || (s.convfail == FAIL_OTHER);
+      s.ls_retval = 0;
+      s.jcur = jbad_ls;
+      s.ph = PH_LSFINISH;
+      if (jbad_ls) {
+        s.wait = WAIT_JAC;  // savedJ and ls_retval come from the warp
+        return;
+      }
+    }
+    if (s.ph == PH_LSFINISH) {
+      const int r = lsetup_done_(ls_finish_());
+      if (r != SUCCESS) { s.retval = r; s.ph = PH_NLS_END; }
+      else s.ph = PH_NEWTON;
+    }
+    // ---- one Newton iteration (bdf_cell.hpp:978-1000) and
+    //      cvNlsConvTest (bdf_cell.hpp:1035-1048) ----
+    if (s.ph == PH_NEWTON) {
+      s.niters++;
+      const bool inv = (o.jac == 2) && IDX_ELECTRON >= 0;
+      const double cg = inv ? inv_dot_(s.delta) : 0.0;
+      scale_<N>(-1.0, s.delta, s.delta);
+      if (s.fact32) getrs_<N, float>(s.A32, s.piv, s.delta);
+      else getrs_<N, double>(s.A, s.piv, s.delta);
+      if (s.gamrat != 1.0) scale_<N>(2.0 / (1.0 + s.gamrat), s.delta, s.delta);
+      if (inv) inv_set_(s.delta, -cg);
+      lin_sum_<N>(1.0, s.acor, 1.0, s.delta, s.acor);
+      const int m = s.curiter;
+      s.delnrm = wrms_<N>(s.delta, s.ewt);
+      if (m > 0) s.crate = smax_(CRDOWN * s.crate, s.delnrm / s.delp);
+      const double dcon = s.delnrm * smin_(1.0, s.crate) / s.tol;
+      int r;
+      if (dcon <= 1.0) {
+        s.acnrm = (m == 0) ? s.delnrm : wrms_<N>(s.acor, s.ewt);
+        s.acnrmcur = true;
+        r = SUCCESS;
+      } else if ((m >= 1) && (s.delnrm > RDIV * s.delp)) {
+        r = NLS_CONV_RECVR;
+      } else {
+        s.delp = s.delnrm;
+        r = NLS_CONTINUE;
+      }
+      s.curiter++;
+      if (r == SUCCESS) s.nls_jcur = false;
+      if (r == NLS_CONTINUE && s.curiter >= NLS_MAXCOR) r = NLS_CONV_RECVR;
+      if (r != NLS_CONTINUE) {
+        s.retval = r;
+        s.ph = PH_NLS_AFTER;
+      } else {
+        lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
+        request_rhs(s.y, PH_RES_INNER);
+        return;
+      }
+    }
+    // ---- a failed pass retries once with a fresh Jacobian
+    //      (bdf_cell.hpp:1002-1010) ----
+    if (s.ph == PH_NLS_AFTER) {
+      const int r = s.retval;
+      // a Newton failure with FP32 factors: FP64 from the next setup on
+      if (r > 0 && s.fact32) s.lu64 = true;
+      if (r > 0 && !s.nls_jcur) {
+        s.nconvfails++;
+        s.callSetup = true;
+        s.jbad = true;
+        for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+        s.ph = PH_NLS_OUTER;
+      } else {
+        s.ph = PH_NLS_END;
+      }
+    }
+    // ---- cvNls' tail (bdf_cell.hpp:1011-1018), cvHandleNFlag
+    //      (1315-1337), cvDoErrorTest (1339-1381) ----
+    if (s.ph == PH_NLS_END) {
+      const int r = s.retval;
+      if (r > 0 && s.fact32) s.lu64 = true;
+      if (r != SUCCESS) s.nconvfails++;
+      s.st[ST_NNI] += s.niters;
+      s.st[ST_NNF] += s.nconvfails;
+      if (r == SUCCESS) {
+        lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
+        if (!s.acnrmcur) s.acnrm = wrms_<N>(s.acor, s.ewt);
+        s.jcur = false;
+      }
+      s.nflag = r;
+      if (r != SUCCESS) {
+        restore_(s.saved_t);
+        if (r < 0) {
+          fail_solve((r == LSETUP_FAIL || r == LSOLVE_FAIL || r == RHSFUNC_FAIL)
+                         ? r : NLS_FAIL);
+        } else {
+          s.ncf++;
+          s.etamax = 1.0;
+          if (((fabs(s.h) <= 0.0) || (s.ncf == o.max_conv_fails))
+              && (r == NLS_CONV_RECVR || r == RHSFUNC_RECVR)) {
+            fail_solve(r == NLS_CONV_RECVR ? CONV_FAILURE : REPTD_RHSFUNC_ERR);
+          } else {
+            s.eta = smax_(ETA_CF, 0.0 / fabs(s.h));
+            s.nflag = PREV_CONV_FAIL;
+            rescale_();
+            s.ph = PH_ATTEMPT;
+          }
+        }
+      } else {
+        const double dsm = s.acnrm * s.tq[2];
+        s.dsm = dsm;
+        if (dsm <= 1.0) {
+          s.ph = PH_STEP_OK;
+        } else {
+          s.nef++;
+          s.st[ST_NETF]++;
+          s.nflag = PREV_ERR_FAIL;
+          restore_(s.saved_t);
+          if ((fabs(s.h) <= 0.0) || (s.nef == o.max_err_fails)) {
+            fail_solve(ERR_FAILURE);
+          } else {
+            s.etamax = 1.0;
+            if (s.nef <= MXNEF1) {
+              s.eta = 1.0 / (pow(BIAS2 * dsm, 1.0 / s.L) + ADDON);
+              s.eta = smax_(ETA_MIN_EF, smax_(s.eta, 0.0 / fabs(s.h)));
+              if (s.nef >= SMALL_NEF) s.eta = smin_(s.eta, ETA_MAX_EF);
+              rescale_();
+              s.ph = PH_ATTEMPT;
+            } else if (s.q > 1) {
+              s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
+              adjust_order_(-1);
+              s.L = s.q;
+              s.q--;
+              s.qwait = s.L;
+              rescale_();
+              s.ph = PH_ATTEMPT;
+            } else {
+              // order 1: restart the history from y' = f(tn, y)
+              s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
+              s.h *= s.eta;
+              s.next_h = s.h;
+              s.hscale = s.h;
+              s.qwait = LONG_WAIT;
+              s.nscon = 0;
+              request_rhs(s.zn[0], PH_ERRTEST_RHS);
+              return;
+            }
+          }
+        }
+      }
+    }
+    if (s.ph == PH_ERRTEST_RHS) {
+      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      s.st[ST_NFE]++;
+      if (s.rhs_ret > 0) {
+        fail_solve(UNREC_RHSFUNC_ERR);
+      } else {
+        scale_<N>(s.h, s.tempv, s.zn[1]);
+        s.ph = PH_ATTEMPT;
+      }
+    }
+    // ---- the accepted step and CVode's tout test (bdf_cell.hpp:620-636,
+    //      1386-1500) ----
+    if (s.ph == PH_STEP_OK) {
+      complete_step_();
+      prepare_next_step_(s.dsm);
+      s.etamax = (s.st[ST_NST] <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
+      scale_<N>(s.tq[2], s.acor, s.acor);
+      s.nstloc++;
+      if ((s.tn - s.dt) * s.h >= 0.0) {
+        s.tret = s.dt;
+        get_dky_(s.dt, s.y);  // y(tout) into y
+        s.next_q = s.qprime;
+        s.next_h = s.hprime;
+        s.retval = SUCCESS;
+        s.ph = PH_SOLVE_END;
+      } else {
+        s.ph = PH_STEP;
+      }
+    }
+    // ---- the restart wrapper (bdf_cell.hpp:1536-1546). y holds y(tout)
+    //      on success; on failure the last accepted state, which is zn[0]
+    //      (also when the failure precedes the first step: zn[0] is then
+    //      the state of the last reinit, the reference's untouched
+    //      yout) ----
+    if (s.ph == PH_SOLVE_END) {
+      const int r = s.retval;
+      if (r < 0)
+        for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
+      for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
+      const bool restartable = r == ERR_FAILURE || r == CONV_FAILURE
+                               || r == REPTD_RHSFUNC_ERR;
+      if (r >= 0 || !restartable || s.restarts >= o.max_restarts) {
+        s.flag = r >= 0 ? 0 : r;
+        s.ph = PH_DONE;
+        return;
+      }
+      ++s.restarts;
+      const double hcur = s.next_h;
+      reinit(s.tret, s.y, hcur > 0.0 ? 0.1 * hcur : 0.0);
+      s.ph = PH_SOLVE;
+    }
+    // ---- CVode(dt)'s first-call block (bdf_cell.hpp:570-593) ----
+    if (s.ph == PH_SOLVE) {
       s.tret = s.tn;
       const double tout = s.dt;
       const double tdist = fabs(tout - s.tn);
       const double tround = UROUND * smax_(fabs(s.tn), fabs(tout));
-      if (tdist == 0.0 || tdist < 2.0 * tround) { retval = TOO_CLOSE; goto L_solve_end; }
-      if (ewt_set(s.zn[0], s.ewt) != 0) { retval = ILL_INPUT; goto L_solve_end; }
-      request_rhs(s.zn[0], PC_FIRST_RHS);
-      return REQ_RHS;
+      if (tdist == 0.0 || tdist < 2.0 * tround) {
+        fail_solve(TOO_CLOSE);
+        return;
+      }
+      if (ewt_set(s.zn[0], s.ewt) != 0) {
+        fail_solve(ILL_INPUT);
+        return;
+      }
+      request_rhs(s.zn[0], PH_FIRST_RHS);
+      return;
     }
-  L_first_rhs: {
+    if (s.ph == PH_FIRST_RHS) {
       for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
       s.st[ST_NFE]++;
-      if (s.rhs_ret > 0) { retval = FIRST_RHSFUNC_ERR; goto L_solve_end; }
+      if (s.rhs_ret > 0) {
+        fail_solve(FIRST_RHSFUNC_ERR);
+        return;
+      }
       s.h = s.hin;
+      if (s.h != 0.0 && (s.dt - s.tn) * s.h < 0.0) {
+        fail_solve(ILL_INPUT);
+        return;
+      }
+      s.ph = (s.h != 0.0) ? PH_AFTER_HIN : PH_HIN_START;
+    }
+    // ---- cvHin (bdf_cell.hpp:717-794) ----
+    if (s.ph == PH_HIN_START) {
       const double tout = s.dt;
-      if (s.h != 0.0 && (tout - s.tn) * s.h < 0.0) { retval = ILL_INPUT; goto L_solve_end; }
-      if (s.h != 0.0) goto L_after_hin;
-      // cvHin (bdf_cell.hpp:717-794)
       const double tdiff = tout - s.tn;
       s.hin_sign = (tdiff > 0.0) ? 1 : -1;
       const double tdist = fabs(tdiff);
@@ -558,85 +851,93 @@ struct Machine {
       s.hin_hg = ssqrt_(s.hin_hlb * s.hin_hub);
       if (s.hin_hub < s.hin_hlb) {
         s.h = s.hin_sign == -1 ? -s.hin_hg : s.hin_hg;
-        goto L_after_hin;
+        s.ph = PH_AFTER_HIN;
+      } else {
+        s.hin_hs = s.hin_hg;
+        s.hin_hnew = s.hin_hg;
+        s.hin_count1 = 1;
+        s.hin_count2 = 1;
+        s.ph = PH_HIN_REQ;
       }
-      s.hin_hs = s.hin_hg;
-      s.hin_hnew = s.hin_hg;
-      s.hin_count1 = 1;
     }
-  L_hin_c1: {
-      s.hin_count2 = 1;
-    }
-  L_hin_c2: {
-      s.hin_hgs = s.hin_hg * s.hin_sign;
-      lin_sum_<N>(s.hin_hgs, s.zn[1], 1.0, s.zn[0], s.y);
-      request_rhs(s.y, PC_HIN_RHS);
-      return REQ_RHS;
-    }
-  L_hin_rhs: {
+    if (s.ph == PH_HIN_RHS) {
       for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
       s.st[ST_NFE]++;
-      bool hgOK = false;
-      double yddnrm = 0.0;
+      bool done = false;
       if (s.rhs_ret == 0) {
         lin_sum_<N>(1.0 / s.hin_hgs, s.tempv, -1.0 / s.hin_hgs, s.zn[1], s.tempv);
-        yddnrm = wrms_<N>(s.tempv, s.ewt);
-        hgOK = true;
+        const double yddnrm = wrms_<N>(s.tempv, s.ewt);
+        s.hin_hs = s.hin_hg;
+        const double hub = s.hin_hub;
+        s.hin_hnew = (yddnrm * hub * hub > 2.0) ? ssqrt_(2.0 / yddnrm)
+                                                : ssqrt_(s.hin_hg * hub);
+        const double hrat = s.hin_hnew / s.hin_hg;
+        if (s.hin_count1 == MAX_ITERS || ((hrat > 0.5) && (hrat < 2.0))) {
+          done = true;
+        } else if ((s.hin_count1 > 1) && (hrat > 2.0)) {
+          s.hin_hnew = s.hin_hg;
+          done = true;
+        } else {
+          s.hin_hg = s.hin_hnew;
+          s.hin_count1++;
+          s.hin_count2 = 1;
+          s.ph = PH_HIN_REQ;
+        }
       } else {
         s.hin_hg *= 0.2;
-        if (++s.hin_count2 <= MAX_ITERS) goto L_hin_c2;
+        if (++s.hin_count2 <= MAX_ITERS) {
+          s.ph = PH_HIN_REQ;
+        } else if (s.hin_count1 <= 2) {
+          fail_solve(REPTD_RHSFUNC_ERR);
+          return;
+        } else {
+          s.hin_hnew = s.hin_hs;
+          done = true;
+        }
       }
-      if (!hgOK) {
-        if (s.hin_count1 <= 2) { retval = REPTD_RHSFUNC_ERR; goto L_solve_end; }
-        s.hin_hnew = s.hin_hs;
-        goto L_hin_done;
+      if (done) {
+        double h0 = H_BIAS * s.hin_hnew;
+        if (h0 < s.hin_hlb) h0 = s.hin_hlb;
+        if (h0 > s.hin_hub) h0 = s.hin_hub;
+        if (s.hin_sign == -1) h0 = -h0;
+        s.h = h0;
+        s.ph = PH_AFTER_HIN;
       }
-      s.hin_hs = s.hin_hg;
-      const double hub = s.hin_hub;
-      s.hin_hnew = (yddnrm * hub * hub > 2.0) ? ssqrt_(2.0 / yddnrm)
-                                              : ssqrt_(s.hin_hg * hub);
-      if (s.hin_count1 == MAX_ITERS) goto L_hin_done;
-      const double hrat = s.hin_hnew / s.hin_hg;
-      if ((hrat > 0.5) && (hrat < 2.0)) goto L_hin_done;
-      if ((s.hin_count1 > 1) && (hrat > 2.0)) {
-        s.hin_hnew = s.hin_hg;
-        goto L_hin_done;
-      }
-      s.hin_hg = s.hin_hnew;
-      s.hin_count1++;
-      goto L_hin_c1;
     }
-  L_hin_done: {
-      double h0 = H_BIAS * s.hin_hnew;
-      if (h0 < s.hin_hlb) h0 = s.hin_hlb;
-      if (h0 > s.hin_hub) h0 = s.hin_hub;
-      if (s.hin_sign == -1) h0 = -h0;
-      s.h = h0;
+    if (s.ph == PH_HIN_REQ) {
+      s.hin_hgs = s.hin_hg * s.hin_sign;
+      lin_sum_<N>(s.hin_hgs, s.zn[1], 1.0, s.zn[0], s.y);
+      request_rhs(s.y, PH_HIN_RHS);
+      return;
     }
-  L_after_hin: {
+    if (s.ph == PH_AFTER_HIN) {
       s.hscale = s.h;
       s.hprime = s.h;
       scale_<N>(s.h, s.zn[1], s.zn[1]);
       s.nstloc = 0;
+      s.ph = PH_STEP;
     }
-  L_step_loop: {
-      // the CVode main loop (bdf_cell.hpp:595-636)
+    // ---- the CVode main loop's top (bdf_cell.hpp:595-619) and cvStep's
+    //      prologue (798-805) ----
+    if (s.ph == PH_STEP) {
       s.next_h = s.h;
       s.next_q = s.q;
       if (s.st[ST_NST] > 0 && ewt_set(s.zn[0], s.ewt) != 0) {
-        retval = ILL_INPUT; s.tret = s.tn; goto L_solve_end;
+        fail_solve(ILL_INPUT);
+        return;
       }
       if (s.mxstep > 0 && s.nstloc >= s.mxstep) {
-        retval = TOO_MUCH_WORK; s.tret = s.tn; goto L_solve_end;
+        fail_solve(TOO_MUCH_WORK);
+        return;
       }
       const double nrm = wrms_<N>(s.zn[0], s.ewt);
       s.tolsf = UROUND * nrm;
       if (s.tolsf > 1.0) {
-        retval = TOO_MUCH_ACC; s.tret = s.tn; s.tolsf *= 2.0;
-        goto L_solve_end;
+        s.tolsf *= 2.0;
+        fail_solve(TOO_MUCH_ACC);
+        return;
       }
       s.tolsf = 1.0;
-      // cvStep (bdf_cell.hpp:798-822)
       s.ncf = 0;
       s.nef = 0;
       s.dsm = 0.0;
@@ -651,11 +952,13 @@ struct Machine {
       }
       s.saved_t = s.tn;
       s.nflag = FIRST_CALL;
+      s.ph = PH_ATTEMPT;
     }
-  L_attempt: {
+    // ---- an attempt: predict, cvSet, cvNls' set-up
+    //      (bdf_cell.hpp:806-808, 958-977) ----
+    if (s.ph == PH_ATTEMPT) {
       predict_();
       set_();
-      // cvNls (bdf_cell.hpp:958-1019)
       s.convfail = ((s.nflag == FIRST_CALL) || (s.nflag == PREV_ERR_FAIL))
                        ? NO_FAILURES : FAIL_OTHER;
       s.callSetup = (s.nflag == PREV_CONV_FAIL) || (s.nflag == PREV_ERR_FAIL)
@@ -666,209 +969,17 @@ struct Machine {
       s.jbad = false;
       s.niters = 0;
       s.nconvfails = 0;
+      s.ph = PH_NLS_OUTER;
     }
-  L_nls_outer: {
+    if (s.ph == PH_NLS_OUTER) {
       s.curiter = 0;
       lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
-      request_rhs(s.y, PC_RES_OUTER);
-      return REQ_RHS;
-    }
-  L_res_outer: {
-      retval = residual_done_();
-      if (retval != SUCCESS) goto L_nls_after_outer;
-      if (!s.callSetup) goto L_newton_iter;
-      // cvNlsLSetup -> cvLsSetup (bdf_cell.hpp:1051-1096)
-      if (s.jbad) s.convfail = FAIL_BAD_J;
-      {
-        const double dgamma = fabs((s.gamma / s.gammap) - 1.0);
-        const bool jbad_ls = (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlj + MSBJ)
-            || ((s.convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
-            || (s.convfail == FAIL_OTHER);
-        s.ls_retval = 0;
-        if (!jbad_ls) {
-          s.jcur = false;
-        } else {
-          s.jcur = true;
-          s.pc = PC_JAC;
-          return REQ_JAC;  // savedJ from the warp (ls_retval set there)
-        }
-      }
-    }
-  L_jac: {
-      retval = lsetup_done_(ls_finish_());
-      if (retval != SUCCESS) goto L_nls_after_outer;
-    }
-  L_newton_iter: {
-      s.niters++;
-      const bool inv = (o.jac == 2) && IDX_ELECTRON >= 0;
-      const double cg = inv ? inv_dot_(s.delta) : 0.0;
-      scale_<N>(-1.0, s.delta, s.delta);
-      getrs_<N>(s.A, s.piv, s.delta);
-      if (s.gamrat != 1.0) scale_<N>(2.0 / (1.0 + s.gamrat), s.delta, s.delta);
-      if (inv) inv_set_(s.delta, -cg);
-      lin_sum_<N>(1.0, s.acor, 1.0, s.delta, s.acor);
-      // cvNlsConvTest (bdf_cell.hpp:1035-1048)
-      const int m = s.curiter;
-      s.delnrm = wrms_<N>(s.delta, s.ewt);
-      if (m > 0) s.crate = smax_(CRDOWN * s.crate, s.delnrm / s.delp);
-      const double dcon = s.delnrm * smin_(1.0, s.crate) / s.tol;
-      if (dcon <= 1.0) {
-        s.acnrm = (m == 0) ? s.delnrm : wrms_<N>(s.acor, s.ewt);
-        s.acnrmcur = true;
-        retval = SUCCESS;
-      } else if ((m >= 1) && (s.delnrm > RDIV * s.delp)) {
-        retval = NLS_CONV_RECVR;
-      } else {
-        s.delp = s.delnrm;
-        retval = NLS_CONTINUE;
-      }
-      s.curiter++;
-      if (retval == SUCCESS) { s.nls_jcur = false; goto L_nls_after_outer; }
-      if (retval != NLS_CONTINUE) goto L_nls_after_outer;
-      if (s.curiter >= NLS_MAXCOR) { retval = NLS_CONV_RECVR; goto L_nls_after_outer; }
-      lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
-      request_rhs(s.y, PC_RES_INNER);
-      return REQ_RHS;
-    }
-  L_res_inner: {
-      retval = residual_done_();
-      if (retval != SUCCESS) goto L_nls_after_outer;
-      goto L_newton_iter;
-    }
-  L_nls_after_outer: {
-      if (retval == SUCCESS) goto L_nls_end;
-      if ((retval > 0) && !s.nls_jcur) {
-        s.nconvfails++;
-        s.callSetup = true;
-        s.jbad = true;
-        for (int i = 0; i < N; i++) s.acor[i] = 0.0;
-        goto L_nls_outer;
-      }
-    }
-  L_nls_end: {
-      if (retval != SUCCESS) s.nconvfails++;
-      s.st[ST_NNI] += s.niters;
-      s.st[ST_NNF] += s.nconvfails;
-      if (retval == SUCCESS) {
-        lin_sum_<N>(1.0, s.zn[0], 1.0, s.acor, s.y);
-        if (!s.acnrmcur) s.acnrm = wrms_<N>(s.acor, s.ewt);
-        s.jcur = false;
-      }
-      s.nflag = retval;
-      // cvHandleNFlag (bdf_cell.hpp:1315-1337)
-      if (s.nflag != SUCCESS) {
-        restore_(s.saved_t);
-        if (s.nflag < 0) {
-          retval = (s.nflag == LSETUP_FAIL || s.nflag == LSOLVE_FAIL
-                    || s.nflag == RHSFUNC_FAIL) ? s.nflag : NLS_FAIL;
-          goto L_step_fail;
-        }
-        s.ncf++;
-        s.etamax = 1.0;
-        if ((fabs(s.h) <= 0.0) || (s.ncf == o.max_conv_fails)) {
-          if (s.nflag == NLS_CONV_RECVR) { retval = CONV_FAILURE; goto L_step_fail; }
-          if (s.nflag == RHSFUNC_RECVR) { retval = REPTD_RHSFUNC_ERR; goto L_step_fail; }
-        }
-        s.eta = smax_(ETA_CF, 0.0 / fabs(s.h));
-        s.nflag = PREV_CONV_FAIL;
-        rescale_();
-        goto L_attempt;
-      }
-      // cvDoErrorTest (bdf_cell.hpp:1339-1381)
-      const double dsm = s.acnrm * s.tq[2];
-      s.dsm = dsm;
-      if (dsm <= 1.0) goto L_step_ok;
-      s.nef++;
-      s.st[ST_NETF]++;
-      s.nflag = PREV_ERR_FAIL;
-      restore_(s.saved_t);
-      if ((fabs(s.h) <= 0.0) || (s.nef == o.max_err_fails)) {
-        retval = ERR_FAILURE;
-        goto L_step_fail;
-      }
-      s.etamax = 1.0;
-      if (s.nef <= MXNEF1) {
-        s.eta = 1.0 / (pow(BIAS2 * dsm, 1.0 / s.L) + ADDON);
-        s.eta = smax_(ETA_MIN_EF, smax_(s.eta, 0.0 / fabs(s.h)));
-        if (s.nef >= SMALL_NEF) s.eta = smin_(s.eta, ETA_MAX_EF);
-        rescale_();
-        goto L_attempt;
-      }
-      if (s.q > 1) {
-        s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
-        adjust_order_(-1);
-        s.L = s.q;
-        s.q--;
-        s.qwait = s.L;
-        rescale_();
-        goto L_attempt;
-      }
-      s.eta = smax_(ETA_MIN_EF, 0.0 / fabs(s.h));
-      s.h *= s.eta;
-      s.next_h = s.h;
-      s.hscale = s.h;
-      s.qwait = LONG_WAIT;
-      s.nscon = 0;
-      request_rhs(s.zn[0], PC_ERRTEST_RHS);
-      return REQ_RHS;
-    }
-  L_errtest_rhs: {
-      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
-      s.st[ST_NFE]++;
-      if (s.rhs_ret > 0) { retval = UNREC_RHSFUNC_ERR; goto L_step_fail; }
-      scale_<N>(s.h, s.tempv, s.zn[1]);
-      goto L_attempt;
-    }
-  L_step_ok: {
-      complete_step_();
-      prepare_next_step_(s.dsm);
-      s.etamax = (s.st[ST_NST] <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
-      scale_<N>(s.tq[2], s.acor, s.acor);
-      s.nstloc++;
-      if ((s.tn - s.dt) * s.h >= 0.0) {
-        s.tret = s.dt;
-        get_dky_(s.dt, s.y);  // y(tout) into y
-        s.next_q = s.qprime;
-        s.next_h = s.hprime;
-        retval = SUCCESS;
-        goto L_solve_end;
-      }
-      goto L_step_loop;
-    }
-  L_step_fail: {
-      s.tret = s.tn;
-      goto L_solve_end;
-    }
-  L_solve_end: {
-      // the restart wrapper (bdf_cell.hpp:1536-1546). y holds y(tout) on
-      // success; on failure the last accepted state, which is zn[0] (also
-      // when the failure precedes the first step: zn[0] is then the state
-      // of the last reinit, the reference's untouched yout)
-      if (retval < 0) {
-        for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
-      }
-      for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
-      if (retval >= 0) {
-        *flag_out = 0;
-        s.pc = PC_IDLE;
-        return REQ_DONE;
-      }
-      const bool restartable = retval == ERR_FAILURE || retval == CONV_FAILURE
-                               || retval == REPTD_RHSFUNC_ERR;
-      if (!restartable || s.restarts >= o.max_restarts) {
-        *flag_out = retval;
-        s.pc = PC_IDLE;
-        return REQ_DONE;
-      }
-      ++s.restarts;
-      const double hcur = s.next_h;
-      reinit(s.tret, s.y, hcur > 0.0 ? 0.1 * hcur : 0.0);
-      goto L_solve;
+      request_rhs(s.y, PH_RES_OUTER);
     }
   }
 
   // cvNlsResidual's tail after its rhs (bdf_cell.hpp:1022-1032)
-  __device__ int residual_done_() {
+  __device__ KBL_HELPER int residual_done_() {
     for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
     s.st[ST_NFE]++;
     if (s.rhs_ret > 0) return RHSFUNC_RECVR;

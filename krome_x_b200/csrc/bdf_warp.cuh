@@ -81,7 +81,7 @@ constexpr double UROUND = DBL_EPSILON;
 // reference's SolveStats, runtime/krome.hpp:257-268)
 enum : int {
   ST_NST, ST_NFE, ST_NFEDQ, ST_NJE, ST_NSETUPS, ST_NNI, ST_NNF, ST_NETF,
-  ST_RESTARTS, NSTAT
+  ST_RESTARTS, ST_NLU64, NSTAT
 };
 
 // the options of one solve (the krome_opts keys the hot path reads)
@@ -94,6 +94,7 @@ struct SolveOpts {
   int clip_negative;
   int fail_every;  // fault injection: cells c with (c + 1) % fail_every == 0
                    // report TOO_MUCH_WORK without integrating (0: off)
+  int lu32;        // the Newton matrix factored in FP32 (lane layout only)
 };
 
 __device__ __forceinline__ double smax_(double a, double b) { return a > b ? a : b; }

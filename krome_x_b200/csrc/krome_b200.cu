@@ -161,7 +161,8 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   s.mxstep = so.max_steps == 0 ? 500
              : (so.max_steps < 0 ? KB_MAX_STEPS_CAP : so.max_steps);
   m.reinit(0.0, y0, 0.0);
-  s.pc = kbl::PC_NEW;
+  s.ph = kbl::PH_SOLVE;
+  s.wait = kbl::WAIT_NONE;
   return true;
 }
 
@@ -200,8 +201,10 @@ __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
 // cell of its global thread index; persistent == 1: lanes pull cells from
 // the device work queue (`cursor`) until it is exhausted.
 //
-// Each round: (1) every lane advances its cell to its next request;
-// (2) the warp evaluates the requests with ONE rhs call site: pass 0 the
+// Each round: (1) one sweep of the phase handlers takes every lane to its
+// next request (lanes whose cell finished write it back, take their next
+// cell and sweep once more); (2) the warp evaluates the requests with ONE
+// rhs call site: pass 0 the
 // lanes' own rhs requests, then one pass per group of Jacobian requests,
 // where request r of the pass occupies lanes [r*JL, (r+1)*JL) (JL the lanes
 // one Jacobian needs) and lane r*JL + j evaluates its column / term j; the
@@ -221,17 +224,20 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
   kbl::LaneCell<N> s;
   kbl::Machine<N, EVT> m(s, so);
   s.cell = -1;
-  s.pc = kbl::PC_IDLE;
+  s.ph = kbl::PH_DONE;  // take a first cell
+  s.wait = kbl::WAIT_NONE;
   bool static_taken = false;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  bool exhausted = false;
   const bool dq = so.jac == 2;
   const int JL = dq ? LaneGeo<EVT>::JLANES_DQ : LaneGeo<EVT>::JLANES_AN;
   const int per_pass = 32 / JL;
   for (;;) {
-    int req = kbl::REQ_NONE;
-    while (!exhausted) {
-      if (s.cell < 0) {
+    // a lane whose cell finished in the first sweep takes its next cell
+    // and sweeps again in the same round
+    for (int sweep = 0; sweep < 2; ++sweep) {
+      // bounded: every iteration consumes a cell index (at most ncell)
+      while (s.ph == kbl::PH_DONE) {
+        if (s.cell >= 0) lane_finish<EVT>(s, s.flag, n, T, flags, stats, so);
         int c;
         if (persistent) {
           c = (int)atomicAdd(cursor, 1u);
@@ -239,21 +245,15 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
           c = static_taken ? ncell : gtid;
           static_taken = true;
         }
-        if (c >= ncell) { exhausted = true; break; }
-        if (!lane_start<EVT>(s, m, c, n, T, dt, par, pstride, flags, stats, so))
-          continue;
+        if (c >= ncell) s.ph = kbl::PH_IDLE;
+        else lane_start<EVT>(s, m, c, n, T, dt, par, pstride, flags, stats, so);
       }
-      int flag = 0;
-      req = m.advance(&flag);
-      if (req == kbl::REQ_DONE) {
-        lane_finish<EVT>(s, flag, n, T, flags, stats, so);
-        req = kbl::REQ_NONE;
-        continue;
-      }
-      break;
+      if (s.ph != kbl::PH_IDLE) m.sweep();
+      if (!__any_sync(FULLM, s.ph == kbl::PH_DONE)) break;
     }
-    if (__all_sync(FULLM, exhausted)) break;
-    const unsigned jm = __ballot_sync(FULLM, req == kbl::REQ_JAC);
+    if (__all_sync(FULLM, s.ph == kbl::PH_IDLE)) break;
+    const int req = s.wait;
+    const unsigned jm = __ballot_sync(FULLM, req == kbl::WAIT_JAC);
     const int nj = __popc(jm);
     const int npass = 1 + (nj + per_pass - 1) / per_pass;
     unsigned jrest = jm;
@@ -263,7 +263,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
       int src = lane, role = 0;
       unsigned passm = 0;  // the requesting lanes served in this pass
       if (pass == 0) {
-        active = req == kbl::REQ_RHS;
+        active = req == kbl::WAIT_RHS;
       } else {
         for (int r = 0; r < per_pass && jrest; ++r) {
           const unsigned b = jrest & (~jrest + 1u);
@@ -356,6 +356,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
         if (active) {
           KB_UNROLL for (int i = 0; i < N; ++i) s.freq[i] = f[i];
           s.rhs_ret = r;
+          s.wait = kbl::WAIT_NONE;
           if (hit) s.hitT0 = true;
         }
         continue;
@@ -408,6 +409,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
         }
         if (hitm & (((JL >= 32) ? FULLM : ((1u << JL) - 1u)) << base))
           s.hitT0 = true;
+        s.wait = kbl::WAIT_NONE;
       }
       __syncwarp();
     }
@@ -435,6 +437,8 @@ struct krome_opts {
   int queue_chunk = 1;     // cells per queue pop
   int blocks_per_sm = 0;   // persistent grid: 0 = occupancy limit
   int fail_every = 0;      // fault injection (tests)
+  int lu32 = 0;            // Newton-matrix LU in FP32, FP64 after a Newton
+                           // failure (lane layout)
 };
 
 namespace {
@@ -481,6 +485,7 @@ SolveOpts to_solve_opts(const krome_opts& h) {
   so.max_restarts = h.max_restarts;
   so.clip_negative = h.clip_negative;
   so.fail_every = h.fail_every;
+  so.lu32 = h.lu32;
   return so;
 }
 
@@ -672,6 +677,7 @@ int* int_key(krome_opts* h, const char* k) {
       {"queue_chunk", offsetof(krome_opts, queue_chunk)},
       {"blocks_per_sm", offsetof(krome_opts, blocks_per_sm)},
       {"fail_every", offsetof(krome_opts, fail_every)},
+      {"lu32", offsetof(krome_opts, lu32)},
   };
   for (const auto& e : keys)
     if (!std::strcmp(e.name, k))
@@ -688,7 +694,7 @@ double* dbl_key(krome_opts* h, const char* k) {
 bool bool_key(const char* k) {
   return !std::strcmp(k, "evolve_T") || !std::strcmp(k, "clip_negative")
          || !std::strcmp(k, "error_report") || !std::strcmp(k, "renormalize_x")
-         || !std::strcmp(k, "device_cache");
+         || !std::strcmp(k, "device_cache") || !std::strcmp(k, "lu32");
 }
 }  // namespace
 
@@ -757,10 +763,12 @@ KB_API int krome_opts_get(const krome_opts* hc, const char* key, double* v) {
 namespace {
 // what this library does not implement returns FLAG_UNSUPPORTED before any
 // work: LAPACK and the sparse LU (small networks use the dense LU),
-// conservation, photon bins
+// conservation, photon bins; the FP32 Newton-matrix form exists in the
+// lane layout only
 int unsupported(const krome_opts& h) {
   if (h.linsol == 2 || h.linsol == 3) return -104;
   if (h.conserve != 0) return -104;
+  if (h.lu32 != 0 && h.layout != 1) return -104;
   return 0;
 }
 }  // namespace
@@ -1010,6 +1018,70 @@ KB_API void krome_b200_graph_free(void* handle) {
   cudaGraphExecDestroy(g->exec);
   cudaGraphDestroy(g->graph);
   delete g;
+}
+
+// the network rhs alone at full SIMT width: every thread evaluates the rhs
+// of its cell `reps` times (each evaluation feeds a negligible increment
+// back into the state, so none can be hoisted); the rhs-throughput bound of
+// the solve kernels
+namespace {
+__global__ void kb_rhs_loop(int ncell, const double* n, const double* T,
+                            const double* par, int pstride, int reps,
+                            double* sink) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  using namespace kbnet;
+  constexpr int N = NSPEC + 1;
+  double yf[N], f[N], k[NREA + 1];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) yf[i] = n[(long)c * NSPEC + i];
+  yf[N - 1] = T[c];
+  Params p;
+  params_from_row(par + (long)c * pstride, p);
+  double acc = 0.0;
+  for (int r = 0; r < reps; ++r) {
+    kbw::full_rhs<N, true>(yf, f, p, 0.0, k);
+    yf[0] += 1e-300 * f[0];
+    acc += f[N - 1];
+  }
+  if (acc == 1.2345e-300) sink[c] = acc;
+}
+}  // namespace
+
+KB_API int krome_b200_rhs_throughput(int ncell, const double* n,
+                                     const double* Tgas, const double* par,
+                                     int par_stride, int reps,
+                                     double* rhs_per_s) {
+  if (ncell <= 0 || reps <= 0 || rhs_per_s == nullptr) return -1;
+  const size_t nb = sizeof(double) * (size_t)ncell * kbnet::NSPEC;
+  const size_t tb = sizeof(double) * (size_t)ncell;
+  const size_t pb = sizeof(double) * (size_t)ncell * kbnet::NPAR;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (g_buf.ensure(al(nb) + 2 * al(tb) + al(pb)) != cudaSuccess) return -111;
+  char* b = static_cast<char*>(g_buf.p);
+  double* dn = reinterpret_cast<double*>(b); b += al(nb);
+  double* dT = reinterpret_cast<double*>(b); b += al(tb);
+  double* ds = reinterpret_cast<double*>(b); b += al(tb);
+  double* dp = reinterpret_cast<double*>(b);
+  cudaMemcpy(dn, n, nb, cudaMemcpyHostToDevice);
+  cudaMemcpy(dT, Tgas, tb, cudaMemcpyHostToDevice);
+  cudaMemcpy(dp, par, par_stride ? pb : sizeof(double) * kbnet::NPAR,
+             cudaMemcpyHostToDevice);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  kb_rhs_loop<<<(ncell + 127) / 128, 128>>>(ncell, dn, dT, dp, par_stride, 1, ds);
+  cudaEventRecord(e0);
+  kb_rhs_loop<<<(ncell + 127) / 128, 128>>>(ncell, dn, dT, dp, par_stride, reps, ds);
+  cudaEventRecord(e1);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess || ms <= 0.0f) return -104;
+  *rhs_per_s = (double)ncell * reps / (ms * 1e-3);
+  return 0;
 }
 
 // the FP64 pipe's peak, measured: independent DFMA chains in registers,

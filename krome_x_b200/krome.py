@@ -32,7 +32,7 @@ _ENUMS = {"jac": ("auto", "analytic", "fd"),
           "path": ("auto", "percell", "device"),
           "kernel": ("plain", "persistent")}
 STAT_NAMES = ("nst", "nfe", "nfeDQ", "nje", "nsetups", "nni", "nnf", "netf",
-              "restarts")
+              "restarts", "nlu64")
 LIBDIR = Path(__file__).resolve().parent / "lib"
 
 

@@ -73,7 +73,11 @@ def primordial3(ncell, info, seed=0):
     n[:, ix["H+"]] = xe * nH
     n[:, ix["e-"]] = xe * nH
     n[:, ix["He"]] = 0.0775 * nH
-    n[:, ix["H"]] = nH - 2.0 * n[:, ix["H2"]] - n[:, ix["H+"]]
+    # H = n_H - 2 n_H2 - n_H+, floored at the trace level: with x_H2 near
+    # 0.5 and a large ionisation fraction the difference is negative, an
+    # unphysical input whose clipping would break the nuclei balance
+    n[:, ix["H"]] = np.maximum(nH - 2.0 * n[:, ix["H2"]] - n[:, ix["H+"]],
+                               1e-20 * nH)
     par = _default_rows(ncell, info)
     tff = free_fall_time(n, mass_g)
     par[:, param_names.index("tff")] = tff

@@ -128,48 +128,53 @@ double max_norm_(int N, const double* x) {
   return mx;
 }
 
-// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457)
-int getrf_(double* a, int n, int* p) {
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457). R is
+// the factors' type: double, or float for the FP32 Newton-matrix form (the
+// factorisation's arithmetic in float; the solve's right-hand side and its
+// accumulation stay double)
+template <class R>
+int getrf_(R* a, int n, int* p) {
   for (int k = 0; k < n; k++) {
-    double* col_k = a + (long)k * n;
+    R* col_k = a + (long)k * n;
     int l = k;
     for (int i = k + 1; i < n; i++)
       if (std::fabs(col_k[i]) > std::fabs(col_k[l])) l = i;
     p[k] = l;
-    if (col_k[l] == 0.0) return k + 1;
+    if (col_k[l] == R(0)) return k + 1;
     if (l != k)
       for (int i = 0; i < n; i++) {
-        double* ci = a + (long)i * n;
-        const double t = ci[l];
+        R* ci = a + (long)i * n;
+        const R t = ci[l];
         ci[l] = ci[k];
         ci[k] = t;
       }
-    const double mult = 1.0 / col_k[k];
+    const R mult = R(1) / col_k[k];
     for (int i = k + 1; i < n; i++) col_k[i] *= mult;
     for (int j = k + 1; j < n; j++) {
-      double* col_j = a + (long)j * n;
-      const double a_kj = col_j[k];
-      if (a_kj != 0.0)
+      R* col_j = a + (long)j * n;
+      const R a_kj = col_j[k];
+      if (a_kj != R(0))
         for (int i = k + 1; i < n; i++) col_j[i] -= a_kj * col_k[i];
     }
   }
   return 0;
 }
-void getrs_(const double* a, int n, const int* p, double* b) {
+template <class R>
+void getrs_(const R* a, int n, const int* p, double* b) {
   for (int k = 0; k < n; k++) {
     const int pk = p[k];
     if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
   }
   for (int k = 0; k < n - 1; k++) {
-    const double* col_k = a + (long)k * n;
-    for (int i = k + 1; i < n; i++) b[i] -= col_k[i] * b[k];
+    const R* col_k = a + (long)k * n;
+    for (int i = k + 1; i < n; i++) b[i] -= (double)col_k[i] * b[k];
   }
   for (int k = n - 1; k > 0; k--) {
-    const double* col_k = a + (long)k * n;
-    b[k] /= col_k[k];
-    for (int i = 0; i < k; i++) b[i] -= col_k[i] * b[k];
+    const R* col_k = a + (long)k * n;
+    b[k] /= (double)col_k[k];
+    for (int i = 0; i < k; i++) b[i] -= (double)col_k[i] * b[k];
   }
-  b[0] /= a[0];
+  b[0] /= (double)a[0];
 }
 
 // ---- the per-cell problem (solve_cell.hpp:438-813, 883-1132) ------------
@@ -275,11 +280,11 @@ struct Problem {
 
 struct Stats {
   long nst = 0, nfe = 0, nfeDQ = 0, nje = 0, nsetups = 0, nni = 0, nnf = 0,
-       ncfn = 0, netf = 0;
+       ncfn = 0, netf = 0, nlu64 = 0;
   void add(const Stats& s) {
     nst += s.nst; nfe += s.nfe; nfeDQ += s.nfeDQ; nje += s.nje;
     nsetups += s.nsetups; nni += s.nni; nnf += s.nnf; ncfn += s.ncfn;
-    netf += s.netf;
+    netf += s.netf; nlu64 += s.nlu64;
   }
 };
 
@@ -291,6 +296,10 @@ struct BdfOpts {
   double h0 = 0.0;
   bool dq_jac = false;
   int inv_row = -1, inv_n = 0;
+  // the Newton matrix factored in FP32 (residuals, rhs, history and error
+  // test stay FP64), refactored in FP64 after a Newton failure until the
+  // next accepted step
+  bool lu32 = false;
 };
 
 // one cell's CVODE BDF (bdf_cell.hpp:490-1501), unit stride, dense LU
@@ -298,7 +307,8 @@ class Cvode {
  public:
   Stats st;
   Cvode(Problem& prob, int n, const BdfOpts& opts)
-      : P(prob), N(n), o(opts), work((L_MAX + 9) * n + 2 * n * n), piv(n) {
+      : P(prob), N(n), o(opts), work((L_MAX + 9) * n + 2 * n * n),
+        A32(opts.lu32 ? (long)n * n : 0), piv(n) {
     double* w = work.data();
     for (int j = 0; j < L_MAX; j++, w += N) zn[j] = w;
     ewt = w; w += N;
@@ -330,6 +340,7 @@ class Cvode {
     hin = h_init;
     nstlj = 0;
     acnrmcur = false; nls_jcur = false; jcur = false;
+    lu64 = false; fact32 = false;
     saved_tq5 = 0.0;
     for (int i = 0; i <= L_MAX; i++) tau[i] = 0.0;
     eta = 1.0;
@@ -400,7 +411,10 @@ class Cvode {
   const int N;
   const BdfOpts o;
   std::vector<double> work;
+  std::vector<float> A32;  // the FP32 factors (lu32)
   std::vector<int> piv;
+  bool lu64 = false;       // lu32: factor in FP64 until the next accepted step
+  bool fact32 = false;     // the current factors are A32's
   long mxstep;
   bool atolmin0;
   double* zn[L_MAX];
@@ -704,6 +718,8 @@ class Cvode {
         if (retval != SUCCESS) break;
       }
       if (retval == SUCCESS) break;
+      // a Newton failure with FP32 factors: FP64 from the next setup on
+      if (retval > 0 && fact32) lu64 = true;
       if ((retval > 0) && !nls_jcur) {
         nconvfails++;
         callSetup = true;
@@ -713,6 +729,7 @@ class Cvode {
       }
       break;
     }
+    if (retval > 0 && fact32) lu64 = true;
     if (retval != SUCCESS) nconvfails++;
     st.nni += niters;
     st.nnf += nconvfails;
@@ -793,10 +810,17 @@ class Cvode {
       nstlj = st.nst;
     }
     if (retval != 0) return retval;
+    fact32 = o.lu32 && !lu64;
+    if (fact32) {
+      for (long k = 0; k < NN; k++) A32[k] = (float)A[k];
+      return getrf_(A32.data(), N, piv.data()) > 0 ? LS_LUFACT_FAIL : 0;
+    }
+    if (o.lu32) st.nlu64++;
     return getrf_(A, N, piv.data()) > 0 ? LS_LUFACT_FAIL : 0;
   }
   int lsolve_(double* b) {
-    getrs_(A, N, piv.data(), b);
+    if (fact32) getrs_(A32.data(), N, piv.data(), b);
+    else getrs_(A, N, piv.data(), b);
     if (gamrat != 1.0) scale_(N, 2.0 / (1.0 + gamrat), b, b);
     return SUCCESS;
   }
@@ -887,6 +911,7 @@ class Cvode {
     return TRY_AGAIN;
   }
   void complete_step_() {
+    lu64 = false;
     st.nst++;
     nscon++;
     hu = h;
@@ -998,10 +1023,12 @@ struct oracle_opts {
   long max_steps;
   int max_err_fails, max_conv_fails, max_restarts;
   int clip_negative;
+  int lu32;     // the Newton matrix factored in FP32 (FP64 fallback)
 };
 
-// per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf, restarts
-constexpr int ORACLE_NSTAT = 9;
+// per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf,
+// restarts, nlu64 (FP64 refactors of the lu32 form)
+constexpr int ORACLE_NSTAT = 10;
 
 #define ORACLE_API __attribute__((visibility("default")))
 
@@ -1056,6 +1083,7 @@ ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, doub
   bo.max_err_fails = so->max_err_fails;
   bo.max_conv_fails = so->max_conv_fails;
   bo.dq_jac = jac == 2;
+  bo.lu32 = so->lu32 != 0;
   if (IDX_ELECTRON >= 0) {  // charge_newton_ (solve_cell.hpp:1631-1642)
     bo.inv_row = IDX_ELECTRON;
     bo.inv_n = NSPEC;
@@ -1082,7 +1110,7 @@ ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, doub
   if (stats != nullptr) {
     const long s[ORACLE_NSTAT] = {bs.nst, bs.nfe, bs.nfeDQ, bs.nje,
                                   bs.nsetups, bs.nni, bs.nnf, bs.netf,
-                                  (long)restarts};
+                                  (long)restarts, bs.nlu64};
     for (int i = 0; i < ORACLE_NSTAT; ++i) stats[i] = s[i];
   }
   if (flag == 0 && c.iT >= 0 && !(y[c.iT] > 0.0 && std::isfinite(y[c.iT])))

@@ -124,10 +124,11 @@ def test_python_binding_raises_before_the_call_on_missing_parameter():
 def test_unsupported_configurations_return_minus_104():
     net = krome.load("galaxy_ism")
     n = np.ones((2, net.nspec))
-    opts = net.options(linsol="sparse")
-    r = net.solve(n, 100.0, 1e5, opts=opts, check=False)
-    assert r.ierr == -104 and (r.flags == -104).all()
-    np.testing.assert_array_equal(r.n, n)
+    for o in (dict(linsol="sparse"), dict(lu32=1, layout=0)):
+        opts = net.options(**o)
+        r = net.solve(n, 100.0, 1e5, opts=opts, check=False)
+        assert r.ierr == -104 and (r.flags == -104).all(), o
+        np.testing.assert_array_equal(r.n, n)
 
 
 def test_solve_batch_requires_strict_shapes():

@@ -237,3 +237,50 @@ def test_full_size_batch_conserves_nuclei_and_charge():
     assert np.max(np.abs(He(r.n) / He(n) - 1.0)) < 1e-4
     assert np.max(np.abs(q(r.n)) / qabs(r.n)) < 1e-4
     assert (r.Tgas > 0).all() and np.isfinite(r.n).all()
+
+
+# ---- the FP32 Newton-matrix form (option lu32) ----
+# The LU of I - gamma J in FP32; residuals, rhs, Nordsieck history and the
+# error test in FP64; after a Newton failure with FP32 factors the matrix is
+# refactored in FP64 until the next accepted step (counter nlu64).
+
+@pytest.mark.parametrize("key", ["galaxy_ism", "primordial3"])
+def test_lu32_parity_with_oracle(key):
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](1024, info, seed=31)
+    ref = Oracle(key).solve(n, T, dt, par, lu32=1, **workloads.OPTIONS[key])
+    net = krome.load(key)
+    r = net.solve_batch(n, T, dt, par, opts=opts_for(net, key, lu32=1),
+                        check=False, stats=True)
+    m = parity(r.n, r.Tgas, r.flags, ref["n"], ref["T"], ref["flags"],
+               workloads.OPTIONS[key]["rtol"])
+    assert m["flags_equal"] == 1.0, m
+    assert m["frac"] >= FLOOR[key], m
+    assert m["max_rel"] < 1e-3 and m["max_relT"] < 1e-3, m
+    # the FP64 refactors: as many as the oracle's twin makes, up to the
+    # chaotic spread of the step sequence
+    g, c = int(r.stats[:, 9].sum()), int(ref["stats"][:, 9].sum())
+    assert c > 0 and abs(g - c) <= 0.25 * c + 5, (g, c)
+
+
+def test_lu32_error_against_tight_oracle():
+    """galaxy_ism: both forms against the rtol = 1e-12 FP64 oracle; the FP32
+    factorisation leaves the error of the FP64 form unchanged"""
+    key = "galaxy_ism"
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](1024, info, seed=33)
+    o = workloads.OPTIONS[key]
+    tight = Oracle(key).solve(n, T, dt, par,
+                              **dict(o, rtol=1e-12, max_steps=2000000))
+    net = krome.load(key)
+    res = {}
+    for lu32 in (0, 1):
+        r = net.solve_batch(n, T, dt, par, opts=opts_for(net, key, lu32=lu32),
+                            check=False, stats=True)
+        res[lu32] = parity(r.n, r.Tgas, r.flags, tight["n"], tight["T"],
+                           tight["flags"], o["rtol"])
+        if lu32 == 0:
+            assert (r.stats[:, 9] == 0).all()
+    assert res[1]["flags_equal"] == 1.0 and res[0]["flags_equal"] == 1.0
+    assert res[1]["frac"] >= res[0]["frac"] - 0.02, res
+    assert res[1]["max_rel"] < 1e-3, res

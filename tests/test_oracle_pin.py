@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import NETWORKS, ROOT, golden
+from conftest import NETWORKS, ROOT, golden, parity
 from krome_x_b200 import netinfo, workloads
 from oracle import Oracle, reference_solve
 
@@ -96,3 +96,25 @@ def test_oracle_nonpositive_dt_skipped():
     np.testing.assert_array_equal(out["n"][[1, 4]], n[[1, 4]])
     assert (out["stats"][[1, 4]] == 0).all()
     assert (out["stats"][[0, 2, 3, 5], 0] > 0).all()
+
+
+def test_oracle_lu32_form_keeps_the_fp64_error():
+    """the oracle's twin of the FP32 Newton-matrix form: against the
+    rtol = 1e-12 solve its error is the FP64 form's, and its FP64 refactor
+    fallback is exercised (nlu64 > 0) while the FP64 form never counts one"""
+    key = "galaxy_ism"
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](384, info, seed=41)
+    o = workloads.OPTIONS[key]
+    orc = Oracle(key)
+    tight = orc.solve(n, T, dt, par, **dict(o, rtol=1e-12, max_steps=2000000))
+    r64 = orc.solve(n, T, dt, par, **o)
+    r32 = orc.solve(n, T, dt, par, lu32=1, **o)
+    m64 = parity(r64["n"], r64["T"], r64["flags"], tight["n"], tight["T"],
+                 tight["flags"], o["rtol"])
+    m32 = parity(r32["n"], r32["T"], r32["flags"], tight["n"], tight["T"],
+                 tight["flags"], o["rtol"])
+    assert m32["flags_equal"] == 1.0 and m64["flags_equal"] == 1.0
+    assert m32["frac"] >= m64["frac"] - 0.02, (m32, m64)
+    assert r32["stats"][:, 9].sum() > 0
+    assert (r64["stats"][:, 9] == 0).all()
