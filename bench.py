@@ -43,8 +43,7 @@ sys.path.insert(0, str(ROOT))
 
 NETWORK = "primordial3"
 RTOL = 1e-6
-STAT_NAMES = ("nst", "nfe", "nfeDQ", "nje", "nsetups", "nni", "nnf", "netf",
-              "restarts")
+from krome_x_b200.krome import STAT_NAMES  # the per-cell counters' columns
 
 
 def parse():

@@ -137,6 +137,50 @@ void* krome_b200_graph_new(int ncell, double* n, double* Tgas, double* dt,
 int krome_b200_graph_launch(void* graph, void* stream);
 void krome_b200_graph_free(void* graph);
 
+/* ---- the discrete adjoint (no counterpart in the reference, whose only
+ * rate scaling is a global factor) ----
+ * The solve of krome_b200_solve_batch with every rate coefficient k_r of
+ * cell c multiplied by exp(lnm[c][r]), and the gradient of
+ * sum(gn * n_out) + sum(gT * Tgas_out) with respect to the initial n
+ * (dn0[ncell][nspec]), Tgas (dT0[ncell], evolve_T) and lnm
+ * (dm[ncell][nrea], per cell). The gradient is that of the discrete
+ * solution: the forward solve's step sizes, orders and Newton decisions are
+ * held fixed, each accepted step's corrector is differentiated at its root
+ * with dF/dy re-evaluated at the accepted state. lnm: one row of nrea
+ * (lnm_stride 0) or rows (nrea), NULL for none. tape_cap: doubles of tape
+ * per cell (0: 32768); a cell whose tape outgrows it returns -120 untouched.
+ * Failed cells get zero gradients. Host arrays; the device buffers (the
+ * tapes: ncell * tape_cap * 8 bytes) are allocated per call. Returns 0 or
+ * the lowest-index failing cell's flag. */
+int krome_b200_adjoint(int ncell, double* n, double* Tgas, const double* dt,
+                       const double* par, int par_stride, const double* lnm,
+                       int lnm_stride, const double* gn, const double* gT,
+                       int* flags, double* dn0, double* dT0, double* dm,
+                       long tape_cap, const krome_opts* h);
+
+/* the adjoint's two halves on device arrays, asynchronous on `stream`:
+ * the recording forward solve (mult = exp(lnm), rows [ncell][nrea] with
+ * mult_stride nrea or one row with 0, NULL for none; tape[ncell][tape_cap];
+ * tape_len[ncell] and yfin[ncell][neq] written for the reverse sweep;
+ * n, Tgas updated in place as by krome_b200_solve_device) ... */
+int krome_b200_adjoint_record_device(int ncell, double* n, double* Tgas,
+                                     const double* dt, const double* par,
+                                     int par_stride, const double* mult,
+                                     int mult_stride, int* flags, long* stats,
+                                     unsigned* cursor, double* tape,
+                                     long tape_cap, long* tape_len,
+                                     double* yfin, const krome_opts* h,
+                                     void* stream);
+/* ... and the reverse sweep over those tapes (T0: the initial Tgas) */
+int krome_b200_adjoint_device(int ncell, const double* T0, const double* par,
+                              int par_stride, const double* mult,
+                              int mult_stride, const double* gn,
+                              const double* gT, const int* flags,
+                              const double* tape, long tape_cap,
+                              const long* tape_len, const double* yfin,
+                              double* dn0, double* dT0, double* dm,
+                              const krome_opts* h, void* stream);
+
 /* krome_solve_cells for callers that cannot let the library allocate device
  * memory -- a code that gives the whole GPU to its own memory pool, or a
  * time step that must not pay cudaMalloc's device-wide synchronization.

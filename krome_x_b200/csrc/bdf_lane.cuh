@@ -74,6 +74,24 @@ enum : int {
   PH_IDLE            // no cell left for this lane
 };
 
+// the discrete adjoint's tape: every operation of the forward solve that
+// changes the Nordsieck array zn, in order, one record each
+// [op, payload..., record length]; the records and their payloads are the
+// oracle's (oracle/bdf_oracle.cpp, TapeOp)
+enum : int {
+  TP_INIT = 1,   // zn[0] = y0, zn[1] = h f(y0):            h, y0[N]
+  TP_RESCALE,    // zn[j] *= eta^j, j = 1..q:                eta, q
+  TP_INCREASE,   // zn[L] = A1 zn[QMAX]; zn[j] += l_j zn[L]:  q, A1, l[0..5]
+  TP_DECREASE,   // zn[j] -= l_j zn[q], j = 2..q-1:          q, l[0..5]
+  TP_PREDICT,    // zn[j-1] += zn[j] (Pascal):               q
+  TP_RESTORE,    // zn[j-1] -= zn[j] (Pascal):               q
+  TP_RESET1,     // zn[1] = h f(zn[0]):                      h, y[N]
+  TP_CORRECT,    // zn[j] += l_j acor (+ zn[QMAX] = acor) with
+                 // acor = gamma f(zn0 + acor) - rl1 zn1:   q, gamma, rl1,
+                 //                                           l[0..5], save, y_n[N]
+  TP_DKY         // y = sum_j s^j zn[j]:                     s, q
+};
+
 template <int N>
 struct LaneCell {
   // ---- the cell ----
@@ -128,15 +146,22 @@ struct LaneCell {
   double tol;
   // ls_setup
   int ls_retval;
+  // the adjoint's tape (recording kernels): this cell's region, its
+  // capacity and length in doubles (-1: the capacity was exceeded)
+  double* tp;
+  long tcap, tlen;
+  bool qmax_saved;
 };
 
 // Code size. The control code of the sweep runs on a few lanes at a time
 // and is not where the time goes, but every instruction of it competes with
 // the rhs for the instruction cache; these switches keep it compact: the
-// vector loops rolled (KBL_LOOP), the vector and step helpers out of line
-// (KBL_HELPER, KBL_VEC), the sweep one function (KBL_SWEEP).
+// control loops rolled (KBL_LOOP, on by default: the primordial3 hydro calls
+// run 12% faster than with the loops unrolled), the vector and step helpers
+// out of line (KBL_HELPER, KBL_VEC) and the sweep one function (KBL_SWEEP),
+// both off by default (the calls cost more than the code they save).
 #ifndef KBL_LOOP
-#define KBL_LOOP
+#define KBL_LOOP _Pragma("unroll 1")
 #endif
 #ifndef KBL_VEC
 #define KBL_VEC __forceinline__
@@ -266,43 +291,88 @@ __device__ KBL_HELPER void getrs_(const R* a, const int* p, double* b) {
   b[0] /= (double)a[0];
 }
 
-template <int N, bool EVT>
+template <int N, bool EVT, bool REC = false>
 struct Machine {
   LaneCell<N>& s;
   const SolveOpts& o;
   __device__ Machine(LaneCell<N>& s_, const SolveOpts& o_) : s(s_), o(o_) {}
 
+  // one tape record (REC only): [op, a (na >= 1), b (na == 2), l[] (with_l),
+  // v[N] (v non-null), length]
+  __device__ void rec_(int op, int na, double a, double b, bool with_l,
+                       const double* v) {
+    if constexpr (REC) {
+      if (s.tp == nullptr || s.tlen < 0) return;
+      const long len = 2 + na + (with_l ? L_MAX : 0) + (v != nullptr ? N : 0);
+      if (s.tlen + len > s.tcap) {
+        s.tlen = -1;
+        return;
+      }
+      double* t = s.tp + s.tlen;
+      int w = 0;
+      t[w++] = op;
+      if (na >= 1) t[w++] = a;
+      if (na >= 2) t[w++] = b;
+      if (with_l) KBL_LOOP for (int i = 0; i < L_MAX; i++) t[w++] = s.l[i];
+      if (v != nullptr) KBL_LOOP for (int i = 0; i < N; i++) t[w++] = v[i];
+      t[w++] = (double)len;
+      s.tlen += len;
+    }
+  }
+  // the accepted step's corrector record
+  __device__ void rec_correct_(int q) {
+    if constexpr (REC) {
+      if (s.tp == nullptr || s.tlen < 0) return;
+      const long len = 6 + L_MAX + N;
+      if (s.tlen + len > s.tcap) {
+        s.tlen = -1;
+        return;
+      }
+      double* t = s.tp + s.tlen;
+      int w = 0;
+      t[w++] = TP_CORRECT;
+      t[w++] = q;
+      t[w++] = s.gamma;
+      t[w++] = s.rl1;
+      KBL_LOOP for (int i = 0; i < L_MAX; i++) t[w++] = s.l[i];
+      t[w++] = s.qmax_saved ? 1.0 : 0.0;
+      KBL_LOOP for (int i = 0; i < N; i++) t[w++] = s.y[i];
+      t[w++] = (double)len;
+      s.tlen += len;
+    }
+  }
+
   __device__ KBL_HELPER int ewt_set(const double* ycur, double* w) {
-    for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
-    for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
+    KBL_LOOP for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
+    KBL_LOOP for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
     if (s.atolmin0) {
       double mn = w[0];
-      for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
+      KBL_LOOP for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
       if (mn <= 0.0) return -1;
     }
-    for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
+    KBL_LOOP for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
     return 0;
   }
 
   __device__ KBL_HELPER void reinit(double t0, const double* y0, double h_init) {
     s.tn = t0;
-    for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
+    KBL_LOOP for (int i = 0; i < N; i++) s.zn[0][i] = y0[i];
     s.q = 1; s.L = 2; s.qwait = s.L;
     s.etamax = ETA_MAX_FS;
     s.qu = 0; s.hu = 0.0; s.tolsf = 1.0;
-    for (int i = 0; i < NSTAT; ++i) s.st[i] = 0;
+    KBL_LOOP for (int i = 0; i < NSTAT; ++i) s.st[i] = 0;
     s.nstlp = 0; s.nscon = 0; s.next_h = 0.0; s.next_q = 0;
     s.hin = h_init;
     s.nstlj = 0;
     s.acnrmcur = false; s.nls_jcur = false; s.jcur = false;
     s.lu64 = false; s.fact32 = false;
     s.saved_tq5 = 0.0;
-    for (int i = 0; i <= L_MAX; i++) s.tau[i] = 0.0;
+    KBL_LOOP for (int i = 0; i <= L_MAX; i++) s.tau[i] = 0.0;
     s.eta = 1.0;
   }
 
   __device__ __forceinline__ void request_rhs(const double* yv, int ph) {
-    for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
+    KBL_LOOP for (int i = 0; i < N; i++) s.yreq[i] = yv[i];
     s.ph = ph;
     s.wait = WAIT_RHS;
   }
@@ -315,8 +385,9 @@ struct Machine {
 
   // ---- step helpers (bdf_cell.hpp:825-954, 1386-1500) ----
   __device__ KBL_HELPER void rescale_() {
+    rec_(TP_RESCALE, 2, s.eta, s.q, false, nullptr);
     double c = s.eta;
-    for (int j = 1; j <= s.q; j++) {
+    KBL_LOOP for (int j = 1; j <= s.q; j++) {
       scale_<N>(c, s.zn[j], s.zn[j]);
       c = s.eta * c;
     }
@@ -326,7 +397,7 @@ struct Machine {
     s.nscon = 0;
   }
   __device__ KBL_HELPER void increase_bdf_() {
-    for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
+    KBL_LOOP for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
     double alpha1, prod, xiold, alpha0;
     s.l[2] = alpha1 = prod = xiold = 1.0;
     alpha0 = -1.0;
@@ -338,25 +409,29 @@ struct Machine {
         prod *= xi;
         alpha0 -= 1.0 / (j + 1);
         alpha1 += 1.0 / xi;
-        for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xiold + s.l[i - 1];
+        KBL_LOOP for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xiold + s.l[i - 1];
         xiold = xi;
       }
     const double A1 = (-alpha0 - alpha1) / prod;
     scale_<N>(A1, s.zn[QMAX], s.zn[s.L]);
-    if (s.q > 1)
-      for (int j = 2; j <= s.q; j++) axpy_<N>(s.l[j], s.zn[s.L], s.zn[j]);
+    if (s.q > 1) {
+      KBL_LOOP for (int j = 2; j <= s.q; j++) axpy_<N>(s.l[j], s.zn[s.L], s.zn[j]);
+    }
+    rec_(TP_INCREASE, 2, s.q, A1, true, nullptr);
   }
   __device__ KBL_HELPER void decrease_bdf_() {
-    for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
+    KBL_LOOP for (int i = 0; i <= QMAX; i++) s.l[i] = 0.0;
     s.l[2] = 1.0;
     double hsum = 0.0;
-    for (int j = 1; j <= s.q - 2; j++) {
+    KBL_LOOP for (int j = 1; j <= s.q - 2; j++) {
       hsum += s.tau[j];
       const double xi = hsum / s.hscale;
-      for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xi + s.l[i - 1];
+      KBL_LOOP for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xi + s.l[i - 1];
     }
-    if (s.q > 2)
-      for (int j = 2; j < s.q; j++) axpy_<N>(-s.l[j], s.zn[s.q], s.zn[j]);
+    if (s.q > 2) {
+      KBL_LOOP for (int j = 2; j < s.q; j++) axpy_<N>(-s.l[j], s.zn[s.q], s.zn[j]);
+      rec_(TP_DECREASE, 1, s.q, 0.0, true, nullptr);
+    }
   }
   __device__ KBL_HELPER void adjust_order_(int deltaq) {
     if ((s.q == 2) && (deltaq != 1)) return;
@@ -364,35 +439,37 @@ struct Machine {
     else if (deltaq == -1) decrease_bdf_();
   }
   __device__ KBL_HELPER void predict_() {
+    rec_(TP_PREDICT, 1, s.q, 0.0, false, nullptr);
     s.tn += s.h;
-    for (int k = 1; k <= s.q; k++)
+    KBL_LOOP for (int k = 1; k <= s.q; k++)
       for (int j = s.q; j >= k; j--) axpy_<N>(1.0, s.zn[j], s.zn[j - 1]);
   }
   __device__ KBL_HELPER void restore_(double saved_t) {
+    rec_(TP_RESTORE, 1, s.q, 0.0, false, nullptr);
     s.tn = saved_t;
-    for (int k = 1; k <= s.q; k++)
+    KBL_LOOP for (int k = 1; k <= s.q; k++)
       for (int j = s.q; j >= k; j--) axpy_<N>(-1.0, s.zn[j], s.zn[j - 1]);
   }
   __device__ KBL_HELPER void set_() {
     double xi_inv, xistar_inv, alpha0, alpha0_hat;
     s.l[0] = s.l[1] = xi_inv = xistar_inv = 1.0;
-    for (int i = 2; i <= s.q; i++) s.l[i] = 0.0;
+    KBL_LOOP for (int i = 2; i <= s.q; i++) s.l[i] = 0.0;
     alpha0 = alpha0_hat = -1.0;
     double hsum = s.h;
     const int q = s.q;
     if (q > 1) {
-      for (int j = 2; j < q; j++) {
+      KBL_LOOP for (int j = 2; j < q; j++) {
         hsum += s.tau[j - 1];
         xi_inv = s.h / hsum;
         alpha0 -= 1.0 / j;
-        for (int i = j; i >= 1; i--) s.l[i] += s.l[i - 1] * xi_inv;
+        KBL_LOOP for (int i = j; i >= 1; i--) s.l[i] += s.l[i - 1] * xi_inv;
       }
       alpha0 -= 1.0 / q;
       xistar_inv = -s.l[1] - alpha0;
       hsum += s.tau[q - 1];
       xi_inv = s.h / hsum;
       alpha0_hat = -s.l[1] - xi_inv;
-      for (int i = q; i >= 1; i--) s.l[i] += s.l[i - 1] * xistar_inv;
+      KBL_LOOP for (int i = q; i >= 1; i--) s.l[i] += s.l[i - 1] * xistar_inv;
     }
     const double A1 = 1.0 - alpha0_hat + alpha0;
     const double A2 = 1.0 + q * A1;
@@ -427,13 +504,14 @@ struct Machine {
     s.nscon++;
     s.hu = s.h;
     s.qu = s.q;
-    for (int i = s.q; i >= 2; i--) s.tau[i] = s.tau[i - 1];
+    KBL_LOOP for (int i = s.q; i >= 2; i--) s.tau[i] = s.tau[i - 1];
     if ((s.q == 1) && (s.st[ST_NST] > 1)) s.tau[2] = s.tau[1];
     s.tau[1] = s.h;
-    for (int j = 0; j <= s.q; j++) axpy_<N>(s.l[j], s.acor, s.zn[j]);
+    KBL_LOOP for (int j = 0; j <= s.q; j++) axpy_<N>(s.l[j], s.acor, s.zn[j]);
     s.qwait--;
     if ((s.qwait == 1) && (s.q != QMAX)) {
-      for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      KBL_LOOP for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      if constexpr (REC) s.qmax_saved = true;
       s.saved_tq5 = s.tq[5];
     }
   }
@@ -473,7 +551,7 @@ struct Machine {
     if (s.q != QMAX && s.saved_tq5 != 0.0) {
       const double rr = s.h / s.tau[2];
       double prod = 1.0;
-      for (int i = 1; i <= s.L; i++) prod *= rr;
+      KBL_LOOP for (int i = 1; i <= s.L; i++) prod *= rr;
       const double cquot = (s.tq[5] / s.saved_tq5) * prod;
       lin_sum_<N>(-cquot, s.zn[QMAX], 1.0, s.acor, s.tempv);
       const double dup = wrms_<N>(s.tempv, s.ewt) * s.tq[3];
@@ -492,15 +570,16 @@ struct Machine {
     } else {
       s.eta = s.etaqp1;
       s.qprime = s.q + 1;
-      for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      KBL_LOOP for (int i = 0; i < N; i++) s.zn[QMAX][i] = s.acor[i];
+      if constexpr (REC) s.qmax_saved = true;
     }
     set_eta_();
   }
   __device__ KBL_HELPER void get_dky_(double t, double* dky) {
     const double sv = (t - s.tn) / s.h;
-    for (int j = s.q; j >= 0; j--) {
+    KBL_LOOP for (int j = s.q; j >= 0; j--) {
       double c = 1.0;
-      for (int i = 0; i < j; i++) c *= sv;
+      KBL_LOOP for (int i = 0; i < j; i++) c *= sv;
       if (j == s.q) scale_<N>(c, s.zn[j], dky);
       else axpy_<N>(c, s.zn[j], dky);
     }
@@ -539,7 +618,7 @@ struct Machine {
     const double c = -s.gamma;
     s.fact32 = o.lu32 && !s.lu64;
     if (s.fact32) {
-      for (int j = 0; j < N; j++)
+      KBL_LOOP for (int j = 0; j < N; j++)
         for (int i = 0; i < N; i++) {
           const int k = i + j * N;
           double a = s.savedJ[k] * c;
@@ -548,8 +627,8 @@ struct Machine {
         }
       return getrf_<N, float>(s.A32, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
     }
-    for (int j = 0; j < N; j++) {
-      for (int i = 0; i < N; i++) {
+    KBL_LOOP for (int j = 0; j < N; j++) {
+      KBL_LOOP for (int i = 0; i < N; i++) {
         const int k = i + j * N;
         s.A[k] = s.savedJ[k] * c;
       }
@@ -661,7 +740,7 @@ struct Machine {
         s.nconvfails++;
         s.callSetup = true;
         s.jbad = true;
-        for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+        KBL_LOOP for (int i = 0; i < N; i++) s.acor[i] = 0.0;
         s.ph = PH_NLS_OUTER;
       } else {
         s.ph = PH_NLS_END;
@@ -743,26 +822,31 @@ struct Machine {
       }
     }
     if (s.ph == PH_ERRTEST_RHS) {
-      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      KBL_LOOP for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
       s.st[ST_NFE]++;
       if (s.rhs_ret > 0) {
         fail_solve(UNREC_RHSFUNC_ERR);
       } else {
         scale_<N>(s.h, s.tempv, s.zn[1]);
+        rec_(TP_RESET1, 1, s.h, 0.0, false, s.zn[0]);
         s.ph = PH_ATTEMPT;
       }
     }
     // ---- the accepted step and CVode's tout test (bdf_cell.hpp:620-636,
     //      1386-1500) ----
     if (s.ph == PH_STEP_OK) {
+      if constexpr (REC) s.qmax_saved = false;
+      const int q_step = s.q;
       complete_step_();
       prepare_next_step_(s.dsm);
+      rec_correct_(q_step);  // y holds zn[0] + acor of the accepted attempt
       s.etamax = (s.st[ST_NST] <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
       scale_<N>(s.tq[2], s.acor, s.acor);
       s.nstloc++;
       if ((s.tn - s.dt) * s.h >= 0.0) {
         s.tret = s.dt;
         get_dky_(s.dt, s.y);  // y(tout) into y
+        rec_(TP_DKY, 2, (s.dt - s.tn) / s.h, s.q, false, nullptr);
         s.next_q = s.qprime;
         s.next_h = s.hprime;
         s.retval = SUCCESS;
@@ -780,7 +864,7 @@ struct Machine {
       const int r = s.retval;
       if (r < 0)
         for (int i = 0; i < N; i++) s.y[i] = s.zn[0][i];
-      for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
+      KBL_LOOP for (int i = 0; i < NSTAT; ++i) s.tot[i] += s.st[i];
       const bool restartable = r == ERR_FAILURE || r == CONV_FAILURE
                                || r == REPTD_RHSFUNC_ERR;
       if (r >= 0 || !restartable || s.restarts >= o.max_restarts) {
@@ -811,7 +895,7 @@ struct Machine {
       return;
     }
     if (s.ph == PH_FIRST_RHS) {
-      for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
+      KBL_LOOP for (int i = 0; i < N; i++) s.zn[1][i] = s.freq[i];
       s.st[ST_NFE]++;
       if (s.rhs_ret > 0) {
         fail_solve(FIRST_RHSFUNC_ERR);
@@ -835,14 +919,14 @@ struct Machine {
       {  // cvUpperBoundH0
         double* temp1 = s.tempv;
         double* temp2 = s.acor;
-        for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[0][i]);
+        KBL_LOOP for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[0][i]);
         ewt_set(s.zn[0], temp1);
-        for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
+        KBL_LOOP for (int i = 0; i < N; i++) temp1[i] = 1.0 / temp1[i];
         lin_sum_<N>(HUB_FACTOR, temp2, 1.0, temp1, temp1);
-        for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[1][i]);
-        for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
+        KBL_LOOP for (int i = 0; i < N; i++) temp2[i] = fabs(s.zn[1][i]);
+        KBL_LOOP for (int i = 0; i < N; i++) temp1[i] = temp2[i] / temp1[i];
         double hub_inv = 0.0;
-        for (int i = 0; i < N; i++)
+        KBL_LOOP for (int i = 0; i < N; i++)
           if (fabs(temp1[i]) > hub_inv) hub_inv = fabs(temp1[i]);
         double hub = HUB_FACTOR * tdist;
         if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
@@ -861,7 +945,7 @@ struct Machine {
       }
     }
     if (s.ph == PH_HIN_RHS) {
-      for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
+      KBL_LOOP for (int i = 0; i < N; i++) s.tempv[i] = s.freq[i];
       s.st[ST_NFE]++;
       bool done = false;
       if (s.rhs_ret == 0) {
@@ -914,6 +998,7 @@ struct Machine {
       s.hscale = s.h;
       s.hprime = s.h;
       scale_<N>(s.h, s.zn[1], s.zn[1]);
+      rec_(TP_INIT, 1, s.h, 0.0, false, s.zn[0]);
       s.nstloc = 0;
       s.ph = PH_STEP;
     }
@@ -964,7 +1049,7 @@ struct Machine {
       s.callSetup = (s.nflag == PREV_CONV_FAIL) || (s.nflag == PREV_ERR_FAIL)
                     || (s.st[ST_NST] == 0) || (s.st[ST_NST] >= s.nstlp + MSBP)
                     || (fabs(s.gamrat - 1.0) > DGMAX_LSETUP);
-      for (int i = 0; i < N; i++) s.acor[i] = 0.0;
+      KBL_LOOP for (int i = 0; i < N; i++) s.acor[i] = 0.0;
       s.tol = s.tq[4];
       s.jbad = false;
       s.niters = 0;
@@ -980,7 +1065,7 @@ struct Machine {
 
   // cvNlsResidual's tail after its rhs (bdf_cell.hpp:1022-1032)
   __device__ KBL_HELPER int residual_done_() {
-    for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
+    KBL_LOOP for (int i = 0; i < N; i++) s.ftemp[i] = s.freq[i];
     s.st[ST_NFE]++;
     if (s.rhs_ret > 0) return RHSFUNC_RECVR;
     lin_sum_<N>(s.rl1, s.zn[1], 1.0, s.acor, s.delta);

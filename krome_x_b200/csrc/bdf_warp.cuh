@@ -51,7 +51,8 @@ enum : int {
   CONV_FAILURE = -4, LSETUP_FAIL = -6, LSOLVE_FAIL = -7, RHSFUNC_FAIL = -8,
   FIRST_RHSFUNC_ERR = -9, REPTD_RHSFUNC_ERR = -10, UNREC_RHSFUNC_ERR = -11,
   NLS_FAIL = -16, ILL_INPUT = -22, TOO_CLOSE = -27,
-  FLAG_PARAM_UNSET = -105, FLAG_NONPOSITIVE_T = -110
+  FLAG_PARAM_UNSET = -105, FLAG_NONPOSITIVE_T = -110,
+  FLAG_TAPE_FULL = -120  // the adjoint's tape outgrew its capacity
 };
 enum : int {
   DO_ERROR_TEST = 2, PREDICT_AGAIN = 3, TRY_AGAIN = 5, FIRST_CALL = 6,
@@ -116,17 +117,24 @@ __device__ __forceinline__ bool warp_any(bool b) { return __any_sync(FULL, b); }
 // the network's rhs of one full state (every lane its own), the
 // reference's full_rhs_ (solve_cell.hpp:750-789) with eval_rates_ and the
 // thermal row aux_ (rates at state_T_ = clamp(T, Tcmb, 1e9), thermal
-// terms at thermal_T_ = clamp(T, 2.73, 1e9)); k: NREA scratch
+// terms at thermal_T_ = clamp(T, 2.73, 1e9)); k: NREA scratch; mrow: the
+// per-reaction rate factors exp(m_r) of the adjoint's ln-multipliers, null
+// for none
 template <int N, bool EVT>
 __device__ __forceinline__ void full_rhs(const double (&yf)[N], double (&f)[N],
                                          const Params& p, double Tfix,
-                                         double (&k)[NREA + 1]) {
+                                         double (&k)[NREA + 1],
+                                         const double* mrow = nullptr) {
   const double T0 = EVT ? yf[N - 1] : Tfix;
   const double T = fmin(fmax(T0, p.Tcmb), 1e9);
   KB_UNROLL
   for (int i = 0; i <= NREA; ++i) k[i] = 0.0;
   rates_fixed(T, yf, p, k);
   rates_var(T, yf, p, k);
+  if (mrow != nullptr) {
+    KB_UNROLL
+    for (int i = 0; i < NREA; ++i) k[i] *= mrow[i];
+  }
   rhs(yf, k, f);
   if (EVT) {
     const double Tth = fmin(fmax(yf[N - 1], 2.73), 1e9);

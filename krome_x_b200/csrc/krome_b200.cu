@@ -29,6 +29,7 @@
 #include KB_NET_HEADER
 #include "bdf_warp.cuh"
 #include "bdf_lane.cuh"
+#include "adjoint.cuh"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
 
@@ -122,20 +123,33 @@ struct LaneGeo {
   static constexpr int SMEM_DOUBLES = MAXJ * (N * N + 2 * N);
 };
 
+// the adjoint's forward solve (kb_lane_cells with REC): the rate factors
+// exp(m) and where each cell's tape goes
+struct RecIO {
+  const double* mult;  // [ncell][NREA] (mstride NREA) or one row (0); null: 1
+  int mstride;
+  double* tape;        // [ncell][cap] doubles
+  long cap;
+  long* tlen;          // per cell: its tape's length; 0 not integrated
+  double* yfin;        // [ncell][N]: the final y before the post-solve rules
+};
+
 // start cell c on this lane: false when the cell needs no integration
 // (its flag is written here)
-template <bool EVT>
+template <bool EVT, bool REC>
 __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
-                           kbl::Machine<LaneGeo<EVT>::N, EVT>& m, int c,
+                           kbl::Machine<LaneGeo<EVT>::N, EVT, REC>& m, int c,
                            const double* n, const double* T, const double* dt,
                            const double* par, int pstride, int* flags,
-                           long* stats, const SolveOpts& so) {
+                           long* stats, const SolveOpts& so,
+                           const RecIO& rio) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   const double dtc = dt[c];
   int skip_flag = 1;
   if (so.fail_every > 0 && (c + 1) % so.fail_every == 0) skip_flag = kbw::TOO_MUCH_WORK;
   else if (!(dtc > 0.0)) skip_flag = 0;
+  if constexpr (REC) rio.tlen[c] = 0;
   if (skip_flag != 1) {
     if (flags != nullptr) flags[c] = skip_flag;
     if (stats != nullptr)
@@ -146,6 +160,11 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   if (params_missing(s.p) >= 0) {
     if (flags != nullptr) flags[c] = kbw::FLAG_PARAM_UNSET;
     return false;
+  }
+  if constexpr (REC) {
+    s.tp = rio.tape + (long)c * rio.cap;
+    s.tcap = rio.cap;
+    s.tlen = 0;
   }
   s.cell = c;
   s.dt = dtc;
@@ -168,13 +187,19 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
 
 // the post-solve rules of solve() (solve_cell.hpp:2156-2176) and the
 // write-back of a finished cell
-template <bool EVT>
+template <bool EVT, bool REC>
 __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
                             double* n, double* T, int* flags, long* stats,
-                            const SolveOpts& so) {
+                            const SolveOpts& so, const RecIO& rio) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   const int c = s.cell;
+  if constexpr (REC) {
+    // a tape that outgrew its capacity: no gradient, the cell untouched
+    if (flag == 0 && s.tlen < 0) flag = kbw::FLAG_TAPE_FULL;
+    rio.tlen[c] = s.tlen;
+    KBL_LOOP for (int i = 0; i < N; ++i) rio.yfin[(long)c * N + i] = s.y[i];
+  }
   s.tot[kbw::ST_RESTARTS] = s.restarts;
   if (stats != nullptr)
     for (int i = 0; i < NSTAT; ++i) stats[(long)c * NSTAT + i] = s.tot[i];
@@ -209,11 +234,14 @@ __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
 // where request r of the pass occupies lanes [r*JL, (r+1)*JL) (JL the lanes
 // one Jacobian needs) and lane r*JL + j evaluates its column / term j; the
 // assembled Jacobians go through shared memory to the requesting lanes.
-template <bool EVT, int MINB>
+//
+// REC (the adjoint's forward solve): the rates multiplied by the cells'
+// factors exp(m) and every zn operation recorded on the cell's tape.
+template <bool EVT, int MINB, bool REC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
 kb_lane_cells(int ncell, double* n, double* T, const double* dt,
               const double* par, int pstride, int* flags, long* stats,
-              SolveOpts so, unsigned* cursor, int persistent) {
+              SolveOpts so, unsigned* cursor, int persistent, RecIO rio) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   constexpr unsigned FULLM = 0xffffffffu;
@@ -222,7 +250,8 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
   const int lane = threadIdx.x & 31;
   double* sw = smem + warp * LaneGeo<EVT>::SMEM_DOUBLES;
   kbl::LaneCell<N> s;
-  kbl::Machine<N, EVT> m(s, so);
+  kbl::Machine<N, EVT, REC> m(s, so);
+  s.tp = nullptr;
   s.cell = -1;
   s.ph = kbl::PH_DONE;  // take a first cell
   s.wait = kbl::WAIT_NONE;
@@ -237,7 +266,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
     for (int sweep = 0; sweep < 2; ++sweep) {
       // bounded: every iteration consumes a cell index (at most ncell)
       while (s.ph == kbl::PH_DONE) {
-        if (s.cell >= 0) lane_finish<EVT>(s, s.flag, n, T, flags, stats, so);
+        if (s.cell >= 0) lane_finish<EVT, REC>(s, s.flag, n, T, flags, stats, so, rio);
         int c;
         if (persistent) {
           c = (int)atomicAdd(cursor, 1u);
@@ -246,7 +275,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
           static_taken = true;
         }
         if (c >= ncell) s.ph = kbl::PH_IDLE;
-        else lane_start<EVT>(s, m, c, n, T, dt, par, pstride, flags, stats, so);
+        else lane_start<EVT, REC>(s, m, c, n, T, dt, par, pstride, flags, stats, so, rio);
       }
       if (s.ph != kbl::PH_IDLE) m.sweep();
       if (!__any_sync(FULLM, s.ph == kbl::PH_DONE)) break;
@@ -282,6 +311,11 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
       double yf[N], f[N], k[NREA + 1];
       Params p;
       double Tfix, inc = 1.0, hT = 1.0;
+      const double* mrow = nullptr;  // REC: the evaluated cell's exp(m)
+      if constexpr (REC) {
+        const int ec = __shfl_sync(FULLM, s.cell, src);
+        if (rio.mult != nullptr && ec >= 0) mrow = rio.mult + (long)ec * rio.mstride;
+      }
       if (pass == 0) {
         KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = s.yreq[i];
         p = s.p;
@@ -332,7 +366,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
       bool hit = false;
       int r = 0;
       if (active) {
-        kbw::full_rhs<N, EVT>(yf, f, p, Tfix, k);
+        kbw::full_rhs<N, EVT>(yf, f, p, Tfix, k, mrow);
         // the integrator's checks (rhs_host_, solve_cell.hpp:794-813): a
         // trial Tgas <= 0 or a non-finite f is a recoverable failure; the
         // hybrid Jacobian's terms are plain full_rhs_ evaluations
@@ -400,10 +434,10 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
         const unsigned mbad = bad & (((JL >= 32) ? FULLM : ((1u << JL) - 1u)) << base);
         const int fb = mbad ? (__ffs(mbad) - 1 - base) : N;
         if (!dq) {
-          for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
+          KBL_LOOP for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
           s.ls_retval = 0;
         } else {
-          for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
+          KBL_LOOP for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
           s.ls_retval = mbad ? 1 : 0;
           s.st[kbw::ST_NFEDQ] += mbad ? fb + 1 : N;
         }
@@ -432,7 +466,7 @@ struct krome_opts {
   // this library's keys
   int kernel = 1;          // 0 plain, 1 persistent work queue
   int layout = 1;          // 0 one warp per cell, 1 one lane per cell
-  int lane_minb = 3;       // lane kernel: resident blocks per SM it is
+  int lane_minb = 2;       // lane kernel: resident blocks per SM it is
                            // compiled for (2, 3, 4: the register budget)
   int queue_chunk = 1;     // cells per queue pop
   int blocks_per_sm = 0;   // persistent grid: 0 = occupancy limit
@@ -504,16 +538,18 @@ template <bool EVT>
 cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    const double* dt, const double* par, int pstride,
                    int* flags, long* stats, unsigned* cursor,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, const RecIO* rio = nullptr) {
   const SolveOpts so = to_solve_opts(h);
-  if (h.layout == 1) {  // lane per cell
+  if (h.layout == 1 || rio != nullptr) {  // lane per cell
     const size_t lsmem =
         sizeof(double) * kWarpsPerBlock * LaneGeo<EVT>::SMEM_DOUBLES;
     const int threads = kWarpsPerBlock * 32;
-    // register budget of the kernel: 2, 3 or 4 resident blocks per SM
-    auto kern = h.lane_minb == 2 ? kb_lane_cells<EVT, 2>
-              : h.lane_minb == 4 ? kb_lane_cells<EVT, 4>
-                                 : kb_lane_cells<EVT, 3>;
+    // register budget of the kernel: 2, 3 or 4 resident blocks per SM; the
+    // adjoint's recording forward solve runs the 2-block build
+    auto kern = rio != nullptr ? kb_lane_cells<EVT, 2, true>
+              : h.lane_minb == 3 ? kb_lane_cells<EVT, 3, false>
+              : h.lane_minb == 4 ? kb_lane_cells<EVT, 4, false>
+                                 : kb_lane_cells<EVT, 2, false>;
     long blocks;
     if (h.kernel == 0) {
       blocks = ((long)ncell + threads - 1) / threads;
@@ -530,8 +566,10 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
       cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(unsigned), stream);
       if (e != cudaSuccess) return e;
     }
+    const RecIO none{nullptr, 0, nullptr, 0, nullptr, nullptr};
     kern<<<(int)blocks, threads, lsmem, stream>>>(
-        ncell, n, T, dt, par, pstride, flags, stats, so, cursor, h.kernel);
+        ncell, n, T, dt, par, pstride, flags, stats, so, cursor, h.kernel,
+        rio != nullptr ? *rio : none);
     return cudaGetLastError();
   }
   const size_t smem = sizeof(double) * kWarpsPerBlock * Geo<EVT>::SMEM_DOUBLES;
@@ -643,6 +681,7 @@ KB_API const char* krome_flag_message(int flag) {
     case -105: return "a required parameter is unset (NaN)";
     case -110: return "the integration ended at a non-positive or non-finite Tgas (input untouched)";
     case -111: return "device path: the cells do not fit in the device memory (FLAG_DEVICE_MEMORY)";
+    case -120: return "adjoint: the cell's tape outgrew its capacity (no gradient; input untouched)";
     default: break;
   }
   return flag <= -100 ? "unknown KROME flag" : "integrator failure";
@@ -790,6 +829,180 @@ KB_API int krome_b200_solve_device(int ncell, double* n, double* Tgas,
                                    flags, stats, cursor,
                                    static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? 0 : -104;
+}
+
+// ---- the discrete adjoint (adjoint.cuh) ----
+
+KB_API int krome_has_device(void);
+
+KB_API int krome_b200_adjoint_record_device(
+    int ncell, double* n, double* Tgas, const double* dt, const double* par,
+    int par_stride, const double* mult, int mult_stride, int* flags,
+    long* stats, unsigned* cursor, double* tape, long tape_cap,
+    long* tape_len, double* yfin, const krome_opts* h, void* stream) {
+  if (h == nullptr || ncell < 0) return -1;
+  if (ncell == 0) return 0;
+  if (n == nullptr || Tgas == nullptr || dt == nullptr || par == nullptr
+      || flags == nullptr || tape == nullptr || tape_len == nullptr
+      || yfin == nullptr || tape_cap <= 0)
+    return -1;
+  if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+  if (mult_stride != 0 && mult_stride != kbnet::NREA) return -1;
+  if (cursor == nullptr && h->kernel == 1) return -1;
+  if (h->linsol == 2 || h->linsol == 3 || h->conserve != 0) return -104;
+  const RecIO rio{mult, mult_stride, tape, tape_cap, tape_len, yfin};
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const cudaError_t e =
+      h->evolve_T ? launch<true>(*h, ncell, n, Tgas, dt, par, par_stride, flags,
+                                 stats, cursor, st, &rio)
+                  : launch<false>(*h, ncell, n, Tgas, dt, par, par_stride,
+                                  flags, stats, cursor, st, &rio);
+  return e == cudaSuccess ? 0 : -104;
+}
+
+KB_API int krome_b200_adjoint_device(
+    int ncell, const double* T0, const double* par, int par_stride,
+    const double* mult, int mult_stride, const double* gn, const double* gT,
+    const int* flags, const double* tape, long tape_cap,
+    const long* tape_len, const double* yfin, double* dn0, double* dT0,
+    double* dm, const krome_opts* h, void* stream) {
+  if (h == nullptr || ncell < 0) return -1;
+  if (ncell == 0) return 0;
+  if (T0 == nullptr || par == nullptr || gn == nullptr || flags == nullptr
+      || tape == nullptr || tape_len == nullptr || yfin == nullptr
+      || dn0 == nullptr || dm == nullptr || tape_cap <= 0)
+    return -1;
+  if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+  if (mult_stride != 0 && mult_stride != kbnet::NREA) return -1;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int blocks = (ncell + 127) / 128;
+  if (h->evolve_T)
+    kba::kb_adjoint_cells<true><<<blocks, 128, 0, st>>>(
+        ncell, T0, par, par_stride, mult, mult_stride, gn, gT, flags, tape,
+        tape_cap, tape_len, yfin, h->clip_negative, dn0, dT0, dm);
+  else
+    kba::kb_adjoint_cells<false><<<blocks, 128, 0, st>>>(
+        ncell, T0, par, par_stride, mult, mult_stride, gn, gT, flags, tape,
+        tape_cap, tape_len, yfin, h->clip_negative, dn0, dT0, dm);
+  return cudaGetLastError() == cudaSuccess ? 0 : -104;
+}
+
+KB_API int krome_b200_adjoint(int ncell, double* n, double* Tgas,
+                              const double* dt, const double* par,
+                              int par_stride, const double* lnm,
+                              int lnm_stride, const double* gn,
+                              const double* gT, int* flags, double* dn0,
+                              double* dT0, double* dm, long tape_cap,
+                              const krome_opts* h) {
+  using namespace kbnet;
+  if (h == nullptr || ncell < 0 || n == nullptr || Tgas == nullptr
+      || dt == nullptr || gn == nullptr || dn0 == nullptr || dm == nullptr)
+    return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != NPAR) return -1;
+  if (lnm != nullptr && lnm_stride != 0 && lnm_stride != NREA) return -1;
+  if (ncell == 0) return 0;
+  std::vector<double> dflt(NPAR);
+  krome_params_default(dflt.data());
+  const double* P = par != nullptr ? par : dflt.data();
+  const int ps = par != nullptr ? par_stride : 0;
+  std::vector<int> fl(ncell, 0);
+  int* fo = flags != nullptr ? flags : fl.data();
+  if (check_params(ncell, P, ps, fo) != 0) return -105;
+  if (h->linsol == 2 || h->linsol == 3 || h->conserve != 0) {
+    for (int c = 0; c < ncell; ++c) fo[c] = -104;
+    return -104;
+  }
+  if (!krome_has_device()) {
+    for (int c = 0; c < ncell; ++c) fo[c] = -104;
+    return -104;
+  }
+  const long cap = tape_cap > 0 ? tape_cap : 32768;
+  const int N = NSPEC + (h->evolve_T ? 1 : 0);
+  const long prow = ps == 0 ? 1 : ncell;
+  const long mrows = lnm == nullptr ? 0 : (lnm_stride == 0 ? 1 : ncell);
+  std::vector<double> mult(mrows * NREA);
+  for (long i = 0; i < mrows * NREA; ++i) mult[i] = std::exp(lnm[i]);
+  // device buffers: n T T0 dt par mult gn gT yfin dn0 dT0 dm tape (+ ints)
+  const size_t nd = (size_t)ncell * NSPEC;
+  const size_t dbl = 2 * nd + 3 * (size_t)ncell + prow * NPAR + mrows * NREA
+                     + nd + ncell + (size_t)ncell * N + nd + ncell
+                     + (size_t)ncell * NREA;
+  double* d = nullptr;
+  long* dlen = nullptr;
+  int* dfl = nullptr;
+  unsigned* dcur = nullptr;
+  double* dtape = nullptr;
+  auto release = [&]() {
+    cudaFree(d);
+    cudaFree(dlen);
+    cudaFree(dfl);
+    cudaFree(dcur);
+    cudaFree(dtape);
+  };
+  if (cudaMalloc(&d, dbl * sizeof(double)) != cudaSuccess
+      || cudaMalloc(&dlen, (size_t)ncell * sizeof(long)) != cudaSuccess
+      || cudaMalloc(&dfl, (size_t)ncell * sizeof(int)) != cudaSuccess
+      || cudaMalloc(&dcur, sizeof(unsigned)) != cudaSuccess
+      || cudaMalloc(&dtape, (size_t)ncell * cap * sizeof(double))
+             != cudaSuccess) {
+    release();
+    cudaGetLastError();
+    for (int c = 0; c < ncell; ++c) fo[c] = -111;
+    return -111;
+  }
+  double* dn = d;
+  double* dT = dn + nd;
+  double* dT0v = dT + ncell;
+  double* ddt = dT0v + ncell;
+  double* dpar = ddt + ncell;
+  double* dmult = dpar + prow * NPAR;
+  double* dgn = dmult + mrows * NREA;
+  double* dgT = dgn + nd;
+  double* dyf = dgT + ncell;
+  double* ddn0 = dyf + (size_t)ncell * N;
+  double* ddT0 = ddn0 + nd;
+  double* ddm = ddT0 + ncell;
+  std::vector<double> zero(ncell, 0.0);
+  cudaMemcpy(dn, n, nd * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(dT, Tgas, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(dT0v, Tgas, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(ddt, dt, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(dpar, P, prow * NPAR * sizeof(double), cudaMemcpyHostToDevice);
+  if (mrows > 0)
+    cudaMemcpy(dmult, mult.data(), mrows * NREA * sizeof(double),
+               cudaMemcpyHostToDevice);
+  cudaMemcpy(dgn, gn, nd * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(dgT, gT != nullptr ? gT : zero.data(), ncell * sizeof(double),
+             cudaMemcpyHostToDevice);
+  int r = krome_b200_adjoint_record_device(
+      ncell, dn, dT, ddt, dpar, ps, mrows > 0 ? dmult : nullptr,
+      mrows > 1 ? NREA : 0, dfl, nullptr, dcur, dtape, cap, dlen, dyf, h,
+      nullptr);
+  if (r == 0)
+    r = krome_b200_adjoint_device(ncell, dT0v, dpar, ps,
+                                  mrows > 0 ? dmult : nullptr,
+                                  mrows > 1 ? NREA : 0, dgn, dgT, dfl, dtape,
+                                  cap, dlen, dyf, ddn0, ddT0, ddm, h, nullptr);
+  if (r == 0 && cudaDeviceSynchronize() != cudaSuccess) r = -104;
+  if (r == 0) {
+    cudaMemcpy(n, dn, nd * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(Tgas, dT, ncell * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(fo, dfl, ncell * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(dn0, ddn0, nd * sizeof(double), cudaMemcpyDeviceToHost);
+    if (dT0 != nullptr)
+      cudaMemcpy(dT0, ddT0, ncell * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(dm, ddm, (size_t)ncell * NREA * sizeof(double),
+               cudaMemcpyDeviceToHost);
+    if (cudaGetLastError() != cudaSuccess) r = -104;
+  }
+  release();
+  if (r != 0) {
+    for (int c = 0; c < ncell; ++c) fo[c] = r;
+    return r;
+  }
+  for (int c = 0; c < ncell; ++c)
+    if (fo[c] != 0) return fo[c];
+  return 0;
 }
 
 KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,

@@ -472,21 +472,25 @@ class Emitter:
             out.append(rx)
         return out
 
-    def emit_thermal(self):
-        w = self.w
-        th = self.gen.thermal
-        net = self.net
-        # the H2 chemistry ledger (thermal CHEM)
+    def _chem_terms(self):
+        """the H2 chemistry ledger (thermal CHEM): (heating, cooling)
+        terms as (energy in eV, reaction, critical-density factor)"""
         chem = []
-        for rx in net.reactions:
+        for rx in self.net.reactions:
             R = sorted(r["sp"] for r in rx["reactants"])
             P = sorted(p0["sp"] for p0 in rx["products"])
             for rr, pp, q, ff in CHEM_LEDGER:
                 if R == rr and P == pp:
                     chem.append((q, rx, ff))
                     break
-        heat_terms = [x for x in chem if not x[0].startswith("-")]
-        diss_terms = [x for x in chem if x[0].startswith("-")]
+        return ([x for x in chem if not x[0].startswith("-")],
+                [x for x in chem if x[0].startswith("-")])
+
+    def emit_thermal(self):
+        w = self.w
+        th = self.gen.thermal
+        net = self.net
+        heat_terms, diss_terms = self._chem_terms()
         if th.get("cool_chem"):
             w("KB_HD inline double cooling_chem(const double* n, const double* k) {")
             w("  double c = 0.0;")
@@ -701,11 +705,92 @@ class Emitter:
         w("  return gsum > 0.0 ? 1.0 + ysum / gsum : 5.0 / 3.0;")
         w("}")
 
+    def emit_lnk_vjp(self):
+        """the contraction of d f / d ln k with a vector mu, for the
+        adjoint's per-reaction ln-multipliers: f is linear in each rate
+        coefficient (the mass-action fluxes and the chemical heating and
+        cooling), so d f_i / d ln k_r is reaction r's own term of f_i"""
+        w = self.w
+        th = self.gen.thermal
+        w("// g[r] += sum_i mu_i d f_i / d ln k_r at the state n with the rates k;")
+        w("// muT: mu of the Tgas row (0 without it), Tth the thermal temperature")
+        w("KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, "
+          "const Params& p, const double* mu, double muT, double* g) {")
+        w("  (void)Tth; (void)p; (void)muT;")
+        w("  double flux;")
+        w("  (void)flux;")
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            fac = ["k[%d]" % i] + [self.den(s) for s in self._kin(rx)]
+            terms = (["+ mu[IDX_%s]" % self.cid(pr["sp"]) for pr in rx["products"]]
+                     + ["- mu[IDX_%s]" % self.cid(r["sp"]) for r in rx["reactants"]])
+            if not terms:
+                continue
+            w("  flux = %s;" % "*".join(fac))
+            w("  g[%d] += flux * (%s);" % (i, " ".join(terms).lstrip("+ ")))
+        heat_terms, diss_terms = self._chem_terms()
+        heat = th.get("heat_chem") and heat_terms
+        cool = th.get("cool_chem") and diss_terms
+        if heat or cool:
+            w("  if (muT != 0.0) {")
+            w("    const double c = muT * (gamma_index(Tth, n, p) - 1.0)"
+              " / (kbc::boltzmann_erg * ntot_(n)) * kbc::eV_to_erg;")
+            if cool:
+                for q, rx, _ in diss_terms:
+                    prod = "*".join(self.den(r["sp"]) for r in rx["reactants"])
+                    w("    g[%d] -= c * k[%d] * %s * %s;"
+                      % (rx["id"] - 1, rx["id"] - 1, q[1:], prod))
+            if heat:
+                w("    const double dd = Hnuclei_(n);")
+                w("    const double ncr = 1.0e6 / std::sqrt(Tth)")
+                w("        / (1.6 * std::exp(-std::pow(4.0e2 / Tth, 2.0)) "
+                  "* n[IDX_H] / dd")
+                w("           + 1.4 * std::exp(-1.2e4 / (Tth + 1.2e3)) "
+                  "* n[IDX_H2] / dd);")
+                w("    const double ffac = 1.0 / (1.0 + ncr / dd);")
+                w("    (void)ffac;")
+                for q, rx, ff in heat_terms:
+                    prod = "*".join(self.den(r["sp"]) for r in rx["reactants"])
+                    qexpr = "%s*ffac" % q if ff else q
+                    w("    g[%d] += c * k[%d] * (%s) * %s;"
+                      % (rx["id"] - 1, rx["id"] - 1, qexpr, prod))
+            w("  }")
+        w("}")
+        w("")
+
+    def _rates_depend_on_n(self):
+        """whether a rate coefficient depends on the densities (through
+        rates_var or the v_* variables it calls): then the species block of
+        the analytic Jacobian, taken at fixed k, is not the exact dF/dn"""
+        import re
+        text = "\n".join(self.lines)
+        bodies = {}
+        for m in re.finditer(r"KB_HD inline double (v_\w+)\([^)]*\) \{(.*?)\n\}",
+                             text, re.S):
+            bodies[m.group(1)] = m.group(2)
+        direct = re.compile(r"n\[|\w+_\(n\)")
+
+        def dep(body, seen):
+            if direct.search(body):
+                return True
+            for v in set(re.findall(r"\b(v_\w+)\(", body)) - seen:
+                if v in bodies and dep(bodies[v], seen | {v}):
+                    return True
+            return False
+        m = re.search(r"inline void rates_var\(.*?\n\}", text, re.S)
+        body = m.group(0).split("{", 1)[1] if m else ""
+        body = body.replace("(void)n;", "")
+        return dep(body, set())
+
     def emit_tail(self):
         th = self.gen.thermal
         any_thermal = any(th.get(f) for f in th if f.startswith(("cool_", "heat_")))
         self.w("constexpr bool HAS_THERMAL_TERMS = %s;"
                % ("true" if any_thermal else "false"))
+        self.w("// a rate coefficient depends on the densities (the species block")
+        self.w("// of jac_stoich, taken at fixed k, is then not the exact dF/dn)")
+        self.w("constexpr bool RATES_DEPEND_ON_N = %s;"
+               % ("true" if self._rates_depend_on_n() else "false"))
         self.w("}  // namespace kbnet")
 
     def run(self):
@@ -716,6 +801,7 @@ class Emitter:
         self.emit_rhs()
         self.emit_jac()
         self.emit_thermal()
+        self.emit_lnk_vjp()
         self.emit_tail()
         return "\n".join(self.lines) + "\n"
 

@@ -167,6 +167,17 @@ class Network:
                                                        ctypes.c_void_p]),
             "krome_b200_graph_free": (None, [ctypes.c_void_p]),
             "krome_b200_fp64_peak": (ctypes.c_int, [_D]),
+            "krome_b200_adjoint": (ctypes.c_int, [
+                ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _D, ctypes.c_int,
+                _D, _D, _I, _D, _D, _D, ctypes.c_long, ctypes.c_void_p]),
+            "krome_b200_adjoint_record_device": (ctypes.c_int, [
+                ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_int,
+                ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4
+                + [ctypes.c_long] + [ctypes.c_void_p] * 4),
+            "krome_b200_adjoint_device": (ctypes.c_int, [
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4
+                + [ctypes.c_long] + [ctypes.c_void_p] * 7),
         }
         for name, (res, args) in proto.items():
             fn = getattr(lib, name)
@@ -313,6 +324,58 @@ class Network:
         return self.solve(n, Tgas, dt, par=par, opts=opts, check=check,
                           stats=stats)
 
+    def adjoint(self, n, Tgas, dt, par=None, gn=None, gT=None, lnm=None,
+                opts=None, tape_cap=0, check=True):
+        """the discrete adjoint of the batched solve (krome_b200_adjoint):
+        the solve of n[N, nspec], Tgas[N], dt[N] with every rate
+        coefficient multiplied by exp(lnm) (lnm None, one row [nrea] or
+        [N, nrea]), and the gradient of sum(gn * n_out) + sum(gT * T_out)
+        with respect to the initial n (dn0), Tgas (dT0) and lnm (dm, per
+        cell). tape_cap: doubles of tape per cell (0: the default 32768).
+        Returns a Result with dn0, dT0, dm attached."""
+        n = np.array(n, dtype=float, order="C", copy=True)
+        if n.ndim != 2 or n.shape[1] != self.nspec:
+            raise KromeError("adjoint: n must be (N, %d), got %s"
+                             % (self.nspec, n.shape))
+        N = n.shape[0]
+        T = np.array(Tgas, dtype=float, order="C", copy=True).reshape(N)
+        dtv = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, float), (N,)))
+        opts = self._options(opts)
+        P, stride = self._params(par, N)
+        gn = np.ascontiguousarray(np.zeros_like(n) if gn is None else gn,
+                                  dtype=float).reshape(N, self.nspec)
+        gT = np.ascontiguousarray(np.zeros(N) if gT is None else gT,
+                                  dtype=float).reshape(N)
+        lstride = 0
+        if lnm is not None:
+            lnm = np.ascontiguousarray(lnm, dtype=float)
+            lstride = 0 if lnm.ndim == 1 else self.nrea
+        flags = np.zeros(N, dtype=np.intc)
+        dn0 = np.zeros((N, self.nspec))
+        dT0 = np.zeros(N)
+        dm = np.zeros((N, self.nrea))
+        ierr = self._lib.krome_b200_adjoint(
+            N, _dptr(n), _dptr(T), _dptr(dtv), _dptr(P), stride,
+            None if lnm is None else _dptr(lnm), lstride, _dptr(gn),
+            _dptr(gT), flags.ctypes.data_as(_I), _dptr(dn0), _dptr(dT0),
+            _dptr(dm), int(tape_cap), opts._h)
+        if check and ierr != 0:
+            raise KromeError("krome_b200_adjoint returned %d: %s"
+                             % (ierr, self.flag_message(ierr)))
+        r = Result(n, T, flags, ierr)
+        r.dn0, r.dT0, r.dm = dn0, dT0, dm
+        return r
+
+    def _check_stats(self, stats, N):
+        """a device stats array must hold N rows of the library's counters:
+        the kernels write nstat of them per cell"""
+        if stats is None or isinstance(stats, int):
+            return
+        nst = self._lib.krome_b200_nstat()
+        if tuple(stats.shape) != (N, nst) or stats.dtype.itemsize != 8:
+            raise KromeError("stats must be int64 [%d, %d], got %s %s"
+                             % (N, nst, tuple(stats.shape), stats.dtype))
+
     def solve_device(self, n, Tgas, dt, par, flags, opts=None, stats=None,
                      cursor=None, stream=0):
         """device-resident solve: every argument a CUDA array (torch tensor
@@ -326,6 +389,7 @@ class Network:
         N = int(n.shape[0])
         npar_el = int(par.numel()) if hasattr(par, "numel") else self.npar
         stride = 0 if npar_el == self.npar else self.npar
+        self._check_stats(stats, N)
         opts = self._options(opts)
         r = self._lib.krome_b200_solve_device(
             N, ptr(n), ptr(Tgas), ptr(dt), ptr(par), stride, ptr(flags),
@@ -376,6 +440,7 @@ class HydroGraph:
         self.stream = stream or torch.cuda.Stream()
         self.cursor = cursor if cursor is not None else torch.zeros(
             1, dtype=torch.int32, device=n.device)
+        net._check_stats(stats, int(n.shape[0]))
         self._keep = (n, Tgas, dt, par, flags, stats, opts)
         ptr = lambda x: None if x is None else x.data_ptr()
         self._h = net._lib.krome_b200_graph_new(

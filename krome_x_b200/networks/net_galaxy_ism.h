@@ -1125,5 +1125,108 @@ KB_HD inline double thermal_dTdt(double T, const double* n, const double* k, con
       / (kbc::boltzmann_erg * ntot_(n));
 }
 
+// g[r] += sum_i mu_i d f_i / d ln k_r at the state n with the rates k;
+// muT: mu of the Tgas row (0 without it), Tth the thermal temperature
+KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Params& p, const double* mu, double muT, double* g) {
+  (void)Tth; (void)p; (void)muT;
+  double flux;
+  (void)flux;
+  flux = k[0]*n[IDX_H]*n[IDX_E];
+  g[0] += flux * (mu[IDX_Hj] + mu[IDX_E] + mu[IDX_E] - mu[IDX_H] - mu[IDX_E]);
+  flux = k[1]*n[IDX_Hj]*n[IDX_E];
+  g[1] += flux * (mu[IDX_H] - mu[IDX_Hj] - mu[IDX_E]);
+  flux = k[2]*n[IDX_Hj]*n[IDX_E];
+  g[2] += flux * (mu[IDX_H] - mu[IDX_Hj] - mu[IDX_E]);
+  flux = k[3]*n[IDX_He]*n[IDX_E];
+  g[3] += flux * (mu[IDX_Hej] + mu[IDX_E] + mu[IDX_E] - mu[IDX_He] - mu[IDX_E]);
+  flux = k[4]*n[IDX_Hej]*n[IDX_E];
+  g[4] += flux * (mu[IDX_He] - mu[IDX_Hej] - mu[IDX_E]);
+  flux = k[5]*n[IDX_Hej]*n[IDX_E];
+  g[5] += flux * (mu[IDX_He] - mu[IDX_Hej] - mu[IDX_E]);
+  flux = k[6]*n[IDX_Hej]*n[IDX_E];
+  g[6] += flux * (mu[IDX_Hejj] + mu[IDX_E] + mu[IDX_E] - mu[IDX_Hej] - mu[IDX_E]);
+  flux = k[7]*n[IDX_Hejj]*n[IDX_E];
+  g[7] += flux * (mu[IDX_Hej] - mu[IDX_Hejj] - mu[IDX_E]);
+  flux = k[8]*n[IDX_H]*n[IDX_E];
+  g[8] += flux * (mu[IDX_Hk] - mu[IDX_H] - mu[IDX_E]);
+  flux = k[9]*n[IDX_Hk]*n[IDX_H];
+  g[9] += flux * (mu[IDX_H2] + mu[IDX_E] - mu[IDX_Hk] - mu[IDX_H]);
+  flux = k[10]*n[IDX_H]*n[IDX_Hj];
+  g[10] += flux * (mu[IDX_H2j] - mu[IDX_H] - mu[IDX_Hj]);
+  flux = k[11]*n[IDX_H]*n[IDX_Hj];
+  g[11] += flux * (mu[IDX_H2j] - mu[IDX_H] - mu[IDX_Hj]);
+  flux = k[12]*n[IDX_H2j]*n[IDX_H];
+  g[12] += flux * (mu[IDX_H2] + mu[IDX_Hj] - mu[IDX_H2j] - mu[IDX_H]);
+  flux = k[13]*n[IDX_H2]*n[IDX_Hj];
+  g[13] += flux * (mu[IDX_H2j] + mu[IDX_H] - mu[IDX_H2] - mu[IDX_Hj]);
+  flux = k[14]*n[IDX_H2]*n[IDX_Hj];
+  g[14] += flux * (mu[IDX_H2j] + mu[IDX_H] - mu[IDX_H2] - mu[IDX_Hj]);
+  flux = k[15]*n[IDX_H2]*n[IDX_E];
+  g[15] += flux * (mu[IDX_H] + mu[IDX_Hk] - mu[IDX_H2] - mu[IDX_E]);
+  flux = k[16]*n[IDX_H2]*n[IDX_E];
+  g[16] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_E] - mu[IDX_H2] - mu[IDX_E]);
+  flux = k[17]*n[IDX_H2]*n[IDX_H];
+  g[17] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_H] - mu[IDX_H2] - mu[IDX_H]);
+  flux = k[18]*n[IDX_Hk]*n[IDX_E];
+  g[18] += flux * (mu[IDX_H] + mu[IDX_E] + mu[IDX_E] - mu[IDX_Hk] - mu[IDX_E]);
+  flux = k[19]*n[IDX_Hk]*n[IDX_H];
+  g[19] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_E] - mu[IDX_Hk] - mu[IDX_H]);
+  flux = k[20]*n[IDX_Hk]*n[IDX_H];
+  g[20] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_E] - mu[IDX_Hk] - mu[IDX_H]);
+  flux = k[21]*n[IDX_Hk]*n[IDX_Hj];
+  g[21] += flux * (mu[IDX_H] + mu[IDX_H] - mu[IDX_Hk] - mu[IDX_Hj]);
+  flux = k[22]*n[IDX_Hk]*n[IDX_Hj];
+  g[22] += flux * (mu[IDX_H2j] + mu[IDX_E] - mu[IDX_Hk] - mu[IDX_Hj]);
+  flux = k[23]*n[IDX_H2j]*n[IDX_E];
+  g[23] += flux * (mu[IDX_H] + mu[IDX_H] - mu[IDX_H2j] - mu[IDX_E]);
+  flux = k[24]*n[IDX_H2j]*n[IDX_E];
+  g[24] += flux * (mu[IDX_H] + mu[IDX_H] - mu[IDX_H2j] - mu[IDX_E]);
+  flux = k[25]*n[IDX_H2j]*n[IDX_Hk];
+  g[25] += flux * (mu[IDX_H] + mu[IDX_H2] - mu[IDX_H2j] - mu[IDX_Hk]);
+  flux = k[26]*n[IDX_H2]*n[IDX_H2];
+  g[26] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_H2] - mu[IDX_H2] - mu[IDX_H2]);
+  flux = k[27]*n[IDX_Hej]*n[IDX_H];
+  g[27] += flux * (mu[IDX_He] + mu[IDX_Hj] - mu[IDX_Hej] - mu[IDX_H]);
+  flux = k[28]*n[IDX_He]*n[IDX_Hj];
+  g[28] += flux * (mu[IDX_Hej] + mu[IDX_H] - mu[IDX_He] - mu[IDX_Hj]);
+  flux = k[29]*n[IDX_He]*n[IDX_Hj];
+  g[29] += flux * (mu[IDX_Hej] + mu[IDX_H] - mu[IDX_He] - mu[IDX_Hj]);
+  flux = k[30]*n[IDX_H2]*n[IDX_Hej];
+  g[30] += flux * (mu[IDX_He] + mu[IDX_H] + mu[IDX_Hj] - mu[IDX_H2] - mu[IDX_Hej]);
+  flux = k[31]*n[IDX_H2]*n[IDX_He];
+  g[31] += flux * (mu[IDX_H] + mu[IDX_H] + mu[IDX_He] - mu[IDX_H2] - mu[IDX_He]);
+  flux = k[32]*n[IDX_H2]*n[IDX_Hej];
+  g[32] += flux * (mu[IDX_H2j] + mu[IDX_He] - mu[IDX_H2] - mu[IDX_Hej]);
+  flux = k[33]*n[IDX_H]*n[IDX_H];
+  g[33] += flux * (mu[IDX_H] + mu[IDX_Hj] + mu[IDX_E] - mu[IDX_H] - mu[IDX_H]);
+  flux = k[34]*n[IDX_H]*n[IDX_He];
+  g[34] += flux * (mu[IDX_He] + mu[IDX_Hj] + mu[IDX_E] - mu[IDX_H] - mu[IDX_He]);
+  flux = k[35]*n[IDX_H];
+  g[35] += flux * (mu[IDX_Hj] + mu[IDX_E] - mu[IDX_H]);
+  flux = k[36]*n[IDX_He];
+  g[36] += flux * (mu[IDX_Hej] + mu[IDX_E] - mu[IDX_He]);
+  flux = k[37]*n[IDX_Hej];
+  g[37] += flux * (mu[IDX_Hejj] + mu[IDX_E] - mu[IDX_Hej]);
+  flux = k[38]*n[IDX_Hk];
+  g[38] += flux * (mu[IDX_H] + mu[IDX_E] - mu[IDX_Hk]);
+  flux = k[39]*n[IDX_H2];
+  g[39] += flux * (mu[IDX_H2j] + mu[IDX_E] - mu[IDX_H2]);
+  flux = k[40]*n[IDX_H2j];
+  g[40] += flux * (mu[IDX_Hj] + mu[IDX_H] - mu[IDX_H2j]);
+  flux = k[41]*n[IDX_H2j];
+  g[41] += flux * (mu[IDX_Hj] + mu[IDX_Hj] + mu[IDX_E] - mu[IDX_H2j]);
+  flux = k[42]*n[IDX_H2];
+  g[42] += flux * (mu[IDX_H] + mu[IDX_H] - mu[IDX_H2]);
+  flux = k[43]*n[IDX_H2];
+  g[43] += flux * (mu[IDX_H] + mu[IDX_H] - mu[IDX_H2]);
+  flux = k[44]*n[IDX_Hj]*n[IDX_E];
+  g[44] += flux * (mu[IDX_H] - mu[IDX_Hj] - mu[IDX_E]);
+  flux = k[45]*n[IDX_Hej]*n[IDX_E];
+  g[45] += flux * (mu[IDX_He] - mu[IDX_Hej] - mu[IDX_E]);
+}
+
 constexpr bool HAS_THERMAL_TERMS = false;
+// a rate coefficient depends on the densities (the species block
+// of jac_stoich, taken at fixed k, is then not the exact dF/dn)
+constexpr bool RATES_DEPEND_ON_N = false;
 }  // namespace kbnet

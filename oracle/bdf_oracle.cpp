@@ -193,6 +193,7 @@ struct Problem {
   double k[NREA + 1];
   double k0[NREA + 1], kp[NREA + 1];
   double fm[NSPEC + 1];
+  const double* mult = nullptr;  // per-reaction factors exp(m_r) (adjoint)
 
   double state_T(const double* y) const {
     const double T = iT >= 0 ? y[iT] : Tfix;
@@ -218,6 +219,14 @@ struct Problem {
       rates_fixed(T, y, p, kk);
       rates_var(T, y, p, kk);
     }
+    if (mult != nullptr)
+      for (int i = 0; i < NREA; ++i) kk[i] *= mult[i];
+  }
+  // g[r] += sum_i mu_i d f_i / d ln k_r at y (the emitted lnk_vjp)
+  void lnk_vjp_at(const double* y, const double* mu, double* g) {
+    eval_rates(state_T(y), y, k0);
+    const double Tth = thermal_T(iT >= 0 ? y[iT] : Tfix);
+    lnk_vjp(y, k0, Tth, p, mu, iT >= 0 ? mu[iT] : 0.0, g);
   }
   double aux(const double* y, const double* kk) {
     const double T = thermal_T(iT >= 0 ? y[iT] : Tfix);
@@ -302,10 +311,30 @@ struct BdfOpts {
   bool lu32 = false;
 };
 
+// ---- the discrete adjoint's tape ----
+// The forward solve records every operation that changes the Nordsieck
+// array zn, in order; the step sizes, orders and Newton / error-test
+// decisions are the forward's (constants of the discrete map). Each record
+// is [op, payload..., record length].
+enum TapeOp {
+  TP_INIT = 1,   // zn[0] = y0, zn[1] = h f(y0):           h, y0[N]
+  TP_RESCALE,    // zn[j] *= eta^j, j = 1..q:               eta, q
+  TP_INCREASE,   // zn[L] = A1 zn[QMAX]; zn[j] += l_j zn[L]: q, A1, l[0..5]
+  TP_DECREASE,   // zn[j] -= l_j zn[q], j = 2..q-1:         q, l[0..5]
+  TP_PREDICT,    // zn[j-1] += zn[j] (Pascal):              q
+  TP_RESTORE,    // zn[j-1] -= zn[j] (Pascal):              q
+  TP_RESET1,     // zn[1] = h f(zn[0]):                     h, y[N]
+  TP_CORRECT,    // zn[j] += l_j acor (+ zn[QMAX] = acor),
+                 // acor = gamma f(zn0 + acor) - rl1 zn1:  q, gamma, rl1,
+                 //                                          l[0..5], save, y_n[N]
+  TP_DKY         // y = sum_j s^j zn[j]:                    s, q
+};
+
 // one cell's CVODE BDF (bdf_cell.hpp:490-1501), unit stride, dense LU
 class Cvode {
  public:
   Stats st;
+  std::vector<double>* tape = nullptr;  // recording for the adjoint
   Cvode(Problem& prob, int n, const BdfOpts& opts)
       : P(prob), N(n), o(opts), work((L_MAX + 9) * n + 2 * n * n),
         A32(opts.lu32 ? (long)n * n : 0), piv(n) {
@@ -369,6 +398,7 @@ class Cvode {
       h0u = h;
       hprime = h;
       scale_(N, h, zn[1], zn[1]);
+      rec_(TP_INIT, {h}, zn[0]);
     }
     long nstloc = 0;
     for (;;) {
@@ -397,6 +427,7 @@ class Cvode {
         istate = SUCCESS;
         *tret = tout;
         get_dky_(tout, yout);
+        rec_(TP_DKY, {(tout - tn) / h, (double)q});
         next_q = qprime;
         next_h = hprime;
         break;
@@ -433,6 +464,24 @@ class Cvode {
 
   void copy_(const double* x, double* z) const {
     for (int i = 0; i < N; i++) z[i] = x[i];
+  }
+  bool qmax_saved = false;
+  void rec_(int op, std::initializer_list<double> vals, const double* v = nullptr) {
+    if (tape == nullptr) return;
+    const size_t start = tape->size();
+    tape->push_back(op);
+    for (double x : vals) tape->push_back(x);
+    if (v != nullptr)
+      for (int i = 0; i < N; i++) tape->push_back(v[i]);
+    tape->push_back((double)(tape->size() - start + 1));
+  }
+  void rec_l_(int op, std::initializer_list<double> head) {
+    if (tape == nullptr) return;
+    const size_t start = tape->size();
+    tape->push_back(op);
+    for (double x : head) tape->push_back(x);
+    for (int i = 0; i < L_MAX; i++) tape->push_back(l[i]);
+    tape->push_back((double)(tape->size() - start + 1));
   }
   // cvEwtSetSV (bdf_cell.hpp:689-713)
   int ewt_set(const double* ycur, double* weight) {
@@ -534,8 +583,21 @@ class Cvode {
       if (eflag != SUCCESS) return eflag;
       break;
     }
+    qmax_saved = false;
+    const int q_step = q;
     complete_step_();
     prepare_next_step_(dsm);
+    if (tape != nullptr) {  // y holds zn[0] + acor of the accepted attempt
+      const size_t start = tape->size();
+      tape->push_back(TP_CORRECT);
+      tape->push_back(q_step);
+      tape->push_back(gamma);
+      tape->push_back(rl1);
+      for (int i = 0; i < L_MAX; i++) tape->push_back(l[i]);
+      tape->push_back(qmax_saved ? 1.0 : 0.0);
+      for (int i = 0; i < N; i++) tape->push_back(y[i]);
+      tape->push_back((double)(tape->size() - start + 1));
+    }
     etamax = (st.nst <= SMALL_NST) ? ETA_MAX_ES : ETA_MAX_GS;
     scale_(N, tq[2], acor, acor);
     return SUCCESS;
@@ -574,6 +636,7 @@ class Cvode {
     scale_(N, A1, zn[QMAX], zn[L]);
     if (q > 1)
       for (int j = 2; j <= q; j++) axpy_(N, l[j], zn[L], zn[j]);
+    rec_l_(TP_INCREASE, {(double)q, A1});
   }
   void decrease_bdf_() {
     for (int i = 0; i <= QMAX; i++) l[i] = 0.0;
@@ -584,10 +647,13 @@ class Cvode {
       const double xi = hsum / hscale;
       for (int i = j + 2; i >= 2; i--) l[i] = l[i] * xi + l[i - 1];
     }
-    if (q > 2)
+    if (q > 2) {
       for (int j = 2; j < q; j++) axpy_(N, -l[j], zn[q], zn[j]);
+      rec_l_(TP_DECREASE, {(double)q});
+    }
   }
   void rescale_() {
+    rec_(TP_RESCALE, {eta, (double)q});
     double c = eta;
     for (int j = 1; j <= q; j++) {
       scale_(N, c, zn[j], zn[j]);
@@ -599,11 +665,13 @@ class Cvode {
     nscon = 0;
   }
   void predict_() {
+    rec_(TP_PREDICT, {(double)q});
     tn += h;
     for (int k = 1; k <= q; k++)
       for (int j = q; j >= k; j--) axpy_(N, 1.0, zn[j], zn[j - 1]);
   }
   void restore_(double saved_t) {
+    rec_(TP_RESTORE, {(double)q});
     tn = saved_t;
     for (int k = 1; k <= q; k++)
       for (int j = q; j >= k; j--) axpy_(N, -1.0, zn[j], zn[j - 1]);
@@ -908,6 +976,7 @@ class Cvode {
     if (retval < 0) return RHSFUNC_FAIL;
     if (retval > 0) return UNREC_RHSFUNC_ERR;
     scale_(N, h, tempv, zn[1]);
+    rec_(TP_RESET1, {h}, zn[0]);
     return TRY_AGAIN;
   }
   void complete_step_() {
@@ -923,6 +992,7 @@ class Cvode {
     qwait--;
     if ((qwait == 1) && (q != QMAX)) {
       copy_(acor, zn[QMAX]);
+      qmax_saved = true;
       saved_tq5 = tq[5];
     }
   }
@@ -999,6 +1069,7 @@ class Cvode {
       eta = etaqp1;
       qprime = q + 1;
       copy_(acor, zn[QMAX]);
+      qmax_saved = true;
     }
   }
   void get_dky_(double t, double* dky) {
@@ -1051,9 +1122,15 @@ ORACLE_API const char* oracle_network(void) { return NETWORK_KEY; }
 
 // one cell (solve_cell.hpp:2094-2203 with integrate_ 1662-1705 and the
 // restart wrapper bdf_cell.hpp:1513-1547); n, Tgas in/out
-ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, double dt,
-                     const oracle_opts* so, long* stats) {
+namespace {
+// one cell; mult (exp of the rate ln-multipliers) and tape (the adjoint's
+// recording) may be null; yfin receives the integrator's final y before the
+// post-solve rules (may be null)
+int solve_one_(double* n, double* Tgas, const double* par, double dt,
+               const oracle_opts* so, long* stats, const double* mult,
+               std::vector<double>* tape, double* yfin) {
   Problem c;
+  c.mult = mult;
   params_from_row(par, c.p);
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
   c.Tfix = *Tgas;
@@ -1093,6 +1170,7 @@ ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, doub
   int flag;
   {
     Cvode cv(c, N, bo);
+    cv.tape = tape;
     cv.reinit(0.0, y.data(), bo.h0);
     double t = 0.0;
     for (;;) {
@@ -1118,6 +1196,8 @@ ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, doub
   if (c.hit_T0 && (flag == REPTD_RHSFUNC_ERR || flag == RHSFUNC_FAIL
                    || flag == UNREC_RHSFUNC_ERR || flag == FIRST_RHSFUNC_ERR))
     flag = FLAG_NONPOSITIVE_T;
+  if (yfin != nullptr)
+    for (int i = 0; i < N; ++i) yfin[i] = y[i];
   if (flag == 0) {
     for (int i = 0; i < NSPEC; ++i) {
       n[i] = y[i];
@@ -1126,6 +1206,404 @@ ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, doub
     if (c.iT >= 0) *Tgas = y[c.iT];
   }
   return flag;
+}
+
+// dF/dy at y for the adjoint, column-major: the stoichiometric block where
+// it is exact (rates independent of the densities: the block at fixed k is
+// dF/dn) with central differences for the Tgas column and row, else central
+// differences on every column
+void adjoint_jac_(Problem& P, const double* y, double* J, double* yp,
+                  double* fp, double* fq) {
+  const int N = P.NEQ;
+  for (long k = 0; k < (long)N * N; ++k) J[k] = 0.0;
+  for (int i = 0; i < N; ++i) yp[i] = y[i];
+  const bool analytic = !RATES_DEPEND_ON_N;
+  if (analytic) {
+    P.eval_rates(P.state_T(y), y, P.k0);
+    jac_stoich(y, P.k0, J, 1, N);
+    if (P.iT < 0) return;
+  }
+  for (int j = 0; j < N; ++j) {
+    // with n-independent rates only the Tgas column and the Tgas row
+    // need differences (central, as every column otherwise)
+    const bool row_only = analytic && j != P.iT;
+    const double h = j == P.iT ? std::fmax(1e-6 * std::fabs(y[j]), 1e-8)
+                               : Problem::fd_step_n(y, j);
+    yp[j] = y[j] + h;
+    P.full_rhs(yp, fp);
+    yp[j] = y[j] - h;
+    P.full_rhs(yp, fq);
+    yp[j] = y[j];
+    if (row_only) {
+      J[P.iT + (long)j * N] = (fp[P.iT] - fq[P.iT]) / (2.0 * h);
+    } else {
+      for (int i = 0; i < N; ++i) J[i + (long)j * N] = (fp[i] - fq[i]) / (2.0 * h);
+    }
+  }
+}
+
+// the reverse sweep over one cell's tape. lam_y: the adjoint of the final
+// y; out: lam_y0 (the adjoint of the initial y), gm += the ln-multiplier
+// gradient. The corrector's map is differentiated at its root:
+// (I - gamma J) d acor = gamma J d zn0 - rl1 d zn1 + gamma dF/dm dm.
+void adjoint_sweep_(Problem& P, const std::vector<double>& tape,
+                    const double* lam_y, double* lam_y0, double* gm) {
+  const int N = P.NEQ;
+  std::vector<double> Lam((long)L_MAX * N, 0.0), J((long)N * N), AT((long)N * N);
+  std::vector<double> mu(N), la(N), yp(N), fp(N), fq(N);
+  std::vector<int> piv(N);
+  auto lam = [&](int j) { return Lam.data() + (long)j * N; };
+  // the terms of zn1 = h f(y): lam0 += h J^T lam1, gm += h dF/dm^T lam1
+  auto f_terms = [&](const double* yv, double h) {
+    for (int i = 0; i < N; ++i) mu[i] = h * lam(1)[i];
+    adjoint_jac_(P, yv, J.data(), yp.data(), fp.data(), fq.data());
+    for (int j = 0; j < N; ++j) {
+      double t = 0.0;
+      for (int i = 0; i < N; ++i) t += J[i + (long)j * N] * mu[i];
+      lam(0)[j] += t;
+    }
+    P.lnk_vjp_at(yv, mu.data(), gm);
+    for (int i = 0; i < N; ++i) lam(1)[i] = 0.0;
+  };
+  long pos = (long)tape.size();
+  while (pos > 0) {
+    const long len = (long)tape[pos - 1];
+    const long start = pos - len;
+    const double* r = tape.data() + start;
+    switch ((int)r[0]) {
+      case TP_DKY: {
+        const double sv = r[1];
+        const int q = (int)r[2];
+        for (int j = 0; j <= q; j++) {
+          double c = 1.0;
+          for (int i = 0; i < j; i++) c *= sv;
+          for (int i = 0; i < N; i++) lam(j)[i] += c * lam_y[i];
+        }
+        break;
+      }
+      case TP_CORRECT: {
+        const int q = (int)r[1];
+        const double gam = r[2], rl1 = r[3];
+        const double* l = r + 4;
+        const bool save = r[4 + L_MAX] != 0.0;
+        const double* yn = r + 5 + L_MAX;
+        for (int i = 0; i < N; i++) {
+          double t = save ? lam(QMAX)[i] : 0.0;
+          for (int j = 0; j <= q; j++) t += l[j] * lam(j)[i];
+          la[i] = t;
+        }
+        if (save)
+          for (int i = 0; i < N; i++) lam(QMAX)[i] = 0.0;
+        adjoint_jac_(P, yn, J.data(), yp.data(), fp.data(), fq.data());
+        for (int j = 0; j < N; j++)
+          for (int i = 0; i < N; i++)
+            AT[i + (long)j * N] = (i == j ? 1.0 : 0.0) - gam * J[j + (long)i * N];
+        getrf_(AT.data(), N, piv.data());
+        for (int i = 0; i < N; i++) mu[i] = la[i];
+        getrs_(AT.data(), N, piv.data(), mu.data());
+        for (int j = 0; j < N; j++) {
+          double t = 0.0;
+          for (int i = 0; i < N; i++) t += J[i + (long)j * N] * mu[i];
+          lam(0)[j] += gam * t;
+        }
+        for (int i = 0; i < N; i++) lam(1)[i] -= rl1 * mu[i];
+        for (int i = 0; i < N; i++) mu[i] *= gam;
+        P.lnk_vjp_at(yn, mu.data(), gm);
+        break;
+      }
+      case TP_PREDICT:
+      case TP_RESTORE: {
+        const int q = (int)r[1];
+        const double sg = (int)r[0] == TP_PREDICT ? 1.0 : -1.0;
+        for (int k = q; k >= 1; k--)
+          for (int j = k; j <= q; j++)
+            for (int i = 0; i < N; i++) lam(j)[i] += sg * lam(j - 1)[i];
+        break;
+      }
+      case TP_RESCALE: {
+        const double eta = r[1];
+        const int q = (int)r[2];
+        double c = eta;
+        for (int j = 1; j <= q; j++) {
+          for (int i = 0; i < N; i++) lam(j)[i] *= c;
+          c = eta * c;
+        }
+        break;
+      }
+      case TP_INCREASE: {
+        const int q = (int)r[1];
+        const double A1 = r[2];
+        const double* l = r + 3;
+        const int L = q + 1;
+        for (int j = 2; j <= q; j++)
+          for (int i = 0; i < N; i++) lam(L)[i] += l[j] * lam(j)[i];
+        if (L == QMAX) {
+          for (int i = 0; i < N; i++) lam(QMAX)[i] *= A1;
+        } else {
+          for (int i = 0; i < N; i++) {
+            lam(QMAX)[i] += A1 * lam(L)[i];
+            lam(L)[i] = 0.0;
+          }
+        }
+        break;
+      }
+      case TP_DECREASE: {
+        const int q = (int)r[1];
+        const double* l = r + 2;
+        for (int j = 2; j < q; j++)
+          for (int i = 0; i < N; i++) lam(q)[i] -= l[j] * lam(j)[i];
+        break;
+      }
+      case TP_RESET1:
+        f_terms(r + 2, r[1]);
+        break;
+      case TP_INIT:
+        f_terms(r + 2, r[1]);
+        for (int j = 1; j < L_MAX; j++)
+          for (int i = 0; i < N; i++) lam(j)[i] = 0.0;
+        break;
+      default:
+        break;
+    }
+    pos = start;
+  }
+  for (int i = 0; i < N; i++) lam_y0[i] = lam(0)[i];
+}
+// the tangent (forward-mode) sweep over the same tape: dy0 -> dy_final
+// for the perturbation dy0 of the initial state and dm of the ln-multipliers
+// (the transpose of adjoint_sweep_; the tests check <lam, dy_final> =
+// <lam_y0, dy0> + <gm, dm>)
+void tangent_sweep_(Problem& P, const std::vector<double>& tape,
+                    const double* dy0, const double* dmv, double* dyf) {
+  const int N = P.NEQ;
+  std::vector<double> D((long)L_MAX * N, 0.0), J((long)N * N), A((long)N * N);
+  std::vector<double> b(N), yp(N), fp(N), fq(N), fm(N);
+  std::vector<int> piv(N);
+  bool first = true;
+  auto dz = [&](int j) { return D.data() + (long)j * N; };
+  // dF/dm dm at y: the change of f when ln k moves by dm (f linear in k)
+  auto fm_dm = [&](const double* yv, double* out) {
+    for (int i = 0; i < N; ++i) out[i] = 0.0;
+    if (dmv == nullptr) return;
+    for (int i = 0; i < N; ++i) yp[i] = yv[i];
+    const double* save = P.mult;
+    std::vector<double> mp(NREA), mm(NREA);
+    for (int r = 0; r < NREA; ++r) {
+      const double m0 = save != nullptr ? save[r] : 1.0;
+      mp[r] = m0 * std::exp(1e-6 * dmv[r]);
+      mm[r] = m0 * std::exp(-1e-6 * dmv[r]);
+    }
+    P.mult = mp.data();
+    P.full_rhs(yp.data(), fp.data());
+    P.mult = mm.data();
+    P.full_rhs(yp.data(), fq.data());
+    P.mult = save;
+    for (int i = 0; i < N; ++i) out[i] = (fp[i] - fq[i]) / 2e-6;
+  };
+  for (size_t pos = 0; pos < tape.size();) {
+    const double* r = tape.data() + pos;
+    int len = 0;
+    switch ((int)r[0]) {
+      case TP_INIT: len = 3 + N; break;
+      case TP_RESCALE: len = 4; break;
+      case TP_INCREASE: len = 4 + L_MAX; break;
+      case TP_DECREASE: len = 3 + L_MAX; break;
+      case TP_PREDICT: case TP_RESTORE: len = 3; break;
+      case TP_RESET1: len = 3 + N; break;
+      case TP_CORRECT: len = 6 + L_MAX + N; break;
+      case TP_DKY: len = 4; break;
+      default: return;
+    }
+    switch ((int)r[0]) {
+      case TP_INIT:
+      case TP_RESET1: {
+        const double h = r[1];
+        const double* yv = r + 2;
+        if ((int)r[0] == TP_INIT) {
+          // the first segment starts from dy0; a restart from its zn[0]
+          for (int j = 1; j < L_MAX; ++j)
+            for (int i = 0; i < N; ++i) dz(j)[i] = 0.0;
+          if (first)
+            for (int i = 0; i < N; ++i) dz(0)[i] = dy0[i];
+          first = false;
+        }
+        adjoint_jac_(P, yv, J.data(), yp.data(), fp.data(), fq.data());
+        fm_dm(yv, fm.data());
+        for (int i = 0; i < N; ++i) {
+          double t = fm[i];
+          for (int j = 0; j < N; ++j) t += J[i + (long)j * N] * dz(0)[j];
+          dz(1)[i] = h * t;
+        }
+        break;
+      }
+      case TP_RESCALE: {
+        const double eta = r[1];
+        const int q = (int)r[2];
+        double c = eta;
+        for (int j = 1; j <= q; j++) {
+          for (int i = 0; i < N; i++) dz(j)[i] *= c;
+          c *= eta;
+        }
+        break;
+      }
+      case TP_INCREASE: {
+        const int q = (int)r[1];
+        const double A1 = r[2];
+        const double* l = r + 3;
+        const int L = q + 1;
+        for (int i = 0; i < N; i++) dz(L)[i] = A1 * dz(QMAX)[i];
+        for (int j = 2; j <= q; j++)
+          for (int i = 0; i < N; i++) dz(j)[i] += l[j] * dz(L)[i];
+        break;
+      }
+      case TP_DECREASE: {
+        const int q = (int)r[1];
+        const double* l = r + 2;
+        for (int j = 2; j < q; j++)
+          for (int i = 0; i < N; i++) dz(j)[i] -= l[j] * dz(q)[i];
+        break;
+      }
+      case TP_PREDICT:
+      case TP_RESTORE: {
+        const int q = (int)r[1];
+        const double sg = (int)r[0] == TP_PREDICT ? 1.0 : -1.0;
+        for (int k = 1; k <= q; k++)
+          for (int j = q; j >= k; j--)
+            for (int i = 0; i < N; i++) dz(j - 1)[i] += sg * dz(j)[i];
+        break;
+      }
+      case TP_CORRECT: {
+        const int q = (int)r[1];
+        const double gam = r[2], rl1 = r[3];
+        const double* l = r + 4;
+        const bool save = r[4 + L_MAX] != 0.0;
+        const double* yn = r + 5 + L_MAX;
+        adjoint_jac_(P, yn, J.data(), yp.data(), fp.data(), fq.data());
+        fm_dm(yn, fm.data());
+        for (int i = 0; i < N; i++) {
+          double t = gam * fm[i] - rl1 * dz(1)[i];
+          for (int j = 0; j < N; j++) t += gam * J[i + (long)j * N] * dz(0)[j];
+          b[i] = t;
+        }
+        for (int j = 0; j < N; j++)
+          for (int i = 0; i < N; i++)
+            A[i + (long)j * N] = (i == j ? 1.0 : 0.0) - gam * J[i + (long)j * N];
+        getrf_(A.data(), N, piv.data());
+        getrs_(A.data(), N, piv.data(), b.data());
+        for (int j = 0; j <= q; j++)
+          for (int i = 0; i < N; i++) dz(j)[i] += l[j] * b[i];
+        if (save)
+          for (int i = 0; i < N; i++) dz(QMAX)[i] = b[i];
+        break;
+      }
+      case TP_DKY: {
+        const double sv = r[1];
+        const int q = (int)r[2];
+        for (int i = 0; i < N; i++) dyf[i] = 0.0;
+        for (int j = 0; j <= q; j++) {
+          double c = 1.0;
+          for (int i = 0; i < j; i++) c *= sv;
+          for (int i = 0; i < N; i++) dyf[i] += c * dz(j)[i];
+        }
+        break;
+      }
+    }
+    pos += len;
+  }
+}
+}  // namespace
+
+// one cell's tangent dy_final for the perturbation (dy0, dm), from the tape
+// of its forward solve (lnm one row as in oracle_adjoint_cells): the test of
+// the reverse sweep's transposition, <lam, dy_final> = <lam_y0, dy0> +
+// <gm, dm>
+ORACLE_API int oracle_tangent_one(double* n, double* Tgas, const double* dt,
+                                  const double* par, const double* lnm,
+                                  const double* dy0, const double* dm,
+                                  double* dyf, const oracle_opts* so) {
+  double mult[NREA + 1];
+  for (int r = 0; r < NREA; ++r) mult[r] = lnm != nullptr ? std::exp(lnm[r]) : 1.0;
+  const int N = NSPEC + (so->evolve_T ? 1 : 0);
+  std::vector<double> tape, yfin(N);
+  const double T0 = *Tgas;
+  const int fl = solve_one_(n, Tgas, par, *dt, so, nullptr, mult, &tape, yfin.data());
+  if (fl != 0) return fl;
+  Problem P;
+  P.mult = mult;
+  params_from_row(par, P.p);
+  P.Tfix = T0;
+  P.NEQ = NSPEC;
+  if (so->evolve_T) P.iT = P.NEQ++;
+  tangent_sweep_(P, tape, dy0, dm, dyf);
+  return 0;
+}
+
+ORACLE_API int oracle_solve_one(double* n, double* Tgas, const double* par, double dt,
+                     const oracle_opts* so, long* stats) {
+  return solve_one_(n, Tgas, par, dt, so, stats, nullptr, nullptr, nullptr);
+}
+
+// the discrete adjoint, cell by cell: the forward solve with the rate
+// multipliers exp(lnm) (lnm one row of NREA broadcast, lnm_stride 0, or
+// rows; null: all 0) recording its tape, then the reverse sweep seeded with
+// gn[ncell][nspec], gT[ncell]: the gradient of
+// sum(gn * n_out) + sum(gT * Tgas_out) with respect to the initial n
+// (dn0), Tgas (dT0, evolve_T) and the ln-multipliers (dm[ncell][nrea]).
+// n, Tgas are updated as by oracle_solve_cells; a failed cell's gradients
+// are 0. Returns the lowest-index failing cell's flag.
+ORACLE_API int oracle_adjoint_cells(int ncell, double* n, double* Tgas,
+                                    const double* dt, const double* par,
+                                    int par_stride, const double* lnm,
+                                    int lnm_stride, const double* gn,
+                                    const double* gT, int* flags,
+                                    const oracle_opts* so, double* dn0,
+                                    double* dT0, double* dm, long* stats,
+                                    int nthreads) {
+  if (ncell < 0 || n == nullptr || Tgas == nullptr || dt == nullptr
+      || so == nullptr || gn == nullptr || dn0 == nullptr || dm == nullptr
+      || (par_stride != 0 && par_stride != NPAR)
+      || (lnm_stride != 0 && lnm_stride != NREA))
+    return -1;
+  std::vector<int> fl(ncell, 0);
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int c = 0; c < ncell; ++c) {
+    const double* row = par + (long)c * par_stride;
+    double mult[NREA + 1];
+    for (int r = 0; r < NREA; ++r)
+      mult[r] = lnm != nullptr ? std::exp(lnm[(long)c * lnm_stride + r]) : 1.0;
+    const int N = NSPEC + (so->evolve_T ? 1 : 0);
+    double* gmc = dm + (long)c * NREA;
+    for (int r = 0; r < NREA; ++r) gmc[r] = 0.0;
+    for (int i = 0; i < NSPEC; ++i) dn0[(long)c * NSPEC + i] = 0.0;
+    if (dT0 != nullptr) dT0[c] = 0.0;
+    if (!(dt[c] > 0.0)) continue;
+    std::vector<double> tape, yfin(N), lam_y(N), lam0(N);
+    long* sc = stats != nullptr ? stats + (long)c * ORACLE_NSTAT : nullptr;
+    const double T0 = Tgas[c];
+    fl[c] = solve_one_(n + (long)c * NSPEC, Tgas + c, row, dt[c], so, sc, mult,
+                       &tape, yfin.data());
+    if (fl[c] != 0) continue;
+    Problem P;
+    P.mult = mult;
+    params_from_row(row, P.p);
+    P.Tfix = T0;
+    P.NEQ = NSPEC;
+    if (so->evolve_T) P.iT = P.NEQ++;
+    for (int i = 0; i < NSPEC; ++i) {
+      const bool clipped = so->clip_negative && yfin[i] < 0.0;
+      lam_y[i] = clipped ? 0.0 : gn[(long)c * NSPEC + i];
+    }
+    if (P.iT >= 0) lam_y[P.iT] = gT != nullptr ? gT[c] : 0.0;
+    adjoint_sweep_(P, tape, lam_y.data(), lam0.data(), gmc);
+    for (int i = 0; i < NSPEC; ++i) dn0[(long)c * NSPEC + i] = lam0[i];
+    if (dT0 != nullptr && P.iT >= 0) dT0[c] = lam0[P.iT];
+  }
+  int ret = 0;
+  for (int c = 0; c < ncell; ++c) {
+    if (flags != nullptr) flags[c] = fl[c];
+    if (ret == 0 && fl[c] != 0) ret = fl[c];
+  }
+  return ret;
 }
 
 // many cells (solve_cells.hpp:47-161): the required-parameter rule over

@@ -76,6 +76,52 @@ class Oracle:
         self.seconds = time.perf_counter() - t0
         return dict(n=n, T=T, flags=flags, stats=stats, ret=ret)
 
+    def adjoint(self, n, T, dt, par, gn, gT, lnm=None, evolve_T=1, jac=0,
+                rtol=1e-6, atol_n=1e-20, atol_T=1e-6, max_steps=100000,
+                max_err_fails=7, max_conv_fails=10, max_restarts=5,
+                clip_negative=1, lu32=0, threads=None, **_):
+        """the discrete adjoint (oracle_adjoint_cells): the forward solve
+        with rate multipliers exp(lnm) and the gradient of
+        sum(gn * n_out) + sum(gT * T_out) w.r.t. n0, T0 and lnm"""
+        lib = self.lib
+        if not getattr(self, "_adj", False):
+            lib.oracle_adjoint_cells.restype = ctypes.c_int
+            lib.oracle_adjoint_cells.argtypes = [
+                ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _D, ctypes.c_int,
+                _D, _D, _I, ctypes.POINTER(_Opts), _D, _D, _D, _L,
+                ctypes.c_int]
+            self._adj = True
+        n = np.array(n, dtype=float, order="C", copy=True)
+        T = np.array(T, dtype=float, order="C", copy=True)
+        dt = np.ascontiguousarray(dt, dtype=float)
+        par = np.ascontiguousarray(par, dtype=float)
+        gn = np.ascontiguousarray(gn, dtype=float)
+        gT = np.ascontiguousarray(gT, dtype=float)
+        ncell = n.shape[0]
+        nrea = lib.oracle_nrea()
+        stride = 0 if par.ndim == 1 else self.npar
+        lstride = 0
+        if lnm is not None:
+            lnm = np.ascontiguousarray(lnm, dtype=float)
+            lstride = 0 if lnm.ndim == 1 else nrea
+        flags = np.zeros(ncell, dtype=np.intc)
+        stats = np.zeros((ncell, NSTAT), dtype=np.int64)
+        dn0 = np.zeros((ncell, self.nspec))
+        dT0 = np.zeros(ncell)
+        dm = np.zeros((ncell, nrea))
+        o = _Opts(int(evolve_T), int(jac), rtol, atol_n, atol_T,
+                  int(max_steps), max_err_fails, max_conv_fails,
+                  max_restarts, int(clip_negative), int(lu32))
+        nt = threads or os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ret = lib.oracle_adjoint_cells(
+            ncell, _ptr(n), _ptr(T), _ptr(dt), _ptr(par), stride, _ptr(lnm),
+            lstride, _ptr(gn), _ptr(gT), _ptr(flags, _I), ctypes.byref(o),
+            _ptr(dn0), _ptr(dT0), _ptr(dm), _ptr(stats, _L), nt)
+        self.seconds = time.perf_counter() - t0
+        return dict(n=n, T=T, flags=flags, stats=stats, ret=ret, dn0=dn0,
+                    dT0=dT0, dm=dm)
+
 
 class Reference:
     """the reference's krome_solve_cells (its generated C ABI)"""
