@@ -22,6 +22,20 @@ exists for this path). A step is 262,144 cell-solves.
   cpu_baseline  the reference's own krome_solve_cells (compiled from its
             sources with OpenMP, oracle/_ref) on the host cores, on a sample
             of the same loop
+  forms     (N = 1) the other two forms, each on its own workload:
+            adjoint    the differentiation workload: 65,536 primordial cells
+                       (cooling ATOMIC, H2; heating CHEM, COMPRESS; rtol 1e-6),
+                       the plain solve, the recording solve and the reverse
+                       sweep of the discrete adjoint (gradients of x_H2 and
+                       Tgas w.r.t. n0, T0 and every ln k), device-timed
+            precision  the precision workload: 131,072 galaxy_ism cells, the
+                       Newton matrix factored in FP64 and in FP32 (FP64
+                       refactor after Newton failures): cell-solves/s, the
+                       FP64 refactors, and each form's error against the
+                       rtol 1e-12 FP64 solve (the fraction of cells whose
+                       abundances above atol/rtol and Tgas are within
+                       10 rtol, the median and p99 of the cell's largest
+                       relative error)
 
 ``python bench.py --gpus N --steps K --warmup W [--impl reference]``; with
 N > 1 each rank (torchrun) solves its own 262,144 cells (weak scaling: no
@@ -57,6 +71,8 @@ def parse():
     ap.add_argument("--cpu-cells", type=int, default=8192,
                     help="cells of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the adjoint and precision forms")
     return ap.parse_args()
 
 
@@ -232,6 +248,121 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # this library's leg
 
+def _events(torch):
+    e = torch.cuda.Event(enable_timing=True)
+    e.record()
+    return e
+
+
+def adjoint_form(torch, dev, reps=3):
+    """the discrete adjoint's cost on the differentiation workload"""
+    from krome_x_b200 import autograd, krome, netinfo, workloads
+    key, N = "primordial", 65536
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.primordial(N, info, seed=0)
+    net = krome.load(key)
+    o = workloads.OPTIONS[key]
+    opts = net.options(evolve_T=o["evolve_T"], jac=o["jac"], rtol=o["rtol"],
+                       atol_n=o["atol_n"], atol_T=o["atol_T"])
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    sp = info["species"]
+    w = np.array([{"H": 1, "H+": 1, "H-": 1, "H2": 2, "H2+": 2, "HD": 1}
+                  .get(x, 0) for x in sp], dtype=float)
+    nH = t(n @ w)
+    best = None
+    for _ in range(reps):
+        nd, Td = t(n), t(T)
+        fl = torch.zeros(N, dtype=torch.int32, device=dev)
+        cur = torch.zeros(1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        e0 = _events(torch)
+        net.solve_device(nd, Td, t(dt), t(par), fl, opts=opts, cursor=cur)
+        e1 = _events(torch)
+        torch.cuda.synchronize()
+        plain = e0.elapsed_time(e1)
+        n0, T0 = t(n).requires_grad_(), t(T).requires_grad_()
+        m = torch.zeros(net.nrea, dtype=torch.float64, device=dev,
+                        requires_grad=True)
+        torch.cuda.synchronize()
+        e0 = _events(torch)
+        nout, Tout, flags = autograd.solve(net, n0, T0, m, t(dt), t(par), opts)
+        e1 = _events(torch)
+        loss = (nout[:, sp.index("H2")] / nH).sum() + Tout.sum()
+        e2 = _events(torch)
+        loss.backward()
+        e3 = _events(torch)
+        torch.cuda.synchronize()
+        rec, rev = e0.elapsed_time(e1), e2.elapsed_time(e3)
+        r = (plain, rec, rev, int((flags != 0).sum()))
+        if best is None or r[1] + r[2] < best[1] + best[2]:
+            best = r
+    plain, rec, rev, failed = best
+    return {"workload": "primordial, 65,536 cells, rtol 1e-6, outputs x_H2 "
+                        "and Tgas, inputs n0, T0 and all %d ln k" % net.nrea,
+            "plain_forward_ms": plain, "recording_forward_ms": rec,
+            "reverse_sweep_ms": rev, "reverse_over_forward": rev / plain,
+            "gradient_over_forward": (rec + rev) / plain,
+            "failed_cells": failed, "reps": reps}
+
+
+def precision_form(torch, dev):
+    """FP64 and FP32 Newton-matrix factorisations on the precision workload,
+    against the rtol 1e-12 FP64 solve"""
+    from krome_x_b200 import krome, netinfo, workloads
+    key, N = "galaxy_ism", 131072
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.galaxy_ism(N, info, seed=0)
+    net = krome.load(key)
+    o = workloads.OPTIONS[key]
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+
+    def run(rtol, lu32):
+        opts = net.options(evolve_T=o["evolve_T"], jac=o["jac"], rtol=rtol,
+                           atol_n=o["atol_n"], atol_T=o["atol_T"], lu32=lu32,
+                           max_steps=2000000)
+        nd, Td = t(n), t(T)
+        fl = torch.zeros(N, dtype=torch.int32, device=dev)
+        st = torch.zeros((N, len(STAT_NAMES)), dtype=torch.int64, device=dev)
+        cur = torch.zeros(1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        e0 = _events(torch)
+        net.solve_device(nd, Td, t(dt), t(par), fl, opts=opts, stats=st,
+                         cursor=cur)
+        e1 = _events(torch)
+        torch.cuda.synchronize()
+        return (nd.cpu().numpy(), Td.cpu().numpy(), fl.cpu().numpy(),
+                st.cpu().numpy(), e0.elapsed_time(e1))
+    ref = run(1e-12, 0)
+
+    def error(res):
+        nn, TT, fl, _, _ = res
+        ok = (fl == 0) & (ref[2] == 0)
+        big = np.abs(ref[0][ok]) > o["atol_n"] / o["rtol"]
+        with np.errstate(all="ignore"):
+            rel = np.where(big, np.abs(nn[ok] - ref[0][ok]) / np.abs(ref[0][ok]),
+                           0.0).max(axis=1)
+        relT = np.abs(TT[ok] - ref[1][ok]) / np.abs(ref[1][ok])
+        e = np.maximum(rel, relT)
+        return {"cells_within_10rtol": float((e <= 10 * o["rtol"]).mean()),
+                "median_rel_err": float(np.median(e)),
+                "p99_rel_err": float(np.quantile(e, 0.99)),
+                "failed_cells": int((fl != 0).sum())}
+    out = {"workload": "galaxy_ism, 131,072 cells, rtol 1e-6, dt 3.15e11 s",
+           "reference": "the FP64 solve at rtol 1e-12 on the GPU",
+           "reference_ms": ref[4]}
+    for name, lu32 in (("fp64", 0), ("lu32", 1)):
+        runs = [run(o["rtol"], lu32) for _ in range(3)]
+        best = min(runs, key=lambda r: r[4])
+        d = {"cell_solves_per_s": N / (best[4] * 1e-3), "ms": best[4]}
+        d.update(error(best))
+        if lu32:
+            d["fp64_refactors"] = int(best[3][:, STAT_NAMES.index("nlu64")].sum())
+            d["cells_with_refactor"] = int(
+                (best[3][:, STAT_NAMES.index("nlu64")] > 0).sum())
+        out[name] = d
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -341,6 +472,10 @@ def run_ours(args, rank, world, local):
     h2d = n.nbytes + T.nbytes + dt.nbytes + par.nbytes
     d2h = n.nbytes + T.nbytes + 4 * ncell
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = {"adjoint": adjoint_form(torch, dev),
+                 "precision": precision_form(torch, dev)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_leg(args.cpu_cells, args.warmup, args.steps)
@@ -384,6 +519,8 @@ def run_ours(args, rank, world, local):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if forms is not None:
+        line["forms"] = forms
     print(json.dumps(line), flush=True)
 
 

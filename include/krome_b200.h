@@ -171,7 +171,8 @@ int krome_b200_adjoint_record_device(int ncell, double* n, double* Tgas,
                                      long tape_cap, long* tape_len,
                                      double* yfin, const krome_opts* h,
                                      void* stream);
-/* ... and the reverse sweep over those tapes (T0: the initial Tgas) */
+/* ... and the reverse sweep over those tapes (T0: the initial Tgas;
+ * cursor: one unsigned, the sweep's work queue, reset by the call) */
 int krome_b200_adjoint_device(int ncell, const double* T0, const double* par,
                               int par_stride, const double* mult,
                               int mult_stride, const double* gn,
@@ -179,7 +180,8 @@ int krome_b200_adjoint_device(int ncell, const double* T0, const double* par,
                               const double* tape, long tape_cap,
                               const long* tape_len, const double* yfin,
                               double* dn0, double* dT0, double* dm,
-                              const krome_opts* h, void* stream);
+                              unsigned* cursor, const krome_opts* h,
+                              void* stream);
 
 /* krome_solve_cells for callers that cannot let the library allocate device
  * memory -- a code that gives the whole GPU to its own memory pool, or a

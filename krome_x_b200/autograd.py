@@ -53,7 +53,7 @@ class _Solve(torch.autograd.Function):
         if r != 0:
             raise krome.KromeError("adjoint forward: %d (%s)"
                                    % (r, net.flag_message(r)))
-        ctx.save_for_backward(T0c, P, mult, flags, tape, tlen, yfin)
+        ctx.save_for_backward(T0c, P, mult, flags, tape, tlen, yfin, cursor)
         ctx.net, ctx.opts, ctx.cap = net, opts, tape_cap
         ctx.pstride, ctx.mstride = pstride, mstride
         ctx.mark_non_differentiable(flags)
@@ -61,7 +61,7 @@ class _Solve(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, gn, gT, _gflags):
-        T0c, P, mult, flags, tape, tlen, yfin = ctx.saved_tensors
+        T0c, P, mult, flags, tape, tlen, yfin, cursor = ctx.saved_tensors
         net = ctx.net
         N = int(T0c.shape[0])
         dev = T0c.device
@@ -77,8 +77,8 @@ class _Solve(torch.autograd.Function):
             N, T0c.data_ptr(), P.data_ptr(), ctx.pstride, mult.data_ptr(),
             ctx.mstride, gn.data_ptr(), gT.data_ptr(), flags.data_ptr(),
             tape.data_ptr(), ctx.cap, tlen.data_ptr(), yfin.data_ptr(),
-            dn0.data_ptr(), dT0.data_ptr(), dm.data_ptr(), ctx.opts._h,
-            stream)
+            dn0.data_ptr(), dT0.data_ptr(), dm.data_ptr(), cursor.data_ptr(),
+            ctx.opts._h, stream)
         if r != 0:
             raise krome.KromeError("adjoint backward: %d" % r)
         dlnm = dm if ctx.mstride else dm.sum(0)

@@ -865,25 +865,31 @@ KB_API int krome_b200_adjoint_device(
     const double* mult, int mult_stride, const double* gn, const double* gT,
     const int* flags, const double* tape, long tape_cap,
     const long* tape_len, const double* yfin, double* dn0, double* dT0,
-    double* dm, const krome_opts* h, void* stream) {
+    double* dm, unsigned* cursor, const krome_opts* h, void* stream) {
   if (h == nullptr || ncell < 0) return -1;
   if (ncell == 0) return 0;
   if (T0 == nullptr || par == nullptr || gn == nullptr || flags == nullptr
       || tape == nullptr || tape_len == nullptr || yfin == nullptr
-      || dn0 == nullptr || dm == nullptr || tape_cap <= 0)
+      || dn0 == nullptr || dm == nullptr || cursor == nullptr || tape_cap <= 0)
     return -1;
   if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
   if (mult_stride != 0 && mult_stride != kbnet::NREA) return -1;
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int blocks = (ncell + 127) / 128;
-  if (h->evolve_T)
-    kba::kb_adjoint_cells<true><<<blocks, 128, 0, st>>>(
-        ncell, T0, par, par_stride, mult, mult_stride, gn, gT, flags, tape,
-        tape_cap, tape_len, yfin, h->clip_negative, dn0, dT0, dm);
-  else
-    kba::kb_adjoint_cells<false><<<blocks, 128, 0, st>>>(
-        ncell, T0, par, par_stride, mult, mult_stride, gn, gT, flags, tape,
-        tape_cap, tape_len, yfin, h->clip_negative, dn0, dT0, dm);
+  auto kern = h->evolve_T ? kba::kb_adjoint_cells<true>
+                          : kba::kb_adjoint_cells<false>;
+  // a persistent grid over the work queue
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0);
+  if (per_sm <= 0) per_sm = 1;
+  long blocks = (long)num_sms() * per_sm;
+  const long need = ((long)ncell + 127) / 128;
+  if (blocks > need) blocks = need;
+  if (cudaMemsetAsync(cursor, 0, sizeof(unsigned), st) != cudaSuccess)
+    return -104;
+  kern<<<(int)blocks, 128, 0, st>>>(ncell, T0, par, par_stride, mult,
+                                    mult_stride, gn, gT, flags, tape, tape_cap,
+                                    tape_len, yfin, h->clip_negative, dn0, dT0,
+                                    dm, cursor);
   return cudaGetLastError() == cudaSuccess ? 0 : -104;
 }
 
@@ -982,7 +988,8 @@ KB_API int krome_b200_adjoint(int ncell, double* n, double* Tgas,
     r = krome_b200_adjoint_device(ncell, dT0v, dpar, ps,
                                   mrows > 0 ? dmult : nullptr,
                                   mrows > 1 ? NREA : 0, dgn, dgT, dfl, dtape,
-                                  cap, dlen, dyf, ddn0, ddT0, ddm, h, nullptr);
+                                  cap, dlen, dyf, ddn0, ddT0, ddm, dcur, h,
+                                  nullptr);
   if (r == 0 && cudaDeviceSynchronize() != cudaSuccess) r = -104;
   if (r == 0) {
     cudaMemcpy(n, dn, nd * sizeof(double), cudaMemcpyDeviceToHost);

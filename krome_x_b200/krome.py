@@ -177,7 +177,7 @@ class Network:
             "krome_b200_adjoint_device": (ctypes.c_int, [
                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                 ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4
-                + [ctypes.c_long] + [ctypes.c_void_p] * 7),
+                + [ctypes.c_long] + [ctypes.c_void_p] * 8),
         }
         for name, (res, args) in proto.items():
             fn = getattr(lib, name)

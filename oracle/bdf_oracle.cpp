@@ -1210,23 +1210,39 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
 
 // dF/dy at y for the adjoint, column-major: the stoichiometric block where
 // it is exact (rates independent of the densities: the block at fixed k is
-// dF/dn) with central differences for the Tgas column and row, else central
-// differences on every column
+// dF/dn), a central difference for the Tgas column and forward differences
+// (fd_step_n) for the Tgas row; else central differences on every column
 void adjoint_jac_(Problem& P, const double* y, double* J, double* yp,
                   double* fp, double* fq) {
   const int N = P.NEQ;
   for (long k = 0; k < (long)N * N; ++k) J[k] = 0.0;
   for (int i = 0; i < N; ++i) yp[i] = y[i];
-  const bool analytic = !RATES_DEPEND_ON_N;
-  if (analytic) {
+  if (!RATES_DEPEND_ON_N) {
     P.eval_rates(P.state_T(y), y, P.k0);
     jac_stoich(y, P.k0, J, 1, N);
     if (P.iT < 0) return;
+    const int t = P.iT;
+    {
+      const double h = std::fmax(1e-6 * std::fabs(y[t]), 1e-8);
+      yp[t] = y[t] + h;
+      P.full_rhs(yp, fp);
+      yp[t] = y[t] - h;
+      P.full_rhs(yp, fq);
+      yp[t] = y[t];
+      for (int i = 0; i < N; ++i) J[i + (long)t * N] = (fp[i] - fq[i]) / (2.0 * h);
+    }
+    P.full_rhs(y, fq);
+    const double f0 = fq[t];
+    for (int j = 0; j < NSPEC; ++j) {
+      const double h = Problem::fd_step_n(y, j);
+      yp[j] = y[j] + h;
+      P.full_rhs(yp, fp);
+      yp[j] = y[j];
+      J[t + (long)j * N] = (fp[t] - f0) / h;
+    }
+    return;
   }
   for (int j = 0; j < N; ++j) {
-    // with n-independent rates only the Tgas column and the Tgas row
-    // need differences (central, as every column otherwise)
-    const bool row_only = analytic && j != P.iT;
     const double h = j == P.iT ? std::fmax(1e-6 * std::fabs(y[j]), 1e-8)
                                : Problem::fd_step_n(y, j);
     yp[j] = y[j] + h;
@@ -1234,11 +1250,7 @@ void adjoint_jac_(Problem& P, const double* y, double* J, double* yp,
     yp[j] = y[j] - h;
     P.full_rhs(yp, fq);
     yp[j] = y[j];
-    if (row_only) {
-      J[P.iT + (long)j * N] = (fp[P.iT] - fq[P.iT]) / (2.0 * h);
-    } else {
-      for (int i = 0; i < N; ++i) J[i + (long)j * N] = (fp[i] - fq[i]) / (2.0 * h);
-    }
+    for (int i = 0; i < N; ++i) J[i + (long)j * N] = (fp[i] - fq[i]) / (2.0 * h);
   }
 }
 
