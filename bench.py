@@ -57,6 +57,12 @@ sys.path.insert(0, str(ROOT))
 
 NETWORK = "primordial3"
 RTOL = 1e-6
+# DRAM bytes (read + write) the solve kernel moves per cell-solve in a
+# hydro-loop call: one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the third call of a 3-call primordial3 collapse
+# loop on 65,536 cells, 19.38 GB in one launch; the traffic grows with the
+# cells solved, so a launch of this benchmark moves this x its cells
+TRAFFIC_PER_CELL_SOLVE = 19.38e9 / 65536
 from krome_x_b200.krome import STAT_NAMES  # the per-cell counters' columns
 
 
@@ -509,7 +515,9 @@ def run_ours(args, rank, world, local):
                 "steps": e2e_steps, "failed_cell_solves": e2e_failed},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None,
+                     "traffic": TRAFFIC_PER_CELL_SOLVE * ncell,
+                     "traffic_unit": "bytes per launch (ncu, scaled from "
+                                     "65,536 cells by the cells solved)",
                      "peak_source": "measured live: DFMA chains over all SMs",
                      "work": "per cell-solve %.4g flops (special functions "
                              "counted 1 each: %.4g per cell-solve)"
