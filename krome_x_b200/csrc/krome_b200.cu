@@ -30,6 +30,7 @@
 #include "bdf_warp.cuh"
 #include "bdf_lane.cuh"
 #include "adjoint.cuh"
+#include "bdf_big.cuh"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
 
@@ -46,8 +47,10 @@ struct Geo {
   // per-warp shared memory: the saved Jacobian and two columns
   static constexpr int SMEM_DOUBLES = N * N + 2 * N;
 };
+#ifndef KB_LARGE_NETWORK
 static_assert(kbnet::NSPEC + 3 <= 32,
               "warp-per-cell kernels need NEQ + 2 <= 32 lanes");
+#endif
 
 template <bool EVT>
 __device__ __forceinline__ void one_cell(int c, double* n, double* T,
@@ -450,6 +453,92 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
   }
 }
 
+#ifdef KB_LARGE_NETWORK
+// ---- the large networks: one warp per cell (bdf_big.cuh) ----
+
+// cell c on this warp: the pre-solve rules, the restart wrapper
+// (bdf_cell.hpp:1513-1547) and the post-solve rules (solve_cell.hpp:
+// 2094-2203) around the sparse-path CVODE, fixed Tgas
+__device__ void big_one_cell(int c, double* n, double* T, const double* dt,
+                             const double* par, int pstride, int* flags,
+                             long* stats, const SolveOpts& so, double* ws) {
+  using namespace kbnet;
+  const int lane = threadIdx.x & 31;
+  int flag = 1;
+  if (so.fail_every > 0 && (c + 1) % so.fail_every == 0) flag = kbw::TOO_MUCH_WORK;
+  else if (!(dt[c] > 0.0)) flag = 0;
+  kbg::Net P;
+  P.ws = ws;
+  params_from_row(par + (long)c * pstride, P.p);
+  if (flag == 1 && params_missing(P.p) >= 0) flag = kbw::FLAG_PARAM_UNSET;
+  long tot[kbw::NSTAT];
+  for (int i = 0; i < kbw::NSTAT; ++i) tot[i] = 0;
+  if (flag == 1) {
+    P.T = fmin(fmax(T[c], P.p.Tcmb), 1e9);
+    double* nrow = n + (long)c * NSPEC;
+    double* k = ws + kbg::WS::K;
+    for (int r = lane; r <= NREA; r += 32) k[r] = 0.0;
+    __syncwarp();
+    if (lane == 0) rates_fixed(P.T, nrow, P.p, k);
+    __syncwarp();
+    kbg::BigCvode cv(P, so);
+    double* yout = ws + kbg::WS::YOUT;
+    cv.reinit(0.0, nrow, 0.0);
+    double t = 0.0;
+    int restarts = 0;
+    for (;;) {  // bounded by max_restarts
+      const int f = cv.solve(dt[c], yout, &t);
+      tot[kbw::ST_NST] += cv.st.nst;
+      tot[kbw::ST_NFE] += cv.st.nfe;
+      tot[kbw::ST_NJE] += cv.st.nje;
+      tot[kbw::ST_NSETUPS] += cv.st.nsetups;
+      tot[kbw::ST_NNI] += cv.st.nni;
+      tot[kbw::ST_NNF] += cv.st.nnf;
+      tot[kbw::ST_NETF] += cv.st.netf;
+      if (f >= 0) { flag = 0; break; }
+      const bool restartable = f == kbw::ERR_FAILURE || f == kbw::CONV_FAILURE
+                               || f == kbw::REPTD_RHSFUNC_ERR;
+      if (!restartable || restarts >= so.max_restarts) { flag = f; break; }
+      ++restarts;
+      const double hcur = cv.next_h;
+      cv.reinit(t, yout, hcur > 0.0 ? 0.1 * hcur : 0.0);
+    }
+    tot[kbw::ST_RESTARTS] = restarts;
+    if (flag == 0) {
+      for (int i = lane; i < NSPEC; i += 32) {
+        double v = yout[i];
+        if (so.clip_negative && v < 0.0) v = 0.0;
+        nrow[i] = v;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (flags != nullptr) flags[c] = flag;
+    if (stats != nullptr)
+      for (int i = 0; i < kbw::NSTAT; ++i) stats[(long)c * kbw::NSTAT + i] = tot[i];
+  }
+}
+
+// warps take cells from the work queue `cursor`; each resident warp owns
+// the workspace slot of its global warp index (kbg::WS::SIZE doubles)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+kb_big_cells(int ncell, double* n, double* T, const double* dt,
+             const double* par, int pstride, int* flags, long* stats,
+             SolveOpts so, unsigned* cursor, double* ws_base) {
+  const int lane = threadIdx.x & 31;
+  const long wg = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double* ws = ws_base + wg * kbg::WS::SIZE;
+  for (;;) {  // at most ncell + 1 pops per warp: the cursor only grows
+    unsigned c0 = 0;
+    if (lane == 0) c0 = atomicAdd(cursor, 1u);
+    const int c = (int)__shfl_sync(0xffffffffu, c0, 0);
+    if (c >= ncell) break;
+    big_one_cell(c, n, T, dt, par, pstride, flags, stats, so, ws);
+  }
+}
+#endif
+
 // ---- options (krome_opts keys, reference krome.cpp:198-300) ----
 }  // namespace
 
@@ -534,12 +623,53 @@ int num_sms() {
   return g_num_sms;
 }
 
+#ifdef KB_LARGE_NETWORK
+// the large networks' per-warp workspace: one device buffer, grown to
+// `warps` slots when it is smaller (a cudaMalloc: not inside a stream
+// capture, so graph_new grows it before capturing)
+std::mutex g_ws_mu;
+DevBuf g_ws;
+double* big_workspace(long warps) {
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  const size_t bytes = (size_t)warps * kbg::WS::SIZE * sizeof(double);
+  if (g_ws.p != nullptr && g_ws.cap >= bytes) return (double*)g_ws.p;
+  if (g_ws.ensure(bytes) != cudaSuccess) return nullptr;
+  return (double*)g_ws.p;
+}
+#endif
+
 template <bool EVT>
 cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    const double* dt, const double* par, int pstride,
                    int* flags, long* stats, unsigned* cursor,
                    cudaStream_t stream, const RecIO* rio = nullptr) {
   const SolveOpts so = to_solve_opts(h);
+#ifdef KB_LARGE_NETWORK
+  // the sparse path: one warp per cell over a persistent grid, each warp
+  // with its workspace slot (the library's device buffer, grown before a
+  // launch when needed; never during a graph capture: big_workspace)
+  (void)rio;
+  if (EVT) return cudaErrorNotSupported;
+  {
+    const int threads = kWarpsPerBlock * 32;
+    int per_sm = h.blocks_per_sm;
+    if (per_sm <= 0) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_big_cells,
+                                                    threads, 0);
+      if (per_sm <= 0) per_sm = 1;
+    }
+    long blocks = (long)num_sms() * per_sm;
+    const long need = ((long)ncell + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    double* ws = big_workspace(blocks * kWarpsPerBlock);
+    if (ws == nullptr) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    kb_big_cells<<<(int)blocks, threads, 0, stream>>>(
+        ncell, n, T, dt, par, pstride, flags, stats, so, cursor, ws);
+    return cudaGetLastError();
+  }
+#else
   if (h.layout == 1 || rio != nullptr) {  // lane per cell
     const size_t lsmem =
         sizeof(double) * kWarpsPerBlock * LaneGeo<EVT>::SMEM_DOUBLES;
@@ -595,6 +725,7 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
   kb_cells_persistent<EVT><<<(int)blocks, kWarpsPerBlock * 32, smem, stream>>>(
       ncell, n, T, dt, par, pstride, flags, stats, so, cursor, chunk);
   return cudaGetLastError();
+#endif
 }
 
 cudaError_t launch_any(const krome_opts& h, int ncell, double* n, double* T,
@@ -805,9 +936,16 @@ namespace {
 // conservation, photon bins; the FP32 Newton-matrix form exists in the
 // lane layout only
 int unsupported(const krome_opts& h) {
-  if (h.linsol == 2 || h.linsol == 3) return -104;
   if (h.conserve != 0) return -104;
+#ifdef KB_LARGE_NETWORK
+  // the large networks: the sparse LU (linsol auto or sparse), fixed Tgas,
+  // FP64
+  if (h.linsol == 1 || h.linsol == 2) return -104;
+  if (h.evolve_T != 0 || h.lu32 != 0) return -104;
+#else
+  if (h.linsol == 2 || h.linsol == 3) return -104;
   if (h.lu32 != 0 && h.layout != 1) return -104;
+#endif
   return 0;
 }
 }  // namespace
@@ -841,6 +979,12 @@ KB_API int krome_b200_adjoint_record_device(
     long* stats, unsigned* cursor, double* tape, long tape_cap,
     long* tape_len, double* yfin, const krome_opts* h, void* stream) {
   if (h == nullptr || ncell < 0) return -1;
+#ifdef KB_LARGE_NETWORK
+  (void)n; (void)Tgas; (void)dt; (void)par; (void)par_stride; (void)mult;
+  (void)mult_stride; (void)flags; (void)stats; (void)cursor; (void)tape;
+  (void)tape_cap; (void)tape_len; (void)yfin; (void)stream;
+  return -104;  // the adjoint is built for the small (dense) networks
+#else
   if (ncell == 0) return 0;
   if (n == nullptr || Tgas == nullptr || dt == nullptr || par == nullptr
       || flags == nullptr || tape == nullptr || tape_len == nullptr
@@ -858,6 +1002,7 @@ KB_API int krome_b200_adjoint_record_device(
                   : launch<false>(*h, ncell, n, Tgas, dt, par, par_stride,
                                   flags, stats, cursor, st, &rio);
   return e == cudaSuccess ? 0 : -104;
+#endif
 }
 
 KB_API int krome_b200_adjoint_device(
@@ -867,6 +1012,13 @@ KB_API int krome_b200_adjoint_device(
     const long* tape_len, const double* yfin, double* dn0, double* dT0,
     double* dm, unsigned* cursor, const krome_opts* h, void* stream) {
   if (h == nullptr || ncell < 0) return -1;
+#ifdef KB_LARGE_NETWORK
+  (void)T0; (void)par; (void)par_stride; (void)mult; (void)mult_stride;
+  (void)gn; (void)gT; (void)flags; (void)tape; (void)tape_cap;
+  (void)tape_len; (void)yfin; (void)dn0; (void)dT0; (void)dm; (void)cursor;
+  (void)stream;
+  return -104;  // the adjoint is built for the small (dense) networks
+#else
   if (ncell == 0) return 0;
   if (T0 == nullptr || par == nullptr || gn == nullptr || flags == nullptr
       || tape == nullptr || tape_len == nullptr || yfin == nullptr
@@ -891,6 +1043,7 @@ KB_API int krome_b200_adjoint_device(
                                     tape_len, yfin, h->clip_negative, dn0, dT0,
                                     dm, cursor);
   return cudaGetLastError() == cudaSuccess ? 0 : -104;
+#endif
 }
 
 KB_API int krome_b200_adjoint(int ncell, double* n, double* Tgas,
@@ -1244,6 +1397,7 @@ KB_API void krome_b200_graph_free(void* handle) {
 // of its cell `reps` times (each evaluation feeds a negligible increment
 // back into the state, so none can be hoisted); the rhs-throughput bound of
 // the solve kernels
+#ifndef KB_LARGE_NETWORK
 namespace {
 __global__ void kb_rhs_loop(int ncell, const double* n, const double* T,
                             const double* par, int pstride, int reps,
@@ -1266,12 +1420,17 @@ __global__ void kb_rhs_loop(int ncell, const double* n, const double* T,
   if (acc == 1.2345e-300) sink[c] = acc;
 }
 }  // namespace
+#endif
 
 KB_API int krome_b200_rhs_throughput(int ncell, const double* n,
                                      const double* Tgas, const double* par,
                                      int par_stride, int reps,
                                      double* rhs_per_s) {
   if (ncell <= 0 || reps <= 0 || rhs_per_s == nullptr) return -1;
+#ifdef KB_LARGE_NETWORK
+  (void)n; (void)Tgas; (void)par; (void)par_stride;
+  return -104;  // the per-thread rhs of a large network is not a kernel here
+#else
   const size_t nb = sizeof(double) * (size_t)ncell * kbnet::NSPEC;
   const size_t tb = sizeof(double) * (size_t)ncell;
   const size_t pb = sizeof(double) * (size_t)ncell * kbnet::NPAR;
@@ -1302,6 +1461,7 @@ KB_API int krome_b200_rhs_throughput(int ncell, const double* n,
   if (e != cudaSuccess || ms <= 0.0f) return -104;
   *rhs_per_s = (double)ncell * reps / (ms * 1e-3);
   return 0;
+#endif
 }
 
 // the FP64 pipe's peak, measured: independent DFMA chains in registers,
@@ -1401,6 +1561,10 @@ KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
   if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR)
     return -1;
   if (ncell == 0) return 0;
+#ifdef KB_LARGE_NETWORK
+  (void)flags;
+  return -104;  // a large network's solve needs its allocated workspace
+#endif
   double dflt[kbnet::NPAR];
   for (int i = 0; i < kbnet::NPAR; ++i) dflt[i] = kbnet::param_default(i);
   const double* P = par != nullptr ? par : dflt;

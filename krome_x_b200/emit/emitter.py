@@ -39,6 +39,9 @@ import sys
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent.parent
+# the physical constants of csrc/kb_common.h the emitter folds into numbers
+kbc_boltzmann_erg = 1.380649e-16
+kbc_amu = 1.6605390666e-24
 OUTDIR = PKG / "networks"
 
 # the benchmark networks and their generation options (the reference
@@ -51,7 +54,14 @@ NETWORKS = {
                         heating=["COMPRESS", "CHEM"],
                         h2_opacity="RIPAMONTI", gamma="EXACT"),
     "galaxy_ism": dict(network="galaxy_ism", cooling=[], heating=[]),
+    # config 3: the surface options of the reference's cloudSurface test are
+    # required by Semenov.knet (its binding energies)
+    "semenov": dict(options_toml="examples/tests/cloudSurface/options.toml",
+                    network_file="networks/Semenov.knet"),
 }
+# networks above this many species take the sparse path (one warp per cell,
+# the state in HBM, the static-pivot sparse LU)
+LARGE_NSPEC = 32
 
 # H2-chemistry energy ledger of thermal CHEM (reactants, products, eV,
 # thermalized): formation heats by its exothermicity times the HM79
@@ -82,13 +92,17 @@ def _frontend(cfg):
     from kromex import Preprocessor
     import codegen
     import knet
-    kp = Preprocessor(network=cfg["network"])
-    kp.thermal.cooling = cfg.get("cooling", [])
-    kp.thermal.heating = cfg.get("heating", [])
-    if cfg.get("h2_opacity"):
-        kp.thermal.h2_opacity = cfg["h2_opacity"]
-    if cfg.get("gamma"):
-        kp.thermal.gamma = cfg["gamma"]
+    if cfg.get("options_toml"):
+        kp = Preprocessor.from_file(str(ref / cfg["options_toml"]))
+        kp.project.network = str(ref / cfg["network_file"])
+    else:
+        kp = Preprocessor(network=cfg["network"])
+        kp.thermal.cooling = cfg.get("cooling", [])
+        kp.thermal.heating = cfg.get("heating", [])
+        if cfg.get("h2_opacity"):
+            kp.thermal.h2_opacity = cfg["h2_opacity"]
+        if cfg.get("gamma"):
+            kp.thermal.gamma = cfg["gamma"]
     _, args = kp._args("/tmp/kb_emit_unused")
     args.network_file = args.network_pos or args.network
     net = knet.parse_network(args.network_file)
@@ -758,6 +772,465 @@ class Emitter:
         w("}")
         w("")
 
+    # -- grain-surface chemistry ------------------------------------------
+
+    def emit_surface(self):
+        """the surface processes the rates call (adsorption, thermal and
+        cosmic-ray desorption, Langmuir-Hinshelwood two-body reactions),
+        restated from the generator's resolved surface data: binding
+        energies (bare / water ice), barriers, branching and reactive
+        desorption per reaction. One grain population (the network's
+        surface_grains single(n, a2)); the dust temperature the rates see is
+        the Tdust parameter (no dust tables)."""
+        gen, net, w = self.gen, self.net, self.w
+        surfs = getattr(gen, "_surf", None) or []
+        if not surfs:
+            return
+        sg = net.surface_grains
+        if sg is None or sg.get("kind") != "single" or gen.surface_bins:
+            raise NotImplementedError("surface chemistry on binned dust")
+        sp_sorted = self.species
+        base = {x: gen.surf_base(x) for x in sp_sorted}
+        eb = gen._surf_eb
+        ice = [x for x in sp_sorted if net.species[x]["phase"] != "gas"
+               and base[x] == "H2O" and net.species[x]["label"] != "c"]
+        legacy_nu = gen.surface_nu == "LEGACY"
+        w("// ---- grain-surface chemistry (binding energies %s, vibration"
+          % gen.binding_energies)
+        w("// frequency %s, E_diff = %s E_bind, competition %s, tunnelling %s)"
+          % ("1e12 s^-1" if legacy_nu else "sqrt(2 n_s E_b / (pi^2 m))",
+             self.num(gen.FDIFF[gen.binding_energies]),
+             "on" if gen.surface_competition else "off",
+             "on" if gen.surface_tunnelling else "off"))
+        w("namespace surf {")
+        w("constexpr double SITE_AREA = %s;  // [cm^2]" % self.num(gen.SURF_APP2))
+        w("constexpr double FDIFF = %s;" % self.num(gen.FDIFF[gen.binding_energies]))
+        w("// surface sites per volume: 4 pi n_grain a^2 / site area")
+        w("KB_HD inline double sites(const Params& p) {")
+        w("  return 4.0 * kbc::pi * (%s) * (%s) / SITE_AREA;"
+          % (self.cx(sg["n"], "Tgas"), self.cx(sg["a2"], "Tgas")))
+        w("}")
+        w("// water-ice coverage in monolayers, within [0, 1]")
+        w("KB_HD inline double ice_cover(const double* n, double S) {")
+        if ice:
+            w("  if (!(S > 0.0)) return 0.0;")
+            w("  return fmin(fmax(%s / S, 0.0), 1.0);" % self.den(ice[0]))
+        else:
+            w("  (void)n; (void)S;")
+            w("  return 0.0;")
+        w("}")
+        w("KB_HD inline double nu(double mass_g, double Eb) {")
+        if legacy_nu:
+            w("  (void)mass_g; (void)Eb;")
+            w("  return 1e12;")
+        else:
+            w("  return sqrt(2.0 / SITE_AREA * Eb * kbc::boltzmann_erg "
+              "/ (kbc::pi * kbc::pi * mass_g));")
+        w("}")
+        # binding energies per species (bare, ice), a switch for device code
+        w("KB_HD inline void binding(int sp, double& bare, double& icy) {")
+        w("  switch (sp) {")
+        for i, x in enumerate(sp_sorted):
+            e = eb.get(base[x])
+            if e is not None and (e[0] != 0.0 or e[1] != 0.0):
+                w("  case %d: bare = %s; icy = %s; return;"
+                  % (i, self.num(e[0]), self.num(e[1])))
+        w("  default: bare = 0.0; icy = 0.0; return;")
+        w("  }")
+        w("}")
+        w("}  // namespace surf")
+        kinds = {x["kind"] for x in surfs}
+        vth = self.num(math.sqrt(8.0 * kbc_boltzmann_erg / math.pi))
+        if "ads_s" in kinds:
+            w("// adsorption, without the sticking factor [1/s]: the thermal")
+            w("// speed times the grains' cross section pi n a^2 = S site/4")
+            w("KB_HD inline double surf_adsorption_ns(int sp, double binf, "
+              "double Tgas, const double* n, const Params& p) {")
+            w("  (void)binf; (void)n;")
+            w("  return %s * sqrt(Tgas / species_mass_g(sp)) * surf::sites(p) "
+              "* surf::SITE_AREA * 0.25;" % vth)
+            w("}")
+        if "des" in kinds:
+            cr = gen.cr_desorption
+            w("// thermal desorption nu exp(-E/Td) over the bare and the icy")
+            w("// fractions of the surface%s"
+              % (", plus cosmic-ray spot heating (Hasegawa & Herbst 1993:"
+                 if cr else ""))
+            if cr:
+                w("// the 70 K rate times 3.16e-19 %s / 1.3e-17)" % cr)
+            w("KB_HD inline double surf_desorption(int sp, double binf, "
+              "double Tgas, const double* n, const Params& p) {")
+            w("  (void)binf; (void)Tgas;")
+            w("  const double fi = surf::ice_cover(n, surf::sites(p));")
+            w("  double Eb, Ei;")
+            w("  surf::binding(sp, Eb, Ei);")
+            w("  const double m = species_mass_g(sp);")
+            w("  const double vb = surf::nu(m, Eb), vi = surf::nu(m, Ei);")
+            w("  const double Td = p.Tdust;")
+            w("  double k = (1.0 - fi) * vb * exp(-Eb / Td) + fi * vi * exp(-Ei / Td);")
+            if cr:
+                w("  k += 3.16e-19 * p.%s / 1.3e-17 * ((1.0 - fi) * vb * "
+                  "exp(-Eb / 70.0) + fi * vi * exp(-Ei / 70.0));" % cr)
+            w("  return k;")
+            w("}")
+        hbar = gen.HBAR
+        for q, x in enumerate(surfs):
+            if x["kind"] != "2body":
+                continue
+            A, B = x["A"], x["B"]
+            def spc(b):
+                return b if b in net.species else next(
+                    y for y in sp_sorted if base[y] == b)
+            sA, sB = spc(A), spc(B)
+            rx = x["rx"]
+            same = rx["reactants"][0]["sp"] == rx["reactants"][1]["sp"]
+            eA = eb.get(base[sA], (0.0, 0.0))
+            eB = eb.get(base[sB], (0.0, 0.0))
+            if "Ea" in x:
+                Ea = x["Ea"]
+                if Ea <= 0:
+                    prob = "1.0"
+                elif gen.surface_tunnelling:
+                    mA = net.species[sA]["mass_amu"] * kbc_amu
+                    mB = net.species[sB]["mass_amu"] * kbc_amu
+                    mu = mA * mB / (mA + mB)
+                    tun = math.exp(-2.0 * gen.SURF_TUNNEL_A / hbar
+                                   * math.sqrt(2.0 * mu * Ea * kbc_boltzmann_erg))
+                    prob = "fmax(exp(-%s / Td), %s)" % (self.num(Ea), self.num(tun))
+                else:
+                    prob = "exp(-%s / Td)" % self.num(Ea)
+            else:
+                prob = self.num(x["prob"])
+            cdb, cdi = x["cd"]
+            w("// %s: Langmuir-Hinshelwood%s; mode 0 the whole rate, 1 the"
+              % (rx["eq"], ", identical reactants (1/2)" if same else ""))
+            w("// surface branch (1 - f), 2 the desorbing branch (f), f the")
+            w("// reactive desorption fraction")
+            w("KB_HD inline double surf_2body_%d(double mode, double binf, "
+              "double Tgas, const double* n, const Params& p) {" % q)
+            w("  (void)binf; (void)Tgas;")
+            w("  const double S = surf::sites(p);")
+            w("  if (!(S > 0.0)) return 0.0;")
+            w("  const double fi = surf::ice_cover(n, S), fb = 1.0 - fi;")
+            w("  const double Td = p.Tdust;")
+            w("  const double mA = species_mass_g(IDX_%s), mB = species_mass_g(IDX_%s);"
+              % (self.cid(sA), self.cid(sB)))
+            w("  (void)mA; (void)mB;")
+            w("  const double prob = %s;" % prob)
+            w("  auto k1 = [&](double EA, double EB) {")
+            w("    const double nA = surf::nu(mA, EA), nB = surf::nu(mB, EB);")
+            w("    const double hA = nA * exp(-surf::FDIFF * EA / Td);")
+            w("    const double hB = nB * exp(-surf::FDIFF * EB / Td);")
+            if gen.surface_competition:
+                w("    const double Pr = fmax(nA, nB) * prob;")
+                w("    const double den = Pr + hA + hB + nA * exp(-EA / Td) "
+                  "+ nB * exp(-EB / Td);")
+                w("    const double kap = den > 0.0 ? Pr / den : 0.0;")
+            else:
+                w("    const double kap = prob;")
+            w("    return kap * (hA + hB);")
+            w("  };")
+            w("  double k = %s * (fb * k1(%s, %s) + fi * k1(%s, %s)) / S;"
+              % (self.num(x["branch"] * (0.5 if same else 1.0)),
+                 self.num(eA[0]), self.num(eB[0]), self.num(eA[1]), self.num(eB[1])))
+            w("  const double f = fb * %s + fi * %s;" % (self.num(cdb), self.num(cdi)))
+            w("  if (mode == 1.0) k *= 1.0 - f;")
+            w("  else if (mode == 2.0) k *= f;")
+            w("  return k;")
+            w("}")
+        w("")
+
+    # -- the sparse path of large networks ---------------------------------
+
+    NPART = 32  # a warp's lanes: each evaluates one part
+
+    def _rate_units(self, select):
+        """the selected expr reactions as units: singles, and whole
+        piecewise groups"""
+        units, groups = [], {}
+        for rx in self.net.reactions:
+            if rx["rate"]["kind"] != "expr" or not select(rx):
+                continue
+            if rx.get("group") is None:
+                units.append([rx])
+            else:
+                if rx["group"] not in groups:
+                    groups[rx["group"]] = []
+                    units.append(groups[rx["group"]])
+                groups[rx["group"]].append(rx)
+        return units
+
+    def emit_rate_parts(self):
+        """rates_fixed_part / rates_var_part: the rate coefficients split
+        into NPART parts (lane `part` of a warp computes its part)"""
+        gen = self.gen
+        for name, sel in (("fixed", gen.rate_is_fixed),
+                          ("var", lambda rx: not gen.rate_is_fixed(rx))):
+            units = self._rate_units(sel)
+            part_of = {}
+            for u, unit in enumerate(units):
+                for rx in unit:
+                    part_of[rx["id"]] = u % self.NPART
+            self.w("KB_HD inline void rates_%s_part(int part, double Tgas, "
+                   "const double* n, const Params& p, double* k) {" % name)
+            self.w("  (void)Tgas; (void)n; (void)p; (void)k;")
+            self.w("  switch (part) {")
+            for j in range(self.NPART):
+                self.w("  case %d: {" % j)
+                self.emit_grouped(self._rate_body,
+                                  lambda rx, j=j: sel(rx) and part_of.get(rx["id"]) == j)
+                self.w("  } break;")
+            self.w("  default: break;")
+            self.w("  }")
+            self.w("}")
+        self.w("")
+
+    def _sparse_pattern(self):
+        """the Newton matrix I - gamma J over the species: J_ij != 0 where
+        species i takes part in a reaction with kinetic reactant j; plus the
+        diagonal"""
+        idx = self.idx
+        pat = set((i, i) for i in range(len(self.species)))
+        for rx in self.net.reactions:
+            kin = set(idx[s] for s in self._kin(rx))
+            aff = set(idx[r["sp"]] for r in rx["reactants"]) | \
+                set(idx[p0["sp"]] for p0 in rx["products"])
+            for i in aff:
+                for j in kin:
+                    pat.add((i, j))
+        return pat
+
+    @staticmethod
+    def _min_degree(n, pat):
+        """a minimum-degree elimination order of the symmetrised pattern
+        (each elimination joins its neighbours into a clique: the fill)"""
+        import heapq
+        adj = [set() for _ in range(n)]
+        for i, j in pat:
+            if i != j:
+                adj[i].add(j)
+                adj[j].add(i)
+        heap = [(len(adj[v]), v) for v in range(n)]
+        heapq.heapify(heap)
+        alive = set(range(n))
+        order = []
+        while heap:
+            d, v = heapq.heappop(heap)
+            if v not in alive or d != len(adj[v]):
+                continue
+            order.append(v)
+            alive.discard(v)
+            nb = adj[v]
+            for u in nb:
+                adj[u].discard(v)
+                adj[u] |= nb - {u}
+                heapq.heappush(heap, (len(adj[u]), u))
+            adj[v] = set()
+        return order
+
+    @staticmethod
+    def _symbolic_lu(n, rows):
+        """the fill of a row-oriented (IKJ) LU without pivoting: row i gains
+        the upper part of every row k < i it eliminates, in increasing k"""
+        import heapq
+        upper = [None] * n
+        for i in range(n):
+            r = rows[i]
+            ks = [k for k in r if k < i]
+            heapq.heapify(ks)
+            seen = set(ks)
+            while ks:
+                k = heapq.heappop(ks)
+                for j in upper[k]:
+                    if j not in r:
+                        r.add(j)
+                        if j < i and j not in seen:
+                            heapq.heappush(ks, j)
+                            seen.add(j)
+            upper[i] = sorted(j for j in r if j > i)
+        return rows
+
+    def _table(self, name, vals):
+        body = ",".join(str(v) for v in vals)
+        self.w("#define KB_T_%s %s" % (name, body))
+        self.w("inline const int %s[%d] = {KB_T_%s};" % (name, len(vals), name))
+        self.w("#ifdef __CUDACC__")
+        self.w("__device__ const int d_%s[%d] = {KB_T_%s};" % (name, len(vals), name))
+        self.w("#endif")
+        self.w("#undef KB_T_%s" % name)
+
+    def emit_sparse(self):
+        """the static-pivot sparse LU structure (fixed at generation) and
+        the gather forms of the flux, rhs and Jacobian, split into parts"""
+        w = self.w
+        n = len(self.species)
+        idx = self.idx
+        pat = self._sparse_pattern()
+        order = self._min_degree(n, pat)
+        new = {v: k for k, v in enumerate(order)}
+        rows = [set() for _ in range(n)]
+        for i, j in pat:
+            rows[new[i]].add(new[j])
+        rows = self._symbolic_lu(n, rows)
+        rp, ci, di = [0], [], []
+        pos = {}
+        for i in range(n):
+            cols = sorted(rows[i])
+            for j in cols:
+                pos[(i, j)] = len(ci)
+                ci.append(j)
+            di.append(pos[(i, i)])
+            rp.append(len(ci))
+        # the Jacobian's entries (original indices), sorted by their row
+        ent = sorted((i, j) for i, j in pat if True)
+        eidx = {e: k for k, e in enumerate(ent)}
+        jpos = [pos[(new[i], new[j])] for i, j in ent]
+        self.meta["nnz_lu"] = len(ci)
+        self.meta["nnz_j"] = len(ent)
+        w("// ---- the sparse path: static-pivot LU of I - gamma J ----")
+        w("// rows / columns in the elimination order sp_perm (a minimum-degree")
+        w("// order of the symmetrised pattern); the pattern includes the fill")
+        w("#define KB_LARGE_NETWORK 1")
+        w("constexpr int NNZ_LU = %d;" % len(ci))
+        w("constexpr int NNZ_J = %d;" % len(ent))
+        w("constexpr int NPART = %d;" % self.NPART)
+        self._table("sp_rp", rp)
+        self._table("sp_ci", ci)
+        self._table("sp_di", di)
+        self._table("sp_perm", order)
+        self._table("sp_iperm", [new[v] for v in range(n)])
+        self._table("sp_jpos", jpos)
+        w("")
+        P = self.NPART
+        # fluxes: fl[r] = k[r] * (kinetic reactants)
+        w("KB_HD inline void flux_part(int part, const double* n, "
+          "const double* k, double* fl) {")
+        w("  (void)n; (void)k; (void)fl;")
+        w("  switch (part) {")
+        for j in range(P):
+            w("  case %d:" % j)
+            for rx in self.net.reactions[j::P]:
+                i = rx["id"] - 1
+                fac = ["k[%d]" % i] + [self.den(s0) for s0 in self._kin(rx)]
+                w("    fl[%d] = %s;" % (i, "*".join(fac)))
+            w("    break;")
+        w("  default: break;")
+        w("  }")
+        w("}")
+        # the rhs per species, its flux terms in reaction order (the
+        # unrolled rhs's order: reactants' minus before products' plus)
+        terms = [[] for _ in range(n)]
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            for r in rx["reactants"]:
+                terms[idx[r["sp"]]].append("-= fl[%d]" % i)
+            for p0 in rx["products"]:
+                terms[idx[p0["sp"]]].append("+= fl[%d]" % i)
+        w("KB_HD inline void rhs_gather_part(int part, const double* fl, "
+          "double* f) {")
+        w("  (void)fl; (void)f;")
+        w("  switch (part) {")
+        for j in range(P):
+            w("  case %d: {" % j)
+            for sidx in range(j, n, P):
+                w("    { double a = 0.0;")
+                for t in terms[sidx]:
+                    w("      a %s;" % t)
+                w("      f[%d] = a; }" % sidx)
+            w("  } break;")
+        w("  default: break;")
+        w("  }")
+        w("}")
+        # the Jacobian per entry: the jac_stoich terms of entry (i, j) in
+        # reaction order
+        jterms = [[] for _ in ent]
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            targets = {}
+            for s0 in self._kin(rx):
+                targets[s0] = targets.get(s0, 0) + 1
+            for tgt, mult in sorted(targets.items()):
+                rest = ["k[%d]" % i]
+                for s0, c in sorted(targets.items()):
+                    rest += [self.den(s0)] * (c - 1 if s0 == tgt else c)
+                coef = ("%d.0*" % mult) if mult > 1 else ""
+                d = coef + "*".join(rest)
+                jt = idx[tgt]
+                for r in rx["reactants"]:
+                    jterms[eidx[(idx[r["sp"]], jt)]].append("-= " + d)
+                for p0 in rx["products"]:
+                    jterms[eidx[(idx[p0["sp"]], jt)]].append("+= " + d)
+        # the same three forms as tables, for evaluation with one lane per
+        # reaction / species / entry (a slot n[NSPEC] = 1 pads the products)
+        kinr = [[idx[s0] for s0 in self._kin(rx)] for rx in self.net.reactions]
+        if max(len(x) for x in kinr) > 3:
+            raise NotImplementedError("more than three kinetic reactants")
+        pad = lambda x, m: x + [n] * (m - len(x))
+        fx = [pad(x, 3) for x in kinr]
+        self._table("fx_a", [x[0] for x in fx])
+        self._table("fx_b", [x[1] for x in fx])
+        self._table("fx_c", [x[2] for x in fx])
+        rs_rp, rs_r, rs_s = [0], [], []
+        for sidx in range(n):
+            for t in terms[sidx]:
+                rs_r.append(int(t.split("[")[1].split("]")[0]))
+                rs_s.append(-1 if t.startswith("-") else 1)
+            rs_rp.append(len(rs_r))
+        self._table("rs_rp", rs_rp)
+        self._table("rs_r", rs_r)
+        self._table("rs_s", rs_s)
+        jt_rp, jt_r, jt_c, jt_o0, jt_o1 = [0], [], [], [], []
+        jtab = [[] for _ in ent]
+        for rx in self.net.reactions:
+            i = rx["id"] - 1
+            targets = {}
+            for s0 in self._kin(rx):
+                targets[s0] = targets.get(s0, 0) + 1
+            for tgt, mult in sorted(targets.items()):
+                others = []
+                for s0, c in sorted(targets.items()):
+                    others += [idx[s0]] * (c - 1 if s0 == tgt else c)
+                if len(others) > 2:
+                    raise NotImplementedError("a Jacobian term of four factors")
+                others = pad(others, 2)
+                jt = idx[tgt]
+                for r in rx["reactants"]:
+                    jtab[eidx[(idx[r["sp"]], jt)]].append((i, -mult, others))
+                for p0 in rx["products"]:
+                    jtab[eidx[(idx[p0["sp"]], jt)]].append((i, mult, others))
+        for e in range(len(ent)):
+            for (i, c, o) in jtab[e]:
+                jt_r.append(i)
+                jt_c.append(c)
+                jt_o0.append(o[0])
+                jt_o1.append(o[1])
+            jt_rp.append(len(jt_r))
+        self._table("jt_rp", jt_rp)
+        self._table("jt_r", jt_r)
+        self._table("jt_c", jt_c)
+        self._table("jt_o0", jt_o0)
+        self._table("jt_o1", jt_o1)
+        w("constexpr int NTERM_RHS = %d;" % len(rs_r))
+        w("constexpr int NTERM_JAC = %d;" % len(jt_r))
+        w("// Jc[e] = dF_i/dn_j of entry e = (i, j) at fixed k (sp_jpos[e]: its")
+        w("// place in the LU values)")
+        w("KB_HD inline void jac_gather_part(int part, const double* n, "
+          "const double* k, double* Jc) {")
+        w("  (void)n; (void)k; (void)Jc;")
+        w("  switch (part) {")
+        for j in range(P):
+            w("  case %d: {" % j)
+            for e in range(j, len(ent), P):
+                w("    { double a = 0.0;")
+                for t in jterms[e]:
+                    w("      a %s;" % t)
+                w("      Jc[%d] = a; }" % e)
+            w("  } break;")
+        w("  default: break;")
+        w("  }")
+        w("}")
+        w("")
+
     def _rates_depend_on_n(self):
         """whether a rate coefficient depends on the densities (through
         rates_var or the v_* variables it calls): then the species block of
@@ -797,11 +1270,15 @@ class Emitter:
         self.emit_head()
         self.emit_physics()
         self.emit_vars()
+        self.emit_surface()
         self.emit_rates()
         self.emit_rhs()
         self.emit_jac()
         self.emit_thermal()
         self.emit_lnk_vjp()
+        if len(self.species) > LARGE_NSPEC:
+            self.emit_rate_parts()
+            self.emit_sparse()
         self.emit_tail()
         return "\n".join(self.lines) + "\n"
 

@@ -16,6 +16,15 @@ the network's code-point order, ``Tgas[ncell]``, ``dt[ncell]``,
   1e-20 n_H. The hydro loop: per call tff = t_ff(n), every density x 1.01,
   dt = 0.01 tff (the reference's collapse driver,
   examples/tests/collapse/test.cpp:47-63).
+* ``semenov``      (config 3) n_H log-uniform in [1e2, 1e7], Tgas in
+  [10, 300] K (fixed); the initial abundances of the reference's
+  cloudSurface test (Semenov 2010: He 0.09, H2 0.5, C+ 1.2e-4, N 7.6e-5,
+  O 2.56e-4, S+ 8e-8, Si+ 8e-9, Fe+ 3e-9, Na+ 2e-9, Mg+ 7e-9, P+ 2e-10,
+  Cl+ 1e-9, times n_H) each x log-uniform [0.5, 2], every other species
+  1e-20 n_H, electrons for neutrality; that test's parameters (Av 10,
+  crflux 1.3e-17, grains of 0.1 micron: gsize 1e-5, gsize2 1e-10, xdust =
+  0.01 rho / (4/3 pi 3 a^3 1.43) grains per cm^3, also GRAIN0's density,
+  Tdust = Tgas); dt = 3.15e13 s (examples/tests/cloudSurface/test.cpp).
 * ``galaxy_ism``   (config 4) n_H log-uniform in [1e-2, 1e4], Tgas in
   [10, 1e6] K, crate in [1e-17, 1e-16], G0 in [0.3, 3], d2g in
   [0.003, 0.03] (log-uniform, one decade around the typical values);
@@ -114,6 +123,39 @@ def galaxy_ism(ncell, info, seed=0):
     return n, T, dt, par
 
 
+SEMENOV_INITIAL = (("He", 9e-2), ("H2", 0.5), ("C+", 1.2e-4), ("N", 7.6e-5),
+                   ("O", 2.56e-4), ("S+", 8e-8), ("Si+", 8e-9), ("Fe+", 3e-9),
+                   ("Na+", 2e-9), ("Mg+", 7e-9), ("P+", 2e-10), ("Cl+", 1e-9))
+
+
+def semenov(ncell, info, seed=0):
+    species, mass_g, param_names = info["species"], info["mass_g"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1e2, 1e7, ncell)
+    T = loguniform(rng, 10.0, 300.0, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    for s, x in SEMENOV_INITIAL:
+        n[:, ix[s]] = x * nH * loguniform(rng, 0.5, 2.0, ncell)
+    charge = np.asarray(info["charge"], dtype=float)
+    ions = [i for i, s in enumerate(species) if s != "e-"]
+    n[:, ix["e-"]] = np.maximum((n[:, ions] * charge[ions]).sum(axis=1), 0.0)
+    rho = np.zeros(ncell)
+    for i in range(len(species)):
+        rho = rho + n[:, i] * mass_g[i]
+    a = 1e-5
+    xdust = 0.01 * rho / (4.0 / 3.0 * PI * 3.0 * a ** 3 * 1.43)
+    n[:, ix["GRAIN0"]] = xdust
+    par = _default_rows(ncell, info)
+    for name, v in (("Av", 10.0), ("crflux", 1.3e-17), ("gsize", a),
+                    ("gsize2", a * a)):
+        par[:, param_names.index(name)] = v
+    par[:, param_names.index("xdust")] = xdust
+    par[:, param_names.index("Tdust")] = T
+    dt = np.full(ncell, 3.15e13)
+    return n, T, dt, par
+
+
 def _default_rows(ncell, info):
     """every cell's parameter row at the network defaults (NaN: required)"""
     return np.repeat(np.asarray(info["defaults"], dtype=float)[None, :],
@@ -125,7 +167,7 @@ def hydro_step_info(n, par, info):
 
 
 GENERATORS = {"primordial": primordial, "primordial3": primordial3,
-              "galaxy_ism": galaxy_ism}
+              "galaxy_ism": galaxy_ism, "semenov": semenov}
 
 # the solve options of each workload (krome_opts keys)
 OPTIONS = {
@@ -135,4 +177,6 @@ OPTIONS = {
                         atol_n=1e-20, atol_T=1e-6),
     "galaxy_ism": dict(evolve_T=1, jac=0, linsol=0, rtol=1e-6,
                        atol_n=1e-20, atol_T=1e-6),
+    "semenov": dict(evolve_T=0, jac=0, linsol=3, rtol=1e-6, atol_n=1e-20,
+                    atol_T=1e-6, max_steps=1000000),
 }

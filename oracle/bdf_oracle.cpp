@@ -177,6 +177,51 @@ void getrs_(const R* a, int n, const int* p, double* b) {
   b[0] /= (double)a[0];
 }
 
+#ifdef KB_LARGE_NETWORK
+// ---- the static-pivot sparse LU of the large networks ----
+// The reference's sparse path (bdf_cell.hpp:1163-1264: a row-form IKJ LU
+// over a pattern fixed when the network is generated, static pivots in the
+// pattern's order, failure on a zero or non-finite pivot) restated over this
+// build's generation-time structure (net_<net>.h: sp_rp / sp_ci / sp_di in
+// the elimination order sp_perm). a: the values in the pattern; w: a zeroed
+// dense row of N doubles (left zeroed). Returns 0, or the failing row + 1.
+int sp_getrf_(double* a, double* w) {
+  for (int i = 0; i < NSPEC; i++) {
+    const int p0 = sp_rp[i], p1 = sp_rp[i + 1], pd = sp_di[i];
+    for (int p = p0; p < p1; p++) w[sp_ci[p]] = a[p];
+    for (int p = p0; p < pd; p++) {
+      const int k = sp_ci[p];
+      const double l = w[k] / a[sp_di[k]];
+      w[k] = l;
+      for (int q = sp_di[k] + 1; q < sp_rp[k + 1]; q++) w[sp_ci[q]] -= l * a[q];
+    }
+    const double piv = w[i];
+    for (int p = p0; p < p1; p++) {
+      a[p] = w[sp_ci[p]];
+      w[sp_ci[p]] = 0.0;
+    }
+    if (piv == 0.0 || !std::isfinite(piv)) return i + 1;
+  }
+  return 0;
+}
+// x = A^-1 b with the factors of sp_getrf_ (b in the species order; t: N
+// doubles of scratch); x may alias b
+void sp_getrs_(const double* a, const double* b, double* t, double* x) {
+  for (int i = 0; i < NSPEC; i++) t[i] = b[sp_perm[i]];
+  for (int i = 0; i < NSPEC; i++) {
+    double s = t[i];
+    for (int p = sp_rp[i]; p < sp_di[i]; p++) s -= a[p] * t[sp_ci[p]];
+    t[i] = s;
+  }
+  for (int i = NSPEC - 1; i >= 0; i--) {
+    double s = t[i];
+    for (int p = sp_di[i] + 1; p < sp_rp[i + 1]; p++) s -= a[p] * t[sp_ci[p]];
+    t[i] = s / a[sp_di[i]];
+  }
+  for (int i = 0; i < NSPEC; i++) x[sp_perm[i]] = t[i];
+}
+#endif
+
 // ---- the per-cell problem (solve_cell.hpp:438-813, 883-1132) ------------
 struct Problem {
   Params p;
@@ -222,6 +267,15 @@ struct Problem {
     if (mult != nullptr)
       for (int i = 0; i < NREA; ++i) kk[i] *= mult[i];
   }
+#ifdef KB_LARGE_NETWORK
+  // the sparse Jacobian of the species at fixed k (the emitted gather
+  // form, entry e at sp_jpos[e] of the LU pattern)
+  int jac_sparse_cb(const double* y, double* Jc) {
+    eval_rates(state_T(y), y, k0);
+    for (int part = 0; part < NPART; ++part) jac_gather_part(part, y, k0, Jc);
+    return 0;
+  }
+#endif
   // g[r] += sum_i mu_i d f_i / d ln k_r at y (the emitted lnk_vjp)
   void lnk_vjp_at(const double* y, const double* mu, double* g) {
     eval_rates(state_T(y), y, k0);
@@ -336,7 +390,12 @@ class Cvode {
   Stats st;
   std::vector<double>* tape = nullptr;  // recording for the adjoint
   Cvode(Problem& prob, int n, const BdfOpts& opts)
-      : P(prob), N(n), o(opts), work((L_MAX + 9) * n + 2 * n * n),
+      : P(prob), N(n), o(opts),
+#ifdef KB_LARGE_NETWORK
+        work((L_MAX + 10) * n + NNZ_LU + NNZ_J),
+#else
+        work((L_MAX + 9) * n + 2 * n * n),
+#endif
         A32(opts.lu32 ? (long)n * n : 0), piv(n) {
     double* w = work.data();
     for (int j = 0; j < L_MAX; j++, w += N) zn[j] = w;
@@ -349,8 +408,15 @@ class Cvode {
     vtemp1 = w; w += N;
     vtemp2 = w; w += N;
     vtemp3 = w; w += N;
+#ifdef KB_LARGE_NETWORK
+    A = w; w += NNZ_LU;       // the LU values in the sparse pattern
+    savedJ = w; w += NNZ_J;   // the Jacobian's entries
+    spw = w;                  // the LU's dense work row (kept zeroed)
+    for (int i = 0; i < N; i++) spw[i] = 0.0;
+#else
     A = w; w += (long)N * N;
     savedJ = w;
+#endif
     mxstep = o.max_steps == 0 ? 500 : o.max_steps;
     double mn = o.atol[0];
     for (int i = 1; i < N; i++)
@@ -451,6 +517,7 @@ class Cvode {
   double* zn[L_MAX];
   double *ewt, *y, *acor, *tempv, *ftemp, *delta, *vtemp1, *vtemp2, *vtemp3;
   double *A, *savedJ;
+  double* spw = nullptr;
   double tn = 0.0, h = 0.0, hin = 0.0, hprime = 0.0, hscale = 0.0, h0u = 0.0;
   double next_h = 0.0, hu = 0.0, eta = 1.0, etamax = 0.0, etaq = 0.0;
   double etaqm1 = 0.0, etaqp1 = 0.0, tolsf = 1.0, saved_tq5 = 0.0;
@@ -846,6 +913,26 @@ class Cvode {
   }
   // cvLsSetup + A = I - gamma J + dense LU (bdf_cell.hpp:1069-1130)
   int ls_setup_() {
+#ifdef KB_LARGE_NETWORK
+    {
+      const double dgamma = std::fabs((gamma / gammap) - 1.0);
+      const bool jbad_ls = (st.nst == 0) || (st.nst >= nstlj + MSBJ)
+                           || ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
+                           || (convfail == FAIL_OTHER);
+      jcur = jbad_ls;
+      if (jbad_ls) P.jac_sparse_cb(y, savedJ);
+      const double c = -gamma;
+      for (int k = 0; k < NNZ_LU; k++) A[k] = 0.0;
+      for (int e = 0; e < NNZ_J; e++) A[sp_jpos[e]] = savedJ[e] * c;
+      for (int i = 0; i < N; i++) A[sp_di[i]] += 1.0;
+      if (jcur) {
+        st.nje++;
+        nstlj = st.nst;
+      }
+      fact32 = false;
+      return sp_getrf_(A, spw) > 0 ? LS_LUFACT_FAIL : 0;
+    }
+#endif
     const long NN = (long)N * N;
     const double dgamma = std::fabs((gamma / gammap) - 1.0);
     const bool jbad_ls = (st.nst == 0) || (st.nst >= nstlj + MSBJ)
@@ -887,8 +974,12 @@ class Cvode {
     return getrf_(A, N, piv.data()) > 0 ? LS_LUFACT_FAIL : 0;
   }
   int lsolve_(double* b) {
+#ifdef KB_LARGE_NETWORK
+    sp_getrs_(A, b, vtemp3, b);
+#else
     if (fact32) getrs_(A32.data(), N, piv.data(), b);
     else getrs_(A, N, piv.data(), b);
+#endif
     if (gamrat != 1.0) scale_(N, 2.0 / (1.0 + gamrat), b, b);
     return SUCCESS;
   }

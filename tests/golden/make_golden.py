@@ -9,7 +9,8 @@ Run where the reference tree and oracle/_ref (oracle/build_ref.py) exist:
   krome_check.cpp (rate coefficients at three temperatures, computed by its
   independent network interpreter, kromex/netcheck.py), with the probe
   parameters of that check (every parameter 1.3e-17, Tdust 10 K);
-* ``n, T, dt, par`` / ``n_out, T_out, flags``: 64 seeded cells of the
+* ``n, T, dt, par`` / ``n_out, T_out, flags``: 64 seeded cells (16 for
+  Semenov) of the
   benchmark workload solved by the reference's strict build
   (oracle/_ref/libkrome_<net>_strict.so, krome_solve_cells) with the
   workload's options, each network in its own process (the generated
@@ -39,15 +40,17 @@ def _array(text, name):
     return np.array(eval(body), dtype=float)
 
 
-def main():
-    for key in ("primordial", "primordial3", "galaxy_ism"):
+def main(keys=None):
+    for key in keys or ("primordial", "primordial3", "galaxy_ism", "semenov"):
         info = netinfo.load(key)
         chk = (ROOT / "oracle" / "_ref" / "gen" / key / "krome_check.cpp").read_text()
         k_T = _array(chk, "T_REF")
         k_n = _array(chk, "N_REF")
         k_idx = _array(chk, "I_REF").astype(np.int32)
         k_ref = _array(chk, "K_REF")
-        n, T, dt, par = workloads.GENERATORS[key](NCELL, info, seed=11)
+        # the large network's cells take ~1 s each in the reference
+        ncell = 16 if key == "semenov" else NCELL
+        n, T, dt, par = workloads.GENERATORS[key](ncell, info, seed=11)
         opts = dict(workloads.OPTIONS[key])
         out = reference_solve(key, n, T, dt, par, strict=True, **opts)
         np.savez_compressed(HERE / ("%s.npz" % key), k_T=k_T, k_n=k_n,
@@ -58,4 +61,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

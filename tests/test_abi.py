@@ -8,7 +8,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import NETWORKS, ROOT
+from conftest import ALL_NETWORKS, ROOT
 from krome_x_b200 import build, krome, netinfo
 
 HEADER = ROOT / "include" / "krome_b200.h"
@@ -31,14 +31,14 @@ def test_header_declares_the_reference_entry_points():
         assert s in syms
 
 
-@pytest.mark.parametrize("key", NETWORKS)
+@pytest.mark.parametrize("key", ALL_NETWORKS)
 def test_library_exports_every_declared_symbol(key):
     lib = ctypes.CDLL(str(build.build(key)))
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert not missing, missing
 
 
-@pytest.mark.parametrize("key", NETWORKS)
+@pytest.mark.parametrize("key", ALL_NETWORKS)
 def test_network_description_matches_metadata(key):
     net = krome.load(key)
     info = netinfo.load(key)
