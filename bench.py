@@ -36,6 +36,11 @@ exists for this path). A step is 262,144 cell-solves.
                        abundances above atol/rtol and Tgas are within
                        10 rtol, the median and p99 of the cell's largest
                        relative error)
+            large_network  the large-network workload: Semenov (655 species,
+                       5,639 reactions, grain-surface chemistry), fixed Tgas,
+                       the sparse-LU block-per-cell kernel on a seeded subset
+                       of the 16,384-cell batch: cell-solves/s and its DRAM
+                       traffic against the HBM peak
 
 ``python bench.py --gpus N --steps K --warmup W [--impl reference]``; with
 N > 1 each rank (torchrun) solves its own 262,144 cells (weak scaling: no
@@ -369,6 +374,68 @@ def precision_form(torch, dev):
     return out
 
 
+# the large-network form: DRAM bytes (read + write) of its solve kernel per
+# integration step, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of 148 Semenov cells over 3.15e9 s (154,453 steps:
+# 8.49 GB); the per-cell workspace (~600 KB) stays in L2
+SEMENOV_DRAM_PER_STEP = 8.49e9 / 154453
+SEMENOV_CELLS = 2048
+
+
+def large_network_form(torch, dev, ncell=SEMENOV_CELLS):
+    """the sparse-LU path on the large-network workload: Semenov (655
+    species, 5,639 reactions), fixed Tgas, one launch of the block-per-cell
+    kernel over a seeded subset of the 16,384-cell batch"""
+    from krome_x_b200 import krome, netinfo, workloads
+    key = "semenov"
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.semenov(ncell, info, seed=0)
+    net = krome.load(key)
+    opts = net.options(**workloads.OPTIONS[key])
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    nd, Td = t(n), t(T)
+    fl = torch.zeros(ncell, dtype=torch.int32, device=dev)
+    st = torch.zeros((ncell, len(STAT_NAMES)), dtype=torch.int64, device=dev)
+    cur = torch.zeros(1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    e0 = _events(torch)
+    net.solve_device(nd, Td, t(dt), t(par), fl, opts=opts, stats=st,
+                     cursor=cur)
+    e1 = _events(torch)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    S = st.cpu().numpy()
+    steps = int(S[:, STAT_NAMES.index("nst")].sum())
+    dram = SEMENOV_DRAM_PER_STEP * steps
+    io = ncell * 8 * (2 * net.nspec + net.npar + 2)
+    peak = _hbm_peak()
+    mass = np.asarray(info["mass_g"])
+    out = nd.cpu().numpy()
+    return {"workload": "Semenov (655 species, 5,639 reactions), fixed Tgas, "
+                        "rtol 1e-6, dt 3.15e13 s, sparse LU; %d seeded cells "
+                        "of the 16,384-cell batch" % ncell,
+            "cell_solves_per_s": ncell / (ms * 1e-3), "ms": ms,
+            "failed_cells": int((fl != 0).sum().item()),
+            "mean_steps_per_cell": steps / ncell,
+            "mass_conservation_max_rel": float(
+                np.abs(out @ mass / (n @ mass) - 1).max()),
+            "hbm": {"achieved_gbs": dram / (ms * 1e-3) / 1e9,
+                    "peak_gbs": peak, "frac": dram / (ms * 1e-3) / 1e9 / peak,
+                    "traffic_bytes": dram,
+                    "traffic_source": "ncu DRAM bytes per integration step "
+                                      "x the steps taken",
+                    "algorithmic_bytes": io,
+                    "algorithmic_gbs": io / (ms * 1e-3) / 1e9}}
+
+
+def _hbm_peak():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -481,7 +548,8 @@ def run_ours(args, rank, world, local):
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = {"adjoint": adjoint_form(torch, dev),
-                 "precision": precision_form(torch, dev)}
+                 "precision": precision_form(torch, dev),
+                 "large_network": large_network_form(torch, dev)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_leg(args.cpu_cells, args.warmup, args.steps)

@@ -1,36 +1,57 @@
-// Warp-per-cell CVODE BDF for the large networks: the sparse path.
+// Block-per-cell CVODE BDF for the large networks: the sparse path.
 //
 // A network of hundreds of species (Semenov: 655 species, 5,639 reactions)
-// cannot keep a cell's state in registers or shared memory: the Nordsieck
-// array, the vectors, the rate coefficients and fluxes, the saved Jacobian
-// (NNZ_J entries) and the LU factors of I - gamma J in their generation-time
-// pattern (NNZ_LU values) take ~570 KB per cell. One warp integrates one
-// cell with that state in an HBM workspace slot of its own; the 32 lanes
-// split every vector operation (component i on lane i mod 32) and evaluate
-// the table-driven forms the emitter writes for this path:
+// cannot keep a cell's state in registers: the Nordsieck array, the vectors,
+// the rate coefficients and fluxes, the saved Jacobian (NNZ_J entries) and
+// the LU factors of I - gamma J in their generation-time pattern (NNZ_LU
+// values) take ~600 KB per cell. One thread block of NT threads integrates
+// one cell, one block per SM over a persistent work queue; the cell's state
+// lives in a global-memory workspace slot of its block (148 slots, ~90 MB,
+// mostly L2-resident), and the hot part of the Newton matrix in shared
+// memory:
 //
-//   fluxes     fl[r] = k[r] n[a_r] n[b_r] n[c_r], one lane per reaction
-//   rhs        f_i = the reaction-ordered sum of its flux terms, one lane per
-//              species (the order of the generated rhs)
-//   Jacobian   Jc[e] = the reaction-ordered sum of entry e's terms, one lane
+//   vectors    component i on thread i mod NT; element-wise operations need
+//              no barrier (each thread touches its own components), every
+//              operation that reads other threads' components (rhs, Jacobian,
+//              setup, solve, reductions) is bracketed by block barriers
+//   rates      the Tgas/parameter-only rates once per solve (one generated
+//              part per thread, RPART parts); the density-dependent ones (the
+//              grain-surface processes) depend on the state only through the
+//              water-ice coverage fi (affinely) and the H-nuclei density
+//              hnuc (linearly), so with Tgas and Tdust fixed the generated
+//              code runs at three points per solve (fi = 0, fi = 1, hnuc = 1)
+//              and every rhs forms k = e0 (1 - fi) + e1 fi + eh hnuc, a
+//              thread per rate (networks whose rates read the densities
+//              otherwise, BK_VAR_AFFINE = 0, run the generated parts at every
+//              rhs)
+//   fluxes     fl[r] = k[r] n[a_r] n[b_r] n[c_r], a thread per reaction
+//   rhs        f_i = the sum of its flux terms in reaction order, in chunks
+//              of at most 16 terms (a thread per chunk, then per species the
+//              sum of its chunks in order: the hub species' hundreds of terms
+//              spread over the block)
+//   Jacobian   Jc[e] = the reaction-ordered sum of entry e's terms, a thread
 //              per entry, at fixed rates
-//   LU         the static-pivot row-form (IKJ) sparse LU: a row at a time,
-//              each eliminated row's update split over the lanes, through a
-//              dense work row of N doubles
-//   solves     the unit-lower and upper triangular sweeps, a row at a time,
-//              each row's dot product split over the lanes
-//
-// The rate coefficients are generated code: the Tgas/parameter-only rates
-// (rates_fixed) once per solve, the density-dependent ones (rates_var, the
-// grain-surface processes among them) at every rhs, on lane 0.
+//   LU         the static-pivot LU of the generation-time order, split where
+//              the minimum-degree order leaves a dense trailing block: the
+//              first BK_M rows sparse (factored level by level -- the rows of
+//              a level eliminate only with rows of lower levels -- a thread
+//              per row on wide levels, a warp per row on narrow ones), then
+//              the last BK_D rows' sparse columns (a thread per row, the
+//              Schur complement into S), then the dense block S (BK_D x BK_D,
+//              shared memory) by a right-looking LU in panels of 16 columns
+//              with register-tiled rank-16 updates
+//   solves     the same split: sparse rows by level, the dense block by
+//              32-row diagonal blocks (a warp with shuffles) and block
+//              updates, sparse rows back by backward level
 //
 // The CVODE algorithm and every decision are the reference's per-cell
 // integrator (runtime/core/cvode/bdf_cell.hpp:490-1547) with its sparse
-// linear solver (bdf_cell.hpp:1163-1264) -- the same sequence of operations
-// as the CPU restatement (oracle/bdf_oracle.cpp), whose sparse path this
-// follows line for line. Fixed Tgas only (the large networks' benchmark
-// configuration). Every loop is bounded (max_steps, the per-step failure
-// limits, max_restarts, the work queue by the number of cells).
+// linear solver (bdf_cell.hpp:1163-1264): the sequence of operations of the
+// CPU restatement (oracle/bdf_oracle.cpp, sparse path), whose IKJ row LU
+// this factorization equals up to the order of its roundings (same pivots,
+// same pattern, static pivoting). Fixed Tgas only (the large networks'
+// benchmark configuration). Every loop is bounded (max_steps, the per-step
+// failure limits, max_restarts, the work queue by the number of cells).
 #pragma once
 
 #ifdef KB_LARGE_NETWORK
@@ -41,13 +62,16 @@ using namespace kbnet;
 using namespace kbw;
 
 constexpr int N = NSPEC;
+constexpr int NT = 256;  // threads of a cell's block
+constexpr int NWARP = NT / 32;
 constexpr unsigned FULLM = 0xffffffffu;
-// a vector's stride in the workspace: N + the n[N] = 1 slot of the flux
-// products, a multiple of 4 doubles
+static_assert(RPART <= NT, "one rate part per thread");
+// a vector's stride: N + the n[N] = 1 slot of the flux products, a
+// multiple of 4 doubles
 constexpr long NV = ((NSPEC + 1 + 3) / 4) * 4;
 constexpr long rnd4(long x) { return ((x + 3) / 4) * 4; }
 
-// one warp's workspace (doubles)
+// a cell's workspace in global memory (doubles)
 struct WS {
   static constexpr long ZN = 0;                       // zn[L_MAX]
   static constexpr long EWT = ZN + L_MAX * NV;
@@ -56,212 +80,540 @@ struct WS {
   static constexpr long TEMPV = ACOR + NV;
   static constexpr long FTEMP = TEMPV + NV;
   static constexpr long DELTA = FTEMP + NV;
-  static constexpr long YR = DELTA + NV;              // the rhs's input (+1 slot)
-  static constexpr long TS = YR + NV;                 // the solves' scratch
-  static constexpr long WROW = TS + NV;               // the LU's work row
-  static constexpr long YOUT = WROW + NV;             // a solve's output
+  static constexpr long YOUT = DELTA + NV;            // a solve's output
   static constexpr long K = YOUT + NV;                // k[NREA + 1]
   static constexpr long FL = K + rnd4(NREA + 1);      // fl[NREA]
   static constexpr long SJ = FL + rnd4(NREA);         // saved Jacobian
-  static constexpr long A = SJ + rnd4(NNZ_J);         // LU values
+  static constexpr long CP = SJ + rnd4(NNZ_J);        // rhs chunk sums
+  static constexpr long VE = CP + rnd4(NCHUNK);       // e0, e1, eh [BK_NVAR]
+  static constexpr long A = VE + 3 * rnd4(BK_NVAR);   // LU values
   static constexpr long SIZE = A + rnd4(NNZ_LU);
 };
 
-__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+// the block's shared memory (doubles)
+struct SM {
+  static constexpr int S = 0;                         // dense block [D][LD]
+  static constexpr int T = S + BK_D * BK_LD;          // the solves' vector
+  static constexpr int RPIV = T + (int)NV;            // 1 / pivot, per row
+  static constexpr int YR = RPIV + (int)NV;           // the rhs input (+1)
+  static constexpr int RED = YR + (int)NV;            // reductions
+  static constexpr int MISC = RED + NWARP;            // the work queue's cell
+  static constexpr int SIZE = MISC + 2;
+};
+constexpr size_t SMEM_BYTES = SM::SIZE * sizeof(double);
+static_assert(SMEM_BYTES <= 227 * 1024, "the dense block must fit shared memory");
 
-// ---- warp-split vector operations (each ends with the warp's writes
-//      visible to all its lanes) ----
+__device__ __forceinline__ double* smem() {
+  extern __shared__ double kbg_smem[];
+  return kbg_smem;
+}
+
+// block reductions: every thread gets the same value (the warps' partial
+// results summed in warp order)
+__device__ __forceinline__ double blk_sum(double v) {
+  double* red = smem() + SM::RED;
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < NWARP; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+__device__ __forceinline__ double blk_max(double v) {
+  double* red = smem() + SM::RED;
+  v = warp_max(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int w = 1; w < NWARP; ++w) s = fmax(s, red[w]);
+  __syncthreads();
+  return s;
+}
+
+// ---- element-wise vector operations (component i on thread i mod NT) ----
+#define KBG_FOR(i) for (int i = threadIdx.x; i < N; i += NT)
 __device__ __forceinline__ void v_copy(const double* x, double* z) {
-  for (int i = lane_id(); i < N; i += 32) z[i] = x[i];
-  __syncwarp();
+  KBG_FOR(i) z[i] = x[i];
 }
 __device__ __forceinline__ void v_scale(double c, const double* x, double* z) {
-  for (int i = lane_id(); i < N; i += 32) z[i] = c * x[i];
-  __syncwarp();
+  KBG_FOR(i) z[i] = c * x[i];
 }
 __device__ __forceinline__ void v_const(double c, double* z) {
-  for (int i = lane_id(); i < N; i += 32) z[i] = c;
-  __syncwarp();
+  KBG_FOR(i) z[i] = c;
 }
 __device__ __forceinline__ void v_axpy(double a, const double* x, double* y) {
-  const int l = lane_id();
   if (a == 1.0) {
-    for (int i = l; i < N; i += 32) y[i] += x[i];
+    KBG_FOR(i) y[i] += x[i];
   } else if (a == -1.0) {
-    for (int i = l; i < N; i += 32) y[i] -= x[i];
+    KBG_FOR(i) y[i] -= x[i];
   } else {
-    for (int i = l; i < N; i += 32) y[i] += a * x[i];
+    KBG_FOR(i) y[i] += a * x[i];
   }
-  __syncwarp();
 }
 // N_VLinearSum with its special cases (bdf_cell.hpp:296-400)
 __device__ void v_lin_sum(double a, const double* x, double b, const double* y,
                           double* z) {
-  const int l = lane_id();
   if (b == 1.0 && z == y) { v_axpy(a, x, z); return; }
   if (a == 1.0 && z == x) { v_axpy(b, y, z); return; }
   if (a == 1.0 && b == 1.0) {
-    for (int i = l; i < N; i += 32) z[i] = x[i] + y[i];
+    KBG_FOR(i) z[i] = x[i] + y[i];
   } else if ((a == 1.0 && b == -1.0) || (a == -1.0 && b == 1.0)) {
     const bool test = a == 1.0 && b == -1.0;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = l; i < N; i += 32) z[i] = v2[i] - v1[i];
+    KBG_FOR(i) z[i] = v2[i] - v1[i];
   } else if (a == 1.0 || b == 1.0) {
     const bool test = a == 1.0;
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = l; i < N; i += 32) z[i] = (c * v1[i]) + v2[i];
+    KBG_FOR(i) z[i] = (c * v1[i]) + v2[i];
   } else if (a == -1.0 || b == -1.0) {
     const bool test = a == -1.0;
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    for (int i = l; i < N; i += 32) z[i] = (c * v1[i]) - v2[i];
+    KBG_FOR(i) z[i] = (c * v1[i]) - v2[i];
   } else if (a == b) {
-    for (int i = l; i < N; i += 32) z[i] = a * (x[i] + y[i]);
+    KBG_FOR(i) z[i] = a * (x[i] + y[i]);
   } else if (a == -b) {
-    for (int i = l; i < N; i += 32) z[i] = a * (x[i] - y[i]);
+    KBG_FOR(i) z[i] = a * (x[i] - y[i]);
   } else {
-    for (int i = l; i < N; i += 32) z[i] = (a * x[i]) + (b * y[i]);
+    KBG_FOR(i) z[i] = (a * x[i]) + (b * y[i]);
   }
-  __syncwarp();
 }
 __device__ __forceinline__ double v_wrms(const double* x, const double* w) {
   double s = 0.0;
-  for (int i = lane_id(); i < N; i += 32) {
+  KBG_FOR(i) {
     const double pv = x[i] * w[i];
     s += pv * pv;
   }
-  return ssqrt_(warp_sum(s) / N);
+  return ssqrt_(blk_sum(s) / N);
 }
 __device__ __forceinline__ double v_max_norm(const double* x) {
   double m = 0.0;
-  for (int i = lane_id(); i < N; i += 32) m = fmax(m, fabs(x[i]));
-  return warp_max(m);
+  KBG_FOR(i) m = fmax(m, fabs(x[i]));
+  return blk_max(m);
 }
 
-// ---- the network on the warp ----
+// ---- the network on the block ----
 struct Net {
   double* ws;
   Params p;
-  double T;           // the fixed gas temperature
-  const double* atolp;
+  double T;  // the fixed gas temperature
 
-  // f = F(yv): rates_var on lane 0, then the fluxes and the gather over
-  // the lanes; 0, or 1 for a non-finite f (rhs_host_, solve_cell.hpp:
-  // 794-813)
-  __device__ int rhs(const double* yv, double* f) {
-    double* yr = ws + WS::YR;
+  static constexpr long VSTR = rnd4(BK_NVAR);
+
+  // yr (shared memory) = yv with the slot yr[N] = 1, and the H-nuclei
+  // density of yv (a reduction, so it ends with yr visible to the block)
+  __device__ double load_state(const double* yv) {
+    double* yr = smem() + SM::YR;
+    double h = 0.0;
+    KBG_FOR(i) {
+      const double v = yv[i];
+      yr[i] = v;
+      h += v * d_bk_hnuc[i];
+    }
+    if (threadIdx.x == 0) yr[N] = 1.0;
+    return blk_sum(h);
+  }
+  // the density-dependent rates at the state in yr (hnuc its H-nuclei
+  // density)
+  __device__ void rates_at(double hnuc) {
     double* k = ws + WS::K;
-    double* fl = ws + WS::FL;
-    const int l = lane_id();
-    for (int i = l; i < N; i += 32) yr[i] = yv[i];
-    if (l == 0) yr[N] = 1.0;
-    __syncwarp();
-    if (l == 0) rates_var(T, yr, p, k);
-    __syncwarp();
-    for (int r = l; r < NREA; r += 32)
-      fl[r] = k[r] * yr[d_fx_a[r]] * yr[d_fx_b[r]] * yr[d_fx_c[r]];
-    __syncwarp();
-    bool ok = true;
-    for (int i = l; i < N; i += 32) {
-      double a = 0.0;
-      for (int t = d_rs_rp[i]; t < d_rs_rp[i + 1]; ++t) {
-        if (d_rs_s[t] < 0) a -= fl[d_rs_r[t]];
-        else a += fl[d_rs_r[t]];
+    if (BK_VAR_AFFINE) {
+      const double fi = bk_ice_cover(smem() + SM::YR, p);
+      const double* e0 = ws + WS::VE;
+      const double* e1 = e0 + VSTR;
+      const double* eh = e1 + VSTR;
+      for (int j = threadIdx.x; j < BK_NVAR; j += NT)
+        k[d_bk_var[j]] = e0[j] * (1.0 - fi) + e1[j] * fi + eh[j] * hnuc;
+    } else if (threadIdx.x < RPART) {
+      rates_var_part(threadIdx.x, T, smem() + SM::YR, p, hnuc, k);
+    }
+    __syncthreads();
+  }
+  // the density-dependent rates' three points of this solve (e0: fi = 0,
+  // e1: fi = 1, eh: the change at hnuc = 1), from the generated code at the
+  // state y0 with its ice density replaced. Starts and ends with a barrier.
+  __device__ void prepare_var(const double* y0) {
+    if (!BK_VAR_AFFINE) return;
+    double* yr = smem() + SM::YR;
+    double* k = ws + WS::K;
+    double* e0 = ws + WS::VE;
+    double* e1 = e0 + VSTR;
+    double* eh = e1 + VSTR;
+    __syncthreads();
+    KBG_FOR(i) yr[i] = y0[i];
+    for (int pt = 0; pt < 3; ++pt) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        yr[N] = 1.0;
+        bk_set_ice(yr, p, pt == 1);
       }
+      __syncthreads();
+      if (threadIdx.x < RPART)
+        rates_var_part(threadIdx.x, T, yr, p, pt == 2 ? 1.0 : 0.0, k);
+      __syncthreads();
+      double* e = pt == 0 ? e0 : (pt == 1 ? e1 : eh);
+      for (int j = threadIdx.x; j < BK_NVAR; j += NT) {
+        const double v = k[d_bk_var[j]];
+        e[j] = pt == 2 ? v - e0[j] : v;
+      }
+    }
+    __syncthreads();
+  }
+  // f = F(yv); 0, or 1 for a non-finite f (rhs_host_, solve_cell.hpp:
+  // 794-813). Starts and ends with a block barrier.
+  __device__ int rhs(const double* yv, double* f) {
+    __syncthreads();
+    const double* yr = smem() + SM::YR;
+    const double* k = ws + WS::K;
+    double* fl = ws + WS::FL;
+    rates_at(load_state(yv));
+    for (int r = threadIdx.x; r < NREA; r += NT)
+      fl[r] = k[r] * yr[d_fx_a[r]] * yr[d_fx_b[r]] * yr[d_fx_c[r]];
+    __syncthreads();
+    double* cp = ws + WS::CP;
+    for (int c = threadIdx.x; c < NCHUNK; c += NT) {
+      const int t0 = d_ck_t[c], t1 = d_ck_t[c + 1];
+      double v[16];
+#pragma unroll
+      for (int x = 0; x < 16; ++x) v[x] = t0 + x < t1 ? fl[d_rs_r[t0 + x]] : 0.0;
+      double a = 0.0;
+#pragma unroll
+      for (int x = 0; x < 16; ++x)
+        if (t0 + x < t1) {
+          if (d_rs_s[t0 + x] < 0) a -= v[x];
+          else a += v[x];
+        }
+      cp[c] = a;
+    }
+    __syncthreads();
+    bool ok = true;
+    KBG_FOR(i) {
+      double a = 0.0;
+      for (int c = d_ck_rp[i]; c < d_ck_rp[i + 1]; ++c) a += cp[c];
       f[i] = a;
       ok = ok && isfinite(a);
     }
-    __syncwarp();
-    return __all_sync(FULLM, ok) ? 0 : 1;
+    return __syncthreads_and(ok) ? 0 : 1;
   }
   // the saved Jacobian's entries at yv (the rates at yv)
   __device__ void jac(const double* yv, double* Jc) {
-    double* yr = ws + WS::YR;
-    double* k = ws + WS::K;
-    const int l = lane_id();
-    for (int i = l; i < N; i += 32) yr[i] = yv[i];
-    if (l == 0) yr[N] = 1.0;
-    __syncwarp();
-    if (l == 0) rates_var(T, yr, p, k);
-    __syncwarp();
-    for (int e = l; e < NNZ_J; e += 32) {
+    __syncthreads();
+    const double* yr = smem() + SM::YR;
+    const double* k = ws + WS::K;
+    rates_at(load_state(yv));
+    for (int e = threadIdx.x; e < NNZ_J; e += NT) {
       double a = 0.0;
       for (int t = d_jt_rp[e]; t < d_jt_rp[e + 1]; ++t)
         a += d_jt_c[t] * k[d_jt_r[t]] * yr[d_jt_o0[t]] * yr[d_jt_o1[t]];
       Jc[e] = a;
     }
-    __syncwarp();
+    __syncthreads();
   }
 };
 
-// the static-pivot sparse LU of the values a in place (w: a zeroed row of N
-// doubles, left zeroed); 0, or the failing row + 1 (a zero or non-finite
-// pivot)
-__device__ int sp_getrf(double* a, double* w) {
-  const int l = lane_id();
-  for (int i = 0; i < N; ++i) {
-    const int p0 = d_sp_rp[i], p1 = d_sp_rp[i + 1], pd = d_sp_di[i];
-    for (int p = p0 + l; p < p1; p += 32) w[d_sp_ci[p]] = a[p];
-    __syncwarp();
-    for (int p = p0; p < pd; ++p) {
-      const int k = d_sp_ci[p];
-      const double lk = w[k] / a[d_sp_di[k]];
-      const int q1 = d_sp_rp[k + 1];
-      for (int q = d_sp_di[k] + 1 + l; q < q1; q += 32) w[d_sp_ci[q]] -= lk * a[q];
-      __syncwarp();
-      if (l == 0) w[k] = lk;
-      __syncwarp();
+// ---- the factorization ----
+// row i's elimination with the (final) rows k of its L entries [p0, p1):
+// l = a(i, k) / a(k, k), then a(i, j) -= l a(k, j) over row k's U entries
+// (bk_tgt: the places of the (i, j)); by one thread. The updates of one L
+// entry go in batches of 8, every load of a batch before its stores, so a
+// batch costs one memory round trip.
+__device__ __forceinline__ void elim_thread(int p0, int p1, double* A,
+                                            double* S, const double* rpiv) {
+  for (int p = p0; p < p1; ++p) {
+    const int k = d_sp_ci[p];
+    const double l = A[p] * rpiv[k];
+    A[p] = l;
+    const int q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
+    const int* tg = d_bk_tgt + d_bk_uoff[p] - q0;
+    for (int qb = q0; qb < q1; qb += 8) {
+      int t[8];
+      double u[8], a[8];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const bool in = qb + x < q1;
+        t[x] = in ? tg[qb + x] : 0;
+        u[x] = in ? A[qb + x] : 0.0;
+      }
+#pragma unroll
+      for (int x = 0; x < 8; ++x)
+        a[x] = qb + x < q1 ? (t[x] >= 0 ? A[t[x]] : S[-1 - t[x]]) : 0.0;
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        if (qb + x < q1) {
+          const double v = a[x] - l * u[x];
+          if (t[x] >= 0) A[t[x]] = v;
+          else S[-1 - t[x]] = v;
+        }
+      }
     }
-    const double piv = w[i];
-    __syncwarp();
-    for (int p = p0 + l; p < p1; p += 32) {
-      a[p] = w[d_sp_ci[p]];
-      w[d_sp_ci[p]] = 0.0;
-    }
-    __syncwarp();
-    if (piv == 0.0 || !isfinite(piv)) return i + 1;
   }
-  return 0;
 }
-// x = A^-1 b with the factors (b in the species order; t: N doubles of
-// scratch); x may be b
-__device__ void sp_getrs(const double* a, const double* b, double* t,
-                         double* x) {
-  const int l = lane_id();
-  for (int i = l; i < N; i += 32) t[i] = b[d_sp_perm[i]];
-  __syncwarp();
-  for (int i = 0; i < N; ++i) {
-    double s = 0.0;
-    for (int p = d_sp_rp[i] + l; p < d_sp_di[i]; p += 32) s += a[p] * t[d_sp_ci[p]];
-    s = warp_sum(s);
-    if (l == 0) t[i] -= s;
+// the same by a warp: the U entries over the lanes
+__device__ __forceinline__ void elim_warp(int p0, int p1, double* A,
+                                          const double* rpiv) {
+  const int lane = threadIdx.x & 31;
+  for (int p = p0; p < p1; ++p) {
+    const int k = d_sp_ci[p];
+    const double l = A[p] * rpiv[k];
+    const int q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
+    const int* tg = d_bk_tgt + d_bk_uoff[p] - q0;
+    for (int q = q0 + lane; q < q1; q += 32) A[tg[q]] -= l * A[q];
+    __syncwarp();
+    if (lane == 0) A[p] = l;
     __syncwarp();
   }
-  for (int i = N - 1; i >= 0; --i) {
-    double s = 0.0;
-    for (int p = d_sp_di[i] + 1 + l; p < d_sp_rp[i + 1]; p += 32) s += a[p] * t[d_sp_ci[p]];
-    s = warp_sum(s);
-    if (l == 0) t[i] = (t[i] - s) / a[d_sp_di[i]];
-    __syncwarp();
+}
+
+constexpr int PB = 16;  // the dense LU's panel width
+
+// the right-looking LU of the dense block S (no pivoting); rpd[c] = 1 /
+// its pivot c; true for a zero or non-finite pivot
+__device__ bool dense_lu(double* S, double* rpd) {
+  constexpr int D = BK_D, LD = BK_LD;
+  const int tid = threadIdx.x;
+  bool bad = false;
+  for (int c0 = 0; c0 < D; c0 += PB) {
+    const int pe = c0 + PB < D ? c0 + PB : D;
+    // the panel's columns [c0, pe): a thread per row below each pivot
+    for (int c = c0; c < pe; ++c) {
+      const double piv = S[c * LD + c];
+      const double rc = 1.0 / piv;
+      if (tid == 0) {
+        rpd[c] = rc;
+        bad = bad || piv == 0.0 || !isfinite(piv);
+      }
+      for (int i = c + 1 + tid; i < D; i += NT) {
+        double* Si = S + i * LD;
+        const double l = Si[c] * rc;
+        Si[c] = l;
+        for (int j = c + 1; j < pe; ++j) Si[j] -= l * S[c * LD + j];
+      }
+      __syncthreads();
+    }
+    if (pe == D) break;
+    const int w = pe - c0;
+    // the panel's rows beyond it: U12 = L11^-1 A12, a thread per column
+    for (int j = pe + tid; j < D; j += NT) {
+      double u[PB];
+#pragma unroll
+      for (int r = 0; r < PB; ++r) u[r] = r < w ? S[(c0 + r) * LD + j] : 0.0;
+#pragma unroll
+      for (int r = 1; r < PB; ++r) {
+        if (r < w) {
+          double s = u[r];
+#pragma unroll
+          for (int rr = 0; rr < r; ++rr) s -= S[(c0 + r) * LD + c0 + rr] * u[rr];
+          u[r] = s;
+        }
+      }
+#pragma unroll
+      for (int r = 1; r < PB; ++r)
+        if (r < w) S[(c0 + r) * LD + j] = u[r];
+    }
+    __syncthreads();
+    // the trailing block [pe, D)^2 -= L21 U12, 4 x 4 tiles per thread
+    const int R = D - pe, MT = (R + 3) / 4;
+    for (int t = tid; t < MT * MT; t += NT) {
+      const int i0 = pe + (t / MT) * 4, j0 = pe + (t % MT) * 4;
+      double acc[4][4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+      for (int kk = c0; kk < pe; ++kk) {
+        double a[4], b[4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x) a[x] = i0 + x < D ? S[(i0 + x) * LD + kk] : 0.0;
+#pragma unroll
+        for (int y = 0; y < 4; ++y) b[y] = j0 + y < D ? S[kk * LD + j0 + y] : 0.0;
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] += a[x] * b[y];
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+          if (i0 + x < D && j0 + y < D) S[(i0 + x) * LD + j0 + y] -= acc[x][y];
+    }
+    __syncthreads();
   }
-  for (int i = l; i < N; i += 32) x[d_sp_perm[i]] = t[i];
-  __syncwarp();
+  return bad;
+}
+
+// the LU of the Newton matrix: A (sparse rows and the dense rows' sparse
+// columns) and S (the dense block); rpiv[i] = 1 / pivot i. 0, or 1 for a
+// zero or non-finite pivot. Starts and ends with a block barrier.
+__device__ int block_lu(double* A) {
+  double* S = smem() + SM::S;
+  double* rpiv = smem() + SM::RPIV;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  bool bad = false;
+  __syncthreads();
+  for (int L = 0; L < BK_NLF; ++L) {
+    const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
+    if (r1 - r0 >= 16) {
+      for (int r = r0 + tid; r < r1; r += NT) {
+        const int i = d_bk_frow[r];
+        elim_thread(d_sp_rp[i], d_sp_di[i], A, S, rpiv);
+        const double piv = A[d_sp_di[i]];
+        rpiv[i] = 1.0 / piv;
+        bad = bad || piv == 0.0 || !isfinite(piv);
+      }
+    } else {
+      for (int r = r0 + warp; r < r1; r += NWARP) {
+        const int i = d_bk_frow[r];
+        elim_warp(d_sp_rp[i], d_sp_di[i], A, rpiv);
+        if (lane == 0) {
+          const double piv = A[d_sp_di[i]];
+          rpiv[i] = 1.0 / piv;
+          bad = bad || piv == 0.0 || !isfinite(piv);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = BK_M + tid; i < N; i += NT)
+    elim_thread(d_sp_rp[i], d_bk_l21e[i - BK_M], A, S, rpiv);
+  __syncthreads();
+  bad = dense_lu(S, rpiv + BK_M) || bad;
+  return __syncthreads_or(bad) ? 1 : 0;
+}
+
+// ---- the solves ----
+// x = L22^-1 x, L22 the dense block's unit lower factor
+__device__ void dense_fwd(const double* S, double* x) {
+  constexpr int D = BK_D, LD = BK_LD;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int b0 = 0; b0 < D; b0 += 32) {
+    const int be = b0 + 32 < D ? b0 + 32 : D;
+    if (tid < 32) {
+      const int i = b0 + lane;
+      double v = i < be ? x[i] : 0.0;
+      for (int j = b0; j < be - 1; ++j) {
+        const double xj = __shfl_sync(FULLM, v, j - b0);
+        if (i > j && i < be) v -= S[i * LD + j] * xj;
+      }
+      if (i < be) x[i] = v;
+    }
+    __syncthreads();
+    if (be < D) {
+      for (int i = be + tid; i < D; i += NT) {
+        double s = 0.0;
+        for (int j = b0; j < be; ++j) s += S[i * LD + j] * x[j];
+        x[i] -= s;
+      }
+      __syncthreads();
+    }
+  }
+}
+// x = U22^-1 x, U22 the dense block's upper factor (rpd: 1 / its diagonal)
+__device__ void dense_bwd(const double* S, const double* rpd, double* x) {
+  constexpr int D = BK_D, LD = BK_LD;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int be = D; be > 0; be -= 32) {
+    const int b0 = be - 32 > 0 ? be - 32 : 0;
+    if (tid < 32) {
+      const int i = b0 + lane;
+      double v = i < be ? x[i] : 0.0;
+      for (int j = be - 1; j >= b0; --j) {
+        if (i == j) v *= rpd[j];
+        const double xj = __shfl_sync(FULLM, v, j - b0);
+        if (i < j) v -= S[i * LD + j] * xj;
+      }
+      if (i < be) x[i] = v;
+    }
+    __syncthreads();
+    if (b0 > 0) {
+      for (int i = tid; i < b0; i += NT) {
+        double s = 0.0;
+        for (int j = b0; j < be; ++j) s += S[i * LD + j] * x[j];
+        x[i] -= s;
+      }
+      __syncthreads();
+    }
+  }
+}
+// x = A^-1 b with the factors (b and x in the species order; x may be b).
+// Starts and ends with a block barrier.
+__device__ void block_solve(const double* A, const double* b, double* x) {
+  const double* S = smem() + SM::S;
+  const double* rpiv = smem() + SM::RPIV;
+  double* t = smem() + SM::T;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __syncthreads();
+  KBG_FOR(i) t[i] = b[d_sp_perm[i]];
+  __syncthreads();
+  for (int L = 1; L < BK_NLF; ++L) {  // level 0 rows have no L entries
+    const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
+    if (r1 - r0 >= 16) {
+      for (int r = r0 + tid; r < r1; r += NT) {
+        const int i = d_bk_frow[r];
+        double s = 0.0;
+        for (int p = d_sp_rp[i]; p < d_sp_di[i]; ++p) s += A[p] * t[d_sp_ci[p]];
+        t[i] -= s;
+      }
+    } else {
+      for (int r = r0 + warp; r < r1; r += NWARP) {
+        const int i = d_bk_frow[r];
+        double s = 0.0;
+        for (int p = d_sp_rp[i] + lane; p < d_sp_di[i]; p += 32)
+          s += A[p] * t[d_sp_ci[p]];
+        s = warp_sum(s);
+        if (lane == 0) t[i] -= s;
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = BK_M + tid; i < N; i += NT) {
+    double s = 0.0;
+    for (int p = d_sp_rp[i]; p < d_bk_l21e[i - BK_M]; ++p) s += A[p] * t[d_sp_ci[p]];
+    t[i] -= s;
+  }
+  __syncthreads();
+  dense_fwd(S, t + BK_M);
+  dense_bwd(S, rpiv + BK_M, t + BK_M);
+  for (int L = 0; L < BK_NLB; ++L) {
+    const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
+    if (r1 - r0 >= 16) {
+      for (int r = r0 + tid; r < r1; r += NT) {
+        const int i = d_bk_brow[r];
+        double s = 0.0;
+        for (int q = d_sp_di[i] + 1; q < d_sp_rp[i + 1]; ++q) s += A[q] * t[d_sp_ci[q]];
+        t[i] = (t[i] - s) * rpiv[i];
+      }
+    } else {
+      for (int r = r0 + warp; r < r1; r += NWARP) {
+        const int i = d_bk_brow[r];
+        double s = 0.0;
+        for (int q = d_sp_di[i] + 1 + lane; q < d_sp_rp[i + 1]; q += 32)
+          s += A[q] * t[d_sp_ci[q]];
+        s = warp_sum(s);
+        if (lane == 0) t[i] = (t[i] - s) * rpiv[i];
+      }
+    }
+    __syncthreads();
+  }
+  KBG_FOR(i) x[d_sp_perm[i]] = t[i];
+  __syncthreads();
 }
 
 struct Stats9 {
   long nst, nfe, nje, nsetups, nni, nnf, netf;
 };
 
-// one cell's CVODE (the oracle's Cvode, sparse path, one warp)
+// one cell's CVODE (the oracle's Cvode, sparse path, one block)
 struct BigCvode {
   Net& P;
   const SolveOpts& o;
   double* zn[L_MAX];
-  double *ewt, *y, *acor, *tempv, *ftemp, *delta, *A, *savedJ, *ts, *wrow;
+  double *ewt, *y, *acor, *tempv, *ftemp, *delta, *A, *savedJ;
   Stats9 st;
   long mxstep;
   double tn, h, hin, hprime, hscale, next_h, hu, eta, etamax, etaq;
@@ -282,13 +634,10 @@ struct BigCvode {
     tempv = w + WS::TEMPV;
     ftemp = w + WS::FTEMP;
     delta = w + WS::DELTA;
-    ts = w + WS::TS;
-    wrow = w + WS::WROW;
     savedJ = w + WS::SJ;
     A = w + WS::A;
     mxstep = o.max_steps == 0 ? 500
              : (o.max_steps < 0 ? KB_MAX_STEPS_CAP : o.max_steps);
-    v_const(0.0, wrow);
   }
 
   __device__ void reinit(double t0, const double* y0, double h_init) {
@@ -311,13 +660,12 @@ struct BigCvode {
   __device__ int ewt_set(const double* ycur, double* wt) {
     const double at = o.atol_n;
     bool bad = false;
-    for (int i = lane_id(); i < N; i += 32) {
+    KBG_FOR(i) {
       const double v = (o.rtol * fabs(ycur[i])) + at;
       bad = bad || !(v > 0.0);
       wt[i] = 1.0 / v;
     }
-    __syncwarp();
-    return __any_sync(FULLM, bad) ? -1 : 0;
+    return __syncthreads_or(bad) ? -1 : 0;
   }
 
   // CVode(tout, NORMAL) (bdf_cell.hpp:566-638); y(tout) into yout
@@ -423,16 +771,12 @@ struct BigCvode {
   __device__ double upper_bound_h0_(double tdist) {
     double* temp1 = tempv;
     double* temp2 = acor;
-    for (int i = lane_id(); i < N; i += 32) temp2[i] = fabs(zn[0][i]);
-    __syncwarp();
+    KBG_FOR(i) temp2[i] = fabs(zn[0][i]);
     ewt_set(zn[0], temp1);
-    for (int i = lane_id(); i < N; i += 32) temp1[i] = 1.0 / temp1[i];
-    __syncwarp();
+    KBG_FOR(i) temp1[i] = 1.0 / temp1[i];
     v_lin_sum(HUB_FACTOR, temp2, 1.0, temp1, temp1);
-    for (int i = lane_id(); i < N; i += 32) temp2[i] = fabs(zn[1][i]);
-    __syncwarp();
-    for (int i = lane_id(); i < N; i += 32) temp1[i] = temp2[i] / temp1[i];
-    __syncwarp();
+    KBG_FOR(i) temp2[i] = fabs(zn[1][i]);
+    KBG_FOR(i) temp1[i] = temp2[i] / temp1[i];
     const double hub_inv = v_max_norm(temp1);
     double hub = HUB_FACTOR * tdist;
     if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
@@ -615,7 +959,7 @@ struct BigCvode {
       for (;;) {
         niters++;
         v_scale(-1.0, delta, delta);
-        sp_getrs(A, delta, ts, delta);
+        block_solve(A, delta, delta);
         if (gamrat != 1.0) v_scale(2.0 / (1.0 + gamrat), delta, delta);
         v_lin_sum(1.0, acor, 1.0, delta, acor);
         retval = conv_test_(curiter, tol);
@@ -691,18 +1035,26 @@ struct BigCvode {
     jcur = jbad_ls;
     if (jbad_ls) P.jac(y, savedJ);
     const double c = -gamma;
-    const int l0 = lane_id();
-    for (int k = l0; k < NNZ_LU; k += 32) A[k] = 0.0;
-    __syncwarp();
-    for (int e = l0; e < NNZ_J; e += 32) A[d_sp_jpos[e]] = savedJ[e] * c;
-    __syncwarp();
-    for (int i = l0; i < N; i += 32) A[d_sp_di[i]] += 1.0;
-    __syncwarp();
+    double* S = smem() + SM::S;
+    for (int k = threadIdx.x; k < NNZ_LU; k += NT) A[k] = 0.0;
+    for (int k = threadIdx.x; k < BK_D * BK_LD; k += NT) S[k] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < NNZ_J; e += NT) {
+      const int t = d_bk_jt[e];
+      const double v = savedJ[e] * c;
+      if (t >= 0) A[t] = v;
+      else S[-1 - t] = v;
+    }
+    __syncthreads();
+    KBG_FOR(i) {
+      if (i < BK_M) A[d_sp_di[i]] += 1.0;
+      else S[(i - BK_M) * (BK_LD + 1)] += 1.0;
+    }
     if (jcur) {
       st.nje++;
       nstlj = st.nst;
     }
-    return sp_getrf(A, wrow) > 0 ? LS_LUFACT_FAIL : 0;
+    return block_lu(A) > 0 ? LS_LUFACT_FAIL : 0;
   }
   __device__ int handle_nflag_(int* nflagPtr, double saved_t, int* ncfPtr) {
     const int nflag = *nflagPtr;

@@ -454,16 +454,16 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
 }
 
 #ifdef KB_LARGE_NETWORK
-// ---- the large networks: one warp per cell (bdf_big.cuh) ----
+// ---- the large networks: one thread block per cell (bdf_big.cuh) ----
 
-// cell c on this warp: the pre-solve rules, the restart wrapper
+// cell c on this block: the pre-solve rules, the restart wrapper
 // (bdf_cell.hpp:1513-1547) and the post-solve rules (solve_cell.hpp:
-// 2094-2203) around the sparse-path CVODE, fixed Tgas
+// 2094-2203) around the sparse-path CVODE, fixed Tgas. Every thread runs
+// the same control flow (the CVODE scalars are the same in every thread).
 __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
                              const double* par, int pstride, int* flags,
                              long* stats, const SolveOpts& so, double* ws) {
   using namespace kbnet;
-  const int lane = threadIdx.x & 31;
   int flag = 1;
   if (so.fail_every > 0 && (c + 1) % so.fail_every == 0) flag = kbw::TOO_MUCH_WORK;
   else if (!(dt[c] > 0.0)) flag = 0;
@@ -477,10 +477,14 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
     P.T = fmin(fmax(T[c], P.p.Tcmb), 1e9);
     double* nrow = n + (long)c * NSPEC;
     double* k = ws + kbg::WS::K;
-    for (int r = lane; r <= NREA; r += 32) k[r] = 0.0;
-    __syncwarp();
-    if (lane == 0) rates_fixed(P.T, nrow, P.p, k);
-    __syncwarp();
+    for (int r = threadIdx.x; r <= NREA; r += kbg::NT) k[r] = 0.0;
+    __syncthreads();
+    // the Tgas/parameter-only rates once per solve, and the three points
+    // of the density-dependent ones
+    const double hnuc = P.load_state(nrow);
+    if (threadIdx.x < RPART)
+      rates_fixed_part(threadIdx.x, P.T, kbg::smem() + kbg::SM::YR, P.p, hnuc, k);
+    P.prepare_var(nrow);
     kbg::BigCvode cv(P, so);
     double* yout = ws + kbg::WS::YOUT;
     cv.reinit(0.0, nrow, 0.0);
@@ -505,36 +509,36 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
     }
     tot[kbw::ST_RESTARTS] = restarts;
     if (flag == 0) {
-      for (int i = lane; i < NSPEC; i += 32) {
+      for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) {
         double v = yout[i];
         if (so.clip_negative && v < 0.0) v = 0.0;
         nrow[i] = v;
       }
     }
-    __syncwarp();
   }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     if (flags != nullptr) flags[c] = flag;
     if (stats != nullptr)
       for (int i = 0; i < kbw::NSTAT; ++i) stats[(long)c * kbw::NSTAT + i] = tot[i];
   }
+  __syncthreads();  // the workspace and shared memory are free again
 }
 
-// warps take cells from the work queue `cursor`; each resident warp owns
-// the workspace slot of its global warp index (kbg::WS::SIZE doubles)
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// blocks take cells from the work queue `cursor`; each resident block owns
+// the workspace slot of its block index (kbg::WS::SIZE doubles)
+__global__ void __launch_bounds__(kbg::NT, 1)
 kb_big_cells(int ncell, double* n, double* T, const double* dt,
              const double* par, int pstride, int* flags, long* stats,
              SolveOpts so, unsigned* cursor, double* ws_base) {
-  const int lane = threadIdx.x & 31;
-  const long wg = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  double* ws = ws_base + wg * kbg::WS::SIZE;
-  for (;;) {  // at most ncell + 1 pops per warp: the cursor only grows
-    unsigned c0 = 0;
-    if (lane == 0) c0 = atomicAdd(cursor, 1u);
-    const int c = (int)__shfl_sync(0xffffffffu, c0, 0);
-    if (c >= ncell) break;
-    big_one_cell(c, n, T, dt, par, pstride, flags, stats, so, ws);
+  double* ws = ws_base + (long)blockIdx.x * kbg::WS::SIZE;
+  double* slot = kbg::smem() + kbg::SM::MISC;
+  for (;;) {  // at most ncell + 1 pops per block: the cursor only grows
+    if (threadIdx.x == 0) slot[0] = (double)atomicAdd(cursor, 1u);
+    __syncthreads();
+    const double cd = slot[0];
+    __syncthreads();
+    if (cd >= (double)ncell) break;
+    big_one_cell((int)cd, n, T, dt, par, pstride, flags, stats, so, ws);
   }
 }
 #endif
@@ -624,14 +628,14 @@ int num_sms() {
 }
 
 #ifdef KB_LARGE_NETWORK
-// the large networks' per-warp workspace: one device buffer, grown to
-// `warps` slots when it is smaller (a cudaMalloc: not inside a stream
+// the large networks' per-block workspace: one device buffer, grown to
+// `slots` slots when it is smaller (a cudaMalloc: not inside a stream
 // capture, so graph_new grows it before capturing)
 std::mutex g_ws_mu;
 DevBuf g_ws;
-double* big_workspace(long warps) {
+double* big_workspace(long slots) {
   std::lock_guard<std::mutex> lk(g_ws_mu);
-  const size_t bytes = (size_t)warps * kbg::WS::SIZE * sizeof(double);
+  const size_t bytes = (size_t)slots * kbg::WS::SIZE * sizeof(double);
   if (g_ws.p != nullptr && g_ws.cap >= bytes) return (double*)g_ws.p;
   if (g_ws.ensure(bytes) != cudaSuccess) return nullptr;
   return (double*)g_ws.p;
@@ -645,27 +649,38 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    cudaStream_t stream, const RecIO* rio = nullptr) {
   const SolveOpts so = to_solve_opts(h);
 #ifdef KB_LARGE_NETWORK
-  // the sparse path: one warp per cell over a persistent grid, each warp
-  // with its workspace slot (the library's device buffer, grown before a
-  // launch when needed; never during a graph capture: big_workspace)
+  // the sparse path: one block per cell over a persistent grid (one block
+  // per SM: the dense block of the LU fills shared memory), each block with
+  // its workspace slot (the library's device buffer, grown before a launch
+  // when needed; never during a graph capture: big_workspace)
   (void)rio;
   if (EVT) return cudaErrorNotSupported;
+  if (cursor == nullptr) return cudaErrorInvalidValue;  // always the queue
   {
-    const int threads = kWarpsPerBlock * 32;
-    int per_sm = h.blocks_per_sm;
-    if (per_sm <= 0) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_big_cells,
-                                                    threads, 0);
-      if (per_sm <= 0) per_sm = 1;
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+      const cudaError_t e = cudaFuncSetAttribute(
+          kb_big_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int)kbg::SMEM_BYTES);
+      if (e != cudaSuccess) return e;
+      attr[dev] = true;
     }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_big_cells,
+                                                  kbg::NT, kbg::SMEM_BYTES);
+    if (per_sm <= 0) per_sm = 1;
     long blocks = (long)num_sms() * per_sm;
-    const long need = ((long)ncell + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    if (blocks > need) blocks = need > 0 ? need : 1;
-    double* ws = big_workspace(blocks * kWarpsPerBlock);
+    if (h.blocks_per_sm > 0 && h.blocks_per_sm < per_sm)
+      blocks = (long)num_sms() * h.blocks_per_sm;
+    if (blocks > ncell) blocks = ncell > 0 ? ncell : 1;
+    double* ws = big_workspace(blocks);
     if (ws == nullptr) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
-    kb_big_cells<<<(int)blocks, threads, 0, stream>>>(
+    kb_big_cells<<<(int)blocks, kbg::NT, kbg::SMEM_BYTES, stream>>>(
         ncell, n, T, dt, par, pstride, flags, stats, so, cursor, ws);
     return cudaGetLastError();
   }
@@ -961,6 +976,9 @@ KB_API int krome_b200_solve_device(int ncell, double* n, double* Tgas,
       || flags == nullptr)
     return -1;
   if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+#ifdef KB_LARGE_NETWORK
+  if (cursor == nullptr) return -1;  // the large path always takes the queue
+#endif
   if (cursor == nullptr && (h->kernel == 1)) return -1;
   if (const int u = unsupported(*h)) return u;
   const cudaError_t e = launch_any(*h, ncell, n, Tgas, dt, par, par_stride,

@@ -205,19 +205,32 @@ class Emitter:
         nH = [float(self.gen._natoms_H(s)) if hasattr(self.gen, "_natoms_H")
               else float((sp[s]["composition"] or {}).get("H", 0))
               for s in self.species]
-        w("KB_HD inline double species_mass_g(int i) {")
-        w("  constexpr double t_[NSPEC] = {%s};"
-          % ", ".join(repr(float(m)) for m in mass_g))
-        w("  return t_[i];")
-        w("}")
-        w("KB_HD inline int species_charge(int i) {")
-        w("  constexpr int t_[NSPEC] = {%s};" % ", ".join(str(c) for c in charge))
-        w("  return t_[i];")
-        w("}")
-        w("KB_HD inline double species_natoms_H(int i) {")
-        w("  constexpr double t_[NSPEC] = {%s};" % ", ".join(repr(x) for x in nH))
-        w("  return t_[i];")
-        w("}")
+        tabs = (("double", "species_mass_g", [repr(float(m)) for m in mass_g]),
+                ("int", "species_charge", [str(c) for c in charge]),
+                ("double", "species_natoms_H", [repr(x) for x in nH]))
+        self.natoms_H = list(nH)
+        for ty, name, vals in tabs:
+            body = ", ".join(vals)
+            if ns > LARGE_NSPEC:
+                # a large network's tables live in global memory on the
+                # device (a function-local array indexed at run time would
+                # be rebuilt in local memory at every call)
+                w("inline constexpr %s %s_t_[NSPEC] = {%s};" % (ty, name, body))
+                w("#ifdef __CUDACC__")
+                w("__device__ const %s d_%s_[NSPEC] = {%s};" % (ty, name, body))
+                w("#endif")
+                w("KB_HD inline %s %s(int i) {" % (ty, name))
+                w("#ifdef __CUDA_ARCH__")
+                w("  return d_%s_[i];" % name)
+                w("#else")
+                w("  return %s_t_[i];" % name)
+                w("#endif")
+                w("}")
+            else:
+                w("KB_HD inline %s %s(int i) {" % (ty, name))
+                w("  constexpr %s t_[NSPEC] = {%s};" % (ty, body))
+                w("  return t_[i];")
+                w("}")
         # summing helpers: sequential sums in species order (reference:
         # generated net_<name>_core.hpp ntot_ / Hnuclei_ / rho_)
         w("KB_HD inline double ntot_(const double* n) {")
@@ -794,6 +807,7 @@ class Emitter:
         eb = gen._surf_eb
         ice = [x for x in sp_sorted if net.species[x]["phase"] != "gas"
                and base[x] == "H2O" and net.species[x]["label"] != "c"]
+        self.ice_idx = self.idx[ice[0]] if ice else -1
         legacy_nu = gen.surface_nu == "LEGACY"
         w("// ---- grain-surface chemistry (binding energies %s, vibration"
           % gen.binding_energies)
@@ -960,29 +974,101 @@ class Emitter:
                 groups[rx["group"]].append(rx)
         return units
 
+    RPART = 256  # rate parts of a large network: one per thread of a cell's block
+
+    def _var_closure(self, names):
+        """the vars `names` and every var they reference, in the order the
+        vars are defined (dependencies first)"""
+        net = self.net
+        need, todo = set(), list(names)
+        while todo:
+            v = todo.pop()
+            if v in need:
+                continue
+            need.add(v)
+            for nd in self.gen.deep_walk(net.vars[v]):
+                if nd.get("kind") == "var":
+                    todo.append(nd["s"])
+        order = getattr(net, "var_order", None) or list(net.vars)
+        return [v for v in order if v in need]
+
+    def _hoist_inline(self, rxs, tvar, indent):
+        """hoist() for the rate parts: the vars as expressions of locals,
+        with the H-nuclei density the parameter hnuc (one block reduction per
+        evaluation instead of a species sum in every part)"""
+        names = sorted({nd["s"] for rx in rxs
+                        for nd in self.gen.deep_walk(rx["rate"]["ast"])
+                        if nd.get("kind") == "var"})
+        self.hoisted = {}
+        for v in self._var_closure(names):
+            e = self.cx(self.net.vars[v], tvar).replace("Hnuclei_(n)", "hnuc")
+            self.w("%sconst double vh_%s = %s;" % (indent, v, e))
+            self.w("%s(void)vh_%s;" % (indent, v))
+            self.hoisted[v] = "vh_" + v
+
     def emit_rate_parts(self):
         """rates_fixed_part / rates_var_part: the rate coefficients split
-        into NPART parts (lane `part` of a warp computes its part)"""
+        into RPART parts (thread `part` of a cell's block computes its
+        part); hnuc = Hnuclei_(n) of the same n"""
         gen = self.gen
+        self.w("constexpr int RPART = %d;" % self.RPART)
+        hoist0 = self.hoist
+        self.hoist = self._hoist_inline
         for name, sel in (("fixed", gen.rate_is_fixed),
                           ("var", lambda rx: not gen.rate_is_fixed(rx))):
             units = self._rate_units(sel)
             part_of = {}
             for u, unit in enumerate(units):
                 for rx in unit:
-                    part_of[rx["id"]] = u % self.NPART
+                    part_of[rx["id"]] = u % self.RPART
             self.w("KB_HD inline void rates_%s_part(int part, double Tgas, "
-                   "const double* n, const Params& p, double* k) {" % name)
-            self.w("  (void)Tgas; (void)n; (void)p; (void)k;")
+                   "const double* n, const Params& p, double hnuc, double* k) {"
+                   % name)
+            self.w("  (void)Tgas; (void)n; (void)p; (void)hnuc; (void)k;")
             self.w("  switch (part) {")
-            for j in range(self.NPART):
+            for j in range(self.RPART):
                 self.w("  case %d: {" % j)
+                first = len(self.lines)
                 self.emit_grouped(self._rate_body,
                                   lambda rx, j=j: sel(rx) and part_of.get(rx["id"]) == j)
+                for q in range(first, len(self.lines)):
+                    self.lines[q] = self.lines[q].replace("Hnuclei_(n)", "hnuc")
                 self.w("  } break;")
             self.w("  default: break;")
             self.w("  }")
             self.w("}")
+        self.hoist = hoist0
+        # the density-dependent rates, and how they depend on the state:
+        # through the water-ice coverage fi of the surface functions (affine
+        # in fi) and the H-nuclei density (linear), nothing else -- then
+        # with Tgas and Tdust fixed a solve needs each of them at three
+        # points only (fi = 0, fi = 1, hnuc = 1; a test checks the form
+        # against the direct evaluation)
+        var_rx = [rx for rx in self.net.reactions
+                  if rx["rate"]["kind"] == "expr" and not gen.rate_is_fixed(rx)]
+        var = sorted(rx["id"] - 1 for rx in var_rx)
+        direct = any(nd.get("kind") == "density" for rx in var_rx
+                     for nd in gen.deep_walk(rx["rate"]["ast"]))
+        self.w("constexpr int BK_NVAR = %d;" % len(var))
+        self.w("constexpr int BK_ICE = %d;  // the ice species (-1: none)"
+               % getattr(self, "ice_idx", -1))
+        self.w("constexpr int BK_VAR_AFFINE = %d;" % (0 if direct else 1))
+        self._table("bk_var", var or [0])
+        ice = getattr(self, "ice_idx", -1)
+        self.w("// the ice coverage of state n, and n with coverage 0 or 1")
+        self.w("KB_HD inline double bk_ice_cover(const double* n, const Params& p) {")
+        if ice >= 0:
+            self.w("  return surf::ice_cover(n, surf::sites(p));")
+        else:
+            self.w("  (void)n; (void)p;")
+            self.w("  return 0.0;")
+        self.w("}")
+        self.w("KB_HD inline void bk_set_ice(double* n, const Params& p, int full) {")
+        if ice >= 0:
+            self.w("  n[%d] = full ? surf::sites(p) : 0.0;" % ice)
+        else:
+            self.w("  (void)n; (void)p; (void)full;")
+        self.w("}")
         self.w("")
 
     def _sparse_pattern(self):
@@ -1100,6 +1186,7 @@ class Emitter:
         self._table("sp_perm", order)
         self._table("sp_iperm", [new[v] for v in range(n)])
         self._table("sp_jpos", jpos)
+        self._emit_block_tables(n, rp, ci, di, pos, jpos)
         w("")
         P = self.NPART
         # fluxes: fl[r] = k[r] * (kinetic reactants)
@@ -1179,6 +1266,19 @@ class Emitter:
         self._table("rs_rp", rs_rp)
         self._table("rs_r", rs_r)
         self._table("rs_s", rs_s)
+        # the same terms in chunks of at most GCHUNK (a species' chunks
+        # consecutive): a thread sums a chunk, then a species its chunks in
+        # order -- the hub species' hundreds of terms spread over threads
+        GCHUNK = 16
+        ck_t, ck_rp = [], [0]
+        for sidx in range(n):
+            for a in range(rs_rp[sidx], rs_rp[sidx + 1], GCHUNK):
+                ck_t.append(a)
+            ck_rp.append(len(ck_t))
+        ck_t.append(rs_rp[n])
+        w("constexpr int NCHUNK = %d;  // rhs term chunks" % (len(ck_t) - 1))
+        self._table("ck_t", ck_t)
+        self._table("ck_rp", ck_rp)
         jt_rp, jt_r, jt_c, jt_o0, jt_o1 = [0], [], [], [], []
         jtab = [[] for _ in ent]
         for rx in self.net.reactions:
@@ -1230,6 +1330,95 @@ class Emitter:
         w("  }")
         w("}")
         w("")
+
+    BK_DMAX = 160  # the dense trailing block of a cell's LU, in shared memory
+
+    def _emit_block_tables(self, n, rp, ci, di, pos, jpos):
+        """the schedule of the block-per-cell factorization and solves: the
+        first BK_M rows of the elimination order are sparse, the last BK_D
+        rows and columns form a dense block S (row stride BK_LD, in shared
+        memory).
+          bk_frow / bk_flp   the sparse rows by forward level (a row's level
+                             is one above the highest level of the rows its
+                             L entries eliminate with; level 0: no L entries)
+          bk_brow / bk_blp   the sparse rows by backward level (over the U
+                             entries in sparse columns)
+          bk_uoff[p]         for an L entry p = (i, k) with k a sparse row:
+                             where the targets of its update start in bk_tgt
+          bk_tgt             per L entry (i, k), per U entry (k, j) of row k
+                             in order: the place of (i, j) -- an index into
+                             the LU values (>= 0) or -1 - its index in S
+          bk_jt[e]           the place of Jacobian entry e, the same way
+          bk_l21e[i - BK_M]  the end of dense row i's sparse-column L entries
+          d_bk_hnuc          H nuclei per species (the terms of Hnuclei_)"""
+        w = self.w
+        D = min(self.BK_DMAX, n)
+        m = n - D
+        LD = D + 1 if D % 2 == 0 else D
+        code = lambda i, j: (pos[(i, j)] if (i < m or j < m)
+                             else -1 - ((i - m) * LD + (j - m)))
+        lf = [0] * n
+        for i in range(m):
+            ks = ci[rp[i]:di[i]]
+            lf[i] = 1 + max(lf[k] for k in ks) if ks else 0
+        nlf = (max(lf[:m]) + 1) if m else 0
+        frow = sorted(range(m), key=lambda i: (lf[i], i))
+        flp = [0] * (nlf + 1)
+        for i in range(m):
+            flp[lf[i] + 1] += 1
+        for L in range(nlf):
+            flp[L + 1] += flp[L]
+        lb = [0] * n
+        for i in range(m - 1, -1, -1):
+            js = [j for j in ci[di[i] + 1:rp[i + 1]] if j < m]
+            lb[i] = 1 + max(lb[j] for j in js) if js else 0
+        nlb = (max(lb[:m]) + 1) if m else 0
+        brow = sorted(range(m), key=lambda i: (lb[i], i))
+        blp = [0] * (nlb + 1)
+        for i in range(m):
+            blp[lb[i] + 1] += 1
+        for L in range(nlb):
+            blp[L + 1] += blp[L]
+        uoff = [-1] * len(ci)
+        tgt = []
+        l21e = []
+        for i in range(n):
+            for p in range(rp[i], di[i]):
+                k = ci[p]
+                if k >= m:
+                    continue
+                uoff[p] = len(tgt)
+                for q in range(di[k] + 1, rp[k + 1]):
+                    tgt.append(code(i, ci[q]))
+            if i >= m:
+                e = rp[i]
+                while e < rp[i + 1] and ci[e] < m:
+                    e += 1
+                l21e.append(e)
+        inv = {v: key for key, v in pos.items()}
+        jt = [code(*inv[q]) for q in jpos]
+        self.meta["bk_m"] = m
+        self.meta["bk_d"] = D
+        w("// the block-per-cell LU: sparse rows [0, BK_M), dense block S of the")
+        w("// last BK_D rows (row stride BK_LD) in shared memory")
+        w("constexpr int BK_M = %d;" % m)
+        w("constexpr int BK_D = %d;" % D)
+        w("constexpr int BK_LD = %d;" % LD)
+        w("constexpr int BK_NLF = %d;" % nlf)
+        w("constexpr int BK_NLB = %d;" % nlb)
+        w("constexpr int BK_NTGT = %d;" % len(tgt))
+        self._table("bk_frow", frow or [0])
+        self._table("bk_flp", flp)
+        self._table("bk_brow", brow or [0])
+        self._table("bk_blp", blp)
+        self._table("bk_uoff", uoff)
+        self._table("bk_tgt", tgt or [0])
+        self._table("bk_jt", jt)
+        self._table("bk_l21e", l21e or [0])
+        w("#ifdef __CUDACC__")
+        w("__device__ const double d_bk_hnuc[NSPEC] = {%s};"
+          % ",".join(repr(float(v)) for v in self.natoms_H))
+        w("#endif")
 
     def _rates_depend_on_n(self):
         """whether a rate coefficient depends on the densities (through

@@ -1206,6 +1206,43 @@ ORACLE_API void oracle_rates(double T, const double* n, const double* par,
   rates_fixed(T, n, p, k);
   rates_var(T, n, p, k);
 }
+#ifdef KB_LARGE_NETWORK
+// the large path's forms of the rate coefficients, beside the direct
+// evaluation of oracle_rates: kp from the generated parts (hnuc =
+// Hnuclei_(n)), ka with the density-dependent rates from their three points
+// (fi = 0, fi = 1, hnuc = 1) as e0 (1 - fi) + e1 fi + eh hnuc. Returns
+// BK_VAR_AFFINE.
+ORACLE_API int oracle_rates_forms(double T, const double* n,
+                                  const double* par, double* kp, double* ka) {
+  Params p;
+  params_from_row(par, p);
+  const double h = Hnuclei_(n);
+  for (int i = 0; i < NREA; ++i) kp[i] = 0.0;
+  for (int part = 0; part < RPART; ++part) {
+    rates_fixed_part(part, T, n, p, h, kp);
+    rates_var_part(part, T, n, p, h, kp);
+  }
+  std::vector<double> y(n, n + NSPEC);
+  y.push_back(1.0);
+  std::vector<double> k(NREA, 0.0), e0(BK_NVAR), e1(BK_NVAR), eh(BK_NVAR);
+  for (int pt = 0; pt < 3; ++pt) {
+    bk_set_ice(y.data(), p, pt == 1);
+    for (int part = 0; part < RPART; ++part)
+      rates_var_part(part, T, y.data(), p, pt == 2 ? 1.0 : 0.0, k.data());
+    for (int j = 0; j < BK_NVAR; ++j) {
+      const double v = k[bk_var[j]];
+      if (pt == 0) e0[j] = v;
+      else if (pt == 1) e1[j] = v;
+      else eh[j] = v - e0[j];
+    }
+  }
+  const double fi = bk_ice_cover(n, p);
+  for (int i = 0; i < NREA; ++i) ka[i] = kp[i];
+  for (int j = 0; j < BK_NVAR; ++j)
+    ka[bk_var[j]] = e0[j] * (1.0 - fi) + e1[j] * fi + eh[j] * h;
+  return BK_VAR_AFFINE;
+}
+#endif
 ORACLE_API int oracle_nrea(void) { return NREA; }
 ORACLE_API int oracle_nspec(void) { return NSPEC; }
 ORACLE_API int oracle_npar(void) { return NPAR; }

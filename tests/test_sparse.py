@@ -8,22 +8,236 @@ large-network parity metric (conftest.parity_major): every abundance above
 up to ~5e-5 on this workload -- most cells within 10 rtol, flags equal, and
 the total mass conserved."""
 import ctypes
+import re
 
 import numpy as np
 import pytest
 
-from conftest import golden, parity_major
+from conftest import ROOT, golden, parity_major
 from krome_x_b200 import krome, netinfo, workloads
 from oracle import Oracle
 
 KEY = "semenov"
+TABLES = ("sp_rp", "sp_ci", "sp_di", "sp_perm", "sp_jpos", "bk_frow",
+          "bk_flp", "bk_brow", "bk_blp", "bk_uoff", "bk_tgt", "bk_jt",
+          "bk_l21e")
+
+
+@pytest.fixture(scope="module")
+def sched():
+    """the sparse LU's generation-time tables and constants, read from the
+    generated network header"""
+    text = (ROOT / "krome_x_b200" / "networks" / ("net_%s.h" % KEY)).read_text()
+    t = {}
+    for name in TABLES:
+        m = re.search(r"#define KB_T_%s ([0-9,\-]+)" % name, text)
+        t[name] = np.array([int(x) for x in m.group(1).split(",")])
+    for k, v in re.findall(r"constexpr int (BK_\w+|NSPEC|NNZ_LU|NNZ_J) = "
+                           r"(-?\d+);", text):
+        t[k] = int(v)
+    return t
+
+
+def _block_lu(t, A, S):
+    """the kernel's factorization (bdf_big.cuh block_lu), phase by phase:
+    the sparse rows level by level (each level's rows in reverse order: the
+    rows of a level are independent), the dense rows' sparse columns, the
+    dense block in panels of 16. Returns 1 / the pivots."""
+    rp, ci, di = t["sp_rp"], t["sp_ci"], t["sp_di"]
+    m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
+    rpiv = np.zeros(n)
+
+    def elim(p0, p1):
+        for p in range(p0, p1):
+            k = ci[p]
+            l = A[p] * rpiv[k]
+            A[p] = l
+            q0, q1 = di[k] + 1, rp[k + 1]
+            tg = t["bk_tgt"][t["bk_uoff"][p]:t["bk_uoff"][p] + q1 - q0]
+            u = A[q0:q1].copy()
+            a = tg >= 0
+            A[tg[a]] -= l * u[a]
+            S[-1 - tg[~a]] -= l * u[~a]
+    flp, frow = t["bk_flp"], t["bk_frow"]
+    for L in range(t["BK_NLF"]):
+        for i in frow[flp[L]:flp[L + 1]][::-1]:
+            elim(rp[i], di[i])
+            rpiv[i] = 1.0 / A[di[i]]
+    for i in range(m, n):
+        elim(rp[i], t["bk_l21e"][i - m])
+    Sm = S.reshape(D, LD)[:, :D]
+    for c0 in range(0, D, 16):
+        pe = min(c0 + 16, D)
+        for c in range(c0, pe):
+            rpiv[m + c] = 1.0 / Sm[c, c]
+            Sm[c + 1:, c] *= rpiv[m + c]
+            Sm[c + 1:, c + 1:pe] -= np.outer(Sm[c + 1:, c], Sm[c, c + 1:pe])
+        if pe == D:
+            break
+        for r in range(1, pe - c0):
+            Sm[c0 + r, pe:] -= Sm[c0 + r, c0:c0 + r] @ Sm[c0:c0 + r, pe:]
+        Sm[pe:, pe:] -= Sm[pe:, c0:pe] @ Sm[c0:pe, pe:]
+    return rpiv
+
+
+def _block_solve(t, A, S, rpiv, b):
+    """the kernel's solve (bdf_big.cuh block_solve)"""
+    rp, ci, di, perm = t["sp_rp"], t["sp_ci"], t["sp_di"], t["sp_perm"]
+    m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
+    x = np.empty(n)
+    v = b[perm].copy()
+    flp, frow = t["bk_flp"], t["bk_frow"]
+    for L in range(1, t["BK_NLF"]):
+        for i in frow[flp[L]:flp[L + 1]]:
+            v[i] -= A[rp[i]:di[i]] @ v[ci[rp[i]:di[i]]]
+    for i in range(m, n):
+        e = t["bk_l21e"][i - m]
+        v[i] -= A[rp[i]:e] @ v[ci[rp[i]:e]]
+    Sm = S.reshape(D, LD)[:, :D]
+    w = v[m:]
+    for b0 in range(0, D, 32):
+        be = min(b0 + 32, D)
+        for j in range(b0, be):
+            w[j + 1:be] -= Sm[j + 1:be, j] * w[j]
+        w[be:] -= Sm[be:, b0:be] @ w[b0:be]
+    for be in range(D, 0, -32):
+        b0 = max(be - 32, 0)
+        for j in range(be - 1, b0 - 1, -1):
+            w[j] *= rpiv[m + j]
+            w[b0:j] -= Sm[b0:j, j] * w[j]
+        w[:b0] -= Sm[:b0, b0:be] @ w[b0:be]
+    blp, brow = t["bk_blp"], t["bk_brow"]
+    for L in range(t["BK_NLB"]):
+        for i in brow[blp[L]:blp[L + 1]]:
+            q0, q1 = di[i] + 1, rp[i + 1]
+            v[i] = (v[i] - A[q0:q1] @ v[ci[q0:q1]]) * rpiv[i]
+    x[perm] = v
+    return x
+
+
+def test_block_schedule_is_consistent(sched):
+    """each sparse row eliminates only with rows of lower levels, its
+    updates land in its own row, the Jacobian's places agree with the LU
+    pattern's"""
+    t = sched
+    rp, ci, di = t["sp_rp"], t["sp_ci"], t["sp_di"]
+    m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
+    assert m + D == n and LD >= D and D * LD * 8 <= 210 * 1024
+    lev = np.full(n, -1)
+    for L in range(t["BK_NLF"]):
+        lev[t["bk_frow"][t["bk_flp"][L]:t["bk_flp"][L + 1]]] = L
+    assert (lev[:m] >= 0).all() and sorted(t["bk_frow"]) == list(range(m))
+    for i in range(m):
+        ks = ci[rp[i]:di[i]]
+        assert (lev[ks] < lev[i]).all()
+    blev = np.full(n, -1)
+    for L in range(t["BK_NLB"]):
+        blev[t["bk_brow"][t["bk_blp"][L]:t["bk_blp"][L + 1]]] = L
+    for i in range(m):
+        js = ci[di[i] + 1:rp[i + 1]]
+        js = js[js < m]
+        assert (blev[js] < blev[i]).all()
+    row_of = np.repeat(np.arange(n), np.diff(rp))
+    for i in range(n):
+        for p in range(rp[i], di[i]):
+            k = ci[p]
+            if k >= m:
+                continue
+            q0, q1 = di[k] + 1, rp[k + 1]
+            tg = t["bk_tgt"][t["bk_uoff"][p]:t["bk_uoff"][p] + q1 - q0]
+            for q, g in zip(range(q0, q1), tg):
+                j = ci[q]
+                if g >= 0:
+                    assert row_of[g] == i and ci[g] == j
+                else:
+                    assert i >= m and j >= m and -1 - g == (i - m) * LD + (j - m)
+    for q, g in zip(t["sp_jpos"], t["bk_jt"]):
+        i, j = row_of[q], ci[q]
+        if i < m or j < m:
+            assert g == q
+        else:
+            assert -1 - g == (i - m) * LD + (j - m)
+
+
+def test_block_schedule_factors_and_solves_the_newton_matrix(sched):
+    """the kernel's factorization and solve, restated on the CPU from the
+    generated tables, solve I - gamma J (a diagonally dominant J on the
+    network's pattern) to 1e-12 of numpy's dense solve"""
+    t = sched
+    rp, ci, perm = t["sp_rp"], t["sp_ci"], t["sp_perm"]
+    m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
+    rng = np.random.default_rng(5)
+    row_of = np.repeat(np.arange(n), np.diff(rp))
+    jpos = t["sp_jpos"]
+    cnt = np.bincount(row_of[jpos], minlength=n)
+    J = rng.uniform(-1.0, 1.0, len(jpos)) / cnt[row_of[jpos]]
+    c = -0.9
+    M = np.eye(n)
+    A = np.zeros(t["NNZ_LU"])
+    S = np.zeros(D * LD)
+    for e, q in enumerate(jpos):
+        M[perm[row_of[q]], perm[ci[q]]] += J[e] * c
+        g = t["bk_jt"][e]
+        if g >= 0:
+            A[g] = J[e] * c
+        else:
+            S[-1 - g] = J[e] * c
+    for i in range(n):
+        if i < m:
+            A[t["sp_di"][i]] += 1.0
+        else:
+            S[(i - m) * (LD + 1)] += 1.0
+    rpiv = _block_lu(t, A, S)
+    assert np.isfinite(rpiv).all()
+    for _ in range(3):
+        b = rng.standard_normal(n)
+        x = _block_solve(t, A, S, rpiv, b)
+        ref = np.linalg.solve(M, b)
+        np.testing.assert_allclose(x, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+def test_rate_forms_of_the_large_path_equal_the_direct_rates():
+    """the generated rate parts (with the H-nuclei density passed in) are the
+    generated rates bit for bit; the three-point form of the density-
+    dependent rates the kernel evaluates at every rhs matches them to 1e-12
+    over states with every ice coverage (bare, partial, saturated)"""
+    info = netinfo.load(KEY)
+    lib = Oracle(KEY).lib
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.oracle_rates.argtypes = [ctypes.c_double, D, D, D]
+    lib.oracle_rates.restype = None
+    lib.oracle_rates_forms.argtypes = [ctypes.c_double, D, D, D, D]
+    lib.oracle_rates_forms.restype = ctypes.c_int
+    n, T, dt, par = workloads.semenov(12, info, seed=8)
+    ice = info["species"].index("H2O_DUST")
+    P = info["params"]
+    sites = (4 * np.pi * par[:, P.index("xdust")] * par[:, P.index("gsize2")]
+             / 9e-16)
+    n[:4, ice] = 0.0
+    n[4:8, ice] = sites[4:8] * np.linspace(0.1, 0.9, 4)
+    n[8:, ice] = sites[8:] * 3.0
+    nrea = lib.oracle_nrea()
+    worst = 0.0
+    for c in range(len(n)):
+        row = np.ascontiguousarray(n[c])
+        pr = np.ascontiguousarray(par[c])
+        kd, kp, ka = np.zeros(nrea), np.zeros(nrea), np.zeros(nrea)
+        lib.oracle_rates(T[c], row.ctypes.data_as(D), pr.ctypes.data_as(D),
+                         kd.ctypes.data_as(D))
+        aff = lib.oracle_rates_forms(T[c], row.ctypes.data_as(D),
+                                     pr.ctypes.data_as(D),
+                                     kp.ctypes.data_as(D), ka.ctypes.data_as(D))
+        assert aff == 1
+        np.testing.assert_array_equal(kp, kd)
+        big = np.abs(kd) > 1e-300
+        worst = max(worst, (np.abs(ka - kd)[big] / np.abs(kd[big])).max())
+    assert worst < 1e-12, worst
 
 
 def _opts(net, **extra):
-    o = workloads.OPTIONS[KEY]
-    return net.options(evolve_T=o["evolve_T"], jac=o["jac"], linsol=o["linsol"],
-                       rtol=o["rtol"], atol_n=o["atol_n"], atol_T=o["atol_T"],
-                       max_steps=o["max_steps"], **extra)
+    o = dict(workloads.OPTIONS[KEY])
+    o.update(extra)
+    return net.options(**o)
 
 
 def test_workload_is_neutral_and_sets_the_surface_parameters():
