@@ -35,9 +35,11 @@
 //              the minimum-degree order leaves a dense trailing block: the
 //              first BK_M rows sparse (factored level by level -- the rows of
 //              a level eliminate only with rows of lower levels -- a thread
-//              per row on wide levels, a warp per row on narrow ones), then
-//              the last BK_D rows' sparse columns (a thread per row, the
-//              Schur complement into S), then the dense block S (BK_D x BK_D,
+//              per row on wide levels, a warp per row through a shared-memory
+//              work row on narrow ones), then the last BK_D rows' sparse
+//              columns pivot by pivot (the Schur complement into S, every
+//              row and U entry of a pivot in parallel), then the dense block
+//              S (BK_D x BK_D,
 //              shared memory) by a right-looking LU in panels of 16 columns
 //              with register-tiled rank-16 updates
 //   solves     the same split: sparse rows by level, the dense block by
@@ -353,19 +355,86 @@ __device__ __forceinline__ void elim_thread(int p0, int p1, double* A,
     }
   }
 }
-// the same by a warp: the U entries over the lanes
-__device__ __forceinline__ void elim_warp(int p0, int p1, double* A,
-                                          const double* rpiv) {
+// sparse row i's elimination by a warp through a dense work row w (shared
+// memory, zero on entry and on exit): the row scattered into w by column,
+// each L entry's update applied to w over the lanes -- the U row of the next
+// L entry loaded into registers while the current one is applied, so the
+// chain of L entries runs at shared-memory latency -- then the row gathered
+// back; returns the pivot
+__device__ double elim_warp(int i, double* A, const double* rpiv, double* w) {
   const int lane = threadIdx.x & 31;
-  for (int p = p0; p < p1; ++p) {
+  const int p0 = d_sp_rp[i], pd = d_sp_di[i], p1 = d_sp_rp[i + 1];
+  for (int p = p0 + lane; p < p1; p += 32) w[d_sp_ci[p]] = A[p];
+  __syncwarp();
+  double u[4];
+  int c[4];
+  auto fetch = [&](int p) {
+    const int k = d_sp_ci[p], q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int q = q0 + lane + 32 * s;
+      c[s] = q < q1 ? d_sp_ci[q] : -1;
+      u[s] = q < q1 ? A[q] : 0.0;
+    }
+  };
+  if (p0 < pd) fetch(p0);
+  for (int p = p0; p < pd; ++p) {
     const int k = d_sp_ci[p];
-    const double l = A[p] * rpiv[k];
+    const double l = w[k] * rpiv[k];
+    double uc[4];
+    int cc[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      uc[s] = u[s];
+      cc[s] = c[s];
+    }
+    if (p + 1 < pd) fetch(p + 1);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+      if (cc[s] >= 0) w[cc[s]] -= l * uc[s];
     const int q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
-    const int* tg = d_bk_tgt + d_bk_uoff[p] - q0;
-    for (int q = q0 + lane; q < q1; q += 32) A[tg[q]] -= l * A[q];
+    for (int q = q0 + 128 + lane; q < q1; q += 32) w[d_sp_ci[q]] -= l * A[q];
     __syncwarp();
-    if (lane == 0) A[p] = l;
+    if (lane == 0) w[k] = l;
     __syncwarp();
+  }
+  const double piv = w[i];
+  __syncwarp();
+  for (int p = p0 + lane; p < p1; p += 32) {
+    const int j = d_sp_ci[p];
+    A[p] = w[j];
+    w[j] = 0.0;
+  }
+  __syncwarp();
+  return piv;
+}
+
+// the dense rows' sparse columns (the Schur complement into S), right-
+// looking: at step s, with pivot row k = bk_sk[s] final, the dense rows' L
+// entries (i, k) are final too; each gets l = a(i, k) / a(k, k) (into lb, a
+// scratch of BK_D doubles), then every pair (i, U entry (k, j)) applies
+// a(i, j) -= l a(k, j) -- distinct targets within a step, so all pairs run
+// in parallel. Per element the operations and their order are those of the
+// row-wise (IKJ) elimination. Two barriers per step.
+__device__ void schur(double* A, double* S, const double* rpiv, double* lb) {
+  const int tid = threadIdx.x;
+  for (int s = 0; s < BK_NSCHUR; ++s) {
+    const int k = d_bk_sk[s];
+    const int c0 = d_bk_sp[s], nc = d_bk_sp[s + 1] - c0;
+    const double rk = rpiv[k];
+    for (int c = tid; c < nc; c += NT) lb[c] = A[d_bk_sl[c0 + c]] * rk;
+    __syncthreads();
+    const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
+    for (int x = tid; x < nc * nq; x += NT) {
+      const int c = x / nq, qq = x - c * nq;
+      const int p = d_bk_sl[c0 + c];
+      const int t = d_bk_tgt[d_bk_uoff[p] + qq];
+      const double v = lb[c] * A[q0 + qq];
+      if (t >= 0) A[t] -= v;
+      else S[-1 - t] -= v;
+    }
+    for (int c = tid; c < nc; c += NT) A[d_bk_sl[c0 + c]] = lb[c];
+    __syncthreads();
   }
 }
 
@@ -455,10 +524,18 @@ __device__ int block_lu(double* A) {
   double* rpiv = smem() + SM::RPIV;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   bool bad = false;
+  // the narrow levels' two work rows: the solve vector and the rhs input,
+  // both free during the factorization
+  double* wrow = smem() + (warp == 0 ? SM::T : SM::YR);
+  __syncthreads();
+  for (int i = tid; i < (int)NV; i += NT) {
+    smem()[SM::T + i] = 0.0;
+    smem()[SM::YR + i] = 0.0;
+  }
   __syncthreads();
   for (int L = 0; L < BK_NLF; ++L) {
     const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
-    if (r1 - r0 >= 16) {
+    if (r1 - r0 >= 16) {  // wide: a thread per row
       for (int r = r0 + tid; r < r1; r += NT) {
         const int i = d_bk_frow[r];
         elim_thread(d_sp_rp[i], d_sp_di[i], A, S, rpiv);
@@ -466,22 +543,20 @@ __device__ int block_lu(double* A) {
         rpiv[i] = 1.0 / piv;
         bad = bad || piv == 0.0 || !isfinite(piv);
       }
-    } else {
-      for (int r = r0 + warp; r < r1; r += NWARP) {
+    } else if (warp < 2) {  // narrow: warps 0 and 1, a row at a time each
+      for (int r = r0 + warp; r < r1; r += 2) {
         const int i = d_bk_frow[r];
-        elim_warp(d_sp_rp[i], d_sp_di[i], A, rpiv);
+        const double piv = elim_warp(i, A, rpiv, wrow);
         if (lane == 0) {
-          const double piv = A[d_sp_di[i]];
           rpiv[i] = 1.0 / piv;
           bad = bad || piv == 0.0 || !isfinite(piv);
         }
+        __syncwarp();
       }
     }
     __syncthreads();
   }
-  for (int i = BK_M + tid; i < N; i += NT)
-    elim_thread(d_sp_rp[i], d_bk_l21e[i - BK_M], A, S, rpiv);
-  __syncthreads();
+  schur(A, S, rpiv, smem() + SM::T);
   bad = dense_lu(S, rpiv + BK_M) || bad;
   return __syncthreads_or(bad) ? 1 : 0;
 }
@@ -540,8 +615,58 @@ __device__ void dense_bwd(const double* S, const double* rpd, double* x) {
     }
   }
 }
+// t[i] = (t[i] - sum_p a[p] t[ci[p]]) * sc over the entries [p0, p1) of
+// each row i = rows[r], r in [r0, r1), one row after another by one warp
+// (lanes over the entries, a warp sum), the next row's entries loaded while
+// the current one is summed; sc = 1 (forward, unit diagonal) or 1 / the
+// pivot (backward). FWD picks the entry range of a row.
+template <bool FWD>
+__device__ void rows_by_warp(const int* rows, int r0, int r1, const double* A,
+                             const double* rpiv, double* t) {
+  const int lane = threadIdx.x & 31;
+  auto range = [&](int i, int& p0, int& p1) {
+    if (FWD) { p0 = d_sp_rp[i]; p1 = d_sp_di[i]; }
+    else { p0 = d_sp_di[i] + 1; p1 = d_sp_rp[i + 1]; }
+  };
+  double a[4];
+  int c[4];
+  auto fetch = [&](int r) {
+    int p0, p1;
+    range(rows[r], p0, p1);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int p = p0 + lane + 32 * s;
+      c[s] = p < p1 ? d_sp_ci[p] : -1;
+      a[s] = p < p1 ? A[p] : 0.0;
+    }
+  };
+  if (r0 < r1) fetch(r0);
+  for (int r = r0; r < r1; ++r) {
+    const int i = rows[r];
+    double ac[4];
+    int cc[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      ac[s] = a[s];
+      cc[s] = c[s];
+    }
+    if (r + 1 < r1) fetch(r + 1);
+    double sum = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+      if (cc[s] >= 0) sum += ac[s] * t[cc[s]];
+    int p0, p1;
+    range(i, p0, p1);
+    for (int p = p0 + 128 + lane; p < p1; p += 32) sum += A[p] * t[d_sp_ci[p]];
+    sum = warp_sum(sum);
+    if (lane == 0) t[i] = FWD ? t[i] - sum : (t[i] - sum) * rpiv[i];
+    __syncwarp();
+  }
+}
+
 // x = A^-1 b with the factors (b and x in the species order; x may be b).
-// Starts and ends with a block barrier.
+// Starts and ends with a block barrier. Narrow levels (< 16 rows) go to
+// warp 0 alone with warp syncs; block barriers only around the wide ones.
 __device__ void block_solve(const double* A, const double* b, double* x) {
   const double* S = smem() + SM::S;
   const double* rpiv = smem() + SM::RPIV;
@@ -550,27 +675,25 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   __syncthreads();
   KBG_FOR(i) t[i] = b[d_sp_perm[i]];
   __syncthreads();
+  bool narrow = false;  // the previous level ran on warp 0 alone
   for (int L = 1; L < BK_NLF; ++L) {  // level 0 rows have no L entries
     const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
     if (r1 - r0 >= 16) {
+      if (narrow) __syncthreads();
       for (int r = r0 + tid; r < r1; r += NT) {
         const int i = d_bk_frow[r];
         double s = 0.0;
         for (int p = d_sp_rp[i]; p < d_sp_di[i]; ++p) s += A[p] * t[d_sp_ci[p]];
         t[i] -= s;
       }
+      __syncthreads();
+      narrow = false;
     } else {
-      for (int r = r0 + warp; r < r1; r += NWARP) {
-        const int i = d_bk_frow[r];
-        double s = 0.0;
-        for (int p = d_sp_rp[i] + lane; p < d_sp_di[i]; p += 32)
-          s += A[p] * t[d_sp_ci[p]];
-        s = warp_sum(s);
-        if (lane == 0) t[i] -= s;
-      }
+      if (warp == 0) rows_by_warp<true>(d_bk_frow, r0, r1, A, rpiv, t);
+      narrow = true;
     }
-    __syncthreads();
   }
+  if (narrow) __syncthreads();
   for (int i = BK_M + tid; i < N; i += NT) {
     double s = 0.0;
     for (int p = d_sp_rp[i]; p < d_bk_l21e[i - BK_M]; ++p) s += A[p] * t[d_sp_ci[p]];
@@ -579,27 +702,25 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   __syncthreads();
   dense_fwd(S, t + BK_M);
   dense_bwd(S, rpiv + BK_M, t + BK_M);
+  narrow = false;
   for (int L = 0; L < BK_NLB; ++L) {
     const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
     if (r1 - r0 >= 16) {
+      if (narrow) __syncthreads();
       for (int r = r0 + tid; r < r1; r += NT) {
         const int i = d_bk_brow[r];
         double s = 0.0;
         for (int q = d_sp_di[i] + 1; q < d_sp_rp[i + 1]; ++q) s += A[q] * t[d_sp_ci[q]];
         t[i] = (t[i] - s) * rpiv[i];
       }
+      __syncthreads();
+      narrow = false;
     } else {
-      for (int r = r0 + warp; r < r1; r += NWARP) {
-        const int i = d_bk_brow[r];
-        double s = 0.0;
-        for (int q = d_sp_di[i] + 1 + lane; q < d_sp_rp[i + 1]; q += 32)
-          s += A[q] * t[d_sp_ci[q]];
-        s = warp_sum(s);
-        if (lane == 0) t[i] = (t[i] - s) * rpiv[i];
-      }
+      if (warp == 0) rows_by_warp<false>(d_bk_brow, r0, r1, A, rpiv, t);
+      narrow = true;
     }
-    __syncthreads();
   }
+  if (narrow) __syncthreads();
   KBG_FOR(i) x[d_sp_perm[i]] = t[i];
   __syncthreads();
 }

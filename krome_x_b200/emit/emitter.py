@@ -1350,6 +1350,10 @@ class Emitter:
                              the LU values (>= 0) or -1 - its index in S
           bk_jt[e]           the place of Jacobian entry e, the same way
           bk_l21e[i - BK_M]  the end of dense row i's sparse-column L entries
+          bk_sk / bk_sp / bk_sl  the Schur complement pivot by pivot: step
+                             s eliminates with sparse row bk_sk[s] the dense
+                             rows' L entries bk_sl[bk_sp[s] .. bk_sp[s+1])
+                             (their places, in row order)
           d_bk_hnuc          H nuclei per species (the terms of Hnuclei_)"""
         w = self.w
         D = min(self.BK_DMAX, n)
@@ -1395,6 +1399,15 @@ class Emitter:
                 while e < rp[i + 1] and ci[e] < m:
                     e += 1
                 l21e.append(e)
+        cols = {}
+        for i in range(m, n):
+            for p in range(rp[i], l21e[i - m]):
+                cols.setdefault(ci[p], []).append(p)
+        sk = sorted(cols)
+        sp_, sl = [0], []
+        for k in sk:
+            sl += cols[k]
+            sp_.append(len(sl))
         inv = {v: key for key, v in pos.items()}
         jt = [code(*inv[q]) for q in jpos]
         self.meta["bk_m"] = m
@@ -1407,6 +1420,7 @@ class Emitter:
         w("constexpr int BK_NLF = %d;" % nlf)
         w("constexpr int BK_NLB = %d;" % nlb)
         w("constexpr int BK_NTGT = %d;" % len(tgt))
+        w("constexpr int BK_NSCHUR = %d;  // Schur steps (pivots)" % len(sk))
         self._table("bk_frow", frow or [0])
         self._table("bk_flp", flp)
         self._table("bk_brow", brow or [0])
@@ -1415,6 +1429,9 @@ class Emitter:
         self._table("bk_tgt", tgt or [0])
         self._table("bk_jt", jt)
         self._table("bk_l21e", l21e or [0])
+        self._table("bk_sk", sk or [0])
+        self._table("bk_sp", sp_)
+        self._table("bk_sl", sl or [0])
         w("#ifdef __CUDACC__")
         w("__device__ const double d_bk_hnuc[NSPEC] = {%s};"
           % ",".join(repr(float(v)) for v in self.natoms_H))

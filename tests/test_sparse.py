@@ -20,7 +20,7 @@ from oracle import Oracle
 KEY = "semenov"
 TABLES = ("sp_rp", "sp_ci", "sp_di", "sp_perm", "sp_jpos", "bk_frow",
           "bk_flp", "bk_brow", "bk_blp", "bk_uoff", "bk_tgt", "bk_jt",
-          "bk_l21e")
+          "bk_l21e", "bk_sk", "bk_sp", "bk_sl")
 
 
 @pytest.fixture(scope="module")
@@ -41,8 +41,9 @@ def sched():
 def _block_lu(t, A, S):
     """the kernel's factorization (bdf_big.cuh block_lu), phase by phase:
     the sparse rows level by level (each level's rows in reverse order: the
-    rows of a level are independent), the dense rows' sparse columns, the
-    dense block in panels of 16. Returns 1 / the pivots."""
+    rows of a level are independent), the dense rows' sparse columns pivot
+    by pivot (bk_sk / bk_sp / bk_sl), the dense block in panels of 16.
+    Returns 1 / the pivots."""
     rp, ci, di = t["sp_rp"], t["sp_ci"], t["sp_di"]
     m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
     rpiv = np.zeros(n)
@@ -63,8 +64,19 @@ def _block_lu(t, A, S):
         for i in frow[flp[L]:flp[L + 1]][::-1]:
             elim(rp[i], di[i])
             rpiv[i] = 1.0 / A[di[i]]
-    for i in range(m, n):
-        elim(rp[i], t["bk_l21e"][i - m])
+    sk, sp, sl = t["bk_sk"], t["bk_sp"], t["bk_sl"]
+    for s in range(t["BK_NSCHUR"]):  # the dense rows' columns, pivot by pivot
+        k = sk[s]
+        ps = sl[sp[s]:sp[s + 1]]
+        lb = A[ps] * rpiv[k]
+        q0, q1 = di[k] + 1, rp[k + 1]
+        for p, l in zip(ps, lb):
+            tg = t["bk_tgt"][t["bk_uoff"][p]:t["bk_uoff"][p] + q1 - q0]
+            a = tg >= 0
+            u = A[q0:q1]
+            A[tg[a]] -= l * u[a]
+            S[-1 - tg[~a]] -= l * u[~a]
+        A[ps] = lb
     Sm = S.reshape(D, LD)[:, :D]
     for c0 in range(0, D, 16):
         pe = min(c0 + 16, D)
@@ -151,6 +163,15 @@ def test_block_schedule_is_consistent(sched):
                     assert row_of[g] == i and ci[g] == j
                 else:
                     assert i >= m and j >= m and -1 - g == (i - m) * LD + (j - m)
+    # the Schur steps: every dense row's sparse-column L entry once, each
+    # pivot's entries after those of lower pivots, rows in order
+    sl, sk, sp = t["bk_sl"], t["bk_sk"], t["bk_sp"]
+    assert (np.diff(sk) > 0).all() and len(sl) == len(set(sl.tolist()))
+    want = [p for i in range(m, n) for p in range(rp[i], t["bk_l21e"][i - m])]
+    assert sorted(want) == sorted(sl.tolist())
+    for s in range(t["BK_NSCHUR"]):
+        ps = sl[sp[s]:sp[s + 1]]
+        assert (ci[ps] == sk[s]).all() and (np.diff(row_of[ps]) > 0).all()
     for q, g in zip(t["sp_jpos"], t["bk_jt"]):
         i, j = row_of[q], ci[q]
         if i < m or j < m:
