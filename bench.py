@@ -376,9 +376,10 @@ def precision_form(torch, dev):
 
 # the large-network form: DRAM bytes (read + write) of its solve kernel per
 # integration step, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of 148 Semenov cells over 3.15e9 s (154,453 steps:
-# 8.49 GB); the per-cell workspace (~600 KB) stays in L2
-SEMENOV_DRAM_PER_STEP = 8.49e9 / 154453
+# dram__bytes_write.sum) of `python -m krome_x_b200.run semenov 148 --dt
+# 3.15e9` (154,747 steps: 2.29 + 6.27 GB); the per-cell workspace (~600 KB)
+# stays in L2
+SEMENOV_DRAM_PER_STEP = 8.57e9 / 154747
 SEMENOV_CELLS = 2048
 
 

@@ -425,10 +425,10 @@ __device__ void schur(double* A, double* S, const double* rpiv, double* lb) {
     for (int c = tid; c < nc; c += NT) lb[c] = A[d_bk_sl[c0 + c]] * rk;
     __syncthreads();
     const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
+    const int* st = d_bk_st + d_bk_so[s];
     for (int x = tid; x < nc * nq; x += NT) {
       const int c = x / nq, qq = x - c * nq;
-      const int p = d_bk_sl[c0 + c];
-      const int t = d_bk_tgt[d_bk_uoff[p] + qq];
+      const int t = st[x];
       const double v = lb[c] * A[q0 + qq];
       if (t >= 0) A[t] -= v;
       else S[-1 - t] -= v;
@@ -615,24 +615,29 @@ __device__ void dense_bwd(const double* S, const double* rpd, double* x) {
     }
   }
 }
+// the rows of a solve phase summed by a warp
+enum { RW_FWD, RW_BWD, RW_L21 };
 // t[i] = (t[i] - sum_p a[p] t[ci[p]]) * sc over the entries [p0, p1) of
-// each row i = rows[r], r in [r0, r1), one row after another by one warp
-// (lanes over the entries, a warp sum), the next row's entries loaded while
-// the current one is summed; sc = 1 (forward, unit diagonal) or 1 / the
-// pivot (backward). FWD picks the entry range of a row.
-template <bool FWD>
-__device__ void rows_by_warp(const int* rows, int r0, int r1, const double* A,
-                             const double* rpiv, double* t) {
+// each row i = rows[r] (rows == nullptr: i = r), r = r0, r0 + rs, ... < r1,
+// one row after another by one warp (lanes over the entries, a warp sum),
+// the next row's entries loaded while the current one is summed. MODE:
+// RW_FWD the L entries (sc = 1, unit diagonal), RW_BWD the U entries (sc =
+// 1 / the pivot), RW_L21 a dense row's sparse-column L entries (sc = 1).
+template <int MODE>
+__device__ void rows_by_warp(const int* rows, int r0, int r1, int rs,
+                             const double* A, const double* rpiv, double* t) {
   const int lane = threadIdx.x & 31;
   auto range = [&](int i, int& p0, int& p1) {
-    if (FWD) { p0 = d_sp_rp[i]; p1 = d_sp_di[i]; }
-    else { p0 = d_sp_di[i] + 1; p1 = d_sp_rp[i + 1]; }
+    if (MODE == RW_FWD) { p0 = d_sp_rp[i]; p1 = d_sp_di[i]; }
+    else if (MODE == RW_BWD) { p0 = d_sp_di[i] + 1; p1 = d_sp_rp[i + 1]; }
+    else { p0 = d_sp_rp[i]; p1 = d_bk_l21e[i - BK_M]; }
   };
+  auto row = [&](int r) { return rows != nullptr ? rows[r] : r; };
   double a[4];
   int c[4];
   auto fetch = [&](int r) {
     int p0, p1;
-    range(rows[r], p0, p1);
+    range(row(r), p0, p1);
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const int p = p0 + lane + 32 * s;
@@ -641,8 +646,8 @@ __device__ void rows_by_warp(const int* rows, int r0, int r1, const double* A,
     }
   };
   if (r0 < r1) fetch(r0);
-  for (int r = r0; r < r1; ++r) {
-    const int i = rows[r];
+  for (int r = r0; r < r1; r += rs) {
+    const int i = row(r);
     double ac[4];
     int cc[4];
 #pragma unroll
@@ -650,7 +655,7 @@ __device__ void rows_by_warp(const int* rows, int r0, int r1, const double* A,
       ac[s] = a[s];
       cc[s] = c[s];
     }
-    if (r + 1 < r1) fetch(r + 1);
+    if (r + rs < r1) fetch(r + rs);
     double sum = 0.0;
 #pragma unroll
     for (int s = 0; s < 4; ++s)
@@ -659,14 +664,13 @@ __device__ void rows_by_warp(const int* rows, int r0, int r1, const double* A,
     range(i, p0, p1);
     for (int p = p0 + 128 + lane; p < p1; p += 32) sum += A[p] * t[d_sp_ci[p]];
     sum = warp_sum(sum);
-    if (lane == 0) t[i] = FWD ? t[i] - sum : (t[i] - sum) * rpiv[i];
+    if (lane == 0) t[i] = MODE == RW_BWD ? (t[i] - sum) * rpiv[i] : t[i] - sum;
     __syncwarp();
   }
 }
 
 // x = A^-1 b with the factors (b and x in the species order; x may be b).
-// Starts and ends with a block barrier. Narrow levels (< 16 rows) go to
-// warp 0 alone with warp syncs; block barriers only around the wide ones.
+// Starts and ends with a block barrier; one barrier per level.
 __device__ void block_solve(const double* A, const double* b, double* x) {
   const double* S = smem() + SM::S;
   const double* rpiv = smem() + SM::RPIV;
@@ -675,52 +679,31 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   __syncthreads();
   KBG_FOR(i) t[i] = b[d_sp_perm[i]];
   __syncthreads();
-  bool narrow = false;  // the previous level ran on warp 0 alone
   for (int L = 1; L < BK_NLF; ++L) {  // level 0 rows have no L entries
     const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
-    if (r1 - r0 >= 16) {
-      if (narrow) __syncthreads();
+    if (r1 - r0 >= 16) {  // wide levels' rows have a few L entries each
       for (int r = r0 + tid; r < r1; r += NT) {
         const int i = d_bk_frow[r];
         double s = 0.0;
         for (int p = d_sp_rp[i]; p < d_sp_di[i]; ++p) s += A[p] * t[d_sp_ci[p]];
         t[i] -= s;
       }
-      __syncthreads();
-      narrow = false;
     } else {
-      if (warp == 0) rows_by_warp<true>(d_bk_frow, r0, r1, A, rpiv, t);
-      narrow = true;
+      rows_by_warp<RW_FWD>(d_bk_frow, r0 + warp, r1, NWARP, A, rpiv, t);
     }
+    __syncthreads();
   }
-  if (narrow) __syncthreads();
-  for (int i = BK_M + tid; i < N; i += NT) {
-    double s = 0.0;
-    for (int p = d_sp_rp[i]; p < d_bk_l21e[i - BK_M]; ++p) s += A[p] * t[d_sp_ci[p]];
-    t[i] -= s;
-  }
+  // the dense rows' sparse columns: a warp per row (a hub row has hundreds)
+  rows_by_warp<RW_L21>(nullptr, BK_M + warp, N, NWARP, A, rpiv, t);
   __syncthreads();
   dense_fwd(S, t + BK_M);
   dense_bwd(S, rpiv + BK_M, t + BK_M);
-  narrow = false;
-  for (int L = 0; L < BK_NLB; ++L) {
+  for (int L = 0; L < BK_NLB; ++L) {  // a warp per row (U rows reach into
+                                      // the dense columns)
     const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
-    if (r1 - r0 >= 16) {
-      if (narrow) __syncthreads();
-      for (int r = r0 + tid; r < r1; r += NT) {
-        const int i = d_bk_brow[r];
-        double s = 0.0;
-        for (int q = d_sp_di[i] + 1; q < d_sp_rp[i + 1]; ++q) s += A[q] * t[d_sp_ci[q]];
-        t[i] = (t[i] - s) * rpiv[i];
-      }
-      __syncthreads();
-      narrow = false;
-    } else {
-      if (warp == 0) rows_by_warp<false>(d_bk_brow, r0, r1, A, rpiv, t);
-      narrow = true;
-    }
+    rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t);
+    __syncthreads();
   }
-  if (narrow) __syncthreads();
   KBG_FOR(i) x[d_sp_perm[i]] = t[i];
   __syncthreads();
 }

@@ -1353,7 +1353,10 @@ class Emitter:
           bk_sk / bk_sp / bk_sl  the Schur complement pivot by pivot: step
                              s eliminates with sparse row bk_sk[s] the dense
                              rows' L entries bk_sl[bk_sp[s] .. bk_sp[s+1])
-                             (their places, in row order)
+                             (their places, in row order); bk_st
+                             [bk_so[s] .. bk_so[s+1]) the step's update
+                             targets, entry by entry then U entry by U
+                             entry (bk_tgt in step order)
           d_bk_hnuc          H nuclei per species (the terms of Hnuclei_)"""
         w = self.w
         D = min(self.BK_DMAX, n)
@@ -1404,10 +1407,14 @@ class Emitter:
             for p in range(rp[i], l21e[i - m]):
                 cols.setdefault(ci[p], []).append(p)
         sk = sorted(cols)
-        sp_, sl = [0], []
+        sp_, sl, so, st = [0], [], [0], []
         for k in sk:
             sl += cols[k]
             sp_.append(len(sl))
+            nq = rp[k + 1] - di[k] - 1
+            for p in cols[k]:
+                st += tgt[uoff[p]:uoff[p] + nq]
+            so.append(len(st))
         inv = {v: key for key, v in pos.items()}
         jt = [code(*inv[q]) for q in jpos]
         self.meta["bk_m"] = m
@@ -1432,6 +1439,8 @@ class Emitter:
         self._table("bk_sk", sk or [0])
         self._table("bk_sp", sp_)
         self._table("bk_sl", sl or [0])
+        self._table("bk_so", so)
+        self._table("bk_st", st or [0])
         w("#ifdef __CUDACC__")
         w("__device__ const double d_bk_hnuc[NSPEC] = {%s};"
           % ",".join(repr(float(v)) for v in self.natoms_H))

@@ -3,6 +3,7 @@
     python -m krome_x_b200.run primordial3 65536 [--layout lane|warp]
         [--kernel persistent|plain] [--seed 5] [--calls 1] [--lu32]
     python -m krome_x_b200.run primordial 8192 --adjoint
+    python -m krome_x_b200.run semenov 148 --dt 3.15e9
 
 Draws the seeded workload (krome_x_b200.workloads), solves it through the
 C ABI (krome_b200_solve_batch) and prints the elapsed time, the cell-solves
@@ -10,7 +11,8 @@ per second and the failed cells; with --calls > 1 it runs that many steps
 of the collapse driver's hydro loop on the host arrays. With --adjoint it
 runs the discrete adjoint through the torch.autograd wrapper instead (the
 recording forward solve and the reverse sweep, gradients of sum(n_H2) +
-sum(Tgas)). Used to profile a single kernel launch (ncu -k ... python -m
+sum(Tgas)). --dt replaces every cell's time step (a shorter solve of the
+same cells, e.g. to profile the large networks' kernel). Used to profile a single kernel launch (ncu -k ... python -m
 krome_x_b200.run ...).
 """
 import argparse
@@ -31,15 +33,19 @@ def main(argv=None):
     ap.add_argument("--lane-minb", type=int, default=2)
     ap.add_argument("--lu32", action="store_true")
     ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--dt", type=float, default=None)
     a = ap.parse_args(argv)
     info = netinfo.load(a.network)
     n, T, dt, par = workloads.GENERATORS[a.network](a.cells, info, seed=a.seed)
+    if a.dt is not None:
+        dt[:] = a.dt
     o = workloads.OPTIONS[a.network]
     net = krome.load(a.network)
     opts = net.options(evolve_T=o["evolve_T"], jac=o["jac"], rtol=o["rtol"],
                        atol_n=o["atol_n"], atol_T=o["atol_T"],
                        kernel=a.kernel, layout=0 if a.layout == "warp" else 1,
-                       lane_minb=a.lane_minb, lu32=int(a.lu32))
+                       lane_minb=a.lane_minb, lu32=int(a.lu32),
+                       max_steps=o.get("max_steps", 100000))
     if a.adjoint:
         return adjoint(a, net, opts, info, n, T, dt, par)
     failed = 0

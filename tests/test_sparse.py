@@ -20,7 +20,7 @@ from oracle import Oracle
 KEY = "semenov"
 TABLES = ("sp_rp", "sp_ci", "sp_di", "sp_perm", "sp_jpos", "bk_frow",
           "bk_flp", "bk_brow", "bk_blp", "bk_uoff", "bk_tgt", "bk_jt",
-          "bk_l21e", "bk_sk", "bk_sp", "bk_sl")
+          "bk_l21e", "bk_sk", "bk_sp", "bk_sl", "bk_so", "bk_st")
 
 
 @pytest.fixture(scope="module")
@@ -70,8 +70,8 @@ def _block_lu(t, A, S):
         ps = sl[sp[s]:sp[s + 1]]
         lb = A[ps] * rpiv[k]
         q0, q1 = di[k] + 1, rp[k + 1]
-        for p, l in zip(ps, lb):
-            tg = t["bk_tgt"][t["bk_uoff"][p]:t["bk_uoff"][p] + q1 - q0]
+        steps = t["bk_st"][t["bk_so"][s]:t["bk_so"][s + 1]].reshape(len(ps), q1 - q0)
+        for p, l, tg in zip(ps, lb, steps):
             a = tg >= 0
             u = A[q0:q1]
             A[tg[a]] -= l * u[a]
