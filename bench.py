@@ -94,6 +94,29 @@ def dist_env():
     return rank, world, local
 
 
+def rank_seed(rank):
+    """each rank draws its own cells (weak scaling: one shard per rank, no
+    exchange between ranks)"""
+    return 1000 + rank
+
+
+def job_times(values, dev, world):
+    """the job's times: per entry the max over ranks of the local times
+    (an all_reduce MAX; nothing on one rank)"""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def job_rate(units_per_rank, world, seconds):
+    """whole-job throughput: the units all ranks processed over the job's
+    time"""
+    return units_per_rank * world / seconds
+
+
 def inputs(ncell, seed):
     from krome_x_b200 import netinfo, workloads
     info = netinfo.load(NETWORK)
@@ -451,7 +474,7 @@ def run_ours(args, rank, world, local):
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     net = krome.load(NETWORK)
-    info, n, T, dt, par = inputs(args.cells, seed=1000 + rank)
+    info, n, T, dt, par = inputs(args.cells, seed=rank_seed(rank))
     ncell = args.cells
     opts = options(net)
     flops = json.loads((ROOT / "krome_x_b200" / "networks"
@@ -503,20 +526,17 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) / 1e3
     kernel_s = sum(a.elapsed_time(b) for a, b in zip(kst, ken)) / 1e3
-    tt = torch.tensor([elapsed, kernel_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    elapsed, kernel_s = float(tt[0]), float(tt[1])
+    elapsed, kernel_s = job_times([elapsed, kernel_s], dev, world)
     stats_sum = stats_acc.cpu().numpy().astype(float)
     n_failed = int(fails.item())
-    value = args.steps * ncell * world / elapsed
+    value = job_rate(args.steps * ncell, world, elapsed)
     W, special = algorithmic_flops(stats_sum, flops, N, args.steps * ncell)
     achieved = W / kernel_s / 1e12
     graph.free()
 
     # ---- end to end through the public API (pinned host arrays) ----
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
-    info2, n2, T2, dt2, par2 = inputs(ncell, seed=1000 + rank)
+    info2, n2, T2, dt2, par2 = inputs(ncell, seed=rank_seed(rank))
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     n2, T2, dt2, par2 = pin(n2), pin(T2), pin(dt2), pin(par2)
     fl2 = pin(np.zeros(ncell, dtype=np.intc))
@@ -542,10 +562,8 @@ def run_ours(args, rank, world, local):
     for _ in range(e2e_steps):
         e2e_failed += public_step()
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = e2e_steps * ncell * world / float(te[0])
+    e2e_s, = job_times([e2e_s], dev, world)
+    e2e_value = job_rate(e2e_steps * ncell, world, e2e_s)
     h2d = n.nbytes + T.nbytes + dt.nbytes + par.nbytes
     d2h = n.nbytes + T.nbytes + 4 * ncell
 
