@@ -68,6 +68,7 @@ constexpr int NT = 256;  // threads of a cell's block
 constexpr int NWARP = NT / 32;
 constexpr unsigned FULLM = 0xffffffffu;
 static_assert(RPART <= NT, "one rate part per thread");
+static_assert(BK_D <= NT, "a thread per dense row in the Schur steps");
 // a vector's stride: N + the n[N] = 1 slot of the flux products, a
 // multiple of 4 doubles
 constexpr long NV = ((NSPEC + 1 + 3) / 4) * 4;
@@ -415,25 +416,48 @@ __device__ double elim_warp(int i, double* A, const double* rpiv, double* w) {
 // scratch of BK_D doubles), then every pair (i, U entry (k, j)) applies
 // a(i, j) -= l a(k, j) -- distinct targets within a step, so all pairs run
 // in parallel. Per element the operations and their order are those of the
-// row-wise (IKJ) elimination. Two barriers per step.
+// row-wise (IKJ) elimination. Two barriers per step; what a step reads that
+// no step writes (its L entries' places, its first pairs' targets and U
+// values) is loaded during the step before.
 __device__ void schur(double* A, double* S, const double* rpiv, double* lb) {
   const int tid = threadIdx.x;
-  for (int s = 0; s < BK_NSCHUR; ++s) {
-    const int k = d_bk_sk[s];
-    const int c0 = d_bk_sp[s], nc = d_bk_sp[s + 1] - c0;
-    const double rk = rpiv[k];
-    for (int c = tid; c < nc; c += NT) lb[c] = A[d_bk_sl[c0 + c]] * rk;
-    __syncthreads();
+  int pp = -1;  // this thread's L entry of the next step (a place in A)
+  int pt[2];    // the next step's pairs tid and tid + NT: targets, U values
+  double pu[2];
+  auto prefetch = [&](int s) {
+    const int k = d_bk_sk[s], c0 = d_bk_sp[s], nc = d_bk_sp[s + 1] - c0;
     const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
     const int* st = d_bk_st + d_bk_so[s];
-    for (int x = tid; x < nc * nq; x += NT) {
-      const int c = x / nq, qq = x - c * nq;
-      const int t = st[x];
-      const double v = lb[c] * A[q0 + qq];
+    pp = tid < nc ? d_bk_sl[c0 + tid] : -1;
+#pragma unroll
+    for (int y = 0; y < 2; ++y) {
+      const int x = tid + y * NT;
+      const bool in = x < nc * nq;
+      pt[y] = in ? st[x] : 0;
+      pu[y] = in ? A[q0 + x % nq] : 0.0;
+    }
+  };
+  if (BK_NSCHUR > 0) prefetch(0);
+  for (int s = 0; s < BK_NSCHUR; ++s) {
+    const int k = d_bk_sk[s];
+    const int nc = d_bk_sp[s + 1] - d_bk_sp[s];
+    const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
+    const int* st = d_bk_st + d_bk_so[s];
+    const int myp = pp;
+    if (myp >= 0) lb[tid] = A[myp] * rpiv[k];
+    const int t0 = pt[0], t1 = pt[1];
+    const double u0 = pu[0], u1 = pu[1];
+    __syncthreads();
+    if (s + 1 < BK_NSCHUR) prefetch(s + 1);
+    for (int x = tid, y = 0; x < nc * nq; x += NT, ++y) {
+      const int c = x / nq;
+      const int t = y == 0 ? t0 : (y == 1 ? t1 : st[x]);
+      const double u = y == 0 ? u0 : (y == 1 ? u1 : A[q0 + (x - c * nq)]);
+      const double v = lb[c] * u;
       if (t >= 0) A[t] -= v;
       else S[-1 - t] -= v;
     }
-    for (int c = tid; c < nc; c += NT) A[d_bk_sl[c0 + c]] = lb[c];
+    if (myp >= 0) A[myp] = lb[tid];
     __syncthreads();
   }
 }
