@@ -75,6 +75,51 @@ int krome_solve_cells(int ncell, double* n, double* Tgas, const double* dt,
                       const double* par, int par_stride, const void* extra,
                       int* flags, const krome_opts* h);
 
+/* krome_solve_cells with mass fractions (reference krome.h:302-306):
+ * x[ncell][nspec] and the gas density rho[ncell] [g cm^-3]; n = rho x / m
+ * on the way in (0 for a species without mass), x = m n / rho on the way
+ * out for the cells that succeed (rescaled to the input sum of the
+ * fractions with the renormalize_x key); a failed cell keeps its input x.
+ * Host arrays; flags may be NULL. */
+int krome_solve_cells_x(int ncell, double* x, const double* rho,
+                        double* Tgas, const double* dt, const double* par,
+                        int par_stride, const void* extra, int* flags,
+                        const krome_opts* h);
+
+/* ---- device-resident data (reference krome.h:308-349) ----
+ * krome_solve_cells and _x on arrays in device memory, in one of two
+ * layouts: species-major n[i * ld + c] (ld >= ncell; 0: ncell, a Fortran
+ * n(ld, nspec)) or cell-major n[c * nspec + i]. Tgas, dt (and rho) [ncell]
+ * on the device; par device rows (par_stride 0 or npar) or NULL for the
+ * defaults; extra must be NULL; flags[ncell] on the device, may be NULL;
+ * summary (host, may be NULL) counts the cells: solved on the device,
+ * recovered on the host (always 0: there is no CPU fallback), failed. The
+ * device is synchronized before and after the call. Returns 0, the lowest
+ * failing cell's flag, -105 (a required parameter unset in some row:
+ * nothing integrated), -104 (unsupported configuration or a CUDA error),
+ * -111 (no device memory for the staging buffer) or -1 (bad arguments). */
+#define KROME_LAYOUT_SPECIES_MAJOR 0
+#define KROME_LAYOUT_CELL_MAJOR 1
+typedef struct {
+  long device; /* cells solved on the device */
+  long host;   /* failed on the device, solved on the host (0 here) */
+  long failed; /* failed */
+} krome_device_summary;
+/* krome.h:339-344 */
+int krome_solve_cells_device(int ncell, double* n, int layout, long ld,
+                             double* Tgas, const double* dt,
+                             const double* par, int par_stride,
+                             const void* extra, int* flags,
+                             krome_device_summary* summary,
+                             const krome_opts* h);
+/* krome.h:345-350 */
+int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
+                               int layout, long ld, double* Tgas,
+                               const double* dt, const double* par,
+                               int par_stride, const void* extra,
+                               int* flags, krome_device_summary* summary,
+                               const krome_opts* h);
+
 /* krome_get_rates (reference krome.h:387-389): k[ncell][nrea] at each
  * cell's rate temperature clamp(Tgas, Tcmb, 1e9); Phi and h unused */
 int krome_get_rates(int ncell, const double* n, const double* Tgas,

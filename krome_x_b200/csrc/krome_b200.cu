@@ -1259,6 +1259,239 @@ KB_API int krome_solve_cells(int ncell, double* n, double* Tgas,
                                 nullptr, h);
 }
 
+// ---- mass fractions and device-resident arrays (reference krome.h:
+// 296-349) ----
+
+// the reference's count of a device call's cells (krome.h:339-343); host
+// recovery does not exist in this library, so `host` stays 0
+struct krome_device_summary {
+  long device;
+  long host;
+  long failed;
+};
+
+namespace {
+// x_to_n_ / n_to_x_ / x_sum_ / n_to_x_out_ (solve_cell.hpp:2210-2233): n =
+// rho x / m (0 for a species without mass), x = m n / rho, rescaled to the
+// input sum of the fractions with renormalize_x
+KB_HD inline void x_to_n(const double* x, double rho, double* n) {
+  for (int i = 0; i < kbnet::NSPEC; ++i) {
+    const double m = kbnet::species_mass_g(i);
+    n[i] = m > 0.0 ? rho * x[i] / m : 0.0;
+  }
+}
+KB_HD inline double x_sum(const double* x) {
+  double s = 0.0;
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    if (kbnet::species_mass_g(i) > 0.0) s += x[i];
+  return s;
+}
+KB_HD inline void n_to_x_out(const double* n, double rho, double xin,
+                             int renormalize, double* x) {
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    x[i] = kbnet::species_mass_g(i) * n[i] / rho;
+  if (!renormalize) return;
+  const double s = x_sum(x);
+  if (s > 0.0)
+    for (int i = 0; i < kbnet::NSPEC; ++i) x[i] *= xin / s;
+}
+
+// species i of cell c in the caller's layout (krome.h:311-314): species-
+// major n[i * ld + c] (0) or cell-major n[c * nspec + i] (1)
+__device__ __forceinline__ long at_(int layout, long ld, int c, int i) {
+  return layout == 0 ? (long)i * ld + c : (long)c * kbnet::NSPEC + i;
+}
+// the caller's species (densities, or fractions with rho) into the
+// cell-major densities the solve takes; xin the fractions' input sums
+__global__ void kb_gather_in(int ncell, const double* src, int layout, long ld,
+                             const double* rho, double* n, double* xin) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  double v[kbnet::NSPEC];
+  for (int i = 0; i < kbnet::NSPEC; ++i) v[i] = src[at_(layout, ld, c, i)];
+  double* nc = n + (long)c * kbnet::NSPEC;
+  if (rho == nullptr) {
+    for (int i = 0; i < kbnet::NSPEC; ++i) nc[i] = v[i];
+    return;
+  }
+  xin[c] = x_sum(v);
+  x_to_n(v, rho[c], nc);
+}
+// the solved cells back into the caller's layout (a failed cell keeps its
+// input)
+__global__ void kb_scatter_out(int ncell, const double* n, const int* fl,
+                               int layout, long ld, const double* rho,
+                               const double* xin, int renormalize,
+                               double* dst) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell || fl[c] != 0) return;
+  const double* nc = n + (long)c * kbnet::NSPEC;
+  double v[kbnet::NSPEC];
+  if (rho == nullptr) {
+    for (int i = 0; i < kbnet::NSPEC; ++i) v[i] = nc[i];
+  } else {
+    n_to_x_out(nc, rho[c], xin[c], renormalize, v);
+  }
+  for (int i = 0; i < kbnet::NSPEC; ++i) dst[at_(layout, ld, c, i)] = v[i];
+}
+
+std::mutex g_dmu;  // the device entry points' scratch
+DevBuf g_dbuf;
+
+// krome_solve_cells_device and _x_device (krome.h:308-344): arrays in
+// device memory; the device fenced before and after; no host recovery
+int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
+                       long ld, double* Tgas, const double* dt,
+                       const double* par, int par_stride, const void* extra,
+                       int* flags, krome_device_summary* summary,
+                       const krome_opts* h) {
+  if (h == nullptr || ncell < 0 || arr == nullptr || Tgas == nullptr
+      || dt == nullptr)
+    return -1;
+  if (layout != 0 && layout != 1) return -1;
+  if (layout == 0) {
+    if (ld == 0) ld = ncell;
+    if (ld < ncell) return -1;
+  }
+  if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+  if (summary != nullptr) *summary = krome_device_summary{0, 0, 0};
+  if (ncell == 0) return 0;
+  if (extra != nullptr) return -104;  // no photon or dust bins here
+  if (cudaDeviceSynchronize() != cudaSuccess) return -104;
+  // the required-parameter rule on the caller's rows (a host copy)
+  const int ps = par != nullptr ? par_stride : 0;
+  std::vector<double> P(ps ? (size_t)ncell * ps : kbnet::NPAR);
+  if (par != nullptr) {
+    if (cudaMemcpy(P.data(), par, sizeof(double) * P.size(),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -1;
+  } else {
+    krome_params_default(P.data());
+  }
+  std::vector<int> hfl(ncell, 0);
+  int ret = check_params(ncell, P.data(), ps, hfl.data());
+  if (ret == 0) ret = unsupported(*h);
+  if (ret != 0 && ret != -105)
+    for (int c = 0; c < ncell; ++c) hfl[c] = ret;
+  const size_t fb = sizeof(int) * (size_t)ncell;
+  if (ret != 0) {
+    if (flags != nullptr
+        && cudaMemcpy(flags, hfl.data(), fb, cudaMemcpyHostToDevice) != cudaSuccess)
+      return -104;
+    if (summary != nullptr)
+      for (int c = 0; c < ncell; ++c) summary->failed += hfl[c] != 0;
+    return ret;
+  }
+  const bool staged = layout == 0 || rho != nullptr;
+  const size_t nb = staged ? sizeof(double) * (size_t)ncell * kbnet::NSPEC : 0;
+  const size_t xb = rho != nullptr ? sizeof(double) * (size_t)ncell : 0;
+  const size_t pb = par == nullptr ? sizeof(double) * kbnet::NPAR : 0;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  std::lock_guard<std::mutex> lock(g_dmu);
+  if (g_dbuf.ensure(al(nb) + al(xb) + al(pb) + al(fb) + 256) != cudaSuccess)
+    return -111;
+  char* b = static_cast<char*>(g_dbuf.p);
+  double* dn = staged ? reinterpret_cast<double*>(b) : arr; b += al(nb);
+  double* dx = reinterpret_cast<double*>(b); b += al(xb);
+  double* dp = reinterpret_cast<double*>(b); b += al(pb);
+  int* dfl = reinterpret_cast<int*>(b); b += al(fb);
+  unsigned* dcur = reinterpret_cast<unsigned*>(b);
+  const double* Pd = par;
+  cudaError_t e = cudaSuccess;
+  if (par == nullptr) {
+    e = cudaMemcpy(dp, P.data(), pb, cudaMemcpyHostToDevice);
+    Pd = dp;
+  }
+  const int tpb = 128, nblk = (ncell + tpb - 1) / tpb;
+  if (e == cudaSuccess && staged) {
+    kb_gather_in<<<nblk, tpb>>>(ncell, arr, layout, ld, rho, dn, dx);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = launch_any(*h, ncell, dn, Tgas, dt, Pd, ps, dfl, nullptr, dcur, 0);
+  if (e == cudaSuccess && staged) {
+    kb_scatter_out<<<nblk, tpb>>>(ncell, dn, dfl, layout, ld, rho, dx,
+                                  h->renormalize_x, arr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && flags != nullptr)
+    e = cudaMemcpyAsync(flags, dfl, fb, cudaMemcpyDeviceToDevice, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(hfl.data(), dfl, fb, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return -104;
+  }
+  for (int c = 0; c < ncell; ++c) {
+    if (summary != nullptr) {
+      if (hfl[c] == 0) ++summary->device;
+      else ++summary->failed;
+    }
+    if (ret == 0 && hfl[c] != 0) ret = hfl[c];
+  }
+  return ret;
+}
+}  // namespace
+
+// krome_solve_cells with mass fractions x[ncell][nspec] and the gas density
+// rho[ncell] [g cm^-3] (reference krome.h:302-306, krome.cpp:438-470): n =
+// rho x / m on the way in, x = m n / rho on the way out (rescaled to the
+// input sum with renormalize_x) for the cells that succeed; a failed cell
+// keeps its input x
+KB_API int krome_solve_cells_x(int ncell, double* x, const double* rho,
+                               double* Tgas, const double* dt,
+                               const double* par, int par_stride,
+                               const void* extra, int* flags,
+                               const krome_opts* h) {
+  if (h == nullptr || ncell < 0 || x == nullptr || rho == nullptr
+      || Tgas == nullptr || dt == nullptr)
+    return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR) return -1;
+  if (ncell == 0) return 0;
+  std::vector<double> n((size_t)ncell * kbnet::NSPEC), xin(ncell);
+  for (int c = 0; c < ncell; ++c) {
+    const double* xc = x + (size_t)c * kbnet::NSPEC;
+    xin[c] = x_sum(xc);
+    x_to_n(xc, rho[c], n.data() + (size_t)c * kbnet::NSPEC);
+  }
+  std::vector<int> fl(ncell, 0);
+  int* f = flags != nullptr ? flags : fl.data();
+  const int r = krome_solve_cells(ncell, n.data(), Tgas, dt, par, par_stride,
+                                  extra, f, h);
+  for (int c = 0; c < ncell; ++c)
+    if (f[c] == 0)
+      n_to_x_out(n.data() + (size_t)c * kbnet::NSPEC, rho[c], xin[c],
+                 h->renormalize_x, x + (size_t)c * kbnet::NSPEC);
+  return r;
+}
+
+// krome_solve_cells on device arrays (reference krome.h:308-349): n in the
+// species-major (0, leading dimension ld >= ncell, 0 for ncell) or cell-
+// major (1) layout, Tgas, dt [ncell], par rows or NULL (the defaults),
+// flags (device, may be NULL), summary (host, may be NULL)
+KB_API int krome_solve_cells_device(int ncell, double* n, int layout, long ld,
+                                    double* Tgas, const double* dt,
+                                    const double* par, int par_stride,
+                                    const void* extra, int* flags,
+                                    krome_device_summary* summary,
+                                    const krome_opts* h) {
+  return solve_device_entry(ncell, n, nullptr, layout, ld, Tgas, dt, par,
+                            par_stride, extra, flags, summary, h);
+}
+// the same with mass fractions and rho [ncell] on the device
+KB_API int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
+                                      int layout, long ld, double* Tgas,
+                                      const double* dt, const double* par,
+                                      int par_stride, const void* extra,
+                                      int* flags,
+                                      krome_device_summary* summary,
+                                      const krome_opts* h) {
+  if (rho == nullptr) return -1;
+  return solve_device_entry(ncell, x, rho, layout, ld, Tgas, dt, par,
+                            par_stride, extra, flags, summary, h);
+}
+
 namespace {
 // the rate coefficients of each cell at its rate temperature clamp(Tgas,
 // Tcmb, 1e9) (the reference's krome_get_rates query, krome.h:387-389)
