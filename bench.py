@@ -82,6 +82,10 @@ def parse():
     ap.add_argument("--cpu-cells", type=int, default=8192,
                     help="cells of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--large-cells", type=int, default=SEMENOV_CELLS,
+                    help="cells of the large-network form (the workload's "
+                         "batch is 16,384; the default is a seeded subset "
+                         "that keeps the run within minutes)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the adjoint and precision forms")
     return ap.parse_args()
@@ -571,7 +575,8 @@ def run_ours(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_forms:
         forms = {"adjoint": adjoint_form(torch, dev),
                  "precision": precision_form(torch, dev),
-                 "large_network": large_network_form(torch, dev)}
+                 "large_network": large_network_form(torch, dev,
+                                                     args.large_cells)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_leg(args.cpu_cells, args.warmup, args.steps)

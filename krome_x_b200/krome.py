@@ -138,6 +138,9 @@ class Network:
             "krome_solve_cells": (ctypes.c_int, [
                 ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_void_p,
                 _I, ctypes.c_void_p]),
+            "krome_solve_cells_x": (ctypes.c_int, [
+                ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int,
+                ctypes.c_void_p, _I, ctypes.c_void_p]),
             "krome_b200_solve_batch": (ctypes.c_int, [
                 ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _I, _L,
                 ctypes.c_void_p]),
@@ -307,6 +310,39 @@ class Network:
             return Result(n[0], T[0], flags[0], ierr,
                           None if st is None else st[0])
         return Result(n, T, flags, ierr, st)
+
+    def solve_x(self, x, rho, Tgas, dt, par=None, opts=None, check=True):
+        """solve() with mass fractions (reference runtime/interfaces/python/
+        krome.py:509-542): x[nspec] or x[ncell, nspec] and the gas density
+        rho [g cm^-3], scalar or per cell; n = rho x / m on the way in,
+        x = m n / rho on the way out (renormalize_x rescales to the input
+        sum) for the cells that succeed. Returns a Result whose n holds the
+        new mass fractions."""
+        x = np.array(x, dtype=float, order="C", copy=True)
+        if x.ndim == 0 or x.ndim > 2 or x.shape[-1] != self.nspec:
+            raise KromeError("x must have shape (%d,) or (ncell, %d), got %s"
+                             % (self.nspec, self.nspec, x.shape))
+        single = x.ndim == 1
+        x = x.reshape(-1, self.nspec)
+        ncell = x.shape[0]
+        cell = lambda v: np.array(np.broadcast_to(np.asarray(v, dtype=float),
+                                                  (ncell,)), order="C", copy=True)
+        rh, T, dtv = cell(rho), cell(Tgas), cell(dt)
+        opts = self._options(opts)
+        P, stride = self._params(par, ncell)
+        flags = np.zeros(ncell, dtype=np.intc)
+        ierr = self._lib.krome_solve_cells_x(
+            ncell, _dptr(x), _dptr(rh), _dptr(T), _dptr(dtv), _dptr(P), stride,
+            None, flags.ctypes.data_as(_I), opts._h)
+        if check and ierr != 0:
+            bad = np.flatnonzero(flags)
+            raise KromeError("krome_solve_cells_x returned %d: %s (failed "
+                             "cells: %s); pass check=False to get the result "
+                             "anyway" % (ierr, self.flag_message(ierr),
+                                         bad[:20].tolist() or "n/a"))
+        if single:
+            return Result(x[0], T[0], flags[0], ierr)
+        return Result(x, T, flags, ierr)
 
     def solve_batch(self, n, Tgas, dt, par=None, opts=None, check=True,
                     stats=False):

@@ -199,3 +199,23 @@ def test_device_entry_required_parameter_rule():
     assert fl[5] == -105 and (np.delete(fl, 5) == 0).all()
     np.testing.assert_array_equal(dn.cpu().numpy(), n)
     assert (s.device, s.failed) == (0, 1)
+
+
+@pytest.mark.gpu
+def test_python_solve_x_matches_the_c_entry():
+    net = krome.load(KEY)
+    lib = _lib(net)
+    n, T, dt, par, x, rho, _ = _case(64, seed=9)
+    opts = _opts(net)
+    r = net.solve_x(x, rho, T, dt, par, opts=opts, check=False)
+    xh, Th = x.copy(), T.copy()
+    fh = np.zeros(64, dtype=np.intc)
+    lib.krome_solve_cells_x(64, xh.ctypes.data_as(_D), rho.ctypes.data_as(_D),
+                            Th.ctypes.data_as(_D), dt.ctypes.data_as(_D),
+                            par.ctypes.data_as(_D), net.npar, None,
+                            fh.ctypes.data_as(_I), opts._h)
+    np.testing.assert_array_equal(r.n, xh)
+    np.testing.assert_array_equal(r.Tgas, Th)
+    np.testing.assert_array_equal(r.flags, fh)
+    # the caller's arrays are not modified (the reference's contract)
+    np.testing.assert_array_equal(x, _case(64, seed=9)[4])
