@@ -64,15 +64,19 @@ __device__ __noinline__ void adj_jac(const double* yin, const Params& p,
     }
     // the Tgas row's species columns: forward differences of the thermal
     // term at the rates of y, from its value at y (the integrator's
-    // fd_step_n steps)
+    // fd_step_n steps); the cooling's temperature-only parts are evaluated
+    // once for the row (thermal_pre: the same values as per column)
     const double Tth = fmin(fmax(y[N - 1], 2.73), 1e9);
+    ThermalPre tq;
+    thermal_pre(Tth, y, p, tq);
     KBL_LOOP for (int j = 0; j < NSPEC; ++j) {
       double yj = 0.0;
       KB_UNROLL for (int i = 0; i < N; ++i) yj = i == j ? y[i] : yj;
       const double h = fmax(fmax(1e-7 * fabs(yj), 1e-9 * sumabs), 1e-30);
       double yp[N];
       KB_UNROLL for (int i = 0; i < N; ++i) yp[i] = i == j ? yj + h : y[i];
-      J[(N - 1) + j * N] = (thermal_dTdt(Tth, yp, k, p) - f0[N - 1]) / h;
+      J[(N - 1) + j * N] =
+          (thermal_dTdt_with(tq, Tth, yp, k, p) - f0[N - 1]) / h;
     }
     return;
   }

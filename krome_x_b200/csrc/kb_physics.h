@@ -169,6 +169,191 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 KB_HD inline double cooling_H2(double, const double*) { return 0.0; }
 #endif
 
+// ---- the same two fits split at a fixed temperature ----
+// cooling_X_coef(T) evaluates a fit's temperature-only factors once and
+// cooling_X_with(c, n) combines them with the densities in the original
+// expressions' order of operations, so that
+// cooling_X_with(cooling_X_coef(T), n) == cooling_X(T, n) bit for bit: a
+// row of density derivatives at one T (the adjoint's Jacobian) then
+// evaluates the transcendental part once instead of once per column.
+struct CoolAtomicC {
+  double c[7];
+};
+KB_HD inline CoolAtomicC cooling_Atomic_coef(double Tgas) {
+  CoolAtomicC q{};
+#ifdef KB_HAS_E
+  const double temp = std::fmax(Tgas, 10.0);
+  const double T5 = temp / 1e5;
+  q.c[0] = 1.27e-21 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+           * std::exp(-1.578091e5 / temp);
+  q.c[1] = 9.38e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+           * std::exp(-2.853354e5 / temp);
+  q.c[2] = 4.95e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
+           * std::exp(-6.31515e5 / temp);
+  q.c[3] = 5.01e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+           * std::exp(-5.5338e4 / temp);
+  q.c[4] = 7.5e-19 / (1.0 + std::sqrt(T5)) * std::exp(-1.18348e5 / temp);
+  q.c[5] = 9.1e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+           * std::exp(-1.3179e4 / temp);
+  q.c[6] = 5.54e-17 * std::pow(temp, -0.397) / (1.0 + std::sqrt(T5))
+           * std::exp(-4.73638e5 / temp);
+#else
+  (void)Tgas;
+#endif
+  return q;
+}
+KB_HD inline double cooling_Atomic_with(const CoolAtomicC& q, const double* n) {
+#ifdef KB_HAS_E
+  const double ne = n[IDX_E];
+  (void)ne;
+  double cool = 0.0;
+#ifdef KB_HAS_H
+  cool += q.c[0] * ne * n[IDX_H];
+#endif
+#ifdef KB_HAS_He
+  cool += q.c[1] * ne * n[IDX_He];
+#endif
+#ifdef KB_HAS_Hej
+  cool += q.c[2] * ne * n[IDX_Hej];
+  cool += q.c[3] * ne * ne * n[IDX_Hej];
+#endif
+#ifdef KB_HAS_H
+  cool += q.c[4] * ne * n[IDX_H];
+#endif
+#ifdef KB_HAS_Hej
+  cool += q.c[5] * ne * ne * n[IDX_Hej];
+  cool += q.c[6] * ne * n[IDX_Hej];
+#endif
+  return std::fmax(cool, 0.0);
+#else
+  (void)q; (void)n;
+  return 0.0;
+#endif
+}
+
+// H2: per collider the factor a (and b: the fits whose density multiplies
+// before the w14 / w24 weight), the H2-H2 term's w24 x fit, the LTE HDL
+struct CoolH2C {
+  double aH, aHp, bHp, aH2, ae, be, aHe, bHe, HDL;
+  int fHp, fHe;  // 1: the fit is a (x n); 0: (a x n) x b
+};
+KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
+  CoolH2C q{};
+#ifdef KB_HAS_H2
+  const double temp = Tgas;
+  const double T3 = temp * 1e-3;
+  const double logt3 = std::log10(T3);
+  const double logt = std::log10(temp);
+  const double logt32 = logt3 * logt3, logt33 = logt32 * logt3,
+               logt34 = logt33 * logt3, logt35 = logt34 * logt3,
+               logt36 = logt35 * logt3, logt37 = logt36 * logt3,
+               logt38 = logt37 * logt3;
+  const double w14 = wCool_(logt, 1.0, 4.0);
+  const double w24 = wCool_(logt, 2.0, 4.0);
+  (void)w14; (void)logt36; (void)logt37; (void)logt38;
+  if (temp <= 1e2)
+    q.aH = std::pow(10.0, -16.818342 + 37.383713 * logt3
+           + 58.145166 * logt32 + 48.656103 * logt33
+           + 20.159831 * logt34 + 3.8479610 * logt35);
+  else if (temp <= 1e3)
+    q.aH = std::pow(10.0, -24.311209 + 3.5692468 * logt3
+           - 11.332860 * logt32 - 27.850082 * logt33
+           - 21.328264 * logt34 - 4.2519023 * logt35);
+  else if (temp <= 6e3)
+    q.aH = std::pow(10.0, -24.311209 + 4.6450521 * logt3
+           - 3.7209846 * logt32 + 5.9369081 * logt33
+           - 5.5108049 * logt34 + 1.5538288 * logt35);
+  else
+    q.aH = 1.862314467912518e-22 * wCool_(logt, 1.0, std::log10(6e3));
+  if (temp > 1e1 && temp <= 1e4) {
+    q.fHp = 1;
+    q.aHp = std::pow(10.0, -22.089523 + 1.5714711 * logt3
+            + 0.015391166 * logt32 - 0.23619985 * logt33
+            - 0.51002221 * logt34 + 0.32168730 * logt35);
+  } else {
+    q.fHp = 0;
+    q.aHp = 1.182509139382060e-21;
+    q.bHp = w14;
+  }
+  q.aH2 = w24 * std::pow(10.0, -23.962112 + 2.09433740 * logt3
+          - 0.77151436 * logt32 + 0.43693353 * logt33
+          - 0.14913216 * logt34 - 0.033638326 * logt35);
+  if (temp <= 5e2)
+    q.ae = std::pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+           + 96.743155 * logt32 + 343.19180 * logt33
+           + 734.71651 * logt34 + 983.67576 * logt35
+           + 801.81247 * logt36 + 364.14446 * logt37
+           + 70.609154 * logt38, 30.0));
+  else
+    q.ae = std::pow(10.0, -22.921189 + 1.6802758 * logt3
+           + 0.93310622 * logt32 + 4.0406627 * logt33
+           - 4.7274036 * logt34 - 8.8077017 * logt35
+           + 8.9167183 * logt36 + 6.4380698 * logt37
+           - 6.3701156 * logt38);
+  q.be = w24;
+  if (temp > 1e1 && temp <= 1e4) {
+    q.fHe = 1;
+    q.aHe = std::pow(10.0, -23.689237 + 2.1892372 * logt3
+            - 0.81520438 * logt32 + 0.29036281 * logt33
+            - 0.16596184 * logt34 + 0.19191375 * logt35);
+  } else {
+    q.fHe = 0;
+    q.aHe = 1.002560385050777e-22;
+    q.bHe = w14;
+  }
+  if (temp < 2e3) {
+    const double HDLR = 9.5e-22 * std::pow(T3, 3.76)
+                        / (1.0 + 0.12 * std::pow(T3, 2.1))
+                        * std::exp(-std::pow(0.13 / T3, 3.0))
+                        + 3e-24 * std::exp(-0.51 / T3);
+    const double HDLV = 6.7e-19 * std::exp(-5.86 / T3)
+                        + 1.6e-18 * std::exp(-11.7 / T3);
+    q.HDL = HDLR + HDLV;
+  } else if (temp <= 1e4) {
+    q.HDL = std::pow(10.0, -20.584225 + 5.0194035 * logt3
+          - 1.5738805 * logt32 - 4.7155769 * logt33
+          + 2.4714161 * logt34 + 5.4710750 * logt35
+          - 3.9467356 * logt36 - 2.2148338 * logt37
+          + 1.8161874 * logt38);
+  } else {
+    const double dump14 = 1.0
+        / (1.0 + std::exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
+    q.HDL = 5.531333679406485e-19 * dump14;
+  }
+#else
+  (void)Tgas;
+#endif
+  return q;
+}
+KB_HD inline double cooling_H2_with(const CoolH2C& q, const double* n) {
+#ifdef KB_HAS_H2
+  double cool = 0.0;
+#ifdef KB_HAS_H
+  const double fH2H = q.aH * n[IDX_H];
+  cool += fH2H;
+#endif
+#ifdef KB_HAS_Hj
+  const double fH2Hp = q.fHp ? q.aHp * n[IDX_Hj] : q.aHp * n[IDX_Hj] * q.bHp;
+  cool += fH2Hp;
+#endif
+  cool += q.aH2 * n[IDX_H2];
+#ifdef KB_HAS_E
+  const double fH2e = q.ae * n[IDX_E];
+  cool += fH2e * q.be;
+#endif
+#ifdef KB_HAS_He
+  const double fH2He = q.fHe ? q.aHe * n[IDX_He] : q.aHe * n[IDX_He] * q.bHe;
+  cool += fH2He;
+#endif
+  if (cool <= 0.0) return 0.0;
+  if (q.HDL == 0.0) return 0.0;
+  return n[IDX_H2] / (1.0 / q.HDL + 1.0 / cool);
+#else
+  (void)q; (void)n;
+  return 0.0;
+#endif
+}
+
 // Planck mean opacity (Lenzuni+1996, density-only fit)
 KB_HD inline double kpla_(const double* n) {
   const double rho = rho_(n);

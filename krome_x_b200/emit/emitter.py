@@ -589,6 +589,18 @@ class Emitter:
                   % (self.den(ion), j, j))
             w("  return kbc::boltzmann_erg * T * c;")
             w("}")
+            # the same from rates evaluated before (thermal_pre)
+            w("KB_HD inline double cooling_recomb_with_(const double* k0, "
+              "const double* tdk, double Tgas, const double* n, const Params& p) {")
+            w("  const double T = std::fmin(std::fmax(Tgas, p.Tcmb), 1e9);")
+            w("  double c = 0.0;")
+            for j, rx in enumerate(rxs):
+                ion = [r["sp"] for r in rx["reactants"] if r["sp"] != "e-"][0]
+                w("  c += n[IDX_E] * %s * std::fmax(0.0, 1.5 * k0[%d] + tdk[%d]);"
+                  % (self.den(ion), j, j))
+            w("  return kbc::boltzmann_erg * T * c;")
+            w("}")
+            self.n_recomb = nr
         if th.get("cool_H2"):
             mode = self.gen.h2_opacity
             w("KB_HD inline double h2_opacity_(const double* n) {")
@@ -637,6 +649,50 @@ class Emitter:
         for f, expr in cool_order:
             if th.get(f):
                 w("  cool += %s;" % expr)
+        w("  return (gamma_index(T, n, p) - 1.0) * (heat - cool)")
+        w("      / (kbc::boltzmann_erg * ntot_(n));")
+        w("}")
+        # the temperature-only parts of the cooling at T, and dTgas/dt from
+        # them: thermal_dTdt_with(thermal_pre(T), T, n, k, p) ==
+        # thermal_dTdt(T, n, k, p) bit for bit (a row of density
+        # derivatives at one T evaluates them once)
+        atomic, h2 = th.get("cool_atomic"), th.get("cool_H2")
+        w("// the cooling's temperature-only parts at one T (a row of density")
+        w("// derivatives at that T evaluates them once): thermal_dTdt_with of")
+        w("// thermal_pre(T) equals thermal_dTdt bit for bit")
+        w("struct ThermalPre {")
+        if atomic:
+            w("  CoolAtomicC atomic;")
+            w("  double k0[%d], tdk[%d];" % (self.n_recomb, self.n_recomb))
+        if h2:
+            w("  CoolH2C h2;")
+        w("  int unused_;")
+        w("};")
+        w("KB_HD inline void thermal_pre(double T, const double* n, "
+          "const Params& p, ThermalPre& q) {")
+        w("  (void)T; (void)n; (void)p; (void)q;")
+        if atomic:
+            w("  q.atomic = cooling_Atomic_coef(T);")
+            w("  recomb_rates_(std::fmin(std::fmax(T, p.Tcmb), 1e9), n, p, "
+              "q.k0, q.tdk);")
+        if h2:
+            w("  q.h2 = cooling_H2_coef(T);")
+        w("}")
+        w("KB_HD inline double thermal_dTdt_with(const ThermalPre& q, double T, "
+          "const double* n, const double* k, const Params& p) {")
+        w("  (void)q; (void)k; (void)p;")
+        w("  double heat = 0.0, cool = 0.0;")
+        for f, expr in heat_order:
+            if th.get(f):
+                w("  heat += %s;" % expr)
+        with_ = {
+            "cool_atomic": "cooling_Atomic_with(q.atomic, n) + "
+                           "cooling_recomb_with_(q.k0, q.tdk, T, n, p)",
+            "cool_H2": "cooling_H2_with(q.h2, n) * h2_opacity_(n)",
+        }
+        for f, expr in cool_order:
+            if th.get(f):
+                w("  cool += %s;" % with_.get(f, expr))
         w("  return (gamma_index(T, n, p) - 1.0) * (heat - cool)")
         w("      / (kbc::boltzmann_erg * ntot_(n));")
         w("}")

@@ -1124,6 +1124,21 @@ KB_HD inline double thermal_dTdt(double T, const double* n, const double* k, con
   return (gamma_index(T, n, p) - 1.0) * (heat - cool)
       / (kbc::boltzmann_erg * ntot_(n));
 }
+// the cooling's temperature-only parts at one T (a row of density
+// derivatives at that T evaluates them once): thermal_dTdt_with of
+// thermal_pre(T) equals thermal_dTdt bit for bit
+struct ThermalPre {
+  int unused_;
+};
+KB_HD inline void thermal_pre(double T, const double* n, const Params& p, ThermalPre& q) {
+  (void)T; (void)n; (void)p; (void)q;
+}
+KB_HD inline double thermal_dTdt_with(const ThermalPre& q, double T, const double* n, const double* k, const Params& p) {
+  (void)q; (void)k; (void)p;
+  double heat = 0.0, cool = 0.0;
+  return (gamma_index(T, n, p) - 1.0) * (heat - cool)
+      / (kbc::boltzmann_erg * ntot_(n));
+}
 
 // g[r] += sum_i mu_i d f_i / d ln k_r at the state n with the rates k;
 // muT: mu of the Tgas row (0 without it), Tth the thermal temperature

@@ -989,6 +989,17 @@ KB_HD inline double cooling_recomb_(double Tgas, const double* n, const Params& 
   c += n[IDX_E] * n[IDX_Dj] * std::fmax(0.0, 1.5 * k0[5] + tdk[5]);
   return kbc::boltzmann_erg * T * c;
 }
+KB_HD inline double cooling_recomb_with_(const double* k0, const double* tdk, double Tgas, const double* n, const Params& p) {
+  const double T = std::fmin(std::fmax(Tgas, p.Tcmb), 1e9);
+  double c = 0.0;
+  c += n[IDX_E] * n[IDX_Hj] * std::fmax(0.0, 1.5 * k0[0] + tdk[0]);
+  c += n[IDX_E] * n[IDX_Hj] * std::fmax(0.0, 1.5 * k0[1] + tdk[1]);
+  c += n[IDX_E] * n[IDX_Hej] * std::fmax(0.0, 1.5 * k0[2] + tdk[2]);
+  c += n[IDX_E] * n[IDX_Hej] * std::fmax(0.0, 1.5 * k0[3] + tdk[3]);
+  c += n[IDX_E] * n[IDX_Hejj] * std::fmax(0.0, 1.5 * k0[4] + tdk[4]);
+  c += n[IDX_E] * n[IDX_Dj] * std::fmax(0.0, 1.5 * k0[5] + tdk[5]);
+  return kbc::boltzmann_erg * T * c;
+}
 KB_HD inline double h2_opacity_(const double* n) {
   (void)n;
   return 1.0;
@@ -1006,6 +1017,31 @@ KB_HD inline double thermal_dTdt(double T, const double* n, const double* k, con
   heat += ntot_(n) * kbc::boltzmann_erg * T / p.tff;
   cool += cooling_Atomic(T, n) + cooling_recomb_(T, n, p);
   cool += cooling_H2(T, n) * h2_opacity_(n);
+  return (gamma_index(T, n, p) - 1.0) * (heat - cool)
+      / (kbc::boltzmann_erg * ntot_(n));
+}
+// the cooling's temperature-only parts at one T (a row of density
+// derivatives at that T evaluates them once): thermal_dTdt_with of
+// thermal_pre(T) equals thermal_dTdt bit for bit
+struct ThermalPre {
+  CoolAtomicC atomic;
+  double k0[6], tdk[6];
+  CoolH2C h2;
+  int unused_;
+};
+KB_HD inline void thermal_pre(double T, const double* n, const Params& p, ThermalPre& q) {
+  (void)T; (void)n; (void)p; (void)q;
+  q.atomic = cooling_Atomic_coef(T);
+  recomb_rates_(std::fmin(std::fmax(T, p.Tcmb), 1e9), n, p, q.k0, q.tdk);
+  q.h2 = cooling_H2_coef(T);
+}
+KB_HD inline double thermal_dTdt_with(const ThermalPre& q, double T, const double* n, const double* k, const Params& p) {
+  (void)q; (void)k; (void)p;
+  double heat = 0.0, cool = 0.0;
+  heat += heating_chem(T, n, k);
+  heat += ntot_(n) * kbc::boltzmann_erg * T / p.tff;
+  cool += cooling_Atomic_with(q.atomic, n) + cooling_recomb_with_(q.k0, q.tdk, T, n, p);
+  cool += cooling_H2_with(q.h2, n) * h2_opacity_(n);
   return (gamma_index(T, n, p) - 1.0) * (heat - cool)
       / (kbc::boltzmann_erg * ntot_(n));
 }

@@ -901,6 +901,28 @@ KB_HD inline double thermal_dTdt(double T, const double* n, const double* k, con
   return (gamma_index(T, n, p) - 1.0) * (heat - cool)
       / (kbc::boltzmann_erg * ntot_(n));
 }
+// the cooling's temperature-only parts at one T (a row of density
+// derivatives at that T evaluates them once): thermal_dTdt_with of
+// thermal_pre(T) equals thermal_dTdt bit for bit
+struct ThermalPre {
+  CoolH2C h2;
+  int unused_;
+};
+KB_HD inline void thermal_pre(double T, const double* n, const Params& p, ThermalPre& q) {
+  (void)T; (void)n; (void)p; (void)q;
+  q.h2 = cooling_H2_coef(T);
+}
+KB_HD inline double thermal_dTdt_with(const ThermalPre& q, double T, const double* n, const double* k, const Params& p) {
+  (void)q; (void)k; (void)p;
+  double heat = 0.0, cool = 0.0;
+  heat += heating_chem(T, n, k);
+  heat += ntot_(n) * kbc::boltzmann_erg * T / p.tff;
+  cool += cooling_H2_with(q.h2, n) * h2_opacity_(n);
+  cool += cooling_chem(n, k);
+  cool += cooling_Continuum(T, n);
+  return (gamma_index(T, n, p) - 1.0) * (heat - cool)
+      / (kbc::boltzmann_erg * ntot_(n));
+}
 
 // g[r] += sum_i mu_i d f_i / d ln k_r at the state n with the rates k;
 // muT: mu of the Tgas row (0 without it), Tth the thermal temperature

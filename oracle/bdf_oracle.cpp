@@ -1243,6 +1243,19 @@ ORACLE_API int oracle_rates_forms(double T, const double* n,
   return BK_VAR_AFFINE;
 }
 #endif
+// the thermal term directly and from its temperature-only parts evaluated
+// at the state y (the adjoint's Tgas row): out[0] thermal_dTdt(T, n, k, p),
+// out[1] thermal_dTdt_with(thermal_pre(T, y, p), T, n, k, p)
+ORACLE_API void oracle_thermal_forms(double T, const double* y,
+                                     const double* n, const double* k,
+                                     const double* par, double* out) {
+  Params p;
+  params_from_row(par, p);
+  ThermalPre q;
+  thermal_pre(T, y, p, q);
+  out[0] = thermal_dTdt(T, n, k, p);
+  out[1] = thermal_dTdt_with(q, T, n, k, p);
+}
 ORACLE_API int oracle_nrea(void) { return NREA; }
 ORACLE_API int oracle_nspec(void) { return NSPEC; }
 ORACLE_API int oracle_npar(void) { return NPAR; }

@@ -28,6 +28,7 @@ import ctypes
 import numpy as np
 import pytest
 
+from conftest import NETWORKS
 from krome_x_b200 import krome, netinfo, workloads
 from oracle import Oracle
 
@@ -164,6 +165,37 @@ def test_oracle_adjoint_matches_tight_finite_differences():
     res = [orc.adjoint(n, T, dt, par, g, gt, **o) for g, gt in sd]
     check_against_fd(lambda i: (res[i]["dm"], res[i]["dn0"], res[i]["dT0"]),
                      n, T, fd, REACTIONS, species)
+
+
+@pytest.mark.parametrize("key", NETWORKS)
+def test_thermal_row_form_equals_the_thermal_term(key):
+    """the adjoint's Tgas row evaluates the cooling's temperature-only parts
+    once per row (thermal_pre at the accepted state y) and every column from
+    them: the same value as the thermal term itself, bit for bit, at states
+    that differ from y in one density"""
+    D = ctypes.POINTER(ctypes.c_double)
+    lib = Oracle(key).lib
+    lib.oracle_thermal_forms.argtypes = [ctypes.c_double, D, D, D, D, D]
+    lib.oracle_thermal_forms.restype = None
+    lib.oracle_rates.argtypes = [ctypes.c_double, D, D, D]
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](24, info, seed=12)
+    nrea = lib.oracle_nrea()
+    for c in range(len(n)):
+        y = np.ascontiguousarray(n[c])
+        pr = np.ascontiguousarray(np.broadcast_to(par, (len(n), len(info["params"])))[c])
+        k = np.zeros(nrea + 1)
+        lib.oracle_rates(float(T[c]), y.ctypes.data_as(D), pr.ctypes.data_as(D),
+                         k.ctypes.data_as(D))
+        Tth = min(max(float(T[c]), 2.73), 1e9)
+        for j in range(len(y)):
+            yp = y.copy()
+            yp[j] += max(1e-7 * abs(y[j]), 1e-9 * np.abs(y).sum(), 1e-30)
+            out = np.zeros(2)
+            lib.oracle_thermal_forms(Tth, y.ctypes.data_as(D),
+                                     yp.ctypes.data_as(D), k.ctypes.data_as(D),
+                                     pr.ctypes.data_as(D), out.ctypes.data_as(D))
+            assert out[0] == out[1], (key, c, j, out)
 
 
 def test_adjoint_bad_arguments_and_required_parameters():
