@@ -14,9 +14,13 @@
  * Flags: 0 success; CVODE's -1 ... -27 for a failed integration (the cell
  * left untouched); -105 a REQUIRED parameter unset in some row (nothing
  * integrated); -110 the integration ended at Tgas <= 0; -104 a
- * configuration this library does not run (LAPACK or sparse linsol,
- * conservation) or no usable GPU; -111 the device buffers could not be
- * allocated; -1 bad arguments. There is no CPU fallback.
+ * configuration this library does not run (LAPACK linsol; sparse linsol on
+ * the small networks, dense on the large) or no usable GPU; -111 the device
+ * buffers could not be allocated; -1 bad arguments. There is no CPU
+ * fallback. The conserve key (0 off, 1 the electrons restore the input net
+ * charge, 2 the projection onto the input element totals and charge, 3 the
+ * electrons neutralize the ions) applies to the cells that succeed, as the
+ * reference's post-solve rule (solve_cell.hpp:1458-1500).
  */
 #ifndef KROME_B200_H
 #define KROME_B200_H

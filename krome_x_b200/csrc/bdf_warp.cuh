@@ -96,6 +96,7 @@ struct SolveOpts {
   int fail_every;  // fault injection: cells c with (c + 1) % fail_every == 0
                    // report TOO_MUCH_WORK without integrating (0: off)
   int lu32;        // the Newton matrix factored in FP32 (lane layout only)
+  int conserve;    // post-solve conservation mode (kb_conserve.h), 0 none
 };
 
 __device__ __forceinline__ double smax_(double a, double b) { return a > b ? a : b; }
@@ -1087,11 +1088,22 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
               || flag == UNREC_RHSFUNC_ERR || flag == FIRST_RHSFUNC_ERR))
     flag = FLAG_NONPOSITIVE_T;
   if (flag == 0) {
-    if (lane < NSPEC) {
-      double v = yv;
-      if (so.clip_negative && v < 0.0) v = 0.0;
-      n[lane] = v;
+    double v = lane < NSPEC ? yv : 0.0;
+    if (so.clip_negative && v < 0.0) v = 0.0;
+    if (so.conserve > 0) {  // lane 0 conserves the cell against its input
+      const double v0 = lane < NSPEC ? n[lane] : 0.0;
+      double cn[NSPEC], c0[NSPEC];
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
+        cn[i] = __shfl_sync(FULL, v, i);
+        c0[i] = __shfl_sync(FULL, v0, i);
+      }
+      if (lane == 0) kbnet::conserve_cell(c0, cn, so.conserve);
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
+        const double ci = __shfl_sync(FULL, cn[i], 0);
+        if (lane == i) v = ci;
+      }
     }
+    if (lane < NSPEC) n[lane] = v;
     if (EVT && lane == 0) *Tg = Tend;
   }
   return flag;

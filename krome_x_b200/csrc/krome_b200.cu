@@ -214,11 +214,18 @@ __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
                   || flag == kbw::FIRST_RHSFUNC_ERR))
     flag = kbw::FLAG_NONPOSITIVE_T;
   if (flag == 0) {
+    double nv[NSPEC];
     KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
       double v = s.y[i];
       if (so.clip_negative && v < 0.0) v = 0.0;
-      n[(long)c * NSPEC + i] = v;
+      nv[i] = v;
     }
+    if (so.conserve > 0) {  // against the cell's input, still in n
+      double n0[NSPEC];
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) n0[i] = n[(long)c * NSPEC + i];
+      kbnet::conserve_cell(n0, nv, so.conserve);
+    }
+    KB_UNROLL for (int i = 0; i < NSPEC; ++i) n[(long)c * NSPEC + i] = nv[i];
     if (EVT) T[c] = Tend;
   }
   if (flags != nullptr) flags[c] = flag;
@@ -512,8 +519,14 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
       for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) {
         double v = yout[i];
         if (so.clip_negative && v < 0.0) v = 0.0;
-        nrow[i] = v;
+        yout[i] = v;
       }
+      if (so.conserve > 0) {  // thread 0, against the input still in nrow
+        __syncthreads();
+        if (threadIdx.x == 0) conserve_cell(nrow, yout, so.conserve);
+        __syncthreads();
+      }
+      for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) nrow[i] = yout[i];
     }
   }
   if (threadIdx.x == 0) {
@@ -613,6 +626,7 @@ SolveOpts to_solve_opts(const krome_opts& h) {
   so.clip_negative = h.clip_negative;
   so.fail_every = h.fail_every;
   so.lu32 = h.lu32;
+  so.conserve = h.conserve;
   return so;
 }
 
@@ -947,11 +961,9 @@ KB_API int krome_opts_get(const krome_opts* hc, const char* key, double* v) {
 
 namespace {
 // what this library does not implement returns FLAG_UNSUPPORTED before any
-// work: LAPACK and the sparse LU (small networks use the dense LU),
-// conservation, photon bins; the FP32 Newton-matrix form exists in the
-// lane layout only
+// work: LAPACK and the sparse LU (small networks use the dense LU), photon
+// bins; the FP32 Newton-matrix form exists in the lane layout only
 int unsupported(const krome_opts& h) {
-  if (h.conserve != 0) return -104;
 #ifdef KB_LARGE_NETWORK
   // the large networks: the sparse LU (linsol auto or sparse), fixed Tgas,
   // FP64

@@ -205,9 +205,23 @@ class Emitter:
         nH = [float(self.gen._natoms_H(s)) if hasattr(self.gen, "_natoms_H")
               else float((sp[s]["composition"] or {}).get("H", 0))
               for s in self.species]
+        # the element composition (the reference's emit_composition,
+        # kromex/codegen.py:3544-3567: elements in sorted order, an opaque
+        # species all zero), for the post-solve conservation
+        elems = sorted({e for x in self.species
+                        for e in (sp[x]["composition"] or {})})
+        comp = [str((sp[x]["composition"] or {}).get(e, 0)
+                    if not sp[x]["opaque"] else 0)
+                for x in self.species for e in elems] or ["0"]
+        w("constexpr int NELEM = %d;" % len(elems))
+        self.meta_elements = (elems, [[(sp[x]["composition"] or {}).get(e, 0)
+                                       if not sp[x]["opaque"] else 0
+                                       for e in elems] for x in self.species])
         tabs = (("double", "species_mass_g", [repr(float(m)) for m in mass_g]),
                 ("int", "species_charge", [str(c) for c in charge]),
-                ("double", "species_natoms_H", [repr(x) for x in nH]))
+                ("double", "species_natoms_H", [repr(x) for x in nH]),
+                ("int", "species_opaque", ["1" if sp[x]["opaque"] else "0"
+                                           for x in self.species]))
         self.natoms_H = list(nH)
         for ty, name, vals in tabs:
             body = ", ".join(vals)
@@ -231,6 +245,19 @@ class Emitter:
                 w("  constexpr %s t_[NSPEC] = {%s};" % (ty, body))
                 w("  return t_[i];")
                 w("}")
+        # species_element(i, e): atoms of element e in species i
+        body = ", ".join(comp)
+        w("inline constexpr int species_elements_t_[%d] = {%s};" % (len(comp), body))
+        w("#ifdef __CUDACC__")
+        w("__device__ const int d_species_elements_[%d] = {%s};" % (len(comp), body))
+        w("#endif")
+        w("KB_HD inline int species_element(int i, int e) {")
+        w("#ifdef __CUDA_ARCH__")
+        w("  return d_species_elements_[i * NELEM + e];")
+        w("#else")
+        w("  return species_elements_t_[i * NELEM + e];")
+        w("#endif")
+        w("}")
         # summing helpers: sequential sums in species order (reference:
         # generated net_<name>_core.hpp ntot_ / Hnuclei_ / rho_)
         w("KB_HD inline double ntot_(const double* n) {")
@@ -297,11 +324,14 @@ class Emitter:
             defaults=[None if d is None else d for d in dflt],
             required_by={s: gen.param_required_by.get(s, "") for s in pn
                          if s in req},
-            nrea=nr, options=self.cfg)
+            nrea=nr, options=self.cfg,
+            elements=self.meta_elements[0],
+            species_elements=self.meta_elements[1])
         w("")
 
     def emit_physics(self):
         self.w('#include "../csrc/kb_physics.h"')
+        self.w('#include "../csrc/kb_conserve.h"')
         self.w("")
 
     def emit_vars(self):

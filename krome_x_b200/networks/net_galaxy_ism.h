@@ -37,6 +37,7 @@ constexpr int IDX_E = 8;
 constexpr int IDX_ELECTRON = 8;
 
 inline const char* const species_names[NSPEC] = {"H", "H+", "H-", "H2", "H2+", "He", "He+", "He++", "e-"};
+constexpr int NELEM = 2;
 KB_HD inline double species_mass_g(int i) {
   constexpr double t_[NSPEC] = {1.6738233791328e-24, 1.6729124407627538e-24, 1.6747343175028463e-24, 3.3476467582656e-24, 3.346735819895553e-24, 6.64647366797316e-24, 6.645562729603113e-24, 6.644651791233067e-24, 9.10938370046373e-28};
   return t_[i];
@@ -48,6 +49,21 @@ KB_HD inline int species_charge(int i) {
 KB_HD inline double species_natoms_H(int i) {
   constexpr double t_[NSPEC] = {1.0, 1.0, 1.0, 2.0, 2.0, 0.0, 0.0, 0.0, 0.0};
   return t_[i];
+}
+KB_HD inline int species_opaque(int i) {
+  constexpr int t_[NSPEC] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  return t_[i];
+}
+inline constexpr int species_elements_t_[18] = {1, 0, 1, 0, 1, 0, 2, 0, 2, 0, 0, 1, 0, 1, 0, 1, 0, 0};
+#ifdef __CUDACC__
+__device__ const int d_species_elements_[18] = {1, 0, 1, 0, 1, 0, 2, 0, 2, 0, 0, 1, 0, 1, 0, 1, 0, 0};
+#endif
+KB_HD inline int species_element(int i, int e) {
+#ifdef __CUDA_ARCH__
+  return d_species_elements_[i * NELEM + e];
+#else
+  return species_elements_t_[i * NELEM + e];
+#endif
 }
 KB_HD inline double ntot_(const double* n) {
   double s = 0.0;
@@ -96,6 +112,7 @@ KB_HD inline int params_missing(const Params& p) {
 }
 
 #include "../csrc/kb_physics.h"
+#include "../csrc/kb_conserve.h"
 
 KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;

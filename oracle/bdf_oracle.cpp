@@ -1186,6 +1186,7 @@ struct oracle_opts {
   int max_err_fails, max_conv_fails, max_restarts;
   int clip_negative;
   int lu32;     // the Newton matrix factored in FP32 (FP64 fallback)
+  int conserve;  // post-solve conservation mode (solve_cell.hpp:1458-1500)
 };
 
 // per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf,
@@ -1340,10 +1341,13 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
   if (yfin != nullptr)
     for (int i = 0; i < N; ++i) yfin[i] = y[i];
   if (flag == 0) {
+    double n0[NSPEC];
     for (int i = 0; i < NSPEC; ++i) {
+      n0[i] = n[i];
       n[i] = y[i];
       if (so->clip_negative && n[i] < 0.0) n[i] = 0.0;
     }
+    conserve_cell(n0, n, so->conserve);  // solve_cell.hpp:2169-2175
     if (c.iT >= 0) *Tgas = y[c.iT];
   }
   return flag;

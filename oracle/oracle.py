@@ -33,7 +33,8 @@ class _Opts(ctypes.Structure):
                 ("max_err_fails", ctypes.c_int),
                 ("max_conv_fails", ctypes.c_int),
                 ("max_restarts", ctypes.c_int),
-                ("clip_negative", ctypes.c_int), ("lu32", ctypes.c_int)]
+                ("clip_negative", ctypes.c_int), ("lu32", ctypes.c_int),
+                ("conserve", ctypes.c_int)]
 
 
 def _ptr(a, t=_D):
@@ -56,7 +57,7 @@ class Oracle:
     def solve(self, n, T, dt, par, evolve_T=1, jac=0, rtol=1e-6, atol_n=1e-20,
               atol_T=1e-6, max_steps=100000, max_err_fails=7,
               max_conv_fails=10, max_restarts=5, clip_negative=1, lu32=0,
-              threads=None, **_):
+              conserve=0, threads=None, **_):
         n = np.array(n, dtype=float, order="C", copy=True)
         T = np.array(T, dtype=float, order="C", copy=True)
         dt = np.ascontiguousarray(dt, dtype=float)
@@ -67,7 +68,7 @@ class Oracle:
         stats = np.zeros((ncell, NSTAT), dtype=np.int64)
         o = _Opts(int(evolve_T), int(jac), rtol, atol_n, atol_T,
                   int(max_steps), max_err_fails, max_conv_fails,
-                  max_restarts, int(clip_negative), int(lu32))
+                  max_restarts, int(clip_negative), int(lu32), int(conserve))
         nt = threads or os.cpu_count() or 1
         t0 = time.perf_counter()
         ret = self.lib.oracle_solve_cells(
