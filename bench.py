@@ -22,7 +22,10 @@ exists for this path). A step is 262,144 cell-solves.
   cpu_baseline  the reference's own krome_solve_cells (compiled from its
             sources with OpenMP, oracle/_ref) on the host cores, on a sample
             of the same loop
-  forms     (N = 1) the other two forms, each on its own workload:
+  forms     (N = 1) the kernel forms, each on its own workload:
+            batching   one solve of 65,536 primordial3 cells with each
+                       launch form: one lane / one warp per cell, each on
+                       a persistent work-queue grid or a plain grid
             adjoint    the differentiation workload: 65,536 primordial cells
                        (cooling ATOMIC, H2; heating CHEM, COMPRESS; rtol 1e-6),
                        the plain solve, the recording solve and the reverse
@@ -457,6 +460,49 @@ def large_network_form(torch, dev, ncell=SEMENOV_CELLS):
                     "algorithmic_gbs": io / (ms * 1e-3) / 1e9}}
 
 
+def batching_form(torch, dev, ncell=65536, reps=2):
+    """the batching workload's launch forms on one solve of its cells (the
+    first call of the hydro loop: the uneven-stiffness primordial3 batch;
+    65,536 cells of its distribution keep the warp forms within seconds):
+    one lane or one warp per cell, each as a persistent work-queue grid or
+    a plain one-cell-per-lane (warp) grid, device-timed, best of reps"""
+    from krome_x_b200 import krome
+    info, n, T, dt, par = inputs(ncell, seed=rank_seed(0))
+    net = krome.load(NETWORK)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    dtd, pd = t(dt), t(par)
+    out = {"workload": "primordial3, %d cells, one solve (dt = 0.01 tff), "
+                       "rtol 1e-6" % ncell}
+    for layout in ("lane", "warp"):
+        for kernel in ("persistent", "plain"):
+            o = net.options(evolve_T=1, jac="auto", linsol="auto", rtol=RTOL,
+                            atol_n=1e-20, atol_T=1e-6, kernel=kernel,
+                            layout=1 if layout == "lane" else 0, lane_minb=2)
+            best, failed = None, 0
+            for _ in range(reps):
+                nd, Td = t(n), t(T)
+                fl = torch.zeros(ncell, dtype=torch.int32, device=dev)
+                cur = torch.zeros(1, dtype=torch.int32, device=dev)
+                torch.cuda.synchronize()
+                e0 = _events(torch)
+                net.solve_device(nd, Td, dtd, pd, fl, opts=o, cursor=cur)
+                e1 = _events(torch)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+                failed = int((fl != 0).sum().item())
+            out["%s_%s" % (layout, kernel)] = {
+                "cell_solves_per_s": ncell / (best * 1e-3), "ms": best,
+                "failed_cells": failed}
+    out["persistent_lane_over_plain_warp"] = (
+        out["lane_persistent"]["cell_solves_per_s"]
+        / out["warp_plain"]["cell_solves_per_s"])
+    out["persistent_over_plain_warp_layout"] = (
+        out["warp_persistent"]["cell_solves_per_s"]
+        / out["warp_plain"]["cell_solves_per_s"])
+    return out
+
+
 def _hbm_peak():
     """the HBM roofline: the measured copy bandwidth of MEASURED_PEAKS.json,
     else the pool's earlier measurement (6.65 TB/s), and which"""
@@ -573,7 +619,8 @@ def run_ours(args, rank, world, local):
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
-        forms = {"adjoint": adjoint_form(torch, dev),
+        forms = {"batching": batching_form(torch, dev),
+                 "adjoint": adjoint_form(torch, dev),
                  "precision": precision_form(torch, dev),
                  "large_network": large_network_form(torch, dev,
                                                      args.large_cells)}
