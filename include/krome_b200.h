@@ -134,6 +134,37 @@ int krome_get_rates(int ncell, const double* n, const double* Tgas,
  * visible */
 int krome_has_device(void);
 
+/* ---- host utilities (reference krome.h:473-501, 539, 645-652) ---- */
+/* krome.h:476-477: tot[ncell][nelem] element totals [atoms cm^-3], or per
+ * gram [atoms g^-1] from mass fractions */
+int krome_get_element_totals(int ncell, const double* n, double* tot);
+int krome_get_element_totals_x(int ncell, const double* x, double* tot);
+/* krome.h:478-497: consistent advection -- each cell moved to its reference
+ * element totals ref (ref_stride 0 one row, nelem a row per cell) and to
+ * zero net charge; flags 0, -112 (unreachable: corrected as far as
+ * possible) or the warning 2 (a species changed by more than 50 %); par
+ * may be NULL (no freeze directives in these networks) */
+int krome_conserve_cells(int ncell, double* n, const double* ref,
+                         int ref_stride, const double* par, int par_stride,
+                         int* flags);
+int krome_conserve_cells_x(int ncell, double* x, const double* ref,
+                           int ref_stride, const double* par, int par_stride,
+                           int* flags);
+/* krome.h:501, 539: x = m n / rho and back, rho[ncell] [g cm^-3] */
+int krome_n2x(int ncell, const double* n, const double* rho, double* x);
+int krome_x2n(int ncell, const double* x, const double* rho, double* n);
+/* krome.h:646-652: species mass [g] (NaN out of range), charge, elements */
+double krome_species_mass(int i);
+int krome_species_charge(int i);
+int krome_nelem(void);
+const char* krome_element_name(int e);
+int krome_species_natoms(int i, int e);
+/* krome.h:194-201: the device backend's set-up; this library needs none:
+ * 0 with a usable device (-104 without); _id makes the device current */
+int krome_device_initialize(void);
+int krome_device_initialize_id(int device_id);
+int krome_device_finalize(void);
+
 /* ---- additions of this library ---- */
 
 /* the number of per-cell counters, and the equations of a cell */

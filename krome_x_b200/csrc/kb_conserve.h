@@ -39,8 +39,9 @@ KB_HD inline double totals_residual_(const double* n, const double* target,
   return worst;
 }
 
+// fixed: the species that do not move (nullptr: the opaque ones)
 KB_HD inline double project_totals_(double* n, const double* target,
-                                    bool charge) {
+                                    bool charge, const bool* fixed = nullptr) {
   constexpr int NRMAX = NELEM + 1;
   const int NR = NELEM + (charge ? 1 : 0);
   for (int it = 0; it < 20; ++it) {
@@ -52,7 +53,7 @@ KB_HD inline double project_totals_(double* n, const double* target,
       for (int l = 0; l < NR; ++l) {
         double s = 0.0;
         for (int i = 0; i < NSPEC; ++i)
-          if (!species_opaque(i))
+          if (!(fixed != nullptr ? fixed[i] : species_opaque(i)))
             s += conserved_row_(k, i) * conserved_row_(l, i) * n[i];
         M[k][l] = s;
       }
@@ -99,7 +100,7 @@ KB_HD inline double project_totals_(double* n, const double* target,
     }
     bool clipped = false;
     for (int i = 0; i < NSPEC; ++i) {
-      if (species_opaque(i)) continue;
+      if (fixed != nullptr ? fixed[i] : species_opaque(i)) continue;
       double d = 0.0;
       for (int k = 0; k < NR; ++k) d += conserved_row_(k, i) * lam[k];
       n[i] += n[i] * d;
@@ -142,4 +143,58 @@ KB_HD inline void conserve_cell(const double* n0, double* n, int mode) {
     for (int i = 0; i < NSPEC; ++i) target[k] += conserved_row_(k, i) * n0[i];
   }
   project_totals_(n, target, true);
+}
+
+// consistent advection (the reference's conserve_to_n_ / conserve_to_x_,
+// solve_cell.hpp:1504-1560; legacy krome_conserveLin_x): the cell n moved
+// to the element totals ref[NELEM] and to zero net charge. Negatives are
+// clipped first; the elements by the projection without the charge row
+// (the ionization is kept); then the electrons from neutrality, n(e-) =
+// sum q n over the other species, or, when the electrons cannot do it
+// (anions dominate, or no free electrons), the charge too by the
+// projection. fixed species do not move. Returns 0, -112 when the totals
+// or neutrality cannot be reached (corrected as far as possible), or the
+// warning 2 when a species changed by more than 50 %.
+KB_HD inline int conserve_to_n(double* n, const double* ref,
+                               const bool* fixed) {
+  double n0[NSPEC];
+  for (int i = 0; i < NSPEC; ++i) {
+    if (!fixed[i] && n[i] < 0.0) n[i] = 0.0;
+    n0[i] = n[i];
+  }
+  double target[NELEM + 1];
+  for (int k = 0; k < NELEM; ++k) target[k] = ref[k];
+  target[NELEM] = 0.0;
+  project_totals_(n, target, false, fixed);
+  bool charge_done = false;
+  if (IDX_ELECTRON >= 0 && !fixed[IDX_ELECTRON]) {
+    double qi = 0.0;
+    for (int i = 0; i < NSPEC; ++i)
+      if (i != IDX_ELECTRON) qi += species_charge(i) * n[i];
+    if (qi >= 0.0) {
+      n[IDX_ELECTRON] = qi;
+      charge_done = true;
+    } else {
+      n[IDX_ELECTRON] = 0.0;
+    }
+  }
+  if (!charge_done) project_totals_(n, target, true, fixed);
+  if (totals_residual_(n, target, true) > 1e-12) return -112;
+  for (int i = 0; i < NSPEC; ++i)
+    if (n0[i] > 0.0 && std::fabs(n[i] - n0[i]) > 0.5 * n0[i]) return 2;
+  return 0;
+}
+// the same with mass fractions x and ref per gram: n = x / m per gram,
+// corrected, x = m n; a species without mass does not move
+KB_HD inline int conserve_to_x(double* x, const double* ref) {
+  bool fixed[NSPEC];
+  double n[NSPEC];
+  for (int i = 0; i < NSPEC; ++i) {
+    fixed[i] = species_opaque(i) || !(species_mass_g(i) > 0.0);
+    n[i] = species_mass_g(i) > 0.0 ? x[i] / species_mass_g(i) : 0.0;
+  }
+  const int f = conserve_to_n(n, ref, fixed);
+  for (int i = 0; i < NSPEC; ++i)
+    if (!fixed[i]) x[i] = species_mass_g(i) * n[i];
+  return f;
 }

@@ -1504,6 +1504,131 @@ KB_API int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
                             par_stride, extra, flags, summary, h);
 }
 
+// ---- host utilities of the reference's interface (krome.h:473-501, 539,
+// 645-652): element totals, consistent advection, n <-> x, metadata ----
+
+// tot[ncell][nelem] = sum_i (atoms of element e in species i) n_i
+// (query.hpp:153-158), or per gram from mass fractions (162-170)
+KB_API int krome_get_element_totals(int ncell, const double* n, double* tot) {
+  if (ncell < 0 || n == nullptr || tot == nullptr) return -1;
+  using namespace kbnet;
+  for (int c = 0; c < ncell; ++c) {
+    double* t = tot + (size_t)c * NELEM;
+    for (int e = 0; e < NELEM; ++e) t[e] = 0.0;
+    for (int i = 0; i < NSPEC; ++i)
+      for (int e = 0; e < NELEM; ++e)
+        t[e] += species_element(i, e) * n[(size_t)c * NSPEC + i];
+  }
+  return 0;
+}
+KB_API int krome_get_element_totals_x(int ncell, const double* x, double* tot) {
+  if (ncell < 0 || x == nullptr || tot == nullptr) return -1;
+  using namespace kbnet;
+  for (int c = 0; c < ncell; ++c) {
+    double* t = tot + (size_t)c * NELEM;
+    for (int e = 0; e < NELEM; ++e) t[e] = 0.0;
+    for (int i = 0; i < NSPEC; ++i) {
+      if (!(species_mass_g(i) > 0.0)) continue;
+      const double ni = x[(size_t)c * NSPEC + i] / species_mass_g(i);
+      for (int e = 0; e < NELEM; ++e) t[e] += species_element(i, e) * ni;
+    }
+  }
+  return 0;
+}
+
+// consistent advection (krome.h:478-497, solve_cells.hpp:215-243): each cell
+// moved to its reference element totals ref (ref_stride 0: one row for all,
+// nelem: a row per cell) and to zero charge; par (the freeze directives'
+// rows: none in these networks) may be NULL; flags[ncell] (may be NULL) 0,
+// -112 (unreachable) or the warning 2. Returns the lowest failing cell's
+// flag (negative), else 0.
+namespace {
+int conserve_cells_host(int ncell, double* v, const double* ref,
+                        int ref_stride, const double* par, int par_stride,
+                        int* flags, bool x) {
+  using namespace kbnet;
+  (void)par;
+  if (ncell < 0 || v == nullptr || ref == nullptr || ref_stride < 0
+      || par_stride < 0)
+    return -1;
+  if (ref_stride != 0 && ref_stride != NELEM) return -1;
+  int ret = 0;
+  for (int c = 0; c < ncell; ++c) {
+    double* vc = v + (size_t)c * NSPEC;
+    const double* rc = ref + (size_t)c * ref_stride;
+    int f;
+    if (x) {
+      f = conserve_to_x(vc, rc);
+    } else {
+      bool fixed[NSPEC];
+      for (int i = 0; i < NSPEC; ++i) fixed[i] = species_opaque(i) != 0;
+      f = conserve_to_n(vc, rc, fixed);
+    }
+    if (flags != nullptr) flags[c] = f;
+    if (ret == 0 && f < 0) ret = f;
+  }
+  return ret;
+}
+}  // namespace
+KB_API int krome_conserve_cells(int ncell, double* n, const double* ref,
+                                int ref_stride, const double* par,
+                                int par_stride, int* flags) {
+  return conserve_cells_host(ncell, n, ref, ref_stride, par, par_stride,
+                             flags, false);
+}
+KB_API int krome_conserve_cells_x(int ncell, double* x, const double* ref,
+                                  int ref_stride, const double* par,
+                                  int par_stride, int* flags) {
+  return conserve_cells_host(ncell, x, ref, ref_stride, par, par_stride,
+                             flags, true);
+}
+
+// x = m n / rho and n = rho x / m (query.hpp:443-449)
+KB_API int krome_n2x(int ncell, const double* n, const double* rho, double* x) {
+  if (ncell < 0 || n == nullptr || rho == nullptr || x == nullptr) return -1;
+  for (int c = 0; c < ncell; ++c)
+    for (int i = 0; i < kbnet::NSPEC; ++i)
+      x[(size_t)c * kbnet::NSPEC + i] =
+          kbnet::species_mass_g(i) * n[(size_t)c * kbnet::NSPEC + i] / rho[c];
+  return 0;
+}
+KB_API int krome_x2n(int ncell, const double* x, const double* rho, double* n) {
+  if (ncell < 0 || x == nullptr || rho == nullptr || n == nullptr) return -1;
+  for (int c = 0; c < ncell; ++c)
+    x_to_n(x + (size_t)c * kbnet::NSPEC, rho[c], n + (size_t)c * kbnet::NSPEC);
+  return 0;
+}
+
+KB_API double krome_species_mass(int i) {
+  return (i >= 0 && i < kbnet::NSPEC) ? kbnet::species_mass_g(i) : std::nan("");
+}
+KB_API int krome_species_charge(int i) {
+  return (i >= 0 && i < kbnet::NSPEC) ? kbnet::species_charge(i) : 0;
+}
+KB_API int krome_nelem(void) { return kbnet::NELEM; }
+KB_API const char* krome_element_name(int e) {
+  return (e >= 0 && e < kbnet::NELEM) ? kbnet::element_names[e] : nullptr;
+}
+KB_API int krome_species_natoms(int i, int e) {
+  if (i < 0 || i >= kbnet::NSPEC || e < 0 || e >= kbnet::NELEM) return -1;
+  return kbnet::species_element(i, e);
+}
+
+// the device backend's set-up calls (krome.h:187-201): this library needs
+// none (the CUDA runtime initializes itself); 0 with a usable device, -104
+// without one; _id makes device_id current for the calling thread
+KB_API int krome_device_initialize(void) {
+  int nd = 0;
+  return cudaGetDeviceCount(&nd) == cudaSuccess && nd > 0 ? 0 : -104;
+}
+KB_API int krome_device_initialize_id(int device_id) {
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd <= 0) return -104;
+  if (device_id < 0) return 0;
+  return cudaSetDevice(device_id) == cudaSuccess ? 0 : -1;
+}
+KB_API int krome_device_finalize(void) { return krome_device_initialize(); }
+
 namespace {
 // the rate coefficients of each cell at its rate temperature clamp(Tgas,
 // Tcmb, 1e9) (the reference's krome_get_rates query, krome.h:387-389)

@@ -214,6 +214,9 @@ class Emitter:
                     if not sp[x]["opaque"] else 0)
                 for x in self.species for e in elems] or ["0"]
         w("constexpr int NELEM = %d;" % len(elems))
+        w("inline const char* const element_names[%d] = {%s};"
+          % (max(len(elems), 1),
+             ", ".join('"%s"' % e for e in elems) if elems else '""'))
         self.meta_elements = (elems, [[(sp[x]["composition"] or {}).get(e, 0)
                                        if not sp[x]["opaque"] else 0
                                        for e in elems] for x in self.species])

@@ -38,6 +38,7 @@ constexpr int IDX_ELECTRON = 8;
 
 inline const char* const species_names[NSPEC] = {"H", "H+", "H-", "H2", "H2+", "He", "He+", "He++", "e-"};
 constexpr int NELEM = 2;
+inline const char* const element_names[2] = {"H", "He"};
 KB_HD inline double species_mass_g(int i) {
   constexpr double t_[NSPEC] = {1.6738233791328e-24, 1.6729124407627538e-24, 1.6747343175028463e-24, 3.3476467582656e-24, 3.346735819895553e-24, 6.64647366797316e-24, 6.645562729603113e-24, 6.644651791233067e-24, 9.10938370046373e-28};
   return t_[i];

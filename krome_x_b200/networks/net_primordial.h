@@ -40,6 +40,7 @@ constexpr int IDX_ELECTRON = 11;
 
 inline const char* const species_names[NSPEC] = {"D", "D+", "H", "H+", "H-", "H2", "H2+", "HD", "He", "He+", "He++", "e-"};
 constexpr int NELEM = 3;
+inline const char* const element_names[3] = {"D", "H", "He"};
 KB_HD inline double species_mass_g(int i) {
   constexpr double t_[NSPEC] = {3.3443256801323995e-24, 3.343414741762353e-24, 1.6738233791328e-24, 1.6729124407627538e-24, 1.6747343175028463e-24, 3.3476467582656e-24, 3.346735819895553e-24, 5.0181490592651994e-24, 6.64647366797316e-24, 6.645562729603113e-24, 6.644651791233067e-24, 9.10938370046373e-28};
   return t_[i];
