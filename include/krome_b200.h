@@ -70,6 +70,15 @@ krome_opts* krome_opts_new(void);
 void krome_opts_free(krome_opts* h);
 int krome_opts_set(krome_opts* h, const char* key, double value);
 int krome_opts_get(const krome_opts* h, const char* key, double* value);
+/* krome.h:175-185: per-species tolerances atol[NSPEC] / rtol[NSPEC] (a
+ * negative entry: the scalar atol_n / rtol; NULL: the scalar for every
+ * species); set rejects NaN and a zero atol with -1; get writes the
+ * tolerance each species gets. Networks of up to 64 species (the large
+ * networks' solve returns -104 with them set). */
+int krome_opts_set_atol_species(krome_opts* h, const double* atol);
+int krome_opts_set_rtol_species(krome_opts* h, const double* rtol);
+int krome_opts_get_atol_species(const krome_opts* h, double* atol);
+int krome_opts_get_rtol_species(const krome_opts* h, double* rtol);
 
 /* ---- the solve (reference krome.h:291-294, krome.cpp:396-438) ----
  * Host arrays, updated in place; extra (the reference's krome_cells of

@@ -343,6 +343,15 @@ struct Machine {
   }
 
   __device__ KBL_HELPER int ewt_set(const double* ycur, double* w) {
+    if (o.rtol_v) {  // per-species rtol: KROME's per-slot weights
+      KBL_LOOP for (int i = 0; i < N; i++) {
+        const double rt = i < NSPEC ? o.rtol_sp[i < KB_NSP_TOL ? i : 0] : o.rtol;
+        const double d = fma(rt, fabs(ycur[i]), s.atol[i]);
+        if (!(d > 0.0)) return -1;
+        w[i] = 1.0 / d;
+      }
+      return 0;
+    }
     KBL_LOOP for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
     KBL_LOOP for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
     if (s.atolmin0) {

@@ -85,6 +85,9 @@ enum : int {
   ST_RESTARTS, ST_NLU64, NSTAT
 };
 
+// per-species tolerances are carried for networks of up to 64 species
+constexpr int KB_NSP_TOL = kbnet::NSPEC <= 64 ? kbnet::NSPEC : 1;
+
 // the options of one solve (the krome_opts keys the hot path reads)
 struct SolveOpts {
   int evolve_T;
@@ -97,6 +100,12 @@ struct SolveOpts {
                    // report TOO_MUCH_WORK without integrating (0: off)
   int lu32;        // the Newton matrix factored in FP32 (lane layout only)
   int conserve;    // post-solve conservation mode (kb_conserve.h), 0 none
+  // the species' absolute tolerances (atol_n where the caller set none) and,
+  // when some species' relative tolerance differs from rtol (rtol_v = 1),
+  // the relative ones (krome_opts_set_atol_species / rtol_species)
+  double atol_sp[KB_NSP_TOL];
+  double rtol_sp[KB_NSP_TOL];
+  int rtol_v;
 };
 
 __device__ __forceinline__ double smax_(double a, double b) { return a > b ? a : b; }
@@ -222,6 +231,14 @@ struct Cell {
   }
 
   __device__ int ewt_set(double ycur, double& w) {
+    if (o->rtol_v) {  // per-species rtol: KROME's per-slot weights
+      const double rt = lane < NSPEC ? o->rtol_sp[lane < KB_NSP_TOL ? lane : 0]
+                                     : o->rtol;
+      const double d = act() ? fma(rt, fabs(ycur), atol) : 1.0;
+      if (__any_sync(FULL, !(d > 0.0))) return -1;
+      w = 1.0 / d;
+      return 0;
+    }
     double wv = act() ? (o->rtol * fabs(ycur)) + atol : 1.0;
     if (atolmin0) {
       const double mn = -warp_max(act() ? -wv : -1e300);
@@ -1053,10 +1070,10 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
   double y0 = 0.0;
   if (lane < NSPEC) y0 = n[lane];
   if (EVT && lane == N - 1) y0 = T0;
-  c.atol = (lane < NSPEC) ? so.atol_n : so.atol_T;
+  c.atol = (lane < NSPEC) ? so.atol_sp[lane < KB_NSP_TOL ? lane : 0] : so.atol_T;
   c.mxstep = so.max_steps == 0 ? 500
              : (so.max_steps < 0 ? KB_MAX_STEPS_CAP : so.max_steps);
-  c.atolmin0 = (so.atol_n == 0.0) || (EVT && so.atol_T == 0.0);
+  c.atolmin0 = -warp_max(lane < N ? -c.atol : -1e300) == 0.0;
   long tot[NSTAT];
   for (int i = 0; i < NSTAT; ++i) tot[i] = 0;
   double yv = y0;

@@ -178,8 +178,12 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   double y0[N];
   KB_UNROLL for (int i = 0; i < NSPEC; ++i) y0[i] = n[(long)c * NSPEC + i];
   if (EVT) y0[N - 1] = T[c];
-  KB_UNROLL for (int i = 0; i < N; ++i) s.atol[i] = i < NSPEC ? so.atol_n : so.atol_T;
-  s.atolmin0 = (so.atol_n == 0.0) || (EVT && so.atol_T == 0.0);
+  double amin = 1e300;
+  KB_UNROLL for (int i = 0; i < N; ++i) {
+    s.atol[i] = i < NSPEC ? so.atol_sp[i < kbw::KB_NSP_TOL ? i : 0] : so.atol_T;
+    amin = fmin(amin, s.atol[i]);
+  }
+  s.atolmin0 = amin == 0.0;  // CVodeSVtolerances: N_VMin(abstol) == 0
   s.mxstep = so.max_steps == 0 ? 500
              : (so.max_steps < 0 ? KB_MAX_STEPS_CAP : so.max_steps);
   m.reinit(0.0, y0, 0.0);
@@ -579,6 +583,9 @@ struct krome_opts {
   int fail_every = 0;      // fault injection (tests)
   int lu32 = 0;            // Newton-matrix LU in FP32, FP64 after a Newton
                            // failure (lane layout)
+  // per-species tolerances (krome_opts_set_atol_species / rtol_species):
+  // empty, or NSPEC entries (negative: the scalar)
+  std::vector<double> atol_sp, rtol_sp;
 };
 
 namespace {
@@ -627,6 +634,16 @@ SolveOpts to_solve_opts(const krome_opts& h) {
   so.fail_every = h.fail_every;
   so.lu32 = h.lu32;
   so.conserve = h.conserve;
+  // a species' tolerance: its entry, or the scalar (solve_cell.hpp:868-879)
+  auto tol = [](const std::vector<double>& v, int i, double s) {
+    return !v.empty() && !(v[i] < 0.0) ? v[i] : s;
+  };
+  so.rtol_v = 0;
+  for (int i = 0; i < kbw::KB_NSP_TOL; ++i) {
+    so.atol_sp[i] = tol(h.atol_sp, i, h.atol_n);
+    so.rtol_sp[i] = tol(h.rtol_sp, i, h.rtol);
+    if (so.rtol_sp[i] != h.rtol) so.rtol_v = 1;
+  }
   return so;
 }
 
@@ -934,6 +951,45 @@ KB_API int krome_opts_set(krome_opts* h, const char* key, double v) {
   return 0;
 }
 
+// per-species tolerances (reference krome.h:175-185, krome.cpp:494-538):
+// v[NSPEC] copied into the handle (a negative entry: the scalar; NULL: the
+// scalar for every species); NaN, and a zero atol, are rejected. get writes
+// the tolerance each species gets.
+namespace {
+int set_species_tol(krome_opts* h, const double* v, bool atol) {
+  if (h == nullptr) return -1;
+  std::vector<double>& buf = atol ? h->atol_sp : h->rtol_sp;
+  if (v == nullptr) {
+    buf.clear();
+    return 0;
+  }
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    if (std::isnan(v[i]) || (atol && v[i] == 0.0)) return -1;
+  buf.assign(v, v + kbnet::NSPEC);
+  return 0;
+}
+int get_species_tol(const krome_opts* h, double* v, bool atol) {
+  if (h == nullptr || v == nullptr) return -1;
+  const std::vector<double>& buf = atol ? h->atol_sp : h->rtol_sp;
+  const double s = atol ? h->atol_n : h->rtol;
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    v[i] = !buf.empty() && !(buf[i] < 0.0) ? buf[i] : s;
+  return 0;
+}
+}  // namespace
+KB_API int krome_opts_set_atol_species(krome_opts* h, const double* atol) {
+  return set_species_tol(h, atol, true);
+}
+KB_API int krome_opts_set_rtol_species(krome_opts* h, const double* rtol) {
+  return set_species_tol(h, rtol, false);
+}
+KB_API int krome_opts_get_atol_species(const krome_opts* h, double* atol) {
+  return get_species_tol(h, atol, true);
+}
+KB_API int krome_opts_get_rtol_species(const krome_opts* h, double* rtol) {
+  return get_species_tol(h, rtol, false);
+}
+
 KB_API int krome_opts_get(const krome_opts* hc, const char* key, double* v) {
   if (hc == nullptr || key == nullptr || v == nullptr) return -1;
   auto* h = const_cast<krome_opts*>(hc);
@@ -966,8 +1022,9 @@ namespace {
 int unsupported(const krome_opts& h) {
 #ifdef KB_LARGE_NETWORK
   // the large networks: the sparse LU (linsol auto or sparse), fixed Tgas,
-  // FP64
+  // FP64, the scalar tolerances
   if (h.linsol == 1 || h.linsol == 2) return -104;
+  if (!h.atol_sp.empty() || !h.rtol_sp.empty()) return -104;
   if (h.evolve_T != 0 || h.lu32 != 0) return -104;
 #else
   if (h.linsol == 2 || h.linsol == 3) return -104;

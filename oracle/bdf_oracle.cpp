@@ -354,6 +354,7 @@ struct Stats {
 struct BdfOpts {
   double rtol = 1e-4;
   const double* atol = nullptr;
+  const double* rtol_v = nullptr;  // per-slot rtol (KROME's ewt_cb_), or null
   long max_steps = 500;
   int max_err_fails = 7, max_conv_fails = 10;
   double h0 = 0.0;
@@ -550,8 +551,17 @@ class Cvode {
     for (int i = 0; i < L_MAX; i++) tape->push_back(l[i]);
     tape->push_back((double)(tape->size() - start + 1));
   }
-  // cvEwtSetSV (bdf_cell.hpp:689-713)
+  // cvEwtSetSV, or KROME's per-slot weights with rtol_v (bdf_cell.hpp:
+  // 689-713)
   int ewt_set(const double* ycur, double* weight) {
+    if (o.rtol_v != nullptr) {
+      for (int i = 0; i < N; i++) {
+        const double d = std::fma(o.rtol_v[i], std::fabs(ycur[i]), o.atol[i]);
+        if (!(d > 0.0)) return -1;
+        weight[i] = 1.0 / d;
+      }
+      return 0;
+    }
     for (int i = 0; i < N; i++) weight[i] = std::fabs(ycur[i]);
     for (int i = 0; i < N; i++) weight[i] = (o.rtol * weight[i]) + o.atol[i];
     if (atolmin0) {
@@ -1187,6 +1197,9 @@ struct oracle_opts {
   int clip_negative;
   int lu32;     // the Newton matrix factored in FP32 (FP64 fallback)
   int conserve;  // post-solve conservation mode (solve_cell.hpp:1458-1500)
+  // per-species tolerances [NSPEC] (negative entry: the scalar), or null
+  const double* atol_sp;
+  const double* rtol_sp;
 };
 
 // per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf,
@@ -1292,12 +1305,25 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
       c.kT_ok = false;
     }
   }
-  for (int i = 0; i < NSPEC; ++i) avec[i] = so->atol_n;
+  // the species' tolerances (solve_cell.hpp:2129-2139)
+  auto tol = [](const double* v, int i, double s) {
+    return v != nullptr && !(v[i] < 0.0) ? v[i] : s;
+  };
+  for (int i = 0; i < NSPEC; ++i) avec[i] = tol(so->atol_sp, i, so->atol_n);
   if (c.iT >= 0) avec[c.iT] = so->atol_T;
+  std::vector<double> rvec;
+  bool rvar = false;
+  for (int i = 0; i < NSPEC; ++i)
+    rvar = rvar || tol(so->rtol_sp, i, so->rtol) != so->rtol;
+  if (rvar) {
+    rvec.assign(N, so->rtol);
+    for (int i = 0; i < NSPEC; ++i) rvec[i] = tol(so->rtol_sp, i, so->rtol);
+  }
   const int jac = so->jac != 0 ? so->jac : (so->evolve_T ? 2 : 1);
   BdfOpts bo;
   bo.rtol = so->rtol;
   bo.atol = avec.data();
+  bo.rtol_v = rvar ? rvec.data() : nullptr;
   bo.max_steps = so->max_steps;
   bo.max_err_fails = so->max_err_fails;
   bo.max_conv_fails = so->max_conv_fails;

@@ -34,7 +34,9 @@ class _Opts(ctypes.Structure):
                 ("max_conv_fails", ctypes.c_int),
                 ("max_restarts", ctypes.c_int),
                 ("clip_negative", ctypes.c_int), ("lu32", ctypes.c_int),
-                ("conserve", ctypes.c_int)]
+                ("conserve", ctypes.c_int),
+                ("atol_sp", ctypes.POINTER(ctypes.c_double)),
+                ("rtol_sp", ctypes.POINTER(ctypes.c_double))]
 
 
 def _ptr(a, t=_D):
@@ -57,7 +59,8 @@ class Oracle:
     def solve(self, n, T, dt, par, evolve_T=1, jac=0, rtol=1e-6, atol_n=1e-20,
               atol_T=1e-6, max_steps=100000, max_err_fails=7,
               max_conv_fails=10, max_restarts=5, clip_negative=1, lu32=0,
-              conserve=0, threads=None, **_):
+              conserve=0, atol_species=None, rtol_species=None, threads=None,
+              **_):
         n = np.array(n, dtype=float, order="C", copy=True)
         T = np.array(T, dtype=float, order="C", copy=True)
         dt = np.ascontiguousarray(dt, dtype=float)
@@ -69,6 +72,9 @@ class Oracle:
         o = _Opts(int(evolve_T), int(jac), rtol, atol_n, atol_T,
                   int(max_steps), max_err_fails, max_conv_fails,
                   max_restarts, int(clip_negative), int(lu32), int(conserve))
+        sp = [None if v is None else np.ascontiguousarray(v, dtype=float)
+              for v in (atol_species, rtol_species)]
+        o.atol_sp, o.rtol_sp = _ptr(sp[0]), _ptr(sp[1])
         nt = threads or os.cpu_count() or 1
         t0 = time.perf_counter()
         ret = self.lib.oracle_solve_cells(
@@ -159,6 +165,16 @@ class Reference:
         opts = dict(opts)
         opts.setdefault("error_report", 0)
         opts.setdefault("path", 1)
+        keep = []
+        for q in ("atol", "rtol"):  # per-species tolerances
+            v = opts.pop(q + "_species", None)
+            if v is not None:
+                v = np.ascontiguousarray(v, dtype=float)
+                keep.append(v)
+                f = getattr(self.lib, "krome_opts_set_%s_species" % q)
+                f.argtypes = [ctypes.c_void_p, _D]
+                if f(h, _ptr(v)) != 0:
+                    raise KeyError(q + "_species")
         for k, v in opts.items():
             if k in ("threads",):
                 continue
