@@ -121,9 +121,15 @@ struct LaneGeo {
   static constexpr int ROLE_BASE = EVT ? kbnet::NSPEC : 0;
   // per-warp shared memory: the Jacobians being assembled (column-major,
   // one N x N block per request of a pass) and the Tgas +/- h rhs
-  // vectors of the hybrid Jacobian
-  static constexpr int MAXJ = 32 / (JLANES_DQ < JLANES_AN ? JLANES_DQ : JLANES_AN);
-  static constexpr int SMEM_DOUBLES = MAXJ * (N * N + 2 * N);
+  // vectors of the hybrid Jacobian. Requests per pass: as many as the
+  // lanes hold, within 1,536 doubles a warp (the block's four warps stay
+  // under the 48 KB that needs no opt-in), at least one
+  static constexpr int JBLK = N * N + 2 * N;
+  static constexpr int MAXJ_LANES =
+      32 / (JLANES_DQ < JLANES_AN ? JLANES_DQ : JLANES_AN);
+  static constexpr int MAXJ_SMEM = 1536 / JBLK > 0 ? 1536 / JBLK : 1;
+  static constexpr int MAXJ = MAXJ_LANES < MAXJ_SMEM ? MAXJ_LANES : MAXJ_SMEM;
+  static constexpr int SMEM_DOUBLES = MAXJ * JBLK;
 };
 
 // the adjoint's forward solve (kb_lane_cells with REC): the rate factors
@@ -273,7 +279,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const bool dq = so.jac == 2;
   const int JL = dq ? LaneGeo<EVT>::JLANES_DQ : LaneGeo<EVT>::JLANES_AN;
-  const int per_pass = 32 / JL;
+  const int per_pass = 32 / JL < LaneGeo<EVT>::MAXJ ? 32 / JL : LaneGeo<EVT>::MAXJ;
   for (;;) {
     // a lane whose cell finished in the first sweep takes its next cell
     // and sweeps again in the same round
@@ -613,10 +619,22 @@ struct DevBuf {
 };
 DevBuf g_buf;
 
+// the rates that depend on the densities (their dk/dn terms are not in
+// the small networks' analytic Jacobian; the large networks' path takes no
+// jac option)
+#ifdef KB_LARGE_NETWORK
+constexpr int kRateNdep = 0;
+#else
+constexpr int kRateNdep = kbnet::KB_RATE_NDEP;
+#endif
+
 int resolved_jac(const krome_opts& h) {
   if (h.jac == 1) return 1;
   if (h.jac == 2) return 2;
-  return h.evolve_T ? 2 : 1;  // JAC_AUTO (solve_cell.hpp:2141-2142)
+  // JAC_AUTO (solve_cell.hpp:2141-2142); the difference quotients also
+  // where rates depend on the densities (the analytic Jacobian here has no
+  // dk/dn terms: unsupported() refuses it there)
+  return (h.evolve_T || kRateNdep > 0) ? 2 : 1;
 }
 
 SolveOpts to_solve_opts(const krome_opts& h) {
@@ -1028,6 +1046,7 @@ int unsupported(const krome_opts& h) {
   if (h.evolve_T != 0 || h.lu32 != 0) return -104;
 #else
   if (h.linsol == 2 || h.linsol == 3) return -104;
+  if (h.jac == 1 && kRateNdep > 0) return -104;
   if (h.lu32 != 0 && h.layout != 1) return -104;
 #endif
   return 0;

@@ -54,6 +54,9 @@ NETWORKS = {
                         heating=["COMPRESS", "CHEM"],
                         h2_opacity="RIPAMONTI", gamma="EXACT"),
     "galaxy_ism": dict(network="galaxy_ism", cooling=[], heating=[]),
+    # one more of the reference's networks, default thermal options: the
+    # primordial gas with carbon and oxygen chemistry (27 species)
+    "primordialZ": dict(network="primordialZ", cooling=[], heating=[]),
     # config 3: the surface options of the reference's cloudSurface test are
     # required by Semenov.knet (its binding energies)
     "semenov": dict(options_toml="examples/tests/cloudSurface/options.toml",
@@ -186,6 +189,18 @@ class Emitter:
         w('constexpr const char* NETWORK_KEY = "%s";' % self.key)
         w("constexpr int NSPEC = %d;" % ns)
         w("constexpr int NREA = %d;" % nr)
+        # the rates that depend on the densities (directly, through ntot or
+        # Hnuclei, or through an extern function): the reference's analytic
+        # Jacobian adds their dk/dn terms (kromex/codegen.py:8462-8560),
+        # which jac_stoich below does not
+        ndep = 0
+        for rx in net.reactions:
+            if rx["rate"]["kind"] != "expr":
+                continue
+            deps = self.gen.rate_deps(rx["rate"]["ast"])
+            if deps is None or deps[0] or deps[1]:
+                ndep += 1
+        w("constexpr int KB_RATE_NDEP = %d;" % ndep)
         for i, s in enumerate(self.species):
             w("constexpr int IDX_%s = %d;" % (self.cid(s), i))
         for s in self.species:

@@ -12,6 +12,7 @@ constexpr const char* NETWORK_NAME = "galaxy_ism";
 constexpr const char* NETWORK_KEY = "galaxy_ism";
 constexpr int NSPEC = 9;
 constexpr int NREA = 46;
+constexpr int KB_RATE_NDEP = 3;
 constexpr int IDX_H = 0;
 constexpr int IDX_Hj = 1;
 constexpr int IDX_Hk = 2;

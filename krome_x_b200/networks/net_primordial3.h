@@ -12,6 +12,7 @@ constexpr const char* NETWORK_NAME = "primordial3";
 constexpr const char* NETWORK_KEY = "primordial3";
 constexpr int NSPEC = 9;
 constexpr int NREA = 27;
+constexpr int KB_RATE_NDEP = 2;
 constexpr int IDX_H = 0;
 constexpr int IDX_Hj = 1;
 constexpr int IDX_Hk = 2;

@@ -29,6 +29,13 @@ the network's code-point order, ``Tgas[ncell]``, ``dt[ncell]``,
   [10, 1e6] K, crate in [1e-17, 1e-16], G0 in [0.3, 3], d2g in
   [0.003, 0.03] (log-uniform, one decade around the typical values);
   H2 1e-6 n_H, H+ = e- = 1e-4 n_H, He 0.0775 n_H; dt = 3.15e11 s.
+* ``primordialZ``  (a further network, default thermal options, fixed
+  Tgas) n_H log-uniform in [1, 1e6], Tgas in [30, 3000] K, x_H2 in
+  [1e-6, 0.5], x_H+ in [1e-6, 1e-3], metallicity Z in [1e-3, 1] (all
+  log-uniform): C+ 1.4e-4 Z n_H, O 3.2e-4 Z n_H, He 0.0775 n_H, H = n_H -
+  2 n_H2 - n_H+ (floored at the trace level), electrons for neutrality,
+  trace species 1e-20 n_H; dt = 3.15e11 s; the difference-quotient
+  Jacobian (its rates depend on the densities).
 """
 import numpy as np
 
@@ -123,6 +130,32 @@ def galaxy_ism(ncell, info, seed=0):
     return n, T, dt, par
 
 
+def primordialZ(ncell, info, seed=0):
+    species = info["species"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1.0, 1e6, ncell)
+    T = loguniform(rng, 30.0, 3000.0, ncell)
+    xH2 = loguniform(rng, 1e-6, 0.5, ncell)
+    xHp = loguniform(rng, 1e-6, 1e-3, ncell)
+    Z = loguniform(rng, 1e-3, 1.0, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    n[:, ix["H2"]] = xH2 * nH
+    n[:, ix["H+"]] = xHp * nH
+    n[:, ix["H"]] = np.maximum(nH - 2.0 * n[:, ix["H2"]] - n[:, ix["H+"]],
+                               1e-20 * nH)
+    n[:, ix["He"]] = 0.0775 * nH
+    n[:, ix["C+"]] = 1.4e-4 * Z * nH
+    n[:, ix["O"]] = 3.2e-4 * Z * nH
+    q = np.asarray(info["charge"], dtype=float)
+    e = ix["e-"]
+    n[:, e] = 0.0
+    n[:, e] = n @ q
+    par = _default_rows(ncell, info)
+    dt = np.full(ncell, 3.15e11)
+    return n, T, dt, par
+
+
 SEMENOV_INITIAL = (("He", 9e-2), ("H2", 0.5), ("C+", 1.2e-4), ("N", 7.6e-5),
                    ("O", 2.56e-4), ("S+", 8e-8), ("Si+", 8e-9), ("Fe+", 3e-9),
                    ("Na+", 2e-9), ("Mg+", 7e-9), ("P+", 2e-10), ("Cl+", 1e-9))
@@ -167,7 +200,8 @@ def hydro_step_info(n, par, info):
 
 
 GENERATORS = {"primordial": primordial, "primordial3": primordial3,
-              "galaxy_ism": galaxy_ism, "semenov": semenov}
+              "galaxy_ism": galaxy_ism, "semenov": semenov,
+              "primordialZ": primordialZ}
 
 # the solve options of each workload (krome_opts keys)
 OPTIONS = {
@@ -177,6 +211,8 @@ OPTIONS = {
                         atol_n=1e-20, atol_T=1e-6),
     "galaxy_ism": dict(evolve_T=1, jac=0, linsol=0, rtol=1e-6,
                        atol_n=1e-20, atol_T=1e-6),
+    "primordialZ": dict(evolve_T=0, jac=2, linsol=0, rtol=1e-6,
+                        atol_n=1e-20, atol_T=1e-6),
     "semenov": dict(evolve_T=0, jac=0, linsol=3, rtol=1e-6, atol_n=1e-20,
                     atol_T=1e-6, max_steps=1000000),
 }

@@ -1319,7 +1319,17 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
     rvec.assign(N, so->rtol);
     for (int i = 0; i < NSPEC; ++i) rvec[i] = tol(so->rtol_sp, i, so->rtol);
   }
-  const int jac = so->jac != 0 ? so->jac : (so->evolve_T ? 2 : 1);
+  // JAC_AUTO (solve_cell.hpp:2141-2142), the difference quotients also
+  // where rates depend on the densities: this analytic Jacobian has no
+  // dk/dn terms, so it is refused there (-104) like the library does
+#ifdef KB_LARGE_NETWORK
+  constexpr int rate_ndep = 0;
+#else
+  constexpr int rate_ndep = KB_RATE_NDEP;
+#endif
+  const int jac = so->jac != 0 ? so->jac
+                : ((so->evolve_T || rate_ndep > 0) ? 2 : 1);
+  if (jac == 1 && rate_ndep > 0) return -104;
   BdfOpts bo;
   bo.rtol = so->rtol;
   bo.atol = avec.data();

@@ -17,6 +17,7 @@ Network configurations (reference ``kromex.Preprocessor`` options):
 * ``semenov``      examples/tests/cloudSurface/options.toml (the surface
   options are mandatory for Semenov.knet)                       (config 3)
 * ``galaxy_ism``   networks/galaxy_ism.knet, default flags      (config 4)
+* ``primordialZ``  networks/primordialZ.knet, default flags
 
 Two libraries per network: ``libkrome_<net>.so`` with the generated
 projects' production flags (``-O3 -std=c++17 -ffp-contract=fast
@@ -56,8 +57,8 @@ def _configure(key):
         kp.thermal.heating = ["COMPRESS", "CHEM"]
         kp.thermal.h2_opacity = "RIPAMONTI"
         kp.thermal.gamma = "EXACT"
-    elif key == "galaxy_ism":
-        kp = Preprocessor(network="galaxy_ism")
+    elif key in ("galaxy_ism", "primordialZ"):
+        kp = Preprocessor(network=key)
     elif key == "semenov":
         kp = Preprocessor.from_file(
             str(REF / "examples/tests/cloudSurface/options.toml"))
@@ -93,7 +94,8 @@ def main(argv):
     sys.path.insert(0, str(REF))
     sys.path.insert(0, str(REF / "kromex"))
     OUT.mkdir(parents=True, exist_ok=True)
-    keys = argv or ["primordial", "primordial3", "galaxy_ism", "semenov"]
+    keys = argv or ["primordial", "primordial3", "galaxy_ism", "primordialZ",
+                    "semenov"]
     for k in keys:
         build(k)
 
