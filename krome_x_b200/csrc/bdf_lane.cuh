@@ -704,7 +704,7 @@ struct Machine {
     //      cvNlsConvTest (bdf_cell.hpp:1035-1048) ----
     if (s.ph == PH_NEWTON) {
       s.niters++;
-      const bool inv = (o.jac == 2) && IDX_ELECTRON >= 0;
+      const bool inv = (o.jac == 2) && IDX_ELECTRON >= 0 && KB_NFREEZE == 0;
       const double cg = inv ? inv_dot_(s.delta) : 0.0;
       scale_<N>(-1.0, s.delta, s.delta);
       if (s.fact32) getrs_<N, float>(s.A32, s.piv, s.delta);

@@ -595,7 +595,7 @@ struct Cell {
     bool jbad = false;
     long niters = 0, nconvfails = 0;
     int retval;
-    const bool inv = (o->jac == 2) && IDX_ELECTRON >= 0;
+    const bool inv = (o->jac == 2) && IDX_ELECTRON >= 0 && KB_NFREEZE == 0;
     for (;;) {
       int curiter = 0;
       retval = residual_();
@@ -1065,6 +1065,9 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
   c.ncfn_ = 0;
   params_from_row(prow, c.p);
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
+#if KB_NFREEZE > 0
+  if (freeze_active(c.p)) return -104;  // frozen rows are not built
+#endif
   const double T0 = *Tg;
   c.Tfix = T0;
   double y0 = 0.0;

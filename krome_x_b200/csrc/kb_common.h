@@ -22,6 +22,9 @@
 namespace kbc {
 constexpr double boltzmann_eV = 8.617333262145179e-05;
 constexpr double boltzmann_erg = 1.380649e-16;
+constexpr double planck_erg = 6.62607015e-27;
+constexpr double hc_k = 1.4387768775039336;  // cm K: E/k [K] = hc_k E [cm^-1]
+constexpr double e_mass = 9.1093837015e-28;
 constexpr double planck_eV = 4.135667696923859e-15;
 constexpr double gravity = 6.6743e-08;
 constexpr double p_mass = 1.67262192369e-24;

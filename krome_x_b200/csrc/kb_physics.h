@@ -16,6 +16,8 @@
 //                      (dust_rates.hpp:37-66)
 //   H2_solomonLW       Solomon-process H2 photodissociation
 //                      (h2_shielding.hpp:84-93)
+//   recfast_*          RECFAST 1.5.2 H and He I recombination and CMB
+//                      photoionization (special_rates.hpp:106-288)
 //
 // Included inside the network namespace after the generated indices; the
 // KB_HAS_<species> macros select the terms a network has.
@@ -453,5 +455,174 @@ KB_HD inline double H2_solomonLW(double flux_eV, double Tgas, const double* n,
                                  const Params& p) {
   (void)Tgas; (void)n; (void)p;
   return 1.38e9 * flux_eV * kbc::eV_to_erg;
+}
+#endif
+
+#if defined(KB_EXTERN_recfast_H_rec) || defined(KB_EXTERN_recfast_H_ion) \
+    || defined(KB_EXTERN_recfast_He_rec) || defined(KB_EXTERN_recfast_He_ion)
+// Cosmological recombination of H and He I after RECFAST 1.5.2 (Seager,
+// Sasselov & Scott 1999, 2000; Wong, Moss & Scott 2008), as the reference's
+// runtime states it (special_rates.hpp:106-224): each net RECFAST rate
+// C (n_e n_X+ alpha - n_X beta e^(-E/kT)) split into a recombination
+// coefficient C alpha and a CMB photoionization rate C beta e^(-E/kT).
+// The escape factors C use H(z) = hubble0 (1 + z) sqrt(1 + omega0 z).
+// RECFAST's atomic data in cgs (wavenumbers in cm^-1, rates in s^-1,
+// cross sections in cm^2):
+namespace rf {
+constexpr double kH_ion = 1.096787737e5, kH_alpha = 8.225916453e4;
+constexpr double kHe1_ion = 1.98310772e5, kHe_2s = 1.66277434e5;
+constexpr double kHe_2p = 1.71134891e5, kHe_2Pt = 1.690871466e5;
+constexpr double kHe_2St = 1.5985597526e5, kHe2St_ion = 3.8454693845e4;
+constexpr double two_photon_H = 8.2245809, two_photon_He = 51.3;
+constexpr double A2P_singlet = 1.798287e9, A2P_triplet = 177.58;
+constexpr double sigma_2Ps = 1.436289e-18, sigma_2Pt = 1.484872e-18;
+constexpr double mass_ratio_He = 3.9715;
+constexpr double fudge_H = 1.125, fudge_He = 0.86;
+
+struct Rates {
+  double alpha, beta, C;
+};
+struct Common {
+  double T, z, Hz, hck, crT15;
+};
+
+KB_HD inline Common common(double Tgas, const Params& p) {
+  Common c;
+  c.T = Tgas;
+  c.z = p.zredshift;
+  c.Hz = p.hubble0 * (1.0 + c.z) * std::sqrt(1.0 + p.omega0 * c.z);
+  c.hck = kbc::hc_k;
+  // (2 pi m_e k T / h^2)^(3/2)
+  const double cr = 2.0 * kbc::pi * kbc::e_mass * kbc::boltzmann_erg
+      / (kbc::planck_erg * kbc::planck_erg);
+  c.crT15 = std::pow(cr * c.T, 1.5);
+  return c;
+}
+
+// H: case-B alpha of Pequignot, Petitjean & Boisson, the Peebles factor
+// with the fudge and the double-Gaussian correction of K
+KB_HD inline Rates hydrogen(const Common& c, double nH0) {
+  Rates r;
+  const double t4 = c.T * 1e-4;
+  r.alpha = 1e-13 * 4.309 * std::pow(t4, -0.6166)
+      / (1.0 + 0.6703 * std::pow(t4, 0.53));
+  const double up = r.alpha * c.crT15
+      * std::exp(-c.hck * (kH_ion - kH_alpha) / c.T);
+  r.beta = up * std::exp(-c.hck * kH_alpha / c.T);
+  const double lz = std::log(1.0 + c.z);
+  const double g1 = (lz - 7.28) / 0.18, g2 = (lz - 6.73) / 0.33;
+  const double K = 1.0 / (kH_alpha * kH_alpha * kH_alpha)
+      / (8.0 * kbc::pi * c.Hz)
+      * (1.0 - 0.14 * std::exp(-g1 * g1) + 0.079 * std::exp(-g2 * g2));
+  const double KL = K * two_photon_H * nH0;
+  r.C = fudge_H * (1.0 + KL) / (1.0 + KL + fudge_H * K * up * nH0);
+  return r;
+}
+
+// the Sobolev continuum-opacity term of a He I 2P line (Kholupenko,
+// Ivanchik & Varshalovich 2007): A / (1 + a g^b), 0 without neutral H
+KB_HD inline double he_continuum(const Common& c, double nH0, double nHe0,
+                                 double k_line, double A, double sigma,
+                                 double a, double b) {
+  if (!(nH0 > 0.0)) return 0.0;
+  const double mH = kbc::p_mass + kbc::e_mass;
+  const double doppler = kbc::clight * k_line
+      * std::sqrt(2.0 * kbc::boltzmann_erg * c.T
+                  / (mH * mass_ratio_He * kbc::clight * kbc::clight));
+  const double g = 3.0 * A * nHe0 / nH0
+      / (std::sqrt(kbc::pi) * sigma * 8.0 * kbc::pi * doppler * k_line * k_line);
+  return A / (1.0 + a * std::pow(g, b));
+}
+
+// (1 - e^-tau) / tau, 1 for an optically thin line
+KB_HD inline double escape(double tau) {
+  return tau > 1e-8 ? -std::expm1(-tau) / tau : 1.0;
+}
+
+// the He I recombination fits (square-root terms shared by both)
+KB_HD inline double he_alpha(double s0, double s1, double lg, double e) {
+  return std::pow(10.0, lg) / (s0 * std::pow(1.0 + s0, 1.0 - e))
+      / std::pow(1.0 + s1, 1.0 + e);
+}
+
+// He I singlet: the Sobolev escape of 2^1P - 1^1S with the H continuum
+KB_HD inline Rates helium_singlet(const Common& c, double nH0, double nHe0,
+                                  double s0, double s1) {
+  Rates r;
+  r.alpha = he_alpha(s0, s1, -10.744, 0.711);
+  const double up = 4.0 * r.alpha * c.crT15
+      * std::exp(-c.hck * (kHe1_ion - kHe_2s) / c.T);
+  r.beta = up * std::exp(-c.hck * kHe_2s / c.T);
+  const double boltz = std::exp(std::fmin(c.hck * (kHe_2p - kHe_2s) / c.T, 680.0));
+  const double tau = A2P_singlet / (kHe_2p * kHe_2p * kHe_2p)
+      / (8.0 * kbc::pi) * 3.0 * nHe0 / c.Hz;
+  const double cont = he_continuum(c, nH0, nHe0, kHe_2p, A2P_singlet,
+                                   sigma_2Ps, 0.36, fudge_He);
+  // K_He n_He0 = 1 / (3 (A p + A_cont)), finite as n_He0 -> 0
+  const double kn = 1.0 / (3.0 * (A2P_singlet * escape(tau) + cont));
+  r.C = (1.0 + kn * two_photon_He * boltz)
+      / (1.0 + kn * (two_photon_He + up) * boltz);
+  return r;
+}
+
+// He I triplets, C = 1 / (1 + up / cf) with the two Boltzmann factors
+// combined (each alone underflows at low T)
+KB_HD inline Rates helium_triplet(const Common& c, double nH0, double nHe0,
+                                  double s0, double s1) {
+  Rates r;
+  r.alpha = he_alpha(s0, s1, -10.306, 0.761);
+  const double up = r.alpha * std::exp(-c.hck * kHe2St_ion / c.T) * c.crT15
+      * (4.0 / 3.0);
+  r.beta = 3.0 * up * std::exp(-c.hck * kHe_2St / c.T);
+  const double tau = A2P_triplet * nHe0 * 3.0
+      / (8.0 * kbc::pi * c.Hz * kHe_2Pt * kHe_2Pt * kHe_2Pt);
+  const double cont = he_continuum(c, nH0, nHe0, kHe_2Pt, A2P_triplet,
+                                   sigma_2Pt, 0.66, 0.9) / 3.0;
+  const double ru = r.alpha * c.crT15 * (4.0 / 3.0)
+      / (A2P_triplet * escape(tau) + cont)
+      * std::exp(-c.hck * (kHe2St_ion - (kHe_2Pt - kHe_2St)) / c.T);
+  r.C = 1.0 / (1.0 + ru);
+  return r;
+}
+
+KB_HD inline void helium(double Tgas, double nH0, double nHe0,
+                         const Params& p, Rates& s, Rates& t) {
+  const Common c = common(Tgas, p);
+  const double s0 = std::sqrt(c.T / std::pow(10.0, 0.477121));
+  const double s1 = std::sqrt(c.T / std::pow(10.0, 5.114));
+  s = helium_singlet(c, nH0, nHe0, s0, s1);
+  t = helium_triplet(c, nH0, nHe0, s0, s1);
+}
+}  // namespace rf
+
+// H+ + e- -> H: C alpha_B [cm^3 s^-1] (nH0 the neutral H density)
+KB_HD inline double recfast_H_rec(double nH0, double Tgas, const double* n,
+                                  const Params& p) {
+  (void)n;
+  const rf::Rates r = rf::hydrogen(rf::common(Tgas, p), nH0);
+  return r.C * r.alpha;
+}
+// H -> H+ + e- by the CMB: C beta e^(-h nu_a / kT) [s^-1]
+KB_HD inline double recfast_H_ion(double nH0, double Tgas, const double* n,
+                                  const Params& p) {
+  (void)n;
+  const rf::Rates r = rf::hydrogen(rf::common(Tgas, p), nH0);
+  return r.C * r.beta;
+}
+// He+ + e- -> He: singlet + triplet C alpha [cm^3 s^-1]
+KB_HD inline double recfast_He_rec(double nHe0, double nH0, double Tgas,
+                                   const double* n, const Params& p) {
+  (void)n;
+  rf::Rates s, t;
+  rf::helium(Tgas, nH0, nHe0, p, s, t);
+  return s.C * s.alpha + t.C * t.alpha;
+}
+// He -> He+ + e- by the CMB: singlet + triplet [s^-1]
+KB_HD inline double recfast_He_ion(double nHe0, double nH0, double Tgas,
+                                   const double* n, const Params& p) {
+  (void)n;
+  rf::Rates s, t;
+  rf::helium(Tgas, nH0, nHe0, p, s, t);
+  return s.C * s.beta + t.C * t.beta;
 }
 #endif

@@ -27,6 +27,9 @@
 #include <vector>
 
 #include KB_NET_HEADER
+#ifndef KB_NFREEZE
+#define KB_NFREEZE 0  // a network header from before freeze directives
+#endif
 #include "bdf_warp.cuh"
 #include "bdf_lane.cuh"
 #include "adjoint.cuh"
@@ -170,6 +173,12 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
     if (flags != nullptr) flags[c] = kbw::FLAG_PARAM_UNSET;
     return false;
   }
+#if KB_NFREEZE > 0
+  if (freeze_active(s.p)) {  // frozen rows are not built: refused
+    if (flags != nullptr) flags[c] = -104;
+    return false;
+  }
+#endif
   if constexpr (REC) {
     s.tp = rio.tape + (long)c * rio.cap;
     s.tcap = rio.cap;

@@ -57,6 +57,9 @@ NETWORKS = {
     # one more of the reference's networks, default thermal options: the
     # primordial gas with carbon and oxygen chemistry (27 species)
     "primordialZ": dict(network="primordialZ", cooling=[], heating=[]),
+    # the early-universe chemistry (H, D, He, their ions and molecules; 16
+    # species) with its RECFAST recombination rates, default thermal options
+    "earlyUniverse": dict(network="earlyUniverse", cooling=[], heating=[]),
     # config 3: the surface options of the reference's cloudSurface test are
     # required by Semenov.knet (its binding energies)
     "semenov": dict(options_toml="examples/tests/cloudSurface/options.toml",
@@ -201,6 +204,12 @@ class Emitter:
             if deps is None or deps[0] or deps[1]:
                 ndep += 1
         w("constexpr int KB_RATE_NDEP = %d;" % ndep)
+        # species a freeze directive can hold (the reference turns its
+        # charge-invariant Newton correction off on such networks,
+        # solve_cell.hpp:1631-1642; the frozen rows themselves are not
+        # built here: a cell whose freeze holds is refused)
+        w("#define KB_NFREEZE %d"
+          % sum(len(f["species"]) for f in net.freeze))
         for i, s in enumerate(self.species):
             w("constexpr int IDX_%s = %d;" % (self.cid(s), i))
         for s in self.species:
@@ -335,6 +344,16 @@ class Emitter:
                 w("  if (p.%s != p.%s) return %d;" % (s, s, i))
         w("  return -1;")
         w("}")
+        if net.freeze:
+            # whether a freeze directive holds for this parameter row (its
+            # condition uses parameters only, fixed during a call)
+            w("KB_HD inline bool freeze_active(const Params& p) {")
+            w("  (void)p;")
+            for f in net.freeze:
+                cond = "true" if f["cond"] is None else self.gen.cexpr(f["cond"])
+                w("  if (%s) return true;  // knet line %d" % (cond, f["line"]))
+            w("  return false;")
+            w("}")
         self.pnames = pn
         self.meta = dict(
             network=net.name, key=self.key, species=list(self.species),

@@ -13,6 +13,7 @@ constexpr const char* NETWORK_KEY = "galaxy_ism";
 constexpr int NSPEC = 9;
 constexpr int NREA = 46;
 constexpr int KB_RATE_NDEP = 3;
+#define KB_NFREEZE 0
 constexpr int IDX_H = 0;
 constexpr int IDX_Hj = 1;
 constexpr int IDX_Hk = 2;

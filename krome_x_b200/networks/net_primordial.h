@@ -13,6 +13,7 @@ constexpr const char* NETWORK_KEY = "primordial";
 constexpr int NSPEC = 12;
 constexpr int NREA = 38;
 constexpr int KB_RATE_NDEP = 0;
+#define KB_NFREEZE 0
 constexpr int IDX_D = 0;
 constexpr int IDX_Dj = 1;
 constexpr int IDX_H = 2;

@@ -13,6 +13,7 @@ constexpr const char* NETWORK_KEY = "primordial3";
 constexpr int NSPEC = 9;
 constexpr int NREA = 27;
 constexpr int KB_RATE_NDEP = 2;
+#define KB_NFREEZE 0
 constexpr int IDX_H = 0;
 constexpr int IDX_Hj = 1;
 constexpr int IDX_Hk = 2;

@@ -13,6 +13,7 @@ constexpr const char* NETWORK_KEY = "primordialZ";
 constexpr int NSPEC = 27;
 constexpr int NREA = 74;
 constexpr int KB_RATE_NDEP = 43;
+#define KB_NFREEZE 0
 constexpr int IDX_C = 0;
 constexpr int IDX_Cj = 1;
 constexpr int IDX_CH = 2;

@@ -36,6 +36,15 @@ the network's code-point order, ``Tgas[ncell]``, ``dt[ncell]``,
   2 n_H2 - n_H+ (floored at the trace level), electrons for neutrality,
   trace species 1e-20 n_H; dt = 3.15e11 s; the difference-quotient
   Jacobian (its rates depend on the densities).
+* ``earlyUniverse`` (a further network, default thermal options, fixed
+  Tgas) the reference's early-universe driver's cosmology
+  (examples/tests/earlyUniverse/test.cpp: h = 0.704, Omega0 = 1,
+  Omega_b = 0.0456, Tcmb0 = 2.73 K) at redshift z log-uniform in
+  [20, 2000]: n = 0.0456 x 9.19e-6 (1+z)^3 cm^-3, Tgas = Trad = 2.73 (1+z),
+  ionized fraction x log-uniform in [1e-4, 1] for H and D (D/H = 4.3e-5 /
+  0.924), He neutral (He+ 1e-6 of He), electrons for neutrality, trace
+  species 1e-40 n; dt = a 1 % step in 1+z; the difference-quotient
+  Jacobian (its rates depend on the densities).
 """
 import numpy as np
 
@@ -156,6 +165,37 @@ def primordialZ(ncell, info, seed=0):
     return n, T, dt, par
 
 
+def earlyUniverse(ncell, info, seed=0):
+    species, param_names = info["species"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    hubble0 = 1e2 * 0.704 * 1e5 / 3.0856775814913673e24  # s^-1
+    z = loguniform(rng, 20.0, 2000.0, ncell)
+    a = 1.0 + z
+    dd = 0.0456 * 9.19e-6 * a ** 3
+    x = loguniform(rng, 1e-4, 1.0, ncell)
+    n = np.repeat((1e-40 * dd)[:, None], len(species), axis=1)
+    n[:, ix["H+"]] = 0.924 * dd * x
+    n[:, ix["H"]] = 0.924 * dd * (1.0 - x) + 1e-40 * dd
+    n[:, ix["D+"]] = 4.3e-5 * dd * x
+    n[:, ix["D"]] = 4.3e-5 * dd * (1.0 - x) + 1e-40 * dd
+    n[:, ix["He"]] = 0.076 * dd
+    n[:, ix["He+"]] = 0.076e-6 * dd
+    q = np.asarray(info["charge"], dtype=float)
+    e = ix["e-"]
+    n[:, e] = 0.0
+    n[:, e] = n @ q
+    T = 2.73 * a
+    par = _default_rows(ncell, info)
+    par[:, param_names.index("zredshift")] = z
+    par[:, param_names.index("Trad")] = T
+    par[:, param_names.index("Tcmb")] = 2.73
+    par[:, param_names.index("hubble0")] = hubble0
+    par[:, param_names.index("omega0")] = 1.0
+    dt = 0.01 * a / (hubble0 * a * a * np.sqrt(z + 1.0))
+    return n, T, dt, par
+
+
 SEMENOV_INITIAL = (("He", 9e-2), ("H2", 0.5), ("C+", 1.2e-4), ("N", 7.6e-5),
                    ("O", 2.56e-4), ("S+", 8e-8), ("Si+", 8e-9), ("Fe+", 3e-9),
                    ("Na+", 2e-9), ("Mg+", 7e-9), ("P+", 2e-10), ("Cl+", 1e-9))
@@ -201,7 +241,7 @@ def hydro_step_info(n, par, info):
 
 GENERATORS = {"primordial": primordial, "primordial3": primordial3,
               "galaxy_ism": galaxy_ism, "semenov": semenov,
-              "primordialZ": primordialZ}
+              "primordialZ": primordialZ, "earlyUniverse": earlyUniverse}
 
 # the solve options of each workload (krome_opts keys)
 OPTIONS = {
@@ -213,6 +253,8 @@ OPTIONS = {
                        atol_n=1e-20, atol_T=1e-6),
     "primordialZ": dict(evolve_T=0, jac=2, linsol=0, rtol=1e-6,
                         atol_n=1e-20, atol_T=1e-6),
+    "earlyUniverse": dict(evolve_T=0, jac=2, linsol=0, rtol=1e-6,
+                          atol_n=1e-20, atol_T=1e-6),
     "semenov": dict(evolve_T=0, jac=0, linsol=3, rtol=1e-6, atol_n=1e-20,
                     atol_T=1e-6, max_steps=1000000),
 }

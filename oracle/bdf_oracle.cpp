@@ -19,6 +19,9 @@
 #include <cstring>
 #include <vector>
 #include KB_NET_HEADER
+#ifndef KB_NFREEZE
+#define KB_NFREEZE 0  // a network header from before freeze directives
+#endif
 
 using namespace kbnet;
 
@@ -1288,6 +1291,9 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
   c.mult = mult;
   params_from_row(par, c.p);
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
+#if KB_NFREEZE > 0
+  if (freeze_active(c.p)) return -104;  // frozen rows are not built
+#endif
   c.Tfix = *Tgas;
   c.NEQ = NSPEC;
   if (so->evolve_T) c.iT = c.NEQ++;
@@ -1339,7 +1345,7 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
   bo.max_conv_fails = so->max_conv_fails;
   bo.dq_jac = jac == 2;
   bo.lu32 = so->lu32 != 0;
-  if (IDX_ELECTRON >= 0) {  // charge_newton_ (solve_cell.hpp:1631-1642)
+  if (IDX_ELECTRON >= 0 && KB_NFREEZE == 0) {  // charge_newton_ (solve_cell.hpp:1631-1642)
     bo.inv_row = IDX_ELECTRON;
     bo.inv_n = NSPEC;
   }

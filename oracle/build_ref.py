@@ -18,6 +18,7 @@ Network configurations (reference ``kromex.Preprocessor`` options):
   options are mandatory for Semenov.knet)                       (config 3)
 * ``galaxy_ism``   networks/galaxy_ism.knet, default flags      (config 4)
 * ``primordialZ``  networks/primordialZ.knet, default flags
+* ``earlyUniverse``  networks/earlyUniverse.knet, default flags
 
 Two libraries per network: ``libkrome_<net>.so`` with the generated
 projects' production flags (``-O3 -std=c++17 -ffp-contract=fast
@@ -57,7 +58,7 @@ def _configure(key):
         kp.thermal.heating = ["COMPRESS", "CHEM"]
         kp.thermal.h2_opacity = "RIPAMONTI"
         kp.thermal.gamma = "EXACT"
-    elif key in ("galaxy_ism", "primordialZ"):
+    elif key in ("galaxy_ism", "primordialZ", "earlyUniverse"):
         kp = Preprocessor(network=key)
     elif key == "semenov":
         kp = Preprocessor.from_file(
@@ -95,7 +96,7 @@ def main(argv):
     sys.path.insert(0, str(REF / "kromex"))
     OUT.mkdir(parents=True, exist_ok=True)
     keys = argv or ["primordial", "primordial3", "galaxy_ism", "primordialZ",
-                    "semenov"]
+                    "earlyUniverse", "semenov"]
     for k in keys:
         build(k)
 

@@ -1,4 +1,4 @@
-"""A further network through the emitter: primordialZ (the reference's
+"""Further networks through the emitter: primordialZ (the reference's
 networks/primordialZ.knet, default thermal options; 27 species, 74
 reactions, fixed Tgas), solved by the small-network kernels.
 
@@ -9,7 +9,15 @@ the reference's analytic Jacobian adds their dk/dn terms
 not, so such networks take the difference-quotient Jacobian (the default
 resolves to it; an explicit analytic one is refused with -104). With it the
 oracle equals the reference's build bit for bit, and the kernels match the
-oracle."""
+oracle.
+
+earlyUniverse (networks/earlyUniverse.knet, default thermal options, 16
+species, fixed Tgas) adds the RECFAST recombination rates (csrc/
+kb_physics.h) and a freeze directive: its e-, H and D species stop above
+z = 2243. As the reference does (solve_cell.hpp:1631-1642), a network with
+freezable species runs without the charge-invariant Newton correction; the
+frozen rows themselves are not built, so a cell whose freeze holds is
+refused (-104)."""
 import re
 
 import numpy as np
@@ -20,7 +28,8 @@ from krome_x_b200 import krome, netinfo, workloads
 from oracle import Oracle, reference_solve
 
 KEY = "primordialZ"
-SMALL = ("primordial", "primordial3", "galaxy_ism", KEY)
+SMALL = ("primordial", "primordial3", "galaxy_ism", KEY, "earlyUniverse")
+FURTHER = (KEY, "earlyUniverse")
 
 
 def _ndep(key):
@@ -38,14 +47,15 @@ def test_density_dependent_rates_match_the_reference_jacobian(key):
     assert (_ndep(key) > 0) == has_dk
 
 
-def test_oracle_equals_the_reference():
-    if not (ROOT / "oracle" / "_ref" / ("libkrome_%s_strict.so" % KEY)).exists():
+@pytest.mark.parametrize("key", FURTHER)
+def test_oracle_equals_the_reference(key):
+    if not (ROOT / "oracle" / "_ref" / ("libkrome_%s_strict.so" % key)).exists():
         pytest.skip("oracle/_ref not built here (oracle/build_ref.py)")
-    info = netinfo.load(KEY)
-    n, T, dt, par = workloads.GENERATORS[KEY](48, info, seed=61)
-    o = workloads.OPTIONS[KEY]
-    ref = reference_solve(KEY, n, T, dt, par, strict=True, **o)
-    out = Oracle(KEY).solve(n, T, dt, par, **o)
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](48, info, seed=61)
+    o = workloads.OPTIONS[key]
+    ref = reference_solve(key, n, T, dt, par, strict=True, **o)
+    out = Oracle(key).solve(n, T, dt, par, **o)
     assert (ref["flags"] == 0).all()
     np.testing.assert_array_equal(out["flags"], ref["flags"])
     np.testing.assert_array_equal(out["n"], ref["n"])
@@ -64,9 +74,29 @@ def test_oracle_refuses_the_analytic_jacobian_with_rate_terms():
     np.testing.assert_array_equal(a["n"], b["n"])
 
 
-def test_workload_is_physical():
-    info = netinfo.load(KEY)
-    n, T, dt, par = workloads.GENERATORS[KEY](256, info, seed=63)
+def _frozen_case(ncell, seed):
+    """earlyUniverse cells, every other one above the freeze redshift"""
+    key = "earlyUniverse"
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](ncell, info, seed=seed)
+    iz = info["params"].index("zredshift")
+    hot = np.arange(ncell) % 2 == 1
+    par[hot, iz] = 3000.0
+    return key, info, n, T, dt, par, hot
+
+
+def test_oracle_refuses_cells_whose_freeze_holds():
+    key, info, n, T, dt, par, hot = _frozen_case(8, 66)
+    out = Oracle(key).solve(n, T, dt, par, **workloads.OPTIONS[key])
+    assert (out["flags"][hot] == -104).all()
+    assert (out["flags"][~hot] == 0).all()
+    np.testing.assert_array_equal(out["n"][hot], n[hot])
+
+
+@pytest.mark.parametrize("key", FURTHER)
+def test_workload_is_physical(key):
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](256, info, seed=63)
     assert (n > 0).all()
     q = np.asarray(info["charge"], dtype=float)
     np.testing.assert_allclose(n @ q, 0.0, atol=1e-12 * n.sum(axis=1).max())
@@ -75,7 +105,7 @@ def test_workload_is_physical():
 # fixed-Tgas solves of the small networks: primordialZ's workload, and the
 # benchmark networks at fixed Tgas (primordial: the analytic Jacobian;
 # galaxy_ism: the difference quotients its density-dependent rates take)
-FIXED_T = [(KEY, {}), ("primordial", {"evolve_T": 0}),
+FIXED_T = [(KEY, {}), ("earlyUniverse", {}), ("primordial", {"evolve_T": 0}),
            ("galaxy_ism", {"evolve_T": 0})]
 
 
@@ -104,3 +134,17 @@ def test_gpu_refuses_the_analytic_jacobian_with_rate_terms():
     opts = net.options(**dict(workloads.OPTIONS[KEY], jac=1))
     r = net.solve_batch(n, T, dt, par, opts=opts, check=False)
     assert r.ierr == -104 and (r.flags == -104).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["lane", "warp"])
+def test_gpu_refuses_cells_whose_freeze_holds(layout):
+    key, info, n, T, dt, par, hot = _frozen_case(64, 67)
+    o = workloads.OPTIONS[key]
+    ref = Oracle(key).solve(n, T, dt, par, **o)
+    net = krome.load(key)
+    opts = net.options(**dict(o, layout=0 if layout == "warp" else 1))
+    r = net.solve_batch(n, T, dt, par, opts=opts, check=False)
+    np.testing.assert_array_equal(r.flags, ref["flags"])
+    assert (r.flags[hot] == -104).all()
+    np.testing.assert_array_equal(r.n[hot], n[hot])
