@@ -1,197 +1,234 @@
-// The post-solve conservation of a cell (the conserve option), restated for
-// host and device (KB_HD) from the reference's runtime
-// (runtime/core/solve_cell.hpp:1333-1500, conserved_row_, totals_residual_,
-// project_totals_, conserve_cell_):
+// Conservation of a cell's element totals and net charge, for host and
+// device (KB_HD): the post-solve `conserve` option and consistent advection
+// (the behaviour of the reference's runtime/core/solve_cell.hpp:1333-1560,
+// conserve_cell_ / conserve_to_n_ / conserve_to_x_).
+//
+// The behaviour, per mode of the post-solve option:
 //
 //   mode 1   the electrons restore the input net charge
-//   mode 2   the densities projected onto the input element totals and net
-//            charge: the minimal relative correction d_i = n_i sum_k A_ki
-//            lambda_k (a species at zero stays zero), lambda from the small
-//            system (A W A^T) lambda = residual by Gaussian elimination with
-//            partial pivoting (dependent rows skipped), repeated after
-//            clipping negatives up to 20 times until the residual is below
-//            1e-13
+//   mode 2   the densities moved onto the input element totals and net
+//            charge by the least relative change
 //   mode 3   the electrons neutralize the ions, n(e-) = max(sum q n, 0)
 //
-// Rows of A: the element counts (k < NELEM), then the charge. Opaque
-// species do not move (the networks here have no freeze directives).
-// Included inside the network namespace after the species tables; n0 and n
-// are a cell's NSPEC densities (any memory the caller can address).
+// The projection of mode 2 and of consistent advection, written for this
+// library: with the conserved rows a_k (element counts, then the charge) of
+// the movable species and the mismatch r = target - A n, the correction
+// minimising sum_i d_i^2 / n_i under A d = r is d = W A^T lam with
+// W = diag(n) (a species at zero stays zero) and the Gram system
+// G lam = r, G = A W A^T: a symmetric positive semi-definite matrix of at
+// most NELEM + 1 rows, built in one pass over the species and factored by
+// LDL^T with diagonal pivoting. Rows whose remaining pivot falls to 1e-14
+// of the largest diagonal have no independent freedom (no free carrier, or
+// a combination of the other rows); their multiplier stays 0. The
+// correction is unique whenever the system is consistent, so the choice of
+// factorisation changes only the last bits. A correction that drives a
+// species negative clips it to zero; the projection is then repeated from
+// the clipped state, at most 20 passes, until the largest relative
+// mismatch is below 1e-13.
+//
+// Opaque species never move. On networks with freeze directives a cell
+// whose freeze condition holds is refused (-104) before any solve, so the
+// post-solve conservation never meets a frozen species. Included inside the
+// network namespace after the species tables; n0 and n are a cell's NSPEC
+// densities in any memory the caller can address.
 #pragma once
 
-KB_HD inline double conserved_row_(int k, int i) {
+namespace kbcons {
+constexpr int kPasses = 20;          // projection passes after clipping
+constexpr double kDone = 1e-13;      // mismatch that ends the passes
+constexpr double kRankTol = 1e-14;   // pivot / largest diagonal: dependent
+constexpr double kUnreached = 1e-12; // consistent advection: -112 above
+}  // namespace kbcons
+
+// conserved quantity k of species i: atoms of element k (k < NELEM), or the
+// charge (k == NELEM)
+KB_HD inline double cons_coef(int k, int i) {
   return k < NELEM ? (double)species_element(i, k) : (double)species_charge(i);
 }
 
-// the largest relative residual |target - sum A n| / max(|target|, sum |A n|)
-KB_HD inline double totals_residual_(const double* n, const double* target,
-                                     bool charge) {
+// largest relative mismatch of the first `rows` conserved totals of n
+// against target: |target_k - (A n)_k| / max(|target_k|, sum_i |A_ki n_i|)
+KB_HD inline double cons_mismatch(const double* n, const double* target,
+                                  int rows) {
   double worst = 0.0;
-  for (int k = 0; k < NELEM + (charge ? 1 : 0); ++k) {
-    double t = 0.0, sc = std::fabs(target[k]);
+  for (int k = 0; k < rows; ++k) {
+    double sum = 0.0, mag = std::fabs(target[k]);
     for (int i = 0; i < NSPEC; ++i) {
-      const double a = conserved_row_(k, i) * n[i];
-      t += a;
-      sc += std::fabs(a);
+      const double v = cons_coef(k, i) * n[i];
+      sum += v;
+      mag += std::fabs(v);
     }
-    if (sc > 0.0) worst = std::fmax(worst, std::fabs(target[k] - t) / sc);
+    if (mag > 0.0) worst = std::fmax(worst, std::fabs(target[k] - sum) / mag);
   }
   return worst;
 }
 
-// fixed: the species that do not move (nullptr: the opaque ones)
-KB_HD inline double project_totals_(double* n, const double* target,
-                                    bool charge, const bool* fixed = nullptr) {
-  constexpr int NRMAX = NELEM + 1;
-  const int NR = NELEM + (charge ? 1 : 0);
-  for (int it = 0; it < 20; ++it) {
-    double r[NRMAX], M[NRMAX][NRMAX];
-    for (int k = 0; k < NR; ++k) {
-      double t1 = 0.0;
-      for (int i = 0; i < NSPEC; ++i) t1 += conserved_row_(k, i) * n[i];
-      r[k] = target[k] - t1;
-      for (int l = 0; l < NR; ++l) {
-        double s = 0.0;
-        for (int i = 0; i < NSPEC; ++i)
-          if (!(fixed != nullptr ? fixed[i] : species_opaque(i)))
-            s += conserved_row_(k, i) * conserved_row_(l, i) * n[i];
-        M[k][l] = s;
-      }
-    }
-    double lam[NRMAX];
-    for (int k = 0; k < NR; ++k) lam[k] = 0.0;
-    double scale = 0.0;
-    for (int k = 0; k < NR; ++k) scale = std::fmax(scale, std::fabs(M[k][k]));
-    bool used[NRMAX];
-    for (int k = 0; k < NRMAX; ++k) used[k] = false;
-    for (int col = 0; col < NR; ++col) {
-      // a pivot below 1e-14 of the largest diagonal: the row depends on
-      // the others (or has no free species), its lambda stays 0
-      int piv = -1;
-      double best = 1e-14 * scale;
-      for (int row = col; row < NR; ++row)
-        if (std::fabs(M[row][col]) > best) {
-          best = std::fabs(M[row][col]);
-          piv = row;
-        }
-      if (piv < 0) continue;
-      if (piv != col) {
-        for (int l = 0; l < NR; ++l) {
-          const double t = M[piv][l];
-          M[piv][l] = M[col][l];
-          M[col][l] = t;
-        }
-        const double t = r[piv];
-        r[piv] = r[col];
-        r[col] = t;
-      }
-      used[col] = true;
-      for (int row = col + 1; row < NR; ++row) {
-        const double f = M[row][col] / M[col][col];
-        for (int l = col; l < NR; ++l) M[row][l] -= f * M[col][l];
-        r[row] -= f * r[col];
-      }
-    }
-    for (int col = NR - 1; col >= 0; --col) {
-      if (!used[col]) continue;
-      double s = r[col];
-      for (int l = col + 1; l < NR; ++l) s -= M[col][l] * lam[l];
-      lam[col] = s / M[col][col];
-    }
-    bool clipped = false;
-    for (int i = 0; i < NSPEC; ++i) {
-      if (fixed != nullptr ? fixed[i] : species_opaque(i)) continue;
-      double d = 0.0;
-      for (int k = 0; k < NR; ++k) d += conserved_row_(k, i) * lam[k];
-      n[i] += n[i] * d;
-      if (n[i] < 0.0) {
-        n[i] = 0.0;
-        clipped = true;
-      }
-    }
-    if (!clipped || totals_residual_(n, target, charge) < 1e-13) break;
+// one least-change correction of n towards target over the first `rows`
+// conserved quantities; movable[i] marks the species that may move. Returns
+// true when a correction clipped a species at zero.
+KB_HD inline bool cons_correct(double* n, const double* target, int rows,
+                               const bool* movable) {
+  constexpr int R = NELEM + 1;
+  double G[R][R], rhs[R], lam[R];
+  int order[R];
+  // the Gram matrix and the mismatch, one pass over the species
+  for (int k = 0; k < rows; ++k) {
+    rhs[k] = target[k];
+    order[k] = k;
+    lam[k] = 0.0;
+    for (int l = 0; l < rows; ++l) G[k][l] = 0.0;
   }
-  return totals_residual_(n, target, charge);
+  for (int i = 0; i < NSPEC; ++i) {
+    double a[R];
+    for (int k = 0; k < rows; ++k) a[k] = cons_coef(k, i);
+    for (int k = 0; k < rows; ++k) rhs[k] -= a[k] * n[i];
+    if (!movable[i]) continue;
+    for (int k = 0; k < rows; ++k) {
+      if (a[k] == 0.0) continue;
+      const double ak = a[k] * n[i];
+      for (int l = 0; l < rows; ++l) G[k][l] += ak * a[l];
+    }
+  }
+  double dmax = 0.0;
+  for (int k = 0; k < rows; ++k) dmax = std::fmax(dmax, G[k][k]);
+  // LDL^T with diagonal pivoting: step s takes the largest remaining
+  // diagonal; the trailing block is updated in place (upper triangle used)
+  int rank = 0;
+  for (int s = 0; s < rows; ++s) {
+    int m = s;
+    for (int k = s + 1; k < rows; ++k)
+      if (G[k][k] > G[m][m]) m = k;
+    if (!(G[m][m] > kbcons::kRankTol * dmax)) break;
+    if (m != s) {
+      for (int l = 0; l < rows; ++l) {
+        const double t = G[s][l]; G[s][l] = G[m][l]; G[m][l] = t;
+      }
+      for (int l = 0; l < rows; ++l) {
+        const double t = G[l][s]; G[l][s] = G[l][m]; G[l][m] = t;
+      }
+      const double t = rhs[s]; rhs[s] = rhs[m]; rhs[m] = t;
+      const int o = order[s]; order[s] = order[m]; order[m] = o;
+    }
+    const double inv = 1.0 / G[s][s];
+    for (int k = s + 1; k < rows; ++k) {
+      const double f = G[k][s] * inv;
+      if (f == 0.0) continue;
+      for (int l = s + 1; l < rows; ++l) G[k][l] -= f * G[s][l];
+      rhs[k] -= f * rhs[s];
+    }
+    rank = s + 1;
+  }
+  // back substitution over the independent rows
+  double y[R];
+  for (int s = rank - 1; s >= 0; --s) {
+    double v = rhs[s];
+    for (int l = s + 1; l < rank; ++l) v -= G[s][l] * y[l];
+    y[s] = v / G[s][s];
+  }
+  for (int s = 0; s < rank; ++s) lam[order[s]] = y[s];
+  // d_i = n_i sum_k a_ki lam_k
+  bool clipped = false;
+  for (int i = 0; i < NSPEC; ++i) {
+    if (!movable[i]) continue;
+    double g = 0.0;
+    for (int k = 0; k < rows; ++k) g += cons_coef(k, i) * lam[k];
+    const double v = n[i] + n[i] * g;
+    clipped = clipped || v < 0.0;
+    n[i] = v < 0.0 ? 0.0 : v;
+  }
+  return clipped;
 }
 
-// the conservation of a solved cell n against its input n0 (mode 0: none)
+// the projection with its passes; returns the final mismatch
+KB_HD inline double cons_project(double* n, const double* target, int rows,
+                                 const bool* movable) {
+  for (int pass = 0; pass < kbcons::kPasses; ++pass) {
+    const bool clipped = cons_correct(n, target, rows, movable);
+    if (!clipped) break;
+    if (cons_mismatch(n, target, rows) < kbcons::kDone) break;
+  }
+  return cons_mismatch(n, target, rows);
+}
+
+// the net charge sum_i q_i n_i, optionally without one species
+KB_HD inline double cons_charge(const double* n, int skip = -1) {
+  double q = 0.0;
+  for (int i = 0; i < NSPEC; ++i)
+    if (i != skip) q += species_charge(i) * n[i];
+  return q;
+}
+
+// the post-solve conservation of a solved cell n against its input n0
+// (mode 0: none)
 KB_HD inline void conserve_cell(const double* n0, double* n, int mode) {
   if (mode <= 0) return;
+  const int e = IDX_ELECTRON;
   if (mode == 3) {
-    if (IDX_ELECTRON >= 0) {
-      double qi = 0.0;
-      for (int i = 0; i < NSPEC; ++i)
-        if (i != IDX_ELECTRON) qi += species_charge(i) * n[i];
-      n[IDX_ELECTRON] = std::fmax(qi, 0.0);
-    }
+    if (e >= 0) n[e] = std::fmax(cons_charge(n, e), 0.0);
     return;
   }
   if (mode == 1) {
-    if (IDX_ELECTRON >= 0 && !species_opaque(IDX_ELECTRON)) {
-      double q0 = 0.0, q = 0.0;
-      for (int i = 0; i < NSPEC; ++i) {
-        q0 += species_charge(i) * n0[i];
-        q += species_charge(i) * n[i];
-      }
-      n[IDX_ELECTRON] = std::fmax(n[IDX_ELECTRON] + (q - q0), 0.0);
-    }
+    if (e >= 0 && !species_opaque(e))
+      n[e] = std::fmax(n[e] + (cons_charge(n) - cons_charge(n0)), 0.0);
     return;
   }
   double target[NELEM + 1];
   for (int k = 0; k <= NELEM; ++k) {
-    target[k] = 0.0;
-    for (int i = 0; i < NSPEC; ++i) target[k] += conserved_row_(k, i) * n0[i];
+    double t = 0.0;
+    for (int i = 0; i < NSPEC; ++i) t += cons_coef(k, i) * n0[i];
+    target[k] = t;
   }
-  project_totals_(n, target, true);
+  bool movable[NSPEC];
+  for (int i = 0; i < NSPEC; ++i) movable[i] = !species_opaque(i);
+  cons_project(n, target, NELEM + 1, movable);
 }
 
-// consistent advection (the reference's conserve_to_n_ / conserve_to_x_,
-// solve_cell.hpp:1504-1560; legacy krome_conserveLin_x): the cell n moved
-// to the element totals ref[NELEM] and to zero net charge. Negatives are
-// clipped first; the elements by the projection without the charge row
-// (the ionization is kept); then the electrons from neutrality, n(e-) =
-// sum q n over the other species, or, when the electrons cannot do it
-// (anions dominate, or no free electrons), the charge too by the
-// projection. fixed species do not move. Returns 0, -112 when the totals
-// or neutrality cannot be reached (corrected as far as possible), or the
-// warning 2 when a species changed by more than 50 %.
+// consistent advection (legacy krome_conserveLin_x): the advected cell n
+// moved to the element totals ref[NELEM] and to zero net charge. fixed[i]
+// marks the species that do not move. Steps: clip the movable species'
+// negatives; the elements by the projection without the charge row (the
+// ionization is kept); then the electrons from neutrality (the sum of the
+// other charges) when that is non-negative, else the charge row joins the
+// projection. Returns 0, -112 when the totals or neutrality stay out of
+// reach (the cell corrected as far as possible), or the warning 2 when a
+// species changed by more than half.
 KB_HD inline int conserve_to_n(double* n, const double* ref,
                                const bool* fixed) {
-  double n0[NSPEC];
+  double start[NSPEC];
+  bool movable[NSPEC];
   for (int i = 0; i < NSPEC; ++i) {
-    if (!fixed[i] && n[i] < 0.0) n[i] = 0.0;
-    n0[i] = n[i];
+    movable[i] = !fixed[i];
+    if (movable[i] && n[i] < 0.0) n[i] = 0.0;
+    start[i] = n[i];
   }
   double target[NELEM + 1];
   for (int k = 0; k < NELEM; ++k) target[k] = ref[k];
   target[NELEM] = 0.0;
-  project_totals_(n, target, false, fixed);
-  bool charge_done = false;
-  if (IDX_ELECTRON >= 0 && !fixed[IDX_ELECTRON]) {
-    double qi = 0.0;
-    for (int i = 0; i < NSPEC; ++i)
-      if (i != IDX_ELECTRON) qi += species_charge(i) * n[i];
-    if (qi >= 0.0) {
-      n[IDX_ELECTRON] = qi;
-      charge_done = true;
-    } else {
-      n[IDX_ELECTRON] = 0.0;
-    }
+  cons_project(n, target, NELEM, movable);
+  const int e = IDX_ELECTRON;
+  bool neutral = false;
+  if (e >= 0 && movable[e]) {
+    const double q = cons_charge(n, e);
+    neutral = q >= 0.0;
+    n[e] = neutral ? q : 0.0;
   }
-  if (!charge_done) project_totals_(n, target, true, fixed);
-  if (totals_residual_(n, target, true) > 1e-12) return -112;
+  if (!neutral) cons_project(n, target, NELEM + 1, movable);
+  if (cons_mismatch(n, target, NELEM + 1) > kbcons::kUnreached) return -112;
   for (int i = 0; i < NSPEC; ++i)
-    if (n0[i] > 0.0 && std::fabs(n[i] - n0[i]) > 0.5 * n0[i]) return 2;
+    if (start[i] > 0.0 && std::fabs(n[i] - start[i]) > 0.5 * start[i])
+      return 2;
   return 0;
 }
+
 // the same with mass fractions x and ref per gram: n = x / m per gram,
 // corrected, x = m n; a species without mass does not move
 KB_HD inline int conserve_to_x(double* x, const double* ref) {
   bool fixed[NSPEC];
   double n[NSPEC];
   for (int i = 0; i < NSPEC; ++i) {
-    fixed[i] = species_opaque(i) || !(species_mass_g(i) > 0.0);
-    n[i] = species_mass_g(i) > 0.0 ? x[i] / species_mass_g(i) : 0.0;
+    const double m = species_mass_g(i);
+    fixed[i] = species_opaque(i) || !(m > 0.0);
+    n[i] = m > 0.0 ? x[i] / m : 0.0;
   }
   const int f = conserve_to_n(n, ref, fixed);
   for (int i = 0; i < NSPEC; ++i)

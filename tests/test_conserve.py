@@ -3,10 +3,12 @@ runtime/core/solve_cell.hpp:1333-1500, 2169-2175).
 
 Mode 1: the electrons restore the input net charge; mode 2: the densities
 projected onto the input element totals and charge; mode 3: the electrons
-neutralize the ions. The oracle's restatement (csrc/kb_conserve.h, shared
-with the kernels) is checked bit for bit against the reference's own build
-where it exists here, and against the invariant each mode guarantees; the
-GPU kernels are checked against the oracle."""
+neutralize the ions. csrc/kb_conserve.h (shared by the kernels and the
+oracle) is checked against the reference's own build where it exists here
+-- modes 1 and 3 bit for bit, the projection of mode 2 to 1e-13 (its own
+factorisation of the small Gram system rounds differently) -- and against
+the invariant each mode guarantees; the GPU kernels are checked against
+the oracle."""
 import numpy as np
 import pytest
 
@@ -41,8 +43,18 @@ def test_oracle_conservation_equals_the_reference(key, mode):
     ref = reference_solve(key, n, T, dt, par, strict=True, **o)
     out = Oracle(key).solve(n, T, dt, par, **o)
     np.testing.assert_array_equal(out["flags"], ref["flags"])
-    np.testing.assert_array_equal(out["n"], ref["n"])
     np.testing.assert_array_equal(out["T"], ref["T"])
+    if mode != 2:  # the charge sums: same operations, same bits
+        np.testing.assert_array_equal(out["n"], ref["n"])
+        return
+    # the projection: this library's pivoted LDL^T of the Gram system
+    # against the reference's row-pivoted elimination -- the same
+    # correction up to the last bits
+    scale = ref["n"].sum(axis=1, keepdims=True)
+    big = np.abs(ref["n"]) > 1e-30 * scale
+    err = np.abs(out["n"] - ref["n"])
+    assert (err[big] <= 1e-13 * np.abs(ref["n"][big])).all()
+    assert (err[~big] <= 1e-43 * np.broadcast_to(scale, err.shape)[~big]).all()
 
 
 @pytest.mark.parametrize("key", NETWORKS)
