@@ -276,16 +276,23 @@ int krome_b200_adjoint_device(int ncell, const double* T0, const double* par,
  * memory -- a code that gives the whole GPU to its own memory pool, or a
  * time step that must not pay cudaMalloc's device-wide synchronization.
  * No counterpart in the reference (its device path allocates per call).
- * Same arguments, layouts, flags and failed-cell rule as krome_solve_cells
- * (flags may be NULL); the call's device copies go through one array
- * compiled into the library, 16 MiB of device memory per GPU held until
- * the process exits, instead of an allocation: it fits about
- * 16 MiB / (8 (nspec + 2 + npar) + 4) bytes-per-cell cells (per-cell
- * parameter rows), and a larger call returns -111 (FLAG_DEVICE_MEMORY)
- * with nothing touched. The first call on a device looks up the array's
- * device address (once per device); make it before any stream capture.
- * All calls share the array: the entry point serialises its own calls,
- * and calls that overlapped on the GPU would race. */
+ * The arguments of krome_solve_cells without `extra` (no photon or dust
+ * rows); same layouts, flags and failed-cell rule (flags may be NULL). The
+ * call's device copies go through one array compiled into the library,
+ * 16 MiB of device memory per GPU held until the process exits, instead of
+ * an allocation: it fits about 16 MiB / (8 (nspec + 2 + npar) + 4)
+ * bytes-per-cell cells (per-cell parameter rows), and a larger call returns
+ * -111 (FLAG_DEVICE_MEMORY) with nothing touched. Call it once with
+ * ncell == 0 on each device (that device current) before the caller's pool
+ * takes the GPU and before any stream capture: it looks up the array's
+ * device address, which loads the library's device code, and launches the
+ * kernel the options select once with no cells, so that the driver
+ * reserves the kernel's per-thread local memory then; it returns 0, or the
+ * flag the options would give (-104). All calls share the array: the entry
+ * point serialises its own calls, and calls that overlapped on the GPU
+ * would race. Results come back through host staging: a failed copy leaves
+ * the caller's arrays untouched (-104). The large networks (the sparse
+ * path, whose workspace this cannot provide) return -104 in every flag. */
 int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
                                    const double* dt, const double* par,
                                    int par_stride, int* flags,

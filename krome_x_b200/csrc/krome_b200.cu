@@ -756,6 +756,7 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
     long blocks;
     if (h.kernel == 0) {
       blocks = ((long)ncell + threads - 1) / threads;
+      if (blocks < 1) blocks = 1;  // ncell 0: an empty launch (warm-up)
     } else {
       int per_sm = h.blocks_per_sm;
       if (per_sm <= 0) {
@@ -777,7 +778,8 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
   }
   const size_t smem = sizeof(double) * kWarpsPerBlock * Geo<EVT>::SMEM_DOUBLES;
   if (h.kernel == 0) {
-    const int blocks = (ncell + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    int blocks = (ncell + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks < 1) blocks = 1;  // ncell 0: an empty launch (warm-up)
     kb_cells_plain<EVT><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(
         ncell, n, T, dt, par, pstride, flags, stats, so);
     return cudaGetLastError();
@@ -1993,13 +1995,22 @@ KB_API int krome_b200_fp64_peak(double* tflops) {
 // Host code never uses the array's name as an address (on the host it names
 // a stand-in, not device memory): the first call on each device, with that
 // device current, asks cudaGetSymbolAddress for the device address and
-// keeps it. Make that first call before any stream capture. All calls share
-// the one array and it keeps the previous call's contents; the cursor is
-// zeroed by every launch and every cell's flag is written by the kernel.
-// Calls that overlapped on the GPU would race on the array: the entry point
-// serialises its own calls (a mutex held until the results are back on the
-// host).
+// keeps it. That lookup loads the library's device code (CUDA loads modules
+// lazily), and the first launch of a kernel makes the driver reserve the
+// kernel's per-thread local memory; both are device memory the driver takes
+// itself. A call with ncell == 0 does both (the address lookup and one empty
+// launch of the kernel the options select) and solves nothing: make it once
+// per device before the caller's pool takes the GPU and before any stream
+// capture. All calls share the one array and it keeps the previous call's
+// contents; the cursor is zeroed by every launch and every cell's flag is
+// written by the kernel. Calls that overlapped on the GPU would race on the
+// array: the entry point serialises its own calls (a mutex held until the
+// results are back on the host). Results come back through host staging, so
+// a copy that fails part-way leaves the caller's arrays untouched.
+// The large networks' sparse path needs its per-block workspace, which this
+// entry point cannot provide: their builds return -104 and hold no array.
 
+#ifndef KB_LARGE_NETWORK
 #define KB_NOALLOC_BYTES (16u << 20)
 static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_BYTES];
 
@@ -2023,21 +2034,38 @@ void* noalloc_scratch() {
   return g_noalloc_ptr[d];
 }
 }  // namespace
+#endif
 
 KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
                                           const double* dt, const double* par,
                                           int par_stride, int* flags,
                                           const krome_opts* h) {
-  if (h == nullptr || ncell < 0 || n == nullptr || Tgas == nullptr
-      || dt == nullptr)
+  if (h == nullptr || ncell < 0) return -1;
+  if (ncell > 0 && (n == nullptr || Tgas == nullptr || dt == nullptr))
     return -1;
   if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR)
     return -1;
-  if (ncell == 0) return 0;
 #ifdef KB_LARGE_NETWORK
-  (void)flags;
+  (void)par;
+  if (flags != nullptr)
+    for (int c = 0; c < ncell; ++c) flags[c] = -104;
   return -104;  // a large network's solve needs its allocated workspace
-#endif
+#else
+  if (ncell == 0) {
+    // the warm-up: resolve the array, load the module, and launch the
+    // selected kernel once with no cells (its local memory reserved now)
+    if (const int u = unsupported(*h)) return u;  // it launches nothing
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    char* b = static_cast<char*>(noalloc_scratch());
+    if (b == nullptr) return -104;
+    unsigned* dcur = reinterpret_cast<unsigned*>(b);
+    double* dd = reinterpret_cast<double*>(b + 256);
+    cudaError_t e = launch_any(*h, 0, dd, dd, dd, dd, 0,
+                               reinterpret_cast<int*>(b + 256), nullptr, dcur,
+                               0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    return e == cudaSuccess ? 0 : -104;
+  }
   double dflt[kbnet::NPAR];
   for (int i = 0; i < kbnet::NPAR; ++i) dflt[i] = kbnet::param_default(i);
   const double* P = par != nullptr ? par : dflt;
@@ -2065,9 +2093,17 @@ KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
       for (int c = 0; c < ncell; ++c) flags[c] = -111;
     return -111;
   }
+  // host staging of the results: committed to the caller's arrays only
+  // once every copy has succeeded
+  std::vector<double> hn((size_t)ncell * kbnet::NSPEC), hT(ncell);
+  std::vector<int> hfl(ncell);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   char* b = static_cast<char*>(noalloc_scratch());
-  if (b == nullptr) return -104;
+  if (b == nullptr) {
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = -104;
+    return -104;
+  }
   unsigned* dcur = reinterpret_cast<unsigned*>(b); b += 256;
   double* dn = reinterpret_cast<double*>(b); b += al(nb);
   double* dT = reinterpret_cast<double*>(b); b += al(tb);
@@ -2081,31 +2117,24 @@ KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
   if (e == cudaSuccess) e = cudaMemcpyAsync(dp, P, pb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = launch_any(*h, ncell, dn, dT, ddt, dp, ps, dfl, nullptr, dcur, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(n, dn, nb, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(Tgas, dT, tb, cudaMemcpyDeviceToHost, s);
-  if (flags != nullptr && e == cudaSuccess)
-    e = cudaMemcpyAsync(flags, dfl, fb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hn.data(), dn, nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hT.data(), dT, tb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hfl.data(), dfl, fb, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(e));
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = -104;
     return -104;
   }
-  if (flags != nullptr) {
-    for (int c = 0; c < ncell; ++c)
-      if (flags[c] != 0) return flags[c];
-    return 0;
-  }
-  // no flags array: the lowest failing cell's flag, read in fixed chunks
-  int chunk[1024];
-  for (int c0 = 0; c0 < ncell; c0 += 1024) {
-    const int m = ncell - c0 < 1024 ? ncell - c0 : 1024;
-    if (cudaMemcpy(chunk, dfl + c0, sizeof(int) * m, cudaMemcpyDeviceToHost)
-        != cudaSuccess)
-      return -104;
-    for (int i = 0; i < m; ++i)
-      if (chunk[i] != 0) return chunk[i];
-  }
+  // a failed cell's device row still holds its input: copy every row
+  std::memcpy(n, hn.data(), nb);
+  std::memcpy(Tgas, hT.data(), tb);
+  if (flags != nullptr) std::memcpy(flags, hfl.data(), fb);
+  for (int c = 0; c < ncell; ++c)
+    if (hfl[c] != 0) return hfl[c];
   return 0;
+#endif
 }
 
 KB_API int krome_has_device(void) {

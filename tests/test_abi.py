@@ -146,3 +146,33 @@ def test_flag_messages():
     assert "unset" in net.flag_message(-105)
     assert "FLAG_TOO_MUCH_WORK" in net.flag_message(-1)
     assert net.flag_message(0) == "success"
+
+
+def test_noalloc_entry_point_refuses_before_the_device():
+    """the no-allocation solve: bad arguments and the large networks'
+    refusal (their sparse path needs its own workspace) are decided on the
+    host, every flag written"""
+    fn_t = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _I, ctypes.c_void_p]
+    big = krome.load("semenov")
+    fn = big._lib.krome_b200_solve_cells_noalloc
+    fn.restype, fn.argtypes = ctypes.c_int, fn_t
+    n = np.ones((3, big.nspec))
+    T, dt = np.full(3, 20.0), np.full(3, 1e10)
+    fl = np.zeros(3, dtype=np.intc)
+    h = big.options()._h
+    P = lambda a: a.ctypes.data_as(_D)
+    assert fn(3, P(n), P(T), P(dt), None, 0, fl.ctypes.data_as(_I), h) == -104
+    assert (fl == -104).all()
+    small = krome.load("primordial3")
+    fn = small._lib.krome_b200_solve_cells_noalloc
+    fn.restype, fn.argtypes = ctypes.c_int, fn_t
+    n = np.ones((3, small.nspec))
+    assert fn(0, None, None, None, None, 0, None, None) == -1
+    assert fn(3, None, P(T), P(dt), None, 0, None, small.options()._h) == -1
+    par = np.tile(small.params_default(), (3, 1))
+    assert fn(3, P(n), P(T), P(dt), P(par), 5, None, small.options()._h) == -1
+    # an unset REQUIRED parameter (tff): -105 before the device
+    fl[:] = 7
+    assert fn(3, P(n), P(T), P(dt), P(par), small.npar, fl.ctypes.data_as(_I),
+              small.options(evolve_T=1)._h) == -105
+    assert (fl == -105).all()
