@@ -80,12 +80,22 @@ int krome_opts_set_rtol_species(krome_opts* h, const double* rtol);
 int krome_opts_get_atol_species(const krome_opts* h, double* atol);
 int krome_opts_get_rtol_species(const krome_opts* h, double* rtol);
 
+/* the optional per-cell arrays of a call (reference krome.h:258-294):
+ * Phi[ncell][nbins] the photon flux per bin, read with photon bins on the
+ * handle (krome_opts_set_photo); Td and adust (binned dust, not built in
+ * this library) are not read. NULL, or unused members NULL. */
+typedef struct {
+  double* Phi;
+  double* Td;
+  double* adust;
+} krome_cells;
+
 /* ---- the solve (reference krome.h:291-294, krome.cpp:396-438) ----
- * Host arrays, updated in place; extra (the reference's krome_cells of
- * photon / dust rows) must be NULL for these networks; flags[ncell] may
- * be NULL. Returns 0 or the lowest-index failing cell's flag. */
+ * Host arrays, updated in place; extra (krome_cells) may be NULL;
+ * flags[ncell] may be NULL. Returns 0 or the lowest-index failing cell's
+ * flag. */
 int krome_solve_cells(int ncell, double* n, double* Tgas, const double* dt,
-                      const double* par, int par_stride, const void* extra,
+                      const double* par, int par_stride, const krome_cells* extra,
                       int* flags, const krome_opts* h);
 
 /* krome_solve_cells with mass fractions (reference krome.h:302-306):
@@ -96,7 +106,7 @@ int krome_solve_cells(int ncell, double* n, double* Tgas, const double* dt,
  * Host arrays; flags may be NULL. */
 int krome_solve_cells_x(int ncell, double* x, const double* rho,
                         double* Tgas, const double* dt, const double* par,
-                        int par_stride, const void* extra, int* flags,
+                        int par_stride, const krome_cells* extra, int* flags,
                         const krome_opts* h);
 
 /* ---- device-resident data (reference krome.h:308-349) ----
@@ -122,14 +132,14 @@ typedef struct {
 int krome_solve_cells_device(int ncell, double* n, int layout, long ld,
                              double* Tgas, const double* dt,
                              const double* par, int par_stride,
-                             const void* extra, int* flags,
+                             const krome_cells* extra, int* flags,
                              krome_device_summary* summary,
                              const krome_opts* h);
 /* krome.h:345-350 */
 int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
                                int layout, long ld, double* Tgas,
                                const double* dt, const double* par,
-                               int par_stride, const void* extra,
+                               int par_stride, const krome_cells* extra,
                                int* flags, krome_device_summary* summary,
                                const krome_opts* h);
 
@@ -173,6 +183,152 @@ int krome_species_natoms(int i, int e);
 int krome_device_initialize(void);
 int krome_device_initialize_id(int device_id);
 int krome_device_finalize(void);
+
+/* ---- the rest of the reference's interface: metadata, queries and the
+ * photon-field helpers (evaluated on the host; rates at clamp(Tgas, Tcmb,
+ * 1e9), thermal terms at clamp(Tgas, 2.73, 1e9), as the solve) ---- */
+/* krome.h:651 */
+const char* krome_reaction_name(int r);
+/* krome.h:405-418: the active thermal terms (names in the reference's
+ * order), their values, the adiabatic index, the per-reaction energy
+ * release (none in these networks: 0) */
+int krome_nheat(void);
+int krome_ncool(void);
+const char* krome_heating_name(int i);
+const char* krome_cooling_name(int i);
+int krome_get_thermal(int ncell, const double* n, const double* Tgas,
+                      const double* par, int par_stride, const double* Phi,
+                      const krome_opts* h, double* heat, double* cool,
+                      double* heats, double* cools, double* dTdt);
+int krome_get_qeff(int ncell, const double* n, const double* Tgas,
+                   const double* par, int par_stride, double* q);
+int krome_get_gamma(int ncell, const double* n, const double* Tgas,
+                    const double* par, int par_stride, double* gamma);
+/* krome.h:390, 397: reaction fluxes k prod(n); the dust temperature the
+ * rates see (the Tdust parameter; -1 for a network without one) */
+int krome_get_fluxes(int ncell, const double* n, const double* Tgas,
+                     const double* par, int par_stride, const double* Phi,
+                     const krome_opts* h, double* fl);
+int krome_get_Tdust(int ncell, const double* n, const double* Tgas,
+                    const double* par, int par_stride, const double* Phi,
+                    const krome_opts* h, double* Td);
+/* krome.h:424-438: per-cell quantities of the densities */
+int krome_get_mu(int ncell, const double* n, double* out);
+int krome_get_rho(int ncell, const double* n, double* out);
+int krome_get_ntot(int ncell, const double* n, double* out);
+int krome_get_Hnuclei(int ncell, const double* n, double* out);
+int krome_get_charge(int ncell, const double* n, double* out);
+int krome_get_electrons(int ncell, const double* n, double* out);
+int krome_get_free_fall_time(int ncell, const double* n, double* out);
+int krome_get_jeans_length(int ncell, const double* n, const double* Tgas,
+                           double* out);
+int krome_get_free_fall_time_rho(int ncell, const double* rho, double* out);
+int krome_num2col(int ncell, const double* num, const double* n,
+                  const double* Tgas, const double* par, int par_stride,
+                  double* out);
+/* krome.h:521: the neutral atomic metals at metallicity Z */
+int krome_scale_Z(int ncell, double* n, double Z);
+/* krome.h:449-458: line coolants of coolant files (none here: 0 coolants,
+ * -1 for any index) */
+int krome_ncoolant(void);
+const char* krome_coolant_name(int i);
+int krome_coolant_species(int i);
+int krome_coolant_nlev(int i);
+int krome_coolant_levels(int i, double* E, double* g);
+int krome_get_coolant_cooling(int ncell, const double* n, const double* Tgas,
+                              const double* par, int par_stride,
+                              const double* Phi, const krome_opts* h,
+                              double* cool);
+int krome_get_coolant_populations(int ncell, const double* n,
+                                  const double* Tgas, const double* par,
+                                  int par_stride, const double* Phi,
+                                  const krome_opts* h, int i, double* pop);
+/* krome.h:548-595: photon-field helpers (bins, J <-> Phi, spectra integrated
+ * over the bins, dust opacity per bin, the G0 / Av fit); the Haardt &
+ * Madau 2012 background and the Draine dust opacity need tables this
+ * library does not carry: -104 */
+int krome_bins_lin(int nbins, double lower, double upper, double* Elo,
+                   double* Ehi);
+int krome_bins_log(int nbins, double lower, double upper, double* Elo,
+                   double* Ehi);
+int krome_J_to_phi(int nbins, const double* Elo, const double* Ehi,
+                   const double* J, double* phi);
+int krome_phi_to_J(int nbins, const double* Elo, const double* Ehi,
+                   const double* phi, double* J);
+int krome_spectrum_blackbody(int nbins, const double* Elo, const double* Ehi,
+                             double Tbb, double* phi);
+int krome_blackbody_range(double Tbb, double* lower, double* upper);
+int krome_spectrum_draine(int nbins, const double* Elo, const double* Ehi,
+                          double* phi);
+int krome_spectrum_j21(int nbins, const double* Elo, const double* Ehi,
+                       double J21, double alpha, double* phi);
+int krome_spectrum_hm2012(int nbins, const double* Elo, const double* Ehi,
+                          double z, double* phi);
+int krome_spectrum_table(int nbins, const double* Elo, const double* Ehi,
+                         int nE, const double* E, const double* J,
+                         int loglog, double* phi);
+int krome_dust_kappa_bins(int nE, const double* E, const double* kappa,
+                          int nbins, const double* Elo, const double* Ehi,
+                          double* kbin);
+int krome_dust_kappa_draine(int nbins, const double* Elo, const double* Ehi,
+                            double* kbin);
+int krome_find_G0_Av(int nbins, const double* Elo, const double* Ehi,
+                     const double* phi, const double* kbin, double d2g,
+                     double xH, double* G0, double* Av);
+/* krome.h:602-640: the photo reactions, J_LW rates (none here), photon
+ * bins on the handle and the field queries */
+int krome_nphoto(void);
+int krome_photo_reaction(int r);
+int krome_photo_reactant(int r);
+double krome_photo_pdiss(int r);
+double krome_photo_xsec(int r, double E);
+int krome_nlw(void);
+int krome_lw_reaction(int q);
+int krome_lw_reactant(int q);
+double krome_lw_pdiss(int q);
+/* krome.h:206-228 */
+int krome_opts_set_photo(krome_opts* h, int nbins, const double* Elo,
+                         const double* Ehi);
+int krome_opts_nbins(const krome_opts* h);
+int krome_opts_set_photo_broadening(krome_opts* h, double Tgas, double vturb);
+int krome_opts_set_photo_alpha(krome_opts* h, double alpha);
+int krome_opts_set_photo_dust_opacity(krome_opts* h, const double* kappa);
+int krome_opts_lw_weights(const krome_opts* h, double* w);
+int krome_opts_photo_sigma(const krome_opts* h, double* sigma);
+int krome_get_photo_heating(int ncell, const double* n, const double* Tgas,
+                            const double* par, int par_stride,
+                            const double* Phi, const krome_opts* h,
+                            double* heat);
+int krome_get_ratio_flux_draine(int ncell, const double* Phi,
+                                const krome_opts* h, double* ratio);
+int krome_get_habing(int ncell, const double* Phi, const krome_opts* h,
+                     double* G);
+int krome_get_opacity(int ncell, const double* n, const double* Tgas,
+                      const double* par, int par_stride, const krome_opts* h,
+                      const double* d2g, const double* kdust, double* tau);
+int krome_get_absorption(int ncell, const double* n, const double* Tgas,
+                         const double* par, int par_stride,
+                         const krome_opts* h, const double* kdust,
+                         double* kabs);
+/* krome.h:236-256: binned dust is not built in this library: set returns
+ * -104, ndust 0, the rest -1 (as without bins) */
+int krome_opts_set_dustbins(krome_opts* h, int nd, int use_Si, int use_C,
+                            double alow, double aup, double phi);
+int krome_opts_ndust(const krome_opts* h);
+int krome_opts_set_dust_Td(krome_opts* h, const double* Td);
+int krome_opts_get_dust_Td(const krome_opts* h, double* Td);
+int krome_opts_set_dust_a(krome_opts* h, const double* a);
+int krome_opts_get_dust_a(const krome_opts* h, double* a);
+int krome_opts_get_dust_counts(const krome_opts* h, double rho_gas,
+                               double d2g, double* nd);
+int krome_opts_get_dust_types(const krome_opts* h, int* isC);
+/* krome.h:364: the error-report file name (kept; no report is written) */
+int krome_opts_set_error_file(krome_opts* h, const char* path);
+/* krome.h:373: integrate every cell to steady state (eq_* keys) */
+int krome_equilibrium_cells(int ncell, double* n, double* Tgas,
+                            const double* par, int par_stride,
+                            const krome_cells* extra, int* flags,
+                            const krome_opts* h);
 
 /* ---- additions of this library ---- */
 

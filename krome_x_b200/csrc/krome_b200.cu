@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include KB_NET_HEADER
@@ -36,6 +37,13 @@
 #include "bdf_big.cuh"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
+
+// the reference's optional per-cell arrays of a call (krome.h:258-294)
+typedef struct {
+  double* Phi;
+  double* Td;
+  double* adust;
+} krome_cells;
 
 using kbw::SolveOpts;
 using kbw::NSTAT;
@@ -601,6 +609,17 @@ struct krome_opts {
   // per-species tolerances (krome_opts_set_atol_species / rtol_species):
   // empty, or NSPEC entries (negative: the scalar)
   std::vector<double> atol_sp, rtol_sp;
+  // the reference's other keys: the equilibrium driver (first output time,
+  // last time, output factor, convergence tolerances) and the reduced speed
+  // of light of an evolved field
+  double eq_t0 = 100.0 * kbc::seconds_per_year;
+  double eq_tmax = 5e8 * kbc::seconds_per_year;
+  double eq_factor = 3.0, eq_rtol = 1e-5, eq_atol = 1e-12;
+  double c_red = kbc::clight;
+  std::string error_file = "KROME_ERROR_REPORT";
+  // photon bins: the broadening of tabulated cross sections and the
+  // in-bin spectrum dN/dE ~ E^-alpha
+  double broad_T = 0.0, broad_vturb = 0.0, photo_alpha = 1.0;
 };
 
 namespace {
@@ -930,6 +949,12 @@ int* int_key(krome_opts* h, const char* k) {
   return nullptr;
 }
 double* dbl_key(krome_opts* h, const char* k) {
+  if (!std::strcmp(k, "eq_t0")) return &h->eq_t0;
+  if (!std::strcmp(k, "eq_tmax")) return &h->eq_tmax;
+  if (!std::strcmp(k, "eq_factor")) return &h->eq_factor;
+  if (!std::strcmp(k, "eq_rtol")) return &h->eq_rtol;
+  if (!std::strcmp(k, "eq_atol")) return &h->eq_atol;
+  if (!std::strcmp(k, "c_red")) return &h->c_red;
   if (!std::strcmp(k, "rtol")) return &h->rtol;
   if (!std::strcmp(k, "atol_n")) return &h->atol_n;
   if (!std::strcmp(k, "atol_T")) return &h->atol_T;
@@ -1040,6 +1065,8 @@ KB_API int krome_opts_get(const krome_opts* hc, const char* key, double* v) {
   }
   return -1;
 }
+
+#include "kb_queries.h"
 
 // ---------------------------------------------------------------------------
 // the solves
@@ -1351,9 +1378,11 @@ KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
 // the reference's entry point (krome.h:291-294): host arrays, in place
 KB_API int krome_solve_cells(int ncell, double* n, double* Tgas,
                              const double* dt, const double* par,
-                             int par_stride, const void* extra, int* flags,
+                             int par_stride, const krome_cells* extra, int* flags,
                              const krome_opts* h) {
-  (void)extra;  // no photon bins or dust bins in these networks
+  // extra: the per-cell photon / dust rows, read only with photon or dust
+  // bins on the handle (none here)
+  (void)extra;
   return krome_b200_solve_batch(ncell, n, Tgas, dt, par, par_stride, flags,
                                 nullptr, h);
 }
@@ -1441,7 +1470,7 @@ DevBuf g_dbuf;
 // device memory; the device fenced before and after; no host recovery
 int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
                        long ld, double* Tgas, const double* dt,
-                       const double* par, int par_stride, const void* extra,
+                       const double* par, int par_stride, const krome_cells* extra,
                        int* flags, krome_device_summary* summary,
                        const krome_opts* h) {
   if (h == nullptr || ncell < 0 || arr == nullptr || Tgas == nullptr
@@ -1541,7 +1570,7 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
 KB_API int krome_solve_cells_x(int ncell, double* x, const double* rho,
                                double* Tgas, const double* dt,
                                const double* par, int par_stride,
-                               const void* extra, int* flags,
+                               const krome_cells* extra, int* flags,
                                const krome_opts* h) {
   if (h == nullptr || ncell < 0 || x == nullptr || rho == nullptr
       || Tgas == nullptr || dt == nullptr)
@@ -1572,7 +1601,7 @@ KB_API int krome_solve_cells_x(int ncell, double* x, const double* rho,
 KB_API int krome_solve_cells_device(int ncell, double* n, int layout, long ld,
                                     double* Tgas, const double* dt,
                                     const double* par, int par_stride,
-                                    const void* extra, int* flags,
+                                    const krome_cells* extra, int* flags,
                                     krome_device_summary* summary,
                                     const krome_opts* h) {
   return solve_device_entry(ncell, n, nullptr, layout, ld, Tgas, dt, par,
@@ -1582,7 +1611,7 @@ KB_API int krome_solve_cells_device(int ncell, double* n, int layout, long ld,
 KB_API int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
                                       int layout, long ld, double* Tgas,
                                       const double* dt, const double* par,
-                                      int par_stride, const void* extra,
+                                      int par_stride, const krome_cells* extra,
                                       int* flags,
                                       krome_device_summary* summary,
                                       const krome_opts* h) {

@@ -1593,6 +1593,140 @@ class Emitter:
         body = body.replace("(void)n;", "")
         return dep(body, set())
 
+    # the reference's thermal term lists (runtime/core/solve_cell.hpp:
+    # 206-257): name, the generator's flag, and the expression this
+    # header evaluates it with (None: not emitted here)
+    HEAT_TERMS = [("CUSTOM", None, None), ("CR", "heat_CR", None),
+                  ("CHEM", "heat_chem", "heating_chem(T, n, k)"),
+                  ("DH", "heat_dH", None),
+                  ("COMPRESS", "heat_compress",
+                   "ntot_(n) * kbc::boltzmann_erg * T / p.tff"),
+                  ("VISCOUS", "heat_visc", None),
+                  ("PHOTODUST", "heat_photoDust", None),
+                  ("PHOTODUSTNET", "heat_netPhotoDust", None),
+                  ("PHOTOAV", "heat_photoAv", None), ("PHOTO", "heat_photo", None),
+                  ("ZCIE", "heat_ZCIE", None), ("NUCLEAR", "heat_nuclear", None)]
+    COOL_TERMS = [("CUSTOM", None, None),
+                  ("ATOMIC", "cool_atomic",
+                   "cooling_Atomic(T, n) + cooling_recomb_(T, n, p)"),
+                  ("H2", "cool_H2", "cooling_H2(T, n) * h2_opacity_(n)"),
+                  ("HD", "cool_HD", None), ("MOL", "cool_mol", None),
+                  ("Z", "cool_Z", None), ("Z_CIE", "cool_ZCIE", None),
+                  ("Z_EXTENDED", "cool_Zext", None), ("FLOOR", "cooling_floor", None),
+                  ("CHEM", "cool_chem", "cooling_chem(n, k)"),
+                  ("COMPTON", "cool_compton", None), ("CIE", "cool_CIE", None),
+                  ("EXPANSION", "cool_expansion", None),
+                  ("CONT", "cool_cont", "cooling_Continuum(T, n)"),
+                  ("FF", "cool_ff", None), ("DH", "cool_dH", None),
+                  ("DUST", "cool_dust", None), ("DUSTTAB", "cool_dustTab", None),
+                  ("DUSTBINS", "cool_dust_bins", None)]
+
+    def emit_interface(self):
+        """what the reference's interface reports about a network beyond
+        the solve (its query functions): reaction labels, the active
+        thermal terms one by one, reaction fluxes, the metallicity
+        scaling, the column-density estimate and the photo reactions"""
+        w = self.w
+        net, gen = self.net, self.gen
+        th = gen.thermal
+        nrea = len(net.reactions)
+
+        def label(rx):  # the equation, plus the T range of a piece
+            s = rx["eq"]
+            if rx.get("trange"):
+                s += " [%s, %s]" % tuple(self.num(v) for v in rx["trange"])
+            return s.replace("\\", "\\\\").replace('"', '\\"')
+        w("// reaction labels: the equation, and the T range of a piece")
+        w("inline const char* const reaction_names[%d] = {%s};"
+          % (max(nrea, 1), ", ".join('"%s"' % label(rx) for rx in net.reactions)))
+        # the thermal terms, active ones only, in the reference's order
+        heats = [(nm, e) for nm, f, e in self.HEAT_TERMS if f and th.get(f)]
+        cools = [(nm, e) for nm, f, e in self.COOL_TERMS if f and th.get(f)]
+        for nm, e in heats + cools:
+            if e is None:
+                raise NotImplementedError("thermal term %s" % nm)
+        w("constexpr int NHEAT = %d;" % len(heats))
+        w("constexpr int NCOOL = %d;" % len(cools))
+        w("inline const char* const heat_names[%d] = {%s};"
+          % (max(len(heats), 1), ", ".join('"%s"' % nm for nm, _ in heats) or '""'))
+        w("inline const char* const cool_names[%d] = {%s};"
+          % (max(len(cools), 1), ", ".join('"%s"' % nm for nm, _ in cools) or '""'))
+        w("// the thermal terms one by one [erg cm^-3 s^-1] at the thermal")
+        w("// temperature T with the rates k: H[NHEAT], C[NCOOL] in the order")
+        w("// of heat_names / cool_names (their sums are thermal_dTdt's)")
+        w("KB_HD inline void thermal_terms(double T, const double* n, "
+          "const double* k, const Params& p, double* H, double* C) {")
+        w("  (void)T; (void)n; (void)k; (void)p; (void)H; (void)C;")
+        for j, (_, e) in enumerate(heats):
+            w("  H[%d] = %s;" % (j, e))
+        for j, (_, e) in enumerate(cools):
+            w("  C[%d] = %s;" % (j, e))
+        w("}")
+        # reaction fluxes
+        w("// reaction fluxes k prod(n) [cm^-3 s^-1], fl[NREA]")
+        w("KB_HD inline void reaction_fluxes(const double* n, const double* k, "
+          "double* fl) {")
+        for rx in net.reactions:
+            i = rx["id"] - 1
+            w("  fl[%d] = %s;" % (i, "*".join(["k[%d]" % i]
+                                              + [self.den(s) for s in self._kin(rx)])))
+        w("}")
+        for rx in net.reactions:
+            if rx.get("qeff") or rx.get("nuclear"):
+                raise NotImplementedError("qeff / nuclear reactions")
+        # metallicity scaling (legacy krome_scale_Z): the neutral atomic
+        # metals at n_H 10^(Z + log10(n/n_H)_sun), Asplund+09
+        try:
+            solar = gen.load_solar()
+        except FileNotFoundError:
+            solar = {}
+        metals = [s for s in self.species if s in solar and s not in ("H", "He")]
+        w("// the neutral atomic metals (%s) at n_H 10^(Z + log10(n/n_H)_sun)"
+          % (", ".join(metals) or "none"))
+        w("// of the Asplund+09 photospheric abundances, floored at 1e-40")
+        w("KB_HD inline void scale_Z(double* n, double Z) {")
+        w("  (void)n; (void)Z;")
+        if metals and "H" in self.species:
+            w("  const double Htot = Hnuclei_(n);")
+            for m in metals:
+                w("  n[IDX_%s] = std::fmax(Htot * std::pow(10.0, Z + (%s)), 1e-40);"
+                  % (self.cid(m), self.num(solar[m])))
+        w("}")
+        # the column density of a number density (radiation.num2col)
+        if getattr(gen, "num2col", "default") not in ("default", None, ""):
+            raise NotImplementedError("num2col %s" % gen.num2col)
+        w("// the column density [cm^-2] of a number density x [cm^-3]")
+        w("// (the default estimator: 1.87e21 (x / 1e3)^(2/3))")
+        w("KB_HD inline double num2col_(double x) {")
+        w("  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);")
+        w("}")
+        # photo reactions (their rates need a photon field)
+        photo = []
+        for rx in net.reactions:
+            if rx["rate"]["kind"] != "photo":
+                continue
+            if rx["rate"]["xsec"]["kind"] == "h2pd":
+                raise NotImplementedError("h2pd photo channels")
+            ph = gen.resolve_photo(rx)
+            if rx["rate"].get("shield"):
+                raise NotImplementedError("shielded photo rates")
+            photo.append(ph)
+        if any(rx.get("lw") for rx in net.reactions):
+            raise NotImplementedError("J_LW rates")
+        m = len(photo)
+        w("constexpr int NPHOTO = %d;" % m)
+        w("constexpr int NLW = 0;")
+        w("inline const int photo_reaction_[%d] = {%s};"
+          % (max(m, 1), ", ".join(str(p["i"]) for p in photo) or "-1"))
+        w("inline const int photo_reactant_[%d] = {%s};"
+          % (max(m, 1), ", ".join("IDX_" + self.cid(p["reactant"]) for p in photo)
+             or "-1"))
+        w("inline const double photo_pdiss_[%d] = {%s};"
+          % (max(m, 1), ", ".join(self.num(p["rx"].get("pdiss", 1.0)) for p in photo)
+             or "1.0"))
+        w("")
+        self.photo = photo
+
     def emit_tail(self):
         th = self.gen.thermal
         any_thermal = any(th.get(f) for f in th if f.startswith(("cool_", "heat_")))
@@ -1614,6 +1748,7 @@ class Emitter:
         self.emit_jac()
         self.emit_thermal()
         self.emit_lnk_vjp()
+        self.emit_interface()
         if len(self.species) > LARGE_NSPEC:
             self.emit_rate_parts()
             self.emit_sparse()

@@ -1376,6 +1376,101 @@ KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Pa
   g[63] += flux * (mu[IDX_H3j] + mu[IDX_D] - mu[IDX_H2Dj] - mu[IDX_H]);
 }
 
+// reaction labels: the equation, and the T range of a piece
+inline const char* const reaction_names[64] = {"H+ + e- -> H", "H -> H+ + e-", "H + e- -> H-", "H- -> H + e-", "H- + H -> H2 + e- [0.0, 300.0]", "H- + H -> H2 + e- [300.0, INFINITY]", "H- + H+ -> H2+ + e- [0.0, 8000.0]", "H- + H+ -> H2+ + e- [8000.0, INFINITY]", "H- + H+ -> H + H", "H + H+ -> H2+", "H2+ -> H + H+", "H2+ + H -> H2 + H+", "H2+ + e- -> H + H", "H2+ -> H+ + H+ + e-", "H2+ + H2 -> H3+ + H", "H2 + H+ -> H2+ + H [0.0, 10000.0]", "H2 + H+ -> H2+ + H [10000.0, INFINITY]", "H2 + e- -> H + H-", "H2 + e- -> H + H + e-", "H2 -> H2+ + e-", "H3+ + H -> H2+ + H2", "H3+ + e- -> H2 + H", "H2 + H+ -> H3+", "He++ + e- -> He+", "He+ -> He++ + e-", "He+ + e- -> He", "He -> He+ + e-", "He + H+ -> He+ + H [10000.0, INFINITY]", "He+ + H -> He + H+ [6000.0, INFINITY]", "He + H+ -> HeH+ [0.0, 1000.0]", "He + H+ -> HeH+ [1000.0, INFINITY]", "He + H2+ -> HeH+ + H", "He+ + H -> HeH+ [0.0, 4000.0]", "He+ + H -> HeH+ [4000.0, INFINITY]", "HeH+ + H -> He + H2+", "HeH+ + e- -> He + H", "HeH+ + H2 -> H3+ + He", "HeH+ -> He + H+", "HeH+ -> He+ + H", "D+ + e- -> D", "D -> D+ + e-", "D + H+ -> D+ + H", "D+ + H -> D + H+", "D + H -> HD", "D + H2 -> H + HD [250.0, INFINITY]", "HD+ + H -> H+ + HD", "D+ + H2 -> H+ + HD", "HD + H -> H2 + D [200.0, INFINITY]", "HD + H+ -> H2 + D+", "HD + H3+ -> H2 + H2D+", "D + H+ -> HD+", "D+ + H -> HD+", "HD+ -> H + D+", "HD+ -> H+ + D", "HD+ + e- -> H + D", "HD+ + H2 -> H2D+ + H", "HD+ + H2 -> H3+ + D", "D + H3+ -> H2D+ + H", "H2D+ + e- -> H + H + D", "H2D+ + e- -> H2 + D", "H2D+ + e- -> HD + H", "H2D+ + H2 -> H3+ + HD [0.0, 100.0]", "H2D+ + H2 -> H3+ + HD [100.0, INFINITY]", "H2D+ + H -> H3+ + D"};
+constexpr int NHEAT = 0;
+constexpr int NCOOL = 0;
+inline const char* const heat_names[1] = {""};
+inline const char* const cool_names[1] = {""};
+// the thermal terms one by one [erg cm^-3 s^-1] at the thermal
+// temperature T with the rates k: H[NHEAT], C[NCOOL] in the order
+// of heat_names / cool_names (their sums are thermal_dTdt's)
+KB_HD inline void thermal_terms(double T, const double* n, const double* k, const Params& p, double* H, double* C) {
+  (void)T; (void)n; (void)k; (void)p; (void)H; (void)C;
+}
+// reaction fluxes k prod(n) [cm^-3 s^-1], fl[NREA]
+KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) {
+  fl[0] = k[0]*n[IDX_Hj]*n[IDX_E];
+  fl[1] = k[1]*n[IDX_H];
+  fl[2] = k[2]*n[IDX_H]*n[IDX_E];
+  fl[3] = k[3]*n[IDX_Hk];
+  fl[4] = k[4]*n[IDX_Hk]*n[IDX_H];
+  fl[5] = k[5]*n[IDX_Hk]*n[IDX_H];
+  fl[6] = k[6]*n[IDX_Hk]*n[IDX_Hj];
+  fl[7] = k[7]*n[IDX_Hk]*n[IDX_Hj];
+  fl[8] = k[8]*n[IDX_Hk]*n[IDX_Hj];
+  fl[9] = k[9]*n[IDX_H]*n[IDX_Hj];
+  fl[10] = k[10]*n[IDX_H2j];
+  fl[11] = k[11]*n[IDX_H2j]*n[IDX_H];
+  fl[12] = k[12]*n[IDX_H2j]*n[IDX_E];
+  fl[13] = k[13]*n[IDX_H2j];
+  fl[14] = k[14]*n[IDX_H2j]*n[IDX_H2];
+  fl[15] = k[15]*n[IDX_H2]*n[IDX_Hj];
+  fl[16] = k[16]*n[IDX_H2]*n[IDX_Hj];
+  fl[17] = k[17]*n[IDX_H2]*n[IDX_E];
+  fl[18] = k[18]*n[IDX_H2]*n[IDX_E];
+  fl[19] = k[19]*n[IDX_H2];
+  fl[20] = k[20]*n[IDX_H3j]*n[IDX_H];
+  fl[21] = k[21]*n[IDX_H3j]*n[IDX_E];
+  fl[22] = k[22]*n[IDX_H2]*n[IDX_Hj];
+  fl[23] = k[23]*n[IDX_Hejj]*n[IDX_E];
+  fl[24] = k[24]*n[IDX_Hej];
+  fl[25] = k[25]*n[IDX_Hej]*n[IDX_E];
+  fl[26] = k[26]*n[IDX_He];
+  fl[27] = k[27]*n[IDX_He]*n[IDX_Hj];
+  fl[28] = k[28]*n[IDX_Hej]*n[IDX_H];
+  fl[29] = k[29]*n[IDX_He]*n[IDX_Hj];
+  fl[30] = k[30]*n[IDX_He]*n[IDX_Hj];
+  fl[31] = k[31]*n[IDX_He]*n[IDX_H2j];
+  fl[32] = k[32]*n[IDX_Hej]*n[IDX_H];
+  fl[33] = k[33]*n[IDX_Hej]*n[IDX_H];
+  fl[34] = k[34]*n[IDX_HeHj]*n[IDX_H];
+  fl[35] = k[35]*n[IDX_HeHj]*n[IDX_E];
+  fl[36] = k[36]*n[IDX_HeHj]*n[IDX_H2];
+  fl[37] = k[37]*n[IDX_HeHj];
+  fl[38] = k[38]*n[IDX_HeHj];
+  fl[39] = k[39]*n[IDX_Dj]*n[IDX_E];
+  fl[40] = k[40]*n[IDX_D];
+  fl[41] = k[41]*n[IDX_D]*n[IDX_Hj];
+  fl[42] = k[42]*n[IDX_Dj]*n[IDX_H];
+  fl[43] = k[43]*n[IDX_D]*n[IDX_H];
+  fl[44] = k[44]*n[IDX_D]*n[IDX_H2];
+  fl[45] = k[45]*n[IDX_HDj]*n[IDX_H];
+  fl[46] = k[46]*n[IDX_Dj]*n[IDX_H2];
+  fl[47] = k[47]*n[IDX_HD]*n[IDX_H];
+  fl[48] = k[48]*n[IDX_HD]*n[IDX_Hj];
+  fl[49] = k[49]*n[IDX_HD]*n[IDX_H3j];
+  fl[50] = k[50]*n[IDX_D]*n[IDX_Hj];
+  fl[51] = k[51]*n[IDX_Dj]*n[IDX_H];
+  fl[52] = k[52]*n[IDX_HDj];
+  fl[53] = k[53]*n[IDX_HDj];
+  fl[54] = k[54]*n[IDX_HDj]*n[IDX_E];
+  fl[55] = k[55]*n[IDX_HDj]*n[IDX_H2];
+  fl[56] = k[56]*n[IDX_HDj]*n[IDX_H2];
+  fl[57] = k[57]*n[IDX_D]*n[IDX_H3j];
+  fl[58] = k[58]*n[IDX_H2Dj]*n[IDX_E];
+  fl[59] = k[59]*n[IDX_H2Dj]*n[IDX_E];
+  fl[60] = k[60]*n[IDX_H2Dj]*n[IDX_E];
+  fl[61] = k[61]*n[IDX_H2Dj]*n[IDX_H2];
+  fl[62] = k[62]*n[IDX_H2Dj]*n[IDX_H2];
+  fl[63] = k[63]*n[IDX_H2Dj]*n[IDX_H];
+}
+// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// of the Asplund+09 photospheric abundances, floored at 1e-40
+KB_HD inline void scale_Z(double* n, double Z) {
+  (void)n; (void)Z;
+}
+// the column density [cm^-2] of a number density x [cm^-3]
+// (the default estimator: 1.87e21 (x / 1e3)^(2/3))
+KB_HD inline double num2col_(double x) {
+  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+}
+constexpr int NPHOTO = 0;
+constexpr int NLW = 0;
+inline const int photo_reaction_[1] = {-1};
+inline const int photo_reactant_[1] = {-1};
+inline const double photo_pdiss_[1] = {1.0};
+
 constexpr bool HAS_THERMAL_TERMS = false;
 // a rate coefficient depends on the densities (the species block
 // of jac_stoich, taken at fixed k, is then not the exact dF/dn)

@@ -1166,6 +1166,79 @@ KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Pa
   }
 }
 
+// reaction labels: the equation, and the T range of a piece
+inline const char* const reaction_names[38] = {"H + e- -> H+ + e- + e-", "H+ + e- -> H [0.0, 5500.0]", "H+ + e- -> H [5500.0, INFINITY]", "He + e- -> He+ + e- + e-", "He+ + e- -> He [0.0, 9280.0]", "He+ + e- -> He [9280.0, INFINITY]", "He+ + e- -> He++ + e- + e-", "He++ + e- -> He+", "H + e- -> H-", "H- + H -> H2 + e- [0.0, 1160.0]", "H- + H -> H2 + e- [1160.0, INFINITY]", "H + H+ -> H2+ [0.0, 6700.0]", "H + H+ -> H2+ [6700.0, INFINITY]", "H2+ + H -> H2 + H+", "H2 + H+ -> H2+ + H [3480.0, INFINITY]", "H2 + e- -> H + H + e-", "H2 + H -> H + H + H", "H- + e- -> H + e- + e-", "H- + H -> H + H + e- [0.0, 1160.0]", "H- + H -> H + H + e- [1160.0, INFINITY]", "H- + H+ -> H + H", "H- + H+ -> H2+ + e-", "H2+ + e- -> H + H [0.0, 617.0]", "H2+ + e- -> H + H [617.0, INFINITY]", "H2+ + H- -> H + H2", "H + H + H -> H2 + H [0.0, 300.0]", "H + H + H -> H2 + H [300.0, INFINITY]", "H2 + H + H -> H2 + H2 [0.0, 300.0]", "H2 + H + H -> H2 + H2 [300.0, INFINITY]", "H+ + D -> H + D+ [50.0, INFINITY]", "H + D+ -> H+ + D [50.0, INFINITY]", "H2 + D+ -> HD + H+", "HD + H+ -> H2 + D+", "H2 + D -> HD + H [0.0, 2000.0]", "H2 + D -> HD + H [2000.0, INFINITY]", "HD + H -> H2 + D [200.0, INFINITY]", "D + H- -> HD + e-", "D+ + e- -> D"};
+constexpr int NHEAT = 2;
+constexpr int NCOOL = 2;
+inline const char* const heat_names[2] = {"CHEM", "COMPRESS"};
+inline const char* const cool_names[2] = {"ATOMIC", "H2"};
+// the thermal terms one by one [erg cm^-3 s^-1] at the thermal
+// temperature T with the rates k: H[NHEAT], C[NCOOL] in the order
+// of heat_names / cool_names (their sums are thermal_dTdt's)
+KB_HD inline void thermal_terms(double T, const double* n, const double* k, const Params& p, double* H, double* C) {
+  (void)T; (void)n; (void)k; (void)p; (void)H; (void)C;
+  H[0] = heating_chem(T, n, k);
+  H[1] = ntot_(n) * kbc::boltzmann_erg * T / p.tff;
+  C[0] = cooling_Atomic(T, n) + cooling_recomb_(T, n, p);
+  C[1] = cooling_H2(T, n) * h2_opacity_(n);
+}
+// reaction fluxes k prod(n) [cm^-3 s^-1], fl[NREA]
+KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) {
+  fl[0] = k[0]*n[IDX_H]*n[IDX_E];
+  fl[1] = k[1]*n[IDX_Hj]*n[IDX_E];
+  fl[2] = k[2]*n[IDX_Hj]*n[IDX_E];
+  fl[3] = k[3]*n[IDX_He]*n[IDX_E];
+  fl[4] = k[4]*n[IDX_Hej]*n[IDX_E];
+  fl[5] = k[5]*n[IDX_Hej]*n[IDX_E];
+  fl[6] = k[6]*n[IDX_Hej]*n[IDX_E];
+  fl[7] = k[7]*n[IDX_Hejj]*n[IDX_E];
+  fl[8] = k[8]*n[IDX_H]*n[IDX_E];
+  fl[9] = k[9]*n[IDX_Hk]*n[IDX_H];
+  fl[10] = k[10]*n[IDX_Hk]*n[IDX_H];
+  fl[11] = k[11]*n[IDX_H]*n[IDX_Hj];
+  fl[12] = k[12]*n[IDX_H]*n[IDX_Hj];
+  fl[13] = k[13]*n[IDX_H2j]*n[IDX_H];
+  fl[14] = k[14]*n[IDX_H2]*n[IDX_Hj];
+  fl[15] = k[15]*n[IDX_H2]*n[IDX_E];
+  fl[16] = k[16]*n[IDX_H2]*n[IDX_H];
+  fl[17] = k[17]*n[IDX_Hk]*n[IDX_E];
+  fl[18] = k[18]*n[IDX_Hk]*n[IDX_H];
+  fl[19] = k[19]*n[IDX_Hk]*n[IDX_H];
+  fl[20] = k[20]*n[IDX_Hk]*n[IDX_Hj];
+  fl[21] = k[21]*n[IDX_Hk]*n[IDX_Hj];
+  fl[22] = k[22]*n[IDX_H2j]*n[IDX_E];
+  fl[23] = k[23]*n[IDX_H2j]*n[IDX_E];
+  fl[24] = k[24]*n[IDX_H2j]*n[IDX_Hk];
+  fl[25] = k[25]*n[IDX_H]*n[IDX_H]*n[IDX_H];
+  fl[26] = k[26]*n[IDX_H]*n[IDX_H]*n[IDX_H];
+  fl[27] = k[27]*n[IDX_H2]*n[IDX_H]*n[IDX_H];
+  fl[28] = k[28]*n[IDX_H2]*n[IDX_H]*n[IDX_H];
+  fl[29] = k[29]*n[IDX_Hj]*n[IDX_D];
+  fl[30] = k[30]*n[IDX_H]*n[IDX_Dj];
+  fl[31] = k[31]*n[IDX_H2]*n[IDX_Dj];
+  fl[32] = k[32]*n[IDX_HD]*n[IDX_Hj];
+  fl[33] = k[33]*n[IDX_H2]*n[IDX_D];
+  fl[34] = k[34]*n[IDX_H2]*n[IDX_D];
+  fl[35] = k[35]*n[IDX_HD]*n[IDX_H];
+  fl[36] = k[36]*n[IDX_D]*n[IDX_Hk];
+  fl[37] = k[37]*n[IDX_Dj]*n[IDX_E];
+}
+// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// of the Asplund+09 photospheric abundances, floored at 1e-40
+KB_HD inline void scale_Z(double* n, double Z) {
+  (void)n; (void)Z;
+}
+// the column density [cm^-2] of a number density x [cm^-3]
+// (the default estimator: 1.87e21 (x / 1e3)^(2/3))
+KB_HD inline double num2col_(double x) {
+  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+}
+constexpr int NPHOTO = 0;
+constexpr int NLW = 0;
+inline const int photo_reaction_[1] = {-1};
+inline const int photo_reactant_[1] = {-1};
+inline const double photo_pdiss_[1] = {1.0};
+
 constexpr bool HAS_THERMAL_TERMS = true;
 // a rate coefficient depends on the densities (the species block
 // of jac_stoich, taken at fixed k, is then not the exact dF/dn)

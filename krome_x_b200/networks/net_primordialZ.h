@@ -1792,6 +1792,114 @@ KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Pa
   g[73] += flux * (mu[IDX_C] + mu[IDX_O] - mu[IDX_COj] - mu[IDX_E]);
 }
 
+// reaction labels: the equation, and the T range of a piece
+inline const char* const reaction_names[74] = {"H + e- -> H+ + e- + e-", "H+ + e- -> H [0.0, 5500.0]", "H+ + e- -> H [5500.0, INFINITY]", "He + e- -> He+ + e- + e-", "He+ + e- -> He [0.0, 9280.0]", "He+ + e- -> He [9280.0, INFINITY]", "He+ + e- -> He++ + e- + e-", "He++ + e- -> He+", "H + e- -> H-", "H- + H -> H2 + e-", "H + H+ -> H2+ [0.0, 30.0]", "H + H+ -> H2+ [30.0, INFINITY]", "H2+ + H -> H2 + H+", "H2 + H+ -> H2+ + H [100.0, 30000.0]", "H2 + e- -> H + H-", "H2 + e- -> H + H + e-", "H2 + H -> H + H + H", "H- + e- -> H + e- + e-", "H- + H -> H + H + e- [0.0, 1160.0]", "H- + H -> H + H + e- [1160.0, INFINITY]", "H- + H+ -> H + H", "H- + H+ -> H2+ + e-", "H2+ + e- -> H + H", "H2+ + H- -> H + H2", "H + H + H -> H2 + H", "H2 + H + H -> H2 + H2", "H2 + H2 -> H + H + H2", "He+ + H -> He + H+", "He + H+ -> He+ + H [0.0, 10000.0]", "He + H+ -> He+ + H [10000.0, INFINITY]", "O+ + H -> H+ + O", "H+ + O -> O+ + H", "O+ + H2 -> OH+ + H", "OH+ + H2 -> H2O+ + H", "H2O+ + H2 -> H3O+ + H", "H2O+ + e- -> O + H2", "H2O+ + e- -> OH + H", "H3O+ + e- -> H2O + H", "O + H -> OH", "O + H2 -> OH + H", "H2 + OH -> H2O + H", "OH + OH -> H2O + O", "H+ + OH -> OH+ + H", "H+ + H2O -> H2O+ + H", "H + OH -> H2 + O", "H + H2O -> OH + H2", "O + O -> O2", "O + OH -> O2 + H", "H + O2 -> OH + O", "H+ + O2 -> O2+ + H", "O2+ + e- -> O + O", "O + CH -> CO + H", "C + OH -> CO + H", "C + O2 -> CO + O", "C+ + O2 -> O+ + CO", "OH + CO -> CO2 + H", "C+ + e- -> C", "C+ + OH -> CO+ + H", "CO+ + H -> H+ + CO", "C + H -> CH", "C + H2 -> CH + H", "H + CH -> C + H2", "H2 + CH -> CH2 + H", "H + CH2 -> CH + H2", "H2 + CH2 -> CH3 + H", "H + CH3 -> CH2 + H2", "H2 + CH3 -> CH4 + H", "H + CH4 -> H2 + CH3", "H2 + C -> CH2", "H3O+ + e- -> OH + H + H", "OH+ + e- -> O + H", "O+ + e- -> O", "CO+ + e- -> CO", "CO+ + e- -> C + O"};
+constexpr int NHEAT = 0;
+constexpr int NCOOL = 0;
+inline const char* const heat_names[1] = {""};
+inline const char* const cool_names[1] = {""};
+// the thermal terms one by one [erg cm^-3 s^-1] at the thermal
+// temperature T with the rates k: H[NHEAT], C[NCOOL] in the order
+// of heat_names / cool_names (their sums are thermal_dTdt's)
+KB_HD inline void thermal_terms(double T, const double* n, const double* k, const Params& p, double* H, double* C) {
+  (void)T; (void)n; (void)k; (void)p; (void)H; (void)C;
+}
+// reaction fluxes k prod(n) [cm^-3 s^-1], fl[NREA]
+KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) {
+  fl[0] = k[0]*n[IDX_H]*n[IDX_E];
+  fl[1] = k[1]*n[IDX_Hj]*n[IDX_E];
+  fl[2] = k[2]*n[IDX_Hj]*n[IDX_E];
+  fl[3] = k[3]*n[IDX_He]*n[IDX_E];
+  fl[4] = k[4]*n[IDX_Hej]*n[IDX_E];
+  fl[5] = k[5]*n[IDX_Hej]*n[IDX_E];
+  fl[6] = k[6]*n[IDX_Hej]*n[IDX_E];
+  fl[7] = k[7]*n[IDX_Hejj]*n[IDX_E];
+  fl[8] = k[8]*n[IDX_H]*n[IDX_E];
+  fl[9] = k[9]*n[IDX_Hk]*n[IDX_H];
+  fl[10] = k[10]*n[IDX_H]*n[IDX_Hj];
+  fl[11] = k[11]*n[IDX_H]*n[IDX_Hj];
+  fl[12] = k[12]*n[IDX_H2j]*n[IDX_H];
+  fl[13] = k[13]*n[IDX_H2]*n[IDX_Hj];
+  fl[14] = k[14]*n[IDX_H2]*n[IDX_E];
+  fl[15] = k[15]*n[IDX_H2]*n[IDX_E];
+  fl[16] = k[16]*n[IDX_H2]*n[IDX_H];
+  fl[17] = k[17]*n[IDX_Hk]*n[IDX_E];
+  fl[18] = k[18]*n[IDX_Hk]*n[IDX_H];
+  fl[19] = k[19]*n[IDX_Hk]*n[IDX_H];
+  fl[20] = k[20]*n[IDX_Hk]*n[IDX_Hj];
+  fl[21] = k[21]*n[IDX_Hk]*n[IDX_Hj];
+  fl[22] = k[22]*n[IDX_H2j]*n[IDX_E];
+  fl[23] = k[23]*n[IDX_H2j]*n[IDX_Hk];
+  fl[24] = k[24]*n[IDX_H]*n[IDX_H]*n[IDX_H];
+  fl[25] = k[25]*n[IDX_H2]*n[IDX_H]*n[IDX_H];
+  fl[26] = k[26]*n[IDX_H2]*n[IDX_H2];
+  fl[27] = k[27]*n[IDX_Hej]*n[IDX_H];
+  fl[28] = k[28]*n[IDX_He]*n[IDX_Hj];
+  fl[29] = k[29]*n[IDX_He]*n[IDX_Hj];
+  fl[30] = k[30]*n[IDX_Oj]*n[IDX_H];
+  fl[31] = k[31]*n[IDX_Hj]*n[IDX_O];
+  fl[32] = k[32]*n[IDX_Oj]*n[IDX_H2];
+  fl[33] = k[33]*n[IDX_OHj]*n[IDX_H2];
+  fl[34] = k[34]*n[IDX_H2Oj]*n[IDX_H2];
+  fl[35] = k[35]*n[IDX_H2Oj]*n[IDX_E];
+  fl[36] = k[36]*n[IDX_H2Oj]*n[IDX_E];
+  fl[37] = k[37]*n[IDX_H3Oj]*n[IDX_E];
+  fl[38] = k[38]*n[IDX_O]*n[IDX_H];
+  fl[39] = k[39]*n[IDX_O]*n[IDX_H2];
+  fl[40] = k[40]*n[IDX_H2]*n[IDX_OH];
+  fl[41] = k[41]*n[IDX_OH]*n[IDX_OH];
+  fl[42] = k[42]*n[IDX_Hj]*n[IDX_OH];
+  fl[43] = k[43]*n[IDX_Hj]*n[IDX_H2O];
+  fl[44] = k[44]*n[IDX_H]*n[IDX_OH];
+  fl[45] = k[45]*n[IDX_H]*n[IDX_H2O];
+  fl[46] = k[46]*n[IDX_O]*n[IDX_O];
+  fl[47] = k[47]*n[IDX_O]*n[IDX_OH];
+  fl[48] = k[48]*n[IDX_H]*n[IDX_O2];
+  fl[49] = k[49]*n[IDX_Hj]*n[IDX_O2];
+  fl[50] = k[50]*n[IDX_O2j]*n[IDX_E];
+  fl[51] = k[51]*n[IDX_O]*n[IDX_CH];
+  fl[52] = k[52]*n[IDX_C]*n[IDX_OH];
+  fl[53] = k[53]*n[IDX_C]*n[IDX_O2];
+  fl[54] = k[54]*n[IDX_Cj]*n[IDX_O2];
+  fl[55] = k[55]*n[IDX_OH]*n[IDX_CO];
+  fl[56] = k[56]*n[IDX_Cj]*n[IDX_E];
+  fl[57] = k[57]*n[IDX_Cj]*n[IDX_OH];
+  fl[58] = k[58]*n[IDX_COj]*n[IDX_H];
+  fl[59] = k[59]*n[IDX_C]*n[IDX_H];
+  fl[60] = k[60]*n[IDX_C]*n[IDX_H2];
+  fl[61] = k[61]*n[IDX_H]*n[IDX_CH];
+  fl[62] = k[62]*n[IDX_H2]*n[IDX_CH];
+  fl[63] = k[63]*n[IDX_H]*n[IDX_CH2];
+  fl[64] = k[64]*n[IDX_H2]*n[IDX_CH2];
+  fl[65] = k[65]*n[IDX_H]*n[IDX_CH3];
+  fl[66] = k[66]*n[IDX_H2]*n[IDX_CH3];
+  fl[67] = k[67]*n[IDX_H]*n[IDX_CH4];
+  fl[68] = k[68]*n[IDX_H2]*n[IDX_C];
+  fl[69] = k[69]*n[IDX_H3Oj]*n[IDX_E];
+  fl[70] = k[70]*n[IDX_OHj]*n[IDX_E];
+  fl[71] = k[71]*n[IDX_Oj]*n[IDX_E];
+  fl[72] = k[72]*n[IDX_COj]*n[IDX_E];
+  fl[73] = k[73]*n[IDX_COj]*n[IDX_E];
+}
+// the neutral atomic metals (C, O) at n_H 10^(Z + log10(n/n_H)_sun)
+// of the Asplund+09 photospheric abundances, floored at 1e-40
+KB_HD inline void scale_Z(double* n, double Z) {
+  (void)n; (void)Z;
+  const double Htot = Hnuclei_(n);
+  n[IDX_C] = std::fmax(Htot * std::pow(10.0, Z + (-3.5700000000000003)), 1e-40);
+  n[IDX_O] = std::fmax(Htot * std::pow(10.0, Z + (-3.3100000000000005)), 1e-40);
+}
+// the column density [cm^-2] of a number density x [cm^-3]
+// (the default estimator: 1.87e21 (x / 1e3)^(2/3))
+KB_HD inline double num2col_(double x) {
+  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+}
+constexpr int NPHOTO = 0;
+constexpr int NLW = 0;
+inline const int photo_reaction_[1] = {-1};
+inline const int photo_reactant_[1] = {-1};
+inline const double photo_pdiss_[1] = {1.0};
+
 constexpr bool HAS_THERMAL_TERMS = false;
 // a rate coefficient depends on the densities (the species block
 // of jac_stoich, taken at fixed k, is then not the exact dF/dn)
