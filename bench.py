@@ -91,6 +91,21 @@ def parse():
                          "that keeps the run within minutes)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the adjoint and precision forms")
+    # one solve of a workload, outside the benchmark's timing: the command a
+    # profiler wraps to capture a single kernel launch
+    ap.add_argument("--case", default=None, metavar="NETWORK",
+                    help="run one workload of NETWORK and print its time")
+    ap.add_argument("--case-cells", type=int, default=65536)
+    ap.add_argument("--calls", type=int, default=1,
+                    help="--case: steps of the collapse loop")
+    ap.add_argument("--layout", default="lane", choices=["lane", "warp"])
+    ap.add_argument("--kernel", default="persistent",
+                    choices=["persistent", "plain"])
+    ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--lu32", action="store_true")
+    ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--dt", type=float, default=None,
+                    help="--case: every cell's time step")
     return ap.parse_args()
 
 
@@ -406,7 +421,7 @@ def precision_form(torch, dev):
 
 # the large-network form: DRAM bytes (read + write) of its solve kernel per
 # integration step, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of `python -m krome_x_b200.run semenov 148 --dt
+# dram__bytes_write.sum) of `python bench.py --case semenov --case-cells 148 --dt
 # 3.15e9` (154,747 steps: 2.29 + 6.27 GB); the per-cell workspace (~600 KB)
 # stays in L2
 SEMENOV_DRAM_PER_STEP = 8.57e9 / 154747
@@ -674,8 +689,61 @@ def run_ours(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """--case: one workload through the public API, timed on the host (a
+    profiler's capture target; not a benchmark line). With --calls > 1 the
+    collapse driver's hydro loop on the host arrays; with --adjoint the
+    discrete adjoint through the torch.autograd wrapper."""
+    from krome_x_b200 import krome, netinfo, workloads
+    info = netinfo.load(args.case)
+    n, T, dt, par = workloads.GENERATORS[args.case](args.case_cells, info,
+                                                    seed=args.seed)
+    if args.dt is not None:
+        dt[:] = args.dt
+    o = workloads.OPTIONS[args.case]
+    net = krome.load(args.case)
+    opts = net.options(evolve_T=o["evolve_T"], jac=o["jac"], rtol=o["rtol"],
+                       atol_n=o["atol_n"], atol_T=o["atol_T"],
+                       kernel=args.kernel,
+                       layout=0 if args.layout == "warp" else 1,
+                       lu32=int(args.lu32), max_steps=o.get("max_steps", 100000))
+    out = {"case": args.case, "cells": args.case_cells, "calls": args.calls}
+    if args.adjoint:
+        import torch
+        from krome_x_b200 import autograd
+        dev = torch.device("cuda:0")
+        t = lambda x: torch.tensor(x, dtype=torch.float64, device=dev)
+        n0, T0 = t(n).requires_grad_(), t(T).requires_grad_()
+        m = torch.zeros(net.nrea, dtype=torch.float64, device=dev,
+                        requires_grad=True)
+        t0 = time.perf_counter()
+        nout, Tout, flags = autograd.solve(net, n0, T0, m, t(dt), t(par), opts)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        (nout[:, info["species"].index("H2")].sum() + Tout.sum()).backward()
+        torch.cuda.synchronize()
+        out.update(forward_s=t1 - t0, reverse_s=time.perf_counter() - t1,
+                   failed=int((flags != 0).sum()))
+    else:
+        failed = 0
+        t0 = time.perf_counter()
+        for c in range(args.calls):
+            if c > 0:
+                dt = workloads.hydro_step_info(n, par, info)
+            r = net.solve_batch(n, T, dt, par, opts=opts, check=False)
+            n, T = r.n, r.Tgas
+            failed += int((r.flags != 0).sum())
+        el = time.perf_counter() - t0
+        out.update(seconds=el, cell_solves_per_s=args.case_cells * args.calls / el,
+                   failed=failed)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.case is not None:
+        run_case(args)
+        return
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)

@@ -84,8 +84,17 @@ CHEM_LEDGER = [
 ]
 
 
+_REFERENCE = None  # set by main()'s --reference
+
+
 def _reference_root():
-    return Path(os.environ.get("KROME_REFERENCE", "/root/reference"))
+    """the reference tree, whose generator frontend parses the network:
+    --reference PATH, or the KROME_REFERENCE environment variable"""
+    ref = _REFERENCE or os.environ.get("KROME_REFERENCE")
+    if not ref:
+        raise RuntimeError("the emitter needs the reference tree: pass "
+                           "--reference PATH or set KROME_REFERENCE")
+    return Path(ref)
 
 
 def _frontend(cfg):
@@ -1770,6 +1779,11 @@ def emit(key):
 
 
 def main(argv):
+    global _REFERENCE
+    if "--reference" in argv:
+        i = argv.index("--reference")
+        _REFERENCE = argv[i + 1]
+        argv = argv[:i] + argv[i + 2:]
     keys = argv or list(NETWORKS)
     for k in keys:
         print("wrote", emit(k))

@@ -36,6 +36,8 @@ import sys
 import time
 from pathlib import Path
 
+# the reference tree: KROME_REFERENCE, else its mount point in the build
+# container (this recipe is the one place that names it)
 REF = Path(os.environ.get("KROME_REFERENCE", "/root/reference"))
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
