@@ -3,6 +3,7 @@
 Markers: ``gpu`` for tests that need a CUDA device (run on the B200 host with
 ``pytest -m gpu``); everything else runs on the CPU (``-m "not gpu"``).
 """
+import json
 import sys
 from pathlib import Path
 
@@ -17,6 +18,31 @@ NETWORKS = ("primordial", "primordial3", "galaxy_ism")
 # networks past the dense kernels' size, solved by the sparse path
 LARGE = ("semenov",)
 ALL_NETWORKS = NETWORKS + LARGE
+
+
+# the oracle's one-ulp noise floor of each parity case (tests/golden/
+# noise_floor.py): the smallest fraction of passing cells and the worst
+# cell's relative error over five draws of one-ulp input moves
+NOISE_FLOOR = json.loads((ROOT / "tests" / "golden" / "noise_floor.json").read_text())
+# the bars against the floor: the fraction may fall 0.03 below it (a batch
+# of 512 cells has a sampling spread of about that size); the worst cell may
+# reach three times the floor's (the GPU's CUDA math and contraction move
+# many last bits at once: one more draw of the same chaotic amplification,
+# and the maximum of five draws itself moves by up to 1.5x between sets of
+# draws)
+FRAC_MARGIN = 0.03
+WORST_FACTOR = 3.0
+
+
+def assert_at_floor(m, case):
+    """the parity metric m of a GPU solve against the oracle's floor of
+    `case`: flags equal, the fraction of passing cells and the worst cell
+    (abundances and Tgas) at the floor"""
+    f = NOISE_FLOOR[case]
+    assert m["flags_equal"] == 1.0, (case, m)
+    assert m["frac"] >= f["frac"] - FRAC_MARGIN, (case, m, f)
+    assert m["max_rel"] <= WORST_FACTOR * f["max_rel"], (case, m, f)
+    assert m["max_relT"] <= max(WORST_FACTOR * f["max_relT"], 1e-12), (case, m, f)
 
 
 def pytest_configure(config):

@@ -5,21 +5,23 @@ multiply-adds, so its last bits differ from the host's; CVODE's step and
 order decisions amplify last-bit differences chaotically. The bar is
 therefore the benchmark's metric (conftest.parity): every abundance above
 atol/rtol and Tgas within 10 rtol, per cell, on the cells where both
-succeed; the fraction of passing cells must reach the reference's own
-noise floor -- the same metric between the oracle and the oracle with
-every input moved by one ulp: 97.9 % (primordial), 93.0 % (primordial3),
-98.8 % (galaxy_ism) on 1024 cells -- less a small margin. Flags must agree
-on every cell, and no cell may be off grossly (1e-3)."""
+succeed; the fraction of passing cells and the worst cell must sit at the
+reference's own noise floor -- the same metric between the oracle and the
+oracle with every input moved by one ulp, measured per case by
+tests/golden/noise_floor.py (conftest.assert_at_floor). Flags must agree on
+every cell."""
 import numpy as np
 import pytest
 
-from conftest import NETWORKS, golden, parity
+from conftest import (FRAC_MARGIN, NETWORKS, NOISE_FLOOR, assert_at_floor,
+                      golden, parity)
 from krome_x_b200 import krome, netinfo, workloads
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-FLOOR = {"primordial": 0.95, "primordial3": 0.89, "galaxy_ism": 0.96}
+FLOOR = {k: NOISE_FLOOR["%s/first/512/3" % k]["frac"] - FRAC_MARGIN
+         for k in NETWORKS}
 LAYOUTS = [("lane", "persistent"), ("lane", "plain"), ("warp", "persistent"),
            ("warp", "plain")]
 
@@ -48,9 +50,7 @@ def test_parity_with_oracle(case, layout, kernel):
                         check=False, stats=True)
     m = parity(r.n, r.Tgas, r.flags, ref["n"], ref["T"], ref["flags"],
                workloads.OPTIONS[key]["rtol"])
-    assert m["flags_equal"] == 1.0, m
-    assert m["frac"] >= FLOOR[key], m
-    assert m["max_rel"] < 1e-3 and m["max_relT"] < 1e-3, m
+    assert_at_floor(m, "%s/first/512/3" % key)
     # the integrator makes the reference's decisions: its counters agree
     # with the oracle's to within the chaotic spread
     g, c = r.stats.mean(axis=0), ref["stats"].mean(axis=0)
@@ -195,21 +195,22 @@ def test_device_resident_api_and_hydro_graph():
     host = net.solve_batch(n, T, dt, par, opts=opts, check=False)
     np.testing.assert_array_equal(n_d.cpu().numpy(), host.n)
     np.testing.assert_array_equal(fl.cpu().numpy(), host.flags)
-    # three captured hydro steps against three host steps
+    # three captured hydro steps, each equal bit for bit to the host-array
+    # solve of the same inputs: the densities x 1.01 (an exact product on
+    # both sides) with the dt and tff the captured step wrote
     n_d, T_d, dt_d, par_d = t(n), t(T), t(dt), t(par)
     g = net.hydro_graph(n_d, T_d, dt_d, par_d, fl, opts)
-    nh, Th, parh = n.copy(), T.copy(), par.copy()
     for _ in range(3):
-        g.launch()
-        dth = workloads.hydro_step_info(nh, parh, info)
-        r = net.solve_batch(nh, Th, dth, parh, opts=opts, check=False)
-        nh, Th = r.n, r.Tgas
-    torch.cuda.synchronize()
+        n0, T0 = n_d.cpu().numpy(), T_d.cpu().numpy()
+        with torch.cuda.stream(g.stream):
+            g.launch()
+        torch.cuda.synchronize()
+        r = net.solve_batch(n0 * 1.01, T0, dt_d.cpu().numpy(),
+                            par_d.cpu().numpy(), opts=opts, check=False)
+        np.testing.assert_array_equal(n_d.cpu().numpy(), r.n)
+        np.testing.assert_array_equal(T_d.cpu().numpy(), r.Tgas)
+        np.testing.assert_array_equal(fl.cpu().numpy(), r.flags)
     g.free()
-    assert (fl.cpu().numpy() == 0).all()
-    m = parity(n_d.cpu().numpy(), T_d.cpu().numpy(), fl.cpu().numpy(),
-               nh, Th, r.flags, 1e-6)
-    assert m["frac"] >= 0.85 and m["max_rel"] < 1e-3, m
 
 
 def test_full_size_batch_conserves_nuclei_and_charge():
@@ -254,9 +255,7 @@ def test_lu32_parity_with_oracle(key):
                         check=False, stats=True)
     m = parity(r.n, r.Tgas, r.flags, ref["n"], ref["T"], ref["flags"],
                workloads.OPTIONS[key]["rtol"])
-    assert m["flags_equal"] == 1.0, m
-    assert m["frac"] >= FLOOR[key], m
-    assert m["max_rel"] < 1e-3 and m["max_relT"] < 1e-3, m
+    assert_at_floor(m, "%s/first/1024/31" % key)
     # the FP64 refactors: as many as the oracle's twin makes, up to the
     # chaotic spread of the step sequence
     g, c = int(r.stats[:, 9].sum()), int(ref["stats"][:, 9].sum())
@@ -283,4 +282,5 @@ def test_lu32_error_against_tight_oracle():
             assert (r.stats[:, 9] == 0).all()
     assert res[1]["flags_equal"] == 1.0 and res[0]["flags_equal"] == 1.0
     assert res[1]["frac"] >= res[0]["frac"] - 0.02, res
-    assert res[1]["max_rel"] < 1e-3, res
+    # and no cell's error much above the FP64 form's worst
+    assert res[1]["max_rel"] <= 2.0 * res[0]["max_rel"], res

@@ -17,7 +17,7 @@ import multiprocessing as mp
 import numpy as np
 import pytest
 
-from conftest import ALL_NETWORKS, NETWORKS, ROOT, parity
+from conftest import ALL_NETWORKS, NETWORKS, ROOT, assert_at_floor, parity
 from krome_x_b200 import build, netinfo, workloads
 
 GEN = ROOT / "oracle" / "_ref" / "gen"
@@ -154,7 +154,7 @@ def test_reference_binding_solves_on_the_gpu():
     ref = Oracle(key).solve(n, T, dt, par, **o)
     m = parity(res.n, res.Tgas, res.flags, ref["n"], ref["T"], ref["flags"],
                o["rtol"])
-    assert m["flags_equal"] == 1.0 and m["frac"] >= 0.89, m
+    assert_at_floor(m, "primordial3/first/512/52")
     assert res.ierr == ref["ret"]
     # inputs untouched (the binding's solve returns new arrays)
     n2, T2, _, _ = workloads.primordial3(512, info, seed=52)
