@@ -144,10 +144,11 @@ int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
                                const krome_opts* h);
 
 /* krome_get_rates (reference krome.h:387-389): k[ncell][nrea] at each
- * cell's rate temperature clamp(Tgas, Tcmb, 1e9); Phi and h unused */
+ * cell's rate temperature clamp(Tgas, Tcmb, 1e9), the photo rates of
+ * Phi[ncell][nbins] with photon bins on h (-103 without a field) */
 int krome_get_rates(int ncell, const double* n, const double* Tgas,
                     const double* par, int par_stride, const double* Phi,
-                    const void* h, double* k);
+                    const krome_opts* h, double* k);
 
 /* krome_has_device (reference krome.h:193): 1 when a CUDA device is
  * visible */

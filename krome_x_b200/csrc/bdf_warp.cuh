@@ -106,7 +106,34 @@ struct SolveOpts {
   double atol_sp[KB_NSP_TOL];
   double rtol_sp[KB_NSP_TOL];
   int rtol_v;
+  // photon bins (krome_opts_set_photo): the bin-averaged cross sections
+  // sigma[NPHOTO][ph_B] and the cells' fields Phi[ncell][ph_B] on the
+  // device; ph_B = 0: no field
+  const double* ph_sigma;
+  const double* ph_phi;
+  int ph_B;
 };
+
+// a cell's photo rates from its photon field, k_r = sum_b sigma_rb Phi_b,
+// into its parameters (the field is fixed during the solve)
+template <class P>
+__device__ __forceinline__ void photo_rates_of_row(P& p, const double* sigma,
+                                                   const double* phi, int B) {
+  if constexpr (NPHOTO > 0) {
+    for (int r = 0; r < NPHOTO; ++r) {
+      double acc = 0.0;
+      for (int b = 0; b < B; ++b) acc += sigma[(long)r * B + b] * phi[b];
+      p.kph[r] = acc;
+    }
+  } else {
+    (void)p; (void)sigma; (void)phi; (void)B;
+  }
+}
+template <class P>
+__device__ __forceinline__ void photo_rates_of_cell(P& p, long c,
+                                                    const SolveOpts& so) {
+  if (so.ph_B > 0) photo_rates_of_row(p, so.ph_sigma, so.ph_phi + c * so.ph_B, so.ph_B);
+}
 
 __device__ __forceinline__ double smax_(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double smin_(double a, double b) { return a < b ? a : b; }
@@ -1054,7 +1081,8 @@ struct Cell {
 template <int N, bool EVT>
 __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
                           const double* __restrict__ prow, double dt,
-                          const SolveOpts& so, double* smem, long* st_out) {
+                          const SolveOpts& so, double* smem, long* st_out,
+                          long cell) {
   const int lane = threadIdx.x & 31;
   Cell<N, EVT> c;
   c.lane = lane;
@@ -1068,6 +1096,7 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
 #if KB_NFREEZE > 0
   if (freeze_active(c.p)) return -104;  // frozen rows are not built
 #endif
+  photo_rates_of_cell(c.p, cell, so);
   const double T0 = *Tg;
   c.Tfix = T0;
   double y0 = 0.0;

@@ -82,6 +82,17 @@ int cellwise(int ncell, const double* n, double* out) {
   for (int c = 0; c < ncell; ++c) out[c] = G(n + (size_t)c * kbnet::NSPEC);
   return 0;
 }
+// a cell's photo rates from its field row, on the host (the queries)
+template <class P>
+void host_photo_rates(P& p, const krome_opts* h, const double* Phi, int c) {
+  if constexpr (kbnet::NPHOTO > 0) {
+    if (h == nullptr || h->photo.B <= 0 || Phi == nullptr) return;
+    kbphoto::rates_of_field(h->photo.sigma.data(), h->photo.B,
+                            Phi + (size_t)c * h->photo.B, p.kph);
+  } else {
+    (void)p; (void)h; (void)Phi; (void)c;
+  }
+}
 inline double cell_hnuclei(const double* n) { return kbnet::Hnuclei_(n); }
 inline double cell_freefall(const double* n) { return freefall_rho(kbnet::rho_(n)); }
 
@@ -187,14 +198,16 @@ KB_API int krome_get_fluxes(int ncell, const double* n, const double* Tgas,
                             const double* par, int par_stride,
                             const double* Phi, const krome_opts* h,
                             double* fl) {
-  (void)Phi; (void)h;
   if (Tgas == nullptr || fl == nullptr) return -1;
+  if (h != nullptr && h->photo.B > 0 && Phi == nullptr) return -103;
   return for_each_cell(
       ncell, n, Tgas, par, par_stride,
       [&](int c, const double* nc, double T, const kbnet::Params& P) {
         if (kbnet::params_missing(P) >= 0) return -105;
+        kbnet::Params Q = P;
+        host_photo_rates(Q, h, Phi, c);
         double k[kbnet::NREA + 1];
-        cell_rates(nc, rate_T(T, P), P, k);
+        cell_rates(nc, rate_T(T, Q), Q, k);
         kbnet::reaction_fluxes(nc, k, fl + (size_t)c * kbnet::NREA);
         return 0;
       });
@@ -207,14 +220,16 @@ KB_API int krome_get_thermal(int ncell, const double* n, const double* Tgas,
                              const double* Phi, const krome_opts* h,
                              double* heat, double* cool, double* heats,
                              double* cools, double* dTdt) {
-  (void)Phi; (void)h;
   if (Tgas == nullptr) return -1;
+  if (h != nullptr && h->photo.B > 0 && Phi == nullptr) return -103;
   return for_each_cell(
       ncell, n, Tgas, par, par_stride,
       [&](int c, const double* nc, double T, const kbnet::Params& P) {
         if (kbnet::params_missing(P) >= 0) return -105;
+        kbnet::Params Q = P;
+        host_photo_rates(Q, h, Phi, c);
         double k[kbnet::NREA + 1];
-        cell_rates(nc, rate_T(T, P), P, k);
+        cell_rates(nc, rate_T(T, Q), Q, k);
         const double Tth = thermal_T(T);
         double H[kbnet::NHEAT > 0 ? kbnet::NHEAT : 1];
         double C[kbnet::NCOOL > 0 ? kbnet::NCOOL : 1];
@@ -428,54 +443,209 @@ KB_API int krome_opts_set_error_file(krome_opts* h, const char* path) {
   return 0;
 }
 
-// ---- photon bins (krome.h:203-228) ----
-// the broadening and in-bin spectrum are kept on the handle; photon bins
-// themselves are refused (-104)
+// ---- photon bins (krome.h:203-228, 600-640) ----
+
+namespace {
+int rebuild_photo(krome_opts* h) {
+  if (h->photo.B <= 0) return 0;  // applied when the bins are set
+  const std::vector<double> lo = h->photo.lo, hi = h->photo.hi;
+  return kbphoto::build(h->photo, (int)lo.size(), lo.data(), hi.data(),
+                        h->photo_alpha, h->broad_T, h->broad_vturb) ? 0 : -1;
+}
+}  // namespace
+
+// nbins bins [Elo, Ehi] [eV]: the cross sections averaged over them; a
+// solve then needs each cell's field (krome_cells Phi, -103 without)
 KB_API int krome_opts_set_photo(krome_opts* h, int nbins, const double* Elo,
                                 const double* Ehi) {
   if (h == nullptr || !kbspec::bins_valid(nbins, Elo, Ehi)) return -1;
-  return -104;
+  return kbphoto::build(h->photo, nbins, Elo, Ehi, h->photo_alpha, h->broad_T,
+                        h->broad_vturb) ? 0 : -1;
 }
-KB_API int krome_opts_nbins(const krome_opts*) { return 0; }
+KB_API int krome_opts_nbins(const krome_opts* h) {
+  return h != nullptr ? h->photo.B : 0;
+}
+// Doppler broadening of the tabulated cross sections (Tgas [K], vturb
+// [cm/s]); rebuilds the bins already set
 KB_API int krome_opts_set_photo_broadening(krome_opts* h, double Tgas,
                                            double vturb) {
   if (h == nullptr || !(Tgas >= 0.0) || !(vturb >= 0.0)) return -1;
   h->broad_T = Tgas;
   h->broad_vturb = vturb;
-  return 0;
+  return rebuild_photo(h);
 }
+// the in-bin spectrum dN/dE ~ E^-alpha; rebuilds the bins already set
 KB_API int krome_opts_set_photo_alpha(krome_opts* h, double alpha) {
   if (h == nullptr || !std::isfinite(alpha)) return -1;
   h->photo_alpha = alpha;
+  return rebuild_photo(h);
+}
+// the dust opacity per bin [cm^2 per g of dust] (NULL: none), the dust
+// term of krome_get_absorption
+KB_API int krome_opts_set_photo_dust_opacity(krome_opts* h,
+                                             const double* kappa) {
+  if (h == nullptr || h->photo.B <= 0) return -1;
+  if (kappa == nullptr) {
+    h->photo.kdust.clear();
+    return 0;
+  }
+  for (int b = 0; b < h->photo.B; ++b)
+    if (!(kappa[b] >= 0.0)) return -1;
+  h->photo.kdust.assign(kappa, kappa + h->photo.B);
   return 0;
 }
-KB_API int krome_opts_set_photo_dust_opacity(krome_opts*, const double*) {
-  return -1;  // no photon bins on the handle
+// J_LW = sum_b w_b Phi_b
+KB_API int krome_opts_lw_weights(const krome_opts* h, double* w) {
+  if (h == nullptr || h->photo.B <= 0 || w == nullptr) return -1;
+  for (int b = 0; b < h->photo.B; ++b) w[b] = h->photo.lww[b];
+  return 0;
 }
-KB_API int krome_opts_lw_weights(const krome_opts*, double*) { return -1; }
-KB_API int krome_opts_photo_sigma(const krome_opts*, double*) { return -1; }
-KB_API double krome_photo_xsec(int, double) { return std::nan(""); }
-KB_API int krome_get_photo_heating(int, const double*, const double*,
-                                   const double*, int, const double*,
-                                   const krome_opts*, double*) {
-  return -1;
+// the bin-averaged cross sections sigma[nphoto][nbins] [cm^2]
+KB_API int krome_opts_photo_sigma(const krome_opts* h, double* sigma) {
+  if (h == nullptr || h->photo.B <= 0 || sigma == nullptr) return -1;
+  for (size_t i = 0; i < h->photo.sigma.size(); ++i) sigma[i] = h->photo.sigma[i];
+  return 0;
 }
-KB_API int krome_get_ratio_flux_draine(int, const double*, const krome_opts*,
-                                       double*) {
-  return -1;
+// the cross section of photo reaction r at E [eV] (0 outside its range)
+KB_API double krome_photo_xsec(int r, double E) {
+  if (r < 0 || r >= kbnet::NPHOTO) return std::nan("");
+  if (kbnet::kbxs::photo_xsec[r] == nullptr) return std::nan("");
+  return (E >= kbnet::photo_Emin_[r] && E <= kbnet::photo_Emax_[r])
+      ? kbnet::kbxs::photo_xsec[r](E) : 0.0;
 }
-KB_API int krome_get_habing(int, const double*, const krome_opts*, double*) {
-  return -1;
+// the Habing flux G of each cell's field (6-13.6 eV over 1.6e-3 erg
+// cm^-2 s^-1), and its ratio to the Draine field (the photon flux summed
+// over the bins as h / (4 pi) sum Phi_b over 7.95e-8)
+KB_API int krome_get_habing(int ncell, const double* Phi, const krome_opts* h,
+                            double* G) {
+  if (ncell < 0 || h == nullptr || h->photo.B <= 0 || !Phi || !G) return -1;
+  const int B = h->photo.B;
+  for (int c = 0; c < ncell; ++c) {
+    double g = 0.0;
+    for (int b = 0; b < B; ++b) g += h->photo.habw[b] * Phi[(size_t)c * B + b];
+    G[c] = g;
+  }
+  return 0;
 }
-KB_API int krome_get_opacity(int, const double*, const double*, const double*,
-                             int, const krome_opts*, const double*,
-                             const double*, double*) {
-  return -1;
+KB_API int krome_get_ratio_flux_draine(int ncell, const double* Phi,
+                                       const krome_opts* h, double* ratio) {
+  if (ncell < 0 || Phi == nullptr || ratio == nullptr || h == nullptr
+      || h->photo.B <= 0)
+    return -1;
+  const int B = h->photo.B;
+  for (int c = 0; c < ncell; ++c) {
+    double s = 0.0;
+    for (int b = 0; b < B; ++b) s += Phi[(size_t)c * B + b];
+    ratio[c] = s * kbc::planck_eV / (4.0 * kbc::pi) / 7.95e-8;
+  }
+  return 0;
 }
-KB_API int krome_get_absorption(int, const double*, const double*,
-                                const double*, int, const krome_opts*,
-                                const double*, double*) {
-  return -1;
+// the photoheating of each photo reaction [erg cm^-3 s^-1],
+// heat[ncell][nphoto]: its photoelectrons' deposit (0 for the Solomon
+// process)
+KB_API int krome_get_photo_heating(int ncell, const double* n,
+                                   const double* Tgas, const double* par,
+                                   int par_stride, const double* Phi,
+                                   const krome_opts* h, double* heat) {
+  if (Tgas == nullptr || heat == nullptr || h == nullptr || h->photo.B <= 0)
+    return -1;
+  if (Phi == nullptr) return -103;
+  const int B = h->photo.B;
+  return for_each_cell(
+      ncell, n, Tgas, par, par_stride,
+      [&](int c, const double* nc, double, const kbnet::Params& P) {
+        if (kbnet::params_missing(P) >= 0) return -105;
+        for (int r = 0; r < kbnet::NPHOTO; ++r) {
+          double& o = heat[(size_t)c * kbnet::NPHOTO + r];
+          o = 0.0;
+          if (!kbnet::photo_deposit_[r]) continue;
+          double se = 0.0;
+          for (int b = 0; b < B; ++b)
+            se += h->photo.sigmaE[(size_t)r * B + b] * Phi[(size_t)c * B + b];
+          o = se * nc[kbnet::photo_reactant_[r]] * kbc::eV_to_erg;
+        }
+        return 0;
+      });
+}
+
+namespace {
+// the d2g parameter of a cell, or 0 where the network has none
+double cell_d2g(const kbnet::Params& P) {
+  for (int i = 0; i < kbnet::NPAR; ++i)
+    if (!std::strcmp(kbnet::param_names[i], "d2g"))
+      return reinterpret_cast<const double*>(&P)[i];
+  return 0.0;
+}
+bool has_d2g() {
+  for (int i = 0; i < kbnet::NPAR; ++i)
+    if (!std::strcmp(kbnet::param_names[i], "d2g")) return true;
+  return false;
+}
+}  // namespace
+
+// the photon removal per bin [cm^-1], kabs[ncell][nbins]: the photo
+// reactions' sigma_rb n_r / pdiss_r, the handle's dust opacity times the
+// dust mass density (the d2g parameter), and rho_gas kdust_b when given
+KB_API int krome_get_absorption(int ncell, const double* n, const double* Tgas,
+                                const double* par, int par_stride,
+                                const krome_opts* h, const double* kdust,
+                                double* kabs) {
+  if (Tgas == nullptr || kabs == nullptr || h == nullptr || h->photo.B <= 0)
+    return -1;
+  const int B = h->photo.B;
+  return for_each_cell(
+      ncell, n, Tgas, par, par_stride,
+      [&](int c, const double* nc, double, const kbnet::Params& P) {
+        if (kbnet::params_missing(P) >= 0) return -105;
+        double* kc = kabs + (size_t)c * B;
+        for (int b = 0; b < B; ++b) kc[b] = 0.0;
+        for (int r = 0; r < kbnet::NPHOTO; ++r) {
+          const double f = nc[kbnet::photo_reactant_[r]] * 1.0 / kbnet::photo_pdiss_[r];
+          for (int b = 0; b < B; ++b) kc[b] += h->photo.sigma[(size_t)r * B + b] * f;
+        }
+        if (has_d2g() && !h->photo.kdust.empty())
+          for (int b = 0; b < B; ++b)
+            kc[b] += kbnet::rho_(nc) * cell_d2g(P) * h->photo.kdust[b];
+        if (kdust != nullptr) {
+          const double rr = kbnet::rho_(nc);
+          for (int b = 0; b < B; ++b) kc[b] += rr * kdust[b];
+        }
+        return 0;
+      });
+}
+// the optical depth per bin with the column estimates, tau[ncell][nbins]:
+// sigma_rb N_r / pdiss_r (N_r the column of the reactant's density) and,
+// with d2g[ncell], kdust_b d2g Sigma_gas (Sigma_gas = N_H rho / n_H); the
+// reference's default dust opacity (the Draine table) is not carried here:
+// d2g without kdust returns -1
+KB_API int krome_get_opacity(int ncell, const double* n, const double* Tgas,
+                             const double* par, int par_stride,
+                             const krome_opts* h, const double* d2g,
+                             const double* kdust, double* tau) {
+  if (Tgas == nullptr || tau == nullptr || h == nullptr || h->photo.B <= 0)
+    return -1;
+  if (d2g != nullptr && kdust == nullptr) return -1;
+  const int B = h->photo.B;
+  return for_each_cell(
+      ncell, n, Tgas, par, par_stride,
+      [&](int c, const double* nc, double, const kbnet::Params& P) {
+        if (kbnet::params_missing(P) >= 0) return -105;
+        double* tc = tau + (size_t)c * B;
+        for (int b = 0; b < B; ++b) tc[b] = 0.0;
+        for (int r = 0; r < kbnet::NPHOTO; ++r) {
+          const double Ncol = kbnet::num2col_(nc[kbnet::photo_reactant_[r]]);
+          const double I = 1.0 * Ncol;
+          for (int b = 0; b < B; ++b)
+            tc[b] += h->photo.sigma[(size_t)r * B + b] * I / kbnet::photo_pdiss_[r];
+        }
+        const double dg = d2g != nullptr ? d2g[c] : 0.0;
+        if (dg > 0.0) {
+          const double nH = kbnet::Hnuclei_(nc);
+          const double Sg = nH > 0.0 ? kbnet::NH_col_(nc) * kbnet::rho_(nc) / nH : 0.0;
+          for (int b = 0; b < B; ++b) tc[b] += kdust[b] * dg * Sg;
+        }
+        return 0;
+      });
 }
 
 // ---- the equilibrium driver (krome.h:306-330) ----

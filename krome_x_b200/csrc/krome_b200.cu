@@ -35,6 +35,7 @@
 #include "bdf_lane.cuh"
 #include "adjoint.cuh"
 #include "bdf_big.cuh"
+#include "kb_photo.h"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
 
@@ -78,7 +79,7 @@ __device__ __forceinline__ void one_cell(int c, double* n, double* T,
     if (sc != nullptr && lane < NSTAT) sc[lane] = 0;
   } else if (dtc > 0.0) {
     flag = kbw::solve_cell<N, EVT>(n + (long)c * kbnet::NSPEC, T + c,
-                                   par + (long)c * pstride, dtc, so, ws, sc);
+                                   par + (long)c * pstride, dtc, so, ws, sc, c);
   } else if (sc != nullptr && lane < NSTAT) {
     sc[lane] = 0;
   }
@@ -181,6 +182,7 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
     if (flags != nullptr) flags[c] = kbw::FLAG_PARAM_UNSET;
     return false;
   }
+  kbw::photo_rates_of_cell(s.p, c, so);
 #if KB_NFREEZE > 0
   if (freeze_active(s.p)) {  // frozen rows are not built: refused
     if (flags != nullptr) flags[c] = -104;
@@ -360,10 +362,12 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
       } else {
         KB_UNROLL for (int i = 0; i < N; ++i) yf[i] = __shfl_sync(FULLM, s.y[i], src);
         {
-          double row[NPAR];
+          // the evaluated cell's parameters, the photo rates included
+          constexpr int PW = sizeof(Params) / sizeof(double);
+          static_assert(sizeof(Params) == PW * sizeof(double), "Params of doubles");
           const double* ps = reinterpret_cast<const double*>(&s.p);
-          KB_UNROLL for (int i = 0; i < NPAR; ++i) row[i] = __shfl_sync(FULLM, ps[i], src);
-          params_from_row(row, p);
+          double* pd = reinterpret_cast<double*>(&p);
+          KB_UNROLL for (int i = 0; i < PW; ++i) pd[i] = __shfl_sync(FULLM, ps[i], src);
         }
         Tfix = __shfl_sync(FULLM, s.Tfix, src);
         if (dq) {
@@ -620,6 +624,7 @@ struct krome_opts {
   // photon bins: the broadening of tabulated cross sections and the
   // in-bin spectrum dN/dE ~ E^-alpha
   double broad_T = 0.0, broad_vturb = 0.0, photo_alpha = 1.0;
+  kbphoto::Bins photo;  // B = 0: no photon bins
 };
 
 namespace {
@@ -690,8 +695,19 @@ SolveOpts to_solve_opts(const krome_opts& h) {
     so.rtol_sp[i] = tol(h.rtol_sp, i, h.rtol);
     if (so.rtol_sp[i] != h.rtol) so.rtol_v = 1;
   }
+  so.ph_sigma = nullptr;
+  so.ph_phi = nullptr;
+  so.ph_B = 0;
   return so;
 }
+
+// the photon field of a launch: the bins' cross sections and the cells'
+// Phi rows, both on the device (B = 0: none)
+struct PhotoArgs {
+  const double* sigma = nullptr;
+  const double* phi = nullptr;
+  int B = 0;
+};
 
 int g_num_sms = 0;
 int num_sms() {
@@ -723,8 +739,12 @@ template <bool EVT>
 cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    const double* dt, const double* par, int pstride,
                    int* flags, long* stats, unsigned* cursor,
-                   cudaStream_t stream, const RecIO* rio = nullptr) {
-  const SolveOpts so = to_solve_opts(h);
+                   cudaStream_t stream, const RecIO* rio = nullptr,
+                   const PhotoArgs& ph = PhotoArgs()) {
+  SolveOpts so = to_solve_opts(h);
+  so.ph_sigma = ph.sigma;
+  so.ph_phi = ph.phi;
+  so.ph_B = ph.B;
 #ifdef KB_LARGE_NETWORK
   // the sparse path: one block per cell over a persistent grid (one block
   // per SM: the dense block of the LU fills shared memory), each block with
@@ -825,12 +845,13 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
 cudaError_t launch_any(const krome_opts& h, int ncell, double* n, double* T,
                        const double* dt, const double* par, int pstride,
                        int* flags, long* stats, unsigned* cursor,
-                       cudaStream_t stream) {
+                       cudaStream_t stream,
+                       const PhotoArgs& ph = PhotoArgs()) {
   return h.evolve_T
       ? launch<true>(h, ncell, n, T, dt, par, pstride, flags, stats, cursor,
-                     stream)
+                     stream, nullptr, ph)
       : launch<false>(h, ncell, n, T, dt, par, pstride, flags, stats, cursor,
-                      stream);
+                      stream, nullptr, ph);
 }
 
 bool row_missing(const double* row) {
@@ -1107,6 +1128,8 @@ KB_API int krome_b200_solve_device(int ncell, double* n, double* Tgas,
 #endif
   if (cursor == nullptr && (h->kernel == 1)) return -1;
   if (const int u = unsupported(*h)) return u;
+  // photon bins need each cell's field: krome_solve_cells(_device) take it
+  if (h->photo.B > 0) return -103;
   const cudaError_t e = launch_any(*h, ncell, n, Tgas, dt, par, par_stride,
                                    flags, stats, cursor,
                                    static_cast<cudaStream_t>(stream));
@@ -1138,6 +1161,7 @@ KB_API int krome_b200_adjoint_record_device(
   if (mult_stride != 0 && mult_stride != kbnet::NREA) return -1;
   if (cursor == nullptr && h->kernel == 1) return -1;
   if (h->linsol == 2 || h->linsol == 3 || h->conserve != 0) return -104;
+  if (h->photo.B > 0) return -104;  // no adjoint of the photo rates
   const RecIO rio{mult, mult_stride, tape, tape_cap, tape_len, yfin};
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   const cudaError_t e =
@@ -1211,7 +1235,7 @@ KB_API int krome_b200_adjoint(int ncell, double* n, double* Tgas,
   std::vector<int> fl(ncell, 0);
   int* fo = flags != nullptr ? flags : fl.data();
   if (check_params(ncell, P, ps, fo) != 0) return -105;
-  if (h->linsol == 2 || h->linsol == 3 || h->conserve != 0) {
+  if (h->linsol == 2 || h->linsol == 3 || h->conserve != 0 || h->photo.B > 0) {
     for (int c = 0; c < ncell; ++c) fo[c] = -104;
     return -104;
   }
@@ -1309,10 +1333,13 @@ KB_API int krome_b200_adjoint(int ncell, double* n, double* Tgas,
   return 0;
 }
 
-KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
-                                  const double* dt, const double* par,
-                                  int par_stride, int* flags, long* stats,
-                                  const krome_opts* h) {
+namespace {
+// the host-array solve: krome_b200_solve_batch, and krome_solve_cells with
+// the photon field phi[ncell][nbins] of its extra rows (required with photon
+// bins on the handle: -103 without)
+int solve_host(int ncell, double* n, double* Tgas, const double* dt,
+               const double* par, int par_stride, const double* phi,
+               int* flags, long* stats, const krome_opts* h) {
   if (h == nullptr || ncell < 0 || n == nullptr || Tgas == nullptr
       || dt == nullptr)
     return -1;
@@ -1326,7 +1353,10 @@ KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
   std::vector<int> fl(ncell, 0);
   if (check_params(ncell, P, ps, flags != nullptr ? flags : fl.data()) != 0)
     return -105;
-  if (const int u = unsupported(*h)) {
+  int u = unsupported(*h);
+  const int B = h->photo.B;
+  if (u == 0 && B > 0 && phi == nullptr) u = -103;  // bins without a field
+  if (u != 0) {
     if (flags != nullptr)
       for (int c = 0; c < ncell; ++c) flags[c] = u;
     return u;
@@ -1336,8 +1366,11 @@ KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
   const size_t pb = sizeof(double) * (size_t)(ps ? (size_t)ncell * ps : kbnet::NPAR);
   const size_t fb = sizeof(int) * (size_t)ncell;
   const size_t sb = stats != nullptr ? sizeof(long) * (size_t)ncell * NSTAT : 0;
+  const size_t xb = B > 0 ? sizeof(double) * (size_t)kbnet::NPHOTO * B : 0;
+  const size_t hb = B > 0 ? sizeof(double) * (size_t)ncell * B : 0;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  const size_t total = al(nb) + 2 * al(tb) + al(pb) + al(fb) + al(sb) + 256;
+  const size_t total = al(nb) + 2 * al(tb) + al(pb) + al(fb) + al(sb)
+                       + al(xb) + al(hb) + 256;
   std::lock_guard<std::mutex> lock(g_mu);
   if (g_buf.ensure(total) != cudaSuccess) {
     if (flags != nullptr)
@@ -1351,14 +1384,23 @@ KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
   double* dp = reinterpret_cast<double*>(b); b += al(pb);
   int* dfl = reinterpret_cast<int*>(b); b += al(fb);
   long* dst = sb ? reinterpret_cast<long*>(b) : nullptr; b += al(sb);
+  double* dxs = reinterpret_cast<double*>(b); b += al(xb);
+  double* dphi = reinterpret_cast<double*>(b); b += al(hb);
   unsigned* dcur = reinterpret_cast<unsigned*>(b);
   cudaStream_t s = 0;
   cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, Tgas, tb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ddt, dt, tb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dp, P, pb, cudaMemcpyHostToDevice, s);
+  PhotoArgs pa;
+  if (B > 0) {
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dxs, h->photo.sigma.data(), xb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dphi, phi, hb, cudaMemcpyHostToDevice, s);
+    pa = PhotoArgs{dxs, dphi, B};
+  }
   if (e == cudaSuccess)
-    e = launch_any(*h, ncell, dn, dT, ddt, dp, ps, dfl, dst, dcur, s);
+    e = launch_any(*h, ncell, dn, dT, ddt, dp, ps, dfl, dst, dcur, s, pa);
   if (e == cudaSuccess) e = cudaMemcpyAsync(n, dn, nb, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(Tgas, dT, tb, cudaMemcpyDeviceToHost, s);
   int* hfl = flags != nullptr ? flags : fl.data();
@@ -1374,17 +1416,25 @@ KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
     if (hfl[c] != 0) return hfl[c];
   return 0;
 }
+}  // namespace
 
-// the reference's entry point (krome.h:291-294): host arrays, in place
+KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
+                                  const double* dt, const double* par,
+                                  int par_stride, int* flags, long* stats,
+                                  const krome_opts* h) {
+  return solve_host(ncell, n, Tgas, dt, par, par_stride, nullptr, flags,
+                    stats, h);
+}
+
+// the reference's entry point (krome.h:291-294): host arrays, in place;
+// extra->Phi [ncell][nbins] the photon field with photon bins on the handle
+// (Td and adust: binned dust, not built, not read)
 KB_API int krome_solve_cells(int ncell, double* n, double* Tgas,
                              const double* dt, const double* par,
-                             int par_stride, const krome_cells* extra, int* flags,
-                             const krome_opts* h) {
-  // extra: the per-cell photon / dust rows, read only with photon or dust
-  // bins on the handle (none here)
-  (void)extra;
-  return krome_b200_solve_batch(ncell, n, Tgas, dt, par, par_stride, flags,
-                                nullptr, h);
+                             int par_stride, const krome_cells* extra,
+                             int* flags, const krome_opts* h) {
+  return solve_host(ncell, n, Tgas, dt, par, par_stride,
+                    extra != nullptr ? extra->Phi : nullptr, flags, nullptr, h);
 }
 
 // ---- mass fractions and device-resident arrays (reference krome.h:
@@ -1484,7 +1534,10 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
   if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR) return -1;
   if (summary != nullptr) *summary = krome_device_summary{0, 0, 0};
   if (ncell == 0) return 0;
-  if (extra != nullptr) return -104;  // no photon or dust bins here
+  // extra->Phi [ncell][nbins] (device): the photon field, required with
+  // photon bins on the handle; Td and adust (binned dust) are not read
+  const int B = h->photo.B;
+  const double* phi = extra != nullptr ? extra->Phi : nullptr;
   if (cudaDeviceSynchronize() != cudaSuccess) return -104;
   // the required-parameter rule on the caller's rows (a host copy)
   const int ps = par != nullptr ? par_stride : 0;
@@ -1499,6 +1552,7 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
   std::vector<int> hfl(ncell, 0);
   int ret = check_params(ncell, P.data(), ps, hfl.data());
   if (ret == 0) ret = unsupported(*h);
+  if (ret == 0 && B > 0 && phi == nullptr) ret = -103;
   if (ret != 0 && ret != -105)
     for (int c = 0; c < ncell; ++c) hfl[c] = ret;
   const size_t fb = sizeof(int) * (size_t)ncell;
@@ -1514,15 +1568,18 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
   const size_t nb = staged ? sizeof(double) * (size_t)ncell * kbnet::NSPEC : 0;
   const size_t xb = rho != nullptr ? sizeof(double) * (size_t)ncell : 0;
   const size_t pb = par == nullptr ? sizeof(double) * kbnet::NPAR : 0;
+  const size_t sgb = B > 0 ? sizeof(double) * (size_t)kbnet::NPHOTO * B : 0;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   std::lock_guard<std::mutex> lock(g_dmu);
-  if (g_dbuf.ensure(al(nb) + al(xb) + al(pb) + al(fb) + 256) != cudaSuccess)
+  if (g_dbuf.ensure(al(nb) + al(xb) + al(pb) + al(fb) + al(sgb) + 256)
+      != cudaSuccess)
     return -111;
   char* b = static_cast<char*>(g_dbuf.p);
   double* dn = staged ? reinterpret_cast<double*>(b) : arr; b += al(nb);
   double* dx = reinterpret_cast<double*>(b); b += al(xb);
   double* dp = reinterpret_cast<double*>(b); b += al(pb);
   int* dfl = reinterpret_cast<int*>(b); b += al(fb);
+  double* dsg = reinterpret_cast<double*>(b); b += al(sgb);
   unsigned* dcur = reinterpret_cast<unsigned*>(b);
   const double* Pd = par;
   cudaError_t e = cudaSuccess;
@@ -1530,13 +1587,18 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
     e = cudaMemcpy(dp, P.data(), pb, cudaMemcpyHostToDevice);
     Pd = dp;
   }
+  PhotoArgs pa;
+  if (B > 0 && e == cudaSuccess) {
+    e = cudaMemcpy(dsg, h->photo.sigma.data(), sgb, cudaMemcpyHostToDevice);
+    pa = PhotoArgs{dsg, phi, B};
+  }
   const int tpb = 128, nblk = (ncell + tpb - 1) / tpb;
   if (e == cudaSuccess && staged) {
     kb_gather_in<<<nblk, tpb>>>(ncell, arr, layout, ld, rho, dn, dx);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
-    e = launch_any(*h, ncell, dn, Tgas, dt, Pd, ps, dfl, nullptr, dcur, 0);
+    e = launch_any(*h, ncell, dn, Tgas, dt, Pd, ps, dfl, nullptr, dcur, 0, pa);
   if (e == cudaSuccess && staged) {
     kb_scatter_out<<<nblk, tpb>>>(ncell, dn, dfl, layout, ld, rho, dx,
                                   h->renormalize_x, arr);
@@ -1749,7 +1811,8 @@ namespace {
 // the rate coefficients of each cell at its rate temperature clamp(Tgas,
 // Tcmb, 1e9) (the reference's krome_get_rates query, krome.h:387-389)
 __global__ void kb_rates(int ncell, const double* n, const double* T,
-                         const double* par, int pstride, double* k) {
+                         const double* par, int pstride, double* k,
+                         const double* sigma, const double* phi, int B) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   using namespace kbnet;
@@ -1757,6 +1820,7 @@ __global__ void kb_rates(int ncell, const double* n, const double* T,
   KB_UNROLL for (int i = 0; i < NSPEC; ++i) nv[i] = n[(long)c * NSPEC + i];
   Params p;
   params_from_row(par + (long)c * pstride, p);
+  if (B > 0) kbw::photo_rates_of_row(p, sigma, phi + (long)c * B, B);
   const double Tr = fmin(fmax(T[c], p.Tcmb), 1e9);
   KB_UNROLL for (int i = 0; i <= NREA; ++i) kk[i] = 0.0;
   rates_fixed(Tr, nv, p, kk);
@@ -1769,9 +1833,10 @@ __global__ void kb_rates(int ncell, const double* n, const double* T,
 // the photo rates (no photon bins here) are 0. Phi and h are unused.
 KB_API int krome_get_rates(int ncell, const double* n, const double* Tgas,
                            const double* par, int par_stride,
-                           const double* Phi, const void* h, double* k) {
-  (void)Phi; (void)h;
+                           const double* Phi, const krome_opts* h, double* k) {
   if (ncell < 0 || n == nullptr || Tgas == nullptr || k == nullptr) return -1;
+  const int B = h != nullptr ? h->photo.B : 0;
+  if (B > 0 && Phi == nullptr) return -103;  // photon bins without a field
   if (par != nullptr && par_stride != 0 && par_stride != kbnet::NPAR) return -1;
   if (ncell == 0) return 0;
   std::vector<double> dflt(kbnet::NPAR);
@@ -1784,19 +1849,28 @@ KB_API int krome_get_rates(int ncell, const double* n, const double* Tgas,
   const size_t tb = sizeof(double) * (size_t)ncell;
   const size_t pb = sizeof(double) * (ps ? (size_t)ncell * ps : (size_t)kbnet::NPAR);
   const size_t kb = sizeof(double) * (size_t)ncell * kbnet::NREA;
+  const size_t sgb = B > 0 ? sizeof(double) * (size_t)kbnet::NPHOTO * B : 0;
+  const size_t phb = B > 0 ? sizeof(double) * (size_t)ncell * B : 0;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   std::lock_guard<std::mutex> lock(g_mu);
-  if (g_buf.ensure(al(nb) + al(tb) + al(pb) + al(kb)) != cudaSuccess) return -111;
+  if (g_buf.ensure(al(nb) + al(tb) + al(pb) + al(kb) + al(sgb) + al(phb))
+      != cudaSuccess)
+    return -111;
   char* b = static_cast<char*>(g_buf.p);
   double* dn = reinterpret_cast<double*>(b); b += al(nb);
   double* dT = reinterpret_cast<double*>(b); b += al(tb);
   double* dp = reinterpret_cast<double*>(b); b += al(pb);
-  double* dk = reinterpret_cast<double*>(b);
+  double* dk = reinterpret_cast<double*>(b); b += al(kb);
+  double* dsg = reinterpret_cast<double*>(b); b += al(sgb);
+  double* dph = reinterpret_cast<double*>(b);
   cudaError_t e = cudaMemcpy(dn, n, nb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dT, Tgas, tb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dp, P, pb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && B > 0)
+    e = cudaMemcpy(dsg, h->photo.sigma.data(), sgb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && B > 0) e = cudaMemcpy(dph, Phi, phb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    kb_rates<<<(ncell + 127) / 128, 128>>>(ncell, dn, dT, dp, ps, dk);
+    kb_rates<<<(ncell + 127) / 128, 128>>>(ncell, dn, dT, dp, ps, dk, dsg, dph, B);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(k, dk, kb, cudaMemcpyDeviceToHost);
@@ -2106,7 +2180,9 @@ KB_API int krome_b200_solve_cells_noalloc(int ncell, double* n, double* Tgas,
     missing |= m;
   }
   if (missing) return -105;
-  if (const int u = unsupported(*h)) {
+  int u = unsupported(*h);
+  if (u == 0 && h->photo.B > 0) u = -103;  // no field argument here
+  if (u != 0) {
     if (flags != nullptr)
       for (int c = 0; c < ncell; ++c) flags[c] = u;
     return u;

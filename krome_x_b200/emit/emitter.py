@@ -326,10 +326,19 @@ class Emitter:
             else:
                 dv = univ[s][0]
                 dflt.append(None if dv is None else float(dv))
+        # the photo reactions: their rates come from the cell's photon
+        # field, integrated once per solve into Params::kph (0 without one)
+        self.photo_rx = [rx for rx in net.reactions
+                         if rx["rate"]["kind"] == "photo"]
+        nph = len(self.photo_rx)
         w("constexpr int NPAR = %d;" % len(pn))
+        w("constexpr int NPHOTO = %d;" % nph)
         w("struct Params {")
         for s in pn:
             w("  double %s;" % s)
+        if nph:
+            w("  // the photo rates sum_b sigma_rb Phi_b of the cell's field")
+            w("  double kph[NPHOTO];")
         w("};")
         w("inline const char* const param_names[NPAR] = {%s};"
           % ", ".join('"%s"' % s for s in pn))
@@ -345,6 +354,8 @@ class Emitter:
         w("KB_HD inline void params_from_row(const double* row, Params& p) {")
         for i, s in enumerate(pn):
             w("  p.%s = row[%d];" % (s, i))
+        for j in range(nph):
+            w("  p.kph[%d] = 0.0;" % j)
         w("}")
         w("KB_HD inline int params_missing(const Params& p) {")
         w("  (void)p;")
@@ -476,6 +487,9 @@ class Emitter:
                    "const Params& p, double* k) {" % part)
             self.w("  (void)Tgas; (void)n; (void)p; (void)k;")
             self.emit_grouped(self._rate_body, sel)
+            if part == "var":
+                for j, rx in enumerate(self.photo_rx):
+                    self.w("  k[%d] += p.kph[%d];  // %s" % (rx["id"] - 1, j, rx["eq"]))
             self.w("}")
         # which coefficients each part writes
         fixed_ids = sorted(rx["id"] - 1 for rx in fixed)
@@ -1709,6 +1723,13 @@ class Emitter:
         w("KB_HD inline double num2col_(double x) {")
         w("  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);")
         w("}")
+        # the H nuclei column N(H) + N(H+) + 2 N(H2) of those estimates
+        terms = [("" if sp != "H2" else "2.0 * ") + "num2col_(n[IDX_%s])" % self.cid(sp)
+                 for sp in ("H", "H+", "H2") if sp in self.idx]
+        w("KB_HD inline double NH_col_(const double* n) {")
+        w("  (void)n;")
+        w("  return %s;" % (" + ".join(terms) or "0.0"))
+        w("}")
         # photo reactions (their rates need a photon field)
         photo = []
         for rx in net.reactions:
@@ -1717,13 +1738,15 @@ class Emitter:
             if rx["rate"]["xsec"]["kind"] == "h2pd":
                 raise NotImplementedError("h2pd photo channels")
             ph = gen.resolve_photo(rx)
-            if rx["rate"].get("shield"):
+            ph["ch"] = len(photo)
+            ph["shield"] = rx["rate"].get("shield")
+            if ph["shield"]:
                 raise NotImplementedError("shielded photo rates")
             photo.append(ph)
         if any(rx.get("lw") for rx in net.reactions):
             raise NotImplementedError("J_LW rates")
         m = len(photo)
-        w("constexpr int NPHOTO = %d;" % m)
+        assert m == len(self.photo_rx)
         w("constexpr int NLW = 0;")
         w("inline const int photo_reaction_[%d] = {%s};"
           % (max(m, 1), ", ".join(str(p["i"]) for p in photo) or "-1"))
@@ -1733,6 +1756,66 @@ class Emitter:
         w("inline const double photo_pdiss_[%d] = {%s};"
           % (max(m, 1), ", ".join(self.num(p["rx"].get("pdiss", 1.0)) for p in photo)
              or "1.0"))
+        w("// the photoelectron deposit (E - Eth) of each photo rate: none for")
+        w("// the Solomon process (line pumping)")
+        w("inline const bool photo_deposit_[%d] = {%s};"
+          % (max(m, 1), ", ".join("false" if gen.is_solomon(p["rx"]) else "true"
+                                  for p in photo) or "true"))
+        w("inline const double photo_Emin_[%d] = {%s};"
+          % (max(m, 1), ", ".join(self.num(p["Emin"]) for p in photo) or "0.0"))
+        w("inline const double photo_Emax_[%d] = {%s};"
+          % (max(m, 1), ", ".join(self.num(p["Emax"] if p["Emax"] is not None
+                                           else math.inf) for p in photo)
+             or "0.0"))
+        for p in photo:
+            if p.get("edep") or "binned" in p:
+                raise NotImplementedError("inner-shell deposits / binned lines")
+        # the cross sections sigma_r(E) [cm^2] on the host (the photon bins'
+        # averages are built there), rendered by the reference generator's
+        # own photo emitter with its tables inline
+        if m:
+            lines = []
+            gen.DATA_THRESHOLD = 1 << 30
+            gen.emit_photo(lines.append, photo)
+            body = "\n".join(lines)
+            body = body.replace("constants::", "kbc::")
+            # keep the cross sections, drop the generator's runtime tables
+            body = body.split("\nconstexpr int NPHOTO")[0]
+            w("// ---- host: the photo cross sections (photon-bin setup) ----")
+            w("namespace kbxs {")
+            if "H2_sigmaLW" in body:
+                # the H2 Lyman-Werner cross section of legacy KROME's
+                # H2_sigmaLW (reference runtime/core/h2_shielding.hpp:96-120):
+                # the ortho/para-weighted (3:1) sum of the Lyman and Werner
+                # band fits of the v = 0 and v = 1 levels, log10 sigma linear
+                # or cubic-quintic in E over each band's range
+                for ln in (
+                    "inline double H2_sigmaLW(double E) {",
+                    "  auto band = [](double lg) { return 1e-18 * std::pow(10.0, lg); };",
+                    "  double l0 = 0.0, w0 = 0.0, l1 = 0.0, w1 = 0.0;",
+                    "  if (E > 14.675 && E < 16.820) l0 = band(15.1289 - 1.05139 * E);",
+                    "  else if (E > 16.820 && E < 17.6)",
+                    "    l0 = band(-31.41 + 1.8042e-2 * E * E * E - 4.2339e-5 * std::pow(E, 5.0));",
+                    "  if (E > 14.675 && E < 17.7) w0 = band(13.5311 - 0.9182618 * E);",
+                    "  if (E > 14.159 && E < 15.302) l1 = band(12.0218406 - 0.819429 * E);",
+                    "  else if (E > 15.302 && E < 17.2) l1 = band(16.04644 - 1.082438 * E);",
+                    "  if (E > 14.159 && E < 17.2) w1 = band(12.87367 - 0.85088597 * E);",
+                    "  const double para = 1.0 / (3.0 + 1.0);",
+                    "  return para * (l0 + w0) + (1.0 - para) * (l1 + w1);",
+                    "}"):
+                    w(ln)
+            w(body)
+            w("inline double (*const photo_xsec[%d])(double) = {%s};"
+              % (m, ", ".join("photo_xsec_%d" % p["ch"] for p in photo)))
+            w("inline double (*const photo_xsec_int[%d])(double, double) = {%s};"
+              % (m, ", ".join(("photo_xsec_int_%d" % p["ch"]) if "table" in p
+                              else "nullptr" for p in photo)))
+            w("}  // namespace kbxs")
+        else:
+            w("namespace kbxs {  // no photo reactions")
+            w("inline double (*const photo_xsec[1])(double) = {nullptr};")
+            w("inline double (*const photo_xsec_int[1])(double, double) = {nullptr};")
+            w("}  // namespace kbxs")
         w("")
         self.photo = photo
 

@@ -91,6 +91,44 @@ class Options:
             self[k] = v
         return self
 
+    # -- photon bins (reference runtime/interfaces/python/krome.py:1337-1400)
+    def set_photo(self, Elo, Ehi):
+        """photon bins [eV edges]; a solve then needs each cell's field
+        Phi[ncell, nbins] (photons cm^-2 s^-1 per bin)"""
+        lo = np.ascontiguousarray(Elo, dtype=float)
+        hi = np.ascontiguousarray(Ehi, dtype=float)
+        if lo.shape != hi.shape or lo.ndim != 1:
+            raise KromeError("Elo and Ehi must be 1-D arrays of one shape")
+        if self._lib.krome_opts_set_photo(self._h, lo.size, _dptr(lo),
+                                          _dptr(hi)) != 0:
+            raise KromeError("invalid photon bins (need 0 < Elo < Ehi)")
+        return self
+
+    def set_photo_alpha(self, alpha):
+        """the in-bin photon spectrum dN/dE ~ E^-alpha"""
+        if self._lib.krome_opts_set_photo_alpha(self._h, float(alpha)) != 0:
+            raise KromeError("alpha must be finite")
+        return self
+
+    def set_photo_broadening(self, Tgas, vturb=0.0):
+        """Doppler broadening of the tabulated cross sections"""
+        if self._lib.krome_opts_set_photo_broadening(
+                self._h, float(Tgas), float(vturb)) != 0:
+            raise KromeError("broadening needs Tgas >= 0 and vturb >= 0")
+        return self
+
+    @property
+    def nbins(self):
+        return self._lib.krome_opts_nbins(self._h)
+
+    def photo_sigma(self):
+        """the bin-averaged cross sections [nphoto, nbins] [cm^2]"""
+        out = np.zeros((self._lib.krome_nphoto(), self.nbins))
+        if out.size and self._lib.krome_opts_photo_sigma(self._h,
+                                                          _dptr(out)) != 0:
+            raise KromeError("photon bins not configured")
+        return out
+
     def __del__(self):
         try:
             self._lib.krome_opts_free(self._h)
@@ -182,6 +220,25 @@ class Network:
                 ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4
                 + [ctypes.c_long] + [ctypes.c_void_p] * 8),
         }
+        proto.update({
+            "krome_opts_set_photo": (ctypes.c_int, [ctypes.c_void_p,
+                                                    ctypes.c_int, _D, _D]),
+            "krome_opts_set_photo_alpha": (ctypes.c_int, [ctypes.c_void_p,
+                                                          ctypes.c_double]),
+            "krome_opts_set_photo_broadening": (
+                ctypes.c_int, [ctypes.c_void_p, ctypes.c_double,
+                               ctypes.c_double]),
+            "krome_opts_nbins": (ctypes.c_int, [ctypes.c_void_p]),
+            "krome_opts_photo_sigma": (ctypes.c_int, [ctypes.c_void_p, _D]),
+            "krome_nphoto": (ctypes.c_int, []),
+            "krome_bins_log": (ctypes.c_int, [ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_double, _D, _D]),
+            "krome_spectrum_draine": (ctypes.c_int, [ctypes.c_int, _D, _D,
+                                                     _D]),
+            "krome_spectrum_j21": (ctypes.c_int, [ctypes.c_int, _D, _D,
+                                                  ctypes.c_double,
+                                                  ctypes.c_double, _D]),
+        })
         for name, (res, args) in proto.items():
             fn = getattr(lib, name)
             fn.restype, fn.argtypes = res, args
@@ -270,14 +327,26 @@ class Network:
                 "%s (for %s)" % (s, self.required[s]) for s in unset))
         return P, stride
 
-    def _run(self, n, T, dtv, P, stride, opts, check, stats):
+    def _run(self, n, T, dtv, P, stride, opts, check, stats, Phi=None):
         ncell = n.shape[0]
         flags = np.zeros(ncell, dtype=np.intc)
         st = np.zeros((ncell, len(STAT_NAMES)), dtype=np.int64) if stats else None
-        ierr = self._lib.krome_b200_solve_batch(
-            ncell, _dptr(n), _dptr(T), _dptr(dtv), _dptr(P), stride,
-            flags.ctypes.data_as(_I), None if st is None else st.ctypes.data_as(_L),
-            opts._h)
+        if Phi is not None:  # the field rows: krome_solve_cells' extra
+            if stats:
+                raise KromeError("per-cell counters are not returned with a "
+                                 "photon field")
+            F = np.array(np.broadcast_to(np.asarray(Phi, dtype=float),
+                                         (ncell, opts.nbins)), order="C",
+                         copy=True)
+            cells = (_D * 3)(_dptr(F), None, None)
+            ierr = self._lib.krome_solve_cells(
+                ncell, _dptr(n), _dptr(T), _dptr(dtv), _dptr(P), stride,
+                ctypes.addressof(cells), flags.ctypes.data_as(_I), opts._h)
+        else:
+            ierr = self._lib.krome_b200_solve_batch(
+                ncell, _dptr(n), _dptr(T), _dptr(dtv), _dptr(P), stride,
+                flags.ctypes.data_as(_I),
+                None if st is None else st.ctypes.data_as(_L), opts._h)
         if check and ierr != 0:
             bad = np.flatnonzero(flags)
             raise KromeError("krome_solve_cells returned %d: %s (failed cells: "
@@ -287,11 +356,13 @@ class Network:
         return flags, ierr, st
 
     def solve(self, n, Tgas, dt, par=None, opts=None, check=True,
-              stats=False):
+              stats=False, Phi=None):
         """integrate every cell over its own dt [s] (reference
         runtime/interfaces/python/krome.py:458-507): n[nspec] or
         n[ncell, nspec], Tgas and dt scalars or per cell, par None / a dict
-        / one row / rows. Returns a Result with new arrays."""
+        / one row / rows; Phi the photon field per bin (one row for every
+        cell or [ncell, nbins]) with photon bins on opts. Returns a Result
+        with new arrays."""
         n = np.array(n, dtype=float, order="C", copy=True)
         if n.ndim == 0 or n.ndim > 2 or n.shape[-1] != self.nspec:
             raise KromeError("n must have shape (%d,) or (ncell, %d), got %s"
@@ -305,7 +376,11 @@ class Network:
                        order="C", copy=True)
         opts = self._options(opts)
         P, stride = self._params(par, ncell)
-        flags, ierr, st = self._run(n, T, dtv, P, stride, opts, check, stats)
+        if opts.nbins > 0 and Phi is None:
+            raise KromeError("photon bins are configured (set_photo): Phi "
+                             "is required")
+        flags, ierr, st = self._run(n, T, dtv, P, stride, opts, check, stats,
+                                    Phi if opts.nbins > 0 else None)
         if single:
             return Result(n[0], T[0], flags[0], ierr,
                           None if st is None else st[0])
@@ -345,7 +420,7 @@ class Network:
         return Result(x, T, flags, ierr)
 
     def solve_batch(self, n, Tgas, dt, par=None, opts=None, check=True,
-                    stats=False):
+                    stats=False, Phi=None):
         """the batched entry point: n[N, nspec], Tgas[N], dt[N] exactly
         (no scalar broadcast), par None / dict / one row / [N, npar]"""
         n = np.asarray(n, dtype=float)
@@ -358,7 +433,7 @@ class Network:
                 raise KromeError("solve_batch: %s must be (%d,), got %s"
                                  % (name, N, np.shape(v)))
         return self.solve(n, Tgas, dt, par=par, opts=opts, check=check,
-                          stats=stats)
+                          stats=stats, Phi=Phi)
 
     def adjoint(self, n, Tgas, dt, par=None, gn=None, gT=None, lnm=None,
                 opts=None, tape_cap=0, check=True):
@@ -435,20 +510,51 @@ class Network:
                              % (r, self.flag_message(r)))
         return r
 
-    def rates(self, n, Tgas, par=None):
+    def rates(self, n, Tgas, par=None, Phi=None, opts=None):
         """the rate coefficients k[ncell, nrea] at each cell's rate
-        temperature (krome_get_rates, computed on the GPU)"""
+        temperature (krome_get_rates, computed on the GPU), with the photo
+        rates of the field Phi on opts' photon bins"""
         n = np.ascontiguousarray(np.atleast_2d(n), dtype=float)
         ncell = n.shape[0]
         T = np.ascontiguousarray(np.broadcast_to(np.asarray(Tgas, float),
                                                  (ncell,)))
         P, stride = self._params(par, ncell)
         k = np.zeros((ncell, self.nrea))
+        F = None
+        if Phi is not None:
+            F = np.array(np.broadcast_to(np.asarray(Phi, dtype=float),
+                                         (ncell, opts.nbins)), order="C")
         r = self._lib.krome_get_rates(ncell, _dptr(n), _dptr(T), _dptr(P),
-                                      stride, None, None, _dptr(k))
+                                      stride, _dptr(F),
+                                      None if opts is None else opts._h,
+                                      _dptr(k))
         if r != 0:
             raise KromeError("krome_get_rates returned %d" % r)
         return k
+
+    def bins_log(self, nbins, lower, upper):
+        """(Elo, Ehi) of nbins logarithmic bins in [lower, upper] eV"""
+        lo, hi = np.zeros(nbins), np.zeros(nbins)
+        if self._lib.krome_bins_log(nbins, lower, upper, _dptr(lo), _dptr(hi)) != 0:
+            raise KromeError("invalid binning")
+        return lo, hi
+
+    def spectrum_draine(self, Elo, Ehi):
+        """the Draine (1978) interstellar field per bin [photons cm^-2 s^-1]"""
+        lo, hi = np.ascontiguousarray(Elo, float), np.ascontiguousarray(Ehi, float)
+        out = np.zeros(lo.size)
+        if self._lib.krome_spectrum_draine(lo.size, _dptr(lo), _dptr(hi), _dptr(out)) != 0:
+            raise KromeError("invalid bins")
+        return out
+
+    def spectrum_j21(self, Elo, Ehi, J21=1.0, alpha=1.0):
+        """a J21 power-law field per bin [photons cm^-2 s^-1]"""
+        lo, hi = np.ascontiguousarray(Elo, float), np.ascontiguousarray(Ehi, float)
+        out = np.zeros(lo.size)
+        if self._lib.krome_spectrum_j21(lo.size, _dptr(lo), _dptr(hi), J21,
+                                        alpha, _dptr(out)) != 0:
+            raise KromeError("invalid bins")
+        return out
 
     def fp64_peak(self):
         """the measured FP64 peak of the GPU [TFLOP/s]"""

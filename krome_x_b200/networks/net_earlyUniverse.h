@@ -102,6 +102,7 @@ KB_UNROLL
 }
 
 constexpr int NPAR = 6;
+constexpr int NPHOTO = 0;
 struct Params {
   double Trad;
   double gamma_ad;
@@ -1465,11 +1466,23 @@ KB_HD inline void scale_Z(double* n, double Z) {
 KB_HD inline double num2col_(double x) {
   return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
-constexpr int NPHOTO = 0;
+KB_HD inline double NH_col_(const double* n) {
+  (void)n;
+  return num2col_(n[IDX_H]) + num2col_(n[IDX_Hj]) + 2.0 * num2col_(n[IDX_H2]);
+}
 constexpr int NLW = 0;
 inline const int photo_reaction_[1] = {-1};
 inline const int photo_reactant_[1] = {-1};
 inline const double photo_pdiss_[1] = {1.0};
+// the photoelectron deposit (E - Eth) of each photo rate: none for
+// the Solomon process (line pumping)
+inline const bool photo_deposit_[1] = {true};
+inline const double photo_Emin_[1] = {0.0};
+inline const double photo_Emax_[1] = {0.0};
+namespace kbxs {  // no photo reactions
+inline double (*const photo_xsec[1])(double) = {nullptr};
+inline double (*const photo_xsec_int[1])(double, double) = {nullptr};
+}  // namespace kbxs
 
 constexpr bool HAS_THERMAL_TERMS = false;
 // a rate coefficient depends on the densities (the species block

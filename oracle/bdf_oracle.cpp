@@ -19,6 +19,7 @@
 #include <cstring>
 #include <vector>
 #include KB_NET_HEADER
+#include "krome_x_b200/csrc/kb_photo.h"
 #ifndef KB_NFREEZE
 #define KB_NFREEZE 0  // a network header from before freeze directives
 #endif
@@ -1203,6 +1204,12 @@ struct oracle_opts {
   // per-species tolerances [NSPEC] (negative entry: the scalar), or null
   const double* atol_sp;
   const double* rtol_sp;
+  // photon bins: sigma[NPHOTO][ph_B] and the cells' fields Phi[ncell][ph_B]
+  // (ph_B = 0: none); each cell's photo rates k_r = sum_b sigma_rb Phi_b
+  // (solve_cell.hpp:609-614 with photo.hpp photo_rates)
+  const double* ph_sigma;
+  const double* ph_phi;
+  int ph_B;
 };
 
 // per-cell counters: nst, nfe, nfeDQ, nje, nsetups, nni, nnf, netf,
@@ -1284,13 +1291,26 @@ namespace {
 // one cell; mult (exp of the rate ln-multipliers) and tape (the adjoint's
 // recording) may be null; yfin receives the integrator's final y before the
 // post-solve rules (may be null)
+// a cell's photo rates from its field row (none without photo reactions)
+extern "C++" template <class P>
+void photo_rates_(P& p, const oracle_opts* so, const double* phirow) {
+  if constexpr (NPHOTO > 0) {
+    if (phirow != nullptr && so->ph_B > 0)
+      kbphoto::rates_of_field(so->ph_sigma, so->ph_B, phirow, p.kph);
+  } else {
+    (void)p; (void)so; (void)phirow;
+  }
+}
+
 int solve_one_(double* n, double* Tgas, const double* par, double dt,
                const oracle_opts* so, long* stats, const double* mult,
-               std::vector<double>* tape, double* yfin) {
+               std::vector<double>* tape, double* yfin,
+               const double* phirow = nullptr) {
   Problem c;
   c.mult = mult;
   params_from_row(par, c.p);
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
+  photo_rates_(c.p, so, phirow);
 #if KB_NFREEZE > 0
   if (freeze_active(c.p)) return -104;  // frozen rows are not built
 #endif
@@ -1834,8 +1854,10 @@ ORACLE_API int oracle_solve_cells(int ncell, double* n, double* Tgas, const doub
   for (int c = 0; c < ncell; ++c) {
     long* sc = stats != nullptr ? stats + (long)c * ORACLE_NSTAT : nullptr;
     if (dt[c] > 0.0) {
-      fl[c] = oracle_solve_one(n + (long)c * NSPEC, Tgas + c,
-                               P + (long)c * ps, dt[c], so, sc);
+      const double* phirow = so->ph_B > 0 ? so->ph_phi + (long)c * so->ph_B
+                                          : nullptr;
+      fl[c] = solve_one_(n + (long)c * NSPEC, Tgas + c, P + (long)c * ps,
+                         dt[c], so, sc, nullptr, nullptr, nullptr, phirow);
     } else {
       fl[c] = 0;
       if (sc != nullptr)

@@ -36,7 +36,10 @@ class _Opts(ctypes.Structure):
                 ("clip_negative", ctypes.c_int), ("lu32", ctypes.c_int),
                 ("conserve", ctypes.c_int),
                 ("atol_sp", ctypes.POINTER(ctypes.c_double)),
-                ("rtol_sp", ctypes.POINTER(ctypes.c_double))]
+                ("rtol_sp", ctypes.POINTER(ctypes.c_double)),
+                ("ph_sigma", ctypes.POINTER(ctypes.c_double)),
+                ("ph_phi", ctypes.POINTER(ctypes.c_double)),
+                ("ph_B", ctypes.c_int)]
 
 
 def _ptr(a, t=_D):
@@ -60,7 +63,9 @@ class Oracle:
               atol_T=1e-6, max_steps=100000, max_err_fails=7,
               max_conv_fails=10, max_restarts=5, clip_negative=1, lu32=0,
               conserve=0, atol_species=None, rtol_species=None, threads=None,
-              **_):
+              photo_sigma=None, Phi=None, **_):
+        """photo_sigma [nphoto][nbins] (the bins' averaged cross sections)
+        and Phi [ncell][nbins]: each cell's photo rates from its field"""
         n = np.array(n, dtype=float, order="C", copy=True)
         T = np.array(T, dtype=float, order="C", copy=True)
         dt = np.ascontiguousarray(dt, dtype=float)
@@ -75,6 +80,10 @@ class Oracle:
         sp = [None if v is None else np.ascontiguousarray(v, dtype=float)
               for v in (atol_species, rtol_species)]
         o.atol_sp, o.rtol_sp = _ptr(sp[0]), _ptr(sp[1])
+        if Phi is not None:
+            sig = np.ascontiguousarray(photo_sigma, dtype=float)
+            Phi = np.ascontiguousarray(Phi, dtype=float).reshape(ncell, -1)
+            o.ph_sigma, o.ph_phi, o.ph_B = _ptr(sig), _ptr(Phi), Phi.shape[1]
         nt = threads or os.cpu_count() or 1
         t0 = time.perf_counter()
         ret = self.lib.oracle_solve_cells(
@@ -175,6 +184,22 @@ class Reference:
                 f.argtypes = [ctypes.c_void_p, _D]
                 if f(h, _ptr(v)) != 0:
                     raise KeyError(q + "_species")
+        # photon bins (Elo, Ehi) and each cell's field Phi[ncell][nbins]
+        bins = opts.pop("photo_bins", None)
+        Phi = opts.pop("Phi", None)
+        cells = None
+        if bins is not None:
+            lo = np.ascontiguousarray(bins[0], dtype=float)
+            hi = np.ascontiguousarray(bins[1], dtype=float)
+            keep += [lo, hi]
+            self.lib.krome_opts_set_photo.argtypes = [ctypes.c_void_p,
+                                                      ctypes.c_int, _D, _D]
+            if self.lib.krome_opts_set_photo(h, len(lo), _ptr(lo), _ptr(hi)) != 0:
+                raise KeyError("photo_bins")
+        if Phi is not None:
+            Phi = np.ascontiguousarray(Phi, dtype=float).reshape(ncell, -1)
+            keep.append(Phi)
+            cells = (_D * 3)(_ptr(Phi), None, None)
         for k, v in opts.items():
             if k in ("threads",):
                 continue
@@ -182,7 +207,8 @@ class Reference:
                 raise KeyError(k)
         t0 = time.perf_counter()
         ret = self.lib.krome_solve_cells(ncell, _ptr(n), _ptr(T), _ptr(dt),
-                                         _ptr(par), stride, None,
+                                         _ptr(par), stride,
+                                         None if cells is None else ctypes.addressof(cells),
                                          _ptr(flags, _I), h)
         self.seconds = time.perf_counter() - t0
         self.lib.krome_opts_free(h)

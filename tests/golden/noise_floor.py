@@ -14,7 +14,8 @@ error (abundances above atol/rtol; Tgas) over the five draws.
 Cases (each matching a parity test or smoke()): the first call of each
 small network's workload (512 cells, seed 3; 1024 cells, seed 11; the
 FP32-LU tests' 1024 cells, seed 31, solved by the oracle's FP32-LU twin; smoke()'s 64 primordial3 cells, seed
-7; the reference binding's 512 primordial3 cells, seed 52), the full
+7; the reference binding's 512 primordial3 cells, seed 52; 512
+galaxy_ism cells under a photon field, seed 62), the full
 4,096-cell config-0 batch (primordial, analytic Jacobian, seed 0), and the
 primordial3 hydro loop (4,096 cells, seed 1000, 10 calls; each call's
 inputs are the unperturbed loop's state, so the floor is that of one call).
@@ -69,6 +70,17 @@ def first_call(key, ncell, seed, rng, **over):
     return f
 
 
+def photo_floor(ncell, seed, rng):
+    """galaxy_ism under its seeded photon field (tests/test_photo.py); the
+    field rows are held, the cells' other inputs moved"""
+    from test_photo import photo_case
+    net, opts, (n, T, dt, par), Phi, bins, sigma = photo_case(ncell, seed)
+    key = "galaxy_ism"
+    o = dict(workloads.OPTIONS[key], photo_sigma=sigma, Phi=Phi)
+    _, f = floor_of(Oracle(key), key, n, T, dt, par, o, rng)
+    return f
+
+
 def hydro_loop(ncell, seed, calls, rng):
     key = "primordial3"
     info = netinfo.load(key)
@@ -102,6 +114,7 @@ def main():
     out["primordial3/first/64/7"] = first_call("primordial3", 64, 7, rng)
     out["primordial3/first/512/52"] = first_call("primordial3", 512, 52, rng)
     out["primordial/config0/4096/0"] = first_call("primordial", 4096, 0, rng)
+    out["galaxy_ism/photo/512/62"] = photo_floor(512, 62, rng)
     out["primordial3/hydro/4096/1000"] = hydro_loop(4096, 1000, 10, rng)
     (HERE / "noise_floor.json").write_text(json.dumps(out, indent=1) + "\n")
     for k, v in out.items():

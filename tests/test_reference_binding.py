@@ -160,3 +160,67 @@ def test_reference_binding_solves_on_the_gpu():
     n2, T2, _, _ = workloads.primordial3(512, info, seed=52)
     np.testing.assert_array_equal(n, n2)
     np.testing.assert_array_equal(T, T2)
+
+
+def _photo_survey(key, lib_path, n, T, par):
+    """the photon-bin tables and field queries through the binding"""
+    spec = importlib.util.spec_from_file_location(
+        "refkrome_" + key, GEN / key / "krome.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    net = mod.Network(lib_path)
+    out = {"xsec": [[net._lib.krome_photo_xsec(r, E) for E in
+                     (0.8, 3.0, 12.0, 14.0, 14.6, 16.0, 20.0, 40.0, 60.0, 500.0)]
+                    for r in range(len(net.photo_reactions))]}
+    P = par if par.ndim == 2 else np.tile(par, (len(T), 1))
+    for name, (lo, hi), extra in (
+            ("log", net.bins_log(24, 0.7, 300.0), {}),
+            ("lin", net.bins_lin(10, 5.0, 40.0), {}),
+            ("alpha0", net.bins_log(16, 0.7, 100.0), {"alpha": 0.0}),
+            ("alpha2", net.bins_log(16, 0.7, 100.0), {"alpha": 2.0}),
+            ("broad", net.bins_log(16, 2.0, 30.0), {"broad": (3000.0, 2e5)})):
+        o = net.options()
+        if "alpha" in extra:
+            o.set_photo_alpha(extra["alpha"])
+        if "broad" in extra:
+            o.set_photo_broadening(*extra["broad"])
+        o.set_photo(lo, hi)
+        Phi = np.outer(np.linspace(0.5, 2.0, len(T)),
+                       net.spectrum_draine(lo, hi) + net.spectrum_j21(lo, hi, 1.0, 1.0))
+        out[name] = dict(nbins=o.nbins, sigma=o.photo_sigma(), lw=o.lw_weights(),
+                         habing=net.habing(Phi, o) if hasattr(net, "habing") else None,
+                         heat=net.photo_heating(n, T, o, par=P, Phi=Phi),
+                         fluxes=net.fluxes(n, T, par=P, Phi=Phi, opts=o),
+                         ratio=net.ratio_flux_draine(Phi, o))
+    return out
+
+
+def _ref_photo_worker(args):
+    key, n, T, par = args
+    return _photo_survey(key, str(ROOT / "oracle" / "_ref" / ("libkrome_%s.so" % key)),
+                         n, T, par)
+
+
+def test_photon_bins_equal_the_reference():
+    """galaxy_ism's eight photo reactions: the bin-averaged cross sections
+    (several binnings, in-bin spectra, Doppler broadening of the tabulated
+    ones), the Lyman-Werner weights, the photoheating and the reaction
+    fluxes of a field, against the reference's library"""
+    key = "galaxy_ism"
+    if not (ROOT / "oracle" / "_ref" / ("libkrome_%s.so" % key)).exists():
+        pytest.skip("oracle/_ref not built here (oracle/build_ref.py)")
+    _binding(key)
+    n, T, par = _inputs(key)
+    ours = _photo_survey(key, str(build.build(key)), n, T, par)
+    with mp.get_context("spawn").Pool(1) as pool:
+        ref = pool.map(_ref_photo_worker, [(key, n, T, par)])[0]
+    assert set(ours) == set(ref)
+    for k in ref:
+        if isinstance(ref[k], dict):
+            for q in ref[k]:
+                if ref[k][q] is None:
+                    continue
+                assert _same(ours[k][q], ref[k][q], 1e-12), (k, q)
+        else:
+            assert _same(ours[k], ref[k], 1e-13), k
+    assert np.asarray(ours["log"]["sigma"]).max() > 0
