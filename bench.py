@@ -11,7 +11,9 @@ Tgas in [50, 5000] K, x_H2 in [1e-6, 0.5], x_e in [1e-8, 1e-2]; no dataset
 exists for this path). A step is 262,144 cell-solves.
 
   value     device-timed cell-solves/s of the K timed steps (inputs resident
-            in HBM; an L2 flush buffer of 256 MB is written between steps)
+            in HBM; each step's graph replay timed with CUDA events on its
+            stream; an L2 flush of 256 MB is written between steps, outside
+            the steps' events)
   e2e       the same loop through the public API (krome_solve_cells on
             pinned host arrays: host->device and device->host copies and the
             host-side compression inside the timed region)
@@ -20,17 +22,22 @@ exists for this path). A step is 262,144 cell-solves.
             counted work per rhs evaluation, over the kernel's event time;
             the peak is this GPU's DFMA rate measured live
   cpu_baseline  the reference's own krome_solve_cells (compiled from its
-            sources with OpenMP, oracle/_ref) on the host cores, on a sample
-            of the same loop
-  forms     (N = 1) the kernel forms, each on its own workload:
-            batching   one solve of 65,536 primordial3 cells with each
+            sources with OpenMP, oracle/_ref) on the host cores, on the first
+            cells of the same batch through the same loop
+  forms     (N = 1) the kernel forms, each on its own workload, each with
+            the reference's CPU solve of (a sample of) the same cells:
+            small      the plain method's small workload: 4,096 primordial
+                       cells, analytic Jacobian, dense LU, one solve
+            batching   the batching workload itself (262,144 primordial3
+                       cells, the hydro loop's first calls) with each
                        launch form: one lane / one warp per cell, each on
                        a persistent work-queue grid or a plain grid
             adjoint    the differentiation workload: 65,536 primordial cells
                        (cooling ATOMIC, H2; heating CHEM, COMPRESS; rtol 1e-6),
                        the plain solve, the recording solve and the reverse
                        sweep of the discrete adjoint (gradients of x_H2 and
-                       Tgas w.r.t. n0, T0 and every ln k), device-timed
+                       Tgas w.r.t. n0, T0 and every ln k), device-timed; the
+                       CPU's gradient is central differences
             precision  the precision workload: 131,072 galaxy_ism cells, the
                        Newton matrix factored in FP64 and in FP32 (FP64
                        refactor after Newton failures): cell-solves/s, the
@@ -41,9 +48,9 @@ exists for this path). A step is 262,144 cell-solves.
                        relative error)
             large_network  the large-network workload: Semenov (655 species,
                        5,639 reactions, grain-surface chemistry), fixed Tgas,
-                       the sparse-LU block-per-cell kernel on a seeded subset
-                       of the 16,384-cell batch: cell-solves/s and its DRAM
-                       traffic against the HBM peak
+                       the sparse-LU block-per-cell kernel on the first cells
+                       of the seeded 16,384-cell batch: cell-solves/s, its
+                       algorithmic bytes and DRAM traffic against the HBM peak
 
 ``python bench.py --gpus N --steps K --warmup W [--impl reference]``; with
 N > 1 each rank (torchrun) solves its own 262,144 cells (weak scaling: no
@@ -89,6 +96,8 @@ def parse():
                     help="cells of the large-network form (the workload's "
                          "batch is 16,384; the default is a seeded subset "
                          "that keeps the run within minutes)")
+    ap.add_argument("--large-cpu-cells", type=int, default=512,
+                    help="cells of the large-network form's CPU baseline")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the adjoint and precision forms")
     # one solve of a workload, outside the benchmark's timing: the command a
@@ -228,25 +237,29 @@ def algorithmic_flops(stats_sum, flops, N, ncells_solved):
 # ---------------------------------------------------------------------------
 # the CPU legs: the reference's krome_solve_cells on the host cores
 
-def _cpu_loop(args):
-    """the collapse loop on the host with the reference's library (kind
-    'reference') or, where it was not built, the CPU oracle ('port'); run
-    in a spawned process (one generated network per process)"""
-    ncell, warm, steps, threads = args
-    os.environ["OMP_NUM_THREADS"] = str(threads)
+def _cpu_solver(key):
+    """the reference's own library for a network (kind 'reference') or,
+    where it was not built, the CPU oracle ('port')"""
     sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    try:
+        return orc.Reference(key), "reference"
+    except (FileNotFoundError, OSError):
+        return orc.Oracle(key), "port"
+
+
+def _cpu_loop(args):
+    """the collapse loop on the host, on the first `ncell` cells of rank
+    0's seeded batch of `total` cells (the GPU arm's own first cells); run
+    in a spawned process (one generated network per process)"""
+    ncell, total, warm, steps, threads = args
+    os.environ["OMP_NUM_THREADS"] = str(threads)
     from krome_x_b200 import workloads
-    info, n, T, dt, par = inputs(ncell, seed=12345)
+    info, n, T, dt, par = inputs(total, seed=rank_seed(0))
+    n, T, dt, par = (np.ascontiguousarray(a[:ncell]) for a in (n, T, dt, par))
     opts = dict(evolve_T=1, jac=0, linsol=0, rtol=RTOL, atol_n=1e-20,
                 atol_T=1e-6)
-    kind = "reference"
-    try:
-        import oracle as orc
-        solver = orc.Reference(NETWORK)
-    except (FileNotFoundError, OSError):
-        import oracle as orc
-        solver = orc.Oracle(NETWORK)
-        kind = "port"
+    solver, kind = _cpu_solver(NETWORK)
     secs = 0.0
     failed = 0
     for step in range(warm + steps):
@@ -264,20 +277,57 @@ def _cpu_loop(args):
                 failed=failed)
 
 
-def cpu_leg(ncell, warm, steps):
+def cpu_leg(ncell, total, warm, steps):
     import multiprocessing as mp
     threads = os.cpu_count() or 1
     with mp.get_context("spawn").Pool(1) as pool:
-        r = pool.map(_cpu_loop, [(ncell, warm, steps, threads)])[0]
+        r = pool.map(_cpu_loop, [(ncell, total, warm, steps, threads)])[0]
     r["threads"] = threads
     r["value"] = r["cells"] * r["steps"] / r["seconds"]
     return r
 
 
+def _cpu_once(args):
+    """one solve of a form's workload on the host: the first `ncell` cells
+    of the seeded batch of `total` cells the GPU form solves, best of
+    `reps` (spawned process)"""
+    key, total, ncell, seed, opts, threads, reps = args
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from krome_x_b200 import netinfo, workloads
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](total, info, seed=seed)
+    n, T, dt, par = (np.ascontiguousarray(a[:ncell]) for a in (n, T, dt, par))
+    solver, kind = _cpu_solver(key)
+    best, failed = None, 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = solver.solve(n, T, dt, par, threads=threads, **opts)
+        el = time.perf_counter() - t0
+        best = el if best is None else min(best, el)
+        failed = int((out["flags"] != 0).sum())
+    return dict(kind=kind, seconds=best, cells=ncell, failed=failed)
+
+
+def cpu_form(key, total, ncell, seed, opts, reps=1):
+    """a form's CPU baseline: the reference's krome_solve_cells (OpenMP over
+    cells, every host core) on the first ncell cells of the form's batch"""
+    import multiprocessing as mp
+    threads = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(1) as pool:
+        r = pool.map(_cpu_once, [(key, total, ncell, seed, dict(opts),
+                                  threads, reps)])[0]
+    return {"value": r["cells"] / r["seconds"], "unit": "cell-solves/s",
+            "cores": threads, "kind": r["kind"], "seconds": r["seconds"],
+            "failed_cells": r["failed"],
+            "sample": "the first %d cells of the form's seeded %d-cell batch, "
+                      "one solve%s" % (ncell, total,
+                                       ", best of %d" % reps if reps > 1 else "")}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
-    r = cpu_leg(args.cpu_cells, args.warmup, args.steps)
+    r = cpu_leg(args.cpu_cells, args.cells, args.warmup, args.steps)
     line = {
         "impl": "reference",
         "metric": "cell-solves/s", "value": r["value"],
@@ -292,9 +342,11 @@ def run_reference(args, rank):
                    "sample_cells": r["cells"]},
         "cpu_baseline": {"value": r["value"], "unit": "cell-solves/s",
                          "cores": r["threads"], "kind": r["kind"],
-                         "sample": "%d cells x %d loop calls (after %d warm-up "
-                                   "calls) of the same seeded workload"
-                                   % (r["cells"], r["steps"], args.warmup)},
+                         "sample": "the first %d cells of the GPU arm's seeded "
+                                   "%d-cell batch x %d loop calls (after %d "
+                                   "warm-up calls)"
+                                   % (r["cells"], args.cells, r["steps"],
+                                      args.warmup)},
         "e2e": {"value": r["value"], "unit": "cell-solves/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -310,7 +362,7 @@ def _events(torch):
     return e
 
 
-def adjoint_form(torch, dev, reps=3):
+def adjoint_form(torch, dev, reps=3, cpu=True):
     """the discrete adjoint's cost on the differentiation workload"""
     from krome_x_b200 import autograd, krome, netinfo, workloads
     key, N = "primordial", 65536
@@ -353,15 +405,25 @@ def adjoint_form(torch, dev, reps=3):
         if best is None or r[1] + r[2] < best[1] + best[2]:
             best = r
     plain, rec, rev, failed = best
-    return {"workload": "primordial, 65,536 cells, rtol 1e-6, outputs x_H2 "
-                        "and Tgas, inputs n0, T0 and all %d ln k" % net.nrea,
-            "plain_forward_ms": plain, "recording_forward_ms": rec,
-            "reverse_sweep_ms": rev, "reverse_over_forward": rev / plain,
-            "gradient_over_forward": (rec + rev) / plain,
-            "failed_cells": failed, "reps": reps}
+    out = {"workload": "primordial, 65,536 cells, rtol 1e-6, outputs x_H2 "
+                       "and Tgas, inputs n0, T0 and all %d ln k" % net.nrea,
+           "plain_forward_ms": plain, "recording_forward_ms": rec,
+           "reverse_sweep_ms": rev, "reverse_over_forward": rev / plain,
+           "gradient_over_forward": (rec + rev) / plain,
+           "failed_cells": failed, "reps": reps}
+    if cpu:
+        # the reference has no adjoint: its gradient is central differences,
+        # 2 (nspec + 1 + nrea) forward solves per cell
+        cb = cpu_form(key, N, 4096, 0, o)
+        nfd = 2 * (net.nspec + 1 + net.nrea)
+        cb["fd_solves_per_gradient"] = nfd
+        cb["gradient_cells_per_s"] = cb["value"] / nfd
+        out["cpu_baseline"] = cb
+        out["gpu_gradient_cells_per_s"] = N / ((rec + rev) * 1e-3)
+    return out
 
 
-def precision_form(torch, dev):
+def precision_form(torch, dev, cpu=True):
     """FP64 and FP32 Newton-matrix factorisations on the precision workload,
     against the rtol 1e-12 FP64 solve"""
     from krome_x_b200 import krome, netinfo, workloads
@@ -406,6 +468,8 @@ def precision_form(torch, dev):
     out = {"workload": "galaxy_ism, 131,072 cells, rtol 1e-6, dt 3.15e11 s",
            "reference": "the FP64 solve at rtol 1e-12 on the GPU",
            "reference_ms": ref[4]}
+    if cpu:
+        out["cpu_baseline"] = cpu_form(key, N, 8192, 0, o)
     for name, lu32 in (("fp64", 0), ("lu32", 1)):
         runs = [run(o["rtol"], lu32) for _ in range(3)]
         best = min(runs, key=lambda r: r[4])
@@ -426,16 +490,18 @@ def precision_form(torch, dev):
 # stays in L2
 SEMENOV_DRAM_PER_STEP = 8.57e9 / 154747
 SEMENOV_CELLS = 2048
+SEMENOV_BATCH = 16384
 
 
-def large_network_form(torch, dev, ncell=SEMENOV_CELLS):
+def large_network_form(torch, dev, ncell=SEMENOV_CELLS, cpu_cells=512):
     """the sparse-LU path on the large-network workload: Semenov (655
     species, 5,639 reactions), fixed Tgas, one launch of the block-per-cell
     kernel over a seeded subset of the 16,384-cell batch"""
     from krome_x_b200 import krome, netinfo, workloads
     key = "semenov"
     info = netinfo.load(key)
-    n, T, dt, par = workloads.semenov(ncell, info, seed=0)
+    n, T, dt, par = workloads.semenov(SEMENOV_BATCH, info, seed=0)
+    n, T, dt, par = (np.ascontiguousarray(a[:ncell]) for a in (n, T, dt, par))
     net = krome.load(key)
     opts = net.options(**workloads.OPTIONS[key])
     t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
@@ -454,12 +520,20 @@ def large_network_form(torch, dev, ncell=SEMENOV_CELLS):
     steps = int(S[:, STAT_NAMES.index("nst")].sum())
     dram = SEMENOV_DRAM_PER_STEP * steps
     io = ncell * 8 * (2 * net.nspec + net.npar + 2)
+    # the sparse path's algorithmic bytes: per Newton matrix the Jacobian and
+    # the factors written and read, per Newton iteration the factors read,
+    # per rhs the rates and two state vectors:
+    # B = nsetups 8 (nnzJ + 2 nnzLU) + nni 8 nnzLU + nfe 8 (nrea + 2 nspec)
+    tot = dict(zip(STAT_NAMES, S.sum(axis=0).astype(float)))
+    nnz_j, nnz_lu = info["nnz_j"], info["nnz_lu"]
+    alg = 8.0 * (tot["nsetups"] * (nnz_j + 2 * nnz_lu) + tot["nni"] * nnz_lu
+                 + (tot["nfe"] + tot["nfeDQ"]) * (net.nrea + 2 * net.nspec))
     peak, peak_source = _hbm_peak()
     mass = np.asarray(info["mass_g"])
     out = nd.cpu().numpy()
     return {"workload": "Semenov (655 species, 5,639 reactions), fixed Tgas, "
-                        "rtol 1e-6, dt 3.15e13 s, sparse LU; %d seeded cells "
-                        "of the 16,384-cell batch" % ncell,
+                        "rtol 1e-6, dt 3.15e13 s, sparse LU; the first %d "
+                        "cells of the seeded 16,384-cell batch" % ncell,
             "cell_solves_per_s": ncell / (ms * 1e-3), "ms": ms,
             "failed_cells": int((fl != 0).sum().item()),
             "mean_steps_per_cell": steps / ncell,
@@ -471,50 +545,108 @@ def large_network_form(torch, dev, ncell=SEMENOV_CELLS):
                     "traffic_bytes": dram,
                     "traffic_source": "ncu DRAM bytes per integration step "
                                       "x the steps taken",
-                    "algorithmic_bytes": io,
-                    "algorithmic_gbs": io / (ms * 1e-3) / 1e9}}
+                    "algorithmic_bytes": alg,
+                    "algorithmic_gbs": alg / (ms * 1e-3) / 1e9,
+                    "algorithmic_frac": alg / (ms * 1e-3) / 1e9 / peak,
+                    "algorithmic_bytes_formula":
+                        "nsetups 8 (nnzJ + 2 nnzLU) + nni 8 nnzLU + nfe 8 "
+                        "(nrea + 2 nspec), nnzJ %d, nnzLU %d, counters of "
+                        "this launch" % (nnz_j, nnz_lu),
+                    "cell_io_bytes": io},
+            "cpu_baseline": cpu_form(key, SEMENOV_BATCH, cpu_cells, 0,
+                                     workloads.OPTIONS[key])
+            if cpu_cells > 0 else None}
 
 
-def batching_form(torch, dev, ncell=65536, reps=2):
-    """the batching workload's launch forms on one solve of its cells (the
-    first call of the hydro loop: the uneven-stiffness primordial3 batch;
-    65,536 cells of its distribution keep the warp forms within seconds):
-    one lane or one warp per cell, each as a persistent work-queue grid or
-    a plain one-cell-per-lane (warp) grid, device-timed, best of reps"""
-    from krome_x_b200 import krome
+def batching_form(torch, dev, ncell=262144, calls=3):
+    """the batching workload itself (262,144 primordial3 cells of rank 0's
+    seeded batch, the captured hydro loop's first `calls` calls: the first,
+    stiffest solve from the initial conditions, then hydro steps) with each
+    launch form: one lane or one warp per cell, each as a persistent
+    work-queue grid or a plain one-cell-per-lane (warp) grid; device-timed,
+    every form from the same inputs"""
+    from krome_x_b200 import krome, workloads
     info, n, T, dt, par = inputs(ncell, seed=rank_seed(0))
     net = krome.load(NETWORK)
     t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
-    dtd, pd = t(dt), t(par)
-    out = {"workload": "primordial3, %d cells, one solve (dt = 0.01 tff), "
-                       "rtol 1e-6" % ncell}
+    out = {"workload": "primordial3, %d cells, the hydro loop's first %d "
+                       "calls (tff, n x1.01, dt = 0.01 tff; the first call "
+                       "from the initial conditions), rtol 1e-6"
+                       % (ncell, calls)}
     for layout in ("lane", "warp"):
         for kernel in ("persistent", "plain"):
             o = net.options(evolve_T=1, jac="auto", linsol="auto", rtol=RTOL,
                             atol_n=1e-20, atol_T=1e-6, kernel=kernel,
                             layout=1 if layout == "lane" else 0, lane_minb=2)
-            best, failed = None, 0
-            for _ in range(reps):
-                nd, Td = t(n), t(T)
-                fl = torch.zeros(ncell, dtype=torch.int32, device=dev)
-                cur = torch.zeros(1, dtype=torch.int32, device=dev)
+            nd, Td, pd = t(n), t(T), t(par)
+            dtd = t(dt)
+            fl = torch.zeros(ncell, dtype=torch.int32, device=dev)
+            cur = torch.zeros(1, dtype=torch.int32, device=dev)
+            per_call, failed = [], 0
+            for c in range(calls):
                 torch.cuda.synchronize()
                 e0 = _events(torch)
-                net.solve_device(nd, Td, dtd, pd, fl, opts=o, cursor=cur)
+                if c == 0:
+                    net.solve_device(nd, Td, dtd, pd, fl, opts=o, cursor=cur)
+                else:  # the collapse step and the solve on the device arrays
+                    r = net._lib.krome_b200_hydro_step(
+                        ncell, nd.data_ptr(), Td.data_ptr(), dtd.data_ptr(),
+                        pd.data_ptr(), net.npar, net.params.index("tff"),
+                        1.01, 0.01, fl.data_ptr(), None, cur.data_ptr(),
+                        o._h, None)
+                    assert r == 0, r
                 e1 = _events(torch)
                 torch.cuda.synchronize()
-                ms = e0.elapsed_time(e1)
-                best = ms if best is None else min(best, ms)
-                failed = int((fl != 0).sum().item())
+                per_call.append(e0.elapsed_time(e1))
+                failed += int((fl != 0).sum().item())
+            ms = sum(per_call)
             out["%s_%s" % (layout, kernel)] = {
-                "cell_solves_per_s": ncell / (best * 1e-3), "ms": best,
-                "failed_cells": failed}
+                "cell_solves_per_s": calls * ncell / (ms * 1e-3), "ms": ms,
+                "ms_per_call": per_call, "failed_cell_solves": failed}
     out["persistent_lane_over_plain_warp"] = (
         out["lane_persistent"]["cell_solves_per_s"]
         / out["warp_plain"]["cell_solves_per_s"])
+    out["persistent_over_plain_lane_layout"] = (
+        out["lane_persistent"]["cell_solves_per_s"]
+        / out["lane_plain"]["cell_solves_per_s"])
     out["persistent_over_plain_warp_layout"] = (
         out["warp_persistent"]["cell_solves_per_s"]
         / out["warp_plain"]["cell_solves_per_s"])
+    return out
+
+
+def small_form(torch, dev, reps=5, cpu=True):
+    """the plain method on its small CPU-runnable workload: 4,096 primordial
+    cells (cooling ATOMIC, H2; heating CHEM, COMPRESS), dt = 3.15e10 s,
+    rtol 1e-6, the analytic (hybrid) Jacobian, dense LU; device-timed, best
+    of reps, beside the reference's krome_solve_cells on the same cells"""
+    from krome_x_b200 import krome, netinfo, workloads
+    key, N = "primordial", 4096
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.primordial(N, info, seed=rank_seed(0))
+    net = krome.load(key)
+    o = workloads.OPTIONS[key]
+    opts = net.options(**o)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    best, failed = None, 0
+    for _ in range(reps):
+        nd, Td = t(n), t(T)
+        fl = torch.zeros(N, dtype=torch.int32, device=dev)
+        cur = torch.zeros(1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        e0 = _events(torch)
+        net.solve_device(nd, Td, t(dt), t(par), fl, opts=opts, cursor=cur)
+        e1 = _events(torch)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+        failed = int((fl != 0).sum().item())
+    out = {"workload": "primordial, 4,096 cells, dt 3.15e10 s, rtol 1e-6, "
+                       "analytic Jacobian, dense LU",
+           "cell_solves_per_s": N / (best * 1e-3), "ms": best,
+           "failed_cells": failed, "reps": reps}
+    if cpu:
+        out["cpu_baseline"] = cpu_form(key, N, N, rank_seed(0), o, reps=3)
     return out
 
 
@@ -589,9 +721,13 @@ def run_ours(args, rank, world, local):
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
+    # the timed steps are the graph replays (the hydro step: compression
+    # and the solve), each bracketed by events on the launching stream; the
+    # L2 flush and the counter sums between them are not steps
+    bracket = ev0.elapsed_time(ev1) / 1e3
     kernel_s = sum(a.elapsed_time(b) for a, b in zip(kst, ken)) / 1e3
-    elapsed, kernel_s = job_times([elapsed, kernel_s], dev, world)
+    bracket, kernel_s = job_times([bracket, kernel_s], dev, world)
+    elapsed = kernel_s
     stats_sum = stats_acc.cpu().numpy().astype(float)
     n_failed = int(fails.item())
     value = job_rate(args.steps * ncell, world, elapsed)
@@ -634,20 +770,24 @@ def run_ours(args, rank, world, local):
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
-        forms = {"batching": batching_form(torch, dev),
-                 "adjoint": adjoint_form(torch, dev),
-                 "precision": precision_form(torch, dev),
-                 "large_network": large_network_form(torch, dev,
-                                                     args.large_cells)}
+        cpu_forms = not args.no_cpu_baseline
+        forms = {"small": small_form(torch, dev, cpu=cpu_forms),
+                 "batching": batching_form(torch, dev, ncell),
+                 "adjoint": adjoint_form(torch, dev, cpu=cpu_forms),
+                 "precision": precision_form(torch, dev, cpu=cpu_forms),
+                 "large_network": large_network_form(
+                     torch, dev, args.large_cells,
+                     args.large_cpu_cells if cpu_forms else 0)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_leg(args.cpu_cells, args.warmup, args.steps)
+        r = cpu_leg(args.cpu_cells, args.cells, args.warmup, args.steps)
         cpu = {"value": r["value"], "unit": "cell-solves/s",
                "cores": r["threads"], "kind": r["kind"],
-               "sample": "%d cells x %d loop calls (after %d warm-up calls) "
-                         "of the same seeded workload, reference "
-                         "krome_solve_cells with OpenMP over cells"
-                         % (r["cells"], r["steps"], args.warmup)}
+               "sample": "the first %d cells of the timed %d-cell batch "
+                         "x %d loop calls (after %d warm-up calls), the "
+                         "reference's krome_solve_cells with OpenMP over "
+                         "cells" % (r["cells"], ncell, r["steps"],
+                                    args.warmup)}
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -665,6 +805,10 @@ def run_ours(args, rank, world, local):
                    "network": NETWORK, "cells_per_gpu": ncell,
                    "global_cells": ncell * world, "parallelism": "dp%d" % world,
                    "l2": "256 MB flush buffer written between steps",
+                   "timed": "each step's graph replay between CUDA events "
+                            "on its stream (the flush and the counter sums "
+                            "between steps excluded)",
+                   "ms_per_step_with_flush": 1e3 * bracket / args.steps,
                    "failed_cell_solves": n_failed,
                    "counters_per_cell_solve": s},
         "e2e": {"value": e2e_value, "unit": "cell-solves/s",

@@ -114,13 +114,17 @@ int krome_solve_cells_x(int ncell, double* x, const double* rho,
  * layouts: species-major n[i * ld + c] (ld >= ncell; 0: ncell, a Fortran
  * n(ld, nspec)) or cell-major n[c * nspec + i]. Tgas, dt (and rho) [ncell]
  * on the device; par device rows (par_stride 0 or npar) or NULL for the
- * defaults; extra must be NULL; flags[ncell] on the device, may be NULL;
+ * defaults; extra->Phi the cells' photon field (device rows, with photon
+ * bins on the handle); flags[ncell] on the device, may be NULL;
  * summary (host, may be NULL) counts the cells: solved on the device,
  * recovered on the host (always 0: there is no CPU fallback), failed. The
- * device is synchronized before and after the call. Returns 0, the lowest
- * failing cell's flag, -105 (a required parameter unset in some row:
- * nothing integrated), -104 (unsupported configuration or a CUDA error),
- * -111 (no device memory for the staging buffer) or -1 (bad arguments). */
+ * lane-per-cell kernel (the default) reads and writes the caller's layout
+ * and converts mass fractions itself; the other kernels stage through
+ * cell-major copies. The device is synchronized before and after the
+ * call. Returns 0, the lowest failing cell's flag, -105 (a required
+ * parameter unset in some row: nothing integrated), -104 (unsupported
+ * configuration or a CUDA error), -111 (no device memory for the staging
+ * buffer) or -1 (bad arguments). */
 #define KROME_LAYOUT_SPECIES_MAJOR 0
 #define KROME_LAYOUT_CELL_MAJOR 1
 typedef struct {
@@ -142,6 +146,20 @@ int krome_solve_cells_x_device(int ncell, double* x, const double* rho,
                                int par_stride, const krome_cells* extra,
                                int* flags, krome_device_summary* summary,
                                const krome_opts* h);
+
+/* krome.h:351-360: krome_conserve_cells and _x (below) on device arrays in
+ * either layout above; ref [rows][nelem], par and flags on the device too.
+ * One thread per cell; the device is synchronized before the call. Returns
+ * the lowest failing cell's flag (negative), 0, -104 (a CUDA error) or -1
+ * (bad arguments). */
+int krome_conserve_cells_device(int ncell, double* n, int layout, long ld,
+                                const double* ref, int ref_stride,
+                                const double* par, int par_stride,
+                                int* flags);
+int krome_conserve_cells_x_device(int ncell, double* x, int layout, long ld,
+                                  const double* ref, int ref_stride,
+                                  const double* par, int par_stride,
+                                  int* flags);
 
 /* krome_get_rates (reference krome.h:387-389): k[ncell][nrea] at each
  * cell's rate temperature clamp(Tgas, Tcmb, 1e9), the photo rates of

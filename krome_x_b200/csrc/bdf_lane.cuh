@@ -101,6 +101,7 @@ struct LaneCell {
   int flag;        // the finished cell's flag (PH_DONE)
   double dt;
   double Tfix;
+  double xin;      // mass-fraction input: the fractions' input sum
   Params p;
   bool hitT0;
   int restarts;
@@ -153,8 +154,7 @@ struct LaneCell {
   bool qmax_saved;
 };
 
-// Code size. The control code of the sweep runs on a few lanes at a time
-// and is not where the time goes, but every instruction of it competes with
+// Code size. Every instruction of the sweep's control code competes with
 // the rhs for the instruction cache; these switches keep it compact: the
 // control loops rolled (KBL_LOOP, on by default: the primordial3 hydro calls
 // run 12% faster than with the loops unrolled), the vector and step helpers
@@ -162,6 +162,16 @@ struct LaneCell {
 // both off by default (the calls cost more than the code they save).
 #ifndef KBL_LOOP
 #define KBL_LOOP _Pragma("unroll 1")
+#endif
+// the N-vector helpers' loops unrolled (each helper's loads issue together:
+// one memory latency per helper instead of one per element; 3 % on the
+// primordial3 hydro calls), the dense LU's loops as the other control loops
+// (unrolled, the LU's code crowds the rhs out of the instruction cache)
+#ifndef KBL_VLOOP
+#define KBL_VLOOP _Pragma("unroll")
+#endif
+#ifndef KBL_LULOOP
+#define KBL_LULOOP KBL_LOOP
 #endif
 #ifndef KBL_VEC
 #define KBL_VEC __forceinline__
@@ -177,11 +187,11 @@ struct LaneCell {
 template <int N>
 __device__ KBL_VEC void axpy_(double a, const double* x, double* y) {
   if (a == 1.0) {
-    KBL_LOOP for (int i = 0; i < N; i++) y[i] += x[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) y[i] += x[i];
   } else if (a == -1.0) {
-    KBL_LOOP for (int i = 0; i < N; i++) y[i] -= x[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) y[i] -= x[i];
   } else {
-    KBL_LOOP for (int i = 0; i < N; i++) y[i] += a * x[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) y[i] += a * x[i];
   }
 }
 template <int N>
@@ -190,105 +200,164 @@ __device__ KBL_VEC void lin_sum_(double a, const double* x, double b,
   if (b == 1.0 && z == y) { axpy_<N>(a, x, z); return; }
   if (a == 1.0 && z == x) { axpy_<N>(b, y, z); return; }
   if (a == 1.0 && b == 1.0) {
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = x[i] + y[i];
     return;
   }
   bool test;
   if ((test = (a == 1.0 && b == -1.0)) || (a == -1.0 && b == 1.0)) {
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = v2[i] - v1[i];
     return;
   }
   if ((test = (a == 1.0)) || b == 1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) + v2[i];
     return;
   }
   if ((test = (a == -1.0)) || b == -1.0) {
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = (c * v1[i]) - v2[i];
     return;
   }
   if (a == b) {
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] + y[i]);
     return;
   }
   if (a == -b) {
-    KBL_LOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
+    KBL_VLOOP for (int i = 0; i < N; i++) z[i] = a * (x[i] - y[i]);
     return;
   }
-  KBL_LOOP for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
+  KBL_VLOOP for (int i = 0; i < N; i++) z[i] = (a * x[i]) + (b * y[i]);
 }
 template <int N>
 __device__ KBL_VEC void scale_(double c, const double* x, double* z) {
-  KBL_LOOP for (int i = 0; i < N; i++) z[i] = c * x[i];
+  KBL_VLOOP for (int i = 0; i < N; i++) z[i] = c * x[i];
 }
 template <int N>
 __device__ KBL_VEC double wrms_(const double* x, const double* w) {
   double sum = 0.0;
-  KBL_LOOP for (int i = 0; i < N; i++) {
+  KBL_VLOOP for (int i = 0; i < N; i++) {
     const double pv = x[i] * w[i];
     sum += pv * pv;
   }
   return ssqrt_(sum / N);
 }
 
-// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457). R is
-// the factors' type: double, or float for the FP32 Newton-matrix form (the
-// factorisation's arithmetic in float; the solve's right-hand side and its
-// accumulation stay double)
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457): the
+// reference's operations in its order. R is the factors' type: double, or
+// float for the FP32 Newton-matrix form (the factorisation's arithmetic in
+// float; the solve's right-hand side and its accumulation stay double).
+//
+// Memory layout of the work. The factors live in the lane's local memory,
+// whose misses cost an L2 round trip; written as plain loops, every element
+// step would wait for one (the reference's loop nest: ~400 dependent steps
+// per factorisation). Here each pivot step touches whole columns at a time:
+// a column is loaded into registers with all its loads in flight (the
+// element loops unrolled over the compile-time N, rows outside the step
+// masked by predicates), so a factorisation waits for ~65 round trips and a
+// solve for ~30; the pivot-step loops stay rolled to keep the code small
+// (it shares the instruction cache with the rhs).
+
+// v[k] for a runtime k (a select chain: v stays in registers)
+template <int N, class T>
+__device__ __forceinline__ T pick_(const T (&v)[N], int k) {
+  T r = v[0];
+  KB_UNROLL for (int i = 1; i < N; i++) if (i == k) r = v[i];
+  return r;
+}
+
 template <int N, class R>
 __device__ KBL_HELPER int getrf_(R* a, int* p) {
-  KBL_LOOP for (int k = 0; k < N; k++) {
+  KBL_LULOOP for (int k = 0; k < N; k++) {
     R* col_k = a + k * N;
+    R c[N];
+    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
+    // the pivot: the first row of largest |a_ik|, i >= k
     int l = k;
-    KBL_LOOP for (int i = k + 1; i < N; i++)
-      if (fabs(col_k[i]) > fabs(col_k[l])) l = i;
-    p[k] = l;
-    if (col_k[l] == R(0)) return k + 1;
-    if (l != k) {
-      KBL_LOOP for (int i = 0; i < N; i++) {
-        R* ci = a + i * N;
-        const R t = ci[l];
-        ci[l] = ci[k];
-        ci[k] = t;
+    R cl = pick_<N, R>(c, k);
+    KB_UNROLL for (int i = 1; i < N; i++)
+      if (i > k && fabs(c[i]) > fabs(cl)) {
+        l = i;
+        cl = c[i];
       }
+    p[k] = l;
+    if (cl == R(0)) return k + 1;
+    if (l != k) {
+      // rows k and l swap in every column; in registers for column k
+      KB_UNROLL for (int j = 0; j < N; j++) {
+        R* cj = a + j * N;
+        const R t = cj[l];
+        cj[l] = cj[k];
+        cj[k] = t;
+      }
+      const R ck = pick_<N, R>(c, k);
+      KB_UNROLL for (int i = 0; i < N; i++) if (i == l) c[i] = ck;
     }
-    const R mult = R(1) / col_k[k];
-    KBL_LOOP for (int i = k + 1; i < N; i++) col_k[i] *= mult;
-    KBL_LOOP for (int j = k + 1; j < N; j++) {
+    const R mult = R(1) / cl;
+    KB_UNROLL for (int i = 0; i < N; i++)
+      if (i > k) {
+        c[i] *= mult;
+        col_k[i] = c[i];
+      }
+    // the trailing columns: a_ij -= a_kj l_ik where a_kj != 0
+    KBL_LULOOP for (int j = k + 1; j < N; j++) {
       R* col_j = a + j * N;
-      const R a_kj = col_j[k];
+      R v[N];
+      KB_UNROLL for (int i = 0; i < N; i++) v[i] = col_j[i];
+      const R a_kj = pick_<N, R>(v, k);
       if (a_kj != R(0)) {
-        KBL_LOOP for (int i = k + 1; i < N; i++) col_j[i] -= a_kj * col_k[i];
+        KB_UNROLL for (int i = 0; i < N; i++)
+          if (i > k) col_j[i] = v[i] - a_kj * c[i];
       }
     }
   }
   return 0;
 }
 template <int N, class R>
-__device__ KBL_HELPER void getrs_(const R* a, const int* p, double* b) {
-  KBL_LOOP for (int k = 0; k < N; k++) {
-    const int pk = p[k];
-    if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
+__device__ KBL_HELPER void getrs_(const R* a, const int* p, double* bv) {
+  double b[N];
+  int pv[N];
+  KB_UNROLL for (int i = 0; i < N; i++) {
+    b[i] = bv[i];
+    pv[i] = p[i];
   }
-  KBL_LOOP for (int k = 0; k < N - 1; k++) {
-    const R* col_k = a + k * N;
-    const double bk = b[k];
-    KBL_LOOP for (int i = k + 1; i < N; i++) b[i] -= (double)col_k[i] * bk;
+  // the row interchanges, in order
+  KBL_LULOOP for (int k = 0; k < N; k++) {
+    const int pk = pick_<N, int>(pv, k);
+    if (pk != k) {
+      const double bk = pick_<N, double>(b, k), bp = pick_<N, double>(b, pk);
+      KB_UNROLL for (int i = 0; i < N; i++) {
+        if (i == k) b[i] = bp;
+        if (i == pk) b[i] = bk;
+      }
+    }
   }
-  KBL_LOOP for (int k = N - 1; k > 0; k--) {
+  // L y = b (unit diagonal), then U x = y
+  KBL_LULOOP for (int k = 0; k < N - 1; k++) {
     const R* col_k = a + k * N;
-    b[k] /= (double)col_k[k];
-    const double bk = b[k];
-    KBL_LOOP for (int i = 0; i < k; i++) b[i] -= (double)col_k[i] * bk;
+    R c[N];
+    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
+    const double bk = pick_<N, double>(b, k);
+    KB_UNROLL for (int i = 0; i < N; i++)
+      if (i > k) b[i] -= (double)c[i] * bk;
+  }
+  KBL_LULOOP for (int k = N - 1; k > 0; k--) {
+    const R* col_k = a + k * N;
+    R c[N];
+    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
+    const double bk = pick_<N, double>(b, k) / (double)pick_<N, R>(c, k);
+    KB_UNROLL for (int i = 0; i < N; i++) {
+      if (i == k) b[i] = bk;
+      if (i < k) b[i] -= (double)c[i] * bk;
+    }
   }
   b[0] /= (double)a[0];
+  KB_UNROLL for (int i = 0; i < N; i++) bv[i] = b[i];
 }
 
 template <int N, bool EVT, bool REC = false>
@@ -344,7 +413,7 @@ struct Machine {
 
   __device__ KBL_HELPER int ewt_set(const double* ycur, double* w) {
     if (o.rtol_v) {  // per-species rtol: KROME's per-slot weights
-      KBL_LOOP for (int i = 0; i < N; i++) {
+      KBL_VLOOP for (int i = 0; i < N; i++) {
         const double rt = i < NSPEC ? o.rtol_sp[i < KB_NSP_TOL ? i : 0] : o.rtol;
         const double d = fma(rt, fabs(ycur[i]), s.atol[i]);
         if (!(d > 0.0)) return -1;
@@ -352,14 +421,18 @@ struct Machine {
       }
       return 0;
     }
-    KBL_LOOP for (int i = 0; i < N; i++) w[i] = fabs(ycur[i]);
-    KBL_LOOP for (int i = 0; i < N; i++) w[i] = (o.rtol * w[i]) + s.atol[i];
+    // (in registers: ycur and w may be the same array)
+    double v[N];
+    KB_UNROLL for (int i = 0; i < N; i++) v[i] = (o.rtol * fabs(ycur[i])) + s.atol[i];
     if (s.atolmin0) {
-      double mn = w[0];
-      KBL_LOOP for (int i = 1; i < N; i++) if (w[i] < mn) mn = w[i];
-      if (mn <= 0.0) return -1;
+      double mn = v[0];
+      KB_UNROLL for (int i = 1; i < N; i++) if (v[i] < mn) mn = v[i];
+      if (mn <= 0.0) {
+        KB_UNROLL for (int i = 0; i < N; i++) w[i] = v[i];
+        return -1;
+      }
     }
-    KBL_LOOP for (int i = 0; i < N; i++) w[i] = 1.0 / w[i];
+    KB_UNROLL for (int i = 0; i < N; i++) w[i] = 1.0 / v[i];
     return 0;
   }
 
@@ -628,7 +701,7 @@ struct Machine {
     s.fact32 = o.lu32 && !s.lu64;
     if (s.fact32) {
       KBL_LOOP for (int j = 0; j < N; j++)
-        for (int i = 0; i < N; i++) {
+        KB_UNROLL for (int i = 0; i < N; i++) {
           const int k = i + j * N;
           double a = s.savedJ[k] * c;
           if (i == j) a += 1.0;
@@ -637,11 +710,12 @@ struct Machine {
       return getrf_<N, float>(s.A32, s.piv) > 0 ? LS_LUFACT_FAIL : 0;
     }
     KBL_LOOP for (int j = 0; j < N; j++) {
-      KBL_LOOP for (int i = 0; i < N; i++) {
+      KB_UNROLL for (int i = 0; i < N; i++) {
         const int k = i + j * N;
-        s.A[k] = s.savedJ[k] * c;
+        double v = s.savedJ[k] * c;
+        if (i == j) v += 1.0;
+        s.A[k] = v;
       }
-      s.A[j + j * N] += 1.0;
     }
     if (o.lu32) s.st[ST_NLU64]++;
     return getrf_<N, double>(s.A, s.piv) > 0 ? LS_LUFACT_FAIL : 0;

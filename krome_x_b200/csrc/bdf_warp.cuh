@@ -157,6 +157,37 @@ __device__ __forceinline__ bool warp_any(bool b) { return __any_sync(FULL, b); }
 // terms at thermal_T_ = clamp(T, 2.73, 1e9)); k: NREA scratch; mrow: the
 // per-reaction rate factors exp(m_r) of the adjoint's ln-multipliers, null
 // for none
+// the network's freeze directives (the reference's freeze_rows_ and the
+// frozen rows of jac_cell_, solve_cell.hpp:711-720, 1118-1131): the rows of
+// the species a directive holds for these parameters are zero in the rhs
+// and in the analytic Jacobian
+template <int N>
+KB_HD inline void freeze_rows(const Params& p, double (&f)[N]) {
+#if KB_NFREEZE > 0
+  static_assert(NSPEC <= 64, "frozen-row masks hold 64 species");
+  int idx[KB_NFREEZE];
+  const int m = frozen_species(p, idx);
+  unsigned long long mask = 0;
+  for (int q = 0; q < m; ++q) mask |= 1ull << idx[q];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i)
+    if ((mask >> i) & 1ull) f[i] = 0.0;
+#else
+  (void)p; (void)f;
+#endif
+}
+// J's element (i, j) at i rs + j cs
+template <int N>
+KB_HD inline void freeze_jac_rows(const Params& p, double* J, int rs, int cs) {
+#if KB_NFREEZE > 0
+  int idx[KB_NFREEZE];
+  const int m = frozen_species(p, idx);
+  for (int q = 0; q < m; ++q)
+    for (int j = 0; j < N; ++j) J[idx[q] * rs + j * cs] = 0.0;
+#else
+  (void)p; (void)J; (void)rs; (void)cs;
+#endif
+}
+
 template <int N, bool EVT>
 __device__ __forceinline__ void full_rhs(const double (&yf)[N], double (&f)[N],
                                          const Params& p, double Tfix,
@@ -177,6 +208,7 @@ __device__ __forceinline__ void full_rhs(const double (&yf)[N], double (&f)[N],
     const double Tth = fmin(fmax(yf[N - 1], 2.73), 1e9);
     f[N - 1] = thermal_dTdt(Tth, yf, k, p);
   }
+  freeze_rows(p, f);
 }
 
 // the integrator's view of the rhs (rhs_host_, solve_cell.hpp:794-813):
@@ -828,6 +860,10 @@ struct Cell {
         __syncwarp();
       }
       const int jr = (o->jac == 2) ? dq_jac_() : analytic_jac_();
+      if (o->jac != 2) {  // the frozen species' rows of the analytic J
+        if (lane == 0) freeze_jac_rows<N>(p, sJ, N, 1);
+        __syncwarp();
+      }
       if (jr > 0) retval = 1;
     }
     if (retval == 0) {
@@ -1093,9 +1129,6 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
   c.ncfn_ = 0;
   params_from_row(prow, c.p);
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
-#if KB_NFREEZE > 0
-  if (freeze_active(c.p)) return -104;  // frozen rows are not built
-#endif
   photo_rates_of_cell(c.p, cell, so);
   const double T0 = *Tg;
   c.Tfix = T0;
@@ -1146,7 +1179,7 @@ __device__ int solve_cell(double* __restrict__ n, double* __restrict__ Tg,
         cn[i] = __shfl_sync(FULL, v, i);
         c0[i] = __shfl_sync(FULL, v0, i);
       }
-      if (lane == 0) kbnet::conserve_cell(c0, cn, so.conserve);
+      if (lane == 0) kbnet::conserve_cell(c0, cn, so.conserve, c.p);
       KB_UNROLL for (int i = 0; i < NSPEC; ++i) {
         const double ci = __shfl_sync(FULL, cn[i], 0);
         if (lane == i) v = ci;

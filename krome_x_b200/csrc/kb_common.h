@@ -19,6 +19,23 @@
 #define KB_UNROLL
 #endif
 
+// The special functions of the network math (rates, cooling, heating) are
+// called through these wrappers, which the device code keeps out of line:
+// the generated rates and thermal terms call exp / log / pow at ~130 sites
+// per rhs, and CUDA's math routines inlined at every site made the rhs code
+// larger than the instruction caches serve, so the lane kernel stalled on
+// instruction fetch. Out of line, the primordial3 hydro-loop calls ran
+// 16-20 % faster on the B200. The values are the math library's, unchanged.
+#if defined(__CUDACC__)
+#define KB_MATH static __host__ __device__ __noinline__
+#else
+#define KB_MATH static inline
+#endif
+KB_MATH double kb_exp(double x) { return std::exp(x); }
+KB_MATH double kb_log(double x) { return std::log(x); }
+KB_MATH double kb_log10(double x) { return std::log10(x); }
+KB_MATH double kb_pow(double x, double y) { return std::pow(x, y); }
+
 namespace kbc {
 constexpr double boltzmann_eV = 8.617333262145179e-05;
 constexpr double boltzmann_erg = 1.380649e-16;

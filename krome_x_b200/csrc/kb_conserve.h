@@ -26,10 +26,10 @@
 // the clipped state, at most 20 passes, until the largest relative
 // mismatch is below 1e-13.
 //
-// Opaque species never move. On networks with freeze directives a cell
-// whose freeze condition holds is refused (-104) before any solve, so the
-// post-solve conservation never meets a frozen species. Included inside the
-// network namespace after the species tables; n0 and n are a cell's NSPEC
+// Opaque species never move, nor do the species a freeze directive holds
+// for the cell's parameters (the reference's conserved_fixed_,
+// solve_cell.hpp:1442-1450). Included inside the network namespace after
+// the species tables and the parameters; n0 and n are a cell's NSPEC
 // densities in any memory the caller can address.
 #pragma once
 
@@ -158,17 +158,34 @@ KB_HD inline double cons_charge(const double* n, int skip = -1) {
   return q;
 }
 
+// the species that do not move for a cell with parameters p: the opaque
+// ones and those a freeze directive holds
+KB_HD inline void conserved_fixed(const Params& p, bool* fixed) {
+  for (int i = 0; i < NSPEC; ++i) fixed[i] = species_opaque(i) != 0;
+#if KB_NFREEZE > 0
+  int idx[KB_NFREEZE];
+  const int m = frozen_species(p, idx);
+  for (int q = 0; q < m; ++q) fixed[idx[q]] = true;
+#else
+  (void)p;
+#endif
+}
+
 // the post-solve conservation of a solved cell n against its input n0
-// (mode 0: none)
-KB_HD inline void conserve_cell(const double* n0, double* n, int mode) {
+// (mode 0: none); mode 3 sets the electrons even while a freeze directive
+// holds them (the reference's order: applied after the solve)
+KB_HD inline void conserve_cell(const double* n0, double* n, int mode,
+                                const Params& p) {
   if (mode <= 0) return;
   const int e = IDX_ELECTRON;
   if (mode == 3) {
     if (e >= 0) n[e] = std::fmax(cons_charge(n, e), 0.0);
     return;
   }
+  bool fixed[NSPEC];
+  conserved_fixed(p, fixed);
   if (mode == 1) {
-    if (e >= 0 && !species_opaque(e))
+    if (e >= 0 && !fixed[e])
       n[e] = std::fmax(n[e] + (cons_charge(n) - cons_charge(n0)), 0.0);
     return;
   }
@@ -179,7 +196,7 @@ KB_HD inline void conserve_cell(const double* n0, double* n, int mode) {
     target[k] = t;
   }
   bool movable[NSPEC];
-  for (int i = 0; i < NSPEC; ++i) movable[i] = !species_opaque(i);
+  for (int i = 0; i < NSPEC; ++i) movable[i] = !fixed[i];
   cons_project(n, target, NELEM + 1, movable);
 }
 
@@ -220,14 +237,23 @@ KB_HD inline int conserve_to_n(double* n, const double* ref,
   return 0;
 }
 
+// consistent advection of a cell with parameters p (its frozen species do
+// not move)
+KB_HD inline int conserve_to(double* n, const double* ref, const Params& p) {
+  bool fixed[NSPEC];
+  conserved_fixed(p, fixed);
+  return conserve_to_n(n, ref, fixed);
+}
+
 // the same with mass fractions x and ref per gram: n = x / m per gram,
 // corrected, x = m n; a species without mass does not move
-KB_HD inline int conserve_to_x(double* x, const double* ref) {
+KB_HD inline int conserve_to_x(double* x, const double* ref, const Params& p) {
   bool fixed[NSPEC];
+  conserved_fixed(p, fixed);
   double n[NSPEC];
   for (int i = 0; i < NSPEC; ++i) {
     const double m = species_mass_g(i);
-    fixed[i] = species_opaque(i) || !(m > 0.0);
+    if (!(m > 0.0)) fixed[i] = true;
     n[i] = m > 0.0 ? x[i] / m : 0.0;
   }
   const int f = conserve_to_n(n, ref, fixed);

@@ -24,12 +24,12 @@
 #pragma once
 
 KB_HD inline double cool_sigmoid_(double x, double x0, double s) {
-  return 10.0 / (10.0 + std::exp(-s * (x - x0)));
+  return 10.0 / (10.0 + kb_exp(-s * (x - x0)));
 }
 
 KB_HD inline double wCool_(double logT, double logTmin, double logTmax) {
   const double x = (logT - logTmin) / (logTmax - logTmin);
-  const double w = std::pow(10.0, 200.0 * (cool_sigmoid_(x, -0.2, 50.0)
+  const double w = kb_pow(10.0, 200.0 * (cool_sigmoid_(x, -0.2, 50.0)
                             * cool_sigmoid_(-x, -1.2, 50.0) - 1.0));
   return (w < 1e-199) ? 0.0 : w;
 }
@@ -43,27 +43,27 @@ KB_HD inline double cooling_Atomic(double Tgas, const double* n) {
   double cool = 0.0;
 #ifdef KB_HAS_H
   cool += 1.27e-21 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-          * std::exp(-1.578091e5 / temp) * ne * n[IDX_H];
+          * kb_exp(-1.578091e5 / temp) * ne * n[IDX_H];
 #endif
 #ifdef KB_HAS_He
   cool += 9.38e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-          * std::exp(-2.853354e5 / temp) * ne * n[IDX_He];
+          * kb_exp(-2.853354e5 / temp) * ne * n[IDX_He];
 #endif
 #ifdef KB_HAS_Hej
   cool += 4.95e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-          * std::exp(-6.31515e5 / temp) * ne * n[IDX_Hej];
-  cool += 5.01e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
-          * std::exp(-5.5338e4 / temp) * ne * ne * n[IDX_Hej];
+          * kb_exp(-6.31515e5 / temp) * ne * n[IDX_Hej];
+  cool += 5.01e-27 * kb_pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+          * kb_exp(-5.5338e4 / temp) * ne * ne * n[IDX_Hej];
 #endif
 #ifdef KB_HAS_H
-  cool += 7.5e-19 / (1.0 + std::sqrt(T5)) * std::exp(-1.18348e5 / temp)
+  cool += 7.5e-19 / (1.0 + std::sqrt(T5)) * kb_exp(-1.18348e5 / temp)
           * ne * n[IDX_H];
 #endif
 #ifdef KB_HAS_Hej
-  cool += 9.1e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
-          * std::exp(-1.3179e4 / temp) * ne * ne * n[IDX_Hej];
-  cool += 5.54e-17 * std::pow(temp, -0.397) / (1.0 + std::sqrt(T5))
-          * std::exp(-4.73638e5 / temp) * ne * n[IDX_Hej];
+  cool += 9.1e-27 * kb_pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+          * kb_exp(-1.3179e4 / temp) * ne * ne * n[IDX_Hej];
+  cool += 5.54e-17 * kb_pow(temp, -0.397) / (1.0 + std::sqrt(T5))
+          * kb_exp(-4.73638e5 / temp) * ne * n[IDX_Hej];
 #endif
   return std::fmax(cool, 0.0);
 }
@@ -75,8 +75,8 @@ KB_HD inline double cooling_Atomic(double, const double*) { return 0.0; }
 KB_HD inline double cooling_H2(double Tgas, const double* n) {
   const double temp = Tgas;
   const double T3 = temp * 1e-3;
-  const double logt3 = std::log10(T3);
-  const double logt = std::log10(temp);
+  const double logt3 = kb_log10(T3);
+  const double logt = kb_log10(temp);
   const double logt32 = logt3 * logt3, logt33 = logt32 * logt3,
                logt34 = logt33 * logt3, logt35 = logt34 * logt3,
                logt36 = logt35 * logt3, logt37 = logt36 * logt3,
@@ -88,45 +88,45 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 #ifdef KB_HAS_H
   double fH2H;
   if (temp <= 1e2)
-    fH2H = std::pow(10.0, -16.818342 + 37.383713 * logt3
+    fH2H = kb_pow(10.0, -16.818342 + 37.383713 * logt3
            + 58.145166 * logt32 + 48.656103 * logt33
            + 20.159831 * logt34 + 3.8479610 * logt35) * n[IDX_H];
   else if (temp <= 1e3)
-    fH2H = std::pow(10.0, -24.311209 + 3.5692468 * logt3
+    fH2H = kb_pow(10.0, -24.311209 + 3.5692468 * logt3
            - 11.332860 * logt32 - 27.850082 * logt33
            - 21.328264 * logt34 - 4.2519023 * logt35) * n[IDX_H];
   else if (temp <= 6e3)
-    fH2H = std::pow(10.0, -24.311209 + 4.6450521 * logt3
+    fH2H = kb_pow(10.0, -24.311209 + 4.6450521 * logt3
            - 3.7209846 * logt32 + 5.9369081 * logt33
            - 5.5108049 * logt34 + 1.5538288 * logt35) * n[IDX_H];
   else
-    fH2H = 1.862314467912518e-22 * wCool_(logt, 1.0, std::log10(6e3))
+    fH2H = 1.862314467912518e-22 * wCool_(logt, 1.0, kb_log10(6e3))
            * n[IDX_H];
   cool += fH2H;
 #endif
 #ifdef KB_HAS_Hj
   double fH2Hp;
   if (temp > 1e1 && temp <= 1e4)
-    fH2Hp = std::pow(10.0, -22.089523 + 1.5714711 * logt3
+    fH2Hp = kb_pow(10.0, -22.089523 + 1.5714711 * logt3
             + 0.015391166 * logt32 - 0.23619985 * logt33
             - 0.51002221 * logt34 + 0.32168730 * logt35) * n[IDX_Hj];
   else
     fH2Hp = 1.182509139382060e-21 * n[IDX_Hj] * w14;
   cool += fH2Hp;
 #endif
-  cool += w24 * std::pow(10.0, -23.962112 + 2.09433740 * logt3
+  cool += w24 * kb_pow(10.0, -23.962112 + 2.09433740 * logt3
           - 0.77151436 * logt32 + 0.43693353 * logt33
           - 0.14913216 * logt34 - 0.033638326 * logt35) * n[IDX_H2];
 #ifdef KB_HAS_E
   double fH2e;
   if (temp <= 5e2)
-    fH2e = std::pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+    fH2e = kb_pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
            + 96.743155 * logt32 + 343.19180 * logt33
            + 734.71651 * logt34 + 983.67576 * logt35
            + 801.81247 * logt36 + 364.14446 * logt37
            + 70.609154 * logt38, 30.0)) * n[IDX_E];
   else
-    fH2e = std::pow(10.0, -22.921189 + 1.6802758 * logt3
+    fH2e = kb_pow(10.0, -22.921189 + 1.6802758 * logt3
            + 0.93310622 * logt32 + 4.0406627 * logt33
            - 4.7274036 * logt34 - 8.8077017 * logt35
            + 8.9167183 * logt36 + 6.4380698 * logt37
@@ -136,7 +136,7 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 #ifdef KB_HAS_He
   double fH2He;
   if (temp > 1e1 && temp <= 1e4)
-    fH2He = std::pow(10.0, -23.689237 + 2.1892372 * logt3
+    fH2He = kb_pow(10.0, -23.689237 + 2.1892372 * logt3
             - 0.81520438 * logt32 + 0.29036281 * logt33
             - 0.16596184 * logt34 + 0.19191375 * logt35) * n[IDX_He];
   else
@@ -146,22 +146,22 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
   if (cool <= 0.0) return 0.0;
   double HDL;
   if (temp < 2e3) {
-    const double HDLR = 9.5e-22 * std::pow(T3, 3.76)
-                        / (1.0 + 0.12 * std::pow(T3, 2.1))
-                        * std::exp(-std::pow(0.13 / T3, 3.0))
-                        + 3e-24 * std::exp(-0.51 / T3);
-    const double HDLV = 6.7e-19 * std::exp(-5.86 / T3)
-                        + 1.6e-18 * std::exp(-11.7 / T3);
+    const double HDLR = 9.5e-22 * kb_pow(T3, 3.76)
+                        / (1.0 + 0.12 * kb_pow(T3, 2.1))
+                        * kb_exp(-kb_pow(0.13 / T3, 3.0))
+                        + 3e-24 * kb_exp(-0.51 / T3);
+    const double HDLV = 6.7e-19 * kb_exp(-5.86 / T3)
+                        + 1.6e-18 * kb_exp(-11.7 / T3);
     HDL = HDLR + HDLV;
   } else if (temp <= 1e4) {
-    HDL = std::pow(10.0, -20.584225 + 5.0194035 * logt3
+    HDL = kb_pow(10.0, -20.584225 + 5.0194035 * logt3
           - 1.5738805 * logt32 - 4.7155769 * logt33
           + 2.4714161 * logt34 + 5.4710750 * logt35
           - 3.9467356 * logt36 - 2.2148338 * logt37
           + 1.8161874 * logt38);
   } else {
     const double dump14 = 1.0
-        / (1.0 + std::exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
+        / (1.0 + kb_exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
     HDL = 5.531333679406485e-19 * dump14;
   }
   if (HDL == 0.0) return 0.0;
@@ -187,18 +187,18 @@ KB_HD inline CoolAtomicC cooling_Atomic_coef(double Tgas) {
   const double temp = std::fmax(Tgas, 10.0);
   const double T5 = temp / 1e5;
   q.c[0] = 1.27e-21 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-           * std::exp(-1.578091e5 / temp);
+           * kb_exp(-1.578091e5 / temp);
   q.c[1] = 9.38e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-           * std::exp(-2.853354e5 / temp);
+           * kb_exp(-2.853354e5 / temp);
   q.c[2] = 4.95e-22 * std::sqrt(temp) / (1.0 + std::sqrt(T5))
-           * std::exp(-6.31515e5 / temp);
-  q.c[3] = 5.01e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
-           * std::exp(-5.5338e4 / temp);
-  q.c[4] = 7.5e-19 / (1.0 + std::sqrt(T5)) * std::exp(-1.18348e5 / temp);
-  q.c[5] = 9.1e-27 * std::pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
-           * std::exp(-1.3179e4 / temp);
-  q.c[6] = 5.54e-17 * std::pow(temp, -0.397) / (1.0 + std::sqrt(T5))
-           * std::exp(-4.73638e5 / temp);
+           * kb_exp(-6.31515e5 / temp);
+  q.c[3] = 5.01e-27 * kb_pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+           * kb_exp(-5.5338e4 / temp);
+  q.c[4] = 7.5e-19 / (1.0 + std::sqrt(T5)) * kb_exp(-1.18348e5 / temp);
+  q.c[5] = 9.1e-27 * kb_pow(temp, -0.1687) / (1.0 + std::sqrt(T5))
+           * kb_exp(-1.3179e4 / temp);
+  q.c[6] = 5.54e-17 * kb_pow(temp, -0.397) / (1.0 + std::sqrt(T5))
+           * kb_exp(-4.73638e5 / temp);
 #else
   (void)Tgas;
 #endif
@@ -244,8 +244,8 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
 #ifdef KB_HAS_H2
   const double temp = Tgas;
   const double T3 = temp * 1e-3;
-  const double logt3 = std::log10(T3);
-  const double logt = std::log10(temp);
+  const double logt3 = kb_log10(T3);
+  const double logt = kb_log10(temp);
   const double logt32 = logt3 * logt3, logt33 = logt32 * logt3,
                logt34 = logt33 * logt3, logt35 = logt34 * logt3,
                logt36 = logt35 * logt3, logt37 = logt36 * logt3,
@@ -254,22 +254,22 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
   const double w24 = wCool_(logt, 2.0, 4.0);
   (void)w14; (void)logt36; (void)logt37; (void)logt38;
   if (temp <= 1e2)
-    q.aH = std::pow(10.0, -16.818342 + 37.383713 * logt3
+    q.aH = kb_pow(10.0, -16.818342 + 37.383713 * logt3
            + 58.145166 * logt32 + 48.656103 * logt33
            + 20.159831 * logt34 + 3.8479610 * logt35);
   else if (temp <= 1e3)
-    q.aH = std::pow(10.0, -24.311209 + 3.5692468 * logt3
+    q.aH = kb_pow(10.0, -24.311209 + 3.5692468 * logt3
            - 11.332860 * logt32 - 27.850082 * logt33
            - 21.328264 * logt34 - 4.2519023 * logt35);
   else if (temp <= 6e3)
-    q.aH = std::pow(10.0, -24.311209 + 4.6450521 * logt3
+    q.aH = kb_pow(10.0, -24.311209 + 4.6450521 * logt3
            - 3.7209846 * logt32 + 5.9369081 * logt33
            - 5.5108049 * logt34 + 1.5538288 * logt35);
   else
-    q.aH = 1.862314467912518e-22 * wCool_(logt, 1.0, std::log10(6e3));
+    q.aH = 1.862314467912518e-22 * wCool_(logt, 1.0, kb_log10(6e3));
   if (temp > 1e1 && temp <= 1e4) {
     q.fHp = 1;
-    q.aHp = std::pow(10.0, -22.089523 + 1.5714711 * logt3
+    q.aHp = kb_pow(10.0, -22.089523 + 1.5714711 * logt3
             + 0.015391166 * logt32 - 0.23619985 * logt33
             - 0.51002221 * logt34 + 0.32168730 * logt35);
   } else {
@@ -277,17 +277,17 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
     q.aHp = 1.182509139382060e-21;
     q.bHp = w14;
   }
-  q.aH2 = w24 * std::pow(10.0, -23.962112 + 2.09433740 * logt3
+  q.aH2 = w24 * kb_pow(10.0, -23.962112 + 2.09433740 * logt3
           - 0.77151436 * logt32 + 0.43693353 * logt33
           - 0.14913216 * logt34 - 0.033638326 * logt35);
   if (temp <= 5e2)
-    q.ae = std::pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+    q.ae = kb_pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
            + 96.743155 * logt32 + 343.19180 * logt33
            + 734.71651 * logt34 + 983.67576 * logt35
            + 801.81247 * logt36 + 364.14446 * logt37
            + 70.609154 * logt38, 30.0));
   else
-    q.ae = std::pow(10.0, -22.921189 + 1.6802758 * logt3
+    q.ae = kb_pow(10.0, -22.921189 + 1.6802758 * logt3
            + 0.93310622 * logt32 + 4.0406627 * logt33
            - 4.7274036 * logt34 - 8.8077017 * logt35
            + 8.9167183 * logt36 + 6.4380698 * logt37
@@ -295,7 +295,7 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
   q.be = w24;
   if (temp > 1e1 && temp <= 1e4) {
     q.fHe = 1;
-    q.aHe = std::pow(10.0, -23.689237 + 2.1892372 * logt3
+    q.aHe = kb_pow(10.0, -23.689237 + 2.1892372 * logt3
             - 0.81520438 * logt32 + 0.29036281 * logt33
             - 0.16596184 * logt34 + 0.19191375 * logt35);
   } else {
@@ -304,22 +304,22 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
     q.bHe = w14;
   }
   if (temp < 2e3) {
-    const double HDLR = 9.5e-22 * std::pow(T3, 3.76)
-                        / (1.0 + 0.12 * std::pow(T3, 2.1))
-                        * std::exp(-std::pow(0.13 / T3, 3.0))
-                        + 3e-24 * std::exp(-0.51 / T3);
-    const double HDLV = 6.7e-19 * std::exp(-5.86 / T3)
-                        + 1.6e-18 * std::exp(-11.7 / T3);
+    const double HDLR = 9.5e-22 * kb_pow(T3, 3.76)
+                        / (1.0 + 0.12 * kb_pow(T3, 2.1))
+                        * kb_exp(-kb_pow(0.13 / T3, 3.0))
+                        + 3e-24 * kb_exp(-0.51 / T3);
+    const double HDLV = 6.7e-19 * kb_exp(-5.86 / T3)
+                        + 1.6e-18 * kb_exp(-11.7 / T3);
     q.HDL = HDLR + HDLV;
   } else if (temp <= 1e4) {
-    q.HDL = std::pow(10.0, -20.584225 + 5.0194035 * logt3
+    q.HDL = kb_pow(10.0, -20.584225 + 5.0194035 * logt3
           - 1.5738805 * logt32 - 4.7155769 * logt33
           + 2.4714161 * logt34 + 5.4710750 * logt35
           - 3.9467356 * logt36 - 2.2148338 * logt37
           + 1.8161874 * logt38);
   } else {
     const double dump14 = 1.0
-        / (1.0 + std::exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
+        / (1.0 + kb_exp(std::fmin((temp - 3e4) * 2e-4, 3e2)));
     q.HDL = 5.531333679406485e-19 * dump14;
   }
 #else
@@ -360,8 +360,8 @@ KB_HD inline double cooling_H2_with(const CoolH2C& q, const double* n) {
 KB_HD inline double kpla_(const double* n) {
   const double rho = rho_(n);
   if (rho < 1e-12) return 0.0;
-  const double y = std::log10(std::fmin(rho, 0.5));
-  return std::pow(10.0, 1.000042 * y + 2.14989);
+  const double y = kb_log10(std::fmin(rho, 0.5));
+  return kb_pow(10.0, 1.000042 * y + 2.14989);
 }
 
 KB_HD inline double cooling_Continuum(double Tgas, const double* n) {
@@ -391,7 +391,7 @@ KB_HD inline double dissH2_Martin96(double Tgas_in, const double* n,
        -23125.20, 9.305564, -2.464009, 0.1985955, 743.0600, -1.174242,
        0.7502286, 0.2358848, 2.937507}};
   const double n_H = Hnuclei_(n);
-  const double logT = std::log10(Tgas);
+  const double logT = kb_log10(Tgas);
   const double invT = 1.0 / Tgas;
   const double logT2 = logT * logT;
   const double logT3 = logT2 * logT;
@@ -400,23 +400,23 @@ KB_UNROLL
   for (int i = 0; i < 2; ++i) {
     const double* c = m[i];
     const double logk_h1 = c[0] + c[1] * logT + c[2] * logT2
-        + c[3] * logT3 + c[4] * std::log10(1.0 + c[5] * invT);
+        + c[3] * logT3 + c[4] * kb_log10(1.0 + c[5] * invT);
     const double logk_h2 = c[6] * invT;
     const double logk_l1 = c[7] + c[8] * logT + c[9] * logT2
-        + c[10] * std::log10(1.0 + c[11] * invT);
+        + c[10] * kb_log10(1.0 + c[11] * invT);
     const double logk_l2 = c[12] * invT;
     const double logn_c1 = c[13] + c[14] * logT + c[15] * logT2
         + c[16] * invT;
     const double logn_c2 = c[17] + logn_c1;
-    const double pp = c[18] + c[19] * std::exp(-Tgas / 1.850e3)
-        + c[20] * std::exp(-Tgas / 4.40e2);
-    const double n_c1 = std::pow(10.0, logn_c1);
-    const double n_c2 = std::pow(10.0, logn_c2);
+    const double pp = c[18] + c[19] * kb_exp(-Tgas / 1.850e3)
+        + c[20] * kb_exp(-Tgas / 4.40e2);
+    const double n_c1 = kb_pow(10.0, logn_c1);
+    const double n_c2 = kb_pow(10.0, logn_c2);
     const double logk_CID = logk_h1
-        - (logk_h1 - logk_l1) / (1.0 + std::pow(n_H / n_c1, pp))
+        - (logk_h1 - logk_l1) / (1.0 + kb_pow(n_H / n_c1, pp))
         + logk_h2
-        - (logk_h2 - logk_l2) / (1.0 + std::pow(n_H / n_c2, pp));
-    k_CID += std::pow(10.0, logk_CID);
+        - (logk_h2 - logk_l2) / (1.0 + kb_pow(n_H / n_c2, pp));
+    k_CID += kb_pow(10.0, logk_CID);
   }
   return k_CID;
 }
@@ -431,9 +431,9 @@ KB_HD inline double wd01_fit_(double pre, double c1, double p1, double c2,
   const double scale = pre * (p.d2g / 1e-2);
   const double psi = p.G0 * std::sqrt(Tgas) / n[IDX_E];
   if (psi <= 0.0) return scale;
-  return scale / (1.0 + c1 * std::pow(psi, p1)
-                  * (1.0 + c2 * std::pow(Tgas, q)
-                     * std::pow(psi, p2a + p2b * std::log(Tgas))));
+  return scale / (1.0 + c1 * kb_pow(psi, p1)
+                  * (1.0 + c2 * kb_pow(Tgas, q)
+                     * kb_pow(psi, p2a + p2b * kb_log(Tgas))));
 }
 #endif
 #ifdef KB_EXTERN_H_recombination_on_dust
@@ -495,7 +495,7 @@ KB_HD inline Common common(double Tgas, const Params& p) {
   // (2 pi m_e k T / h^2)^(3/2)
   const double cr = 2.0 * kbc::pi * kbc::e_mass * kbc::boltzmann_erg
       / (kbc::planck_erg * kbc::planck_erg);
-  c.crT15 = std::pow(cr * c.T, 1.5);
+  c.crT15 = kb_pow(cr * c.T, 1.5);
   return c;
 }
 
@@ -504,16 +504,16 @@ KB_HD inline Common common(double Tgas, const Params& p) {
 KB_HD inline Rates hydrogen(const Common& c, double nH0) {
   Rates r;
   const double t4 = c.T * 1e-4;
-  r.alpha = 1e-13 * 4.309 * std::pow(t4, -0.6166)
-      / (1.0 + 0.6703 * std::pow(t4, 0.53));
+  r.alpha = 1e-13 * 4.309 * kb_pow(t4, -0.6166)
+      / (1.0 + 0.6703 * kb_pow(t4, 0.53));
   const double up = r.alpha * c.crT15
-      * std::exp(-c.hck * (kH_ion - kH_alpha) / c.T);
-  r.beta = up * std::exp(-c.hck * kH_alpha / c.T);
-  const double lz = std::log(1.0 + c.z);
+      * kb_exp(-c.hck * (kH_ion - kH_alpha) / c.T);
+  r.beta = up * kb_exp(-c.hck * kH_alpha / c.T);
+  const double lz = kb_log(1.0 + c.z);
   const double g1 = (lz - 7.28) / 0.18, g2 = (lz - 6.73) / 0.33;
   const double K = 1.0 / (kH_alpha * kH_alpha * kH_alpha)
       / (8.0 * kbc::pi * c.Hz)
-      * (1.0 - 0.14 * std::exp(-g1 * g1) + 0.079 * std::exp(-g2 * g2));
+      * (1.0 - 0.14 * kb_exp(-g1 * g1) + 0.079 * kb_exp(-g2 * g2));
   const double KL = K * two_photon_H * nH0;
   r.C = fudge_H * (1.0 + KL) / (1.0 + KL + fudge_H * K * up * nH0);
   return r;
@@ -531,7 +531,7 @@ KB_HD inline double he_continuum(const Common& c, double nH0, double nHe0,
                   / (mH * mass_ratio_He * kbc::clight * kbc::clight));
   const double g = 3.0 * A * nHe0 / nH0
       / (std::sqrt(kbc::pi) * sigma * 8.0 * kbc::pi * doppler * k_line * k_line);
-  return A / (1.0 + a * std::pow(g, b));
+  return A / (1.0 + a * kb_pow(g, b));
 }
 
 // (1 - e^-tau) / tau, 1 for an optically thin line
@@ -541,8 +541,8 @@ KB_HD inline double escape(double tau) {
 
 // the He I recombination fits (square-root terms shared by both)
 KB_HD inline double he_alpha(double s0, double s1, double lg, double e) {
-  return std::pow(10.0, lg) / (s0 * std::pow(1.0 + s0, 1.0 - e))
-      / std::pow(1.0 + s1, 1.0 + e);
+  return kb_pow(10.0, lg) / (s0 * kb_pow(1.0 + s0, 1.0 - e))
+      / kb_pow(1.0 + s1, 1.0 + e);
 }
 
 // He I singlet: the Sobolev escape of 2^1P - 1^1S with the H continuum
@@ -551,9 +551,9 @@ KB_HD inline Rates helium_singlet(const Common& c, double nH0, double nHe0,
   Rates r;
   r.alpha = he_alpha(s0, s1, -10.744, 0.711);
   const double up = 4.0 * r.alpha * c.crT15
-      * std::exp(-c.hck * (kHe1_ion - kHe_2s) / c.T);
-  r.beta = up * std::exp(-c.hck * kHe_2s / c.T);
-  const double boltz = std::exp(std::fmin(c.hck * (kHe_2p - kHe_2s) / c.T, 680.0));
+      * kb_exp(-c.hck * (kHe1_ion - kHe_2s) / c.T);
+  r.beta = up * kb_exp(-c.hck * kHe_2s / c.T);
+  const double boltz = kb_exp(std::fmin(c.hck * (kHe_2p - kHe_2s) / c.T, 680.0));
   const double tau = A2P_singlet / (kHe_2p * kHe_2p * kHe_2p)
       / (8.0 * kbc::pi) * 3.0 * nHe0 / c.Hz;
   const double cont = he_continuum(c, nH0, nHe0, kHe_2p, A2P_singlet,
@@ -571,16 +571,16 @@ KB_HD inline Rates helium_triplet(const Common& c, double nH0, double nHe0,
                                   double s0, double s1) {
   Rates r;
   r.alpha = he_alpha(s0, s1, -10.306, 0.761);
-  const double up = r.alpha * std::exp(-c.hck * kHe2St_ion / c.T) * c.crT15
+  const double up = r.alpha * kb_exp(-c.hck * kHe2St_ion / c.T) * c.crT15
       * (4.0 / 3.0);
-  r.beta = 3.0 * up * std::exp(-c.hck * kHe_2St / c.T);
+  r.beta = 3.0 * up * kb_exp(-c.hck * kHe_2St / c.T);
   const double tau = A2P_triplet * nHe0 * 3.0
       / (8.0 * kbc::pi * c.Hz * kHe_2Pt * kHe_2Pt * kHe_2Pt);
   const double cont = he_continuum(c, nH0, nHe0, kHe_2Pt, A2P_triplet,
                                    sigma_2Pt, 0.66, 0.9) / 3.0;
   const double ru = r.alpha * c.crT15 * (4.0 / 3.0)
       / (A2P_triplet * escape(tau) + cont)
-      * std::exp(-c.hck * (kHe2St_ion - (kHe_2Pt - kHe_2St)) / c.T);
+      * kb_exp(-c.hck * (kHe2St_ion - (kHe_2Pt - kHe_2St)) / c.T);
   r.C = 1.0 / (1.0 + ru);
   return r;
 }
@@ -588,8 +588,8 @@ KB_HD inline Rates helium_triplet(const Common& c, double nH0, double nHe0,
 KB_HD inline void helium(double Tgas, double nH0, double nHe0,
                          const Params& p, Rates& s, Rates& t) {
   const Common c = common(Tgas, p);
-  const double s0 = std::sqrt(c.T / std::pow(10.0, 0.477121));
-  const double s1 = std::sqrt(c.T / std::pow(10.0, 5.114));
+  const double s0 = std::sqrt(c.T / kb_pow(10.0, 0.477121));
+  const double s1 = std::sqrt(c.T / kb_pow(10.0, 5.114));
   s = helium_singlet(c, nH0, nHe0, s0, s1);
   t = helium_triplet(c, nH0, nHe0, s0, s1);
 }

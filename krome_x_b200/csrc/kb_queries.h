@@ -648,14 +648,5 @@ KB_API int krome_get_opacity(int ncell, const double* n, const double* Tgas,
       });
 }
 
-// ---- the equilibrium driver (krome.h:306-330) ----
-KB_API int krome_equilibrium_cells(int ncell, double* n, double* Tgas,
-                                   const double* par, int par_stride,
-                                   const krome_cells* extra, int* flags,
-                                   const krome_opts* h) {
-  (void)par; (void)par_stride; (void)extra;
-  if (h == nullptr || Tgas == nullptr || ncell < 0 || n == nullptr) return -1;
-  if (flags != nullptr)
-    for (int c = 0; c < ncell; ++c) flags[c] = -104;
-  return ncell > 0 ? -104 : 0;
-}
+// (the equilibrium driver, krome_equilibrium_cells, is in krome_b200.cu:
+// it runs the device solve)

@@ -155,6 +155,62 @@ struct RecIO {
   double* yfin;        // [ncell][N]: the final y before the post-solve rules
 };
 
+// where the lane kernel reads and writes each cell's species: the caller's
+// layout (krome.h:311-314: species-major n[i * ld + c], or cell-major
+// n[c * nspec + i]) and, with rho, mass fractions x = m n / rho converted
+// on the way in and out (solve_cell.hpp:2210-2233), so that the device-
+// resident entry points need no staging passes around the solve
+struct CellIO {
+  int layout = 1;               // 0 species-major, 1 cell-major
+  long ld = 0;                  // the species-major leading dimension
+  const double* rho = nullptr;  // [ncell] g cm^-3: the species are x
+  int renormalize = 0;          // x rescaled to its input sum on the way out
+  __device__ __forceinline__ long at(int c, int i) const {
+    return layout == 0 ? (long)i * ld + c : (long)c * kbnet::NSPEC + i;
+  }
+};
+
+// x_to_n_ / x_sum_ / n_to_x_out_ (solve_cell.hpp:2210-2233): n = rho x / m
+// (0 for a species without mass), x = m n / rho, rescaled to the input sum
+// of the fractions with renormalize_x
+KB_HD inline void x_to_n(const double* x, double rho, double* n) {
+  for (int i = 0; i < kbnet::NSPEC; ++i) {
+    const double m = kbnet::species_mass_g(i);
+    n[i] = m > 0.0 ? rho * x[i] / m : 0.0;
+  }
+}
+KB_HD inline double x_sum(const double* x) {
+  double s = 0.0;
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    if (kbnet::species_mass_g(i) > 0.0) s += x[i];
+  return s;
+}
+KB_HD inline void n_to_x_out(const double* n, double rho, double xin,
+                             int renormalize, double* x) {
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    x[i] = kbnet::species_mass_g(i) * n[i] / rho;
+  if (!renormalize) return;
+  const double s = x_sum(x);
+  if (s > 0.0)
+    for (int i = 0; i < kbnet::NSPEC; ++i) x[i] *= xin / s;
+}
+
+// cell c's input densities from the caller's arrays (xin: the input sum of
+// the mass fractions)
+__device__ __forceinline__ void cell_densities(const double* n, const CellIO& io,
+                                               int c, double* nc, double* xin) {
+  using namespace kbnet;
+  double v[NSPEC];
+  KB_UNROLL for (int i = 0; i < NSPEC; ++i) v[i] = n[io.at(c, i)];
+  if (io.rho == nullptr) {
+    KB_UNROLL for (int i = 0; i < NSPEC; ++i) nc[i] = v[i];
+    *xin = 0.0;
+    return;
+  }
+  *xin = x_sum(v);
+  x_to_n(v, io.rho[c], nc);
+}
+
 // start cell c on this lane: false when the cell needs no integration
 // (its flag is written here)
 template <bool EVT, bool REC>
@@ -163,7 +219,7 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
                            const double* n, const double* T, const double* dt,
                            const double* par, int pstride, int* flags,
                            long* stats, const SolveOpts& so,
-                           const RecIO& rio) {
+                           const RecIO& rio, const CellIO& io) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   const double dtc = dt[c];
@@ -184,7 +240,8 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   }
   kbw::photo_rates_of_cell(s.p, c, so);
 #if KB_NFREEZE > 0
-  if (freeze_active(s.p)) {  // frozen rows are not built: refused
+  // the adjoint does not differentiate frozen rows: refused there
+  if (REC && freeze_active(s.p)) {
     if (flags != nullptr) flags[c] = -104;
     return false;
   }
@@ -201,7 +258,7 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   s.restarts = 0;
   for (int i = 0; i < NSTAT; ++i) s.tot[i] = 0;
   double y0[N];
-  KB_UNROLL for (int i = 0; i < NSPEC; ++i) y0[i] = n[(long)c * NSPEC + i];
+  cell_densities(n, io, c, y0, &s.xin);
   if (EVT) y0[N - 1] = T[c];
   double amin = 1e300;
   KB_UNROLL for (int i = 0; i < N; ++i) {
@@ -222,7 +279,8 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
 template <bool EVT, bool REC>
 __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
                             double* n, double* T, int* flags, long* stats,
-                            const SolveOpts& so, const RecIO& rio) {
+                            const SolveOpts& so, const RecIO& rio,
+                            const CellIO& io) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   const int c = s.cell;
@@ -250,11 +308,17 @@ __device__ void lane_finish(kbl::LaneCell<LaneGeo<EVT>::N>& s, int flag,
       nv[i] = v;
     }
     if (so.conserve > 0) {  // against the cell's input, still in n
-      double n0[NSPEC];
-      KB_UNROLL for (int i = 0; i < NSPEC; ++i) n0[i] = n[(long)c * NSPEC + i];
-      kbnet::conserve_cell(n0, nv, so.conserve);
+      double n0[NSPEC], x0;
+      cell_densities(n, io, c, n0, &x0);
+      kbnet::conserve_cell(n0, nv, so.conserve, s.p);
     }
-    KB_UNROLL for (int i = 0; i < NSPEC; ++i) n[(long)c * NSPEC + i] = nv[i];
+    if (io.rho != nullptr) {
+      double xv[NSPEC];
+      n_to_x_out(nv, io.rho[c], s.xin, io.renormalize, xv);
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) n[io.at(c, i)] = xv[i];
+    } else {
+      KB_UNROLL for (int i = 0; i < NSPEC; ++i) n[io.at(c, i)] = nv[i];
+    }
     if (EVT) T[c] = Tend;
   }
   if (flags != nullptr) flags[c] = flag;
@@ -280,7 +344,8 @@ template <bool EVT, int MINB, bool REC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
 kb_lane_cells(int ncell, double* n, double* T, const double* dt,
               const double* par, int pstride, int* flags, long* stats,
-              SolveOpts so, unsigned* cursor, int persistent, RecIO rio) {
+              SolveOpts so, unsigned* cursor, int persistent, RecIO rio,
+              CellIO io) {
   constexpr int N = LaneGeo<EVT>::N;
   using namespace kbnet;
   constexpr unsigned FULLM = 0xffffffffu;
@@ -305,7 +370,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
     for (int sweep = 0; sweep < 2; ++sweep) {
       // bounded: every iteration consumes a cell index (at most ncell)
       while (s.ph == kbl::PH_DONE) {
-        if (s.cell >= 0) lane_finish<EVT, REC>(s, s.flag, n, T, flags, stats, so, rio);
+        if (s.cell >= 0) lane_finish<EVT, REC>(s, s.flag, n, T, flags, stats, so, rio, io);
         int c;
         if (persistent) {
           c = (int)atomicAdd(cursor, 1u);
@@ -314,7 +379,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
           static_taken = true;
         }
         if (c >= ncell) s.ph = kbl::PH_IDLE;
-        else lane_start<EVT, REC>(s, m, c, n, T, dt, par, pstride, flags, stats, so, rio);
+        else lane_start<EVT, REC>(s, m, c, n, T, dt, par, pstride, flags, stats, so, rio, io);
       }
       if (s.ph != kbl::PH_IDLE) m.sweep();
       if (!__any_sync(FULLM, s.ph == kbl::PH_DONE)) break;
@@ -476,6 +541,7 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
         const int fb = mbad ? (__ffs(mbad) - 1 - base) : N;
         if (!dq) {
           KBL_LOOP for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
+          kbw::freeze_jac_rows<N>(s.p, s.savedJ, 1, N);
           s.ls_retval = 0;
         } else {
           KBL_LOOP for (int i = 0; i < N * N; ++i) s.savedJ[i] = myblk[i];
@@ -554,7 +620,7 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
       }
       if (so.conserve > 0) {  // thread 0, against the input still in nrow
         __syncthreads();
-        if (threadIdx.x == 0) conserve_cell(nrow, yout, so.conserve);
+        if (threadIdx.x == 0) conserve_cell(nrow, yout, so.conserve, P.p);
         __syncthreads();
       }
       for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) nrow[i] = yout[i];
@@ -652,6 +718,51 @@ struct DevBuf {
 };
 DevBuf g_buf;
 
+// A host-array call's device staging: a buffer and a stream of its own.
+// Concurrent host callers each take an idle slot -- the reference's
+// private-buffer fallback for a busy device cache (solve_kokkos.hpp:
+// 1223-1241) --, so their copies and kernels overlap on the GPU instead of
+// queueing behind one lock. A slot is made on first need (per device) and
+// kept for later calls; the pool holds as many slots as calls ever ran at
+// once.
+struct Slot {
+  DevBuf buf;
+  cudaStream_t stream = nullptr;
+  int dev = -1;
+};
+std::mutex g_slot_mu;
+std::vector<Slot*> g_idle;
+Slot* take_slot() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) return nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (size_t i = 0; i < g_idle.size(); ++i)
+      if (g_idle[i]->dev == d) {
+        Slot* s = g_idle[i];
+        g_idle.erase(g_idle.begin() + i);
+        return s;
+      }
+  }
+  Slot* s = new Slot;
+  s->dev = d;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)
+      != cudaSuccess) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+struct SlotLease {
+  Slot* s;
+  SlotLease() : s(take_slot()) {}
+  ~SlotLease() {
+    if (s == nullptr) return;
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    g_idle.push_back(s);
+  }
+};
+
 // the rates that depend on the densities (their dk/dn terms are not in
 // the small networks' analytic Jacobian; the large networks' path takes no
 // jac option)
@@ -740,7 +851,8 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
                    const double* dt, const double* par, int pstride,
                    int* flags, long* stats, unsigned* cursor,
                    cudaStream_t stream, const RecIO* rio = nullptr,
-                   const PhotoArgs& ph = PhotoArgs()) {
+                   const PhotoArgs& ph = PhotoArgs(),
+                   const CellIO& io = CellIO()) {
   SolveOpts so = to_solve_opts(h);
   so.ph_sigma = ph.sigma;
   so.ph_phi = ph.phi;
@@ -812,7 +924,7 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
     const RecIO none{nullptr, 0, nullptr, 0, nullptr, nullptr};
     kern<<<(int)blocks, threads, lsmem, stream>>>(
         ncell, n, T, dt, par, pstride, flags, stats, so, cursor, h.kernel,
-        rio != nullptr ? *rio : none);
+        rio != nullptr ? *rio : none, io);
     return cudaGetLastError();
   }
   const size_t smem = sizeof(double) * kWarpsPerBlock * Geo<EVT>::SMEM_DOUBLES;
@@ -846,12 +958,25 @@ cudaError_t launch_any(const krome_opts& h, int ncell, double* n, double* T,
                        const double* dt, const double* par, int pstride,
                        int* flags, long* stats, unsigned* cursor,
                        cudaStream_t stream,
-                       const PhotoArgs& ph = PhotoArgs()) {
+                       const PhotoArgs& ph = PhotoArgs(),
+                       const CellIO& io = CellIO()) {
   return h.evolve_T
       ? launch<true>(h, ncell, n, T, dt, par, pstride, flags, stats, cursor,
-                     stream, nullptr, ph)
+                     stream, nullptr, ph, io)
       : launch<false>(h, ncell, n, T, dt, par, pstride, flags, stats, cursor,
-                      stream, nullptr, ph);
+                      stream, nullptr, ph, io);
+}
+
+// whether a launch of these options reads and writes the caller's layout
+// itself (the lane-per-cell kernel); the other kernels take cell-major
+// densities
+bool fuses_io(const krome_opts& h) {
+#ifdef KB_LARGE_NETWORK
+  (void)h;
+  return false;
+#else
+  return h.layout == 1;
+#endif
 }
 
 bool row_missing(const double* row) {
@@ -1371,13 +1496,13 @@ int solve_host(int ncell, double* n, double* Tgas, const double* dt,
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t total = al(nb) + 2 * al(tb) + al(pb) + al(fb) + al(sb)
                        + al(xb) + al(hb) + 256;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (g_buf.ensure(total) != cudaSuccess) {
+  SlotLease lease;
+  if (lease.s == nullptr || lease.s->buf.ensure(total) != cudaSuccess) {
     if (flags != nullptr)
       for (int c = 0; c < ncell; ++c) flags[c] = -111;
     return -111;
   }
-  char* b = static_cast<char*>(g_buf.p);
+  char* b = static_cast<char*>(lease.s->buf.p);
   double* dn = reinterpret_cast<double*>(b); b += al(nb);
   double* dT = reinterpret_cast<double*>(b); b += al(tb);
   double* ddt = reinterpret_cast<double*>(b); b += al(tb);
@@ -1387,7 +1512,7 @@ int solve_host(int ncell, double* n, double* Tgas, const double* dt,
   double* dxs = reinterpret_cast<double*>(b); b += al(xb);
   double* dphi = reinterpret_cast<double*>(b); b += al(hb);
   unsigned* dcur = reinterpret_cast<unsigned*>(b);
-  cudaStream_t s = 0;
+  cudaStream_t s = lease.s->stream;
   cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, Tgas, tb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ddt, dt, tb, cudaMemcpyHostToDevice, s);
@@ -1417,6 +1542,219 @@ int solve_host(int ncell, double* n, double* Tgas, const double* dt,
   return 0;
 }
 }  // namespace
+
+// ---- the equilibrium driver (reference krome.h:366-376, krome.cpp:
+// 574-617, solve_equilibrium at solve_cell.hpp:2249-2301) ----
+//
+// Every cell integrates to steady state in intervals: outputs at t0,
+// t0 factor, t0 factor^2, ... (each interval a full solve of the cell from
+// its current state), converged when max_i |dn_i| / max(n_i, eatol ntot)
+// (and |dTgas| / Tgas with evolve_T) between two outputs is below ertol,
+// stopped (flag 1, the state returned) at t_max, or failed (a negative
+// flag, the input restored). On the GPU all cells advance together: each
+// interval is one launch of the solve over the batch, in which the cells
+// already done have dt 0 and are skipped, bracketed by two small kernels
+// that keep the per-cell bookkeeping on the device.
+namespace {
+struct EqCells {
+  double* nin;   // [ncell][nspec] the input, restored on failure
+  double* Tin;
+  double* prev;  // the state before the interval
+  double* Tprev;
+  double* t;     // the time integrated
+  double* dt;    // the next interval
+  int* state;    // 0 integrating, 1 done
+  int* out;      // the cell's flag
+};
+struct EqOpts {
+  double t0, tmax, factor, rtol, atol;
+  int evolve_T;
+};
+
+__global__ void kb_eq_init(int ncell, const double* n, const double* T,
+                           EqCells e, double t0) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    e.nin[(long)c * kbnet::NSPEC + i] = n[(long)c * kbnet::NSPEC + i];
+  e.Tin[c] = T[c];
+  e.t[c] = 0.0;
+  e.dt[c] = t0;
+  e.state[c] = 0;
+  e.out[c] = 0;
+}
+
+__global__ void kb_eq_pre(int ncell, const double* n, const double* T,
+                          EqCells e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  if (e.state[c] != 0) {
+    e.dt[c] = 0.0;  // done: the solve skips the cell
+    return;
+  }
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    e.prev[(long)c * kbnet::NSPEC + i] = n[(long)c * kbnet::NSPEC + i];
+  e.Tprev[c] = T[c];
+}
+
+__global__ void kb_eq_post(int ncell, double* n, double* T, const int* fl,
+                           EqCells e, EqOpts q, unsigned* active) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell || e.state[c] != 0) return;
+  double* nc = n + (long)c * kbnet::NSPEC;
+  if (fl[c] != 0) {  // failed: the input back
+    for (int i = 0; i < kbnet::NSPEC; ++i)
+      nc[i] = e.nin[(long)c * kbnet::NSPEC + i];
+    T[c] = e.Tin[c];
+    e.out[c] = fl[c];
+    e.state[c] = 1;
+    return;
+  }
+  const double t = e.t[c] + e.dt[c];
+  e.t[c] = t;
+  const double floor = q.atol * kbnet::ntot_(nc);
+  double w = q.evolve_T ? fabs(T[c] - e.Tprev[c]) / T[c] : 0.0;
+  for (int i = 0; i < kbnet::NSPEC; ++i)
+    w = fmax(w, fabs(nc[i] - e.prev[(long)c * kbnet::NSPEC + i])
+                    / fmax(nc[i], floor));
+  if (w < q.rtol) {
+    e.out[c] = 0;
+    e.state[c] = 1;
+  } else if (t >= q.tmax) {
+    e.out[c] = 1;
+    e.state[c] = 1;
+  } else {
+    e.dt[c] = fmin((q.factor - 1.0) * t, q.tmax - t);
+    atomicAdd(active, 1u);
+  }
+}
+}  // namespace
+
+// host arrays in place, the krome_solve_cells conventions; handle keys
+// eq_t0, eq_tmax, eq_factor, eq_rtol, eq_atol; flags[c] 0 converged, 1
+// t_max reached first (state returned), < 0 failed (cell untouched).
+// Returns the flag of the first cell that did not converge (0 if all did).
+KB_API int krome_equilibrium_cells(int ncell, double* n, double* Tgas,
+                                   const double* par, int par_stride,
+                                   const krome_cells* extra, int* flags,
+                                   const krome_opts* h) {
+  using namespace kbnet;
+  if (h == nullptr || Tgas == nullptr || ncell < 0 || n == nullptr) return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != NPAR) return -1;
+  const int B = h->photo.B;
+  const double* phi = extra != nullptr ? extra->Phi : nullptr;
+  if (B > 0 && phi == nullptr) return -103;
+  if (ncell == 0) return 0;
+  const int u = unsupported(*h);
+  if (u != 0) {
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = u;
+    return u;
+  }
+  std::vector<double> dflt(NPAR);
+  krome_params_default(dflt.data());
+  const double* P = par != nullptr ? par : dflt.data();
+  const int ps = par != nullptr ? par_stride : 0;
+  const size_t nb = sizeof(double) * (size_t)ncell * NSPEC;
+  const size_t tb = sizeof(double) * (size_t)ncell;
+  const size_t ib = sizeof(int) * (size_t)ncell;
+  const size_t pb = sizeof(double) * (ps ? (size_t)ncell * ps : (size_t)NPAR);
+  const size_t xb = B > 0 ? sizeof(double) * (size_t)NPHOTO * B : 0;
+  const size_t hb = B > 0 ? sizeof(double) * (size_t)ncell * B : 0;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  // n, T, dt, par, flags, cursor + counter, nin, Tin, prev, Tprev, t,
+  // state, out, photon tables
+  const size_t total = 3 * al(nb) + 6 * al(tb) + al(pb) + 3 * al(ib) + 256
+                       + al(xb) + al(hb);
+  SlotLease lease;
+  if (lease.s == nullptr || lease.s->buf.ensure(total) != cudaSuccess) {
+    if (flags != nullptr)
+      for (int c = 0; c < ncell; ++c) flags[c] = -111;
+    return -111;
+  }
+  char* b = static_cast<char*>(lease.s->buf.p);
+  auto carve = [&](size_t bytes) { char* r = b; b += al(bytes); return r; };
+  double* dn = reinterpret_cast<double*>(carve(nb));
+  double* dT = reinterpret_cast<double*>(carve(tb));
+  double* dp = reinterpret_cast<double*>(carve(pb));
+  int* dfl = reinterpret_cast<int*>(carve(ib));
+  EqCells e;
+  e.nin = reinterpret_cast<double*>(carve(nb));
+  e.Tin = reinterpret_cast<double*>(carve(tb));
+  e.prev = reinterpret_cast<double*>(carve(nb));
+  e.Tprev = reinterpret_cast<double*>(carve(tb));
+  e.t = reinterpret_cast<double*>(carve(tb));
+  e.dt = reinterpret_cast<double*>(carve(tb));
+  e.state = reinterpret_cast<int*>(carve(ib));
+  e.out = reinterpret_cast<int*>(carve(ib));
+  double* dxs = reinterpret_cast<double*>(carve(xb));
+  double* dphi = reinterpret_cast<double*>(carve(hb));
+  unsigned* dcur = reinterpret_cast<unsigned*>(b);
+  unsigned* dact = dcur + 1;
+  const EqOpts q{h->eq_t0, h->eq_tmax, h->eq_factor, h->eq_rtol, h->eq_atol,
+                 h->evolve_T};
+  cudaStream_t s = lease.s->stream;
+  cudaError_t err = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(dT, Tgas, tb, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(dp, P, pb, cudaMemcpyHostToDevice, s);
+  PhotoArgs pa;
+  if (B > 0) {
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(dxs, h->photo.sigma.data(), xb,
+                            cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(dphi, phi, hb, cudaMemcpyHostToDevice, s);
+    pa = PhotoArgs{dxs, dphi, B};
+  }
+  const int tpb = 128, nblk = (ncell + tpb - 1) / tpb;
+  if (err == cudaSuccess) {
+    kb_eq_init<<<nblk, tpb, 0, s>>>(ncell, dn, dT, e, q.t0);
+    err = cudaGetLastError();
+  }
+  // bounded: every interval at least multiplies t by factor (or converges
+  // a cell whose interval is empty); 10,000 intervals is far beyond t_max
+  for (int it = 0; it < 10000 && err == cudaSuccess; ++it) {
+    kb_eq_pre<<<nblk, tpb, 0, s>>>(ncell, dn, dT, e);
+    err = cudaGetLastError();
+    if (err == cudaSuccess)
+      err = launch_any(*h, ncell, dn, dT, e.dt, dp, ps, dfl, nullptr, dcur, s,
+                       pa);
+    if (err == cudaSuccess) err = cudaMemsetAsync(dact, 0, sizeof(unsigned), s);
+    if (err == cudaSuccess) {
+      kb_eq_post<<<nblk, tpb, 0, s>>>(ncell, dn, dT, dfl, e, q, dact);
+      err = cudaGetLastError();
+    }
+    unsigned active = 0;
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(&active, dact, sizeof(unsigned),
+                            cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err == cudaSuccess && active == 0) break;
+  }
+  std::vector<double> hn(nb / sizeof(double)), hT(ncell);
+  std::vector<int> hfl(ncell);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(hn.data(), dn, nb, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(hT.data(), dT, tb, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(hfl.data(), e.out, ib, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) {
+    std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(err));
+    return -104;
+  }
+  std::memcpy(n, hn.data(), nb);
+  std::memcpy(Tgas, hT.data(), tb);
+  int first = 0;
+  for (int c = 0; c < ncell; ++c) {
+    if (flags != nullptr) flags[c] = hfl[c];
+    if (first == 0 && hfl[c] != 0) first = hfl[c];
+  }
+  return first;
+}
 
 KB_API int krome_b200_solve_batch(int ncell, double* n, double* Tgas,
                                   const double* dt, const double* par,
@@ -1449,31 +1787,6 @@ struct krome_device_summary {
 };
 
 namespace {
-// x_to_n_ / n_to_x_ / x_sum_ / n_to_x_out_ (solve_cell.hpp:2210-2233): n =
-// rho x / m (0 for a species without mass), x = m n / rho, rescaled to the
-// input sum of the fractions with renormalize_x
-KB_HD inline void x_to_n(const double* x, double rho, double* n) {
-  for (int i = 0; i < kbnet::NSPEC; ++i) {
-    const double m = kbnet::species_mass_g(i);
-    n[i] = m > 0.0 ? rho * x[i] / m : 0.0;
-  }
-}
-KB_HD inline double x_sum(const double* x) {
-  double s = 0.0;
-  for (int i = 0; i < kbnet::NSPEC; ++i)
-    if (kbnet::species_mass_g(i) > 0.0) s += x[i];
-  return s;
-}
-KB_HD inline void n_to_x_out(const double* n, double rho, double xin,
-                             int renormalize, double* x) {
-  for (int i = 0; i < kbnet::NSPEC; ++i)
-    x[i] = kbnet::species_mass_g(i) * n[i] / rho;
-  if (!renormalize) return;
-  const double s = x_sum(x);
-  if (s > 0.0)
-    for (int i = 0; i < kbnet::NSPEC; ++i) x[i] *= xin / s;
-}
-
 // species i of cell c in the caller's layout (krome.h:311-314): species-
 // major n[i * ld + c] (0) or cell-major n[c * nspec + i] (1)
 __device__ __forceinline__ long at_(int layout, long ld, int c, int i) {
@@ -1564,7 +1877,11 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
       for (int c = 0; c < ncell; ++c) summary->failed += hfl[c] != 0;
     return ret;
   }
-  const bool staged = layout == 0 || rho != nullptr;
+  // the lane kernel reads and writes the caller's layout (and converts
+  // mass fractions) itself; the other kernels take staged cell-major
+  // densities
+  const bool fused = fuses_io(*h);
+  const bool staged = !fused && (layout == 0 || rho != nullptr);
   const size_t nb = staged ? sizeof(double) * (size_t)ncell * kbnet::NSPEC : 0;
   const size_t xb = rho != nullptr ? sizeof(double) * (size_t)ncell : 0;
   const size_t pb = par == nullptr ? sizeof(double) * kbnet::NPAR : 0;
@@ -1597,8 +1914,16 @@ int solve_device_entry(int ncell, double* arr, const double* rho, int layout,
     kb_gather_in<<<nblk, tpb>>>(ncell, arr, layout, ld, rho, dn, dx);
     e = cudaGetLastError();
   }
+  CellIO io;
+  if (fused) {
+    io.layout = layout;
+    io.ld = ld;
+    io.rho = rho;
+    io.renormalize = h->renormalize_x;
+  }
   if (e == cudaSuccess)
-    e = launch_any(*h, ncell, dn, Tgas, dt, Pd, ps, dfl, nullptr, dcur, 0, pa);
+    e = launch_any(*h, ncell, dn, Tgas, dt, Pd, ps, dfl, nullptr, dcur, 0, pa,
+                   io);
   if (e == cudaSuccess && staged) {
     kb_scatter_out<<<nblk, tpb>>>(ncell, dn, dfl, layout, ld, rho, dx,
                                   h->renormalize_x, arr);
@@ -1725,23 +2050,21 @@ int conserve_cells_host(int ncell, double* v, const double* ref,
                         int ref_stride, const double* par, int par_stride,
                         int* flags, bool x) {
   using namespace kbnet;
-  (void)par;
   if (ncell < 0 || v == nullptr || ref == nullptr || ref_stride < 0
       || par_stride < 0)
     return -1;
   if (ref_stride != 0 && ref_stride != NELEM) return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != NPAR) return -1;
+  std::vector<double> dflt(NPAR);
+  krome_params_default(dflt.data());
   int ret = 0;
   for (int c = 0; c < ncell; ++c) {
     double* vc = v + (size_t)c * NSPEC;
     const double* rc = ref + (size_t)c * ref_stride;
-    int f;
-    if (x) {
-      f = conserve_to_x(vc, rc);
-    } else {
-      bool fixed[NSPEC];
-      for (int i = 0; i < NSPEC; ++i) fixed[i] = species_opaque(i) != 0;
-      f = conserve_to_n(vc, rc, fixed);
-    }
+    Params p;  // the freeze directives' parameters (NULL: the defaults)
+    params_from_row(par != nullptr ? par + (size_t)c * par_stride
+                                   : dflt.data(), p);
+    const int f = x ? conserve_to_x(vc, rc, p) : conserve_to(vc, rc, p);
     if (flags != nullptr) flags[c] = f;
     if (ret == 0 && f < 0) ret = f;
   }
@@ -1759,6 +2082,95 @@ KB_API int krome_conserve_cells_x(int ncell, double* x, const double* ref,
                                   int par_stride, int* flags) {
   return conserve_cells_host(ncell, x, ref, ref_stride, par, par_stride,
                              flags, true);
+}
+
+// consistent advection on device arrays (reference krome.h:351-360,
+// runtime/core/solve_kokkos.hpp:1787-1823): one thread per cell reads the
+// cell from the caller's layout, moves it to its reference totals with the
+// host path's projection (kb_conserve.h) and writes it back; the lowest
+// failing cell's flag comes back through one 64-bit atomic minimum of
+// (cell << 32 | flag bits), so no second pass is needed
+namespace {
+__global__ void kb_conserve_cells(int ncell, double* v, int mass, int layout,
+                                  long ld, const double* ref, int ref_stride,
+                                  const double* par, int par_stride,
+                                  int* flags, unsigned long long* lowest) {
+  using namespace kbnet;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  double x[NSPEC];
+  for (int i = 0; i < NSPEC; ++i) x[i] = v[at_(layout, ld, c, i)];
+  const double* r = ref + (long)c * ref_stride;
+  Params p;  // the freeze directives' parameters
+  params_from_row(par + (long)c * par_stride, p);
+  const int f = mass ? conserve_to_x(x, r, p) : conserve_to(x, r, p);
+  for (int i = 0; i < NSPEC; ++i) v[at_(layout, ld, c, i)] = x[i];
+  if (flags != nullptr) flags[c] = f;
+  if (f < 0)
+    atomicMin(lowest, ((unsigned long long)c << 32) | (unsigned)f);
+}
+
+int conserve_cells_device(int ncell, double* v, bool mass, int layout,
+                          long ld, const double* ref, int ref_stride,
+                          const double* par, int par_stride, int* flags) {
+  using namespace kbnet;
+  if (ncell < 0 || v == nullptr || ref == nullptr || par_stride < 0)
+    return -1;
+  if (ref_stride != 0 && ref_stride != NELEM) return -1;
+  if (par != nullptr && par_stride != 0 && par_stride != NPAR) return -1;
+  if (layout != 0 && layout != 1) return -1;
+  if (layout == 0) {
+    if (ld == 0) ld = ncell;
+    if (ld < ncell) return -1;
+  }
+  if (ncell == 0) return 0;
+  if (cudaDeviceSynchronize() != cudaSuccess) return -104;
+  std::lock_guard<std::mutex> lock(g_dmu);
+  if (g_dbuf.ensure(256 + sizeof(double) * NPAR) != cudaSuccess) return -111;
+  auto* lowest = static_cast<unsigned long long*>(g_dbuf.p);
+  double* dflt = reinterpret_cast<double*>(static_cast<char*>(g_dbuf.p) + 256);
+  cudaError_t e = cudaMemset(lowest, 0xff, sizeof(unsigned long long));
+  if (e == cudaSuccess && par == nullptr) {  // the default parameter row
+    std::vector<double> row(NPAR);
+    krome_params_default(row.data());
+    e = cudaMemcpy(dflt, row.data(), sizeof(double) * NPAR,
+                   cudaMemcpyHostToDevice);
+  }
+  const int tpb = 128;
+  if (e == cudaSuccess) {
+    kb_conserve_cells<<<(ncell + tpb - 1) / tpb, tpb>>>(
+        ncell, v, mass ? 1 : 0, layout, ld, ref, ref_stride,
+        par != nullptr ? par : dflt, par != nullptr ? par_stride : 0, flags,
+        lowest);
+    e = cudaGetLastError();
+  }
+  unsigned long long key = ~0ull;
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&key, lowest, sizeof(key), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return -104;
+  }
+  return key == ~0ull ? 0 : (int)(unsigned)(key & 0xffffffffull);
+}
+}  // namespace
+
+// krome_conserve_cells and _x on device arrays (krome.h:351-360): v in the
+// species-major (layout 0, leading dimension ld >= ncell, 0 for ncell) or
+// cell-major (1) layout; ref, par and flags on the device too
+KB_API int krome_conserve_cells_device(int ncell, double* n, int layout,
+                                       long ld, const double* ref,
+                                       int ref_stride, const double* par,
+                                       int par_stride, int* flags) {
+  return conserve_cells_device(ncell, n, false, layout, ld, ref, ref_stride,
+                               par, par_stride, flags);
+}
+KB_API int krome_conserve_cells_x_device(int ncell, double* x, int layout,
+                                         long ld, const double* ref,
+                                         int ref_stride, const double* par,
+                                         int par_stride, int* flags) {
+  return conserve_cells_device(ncell, x, true, layout, ld, ref, ref_stride,
+                               par, par_stride, flags);
 }
 
 // x = m n / rho and n = rho x / m (query.hpp:443-449)

@@ -33,6 +33,7 @@ difference-quotient Jacobian column):
   cooling, the EXACT adiabatic index) emitted by the rules the reference
   generator applies (kromex/codegen.py:4900-5000, 6857-6966, 3697-3819).
 """
+import re
 import math
 import os
 import sys
@@ -215,8 +216,7 @@ class Emitter:
         w("constexpr int KB_RATE_NDEP = %d;" % ndep)
         # species a freeze directive can hold (the reference turns its
         # charge-invariant Newton correction off on such networks,
-        # solve_cell.hpp:1631-1642; the frozen rows themselves are not
-        # built here: a cell whose freeze holds is refused)
+        # solve_cell.hpp:1631-1642)
         w("#define KB_NFREEZE %d"
           % sum(len(f["species"]) for f in net.freeze))
         for i, s in enumerate(self.species):
@@ -373,6 +373,26 @@ class Emitter:
                 cond = "true" if f["cond"] is None else self.gen.cexpr(f["cond"])
                 w("  if (%s) return true;  // knet line %d" % (cond, f["line"]))
             w("  return false;")
+            w("}")
+            # the species held while their directive's condition holds:
+            # their rows of the rhs and the Jacobian are zero and they do
+            # not move in the conservation (the reference's generated
+            # frozen_species, used at solve_cell.hpp:711-720, 1118-1131,
+            # 1442-1450)
+            w("KB_HD inline int frozen_species(const Params& p, int* idx) {")
+            w("  (void)p; (void)idx;")
+            w("  int m = 0;")
+            for f in net.freeze:
+                rows = " ".join("idx[m++] = IDX_%s;" % self.cid(sp)
+                                for sp in f["species"])
+                if f["cond"] is None:
+                    w("  %s  // knet line %d" % (rows, f["line"]))
+                else:
+                    w("  if (%s) {  // knet line %d"
+                      % (self.gen.cexpr(f["cond"]), f["line"]))
+                    w("    " + rows)
+                    w("  }")
+            w("  return m;")
             w("}")
         self.pnames = pn
         self.meta = dict(
@@ -1845,7 +1865,14 @@ class Emitter:
             self.emit_rate_parts()
             self.emit_sparse()
         self.emit_tail()
-        return "\n".join(self.lines) + "\n"
+        return outline_math("\n".join(self.lines) + "\n")
+
+
+def outline_math(text):
+    """route the special functions of the emitted code through kb_common.h's
+    wrappers (out of line on the device: one copy of each math routine
+    instead of one per call site)"""
+    return re.sub(r"(?<![\w:])(?:std::)?(exp|log10|log|pow)\(", r"kb_\1(", text)
 
 
 def emit(key):

@@ -137,6 +137,14 @@ KB_HD inline bool freeze_active(const Params& p) {
   if (p.zredshift > 2243.0) return true;  // knet line 45
   return false;
 }
+KB_HD inline int frozen_species(const Params& p, int* idx) {
+  (void)p; (void)idx;
+  int m = 0;
+  if (p.zredshift > 2243.0) {  // knet line 45
+    idx[m++] = IDX_E; idx[m++] = IDX_H; idx[m++] = IDX_H2; idx[m++] = IDX_Hj; idx[m++] = IDX_H2j; idx[m++] = IDX_Hk; idx[m++] = IDX_D; idx[m++] = IDX_Dj; idx[m++] = IDX_HD; idx[m++] = IDX_HDj; idx[m++] = IDX_H2Dj; idx[m++] = IDX_H3j;
+  }
+  return m;
+}
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
@@ -151,40 +159,40 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   (void)Tgas; (void)n; (void)p; (void)k;
   const double vh_invTgas = v_invTgas(Tgas, n, p);
   (void)vh_invTgas;
-  k[2] = 1.4e-18 * std::pow(Tgas, 0.928) * std::exp(-Tgas / 16200.0);  // H + e- -> H-
-  k[3] = 0.11 * std::pow(p.Trad, 2.13) * std::exp(-8823.0 / p.Trad);  // H- -> H + e-
+  k[2] = 1.4e-18 * kb_pow(Tgas, 0.928) * kb_exp(-Tgas / 16200.0);  // H + e- -> H-
+  k[3] = 0.11 * kb_pow(p.Trad, 2.13) * kb_exp(-8823.0 / p.Trad);  // H- -> H + e-
   k[8] = 5.7e-06 * 1.0/(std::sqrt(Tgas)) + 6.3e-08 - 9.2e-11 * std::sqrt(Tgas) + 4.4e-13 * Tgas;  // H- + H+ -> H + H
-  k[9] = std::pow(10.0, -19.38 - 1.523 * std::log10(Tgas) + 1.118 * std::log10(Tgas)*std::log10(Tgas) - 0.1269 * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas));  // H + H+ -> H2+
-  k[10] = 16300000.0 * std::exp(-32400.0 / p.Trad);  // H2+ -> H + H+
+  k[9] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // H + H+ -> H2+
+  k[10] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // H2+ -> H + H+
   k[11] = 6.4e-10;  // H2+ + H -> H2 + H+
   k[12] = 2e-07 * 1.0/(std::sqrt(Tgas));  // H2+ + e- -> H + H
-  k[13] = 90.0 * std::pow(p.Trad, 1.48) * std::exp(-335000.0 / p.Trad);  // H2+ -> H+ + H+ + e-
+  k[13] = 90.0 * kb_pow(p.Trad, 1.48) * kb_exp(-335000.0 / p.Trad);  // H2+ -> H+ + H+ + e-
   k[14] = 2e-09;  // H2+ + H2 -> H3+ + H
-  k[17] = 2.7e-08 * std::pow(Tgas, -1.27) * std::exp(-43000.0 * vh_invTgas);  // H2 + e- -> H + H-
-  k[18] = 4.4e-10 * std::pow(Tgas, 0.35) * std::exp(-102000.0 * vh_invTgas);  // H2 + e- -> H + H + e-
-  k[19] = 290.0 * std::pow(p.Trad, 1.56) * std::exp(-178500.0 / p.Trad);  // H2 -> H2+ + e-
-  k[20] = 7.7e-09 * std::exp(-17560.0 * vh_invTgas);  // H3+ + H -> H2+ + H2
-  k[21] = 4.6e-06 * std::pow(Tgas, -0.65);  // H3+ + e- -> H2 + H
+  k[17] = 2.7e-08 * kb_pow(Tgas, -1.27) * kb_exp(-43000.0 * vh_invTgas);  // H2 + e- -> H + H-
+  k[18] = 4.4e-10 * kb_pow(Tgas, 0.35) * kb_exp(-102000.0 * vh_invTgas);  // H2 + e- -> H + H + e-
+  k[19] = 290.0 * kb_pow(p.Trad, 1.56) * kb_exp(-178500.0 / p.Trad);  // H2 -> H2+ + e-
+  k[20] = 7.7e-09 * kb_exp(-17560.0 * vh_invTgas);  // H3+ + H -> H2+ + H2
+  k[21] = 4.6e-06 * kb_pow(Tgas, -0.65);  // H3+ + e- -> H2 + H
   k[22] = 1e-16;  // H2 + H+ -> H3+
-  k[23] = 1.891e-10 * ipow_<-1>(std::sqrt(Tgas / 9.37) * std::pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * std::pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
-  k[24] = (p.Trad > 1000.0 ? 50.0 * std::pow(p.Trad, 1.63) * std::exp(-590000.0 / p.Trad) : 0.0);  // He+ -> He++ + e-
-  k[31] = 3e-10 * std::exp(-6717.0 * vh_invTgas);  // He + H2+ -> HeH+ + H
+  k[23] = 1.891e-10 * ipow_<-1>(std::sqrt(Tgas / 9.37) * kb_pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * kb_pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
+  k[24] = (p.Trad > 1000.0 ? 50.0 * kb_pow(p.Trad, 1.63) * kb_exp(-590000.0 / p.Trad) : 0.0);  // He+ -> He++ + e-
+  k[31] = 3e-10 * kb_exp(-6717.0 * vh_invTgas);  // He + H2+ -> HeH+ + H
   k[34] = 9.1e-10;  // HeH+ + H -> He + H2+
   k[35] = 1.7e-07 * 1.0/(std::sqrt(Tgas));  // HeH+ + e- -> He + H
   k[36] = 1.3e-09;  // HeH+ + H2 -> H3+ + He
-  k[37] = 0.68 * ipow_<1>(p.Trad) * std::sqrt(p.Trad) * std::exp(-22750.0 / p.Trad);  // HeH+ -> He + H+
-  k[38] = 7800.0 * std::pow(p.Trad, 1.2) * std::exp(-240000.0 / p.Trad);  // HeH+ -> He+ + H
-  k[41] = 3.7e-10 * std::pow(Tgas, 0.28) * std::exp(-43.0 * vh_invTgas);  // D + H+ -> D+ + H
-  k[42] = 3.7e-10 * std::pow(Tgas, 0.28);  // D+ + H -> D + H+
+  k[37] = 0.68 * ipow_<1>(p.Trad) * std::sqrt(p.Trad) * kb_exp(-22750.0 / p.Trad);  // HeH+ -> He + H+
+  k[38] = 7800.0 * kb_pow(p.Trad, 1.2) * kb_exp(-240000.0 / p.Trad);  // HeH+ -> He+ + H
+  k[41] = 3.7e-10 * kb_pow(Tgas, 0.28) * kb_exp(-43.0 * vh_invTgas);  // D + H+ -> D+ + H
+  k[42] = 3.7e-10 * kb_pow(Tgas, 0.28);  // D+ + H -> D + H+
   k[43] = 1e-25;  // D + H -> HD
   k[45] = 6.4e-10;  // HD+ + H -> H+ + HD
   k[46] = 2.1e-09;  // D+ + H2 -> H+ + HD
-  k[48] = 1e-09 * std::exp(-464.0 * vh_invTgas);  // HD + H+ -> H2 + D+
-  k[49] = (2.1 - 0.4 * std::log10(Tgas)) * 1e-09;  // HD + H3+ -> H2 + H2D+
-  k[50] = std::pow(10.0, -19.38 - 1.523 * std::log10(Tgas) + 1.118 * std::log10(Tgas)*std::log10(Tgas) - 0.1269 * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas));  // D + H+ -> HD+
-  k[51] = std::pow(10.0, -19.38 - 1.523 * std::log10(Tgas) + 1.118 * std::log10(Tgas)*std::log10(Tgas) - 0.1269 * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas));  // D+ + H -> HD+
-  k[52] = 16300000.0 * std::exp(-32400.0 / p.Trad);  // HD+ -> H + D+
-  k[53] = 16300000.0 * std::exp(-32400.0 / p.Trad);  // HD+ -> H+ + D
+  k[48] = 1e-09 * kb_exp(-464.0 * vh_invTgas);  // HD + H+ -> H2 + D+
+  k[49] = (2.1 - 0.4 * kb_log10(Tgas)) * 1e-09;  // HD + H3+ -> H2 + H2D+
+  k[50] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D + H+ -> HD+
+  k[51] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D+ + H -> HD+
+  k[52] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // HD+ -> H + D+
+  k[53] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // HD+ -> H+ + D
   k[54] = 7.2e-08 * 1.0/(std::sqrt(Tgas));  // HD+ + e- -> H + D
   k[55] = 2e-09;  // HD+ + H2 -> H2D+ + H
   k[56] = 2e-09;  // HD+ + H2 -> H3+ + D
@@ -192,23 +200,23 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   k[58] = 1e-06 * 1.0/(std::sqrt(Tgas)) * 0.73;  // H2D+ + e- -> H + H + D
   k[59] = 1e-06 * 1.0/(std::sqrt(Tgas)) * 0.07;  // H2D+ + e- -> H2 + D
   k[60] = 1e-06 * 1.0/(std::sqrt(Tgas)) * 0.2;  // H2D+ + e- -> HD + H
-  k[63] = 1e-09 * std::exp(-598.0 * vh_invTgas);  // H2D+ + H -> H3+ + D
+  k[63] = 1e-09 * kb_exp(-598.0 * vh_invTgas);  // H2D+ + H -> H3+ + D
   {  // group 1: H- + H -> H2 + e-
     double T = Tgas;
     if (T < 300.0) {
       k[4] = 1.5e-09;  // H- + H -> H2 + e-
     }
     else if (T >= 300.0) {
-      k[5] = 4e-09 * std::pow(T, -0.17);  // H- + H -> H2 + e-
+      k[5] = 4e-09 * kb_pow(T, -0.17);  // H- + H -> H2 + e-
     }
   }
   {  // group 2: H- + H+ -> H2+ + e-
     double T = Tgas;
     if (T < 8000.0) {
-      k[6] = 6.9e-09 * std::pow(T, -0.35);  // H- + H+ -> H2+ + e-
+      k[6] = 6.9e-09 * kb_pow(T, -0.35);  // H- + H+ -> H2+ + e-
     }
     else if (T >= 8000.0) {
-      k[7] = 9.6e-07 * std::pow(T, -0.9);  // H- + H+ -> H2+ + e-
+      k[7] = 9.6e-07 * kb_pow(T, -0.9);  // H- + H+ -> H2+ + e-
     }
   }
   {  // group 3: H2 + H+ -> H2+ + H
@@ -216,22 +224,22 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTgas = v_invTgas(T, n, p);
     (void)vh_invTgas;
     if (T < 10000.0) {
-      k[15] = 3e-10 * std::exp(-21050.0 * vh_invTgas);  // H2 + H+ -> H2+ + H
+      k[15] = 3e-10 * kb_exp(-21050.0 * vh_invTgas);  // H2 + H+ -> H2+ + H
     }
     else if (T >= 10000.0) {
-      k[16] = 1.5e-10 * std::exp(-14000.0 * vh_invTgas);  // H2 + H+ -> H2+ + H
+      k[16] = 1.5e-10 * kb_exp(-14000.0 * vh_invTgas);  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 4: He + H+ -> He+ + H
     double T = Tgas;
     if (T >= 10000.0 && T >= 10000.0) {
-      k[27] = 4e-37 * std::pow(T, 4.74);  // He + H+ -> He+ + H
+      k[27] = 4e-37 * kb_pow(T, 4.74);  // He + H+ -> He+ + H
     }
   }
   {  // group 5: He+ + H -> He + H+
     double T = Tgas;
     if (T >= 6000.0 && T >= 6000.0) {
-      k[28] = 3.7e-25 * std::pow(T, 2.06) * (1.0 + 9.9 * std::exp(-T / 2570.0));  // He+ + H -> He + H+
+      k[28] = 3.7e-25 * kb_pow(T, 2.06) * (1.0 + 9.9 * kb_exp(-T / 2570.0));  // He+ + H -> He + H+
     }
   }
   {  // group 6: He + H+ -> HeH+
@@ -240,13 +248,13 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[29] = 7.6e-18 * 1.0/(std::sqrt(T)) + 5e-21;  // He + H+ -> HeH+
     }
     else if (T >= 1000.0) {
-      k[30] = 3.45e-16 * std::pow(T, -1.06) + 5e-21;  // He + H+ -> HeH+
+      k[30] = 3.45e-16 * kb_pow(T, -1.06) + 5e-21;  // He + H+ -> HeH+
     }
   }
   {  // group 7: He+ + H -> HeH+
     double T = Tgas;
     if (T < 4000.0) {
-      k[32] = 1.6e-14 * std::pow(T, -0.33);  // He+ + H -> HeH+
+      k[32] = 1.6e-14 * kb_pow(T, -0.33);  // He+ + H -> HeH+
     }
     else if (T >= 4000.0) {
       k[33] = 1e-15;  // He+ + H -> HeH+
@@ -257,7 +265,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTgas = v_invTgas(T, n, p);
     (void)vh_invTgas;
     if (T >= 250.0 && T >= 250.0) {
-      k[44] = 9e-11 * std::exp(-3876.0 * vh_invTgas);  // D + H2 -> H + HD
+      k[44] = 9e-11 * kb_exp(-3876.0 * vh_invTgas);  // D + H2 -> H + HD
     }
   }
   {  // group 9: HD + H -> H2 + D
@@ -265,7 +273,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTgas = v_invTgas(T, n, p);
     (void)vh_invTgas;
     if (T >= 200.0 && T >= 200.0) {
-      k[47] = 3.2e-11 * std::exp(-3624.0 * vh_invTgas);  // HD + H -> H2 + D
+      k[47] = 3.2e-11 * kb_exp(-3624.0 * vh_invTgas);  // HD + H -> H2 + D
     }
   }
   {  // group 10: H2D+ + H2 -> H3+ + HD
@@ -273,7 +281,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTgas = v_invTgas(T, n, p);
     (void)vh_invTgas;
     if (T < 100.0) {
-      k[61] = 4.7e-09 * std::exp(-215.0 * vh_invTgas);  // H2D+ + H2 -> H3+ + HD
+      k[61] = 4.7e-09 * kb_exp(-215.0 * vh_invTgas);  // H2D+ + H2 -> H3+ + HD
     }
     else if (T >= 100.0) {
       k[62] = 5.5e-10;  // H2D+ + H2 -> H3+ + HD
@@ -1456,7 +1464,7 @@ KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) 
   fl[62] = k[62]*n[IDX_H2Dj]*n[IDX_H2];
   fl[63] = k[63]*n[IDX_H2Dj]*n[IDX_H];
 }
-// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// the neutral atomic metals (none) at n_H 10^(Z + kb_log10(n/n_H)_sun)
 // of the Asplund+09 photospheric abundances, floored at 1e-40
 KB_HD inline void scale_Z(double* n, double Z) {
   (void)n; (void)Z;
@@ -1464,7 +1472,7 @@ KB_HD inline void scale_Z(double* n, double Z) {
 // the column density [cm^-2] of a number density x [cm^-3]
 // (the default estimator: 1.87e21 (x / 1e3)^(2/3))
 KB_HD inline double num2col_(double x) {
-  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+  return 1.87e21 * kb_pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
 KB_HD inline double NH_col_(const double* n) {
   (void)n;

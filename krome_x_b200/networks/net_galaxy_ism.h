@@ -134,7 +134,7 @@ KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_lnTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::log(Tgas*kbc::boltzmann_eV);
+  return kb_log(Tgas*kbc::boltzmann_eV);
 }
 KB_HD inline double v_invTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -266,11 +266,11 @@ KB_HD inline double v_bsav7(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_sumsav(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return v_asav0(Tgas, n, p) + v_asav1(Tgas, n, p) * std::log10(Tgas) + v_asav2(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas) + v_asav3(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas) + v_asav4(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas) + v_asav5(Tgas, n, p) * ipow_<5>(std::log10(Tgas)) + v_asav6(Tgas, n, p) * ipow_<6>(std::log10(Tgas)) + v_asav7(Tgas, n, p) * ipow_<7>(std::log10(Tgas));
+  return v_asav0(Tgas, n, p) + v_asav1(Tgas, n, p) * kb_log10(Tgas) + v_asav2(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas) + v_asav3(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas) + v_asav4(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas) + v_asav5(Tgas, n, p) * ipow_<5>(kb_log10(Tgas)) + v_asav6(Tgas, n, p) * ipow_<6>(kb_log10(Tgas)) + v_asav7(Tgas, n, p) * ipow_<7>(kb_log10(Tgas));
 }
 KB_HD inline double v_sumsbv(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return v_bsav0(Tgas, n, p) + v_bsav1(Tgas, n, p) * std::log10(Tgas) + v_bsav2(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas) + v_bsav3(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas) + v_bsav4(Tgas, n, p) * std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas)*std::log10(Tgas) + v_bsav5(Tgas, n, p) * ipow_<5>(std::log10(Tgas)) + v_bsav6(Tgas, n, p) * ipow_<6>(std::log10(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<7>(std::log10(Tgas));
+  return v_bsav0(Tgas, n, p) + v_bsav1(Tgas, n, p) * kb_log10(Tgas) + v_bsav2(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas) + v_bsav3(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas) + v_bsav4(Tgas, n, p) * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas) + v_bsav5(Tgas, n, p) * ipow_<5>(kb_log10(Tgas)) + v_bsav6(Tgas, n, p) * ipow_<6>(kb_log10(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<7>(kb_log10(Tgas));
 }
 KB_HD inline double v_myflux_eV(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -308,26 +308,26 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   (void)vh_invT;
   const double vh_lnTe = v_lnTe(Tgas, n, p);
   (void)vh_lnTe;
-  k[0] = std::exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
-  k[3] = std::exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
-  k[6] = std::exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
-  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * std::pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * std::pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
-  k[8] = 1.4e-18 * std::pow(Tgas, 0.928) * std::exp(-Tgas / 16200.0);  // H + e- -> H-
-  k[9] = vh_a1 * (std::pow(Tgas, vh_a2) + vh_a3 * std::pow(Tgas, vh_a4) + vh_a5 * std::pow(Tgas, vh_a6)) / (1.0 + vh_a7 * std::pow(Tgas, vh_a8) + vh_a9 * std::pow(Tgas, vh_a10) + vh_a11 * std::pow(Tgas, vh_a12));  // H- + H -> H2 + e-
+  k[0] = kb_exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
+  k[3] = kb_exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
+  k[6] = kb_exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
+  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * kb_pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * kb_pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
+  k[8] = 1.4e-18 * kb_pow(Tgas, 0.928) * kb_exp(-Tgas / 16200.0);  // H + e- -> H-
+  k[9] = vh_a1 * (kb_pow(Tgas, vh_a2) + vh_a3 * kb_pow(Tgas, vh_a4) + vh_a5 * kb_pow(Tgas, vh_a6)) / (1.0 + vh_a7 * kb_pow(Tgas, vh_a8) + vh_a9 * kb_pow(Tgas, vh_a10) + vh_a11 * kb_pow(Tgas, vh_a12));  // H- + H -> H2 + e-
   k[12] = 6e-10;  // H2+ + H -> H2 + H+
-  k[15] = 35.5 * std::pow(Tgas, -2.28) * std::exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
-  k[16] = 4.38e-10 * std::exp(-102000.0 / Tgas) * std::pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
-  k[17] = 6.67e-12 * std::sqrt(Tgas) * std::exp(-(1.0 + 63593.0 / Tgas));  // H2 + H -> H + H + H
-  k[18] = std::exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
-  k[22] = 1e-08 * std::pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
+  k[15] = 35.5 * kb_pow(Tgas, -2.28) * kb_exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
+  k[16] = 4.38e-10 * kb_exp(-102000.0 / Tgas) * kb_pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
+  k[17] = 6.67e-12 * std::sqrt(Tgas) * kb_exp(-(1.0 + 63593.0 / Tgas));  // H2 + H -> H + H + H
+  k[18] = kb_exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
+  k[22] = 1e-08 * kb_pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
   k[25] = 5e-07 * std::sqrt(100.0 * vh_invT);  // H2+ + H- -> H + H2
-  k[26] = 5.996e-30 * std::pow(Tgas, 4.1881) * std::pow(1.0 + 6.761e-06 * Tgas, -5.6881) * std::exp(-54657.4 * vh_invT);  // H2 + H2 -> H + H + H2
-  k[27] = 1.2e-15 * std::pow(Tgas / 300.0, 0.25);  // He+ + H -> He + H+
-  k[30] = 3.7e-14 * std::exp(-35.0 / Tgas);  // H2 + He+ -> He + H + H+
-  k[31] = std::pow(10.0, -27.029 + 3.801 * std::log10(Tgas) - 29487.0 / Tgas);  // H2 + He -> H + H + He
+  k[26] = 5.996e-30 * kb_pow(Tgas, 4.1881) * kb_pow(1.0 + 6.761e-06 * Tgas, -5.6881) * kb_exp(-54657.4 * vh_invT);  // H2 + H2 -> H + H + H2
+  k[27] = 1.2e-15 * kb_pow(Tgas / 300.0, 0.25);  // He+ + H -> He + H+
+  k[30] = 3.7e-14 * kb_exp(-35.0 / Tgas);  // H2 + He+ -> He + H + H+
+  k[31] = kb_pow(10.0, -27.029 + 3.801 * kb_log10(Tgas) - 29487.0 / Tgas);  // H2 + He -> H + H + He
   k[32] = 7.2e-15;  // H2 + He+ -> H2+ + He
-  k[33] = 1.2e-17 * std::pow(Tgas, 1.2) * std::exp(-157800.0 * vh_invT);  // H + H -> H + H+ + e-
-  k[34] = 1.75e-17 * std::pow(Tgas, 1.3) * std::exp(-157800.0 * vh_invT);  // H + He -> He + H+ + e-
+  k[33] = 1.2e-17 * kb_pow(Tgas, 1.2) * kb_exp(-157800.0 * vh_invT);  // H + H -> H + H+ + e-
+  k[34] = 1.75e-17 * kb_pow(Tgas, 1.3) * kb_exp(-157800.0 * vh_invT);  // H + He -> He + H+ + e-
   {  // group 1: H+ + e- -> H
     double T = Tgas;
     const double vh_invTe = v_invTe(T, n, p);
@@ -335,10 +335,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 5500.0) {
-      k[1] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // H+ + e- -> H
+      k[1] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // H+ + e- -> H
     }
     else if (T >= 5500.0) {
-      k[2] = std::exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
+      k[2] = kb_exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
     }
   }
   {  // group 2: He+ + e- -> He
@@ -348,19 +348,19 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTe = v_invTe(T, n, p);
     (void)vh_invTe;
     if (T < 9284.0) {
-      k[4] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // He+ + e- -> He
+      k[4] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // He+ + e- -> He
     }
     else if (T >= 9284.0) {
-      k[5] = 1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * vh_invTe)) / (std::exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / std::pow(vh_Te, 0.6353);  // He+ + e- -> He
+      k[5] = 1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * vh_invTe)) / (kb_exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / kb_pow(vh_Te, 0.6353);  // He+ + e- -> He
     }
   }
   {  // group 3: H + H+ -> H2+
     double T = Tgas;
     if (T < 30.0) {
-      k[10] = 2.1e-20 * std::pow(T / 30.0, -0.15);  // H + H+ -> H2+
+      k[10] = 2.1e-20 * kb_pow(T / 30.0, -0.15);  // H + H+ -> H2+
     }
     else if (T >= 30.0) {
-      k[11] = std::pow(10.0, -18.2 - 3.194 * std::log10(T) + 1.786 * std::log10(T)*std::log10(T) - 0.2072 * std::log10(T)*std::log10(T)*std::log10(T));  // H + H+ -> H2+
+      k[11] = kb_pow(10.0, -18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
     }
   }
   {  // group 4: H2 + H+ -> H2+ + H
@@ -403,10 +403,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_sumsbv = v_sumsbv(T, n, p);
     (void)vh_sumsbv;
     if (T >= 100.0 && T >= 100.0 && T < 100000.0) {
-      k[13] = std::pow(10.0, vh_sumsav);  // H2 + H+ -> H2+ + H
+      k[13] = kb_pow(10.0, vh_sumsav);  // H2 + H+ -> H2+ + H
     }
     else if (T >= 100000.0) {
-      k[14] = std::pow(10.0, vh_sumsbv);  // H2 + H+ -> H2+ + H
+      k[14] = kb_pow(10.0, vh_sumsbv);  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 5: H- + H -> H + H + e-
@@ -416,10 +416,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 1160.0) {
-      k[19] = 2.56e-09 * std::pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
+      k[19] = 2.56e-09 * kb_pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
     }
     else if (T >= 1160.0) {
-      k[20] = std::exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
+      k[20] = kb_exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
     }
   }
   {  // group 6: H- + H+ -> H + H
@@ -435,7 +435,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[23] = 1e-08;  // H2+ + e- -> H + H
     }
     else if (T >= 617.0) {
-      k[24] = 1.32e-06 * std::pow(T, -0.76);  // H2+ + e- -> H + H
+      k[24] = 1.32e-06 * kb_pow(T, -0.76);  // H2+ + e- -> H + H
     }
   }
   {  // group 8: He + H+ -> He+ + H
@@ -443,10 +443,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T < 10000.0) {
-      k[28] = 1.26e-09 * std::pow(T, -0.75) * std::exp(-127500.0 * vh_invT);  // He + H+ -> He+ + H
+      k[28] = 1.26e-09 * kb_pow(T, -0.75) * kb_exp(-127500.0 * vh_invT);  // He + H+ -> He+ + H
     }
     else if (T >= 10000.0) {
-      k[29] = 4e-37 * std::pow(T, 4.74);  // He + H+ -> He+ + H
+      k[29] = 4e-37 * kb_pow(T, 4.74);  // He + H+ -> He+ + H
     }
   }
 }
@@ -1340,7 +1340,7 @@ KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) 
   fl[44] = k[44]*n[IDX_Hj]*n[IDX_E];
   fl[45] = k[45]*n[IDX_Hej]*n[IDX_E];
 }
-// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// the neutral atomic metals (none) at n_H 10^(Z + kb_log10(n/n_H)_sun)
 // of the Asplund+09 photospheric abundances, floored at 1e-40
 KB_HD inline void scale_Z(double* n, double Z) {
   (void)n; (void)Z;
@@ -1348,7 +1348,7 @@ KB_HD inline void scale_Z(double* n, double Z) {
 // the column density [cm^-2] of a number density x [cm^-3]
 // (the default estimator: 1.87e21 (x / 1e3)^(2/3))
 KB_HD inline double num2col_(double x) {
-  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+  return 1.87e21 * kb_pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
 KB_HD inline double NH_col_(const double* n) {
   (void)n;
@@ -1366,11 +1366,11 @@ inline const double photo_Emax_[8] = {INFINITY, INFINITY, INFINITY, 12398.419843
 // ---- host: the photo cross sections (photon-bin setup) ----
 namespace kbxs {
 inline double H2_sigmaLW(double E) {
-  auto band = [](double lg) { return 1e-18 * std::pow(10.0, lg); };
+  auto band = [](double lg) { return 1e-18 * kb_pow(10.0, lg); };
   double l0 = 0.0, w0 = 0.0, l1 = 0.0, w1 = 0.0;
   if (E > 14.675 && E < 16.820) l0 = band(15.1289 - 1.05139 * E);
   else if (E > 16.820 && E < 17.6)
-    l0 = band(-31.41 + 1.8042e-2 * E * E * E - 4.2339e-5 * std::pow(E, 5.0));
+    l0 = band(-31.41 + 1.8042e-2 * E * E * E - 4.2339e-5 * kb_pow(E, 5.0));
   if (E > 14.675 && E < 17.7) w0 = band(13.5311 - 0.9182618 * E);
   if (E > 14.159 && E < 15.302) l1 = band(12.0218406 - 0.819429 * E);
   else if (E > 15.302 && E < 17.2) l1 = band(16.04644 - 1.082438 * E);
@@ -1383,8 +1383,8 @@ static inline double sigma_v96(double E, double E0, double s0, double ya, double
   const double x = E/E0 - y0;
   const double y = std::sqrt(x*x + y1*y1);
   const double Fy = ((x - 1.0)*(x - 1.0) + yw*yw)
-      * std::pow(y, 0.5*P - 5.5)
-      * std::pow(1.0 + std::sqrt(y/ya), -P);
+      * kb_pow(y, 0.5*P - 5.5)
+      * kb_pow(1.0 + std::sqrt(y/ya), -P);
   return 1e-18 * s0 * Fy;
 }
 
@@ -1395,8 +1395,8 @@ static inline double sigma_vy95(double E, double Eth, double E0, double s0, doub
   if (E < Eth) return 0.0;
   const double y = E/E0;
   return 1e-18 * s0 * ((y - 1.0)*(y - 1.0) + yw*yw)
-      * std::pow(y, 0.5*P - 5.5 - l)
-      * std::pow(1.0 + std::sqrt(y/ya), -P);
+      * kb_pow(y, 0.5*P - 5.5 - l)
+      * kb_pow(1.0 + std::sqrt(y/ya), -P);
 }
 
 // linear interpolation on a tabulated cross section;
@@ -2050,7 +2050,7 @@ static inline double photo_xsec_int_5(double a, double b) {
 // xsec of H2+ -> H+ + H+ + e- [cm^2]
 static inline double photo_xsec_6(double E_eV) {
   (void)E_eV;
-  return std::pow(10.0, -16.926 - 0.04528 * E_eV + 0.0002238 * E_eV*E_eV + 4.245e-07 * E_eV*E_eV*E_eV);
+  return kb_pow(10.0, -16.926 - 0.04528 * E_eV + 0.0002238 * E_eV*E_eV + 4.245e-07 * E_eV*E_eV*E_eV);
 }
 // xsec of H2 -> H + H [cm^2]
 static inline double photo_xsec_7(double E_eV) {

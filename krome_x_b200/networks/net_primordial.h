@@ -123,7 +123,7 @@ KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_lnTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::log(Tgas*kbc::boltzmann_eV);
+  return kb_log(Tgas*kbc::boltzmann_eV);
 }
 KB_HD inline double v_invTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -157,22 +157,22 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   (void)vh_lnTe;
   const double vh_sqrTgas = v_sqrTgas(Tgas, n, p);
   (void)vh_sqrTgas;
-  k[0] = std::exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
-  k[3] = std::exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
-  k[6] = std::exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
-  k[7] = 3.36e-10 / vh_sqrTgas / std::pow(Tgas / 1000.0, 0.2) / (1.0 + std::pow(Tgas / 1000000.0, 0.7));  // He++ + e- -> He+
-  k[8] = 6.77e-15 * std::pow(vh_Te, 0.8779);  // H + e- -> H-
+  k[0] = kb_exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
+  k[3] = kb_exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
+  k[6] = kb_exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
+  k[7] = 3.36e-10 / vh_sqrTgas / kb_pow(Tgas / 1000.0, 0.2) / (1.0 + kb_pow(Tgas / 1000000.0, 0.7));  // He++ + e- -> He+
+  k[8] = 6.77e-15 * kb_pow(vh_Te, 0.8779);  // H + e- -> H-
   k[13] = 6e-10;  // H2+ + H -> H2 + H+
-  k[15] = 5.6e-11 * std::exp(-102124.0 * vh_invT) * std::sqrt(Tgas);  // H2 + e- -> H + H + e-
-  k[16] = 1.0670825e-10 * std::pow(vh_Te, 2.012) * std::exp(-4.463 * vh_invTe) / std::pow(1.0 + 0.2472 * vh_Te, 3.512);  // H2 + H -> H + H + H
-  k[17] = std::exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
+  k[15] = 5.6e-11 * kb_exp(-102124.0 * vh_invT) * std::sqrt(Tgas);  // H2 + e- -> H + H + e-
+  k[16] = 1.0670825e-10 * kb_pow(vh_Te, 2.012) * kb_exp(-4.463 * vh_invTe) / kb_pow(1.0 + 0.2472 * vh_Te, 3.512);  // H2 + H -> H + H + H
+  k[17] = kb_exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
   k[20] = 6.5e-09 / std::sqrt(vh_Te);  // H- + H+ -> H + H
-  k[21] = 1e-08 * std::pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
+  k[21] = 1e-08 * kb_pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
   k[24] = 5e-07 * std::sqrt(100.0 * vh_invT);  // H2+ + H- -> H + H2
-  k[31] = 1e-09 * (0.417 + 0.846 * std::log10(Tgas) - 0.137 * std::log10(Tgas)*std::log10(Tgas));  // H2 + D+ -> HD + H+
-  k[32] = 1e-09 * std::exp(-457.0 * vh_invT);  // HD + H+ -> H2 + D+
-  k[36] = 1.5e-09 * std::pow(vh_T32, -0.1);  // D + H- -> HD + e-
-  k[37] = 3.6e-12 * std::pow(Tgas / 300.0, -0.75);  // D+ + e- -> D
+  k[31] = 1e-09 * (0.417 + 0.846 * kb_log10(Tgas) - 0.137 * kb_log10(Tgas)*kb_log10(Tgas));  // H2 + D+ -> HD + H+
+  k[32] = 1e-09 * kb_exp(-457.0 * vh_invT);  // HD + H+ -> H2 + D+
+  k[36] = 1.5e-09 * kb_pow(vh_T32, -0.1);  // D + H- -> HD + e-
+  k[37] = 3.6e-12 * kb_pow(Tgas / 300.0, -0.75);  // D+ + e- -> D
   {  // group 1: H+ + e- -> H
     double T = Tgas;
     const double vh_invTe = v_invTe(T, n, p);
@@ -180,10 +180,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 5500.0) {
-      k[1] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // H+ + e- -> H
+      k[1] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // H+ + e- -> H
     }
     else if (T >= 5500.0) {
-      k[2] = std::exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
+      k[2] = kb_exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
     }
   }
   {  // group 2: He+ + e- -> He
@@ -193,10 +193,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTe = v_invTe(T, n, p);
     (void)vh_invTe;
     if (T < 9280.0) {
-      k[4] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // He+ + e- -> He
+      k[4] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // He+ + e- -> He
     }
     else if (T >= 9280.0) {
-      k[5] = 1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * vh_invTe)) / (std::exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / std::pow(vh_Te, 0.6353);  // He+ + e- -> He
+      k[5] = 1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * vh_invTe)) / (kb_exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / kb_pow(vh_Te, 0.6353);  // He+ + e- -> He
     }
   }
   {  // group 3: H- + H -> H2 + e-
@@ -207,16 +207,16 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[9] = 1.43e-09;  // H- + H -> H2 + e-
     }
     else if (T >= 1160.0) {
-      k[10] = std::exp(-20.06913897587003 + 0.2289800603272916 * vh_lnTe + 0.03599837721023835 * vh_lnTe*vh_lnTe - 0.004555120027032095 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003105115447124016 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0001073294010367247 * ipow_<5>(vh_lnTe) - 8.36671960467864e-06 * ipow_<6>(vh_lnTe) + 2.238306228891639e-07 * ipow_<7>(vh_lnTe));  // H- + H -> H2 + e-
+      k[10] = kb_exp(-20.06913897587003 + 0.2289800603272916 * vh_lnTe + 0.03599837721023835 * vh_lnTe*vh_lnTe - 0.004555120027032095 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003105115447124016 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0001073294010367247 * ipow_<5>(vh_lnTe) - 8.36671960467864e-06 * ipow_<6>(vh_lnTe) + 2.238306228891639e-07 * ipow_<7>(vh_lnTe));  // H- + H -> H2 + e-
     }
   }
   {  // group 4: H + H+ -> H2+
     double T = Tgas;
     if (T < 6700.0) {
-      k[11] = 1.85e-23 * std::pow(T, 1.8);  // H + H+ -> H2+
+      k[11] = 1.85e-23 * kb_pow(T, 1.8);  // H + H+ -> H2+
     }
     else if (T >= 6700.0) {
-      k[12] = 5.81e-16 * std::pow(T / 56200.0, -0.6657 * std::log10(T / 56200.0));  // H + H+ -> H2+
+      k[12] = 5.81e-16 * kb_pow(T / 56200.0, -0.6657 * kb_log10(T / 56200.0));  // H + H+ -> H2+
     }
   }
   {  // group 5: H2 + H+ -> H2+ + H
@@ -224,7 +224,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T >= 3480.0 && T >= 3480.0) {
-      k[14] = std::exp(-24.24914687731536 + 3.400824447095291 * vh_lnTe - 3.898003964650152 * vh_lnTe*vh_lnTe + 2.045587822403071 * vh_lnTe*vh_lnTe*vh_lnTe - 0.5416182856220388 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0841077503763412 * ipow_<5>(vh_lnTe) - 0.007879026154483455 * ipow_<6>(vh_lnTe) + 0.0004138398421504563 * ipow_<7>(vh_lnTe) - 9.36345888928611e-06 * ipow_<8>(vh_lnTe));  // H2 + H+ -> H2+ + H
+      k[14] = kb_exp(-24.24914687731536 + 3.400824447095291 * vh_lnTe - 3.898003964650152 * vh_lnTe*vh_lnTe + 2.045587822403071 * vh_lnTe*vh_lnTe*vh_lnTe - 0.5416182856220388 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0841077503763412 * ipow_<5>(vh_lnTe) - 0.007879026154483455 * ipow_<6>(vh_lnTe) + 0.0004138398421504563 * ipow_<7>(vh_lnTe) - 9.36345888928611e-06 * ipow_<8>(vh_lnTe));  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 6: H- + H -> H + H + e-
@@ -234,10 +234,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 1160.0) {
-      k[18] = 2.56e-09 * std::pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
+      k[18] = 2.56e-09 * kb_pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
     }
     else if (T >= 1160.0) {
-      k[19] = std::exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
+      k[19] = kb_exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
     }
   }
   {  // group 7: H2+ + e- -> H + H
@@ -246,7 +246,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[22] = 1e-08;  // H2+ + e- -> H + H
     }
     else if (T >= 617.0) {
-      k[23] = 1.32e-06 * std::pow(T, -0.76);  // H2+ + e- -> H + H
+      k[23] = 1.32e-06 * kb_pow(T, -0.76);  // H2+ + e- -> H + H
     }
   }
   {  // group 8: H + H + H -> H2 + H
@@ -254,7 +254,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_T32 = v_T32(T, n, p);
     (void)vh_T32;
     if (T < 300.0) {
-      k[25] = 1.3e-32 * std::pow(vh_T32, -0.38);  // H + H + H -> H2 + H
+      k[25] = 1.3e-32 * kb_pow(vh_T32, -0.38);  // H + H + H -> H2 + H
     }
     else if (T >= 300.0) {
       k[26] = 1.3e-32 * ipow_<-1>(vh_T32);  // H + H + H -> H2 + H
@@ -265,7 +265,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_T32 = v_T32(T, n, p);
     (void)vh_T32;
     if (T < 300.0) {
-      k[27] = 1.3e-32 * std::pow(vh_T32, -0.38) / 8.0;  // H2 + H + H -> H2 + H2
+      k[27] = 1.3e-32 * kb_pow(vh_T32, -0.38) / 8.0;  // H2 + H + H -> H2 + H2
     }
     else if (T >= 300.0) {
       k[28] = 1.3e-32 * ipow_<-1>(vh_T32) / 8.0;  // H2 + H + H -> H2 + H2
@@ -276,7 +276,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T >= 50.0 && T >= 50.0) {
-      k[29] = 2e-10 * std::pow(T, 0.402) * std::exp(-37.1 * vh_invT) - 3.31e-17 * std::pow(T, 1.48);  // H+ + D -> H + D+
+      k[29] = 2e-10 * kb_pow(T, 0.402) * kb_exp(-37.1 * vh_invT) - 3.31e-17 * kb_pow(T, 1.48);  // H+ + D -> H + D+
     }
   }
   {  // group 11: H + D+ -> H+ + D
@@ -284,7 +284,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T >= 50.0 && T >= 50.0) {
-      k[30] = 2.06e-10 * std::pow(T, 0.396) * std::exp(-33.0 * vh_invT) + 2.03e-09 * std::pow(T, -0.332);  // H + D+ -> H+ + D
+      k[30] = 2.06e-10 * kb_pow(T, 0.396) * kb_exp(-33.0 * vh_invT) + 2.03e-09 * kb_pow(T, -0.332);  // H + D+ -> H+ + D
     }
   }
   {  // group 12: H2 + D -> HD + H
@@ -292,10 +292,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T < 2000.0) {
-      k[33] = std::pow(10.0, -56.4737 + 5.88886 * std::log10(T) + 7.19692 * std::log10(T)*std::log10(T) + 2.25069 * std::log10(T)*std::log10(T)*std::log10(T) - 2.16903 * std::log10(T)*std::log10(T)*std::log10(T)*std::log10(T) + 0.317887 * ipow_<5>(std::log10(T)));  // H2 + D -> HD + H
+      k[33] = kb_pow(10.0, -56.4737 + 5.88886 * kb_log10(T) + 7.19692 * kb_log10(T)*kb_log10(T) + 2.25069 * kb_log10(T)*kb_log10(T)*kb_log10(T) - 2.16903 * kb_log10(T)*kb_log10(T)*kb_log10(T)*kb_log10(T) + 0.317887 * ipow_<5>(kb_log10(T)));  // H2 + D -> HD + H
     }
     else if (T >= 2000.0) {
-      k[34] = 3.17e-10 * std::exp(-5207.0 * vh_invT);  // H2 + D -> HD + H
+      k[34] = 3.17e-10 * kb_exp(-5207.0 * vh_invT);  // H2 + D -> HD + H
     }
   }
   {  // group 13: HD + H -> H2 + D
@@ -303,7 +303,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T >= 200.0 && T >= 200.0) {
-      k[35] = 5.25e-11 * std::exp(-4430.0 * vh_invT + 173900.0 * vh_invT*vh_invT);  // HD + H -> H2 + D
+      k[35] = 5.25e-11 * kb_exp(-4430.0 * vh_invT + 173900.0 * vh_invT*vh_invT);  // HD + H -> H2 + D
     }
   }
 }
@@ -944,8 +944,8 @@ KB_HD inline double heating_chem(double Tgas, const double* n, const double* k) 
   const double ev2erg = kbc::eV_to_erg;
   const double dd = Hnuclei_(n);
   const double ncr = 1.0e6 / std::sqrt(Tgas)
-      / (1.6 * std::exp(-std::pow(4.0e2 / Tgas, 2.0)) * n[IDX_H] / dd
-         + 1.4 * std::exp(-1.2e4 / (Tgas + 1.2e3)) * n[IDX_H2] / dd);
+      / (1.6 * kb_exp(-kb_pow(4.0e2 / Tgas, 2.0)) * n[IDX_H] / dd
+         + 1.4 * kb_exp(-1.2e4 / (Tgas + 1.2e3)) * n[IDX_H2] / dd);
   const double ffac = 1.0 / (1.0 + ncr / dd);
   h += k[9] * (3.53*ffac) * n[IDX_Hk]*n[IDX_H];
   h += k[10] * (3.53*ffac) * n[IDX_Hk]*n[IDX_H];
@@ -964,36 +964,36 @@ KB_HD inline void recomb_rates_(double Tgas, const double* n, const Params& p, d
   (void)n; (void)p;
   const double h = 1e-4;
   for (int j = 0; j < 6; ++j) kr[j] = tdk[j] = 0.0;
-  kr[4] = 3.36e-10 / v_sqrTgas(Tgas, n, p) / std::pow(Tgas / 1000.0, 0.2) / (1.0 + std::pow(Tgas / 1000000.0, 0.7));
+  kr[4] = 3.36e-10 / v_sqrTgas(Tgas, n, p) / kb_pow(Tgas / 1000.0, 0.2) / (1.0 + kb_pow(Tgas / 1000000.0, 0.7));
   { const double Tp_ = Tgas * (1.0 + h), Tm_ = Tgas * (1.0 - h);
-    tdk[4] = ((3.36e-10 / v_sqrTgas(Tp_, n, p) / std::pow(Tp_ / 1000.0, 0.2) / (1.0 + std::pow(Tp_ / 1000000.0, 0.7))) - (3.36e-10 / v_sqrTgas(Tm_, n, p) / std::pow(Tm_ / 1000.0, 0.2) / (1.0 + std::pow(Tm_ / 1000000.0, 0.7)))) / (2.0 * h); }
-  kr[5] = 3.6e-12 * std::pow(Tgas / 300.0, -0.75);
+    tdk[4] = ((3.36e-10 / v_sqrTgas(Tp_, n, p) / kb_pow(Tp_ / 1000.0, 0.2) / (1.0 + kb_pow(Tp_ / 1000000.0, 0.7))) - (3.36e-10 / v_sqrTgas(Tm_, n, p) / kb_pow(Tm_ / 1000.0, 0.2) / (1.0 + kb_pow(Tm_ / 1000000.0, 0.7)))) / (2.0 * h); }
+  kr[5] = 3.6e-12 * kb_pow(Tgas / 300.0, -0.75);
   { const double Tp_ = Tgas * (1.0 + h), Tm_ = Tgas * (1.0 - h);
-    tdk[5] = ((3.6e-12 * std::pow(Tp_ / 300.0, -0.75)) - (3.6e-12 * std::pow(Tm_ / 300.0, -0.75))) / (2.0 * h); }
+    tdk[5] = ((3.6e-12 * kb_pow(Tp_ / 300.0, -0.75)) - (3.6e-12 * kb_pow(Tm_ / 300.0, -0.75))) / (2.0 * h); }
   {  // group 1: H+ + e- -> H
     double T = Tgas;
     if (T < 5500.0) {
-      kr[0] = 3.92e-13 * std::pow(v_invTe(T, n, p), 0.6353);
+      kr[0] = 3.92e-13 * kb_pow(v_invTe(T, n, p), 0.6353);
       if (T == Tgas) { const double Tp_ = T * (1.0 + h), Tm_ = T * (1.0 - h);
-        tdk[0] = ((3.92e-13 * std::pow(v_invTe(Tp_, n, p), 0.6353)) - (3.92e-13 * std::pow(v_invTe(Tm_, n, p), 0.6353))) / (2.0 * h); }
+        tdk[0] = ((3.92e-13 * kb_pow(v_invTe(Tp_, n, p), 0.6353)) - (3.92e-13 * kb_pow(v_invTe(Tm_, n, p), 0.6353))) / (2.0 * h); }
     }
     else if (T >= 5500.0) {
-      kr[1] = std::exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(T, n, p) - 0.02026044731984691 * v_lnTe(T, n, p)*v_lnTe(T, n, p) - 0.002380861877349834 * v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p) - 0.0003212605213188796 * v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(T, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(T, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(T, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(T, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(T, n, p)));
+      kr[1] = kb_exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(T, n, p) - 0.02026044731984691 * v_lnTe(T, n, p)*v_lnTe(T, n, p) - 0.002380861877349834 * v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p) - 0.0003212605213188796 * v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p)*v_lnTe(T, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(T, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(T, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(T, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(T, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(T, n, p)));
       if (T == Tgas) { const double Tp_ = T * (1.0 + h), Tm_ = T * (1.0 - h);
-        tdk[1] = ((std::exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(Tp_, n, p) - 0.02026044731984691 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 0.002380861877349834 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 0.0003212605213188796 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(Tp_, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(Tp_, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(Tp_, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(Tp_, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(Tp_, n, p)))) - (std::exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(Tm_, n, p) - 0.02026044731984691 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 0.002380861877349834 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 0.0003212605213188796 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(Tm_, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(Tm_, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(Tm_, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(Tm_, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(Tm_, n, p))))) / (2.0 * h); }
+        tdk[1] = ((kb_exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(Tp_, n, p) - 0.02026044731984691 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 0.002380861877349834 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 0.0003212605213188796 * v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p)*v_lnTe(Tp_, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(Tp_, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(Tp_, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(Tp_, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(Tp_, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(Tp_, n, p)))) - (kb_exp(-28.61303380689232 - 0.7241125657826851 * v_lnTe(Tm_, n, p) - 0.02026044731984691 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 0.002380861877349834 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 0.0003212605213188796 * v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p)*v_lnTe(Tm_, n, p) - 1.421502914054107e-05 * ipow_<5>(v_lnTe(Tm_, n, p)) + 4.989108920299513e-06 * ipow_<6>(v_lnTe(Tm_, n, p)) + 5.755614137575758e-07 * ipow_<7>(v_lnTe(Tm_, n, p)) - 1.856767039775261e-08 * ipow_<8>(v_lnTe(Tm_, n, p)) - 3.071135243196595e-09 * ipow_<9>(v_lnTe(Tm_, n, p))))) / (2.0 * h); }
     }
   }
   {  // group 2: He+ + e- -> He
     double T = Tgas;
     if (T < 9280.0) {
-      kr[2] = 3.92e-13 * std::pow(v_invTe(T, n, p), 0.6353);
+      kr[2] = 3.92e-13 * kb_pow(v_invTe(T, n, p), 0.6353);
       if (T == Tgas) { const double Tp_ = T * (1.0 + h), Tm_ = T * (1.0 - h);
-        tdk[2] = ((3.92e-13 * std::pow(v_invTe(Tp_, n, p), 0.6353)) - (3.92e-13 * std::pow(v_invTe(Tm_, n, p), 0.6353))) / (2.0 * h); }
+        tdk[2] = ((3.92e-13 * kb_pow(v_invTe(Tp_, n, p), 0.6353)) - (3.92e-13 * kb_pow(v_invTe(Tm_, n, p), 0.6353))) / (2.0 * h); }
     }
     else if (T >= 9280.0) {
-      kr[3] = 1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * v_invTe(T, n, p))) / (std::exp(40.49664394833662 * v_invTe(T, n, p)) * ipow_<1>(v_Te(T, n, p)) * std::sqrt(v_Te(T, n, p))) + 3.92e-13 / std::pow(v_Te(T, n, p), 0.6353);
+      kr[3] = 1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * v_invTe(T, n, p))) / (kb_exp(40.49664394833662 * v_invTe(T, n, p)) * ipow_<1>(v_Te(T, n, p)) * std::sqrt(v_Te(T, n, p))) + 3.92e-13 / kb_pow(v_Te(T, n, p), 0.6353);
       if (T == Tgas) { const double Tp_ = T * (1.0 + h), Tm_ = T * (1.0 - h);
-        tdk[3] = ((1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * v_invTe(Tp_, n, p))) / (std::exp(40.49664394833662 * v_invTe(Tp_, n, p)) * ipow_<1>(v_Te(Tp_, n, p)) * std::sqrt(v_Te(Tp_, n, p))) + 3.92e-13 / std::pow(v_Te(Tp_, n, p), 0.6353)) - (1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * v_invTe(Tm_, n, p))) / (std::exp(40.49664394833662 * v_invTe(Tm_, n, p)) * ipow_<1>(v_Te(Tm_, n, p)) * std::sqrt(v_Te(Tm_, n, p))) + 3.92e-13 / std::pow(v_Te(Tm_, n, p), 0.6353))) / (2.0 * h); }
+        tdk[3] = ((1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * v_invTe(Tp_, n, p))) / (kb_exp(40.49664394833662 * v_invTe(Tp_, n, p)) * ipow_<1>(v_Te(Tp_, n, p)) * std::sqrt(v_Te(Tp_, n, p))) + 3.92e-13 / kb_pow(v_Te(Tp_, n, p), 0.6353)) - (1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * v_invTe(Tm_, n, p))) / (kb_exp(40.49664394833662 * v_invTe(Tm_, n, p)) * ipow_<1>(v_Te(Tm_, n, p)) * std::sqrt(v_Te(Tm_, n, p))) + 3.92e-13 / kb_pow(v_Te(Tm_, n, p), 0.6353))) / (2.0 * h); }
     }
   }
 }
@@ -1153,8 +1153,8 @@ KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Pa
     const double c = muT * (gamma_index(Tth, n, p) - 1.0) / (kbc::boltzmann_erg * ntot_(n)) * kbc::eV_to_erg;
     const double dd = Hnuclei_(n);
     const double ncr = 1.0e6 / std::sqrt(Tth)
-        / (1.6 * std::exp(-std::pow(4.0e2 / Tth, 2.0)) * n[IDX_H] / dd
-           + 1.4 * std::exp(-1.2e4 / (Tth + 1.2e3)) * n[IDX_H2] / dd);
+        / (1.6 * kb_exp(-kb_pow(4.0e2 / Tth, 2.0)) * n[IDX_H] / dd
+           + 1.4 * kb_exp(-1.2e4 / (Tth + 1.2e3)) * n[IDX_H2] / dd);
     const double ffac = 1.0 / (1.0 + ncr / dd);
     (void)ffac;
     g[9] += c * k[9] * (3.53*ffac) * n[IDX_Hk]*n[IDX_H];
@@ -1224,7 +1224,7 @@ KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) 
   fl[36] = k[36]*n[IDX_D]*n[IDX_Hk];
   fl[37] = k[37]*n[IDX_Dj]*n[IDX_E];
 }
-// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// the neutral atomic metals (none) at n_H 10^(Z + kb_log10(n/n_H)_sun)
 // of the Asplund+09 photospheric abundances, floored at 1e-40
 KB_HD inline void scale_Z(double* n, double Z) {
   (void)n; (void)Z;
@@ -1232,7 +1232,7 @@ KB_HD inline void scale_Z(double* n, double Z) {
 // the column density [cm^-2] of a number density x [cm^-3]
 // (the default estimator: 1.87e21 (x / 1e3)^(2/3))
 KB_HD inline double num2col_(double x) {
-  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+  return 1.87e21 * kb_pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
 KB_HD inline double NH_col_(const double* n) {
   (void)n;

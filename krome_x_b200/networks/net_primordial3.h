@@ -118,7 +118,7 @@ KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_lnTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::log(Tgas*kbc::boltzmann_eV);
+  return kb_log(Tgas*kbc::boltzmann_eV);
 }
 KB_HD inline double v_invTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -218,19 +218,19 @@ KB_HD inline double v_bsav8(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_sumsav(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return v_bsav1(Tgas, n, p) + v_bsav2(Tgas, n, p) * std::log(Tgas) + v_bsav3(Tgas, n, p) * std::log(Tgas)*std::log(Tgas) + v_bsav4(Tgas, n, p) * std::log(Tgas)*std::log(Tgas)*std::log(Tgas) + v_bsav5(Tgas, n, p) * std::log(Tgas)*std::log(Tgas)*std::log(Tgas)*std::log(Tgas) + v_bsav6(Tgas, n, p) * ipow_<5>(std::log(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<6>(std::log(Tgas)) + v_bsav8(Tgas, n, p) * ipow_<7>(std::log(Tgas));
+  return v_bsav1(Tgas, n, p) + v_bsav2(Tgas, n, p) * kb_log(Tgas) + v_bsav3(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas) + v_bsav4(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas) + v_bsav5(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas) + v_bsav6(Tgas, n, p) * ipow_<5>(kb_log(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<6>(kb_log(Tgas)) + v_bsav8(Tgas, n, p) * ipow_<7>(kb_log(Tgas));
 }
 KB_HD inline double v_kl21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return 1.18e-10 * std::exp(-69500.0 * v_invT(Tgas, n, p));
+  return 1.18e-10 * kb_exp(-69500.0 * v_invT(Tgas, n, p));
 }
 KB_HD inline double v_kh21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * std::exp(-52000.0 * v_invT(Tgas, n, p)) * (1.0 - std::exp(-6000.0 * v_invT(Tgas, n, p)));
+  return 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * (1.0 - kb_exp(-6000.0 * v_invT(Tgas, n, p)));
 }
 KB_HD inline double v_ncr21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::pow(10.0, 4.845 - 1.3 * std::log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * std::log10(v_T(Tgas, n, p) * 0.0001)*std::log10(v_T(Tgas, n, p) * 0.0001));
+  return kb_pow(10.0, 4.845 - 1.3 * kb_log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * kb_log10(v_T(Tgas, n, p) * 0.0001)*kb_log10(v_T(Tgas, n, p) * 0.0001));
 }
 KB_HD inline double v_a21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -268,20 +268,20 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   (void)vh_invT;
   const double vh_lnTe = v_lnTe(Tgas, n, p);
   (void)vh_lnTe;
-  k[0] = std::exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
-  k[3] = std::exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
-  k[6] = std::exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
-  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * std::pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * std::pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
-  k[8] = 1.4e-18 * std::pow(Tgas, 0.928) * std::exp(-Tgas / 16200.0);  // H + e- -> H-
-  k[9] = vh_a1 * (std::pow(Tgas, vh_a2) + vh_a3 * std::pow(Tgas, vh_a4) + vh_a5 * std::pow(Tgas, vh_a6)) / (1.0 + vh_a7 * std::pow(Tgas, vh_a8) + vh_a9 * std::pow(Tgas, vh_a10) + vh_a11 * std::pow(Tgas, vh_a12));  // H- + H -> H2 + e-
+  k[0] = kb_exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
+  k[3] = kb_exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
+  k[6] = kb_exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
+  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * kb_pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * kb_pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
+  k[8] = 1.4e-18 * kb_pow(Tgas, 0.928) * kb_exp(-Tgas / 16200.0);  // H + e- -> H-
+  k[9] = vh_a1 * (kb_pow(Tgas, vh_a2) + vh_a3 * kb_pow(Tgas, vh_a4) + vh_a5 * kb_pow(Tgas, vh_a6)) / (1.0 + vh_a7 * kb_pow(Tgas, vh_a8) + vh_a9 * kb_pow(Tgas, vh_a10) + vh_a11 * kb_pow(Tgas, vh_a12));  // H- + H -> H2 + e-
   k[12] = 6e-10;  // H2+ + H -> H2 + H+
-  k[14] = 35.5 * std::pow(Tgas, -2.28) * std::exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
-  k[15] = 4.38e-10 * std::exp(-102000.0 / Tgas) * std::pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
-  k[17] = std::exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
-  k[21] = 1e-08 * std::pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
+  k[14] = 35.5 * kb_pow(Tgas, -2.28) * kb_exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
+  k[15] = 4.38e-10 * kb_exp(-102000.0 / Tgas) * kb_pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
+  k[17] = kb_exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
+  k[21] = 1e-08 * kb_pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
   k[23] = 5e-07 * std::sqrt(100.0 * vh_invT);  // H2+ + H- -> H + H2
-  k[24] = 6e-32 * std::pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas));  // H + H + H -> H2 + H
-  k[25] = (6e-32 * std::pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas))) / 8.0;  // H2 + H + H -> H2 + H2
+  k[24] = 6e-32 * kb_pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas));  // H + H + H -> H2 + H
+  k[25] = (6e-32 * kb_pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas))) / 8.0;  // H2 + H + H -> H2 + H2
   {  // group 1: H+ + e- -> H
     double T = Tgas;
     const double vh_invTe = v_invTe(T, n, p);
@@ -289,10 +289,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 5500.0) {
-      k[1] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // H+ + e- -> H
+      k[1] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // H+ + e- -> H
     }
     else if (T >= 5500.0) {
-      k[2] = std::exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
+      k[2] = kb_exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
     }
   }
   {  // group 2: He+ + e- -> He
@@ -302,19 +302,19 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTe = v_invTe(T, n, p);
     (void)vh_invTe;
     if (T < 9280.0) {
-      k[4] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // He+ + e- -> He
+      k[4] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // He+ + e- -> He
     }
     else if (T >= 9280.0) {
-      k[5] = 1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * vh_invTe)) / (std::exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / std::pow(vh_Te, 0.6353);  // He+ + e- -> He
+      k[5] = 1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * vh_invTe)) / (kb_exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / kb_pow(vh_Te, 0.6353);  // He+ + e- -> He
     }
   }
   {  // group 3: H + H+ -> H2+
     double T = Tgas;
     if (T < 30.0) {
-      k[10] = 2.1e-20 * std::pow(T / 30.0, -0.15);  // H + H+ -> H2+
+      k[10] = 2.1e-20 * kb_pow(T / 30.0, -0.15);  // H + H+ -> H2+
     }
     else if (T >= 30.0) {
-      k[11] = std::pow(10.0, -18.2 - 3.194 * std::log10(T) + 1.786 * std::log10(T)*std::log10(T) - 0.2072 * std::log10(T)*std::log10(T)*std::log10(T));  // H + H+ -> H2+
+      k[11] = kb_pow(10.0, -18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
     }
   }
   {  // group 4: H2 + H+ -> H2+ + H
@@ -343,7 +343,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_sumsav = v_sumsav(T, n, p);
     (void)vh_sumsav;
     if (T >= 100.0 && T >= 100.0) {
-      k[13] = vh_sumsav * std::exp(-vh_asav * vh_invT);  // H2 + H+ -> H2+ + H
+      k[13] = vh_sumsav * kb_exp(-vh_asav * vh_invT);  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 5: H- + H -> H + H + e-
@@ -353,10 +353,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 1160.0) {
-      k[18] = 2.56e-09 * std::pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
+      k[18] = 2.56e-09 * kb_pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
     }
     else if (T >= 1160.0) {
-      k[19] = std::exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
+      k[19] = kb_exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
     }
   }
   {  // group 6: H- + H+ -> H + H
@@ -390,7 +390,7 @@ KB_HD inline void rates_var(double Tgas, const double* n, const Params& p, doubl
   const double vh_ncr21 = v_ncr21(Tgas, n, p);
   (void)vh_ncr21;
   k[16] = dissH2_Martin96(Tgas, n, p);  // H2 + H -> H + H + H
-  k[26] = std::pow(vh_kh21, 1.0 - vh_a21) * std::pow(vh_kl21, vh_a21);  // H2 + H2 -> H + H + H2
+  k[26] = kb_pow(vh_kh21, 1.0 - vh_a21) * kb_pow(vh_kl21, vh_a21);  // H2 + H2 -> H + H + H2
 }
 constexpr int NREA_FIXED = 25;
 KB_HD inline bool rate_is_fixed(int r) {
@@ -855,8 +855,8 @@ KB_HD inline double heating_chem(double Tgas, const double* n, const double* k) 
   const double ev2erg = kbc::eV_to_erg;
   const double dd = Hnuclei_(n);
   const double ncr = 1.0e6 / std::sqrt(Tgas)
-      / (1.6 * std::exp(-std::pow(4.0e2 / Tgas, 2.0)) * n[IDX_H] / dd
-         + 1.4 * std::exp(-1.2e4 / (Tgas + 1.2e3)) * n[IDX_H2] / dd);
+      / (1.6 * kb_exp(-kb_pow(4.0e2 / Tgas, 2.0)) * n[IDX_H] / dd
+         + 1.4 * kb_exp(-1.2e4 / (Tgas + 1.2e3)) * n[IDX_H2] / dd);
   const double ffac = 1.0 / (1.0 + ncr / dd);
   h += k[9] * (3.53*ffac) * n[IDX_Hk]*n[IDX_H];
   h += k[12] * (1.83*ffac) * n[IDX_H2j]*n[IDX_H];
@@ -867,7 +867,7 @@ KB_HD inline double heating_chem(double Tgas, const double* n, const double* k) 
 }
 KB_HD inline double h2_opacity_(const double* n) {
   (void)n;
-  return std::fmin(1.0, std::pow(std::fmax(1.25e-10 * ntot_(n), 1e-40), -0.45));
+  return std::fmin(1.0, kb_pow(std::fmax(1.25e-10 * ntot_(n), 1e-40), -0.45));
 }
 KB_HD inline double gamma_rot_(double Tin, double brot) {
   const double ib = brot / std::fmax(Tin, 10.0);
@@ -875,7 +875,7 @@ KB_HD inline double gamma_rot_(double Tin, double brot) {
 KB_UNROLL
   for (int j = 0; j <= 10; ++j) {
     const double E = j * (j + 1.0) * ib;
-    const double g = (2.0 * j + 1.0) * std::exp(-E);
+    const double g = (2.0 * j + 1.0) * kb_exp(-E);
     z += g; e1 += g * E; e2 += g * E * E;
   }
   const double m = e1 / z;
@@ -889,8 +889,8 @@ KB_UNROLL
     const int j1 = j + 1;
     const double Ep = j * (j + 1.0) * ib;
     const double Eo = j1 * (j1 + 1.0) * ib;
-    const double gp = (2.0 * j + 1.0) * std::exp(-Ep);
-    const double go = 3.0 * (2.0 * j1 + 1.0) * std::exp(-Eo);
+    const double gp = (2.0 * j + 1.0) * kb_exp(-Ep);
+    const double go = 3.0 * (2.0 * j1 + 1.0) * kb_exp(-Eo);
     zp += gp; p1 += gp * Ep; p2 += gp * Ep * Ep;
     zo += go; o1 += go * Eo; o2 += go * Eo * Eo;
   }
@@ -901,7 +901,7 @@ KB_UNROLL
 KB_HD inline double gamma_index(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
   const double iTv = 1.0 / std::fmax(Tgas, 63.3236349736972);
-  const double x_H2 = 6332.36349736972 * iTv, e_H2 = std::exp(x_H2);
+  const double x_H2 = 6332.36349736972 * iTv, e_H2 = kb_exp(x_H2);
   const double gi_H2 = 0.5 * (3.0 + 2.0 * gamma_rotop_(Tgas, p.opratio / (p.opratio + 1.0)) + 2.0 * x_H2 * x_H2 * e_H2 / ((e_H2 - 1.0) * (e_H2 - 1.0)));
   const double gi_H2j = 0.5 * (3.0 + 2.0 * gamma_rot_(Tgas, 61.72352804491875) + 0.0);
   const double mosum = n[IDX_H] + n[IDX_Hj] + n[IDX_Hk] + n[IDX_He] + n[IDX_Hej] + n[IDX_Hejj] + n[IDX_E];
@@ -1012,8 +1012,8 @@ KB_HD inline void lnk_vjp(const double* n, const double* k, double Tth, const Pa
     g[26] -= c * k[26] * 4.48 * n[IDX_H2]*n[IDX_H2];
     const double dd = Hnuclei_(n);
     const double ncr = 1.0e6 / std::sqrt(Tth)
-        / (1.6 * std::exp(-std::pow(4.0e2 / Tth, 2.0)) * n[IDX_H] / dd
-           + 1.4 * std::exp(-1.2e4 / (Tth + 1.2e3)) * n[IDX_H2] / dd);
+        / (1.6 * kb_exp(-kb_pow(4.0e2 / Tth, 2.0)) * n[IDX_H] / dd
+           + 1.4 * kb_exp(-1.2e4 / (Tth + 1.2e3)) * n[IDX_H2] / dd);
     const double ffac = 1.0 / (1.0 + ncr / dd);
     (void)ffac;
     g[9] += c * k[9] * (3.53*ffac) * n[IDX_Hk]*n[IDX_H];
@@ -1070,7 +1070,7 @@ KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) 
   fl[25] = k[25]*n[IDX_H2]*n[IDX_H]*n[IDX_H];
   fl[26] = k[26]*n[IDX_H2]*n[IDX_H2];
 }
-// the neutral atomic metals (none) at n_H 10^(Z + log10(n/n_H)_sun)
+// the neutral atomic metals (none) at n_H 10^(Z + kb_log10(n/n_H)_sun)
 // of the Asplund+09 photospheric abundances, floored at 1e-40
 KB_HD inline void scale_Z(double* n, double Z) {
   (void)n; (void)Z;
@@ -1078,7 +1078,7 @@ KB_HD inline void scale_Z(double* n, double Z) {
 // the column density [cm^-2] of a number density x [cm^-3]
 // (the default estimator: 1.87e21 (x / 1e3)^(2/3))
 KB_HD inline double num2col_(double x) {
-  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+  return 1.87e21 * kb_pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
 KB_HD inline double NH_col_(const double* n) {
   (void)n;

@@ -151,7 +151,7 @@ KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_lnTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::log(Tgas*kbc::boltzmann_eV);
+  return kb_log(Tgas*kbc::boltzmann_eV);
 }
 KB_HD inline double v_invTe(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -255,19 +255,19 @@ KB_HD inline double v_bsav8(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_sumsav(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return v_bsav1(Tgas, n, p) + v_bsav2(Tgas, n, p) * std::log(Tgas) + v_bsav3(Tgas, n, p) * std::log(Tgas)*std::log(Tgas) + v_bsav4(Tgas, n, p) * std::log(Tgas)*std::log(Tgas)*std::log(Tgas) + v_bsav5(Tgas, n, p) * std::log(Tgas)*std::log(Tgas)*std::log(Tgas)*std::log(Tgas) + v_bsav6(Tgas, n, p) * ipow_<5>(std::log(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<6>(std::log(Tgas)) + v_bsav8(Tgas, n, p) * ipow_<7>(std::log(Tgas));
+  return v_bsav1(Tgas, n, p) + v_bsav2(Tgas, n, p) * kb_log(Tgas) + v_bsav3(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas) + v_bsav4(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas) + v_bsav5(Tgas, n, p) * kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas)*kb_log(Tgas) + v_bsav6(Tgas, n, p) * ipow_<5>(kb_log(Tgas)) + v_bsav7(Tgas, n, p) * ipow_<6>(kb_log(Tgas)) + v_bsav8(Tgas, n, p) * ipow_<7>(kb_log(Tgas));
 }
 KB_HD inline double v_kl21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return 1.18e-10 * std::exp(-69500.0 * v_invT(Tgas, n, p));
+  return 1.18e-10 * kb_exp(-69500.0 * v_invT(Tgas, n, p));
 }
 KB_HD inline double v_kh21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * std::exp(-52000.0 * v_invT(Tgas, n, p)) * (1.0 - std::exp(-6000.0 * v_invT(Tgas, n, p)));
+  return 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * (1.0 - kb_exp(-6000.0 * v_invT(Tgas, n, p)));
 }
 KB_HD inline double v_ncr21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return std::pow(10.0, 4.845 - 1.3 * std::log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * std::log10(v_T(Tgas, n, p) * 0.0001)*std::log10(v_T(Tgas, n, p) * 0.0001));
+  return kb_pow(10.0, 4.845 - 1.3 * kb_log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * kb_log10(v_T(Tgas, n, p) * 0.0001)*kb_log10(v_T(Tgas, n, p) * 0.0001));
 }
 KB_HD inline double v_a21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -305,26 +305,26 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   (void)vh_invT;
   const double vh_lnTe = v_lnTe(Tgas, n, p);
   (void)vh_lnTe;
-  k[0] = std::exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
-  k[3] = std::exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
-  k[6] = std::exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
-  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * std::pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * std::pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
-  k[8] = 1.4e-18 * std::pow(Tgas, 0.928) * std::exp(-Tgas / 16200.0);  // H + e- -> H-
-  k[9] = vh_a1 * (std::pow(Tgas, vh_a2) + vh_a3 * std::pow(Tgas, vh_a4) + vh_a5 * std::pow(Tgas, vh_a6)) / (1.0 + vh_a7 * std::pow(Tgas, vh_a8) + vh_a9 * std::pow(Tgas, vh_a10) + vh_a11 * std::pow(Tgas, vh_a12));  // H- + H -> H2 + e-
+  k[0] = kb_exp(-32.71396786 + 13.536556 * vh_lnTe - 5.73932875 * vh_lnTe*vh_lnTe + 1.56315498 * vh_lnTe*vh_lnTe*vh_lnTe - 0.2877056 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0348255977 * ipow_<5>(vh_lnTe) - 0.00263197617 * ipow_<6>(vh_lnTe) + 0.000111954395 * ipow_<7>(vh_lnTe) - 2.03914985e-06 * ipow_<8>(vh_lnTe));  // H + e- -> H+ + e- + e-
+  k[3] = kb_exp(-44.09864886 + 23.91596563 * vh_lnTe - 10.7532302 * vh_lnTe*vh_lnTe + 3.05803875 * vh_lnTe*vh_lnTe*vh_lnTe - 0.56851189 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0679539123 * ipow_<5>(vh_lnTe) - 0.0050090561 * ipow_<6>(vh_lnTe) + 0.000206723616 * ipow_<7>(vh_lnTe) - 3.64916141e-06 * ipow_<8>(vh_lnTe));  // He + e- -> He+ + e- + e-
+  k[6] = kb_exp(-68.71040990212 + 43.93347632635 * vh_lnTe - 18.48066993568 * vh_lnTe*vh_lnTe + 4.701626486759002 * vh_lnTe*vh_lnTe*vh_lnTe - 0.7692466334492 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.08113042097303 * ipow_<5>(vh_lnTe) - 0.005324020628287001 * ipow_<6>(vh_lnTe) + 0.0001975705312221 * ipow_<7>(vh_lnTe) - 3.165581065665e-06 * ipow_<8>(vh_lnTe));  // He+ + e- -> He++ + e- + e-
+  k[7] = 1.891e-10 / (std::sqrt(Tgas / 9.37) * kb_pow(1.0 + std::sqrt(Tgas / 9.37), 0.2476) * kb_pow(1.0 + std::sqrt(Tgas / 2774000.0), 1.7524));  // He++ + e- -> He+
+  k[8] = 1.4e-18 * kb_pow(Tgas, 0.928) * kb_exp(-Tgas / 16200.0);  // H + e- -> H-
+  k[9] = vh_a1 * (kb_pow(Tgas, vh_a2) + vh_a3 * kb_pow(Tgas, vh_a4) + vh_a5 * kb_pow(Tgas, vh_a6)) / (1.0 + vh_a7 * kb_pow(Tgas, vh_a8) + vh_a9 * kb_pow(Tgas, vh_a10) + vh_a11 * kb_pow(Tgas, vh_a12));  // H- + H -> H2 + e-
   k[12] = 6e-10;  // H2+ + H -> H2 + H+
-  k[14] = 35.5 * std::pow(Tgas, -2.28) * std::exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
-  k[15] = 4.38e-10 * std::exp(-102000.0 / Tgas) * std::pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
-  k[17] = std::exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
+  k[14] = 35.5 * kb_pow(Tgas, -2.28) * kb_exp(-46707.0 / Tgas);  // H2 + e- -> H + H-
+  k[15] = 4.38e-10 * kb_exp(-102000.0 / Tgas) * kb_pow(Tgas, 0.35);  // H2 + e- -> H + H + e-
+  k[17] = kb_exp(-18.01849334273 + 2.360852208681 * vh_lnTe - 0.2827443061704 * vh_lnTe*vh_lnTe + 0.01623316639567 * vh_lnTe*vh_lnTe*vh_lnTe - 0.03365012031362999 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.01178329782711 * ipow_<5>(vh_lnTe) - 0.001656194699504 * ipow_<6>(vh_lnTe) + 0.0001068275202678 * ipow_<7>(vh_lnTe) - 2.631285809207e-06 * ipow_<8>(vh_lnTe));  // H- + e- -> H + e- + e-
   k[20] = 2.96e-06 / std::sqrt(Tgas) - 1.73e-09 + 2.5e-10 * std::sqrt(Tgas) - 7.77e-13 * Tgas;  // H- + H+ -> H + H
-  k[21] = 1e-08 * std::pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
+  k[21] = 1e-08 * kb_pow(Tgas, -0.4);  // H- + H+ -> H2+ + e-
   k[22] = 1000000.0 * (4.2278e-14 - 2.3088e-17 * Tgas + 7.3428e-21 * Tgas*Tgas - 7.5474e-25 * Tgas*Tgas*Tgas + 3.3468e-29 * Tgas*Tgas*Tgas*Tgas - 5.528e-34 * ipow_<5>(Tgas));  // H2+ + e- -> H + H
   k[23] = 5e-07 * std::sqrt(100.0 * vh_invT);  // H2+ + H- -> H + H2
-  k[24] = 6e-32 * std::pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas));  // H + H + H -> H2 + H
-  k[25] = (6e-32 * std::pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas))) / 8.0;  // H2 + H + H -> H2 + H2
-  k[27] = 1.2e-15 * std::pow(Tgas / 300.0, 0.25);  // He+ + H -> He + H+
-  k[71] = 6.622e-11 / (std::sqrt(Tgas / 4.136) * std::pow(1.0 + std::sqrt(Tgas / 4.136), 1.0 - (0.6109 + 0.4093 * std::exp(-87700.0 / Tgas))) * std::pow(1.0 + std::sqrt(Tgas / 4214000.0), 1.0 + (0.6109 + 0.4093 * std::exp(-87700.0 / Tgas)))) + 1.0/(ipow_<1>(Tgas) * std::sqrt(Tgas)) * (5.629e-08 * std::exp(-5395.0 / Tgas) + 2.55e-07 * std::exp(-17700.0 / Tgas) + 0.0006173 * std::exp(-167100.0 / Tgas) + 0.0001627 * std::exp(-268700.0 / Tgas));  // O+ + e- -> O
+  k[24] = 6e-32 * kb_pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas));  // H + H + H -> H2 + H
+  k[25] = (6e-32 * kb_pow(Tgas, -0.25) + 2e-31 * 1.0/(std::sqrt(Tgas))) / 8.0;  // H2 + H + H -> H2 + H2
+  k[27] = 1.2e-15 * kb_pow(Tgas / 300.0, 0.25);  // He+ + H -> He + H+
+  k[71] = 6.622e-11 / (std::sqrt(Tgas / 4.136) * kb_pow(1.0 + std::sqrt(Tgas / 4.136), 1.0 - (0.6109 + 0.4093 * kb_exp(-87700.0 / Tgas))) * kb_pow(1.0 + std::sqrt(Tgas / 4214000.0), 1.0 + (0.6109 + 0.4093 * kb_exp(-87700.0 / Tgas)))) + 1.0/(ipow_<1>(Tgas) * std::sqrt(Tgas)) * (5.629e-08 * kb_exp(-5395.0 / Tgas) + 2.55e-07 * kb_exp(-17700.0 / Tgas) + 0.0006173 * kb_exp(-167100.0 / Tgas) + 0.0001627 * kb_exp(-268700.0 / Tgas));  // O+ + e- -> O
   k[72] = 0.0;  // CO+ + e- -> CO
-  k[73] = 2.75e-07 * std::pow(Tgas / 300.0, -0.55);  // CO+ + e- -> C + O
+  k[73] = 2.75e-07 * kb_pow(Tgas / 300.0, -0.55);  // CO+ + e- -> C + O
   {  // group 1: H+ + e- -> H
     double T = Tgas;
     const double vh_invTe = v_invTe(T, n, p);
@@ -332,10 +332,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 5500.0) {
-      k[1] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // H+ + e- -> H
+      k[1] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // H+ + e- -> H
     }
     else if (T >= 5500.0) {
-      k[2] = std::exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
+      k[2] = kb_exp(-28.61303380689232 - 0.7241125657826851 * vh_lnTe - 0.02026044731984691 * vh_lnTe*vh_lnTe - 0.002380861877349834 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0003212605213188796 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe - 1.421502914054107e-05 * ipow_<5>(vh_lnTe) + 4.989108920299513e-06 * ipow_<6>(vh_lnTe) + 5.755614137575758e-07 * ipow_<7>(vh_lnTe) - 1.856767039775261e-08 * ipow_<8>(vh_lnTe) - 3.071135243196595e-09 * ipow_<9>(vh_lnTe));  // H+ + e- -> H
     }
   }
   {  // group 2: He+ + e- -> He
@@ -345,19 +345,19 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invTe = v_invTe(T, n, p);
     (void)vh_invTe;
     if (T < 9280.0) {
-      k[4] = 3.92e-13 * std::pow(vh_invTe, 0.6353);  // He+ + e- -> He
+      k[4] = 3.92e-13 * kb_pow(vh_invTe, 0.6353);  // He+ + e- -> He
     }
     else if (T >= 9280.0) {
-      k[5] = 1.54e-09 * (1.0 + 0.3 / std::exp(8.099328789667 * vh_invTe)) / (std::exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / std::pow(vh_Te, 0.6353);  // He+ + e- -> He
+      k[5] = 1.54e-09 * (1.0 + 0.3 / kb_exp(8.099328789667 * vh_invTe)) / (kb_exp(40.49664394833662 * vh_invTe) * ipow_<1>(vh_Te) * std::sqrt(vh_Te)) + 3.92e-13 / kb_pow(vh_Te, 0.6353);  // He+ + e- -> He
     }
   }
   {  // group 3: H + H+ -> H2+
     double T = Tgas;
     if (T < 30.0) {
-      k[10] = 2.1e-20 * std::pow(T / 30.0, -0.15);  // H + H+ -> H2+
+      k[10] = 2.1e-20 * kb_pow(T / 30.0, -0.15);  // H + H+ -> H2+
     }
     else if (T >= 30.0) {
-      k[11] = std::pow(10.0, -18.2 - 3.194 * std::log10(T) + 1.786 * std::log10(T)*std::log10(T) - 0.2072 * std::log10(T)*std::log10(T)*std::log10(T));  // H + H+ -> H2+
+      k[11] = kb_pow(10.0, -18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
     }
   }
   {  // group 4: H2 + H+ -> H2+ + H
@@ -386,7 +386,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_sumsav = v_sumsav(T, n, p);
     (void)vh_sumsav;
     if (T >= 100.0 && T >= 100.0) {
-      k[13] = vh_sumsav * std::exp(-vh_asav * vh_invT);  // H2 + H+ -> H2+ + H
+      k[13] = vh_sumsav * kb_exp(-vh_asav * vh_invT);  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 5: H- + H -> H + H + e-
@@ -396,10 +396,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_lnTe = v_lnTe(T, n, p);
     (void)vh_lnTe;
     if (T < 1160.0) {
-      k[18] = 2.56e-09 * std::pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
+      k[18] = 2.56e-09 * kb_pow(vh_Te, 1.78186);  // H- + H -> H + H + e-
     }
     else if (T >= 1160.0) {
-      k[19] = std::exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
+      k[19] = kb_exp(-20.37260896533324 + 1.139449335841631 * vh_lnTe - 0.1421013521554148 * vh_lnTe*vh_lnTe + 0.00846445538663 * vh_lnTe*vh_lnTe*vh_lnTe - 0.0014327641212992 * vh_lnTe*vh_lnTe*vh_lnTe*vh_lnTe + 0.0002012250284791 * ipow_<5>(vh_lnTe) + 8.66396324309e-05 * ipow_<6>(vh_lnTe) - 2.585009680264e-05 * ipow_<7>(vh_lnTe) + 2.4555011970392e-06 * ipow_<8>(vh_lnTe) - 8.06838246118e-08 * ipow_<9>(vh_lnTe));  // H- + H -> H + H + e-
     }
   }
   {  // group 6: He + H+ -> He+ + H
@@ -407,10 +407,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T < 10000.0) {
-      k[28] = 1.26e-09 * std::pow(T, -0.75) * std::exp(-127500.0 * vh_invT);  // He + H+ -> He+ + H
+      k[28] = 1.26e-09 * kb_pow(T, -0.75) * kb_exp(-127500.0 * vh_invT);  // He + H+ -> He+ + H
     }
     else if (T >= 10000.0) {
-      k[29] = 4e-37 * std::pow(T, 4.74);  // He + H+ -> He+ + H
+      k[29] = 4e-37 * kb_pow(T, 4.74);  // He + H+ -> He+ + H
     }
   }
 }
@@ -432,48 +432,48 @@ KB_HD inline void rates_var(double Tgas, const double* n, const Params& p, doubl
   const double vh_ncr21 = v_ncr21(Tgas, n, p);
   (void)vh_ncr21;
   k[16] = dissH2_Martin96(Tgas, n, p);  // H2 + H -> H + H + H
-  k[26] = std::pow(vh_kh21, 1.0 - vh_a21) * std::pow(vh_kl21, vh_a21);  // H2 + H2 -> H + H + H2
+  k[26] = kb_pow(vh_kh21, 1.0 - vh_a21) * kb_pow(vh_kl21, vh_a21);  // H2 + H2 -> H + H + H2
   k[30] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.8e-10);  // O+ + H -> H+ + O
-  k[31] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7e-10 * std::exp(-232.0 * vh_invT));  // H+ + O -> O+ + H
+  k[31] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7e-10 * kb_exp(-232.0 * vh_invT));  // H+ + O -> O+ + H
   k[32] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.7e-09);  // O+ + H2 -> OH+ + H
   k[33] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.01e-09);  // OH+ + H2 -> H2O+ + H
   k[34] = (ntot_(n) > 100000000000000.0 ? 0.0 : 8.3e-10);  // H2O+ + H2 -> H3O+ + H
   k[35] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2e-07 * 1.0/(std::sqrt(vh_T32)));  // H2O+ + e- -> O + H2
   k[36] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.6e-07 * 1.0/(std::sqrt(vh_T32)));  // H2O+ + e- -> OH + H
   k[37] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.5e-07 * 1.0/(std::sqrt(vh_T32)));  // H3O+ + e- -> H2O + H
-  k[38] = (ntot_(n) > 100000000000000.0 ? 0.0 : 9.9e-19 * std::pow(vh_T32, -0.38));  // O + H -> OH
-  k[39] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.43e-13 * std::pow(vh_T32, 2.67) * std::exp(-3160.0 * vh_invT));  // O + H2 -> OH + H
-  k[40] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.55e-12 * std::pow(vh_T32, 1.6) * std::exp(-1660.0 * vh_invT));  // H2 + OH -> H2O + H
-  k[41] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.65e-12 * std::pow(vh_T32, 1.14) * std::exp(-50.0 * vh_invT));  // OH + OH -> H2O + O
+  k[38] = (ntot_(n) > 100000000000000.0 ? 0.0 : 9.9e-19 * kb_pow(vh_T32, -0.38));  // O + H -> OH
+  k[39] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.43e-13 * kb_pow(vh_T32, 2.67) * kb_exp(-3160.0 * vh_invT));  // O + H2 -> OH + H
+  k[40] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.55e-12 * kb_pow(vh_T32, 1.6) * kb_exp(-1660.0 * vh_invT));  // H2 + OH -> H2O + H
+  k[41] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.65e-12 * kb_pow(vh_T32, 1.14) * kb_exp(-50.0 * vh_invT));  // OH + OH -> H2O + O
   k[42] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2.1e-09);  // H+ + OH -> OH+ + H
   k[43] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.9e-09);  // H+ + H2O -> H2O+ + H
-  k[44] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7e-14 * std::pow(vh_T32, 2.8) * std::exp(-1950.0 * vh_invT));  // H + OH -> H2 + O
-  k[45] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.83e-12 * std::pow(vh_T32, 1.6) * std::exp(-9720.0 * vh_invT));  // H + H2O -> OH + H2
-  k[46] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.9e-20 * std::pow(vh_T32, 1.58));  // O + O -> O2
-  k[47] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.34e-11 * 1.0/(std::sqrt(vh_T32)) * std::exp(-30.0 * vh_invT));  // O + OH -> O2 + H
-  k[48] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.3e-10 * std::exp(-8460.0 * vh_invT));  // H + O2 -> OH + O
+  k[44] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7e-14 * kb_pow(vh_T32, 2.8) * kb_exp(-1950.0 * vh_invT));  // H + OH -> H2 + O
+  k[45] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.83e-12 * kb_pow(vh_T32, 1.6) * kb_exp(-9720.0 * vh_invT));  // H + H2O -> OH + H2
+  k[46] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.9e-20 * kb_pow(vh_T32, 1.58));  // O + O -> O2
+  k[47] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.34e-11 * 1.0/(std::sqrt(vh_T32)) * kb_exp(-30.0 * vh_invT));  // O + OH -> O2 + H
+  k[48] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.3e-10 * kb_exp(-8460.0 * vh_invT));  // H + O2 -> OH + O
   k[49] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2e-09);  // H+ + O2 -> O2+ + H
-  k[50] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.95e-07 * std::pow(vh_T32, -0.7));  // O2+ + e- -> O + O
+  k[50] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.95e-07 * kb_pow(vh_T32, -0.7));  // O2+ + e- -> O + O
   k[51] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.6e-11);  // O + CH -> CO + H
   k[52] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1.1e-10 * std::sqrt(vh_T32));  // C + OH -> CO + H
   k[53] = (ntot_(n) > 100000000000000.0 ? 0.0 : 3.3e-11);  // C + O2 -> CO + O
   k[54] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.2e-10);  // C+ + O2 -> O+ + CO
   k[55] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1e-13);  // OH + CO -> CO2 + H
-  k[56] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.4e-12 * std::pow(vh_T32, -0.61));  // C+ + e- -> C
+  k[56] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.4e-12 * kb_pow(vh_T32, -0.61));  // C+ + e- -> C
   k[57] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7.7e-10);  // C+ + OH -> CO+ + H
   k[58] = (ntot_(n) > 100000000000000.0 ? 0.0 : 7.5e-10);  // CO+ + H -> H+ + CO
   k[59] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1e-17);  // C + H -> CH
-  k[60] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.64e-10 * std::exp(-11700.0 * vh_invT));  // C + H2 -> CH + H
+  k[60] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.64e-10 * kb_exp(-11700.0 * vh_invT));  // C + H2 -> CH + H
   k[61] = (ntot_(n) > 100000000000000.0 ? 0.0 : 4.98e-11);  // H + CH -> C + H2
-  k[62] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2.38e-10 * std::exp(-1760.0 * vh_invT));  // H2 + CH -> CH2 + H
+  k[62] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2.38e-10 * kb_exp(-1760.0 * vh_invT));  // H2 + CH -> CH2 + H
   k[63] = (ntot_(n) > 100000000000000.0 ? 0.0 : 2.7e-10);  // H + CH2 -> CH + H2
-  k[64] = (ntot_(n) > 100000000000000.0 ? 0.0 : 5.18e-11 * std::pow(vh_T32, 0.17) * std::exp(-6400.0 * vh_invT));  // H2 + CH2 -> CH3 + H
-  k[65] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1e-10 * std::exp(-7600.0 * vh_invT));  // H + CH3 -> CH2 + H2
-  k[66] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.86e-14 * std::pow(vh_T32, 2.74) * std::exp(-4740.0 * vh_invT));  // H2 + CH3 -> CH4 + H
-  k[67] = (ntot_(n) > 100000000000000.0 ? 0.0 : 5.82e-13 * vh_T32*vh_T32*vh_T32 * std::exp(-4045.0 * vh_invT));  // H + CH4 -> H2 + CH3
+  k[64] = (ntot_(n) > 100000000000000.0 ? 0.0 : 5.18e-11 * kb_pow(vh_T32, 0.17) * kb_exp(-6400.0 * vh_invT));  // H2 + CH2 -> CH3 + H
+  k[65] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1e-10 * kb_exp(-7600.0 * vh_invT));  // H + CH3 -> CH2 + H2
+  k[66] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.86e-14 * kb_pow(vh_T32, 2.74) * kb_exp(-4740.0 * vh_invT));  // H2 + CH3 -> CH4 + H
+  k[67] = (ntot_(n) > 100000000000000.0 ? 0.0 : 5.82e-13 * vh_T32*vh_T32*vh_T32 * kb_exp(-4045.0 * vh_invT));  // H + CH4 -> H2 + CH3
   k[68] = (ntot_(n) > 100000000000000.0 ? 0.0 : 1e-17);  // H2 + C -> CH2
   k[69] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.5e-07 * 1.0/(std::sqrt(vh_T32)));  // H3O+ + e- -> OH + H + H
-  k[70] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.3e-09 * std::pow(vh_T32, -0.48));  // OH+ + e- -> O + H
+  k[70] = (ntot_(n) > 100000000000000.0 ? 0.0 : 6.3e-09 * kb_pow(vh_T32, -0.48));  // OH+ + e- -> O + H
 }
 constexpr int NREA_FIXED = 31;
 KB_HD inline bool rate_is_fixed(int r) {
@@ -1882,18 +1882,18 @@ KB_HD inline void reaction_fluxes(const double* n, const double* k, double* fl) 
   fl[72] = k[72]*n[IDX_COj]*n[IDX_E];
   fl[73] = k[73]*n[IDX_COj]*n[IDX_E];
 }
-// the neutral atomic metals (C, O) at n_H 10^(Z + log10(n/n_H)_sun)
+// the neutral atomic metals (C, O) at n_H 10^(Z + kb_log10(n/n_H)_sun)
 // of the Asplund+09 photospheric abundances, floored at 1e-40
 KB_HD inline void scale_Z(double* n, double Z) {
   (void)n; (void)Z;
   const double Htot = Hnuclei_(n);
-  n[IDX_C] = std::fmax(Htot * std::pow(10.0, Z + (-3.5700000000000003)), 1e-40);
-  n[IDX_O] = std::fmax(Htot * std::pow(10.0, Z + (-3.3100000000000005)), 1e-40);
+  n[IDX_C] = std::fmax(Htot * kb_pow(10.0, Z + (-3.5700000000000003)), 1e-40);
+  n[IDX_O] = std::fmax(Htot * kb_pow(10.0, Z + (-3.3100000000000005)), 1e-40);
 }
 // the column density [cm^-2] of a number density x [cm^-3]
 // (the default estimator: 1.87e21 (x / 1e3)^(2/3))
 KB_HD inline double num2col_(double x) {
-  return 1.87e21 * std::pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
+  return 1.87e21 * kb_pow(std::fmax(x, 1e-40) * 1e-3, 2.0/3.0);
 }
 KB_HD inline double NH_col_(const double* n) {
   (void)n;

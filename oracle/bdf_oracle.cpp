@@ -290,11 +290,24 @@ struct Problem {
     const double T = thermal_T(iT >= 0 ? y[iT] : Tfix);
     return thermal_dTdt(T, y, kk, p);
   }
+  // the species a freeze directive holds for this cell (none: 0)
+  int frozen(int* idx) const {
+#if KB_NFREEZE > 0
+    return frozen_species(p, idx);
+#else
+    (void)idx;
+    return 0;
+#endif
+  }
   void full_rhs(const double* y, double* f) {
     const double T = state_T(y);
     eval_rates(T, y, k);
     rhs(y, k, f);
     if (iT >= 0) f[iT] = aux(y, k);
+    // freeze_rows_ (solve_cell.hpp:711-720)
+    int idx[KB_NFREEZE > 0 ? KB_NFREEZE : 1];
+    const int m = frozen(idx);
+    for (int q = 0; q < m; ++q) f[idx[q]] = 0.0;
   }
   // the integrator's view: T <= 0 or a non-finite f is recoverable
   int rhs_cb(const double* y, double* f) {
@@ -314,6 +327,15 @@ struct Problem {
   // difference-quotient thermal row (jac_assemble_, solve_cell.hpp:883-1118);
   // J column-major NEQ x NEQ, zeroed by the caller
   int jac_cb(const double* y, double* J, double* yp, double* fp) {
+    jac_assemble(y, J, yp, fp);
+    // jac_cell_: the frozen species' rows zeroed (solve_cell.hpp:1118-1131)
+    int idx[KB_NFREEZE > 0 ? KB_NFREEZE : 1];
+    const int m = frozen(idx);
+    for (int q = 0; q < m; ++q)
+      for (int j = 0; j < NEQ; ++j) J[idx[q] + (long)j * NEQ] = 0.0;
+    return 0;
+  }
+  int jac_assemble(const double* y, double* J, double* yp, double* fp) {
     const int N = NEQ;
     const double T = state_T(y);
     eval_rates(T, y, k0);
@@ -1312,7 +1334,8 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
   if (params_missing(c.p) >= 0) return FLAG_PARAM_UNSET;
   photo_rates_(c.p, so, phirow);
 #if KB_NFREEZE > 0
-  if (freeze_active(c.p)) return -104;  // frozen rows are not built
+  // the adjoint does not differentiate frozen rows: refused there
+  if (tape != nullptr && freeze_active(c.p)) return -104;
 #endif
   c.Tfix = *Tgas;
   c.NEQ = NSPEC;
@@ -1409,7 +1432,7 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
       n[i] = y[i];
       if (so->clip_negative && n[i] < 0.0) n[i] = 0.0;
     }
-    conserve_cell(n0, n, so->conserve);  // solve_cell.hpp:2169-2175
+    conserve_cell(n0, n, so->conserve, c.p);  // solve_cell.hpp:2169-2175
     if (c.iT >= 0) *Tgas = y[c.iT];
   }
   return flag;

@@ -109,9 +109,11 @@ def counting_source(key):
     the math functions routed through the counting type"""
     def conv(text):
         text = re.sub(r"#include \"../csrc/kb_common.h\"", "", text)
+        text = re.sub(r"#include \"../csrc/kb_conserve.h\"", "", text)
         text = re.sub(r"#include \"../csrc/kb_physics.h\"",
                       lambda m: conv((ROOT / "krome_x_b200/csrc/kb_physics.h")
                                      .read_text()), text)
+        text = re.sub(r"\bkb_(exp|log10|log|pow)\(", r"kbfc::\1(", text)
         text = re.sub(r"\bdouble\b", "kbfc::cd", text)
         text = text.replace("std::", "kbfc::")
         text = re.sub(r"(?<![\w:])(isfinite|fmin|fmax|fabs|exp|log|log10|pow|sqrt|tanh)\(",

@@ -92,6 +92,57 @@ class Oracle:
         self.seconds = time.perf_counter() - t0
         return dict(n=n, T=T, flags=flags, stats=stats, ret=ret)
 
+    def equilibrium(self, n, T, par, t0=100 * 31557600.0,
+                    tmax=5e8 * 31557600.0, factor=3.0, ertol=1e-5,
+                    eatol=1e-12, evolve_T=0, **opts):
+        """integrate every cell to steady state, restating the reference's
+        solve_equilibrium (runtime/core/solve_cell.hpp:2249-2301) over this
+        oracle's solve: outputs at t0 factor^k, each interval a solve from
+        the current state; converged (0) when max_i |dn_i| / max(n_i,
+        eatol ntot) (and |dT| / T with evolve_T) between outputs is below
+        ertol, 1 at tmax, a failed interval restores the input (its flag).
+        The defaults are the reference's handle keys eq_t0 (100 yr),
+        eq_tmax (5e8 yr), eq_factor, eq_rtol, eq_atol."""
+        n = np.array(n, dtype=float, order="C", copy=True)
+        T = np.array(T, dtype=float, order="C", copy=True)
+        par = np.ascontiguousarray(par, dtype=float)
+        ncell = n.shape[0]
+        nin, Tin = n.copy(), T.copy()
+        t = np.zeros(ncell)
+        dt = np.full(ncell, t0)
+        done = np.zeros(ncell, dtype=bool)
+        flags = np.zeros(ncell, dtype=np.intc)
+        for _ in range(10000):
+            act = ~done
+            if not act.any():
+                break
+            prev, Tprev = n.copy(), T.copy()
+            d = np.where(act, dt, 0.0)
+            out = self.solve(n, T, d, par, evolve_T=evolve_T, **opts)
+            fail = act & (out["flags"] != 0)
+            n[fail], T[fail] = nin[fail], Tin[fail]
+            flags[fail] = out["flags"][fail]
+            done |= fail
+            ok = act & ~fail
+            n[ok], T[ok] = out["n"][ok], out["T"][ok]
+            for c in np.nonzero(ok)[0]:  # the reference's scalar order
+                t[c] += dt[c]
+                tot = 0.0
+                for v in n[c]:  # ntot_: the sequential sum
+                    tot += v
+                floor = eatol * tot
+                w = abs(T[c] - Tprev[c]) / T[c] if evolve_T else 0.0
+                for i in range(n.shape[1]):
+                    w = max(w, abs(n[c, i] - prev[c, i]) / max(n[c, i], floor))
+                if w < ertol:
+                    done[c] = True
+                elif t[c] >= tmax:
+                    flags[c] = 1
+                    done[c] = True
+                else:
+                    dt[c] = min((factor - 1.0) * t[c], tmax - t[c])
+        return dict(n=n, T=T, flags=flags)
+
     def adjoint(self, n, T, dt, par, gn, gT, lnm=None, evolve_T=1, jac=0,
                 rtol=1e-6, atol_n=1e-20, atol_T=1e-6, max_steps=100000,
                 max_err_fails=7, max_conv_fails=10, max_restarts=5,
@@ -215,10 +266,45 @@ class Reference:
         return dict(n=n, T=T, flags=flags, ret=ret)
 
 
+    def equilibrium(self, n, T, par, **opts):
+        """the reference's krome_equilibrium_cells (krome.h:366-376)"""
+        n = np.array(n, dtype=float, order="C", copy=True)
+        T = np.array(T, dtype=float, order="C", copy=True)
+        par = np.ascontiguousarray(par, dtype=float)
+        ncell = n.shape[0]
+        flags = np.zeros(ncell, dtype=np.intc)
+        h = self.lib.krome_opts_new()
+        opts = dict(opts)
+        opts.setdefault("error_report", 0)
+        for k, v in opts.items():
+            if self.lib.krome_opts_set(h, k.encode(), float(v)) != 0:
+                raise KeyError(k)
+        f = self.lib.krome_equilibrium_cells
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_int, ctypes.c_void_p,
+                      _I, ctypes.c_void_p]
+        ret = f(ncell, _ptr(n), _ptr(T), _ptr(par),
+                0 if par.ndim == 1 else self.npar, None, _ptr(flags, _I), h)
+        self.lib.krome_opts_free(h)
+        return dict(n=n, T=T, flags=flags, ret=ret)
+
+
 def _ref_worker(args):
     net, strict, n, T, dt, par, opts = args
     out = Reference(net, strict=strict).solve(n, T, dt, par, **opts)
     return out
+
+
+def _ref_eq_worker(args):
+    net, strict, n, T, par, opts = args
+    return Reference(net, strict=strict).equilibrium(n, T, par, **opts)
+
+
+def reference_equilibrium(net, n, T, par, strict=False, **opts):
+    """Reference(net).equilibrium in a spawned child process"""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1) as pool:
+        return pool.map(_ref_eq_worker, [(net, strict, n, T, par, opts)])[0]
 
 
 def reference_solve(net, n, T, dt, par, strict=False, **opts):

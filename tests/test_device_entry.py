@@ -2,11 +2,13 @@
 (krome_solve_cells_x, krome_solve_cells_device, krome_solve_cells_x_device;
 reference runtime/interfaces/C/krome.h:296-349).
 
-They stage the caller's layout (species-major with a leading dimension, or
-cell-major; densities or mass fractions with the gas density) into the
-solve the host entry point runs, so their results equal krome_solve_cells'
+The lane-per-cell kernel reads and writes the caller's layout itself
+(species-major with a leading dimension, or cell-major; densities or mass
+fractions with the gas density), so their results equal krome_solve_cells'
 bit for bit on the same cells; a failed cell keeps its input; the summary
-counts the cells; the required-parameter rule rejects the whole call."""
+counts the cells; the required-parameter rule rejects the whole call. The
+device-array consistent advection (krome_conserve_cells_device, _x_device,
+krome.h:351-360) equals the host entry's."""
 import ctypes
 
 import numpy as np
@@ -219,3 +221,88 @@ def test_python_solve_x_matches_the_c_entry():
     np.testing.assert_array_equal(r.flags, fh)
     # the caller's arrays are not modified (the reference's contract)
     np.testing.assert_array_equal(x, _case(64, seed=9)[4])
+
+
+def _conserve_lib(net):
+    lib = ctypes.CDLL(str(net.path))
+    V = ctypes.c_void_p
+    for f in ("krome_conserve_cells_device", "krome_conserve_cells_x_device"):
+        fn = getattr(lib, f)
+        fn.argtypes = [ctypes.c_int, V, ctypes.c_int, ctypes.c_long, V,
+                       ctypes.c_int, V, ctypes.c_int, V]
+        fn.restype = ctypes.c_int
+    for f in ("krome_conserve_cells", "krome_conserve_cells_x",
+              "krome_get_element_totals", "krome_get_element_totals_x"):
+        getattr(lib, f).restype = ctypes.c_int
+    return lib
+
+
+def test_device_conservation_rejects_bad_arguments():
+    net = krome.load(KEY)
+    lib = _conserve_lib(net)
+    buf = (ctypes.c_double * 64)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    f = lib.krome_conserve_cells_device
+    assert f(4, p, 2, 0, p, 0, None, 0, None) == -1          # layout
+    assert f(4, p, 0, 3, p, 0, None, 0, None) == -1          # ld < ncell
+    assert f(4, p, 1, 0, p, 3, None, 0, None) == -1          # ref_stride
+    assert f(4, p, 1, 0, None, 0, None, 0, None) == -1       # no ref
+    assert f(0, p, 1, 0, p, 0, None, 0, None) == 0           # nothing to do
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mass", [0, 1])
+@pytest.mark.parametrize("layout,pad", [(0, 5), (1, 0)])
+def test_device_conservation_equals_the_host_entry(mass, layout, pad):
+    """krome_conserve_cells(_x)_device (reference krome.h:351-360) on the
+    caller's layout: the host entry's cells and flags (the projection's
+    arithmetic may contract differently on the device: 1e-13)"""
+    import torch
+    net = krome.load(KEY)
+    lib = _conserve_lib(net)
+    ncell = 300
+    n, T, dt, par, x, rho, m = _case(ncell, seed=17)
+    nelem = lib.krome_nelem()
+    rng = np.random.default_rng(5)
+    adv = n * rng.uniform(0.7, 1.3, n.shape)
+    adv[3, 0] = -1e-30
+    tot = np.zeros((ncell, nelem))
+    if mass:
+        v = adv * m / rho[:, None]
+        lib.krome_get_element_totals_x(ncell, x.ctypes.data_as(_D),
+                                       tot.ctypes.data_as(_D))
+        host = lib.krome_conserve_cells_x
+        dev_fn = lib.krome_conserve_cells_x_device
+    else:
+        v = adv
+        lib.krome_get_element_totals(ncell, n.ctypes.data_as(_D),
+                                     tot.ctypes.data_as(_D))
+        host = lib.krome_conserve_cells
+        dev_fn = lib.krome_conserve_cells_device
+    vh = v.copy()
+    fh = np.zeros(ncell, dtype=np.intc)
+    rh = host(ncell, vh.ctypes.data_as(_D), tot.ctypes.data_as(_D), nelem,
+              None, 0, fh.ctypes.data_as(_I))
+    dev = torch.device("cuda:0")
+    ld = ncell + pad
+    if layout == 0:
+        a = np.zeros((net.nspec, ld))
+        a[:, :ncell] = v.T
+    else:
+        a = v.copy()
+    t = lambda z: torch.tensor(np.ascontiguousarray(z), device=dev)
+    da, dref = t(a), t(tot)
+    dfl = torch.zeros(ncell, dtype=torch.int32, device=dev)
+    rd = dev_fn(ncell, da.data_ptr(), layout, ld if layout == 0 else 0,
+                dref.data_ptr(), nelem, None, 0, dfl.data_ptr())
+    out = da.cpu().numpy()
+    vd = out[:, :ncell].T if layout == 0 else out
+    assert rd == rh
+    np.testing.assert_array_equal(dfl.cpu().numpy(), fh)
+    np.testing.assert_allclose(vd, vh, rtol=1e-13, atol=1e-300)
+    if layout == 0 and pad:
+        assert (out[:, ncell:] == 0).all()
+    # without flags: the same return value
+    da2 = t(a)
+    assert dev_fn(ncell, da2.data_ptr(), layout, ld if layout == 0 else 0,
+                  dref.data_ptr(), nelem, None, 0, None) == rh

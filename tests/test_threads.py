@@ -2,9 +2,11 @@
 called from several host threads, runtime/core/solve_kokkos.hpp:1223-1241;
 one options handle, only read, serves concurrent calls,
 runtime/interfaces/C/krome.cpp:407-409). Each thread's results must equal
-the same solve made alone, bit for bit."""
+the same solve made alone, bit for bit, and calls from several threads
+overlap on the GPU: each takes its own staging buffer and stream."""
 import ctypes
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -73,3 +75,34 @@ def test_concurrent_callers_equal_serial_calls(key):
         np.testing.assert_array_equal(got[1], want[1])
         np.testing.assert_array_equal(got[2], want[2])
         np.testing.assert_array_equal(got[3], want[3])
+
+
+@pytest.mark.gpu
+def test_concurrent_callers_overlap():
+    """four threads' calls (2,048 cells each: a batch that leaves most SMs
+    idle) finish in well under the time of the same four calls in a row"""
+    key = "primordial3"
+    net = krome.load(key)
+    opts = net.options(**workloads.OPTIONS[key])
+    cases = _cases(key, 4, 2048)
+    for c in cases:  # warm-up: the slots' buffers and streams exist
+        _raw_solve(net, opts, c)
+    t0 = time.perf_counter()
+    serial = [_raw_solve(net, opts, c) for c in cases]
+    t_serial = time.perf_counter() - t0
+    out = [None] * len(cases)
+
+    def work(t):
+        out[t] = _raw_solve(net, opts, cases[t])
+
+    threads = [threading.Thread(target=work, args=(t,)) for t in range(len(cases))]
+    t0 = time.perf_counter()
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(timeout=300)
+    t_conc = time.perf_counter() - t0
+    assert not any(th.is_alive() for th in threads)
+    for got, want in zip(out, serial):
+        np.testing.assert_array_equal(got[2], want[2])
+    assert t_conc < 0.75 * t_serial, (t_conc, t_serial)
