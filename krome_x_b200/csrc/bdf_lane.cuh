@@ -166,7 +166,10 @@ struct LaneCell {
 // the N-vector helpers' loops unrolled (each helper's loads issue together:
 // one memory latency per helper instead of one per element; 3 % on the
 // primordial3 hydro calls), the dense LU's loops as the other control loops
-// (unrolled, the LU's code crowds the rhs out of the instruction cache)
+// (measured on the B200: the LU unrolled, or restructured to load whole
+// columns at a time, ran the hydro calls 5-15 % slower -- its code crowds
+// the rhs out of the instruction cache -- and staging the Nordsieck rows of
+// the step helpers in registers spilled 15 KB per lane)
 #ifndef KBL_VLOOP
 #define KBL_VLOOP _Pragma("unroll")
 #endif
@@ -248,116 +251,57 @@ __device__ KBL_VEC double wrms_(const double* x, const double* w) {
   return ssqrt_(sum / N);
 }
 
-// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457): the
-// reference's operations in its order. R is the factors' type: double, or
-// float for the FP32 Newton-matrix form (the factorisation's arithmetic in
-// float; the solve's right-hand side and its accumulation stay double).
-//
-// Memory layout of the work. The factors live in the lane's local memory,
-// whose misses cost an L2 round trip; written as plain loops, every element
-// step would wait for one (the reference's loop nest: ~400 dependent steps
-// per factorisation). Here each pivot step touches whole columns at a time:
-// a column is loaded into registers with all its loads in flight (the
-// element loops unrolled over the compile-time N, rows outside the step
-// masked by predicates), so a factorisation waits for ~65 round trips and a
-// solve for ~30; the pivot-step loops stay rolled to keep the code small
-// (it shares the instruction cache with the rhs).
-
-// v[k] for a runtime k (a select chain: v stays in registers)
-template <int N, class T>
-__device__ __forceinline__ T pick_(const T (&v)[N], int k) {
-  T r = v[0];
-  KB_UNROLL for (int i = 1; i < N; i++) if (i == k) r = v[i];
-  return r;
-}
-
+// dense LU with partial pivoting, column-major (bdf_cell.hpp:405-457). R is
+// the factors' type: double, or float for the FP32 Newton-matrix form (the
+// factorisation's arithmetic in float; the solve's right-hand side and its
+// accumulation stay double)
 template <int N, class R>
 __device__ KBL_HELPER int getrf_(R* a, int* p) {
   KBL_LULOOP for (int k = 0; k < N; k++) {
     R* col_k = a + k * N;
-    R c[N];
-    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
-    // the pivot: the first row of largest |a_ik|, i >= k
     int l = k;
-    R cl = pick_<N, R>(c, k);
-    KB_UNROLL for (int i = 1; i < N; i++)
-      if (i > k && fabs(c[i]) > fabs(cl)) {
-        l = i;
-        cl = c[i];
-      }
+    KBL_LULOOP for (int i = k + 1; i < N; i++)
+      if (fabs(col_k[i]) > fabs(col_k[l])) l = i;
     p[k] = l;
-    if (cl == R(0)) return k + 1;
+    if (col_k[l] == R(0)) return k + 1;
     if (l != k) {
-      // rows k and l swap in every column; in registers for column k
-      KB_UNROLL for (int j = 0; j < N; j++) {
-        R* cj = a + j * N;
-        const R t = cj[l];
-        cj[l] = cj[k];
-        cj[k] = t;
+      KBL_LULOOP for (int i = 0; i < N; i++) {
+        R* ci = a + i * N;
+        const R t = ci[l];
+        ci[l] = ci[k];
+        ci[k] = t;
       }
-      const R ck = pick_<N, R>(c, k);
-      KB_UNROLL for (int i = 0; i < N; i++) if (i == l) c[i] = ck;
     }
-    const R mult = R(1) / cl;
-    KB_UNROLL for (int i = 0; i < N; i++)
-      if (i > k) {
-        c[i] *= mult;
-        col_k[i] = c[i];
-      }
-    // the trailing columns: a_ij -= a_kj l_ik where a_kj != 0
+    const R mult = R(1) / col_k[k];
+    KBL_LULOOP for (int i = k + 1; i < N; i++) col_k[i] *= mult;
     KBL_LULOOP for (int j = k + 1; j < N; j++) {
       R* col_j = a + j * N;
-      R v[N];
-      KB_UNROLL for (int i = 0; i < N; i++) v[i] = col_j[i];
-      const R a_kj = pick_<N, R>(v, k);
+      const R a_kj = col_j[k];
       if (a_kj != R(0)) {
-        KB_UNROLL for (int i = 0; i < N; i++)
-          if (i > k) col_j[i] = v[i] - a_kj * c[i];
+        KBL_LULOOP for (int i = k + 1; i < N; i++) col_j[i] -= a_kj * col_k[i];
       }
     }
   }
   return 0;
 }
 template <int N, class R>
-__device__ KBL_HELPER void getrs_(const R* a, const int* p, double* bv) {
-  double b[N];
-  int pv[N];
-  KB_UNROLL for (int i = 0; i < N; i++) {
-    b[i] = bv[i];
-    pv[i] = p[i];
-  }
-  // the row interchanges, in order
+__device__ KBL_HELPER void getrs_(const R* a, const int* p, double* b) {
   KBL_LULOOP for (int k = 0; k < N; k++) {
-    const int pk = pick_<N, int>(pv, k);
-    if (pk != k) {
-      const double bk = pick_<N, double>(b, k), bp = pick_<N, double>(b, pk);
-      KB_UNROLL for (int i = 0; i < N; i++) {
-        if (i == k) b[i] = bp;
-        if (i == pk) b[i] = bk;
-      }
-    }
+    const int pk = p[k];
+    if (pk != k) { const double t = b[k]; b[k] = b[pk]; b[pk] = t; }
   }
-  // L y = b (unit diagonal), then U x = y
   KBL_LULOOP for (int k = 0; k < N - 1; k++) {
     const R* col_k = a + k * N;
-    R c[N];
-    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
-    const double bk = pick_<N, double>(b, k);
-    KB_UNROLL for (int i = 0; i < N; i++)
-      if (i > k) b[i] -= (double)c[i] * bk;
+    const double bk = b[k];
+    KBL_LULOOP for (int i = k + 1; i < N; i++) b[i] -= (double)col_k[i] * bk;
   }
   KBL_LULOOP for (int k = N - 1; k > 0; k--) {
     const R* col_k = a + k * N;
-    R c[N];
-    KB_UNROLL for (int i = 0; i < N; i++) c[i] = col_k[i];
-    const double bk = pick_<N, double>(b, k) / (double)pick_<N, R>(c, k);
-    KB_UNROLL for (int i = 0; i < N; i++) {
-      if (i == k) b[i] = bk;
-      if (i < k) b[i] -= (double)c[i] * bk;
-    }
+    b[k] /= (double)col_k[k];
+    const double bk = b[k];
+    KBL_LULOOP for (int i = 0; i < k; i++) b[i] -= (double)col_k[i] * bk;
   }
   b[0] /= (double)a[0];
-  KB_UNROLL for (int i = 0; i < N; i++) bv[i] = b[i];
 }
 
 template <int N, bool EVT, bool REC = false>
@@ -712,7 +656,9 @@ struct Machine {
     KBL_LOOP for (int j = 0; j < N; j++) {
       KB_UNROLL for (int i = 0; i < N; i++) {
         const int k = i + j * N;
-        double v = s.savedJ[k] * c;
+        // the product rounded on its own, as the reference's two passes
+        // (A = -gamma J, then the diagonal's + 1) round it
+        double v = __dmul_rn(s.savedJ[k], c);
         if (i == j) v += 1.0;
         s.A[k] = v;
       }

@@ -895,9 +895,18 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
   }
 #else
   if (h.layout == 1 || rio != nullptr) {  // lane per cell
-    const size_t lsmem =
-        sizeof(double) * kWarpsPerBlock * LaneGeo<EVT>::SMEM_DOUBLES;
-    const int threads = kWarpsPerBlock * 32;
+    // a persistent grid of a small batch spreads its warps over the SMs
+    // (blocks of as many warps as the batch fills on every SM, at least
+    // one): each SM then holds few lanes, whose state stays in its L1, and
+    // every SM takes part (4,096 cells in 4-warp blocks would run on 32 of
+    // the 148 SMs)
+    int warps = kWarpsPerBlock;
+    if (h.kernel != 0 && ncell > 0) {
+      const long fill = (long)ncell / (32L * num_sms());
+      warps = fill < 1 ? 1 : (fill < kWarpsPerBlock ? (int)fill : kWarpsPerBlock);
+    }
+    const size_t lsmem = sizeof(double) * warps * LaneGeo<EVT>::SMEM_DOUBLES;
+    const int threads = warps * 32;
     // register budget of the kernel: 2, 3 or 4 resident blocks per SM; the
     // adjoint's recording forward solve runs the 2-block build
     auto kern = rio != nullptr ? kb_lane_cells<EVT, 2, true>

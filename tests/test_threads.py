@@ -85,24 +85,27 @@ def test_concurrent_callers_overlap():
     net = krome.load(key)
     opts = net.options(**workloads.OPTIONS[key])
     cases = _cases(key, 4, 2048)
-    for c in cases:  # warm-up: the slots' buffers and streams exist
-        _raw_solve(net, opts, c)
-    t0 = time.perf_counter()
-    serial = [_raw_solve(net, opts, c) for c in cases]
-    t_serial = time.perf_counter() - t0
     out = [None] * len(cases)
 
     def work(t):
         out[t] = _raw_solve(net, opts, cases[t])
 
-    threads = [threading.Thread(target=work, args=(t,)) for t in range(len(cases))]
+    def concurrent():
+        threads = [threading.Thread(target=work, args=(t,))
+                   for t in range(len(cases))]
+        t0 = time.perf_counter()
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join(timeout=300)
+        assert not any(th.is_alive() for th in threads)
+        return time.perf_counter() - t0
+
+    concurrent()  # warm-up: four slots (staging buffer and stream) exist
     t0 = time.perf_counter()
-    for th in threads:
-        th.start()
-    for th in threads:
-        th.join(timeout=300)
-    t_conc = time.perf_counter() - t0
-    assert not any(th.is_alive() for th in threads)
+    serial = [_raw_solve(net, opts, c) for c in cases]
+    t_serial = time.perf_counter() - t0
+    t_conc = concurrent()
     for got, want in zip(out, serial):
         np.testing.assert_array_equal(got[2], want[2])
     assert t_conc < 0.75 * t_serial, (t_conc, t_serial)
