@@ -792,6 +792,13 @@ struct Cell {
       rates_fixed(T, yf, p, k0);
       rates_var(T, yf, p, k0);
       jac_stoich(yf, k0, sJ, N, 1);
+#ifndef KB_LARGE_NETWORK
+      if constexpr (KB_RATE_NDEP > 0) {  // the rate-derivative terms
+        double U[NSPEC * NAGG];
+        jac_dk(T, yf, p, k0, sJ, U, N, 1);
+        jac_agg_(sJ, U, N, 1);
+      }
+#endif
     }
     if (!EVT) {
       __syncwarp();

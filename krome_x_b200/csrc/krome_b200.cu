@@ -488,8 +488,20 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
         }
         // the hybrid Jacobian's base-state lane: the stoichiometric block
         // with the rates of the base state (jacobian_split)
-        if (pass > 0 && !dq && role == LaneGeo<EVT>::ROLE_BASE)
-          jac_stoich(yf, k, sw + (lane / JL) * (N * N + 2 * N), 1, N);
+        if (pass > 0 && !dq && role == LaneGeo<EVT>::ROLE_BASE) {
+          double* J = sw + (lane / JL) * (N * N + 2 * N);
+          jac_stoich(yf, k, J, 1, N);
+#ifndef KB_LARGE_NETWORK
+          if constexpr (KB_RATE_NDEP > 0) {
+            // the rate-derivative terms at the base state's rate
+            // temperature, then the aggregates' coupling U W^T
+            double U[NSPEC * NAGG];
+            const double Tr = fmin(fmax(EVT ? yf[N - 1] : Tfix, p.Tcmb), 1e9);
+            jac_dk(Tr, yf, p, k, J, U, 1, N);
+            jac_agg_(J, U, 1, N);
+          }
+#endif
+        }
       }
       // ---- results ----
       if (pass == 0) {
@@ -763,22 +775,12 @@ struct SlotLease {
   }
 };
 
-// the rates that depend on the densities (their dk/dn terms are not in
-// the small networks' analytic Jacobian; the large networks' path takes no
-// jac option)
-#ifdef KB_LARGE_NETWORK
-constexpr int kRateNdep = 0;
-#else
-constexpr int kRateNdep = kbnet::KB_RATE_NDEP;
-#endif
-
 int resolved_jac(const krome_opts& h) {
   if (h.jac == 1) return 1;
   if (h.jac == 2) return 2;
-  // JAC_AUTO (solve_cell.hpp:2141-2142); the difference quotients also
-  // where rates depend on the densities (the analytic Jacobian here has no
-  // dk/dn terms: unsupported() refuses it there)
-  return (h.evolve_T || kRateNdep > 0) ? 2 : 1;
+  // JAC_AUTO (solve_cell.hpp:2141-2142): analytic at fixed Tgas, the
+  // difference quotients when Tgas evolves
+  return h.evolve_T ? 2 : 1;
 }
 
 SolveOpts to_solve_opts(const krome_opts& h) {
@@ -1239,7 +1241,6 @@ int unsupported(const krome_opts& h) {
   if (h.evolve_T != 0 || h.lu32 != 0) return -104;
 #else
   if (h.linsol == 2 || h.linsol == 3) return -104;
-  if (h.jac == 1 && kRateNdep > 0) return -104;
   if (h.lu32 != 0 && h.layout != 1) return -104;
 #endif
   return 0;

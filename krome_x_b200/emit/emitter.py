@@ -409,6 +409,7 @@ class Emitter:
     def emit_physics(self):
         self.w('#include "../csrc/kb_physics.h"')
         self.w('#include "../csrc/kb_conserve.h"')
+        self.w('#include "../csrc/kb_jacdk.h"')
         self.w("")
 
     def emit_vars(self):
@@ -574,6 +575,52 @@ class Emitter:
                     w("  J[IDX_%s*rs + %s*cs] -= d;" % (self.cid(r["sp"]), col))
                 for pr in rx["products"]:
                     w("  J[IDX_%s*rs + %s*cs] += d;" % (self.cid(pr["sp"]), col))
+        w("}")
+        w("")
+
+    def emit_jac_dk(self):
+        """the analytic Jacobian's rate-derivative part: d k_r / d n_j prod n
+        into J and d k_r / d aggregate prod n into U (J += U W^T after), in
+        the reference's jacobian_split form (kromex/codegen.py:8462-8560):
+        the derivative expressions and J / U updates are the reference
+        generator's own rendering (jac_dk_lines), gated by the same
+        piecewise selection as the rates; a rate that calls a fitted
+        function is re-evaluated (rate_<r>) for difference quotients"""
+        w, gen = self.w, self.gen
+        for rx in self.net.reactions:
+            if rx["rate"]["kind"] != "expr" or not gen.has_extern(rx["rate"]["ast"]):
+                continue
+            # the rate function the difference quotients call: Tgas the
+            # (group-clamped) rate temperature, Tg_ the gas temperature
+            w("// %s" % rx["eq"])
+            w("KB_HD inline double rate_%d(double Tgas, const double* n, "
+              "const Params& p, double Tg_) {" % (rx["id"] - 1))
+            w("  (void)Tgas; (void)n; (void)p; (void)Tg_;")
+            gen._hoisted = {}
+            gen._in_ratefn = True
+            try:
+                w("  return %s;" % gen.cexpr(rx["rate"]["ast"])
+                  .replace("constants::", "kbc::"))
+            finally:
+                gen._in_ratefn = False
+            w("}")
+        w("// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + "
+          "j*cs], added to;")
+        w("// U[NSPEC][NAGG] written), gated and clamped like the rates")
+        w("KB_HD inline void jac_dk(double Tgas, const double* n, "
+          "const Params& p, const double* k, double* J, double* U, "
+          "long jrs_, long jcs_) {")
+        w("  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; "
+          "(void)jcs_;")
+        w("  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;")
+        w("  double d;")
+        w("  (void)d;")
+        def body(rx, tv):
+            gen._hoisted = {}
+            gen._in_ratefn = False
+            return [ln.replace("constants::", "kbc::")
+                    for ln in gen.jac_dk_lines(rx, tv)]
+        self.emit_grouped(body, lambda rx: True, hoist=False)
         w("}")
         w("")
 
@@ -1858,6 +1905,8 @@ class Emitter:
         self.emit_rates()
         self.emit_rhs()
         self.emit_jac()
+        if len(self.species) <= LARGE_NSPEC:
+            self.emit_jac_dk()
         self.emit_thermal()
         self.emit_lnk_vjp()
         self.emit_interface()

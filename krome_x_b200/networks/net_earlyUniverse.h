@@ -148,6 +148,7 @@ KB_HD inline int frozen_species(const Params& p, int* idx) {
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
+#include "../csrc/kb_jacdk.h"
 
 KB_HD inline double v_invTgas(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -1219,6 +1220,191 @@ KB_HD inline void jac_stoich(const double* n, const double* k, double* J, int rs
   J[IDX_H*rs + IDX_H2Dj*cs] -= d;
   J[IDX_H3j*rs + IDX_H2Dj*cs] += d;
   J[IDX_D*rs + IDX_H2Dj*cs] += d;
+}
+
+// H+ + e- -> H
+KB_HD inline double rate_0(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_H_rec(n[IDX_H], Tgas, n, p);
+}
+// H -> H+ + e-
+KB_HD inline double rate_1(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_H_ion(n[IDX_H], Tgas, n, p);
+}
+// He+ + e- -> He
+KB_HD inline double rate_25(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_He_rec(n[IDX_He], n[IDX_H], Tgas, n, p);
+}
+// He -> He+ + e-
+KB_HD inline double rate_26(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_He_ion(n[IDX_He], n[IDX_H], Tgas, n, p);
+}
+// D+ + e- -> D
+KB_HD inline double rate_39(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_H_rec(n[IDX_D], Tgas, n, p);
+}
+// D -> D+ + e-
+KB_HD inline double rate_40(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return recfast_H_ion(n[IDX_D], Tgas, n, p);
+}
+// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + j*cs], added to;
+// U[NSPEC][NAGG] written), gated and clamped like the rates
+KB_HD inline void jac_dk(double Tgas, const double* n, const Params& p, const double* k, double* J, double* U, long jrs_, long jcs_) {
+  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; (void)jcs_;
+  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;
+  double d;
+  (void)d;
+  { // numerical dk/dn: H+ + e- -> H (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_0(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_Hj]*n[IDX_E];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[0], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_Hj*jrs_ + jj*jcs_] -= d;
+      J[IDX_E*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: H -> H+ + e- (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_1(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_H];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[1], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_H*jrs_ + jj*jcs_] -= d;
+      J[IDX_Hj*jrs_ + jj*jcs_] += d;
+      J[IDX_E*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: He+ + e- -> He (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_25(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_Hej]*n[IDX_E];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[25], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_Hej*jrs_ + jj*jcs_] -= d;
+      J[IDX_E*jrs_ + jj*jcs_] -= d;
+      J[IDX_He*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: He -> He+ + e- (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_26(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_He];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[26], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_He*jrs_ + jj*jcs_] -= d;
+      J[IDX_Hej*jrs_ + jj*jcs_] += d;
+      J[IDX_E*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: D+ + e- -> D (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_39(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_Dj]*n[IDX_E];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[39], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_Dj*jrs_ + jj*jcs_] -= d;
+      J[IDX_E*jrs_ + jj*jcs_] -= d;
+      J[IDX_D*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: D -> D+ + e- (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_40(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_D];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[40], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_D*jrs_ + jj*jcs_] -= d;
+      J[IDX_Dj*jrs_ + jj*jcs_] += d;
+      J[IDX_E*jrs_ + jj*jcs_] += d;
+    }
+  }
+  {  // group 1: H- + H -> H2 + e-
+    double T = Tgas;
+    if (T < 300.0) {
+    }
+    else if (T >= 300.0) {
+    }
+  }
+  {  // group 2: H- + H+ -> H2+ + e-
+    double T = Tgas;
+    if (T < 8000.0) {
+    }
+    else if (T >= 8000.0) {
+    }
+  }
+  {  // group 3: H2 + H+ -> H2+ + H
+    double T = Tgas;
+    if (T < 10000.0) {
+    }
+    else if (T >= 10000.0) {
+    }
+  }
+  {  // group 4: He + H+ -> He+ + H
+    double T = Tgas;
+    if (T >= 10000.0 && T >= 10000.0) {
+    }
+  }
+  {  // group 5: He+ + H -> He + H+
+    double T = Tgas;
+    if (T >= 6000.0 && T >= 6000.0) {
+    }
+  }
+  {  // group 6: He + H+ -> HeH+
+    double T = Tgas;
+    if (T < 1000.0) {
+    }
+    else if (T >= 1000.0) {
+    }
+  }
+  {  // group 7: He+ + H -> HeH+
+    double T = Tgas;
+    if (T < 4000.0) {
+    }
+    else if (T >= 4000.0) {
+    }
+  }
+  {  // group 8: D + H2 -> H + HD
+    double T = Tgas;
+    if (T >= 250.0 && T >= 250.0) {
+    }
+  }
+  {  // group 9: HD + H -> H2 + D
+    double T = Tgas;
+    if (T >= 200.0 && T >= 200.0) {
+    }
+  }
+  {  // group 10: H2D+ + H2 -> H3+ + HD
+    double T = Tgas;
+    if (T < 100.0) {
+    }
+    else if (T >= 100.0) {
+    }
+  }
 }
 
 KB_HD inline double gamma_index(double Tgas, const double* n, const Params& p) {

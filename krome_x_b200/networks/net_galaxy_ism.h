@@ -127,6 +127,7 @@ KB_HD inline int params_missing(const Params& p) {
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
+#include "../csrc/kb_jacdk.h"
 
 KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -1149,6 +1150,128 @@ KB_HD inline void jac_stoich(const double* n, const double* k, double* J, int rs
   J[IDX_Hej*rs + IDX_E*cs] -= d;
   J[IDX_E*rs + IDX_E*cs] -= d;
   J[IDX_He*rs + IDX_E*cs] += d;
+}
+
+// H2 -> H + H
+KB_HD inline double rate_43(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return H2_solomonLW(v_myflux_eV(Tgas, n, p), Tgas, n, p);
+}
+// H+ + e- -> H
+KB_HD inline double rate_44(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return H_recombination_on_dust(Tgas, n, p);
+}
+// He+ + e- -> He
+KB_HD inline double rate_45(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return He_recombination_on_dust(Tgas, n, p);
+}
+// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + j*cs], added to;
+// U[NSPEC][NAGG] written), gated and clamped like the rates
+KB_HD inline void jac_dk(double Tgas, const double* n, const Params& p, const double* k, double* J, double* U, long jrs_, long jcs_) {
+  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; (void)jcs_;
+  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;
+  double d;
+  (void)d;
+  { // numerical dk/dn: H2 -> H + H (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_43(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_H2];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[43], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_H2*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: H+ + e- -> H (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_44(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_Hj]*n[IDX_E];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[44], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_Hj*jrs_ + jj*jcs_] -= d;
+      J[IDX_E*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+    }
+  }
+  { // numerical dk/dn: He+ + e- -> He (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_45(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_Hej]*n[IDX_E];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[45], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_Hej*jrs_ + jj*jcs_] -= d;
+      J[IDX_E*jrs_ + jj*jcs_] -= d;
+      J[IDX_He*jrs_ + jj*jcs_] += d;
+    }
+  }
+  {  // group 1: H+ + e- -> H
+    double T = Tgas;
+    if (T < 5500.0) {
+    }
+    else if (T >= 5500.0) {
+    }
+  }
+  {  // group 2: He+ + e- -> He
+    double T = Tgas;
+    if (T < 9284.0) {
+    }
+    else if (T >= 9284.0) {
+    }
+  }
+  {  // group 3: H + H+ -> H2+
+    double T = Tgas;
+    if (T < 30.0) {
+    }
+    else if (T >= 30.0) {
+    }
+  }
+  {  // group 4: H2 + H+ -> H2+ + H
+    double T = Tgas;
+    if (T > 100000000.0) T = 100000000.0;
+    if (T >= 100.0 && T >= 100.0 && T < 100000.0) {
+    }
+    else if (T >= 100000.0) {
+    }
+  }
+  {  // group 5: H- + H -> H + H + e-
+    double T = Tgas;
+    if (T < 1160.0) {
+    }
+    else if (T >= 1160.0) {
+    }
+  }
+  {  // group 6: H- + H+ -> H + H
+    double T = Tgas;
+    if (T > 10000000.0) T = 10000000.0;
+    if (T >= 10.0 && T >= 10.0) {
+    }
+  }
+  {  // group 7: H2+ + e- -> H + H
+    double T = Tgas;
+    if (T < 617.0) {
+    }
+    else if (T >= 617.0) {
+    }
+  }
+  {  // group 8: He + H+ -> He+ + H
+    double T = Tgas;
+    if (T < 10000.0) {
+    }
+    else if (T >= 10000.0) {
+    }
+  }
 }
 
 KB_HD inline double gamma_index(double Tgas, const double* n, const Params& p) {

@@ -116,6 +116,7 @@ KB_HD inline int params_missing(const Params& p) {
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
+#include "../csrc/kb_jacdk.h"
 
 KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -937,6 +938,98 @@ KB_HD inline void jac_stoich(const double* n, const double* k, double* J, int rs
   J[IDX_Dj*rs + IDX_E*cs] -= d;
   J[IDX_E*rs + IDX_E*cs] -= d;
   J[IDX_D*rs + IDX_E*cs] += d;
+}
+
+// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + j*cs], added to;
+// U[NSPEC][NAGG] written), gated and clamped like the rates
+KB_HD inline void jac_dk(double Tgas, const double* n, const Params& p, const double* k, double* J, double* U, long jrs_, long jcs_) {
+  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; (void)jcs_;
+  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;
+  double d;
+  (void)d;
+  {  // group 1: H+ + e- -> H
+    double T = Tgas;
+    if (T < 5500.0) {
+    }
+    else if (T >= 5500.0) {
+    }
+  }
+  {  // group 2: He+ + e- -> He
+    double T = Tgas;
+    if (T < 9280.0) {
+    }
+    else if (T >= 9280.0) {
+    }
+  }
+  {  // group 3: H- + H -> H2 + e-
+    double T = Tgas;
+    if (T < 1160.0) {
+    }
+    else if (T >= 1160.0) {
+    }
+  }
+  {  // group 4: H + H+ -> H2+
+    double T = Tgas;
+    if (T < 6700.0) {
+    }
+    else if (T >= 6700.0) {
+    }
+  }
+  {  // group 5: H2 + H+ -> H2+ + H
+    double T = Tgas;
+    if (T >= 3480.0 && T >= 3480.0) {
+    }
+  }
+  {  // group 6: H- + H -> H + H + e-
+    double T = Tgas;
+    if (T < 1160.0) {
+    }
+    else if (T >= 1160.0) {
+    }
+  }
+  {  // group 7: H2+ + e- -> H + H
+    double T = Tgas;
+    if (T < 617.0) {
+    }
+    else if (T >= 617.0) {
+    }
+  }
+  {  // group 8: H + H + H -> H2 + H
+    double T = Tgas;
+    if (T < 300.0) {
+    }
+    else if (T >= 300.0) {
+    }
+  }
+  {  // group 9: H2 + H + H -> H2 + H2
+    double T = Tgas;
+    if (T < 300.0) {
+    }
+    else if (T >= 300.0) {
+    }
+  }
+  {  // group 10: H+ + D -> H + D+
+    double T = Tgas;
+    if (T >= 50.0 && T >= 50.0) {
+    }
+  }
+  {  // group 11: H + D+ -> H+ + D
+    double T = Tgas;
+    if (T >= 50.0 && T >= 50.0) {
+    }
+  }
+  {  // group 12: H2 + D -> HD + H
+    double T = Tgas;
+    if (T < 2000.0) {
+    }
+    else if (T >= 2000.0) {
+    }
+  }
+  {  // group 13: HD + H -> H2 + D
+    double T = Tgas;
+    if (T >= 200.0 && T >= 200.0) {
+    }
+  }
 }
 
 KB_HD inline double heating_chem(double Tgas, const double* n, const double* k) {

@@ -111,6 +111,7 @@ KB_HD inline int params_missing(const Params& p) {
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
+#include "../csrc/kb_jacdk.h"
 
 KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -840,6 +841,88 @@ KB_HD inline void jac_stoich(const double* n, const double* k, double* J, int rs
   J[IDX_H*rs + IDX_H2*cs] += d;
   J[IDX_H*rs + IDX_H2*cs] += d;
   J[IDX_H2*rs + IDX_H2*cs] += d;
+}
+
+// H2 + H -> H + H + H
+KB_HD inline double rate_16(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return dissH2_Martin96(Tgas, n, p);
+}
+// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + j*cs], added to;
+// U[NSPEC][NAGG] written), gated and clamped like the rates
+KB_HD inline void jac_dk(double Tgas, const double* n, const Params& p, const double* k, double* J, double* U, long jrs_, long jcs_) {
+  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; (void)jcs_;
+  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;
+  double d;
+  (void)d;
+  { // numerical dk/dn: H2 + H -> H + H + H (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_16(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_H]*n[IDX_H2];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[16], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_H2*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+    }
+  }
+  d = (dpow_(v_kh21(Tgas, n, p), 1.0 - v_a21(Tgas, n, p), (8.125e-08 * dpow_(v_T(Tgas, n, p), -0.5, 0.0, -0.0) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) + 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)) * (1.0 - kb_exp(-6000.0 * v_invT(Tgas, n, p))) + 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * -(kb_exp(-6000.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)), -(-(1.0 / v_ncr21(Tgas, n, p) / ((1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)) * (1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)))))) * kb_pow(v_kl21(Tgas, n, p), v_a21(Tgas, n, p)) + kb_pow(v_kh21(Tgas, n, p), 1.0 - v_a21(Tgas, n, p)) * dpow_(v_kl21(Tgas, n, p), v_a21(Tgas, n, p), 1.18e-10 * kb_exp(-69500.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p), -(1.0 / v_ncr21(Tgas, n, p) / ((1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)) * (1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p))))))*n[IDX_H2]*n[IDX_H2];  // dk of H2 + H2 -> H + H + H2 wrt Hnuclei
+  U[IDX_H2*NAGG + 1] -= d;
+  U[IDX_H2*NAGG + 1] -= d;
+  U[IDX_H*NAGG + 1] += d;
+  U[IDX_H*NAGG + 1] += d;
+  U[IDX_H2*NAGG + 1] += d;
+  {  // group 1: H+ + e- -> H
+    double T = Tgas;
+    if (T < 5500.0) {
+    }
+    else if (T >= 5500.0) {
+    }
+  }
+  {  // group 2: He+ + e- -> He
+    double T = Tgas;
+    if (T < 9280.0) {
+    }
+    else if (T >= 9280.0) {
+    }
+  }
+  {  // group 3: H + H+ -> H2+
+    double T = Tgas;
+    if (T < 30.0) {
+    }
+    else if (T >= 30.0) {
+    }
+  }
+  {  // group 4: H2 + H+ -> H2+ + H
+    double T = Tgas;
+    if (T > 30000.0) T = 30000.0;
+    if (T >= 100.0 && T >= 100.0) {
+    }
+  }
+  {  // group 5: H- + H -> H + H + e-
+    double T = Tgas;
+    if (T < 1160.0) {
+    }
+    else if (T >= 1160.0) {
+    }
+  }
+  {  // group 6: H- + H+ -> H + H
+    double T = Tgas;
+    if (T > 100000.0) T = 100000.0;
+    if (T >= 10.0 && T >= 10.0) {
+    }
+  }
+  {  // group 7: H2+ + e- -> H + H
+    double T = Tgas;
+    if (T > 10000.0) T = 10000.0;
+    if (true) {
+    }
+  }
 }
 
 KB_HD inline double cooling_chem(const double* n, const double* k) {

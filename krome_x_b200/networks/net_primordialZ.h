@@ -144,6 +144,7 @@ KB_HD inline int params_missing(const Params& p) {
 
 #include "../csrc/kb_physics.h"
 #include "../csrc/kb_conserve.h"
+#include "../csrc/kb_jacdk.h"
 
 KB_HD inline double v_Te(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -1607,6 +1608,284 @@ KB_HD inline void jac_stoich(const double* n, const double* k, double* J, int rs
   J[IDX_E*rs + IDX_E*cs] -= d;
   J[IDX_C*rs + IDX_E*cs] += d;
   J[IDX_O*rs + IDX_E*cs] += d;
+}
+
+// H2 + H -> H + H + H
+KB_HD inline double rate_16(double Tgas, const double* n, const Params& p, double Tg_) {
+  (void)Tgas; (void)n; (void)p; (void)Tg_;
+  return dissH2_Martin96(Tgas, n, p);
+}
+// the rate-derivative part of the analytic Jacobian (J[i*jrs_ + j*cs], added to;
+// U[NSPEC][NAGG] written), gated and clamped like the rates
+KB_HD inline void jac_dk(double Tgas, const double* n, const Params& p, const double* k, double* J, double* U, long jrs_, long jcs_) {
+  (void)Tgas; (void)n; (void)p; (void)k; (void)J; (void)jrs_; (void)jcs_;
+  for (int i = 0; i < NSPEC * NAGG; ++i) U[i] = 0.0;
+  double d;
+  (void)d;
+  { // numerical dk/dn: H2 + H -> H + H + H (extern/table in rate, all species)
+    double np_[NSPEC];
+    for (int q = 0; q < NSPEC; ++q) np_[q] = n[q];
+    auto rf_ = [&](const double* x) { return rate_16(Tgas, x, p, Tgas); };
+    const double pr_ = n[IDX_H]*n[IDX_H2];
+    for (int jj = 0; jj < NSPEC; ++jj) {
+      const double dk_ = fd_dk_(rf_, np_, n, k[16], jj);
+      if (dk_ == 0.0) continue;
+      d = dk_ * pr_;
+      J[IDX_H2*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] -= d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+      J[IDX_H*jrs_ + jj*jcs_] += d;
+    }
+  }
+  d = (dpow_(v_kh21(Tgas, n, p), 1.0 - v_a21(Tgas, n, p), (8.125e-08 * dpow_(v_T(Tgas, n, p), -0.5, 0.0, -0.0) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) + 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)) * (1.0 - kb_exp(-6000.0 * v_invT(Tgas, n, p))) + 8.125e-08 * 1.0/(std::sqrt(v_T(Tgas, n, p))) * kb_exp(-52000.0 * v_invT(Tgas, n, p)) * -(kb_exp(-6000.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)), -(-(1.0 / v_ncr21(Tgas, n, p) / ((1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)) * (1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)))))) * kb_pow(v_kl21(Tgas, n, p), v_a21(Tgas, n, p)) + kb_pow(v_kh21(Tgas, n, p), 1.0 - v_a21(Tgas, n, p)) * dpow_(v_kl21(Tgas, n, p), v_a21(Tgas, n, p), 1.18e-10 * kb_exp(-69500.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p), -(1.0 / v_ncr21(Tgas, n, p) / ((1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p)) * (1.0 + Hnuclei_(n) / v_ncr21(Tgas, n, p))))))*n[IDX_H2]*n[IDX_H2];  // dk of H2 + H2 -> H + H + H2 wrt Hnuclei
+  U[IDX_H2*NAGG + 1] -= d;
+  U[IDX_H2*NAGG + 1] -= d;
+  U[IDX_H*NAGG + 1] += d;
+  U[IDX_H*NAGG + 1] += d;
+  U[IDX_H2*NAGG + 1] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_H]*n[IDX_Oj];  // dk of O+ + H -> H+ + O wrt ntot
+  U[IDX_Oj*NAGG + 0] -= d;
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_Hj*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 7e-10 * kb_exp(-232.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_Hj]*n[IDX_O];  // dk of H+ + O -> O+ + H wrt ntot
+  U[IDX_Hj*NAGG + 0] -= d;
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_Oj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_H2]*n[IDX_Oj];  // dk of O+ + H2 -> OH+ + H wrt ntot
+  U[IDX_Oj*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_OHj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_H2]*n[IDX_OHj];  // dk of OH+ + H2 -> H2O+ + H wrt ntot
+  U[IDX_OHj*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_H2Oj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_H2]*n[IDX_H2Oj];  // dk of H2O+ + H2 -> H3O+ + H wrt ntot
+  U[IDX_H2Oj*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_H3Oj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 2e-07 * dpow_(v_T32(Tgas, n, p), -0.5, 0.0, -0.0)))*n[IDX_H2Oj]*n[IDX_E];  // dk of H2O+ + e- -> O + H2 wrt ntot
+  U[IDX_H2Oj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_O*NAGG + 0] += d;
+  U[IDX_H2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 1.6e-07 * dpow_(v_T32(Tgas, n, p), -0.5, 0.0, -0.0)))*n[IDX_H2Oj]*n[IDX_E];  // dk of H2O+ + e- -> OH + H wrt ntot
+  U[IDX_H2Oj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 3.5e-07 * dpow_(v_T32(Tgas, n, p), -0.5, 0.0, -0.0)))*n[IDX_H3Oj]*n[IDX_E];  // dk of H3O+ + e- -> H2O + H wrt ntot
+  U[IDX_H3Oj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_H2O*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 9.9e-19 * dpow_(v_T32(Tgas, n, p), -0.38, 0.0, -0.0)))*n[IDX_H]*n[IDX_O];  // dk of O + H -> OH wrt ntot
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 3.43e-13 * kb_pow(v_T32(Tgas, n, p), 2.67) * kb_exp(-3160.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_H2]*n[IDX_O];  // dk of O + H2 -> OH + H wrt ntot
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 1.55e-12 * kb_pow(v_T32(Tgas, n, p), 1.6) * kb_exp(-1660.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_H2]*n[IDX_OH];  // dk of H2 + OH -> H2O + H wrt ntot
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_H2O*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 1.65e-12 * kb_pow(v_T32(Tgas, n, p), 1.14) * kb_exp(-50.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_OH]*n[IDX_OH];  // dk of OH + OH -> H2O + O wrt ntot
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_H2O*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_Hj]*n[IDX_OH];  // dk of H+ + OH -> OH+ + H wrt ntot
+  U[IDX_Hj*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_OHj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_Hj]*n[IDX_H2O];  // dk of H+ + H2O -> H2O+ + H wrt ntot
+  U[IDX_Hj*NAGG + 0] -= d;
+  U[IDX_H2O*NAGG + 0] -= d;
+  U[IDX_H2Oj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 7e-14 * kb_pow(v_T32(Tgas, n, p), 2.8) * kb_exp(-1950.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_H]*n[IDX_OH];  // dk of H + OH -> H2 + O wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 6.83e-12 * kb_pow(v_T32(Tgas, n, p), 1.6) * kb_exp(-9720.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_H]*n[IDX_H2O];  // dk of H + H2O -> OH + H2 wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_H2O*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  U[IDX_H2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_O]*n[IDX_O];  // dk of O + O -> O2 wrt ntot
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 4.34e-11 * dpow_(v_T32(Tgas, n, p), -0.5, 0.0, -0.0) * kb_exp(-30.0 * v_invT(Tgas, n, p)) + 4.34e-11 * 1.0/(std::sqrt(v_T32(Tgas, n, p))) * kb_exp(-30.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_O]*n[IDX_OH];  // dk of O + OH -> O2 + H wrt ntot
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 3.3e-10 * kb_exp(-8460.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_H]*n[IDX_O2];  // dk of H + O2 -> OH + O wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_Hj]*n[IDX_O2];  // dk of H+ + O2 -> O2+ + H wrt ntot
+  U[IDX_Hj*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] -= d;
+  U[IDX_O2j*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 1.95e-07 * dpow_(v_T32(Tgas, n, p), -0.7, 0.0, -0.0)))*n[IDX_O2j]*n[IDX_E];  // dk of O2+ + e- -> O + O wrt ntot
+  U[IDX_O2j*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_O*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_CH]*n[IDX_O];  // dk of O + CH -> CO + H wrt ntot
+  U[IDX_O*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] -= d;
+  U[IDX_CO*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_C]*n[IDX_OH];  // dk of C + OH -> CO + H wrt ntot
+  U[IDX_C*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_CO*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_C]*n[IDX_O2];  // dk of C + O2 -> CO + O wrt ntot
+  U[IDX_C*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] -= d;
+  U[IDX_CO*NAGG + 0] += d;
+  U[IDX_O*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_Cj]*n[IDX_O2];  // dk of C+ + O2 -> O+ + CO wrt ntot
+  U[IDX_Cj*NAGG + 0] -= d;
+  U[IDX_O2*NAGG + 0] -= d;
+  U[IDX_Oj*NAGG + 0] += d;
+  U[IDX_CO*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_CO]*n[IDX_OH];  // dk of OH + CO -> CO2 + H wrt ntot
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_CO*NAGG + 0] -= d;
+  U[IDX_CO2*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 4.4e-12 * dpow_(v_T32(Tgas, n, p), -0.61, 0.0, -0.0)))*n[IDX_Cj]*n[IDX_E];  // dk of C+ + e- -> C wrt ntot
+  U[IDX_Cj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_C*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_Cj]*n[IDX_OH];  // dk of C+ + OH -> CO+ + H wrt ntot
+  U[IDX_Cj*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] -= d;
+  U[IDX_COj*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_COj]*n[IDX_H];  // dk of CO+ + H -> H+ + CO wrt ntot
+  U[IDX_COj*NAGG + 0] -= d;
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_Hj*NAGG + 0] += d;
+  U[IDX_CO*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_C]*n[IDX_H];  // dk of C + H -> CH wrt ntot
+  U[IDX_C*NAGG + 0] -= d;
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 6.64e-10 * kb_exp(-11700.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_C]*n[IDX_H2];  // dk of C + H2 -> CH + H wrt ntot
+  U[IDX_C*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_CH]*n[IDX_H];  // dk of H + CH -> C + H2 wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] -= d;
+  U[IDX_C*NAGG + 0] += d;
+  U[IDX_H2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 2.38e-10 * kb_exp(-1760.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_CH]*n[IDX_H2];  // dk of H2 + CH -> CH2 + H wrt ntot
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] -= d;
+  U[IDX_CH2*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_CH2]*n[IDX_H];  // dk of H + CH2 -> CH + H2 wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_CH2*NAGG + 0] -= d;
+  U[IDX_CH*NAGG + 0] += d;
+  U[IDX_H2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 5.18e-11 * kb_pow(v_T32(Tgas, n, p), 0.17) * kb_exp(-6400.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_CH2]*n[IDX_H2];  // dk of H2 + CH2 -> CH3 + H wrt ntot
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_CH2*NAGG + 0] -= d;
+  U[IDX_CH3*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 1e-10 * kb_exp(-7600.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_CH3]*n[IDX_H];  // dk of H + CH3 -> CH2 + H2 wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_CH3*NAGG + 0] -= d;
+  U[IDX_CH2*NAGG + 0] += d;
+  U[IDX_H2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 6.86e-14 * kb_pow(v_T32(Tgas, n, p), 2.74) * kb_exp(-4740.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_CH3]*n[IDX_H2];  // dk of H2 + CH3 -> CH4 + H wrt ntot
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_CH3*NAGG + 0] -= d;
+  U[IDX_CH4*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 5.82e-13 * v_T32(Tgas, n, p)*v_T32(Tgas, n, p)*v_T32(Tgas, n, p) * kb_exp(-4045.0 * v_invT(Tgas, n, p)) * -0.0 * v_invT(Tgas, n, p)))*n[IDX_CH4]*n[IDX_H];  // dk of H + CH4 -> H2 + CH3 wrt ntot
+  U[IDX_H*NAGG + 0] -= d;
+  U[IDX_CH4*NAGG + 0] -= d;
+  U[IDX_H2*NAGG + 0] += d;
+  U[IDX_CH3*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 0.0))*n[IDX_C]*n[IDX_H2];  // dk of H2 + C -> CH2 wrt ntot
+  U[IDX_H2*NAGG + 0] -= d;
+  U[IDX_C*NAGG + 0] -= d;
+  U[IDX_CH2*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 6.5e-07 * dpow_(v_T32(Tgas, n, p), -0.5, 0.0, -0.0)))*n[IDX_H3Oj]*n[IDX_E];  // dk of H3O+ + e- -> OH + H + H wrt ntot
+  U[IDX_H3Oj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_OH*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  d = ((ntot_(n) > 100000000000000.0 ? 0.0 : 6.3e-09 * dpow_(v_T32(Tgas, n, p), -0.48, 0.0, -0.0)))*n[IDX_OHj]*n[IDX_E];  // dk of OH+ + e- -> O + H wrt ntot
+  U[IDX_OHj*NAGG + 0] -= d;
+  U[IDX_E*NAGG + 0] -= d;
+  U[IDX_O*NAGG + 0] += d;
+  U[IDX_H*NAGG + 0] += d;
+  {  // group 1: H+ + e- -> H
+    double T = Tgas;
+    if (T < 5500.0) {
+    }
+    else if (T >= 5500.0) {
+    }
+  }
+  {  // group 2: He+ + e- -> He
+    double T = Tgas;
+    if (T < 9280.0) {
+    }
+    else if (T >= 9280.0) {
+    }
+  }
+  {  // group 3: H + H+ -> H2+
+    double T = Tgas;
+    if (T < 30.0) {
+    }
+    else if (T >= 30.0) {
+    }
+  }
+  {  // group 4: H2 + H+ -> H2+ + H
+    double T = Tgas;
+    if (T > 30000.0) T = 30000.0;
+    if (T >= 100.0 && T >= 100.0) {
+    }
+  }
+  {  // group 5: H- + H -> H + H + e-
+    double T = Tgas;
+    if (T < 1160.0) {
+    }
+    else if (T >= 1160.0) {
+    }
+  }
+  {  // group 6: He + H+ -> He+ + H
+    double T = Tgas;
+    if (T < 10000.0) {
+    }
+    else if (T >= 10000.0) {
+    }
+  }
 }
 
 KB_HD inline double gamma_index(double Tgas, const double* n, const Params& p) {

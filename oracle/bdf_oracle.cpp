@@ -340,6 +340,13 @@ struct Problem {
     const double T = state_T(y);
     eval_rates(T, y, k0);
     jac_stoich(y, k0, J, 1, N);
+#ifndef KB_LARGE_NETWORK
+    if (KB_RATE_NDEP > 0) {  // jacobian_split's rate-derivative part, U W^T
+      double U[NSPEC * NAGG];
+      jac_dk(T, y, p, k0, J, U, 1, N);
+      jac_agg_(J, U, 1, N);
+    }
+#endif
     if (iT < 0) return 0;
     for (int i = 0; i < N; ++i) yp[i] = y[i];
     {
@@ -1368,17 +1375,9 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
     rvec.assign(N, so->rtol);
     for (int i = 0; i < NSPEC; ++i) rvec[i] = tol(so->rtol_sp, i, so->rtol);
   }
-  // JAC_AUTO (solve_cell.hpp:2141-2142), the difference quotients also
-  // where rates depend on the densities: this analytic Jacobian has no
-  // dk/dn terms, so it is refused there (-104) like the library does
-#ifdef KB_LARGE_NETWORK
-  constexpr int rate_ndep = 0;
-#else
-  constexpr int rate_ndep = KB_RATE_NDEP;
-#endif
-  const int jac = so->jac != 0 ? so->jac
-                : ((so->evolve_T || rate_ndep > 0) ? 2 : 1);
-  if (jac == 1 && rate_ndep > 0) return -104;
+  // JAC_AUTO (solve_cell.hpp:2141-2142): analytic at fixed Tgas, the
+  // difference quotients when Tgas evolves
+  const int jac = so->jac != 0 ? so->jac : (so->evolve_T ? 2 : 1);
   BdfOpts bo;
   bo.rtol = so->rtol;
   bo.atol = avec.data();

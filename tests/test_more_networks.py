@@ -4,12 +4,11 @@ reactions, fixed Tgas), solved by the small-network kernels.
 
 Its rates depend on the densities (the metal reactions switch off above
 ntot = 1e14, the H2 dissociation rates depend on the H nuclei density):
-the reference's analytic Jacobian adds their dk/dn terms
-(kromex/codegen.py:8462-8560), which the emitted analytic Jacobian does
-not, so such networks take the difference-quotient Jacobian (the default
-resolves to it; an explicit analytic one is refused with -104). With it the
-oracle equals the reference's build bit for bit, and the kernels match the
-oracle.
+the analytic Jacobian adds their dk/dn terms as the reference's does
+(kromex/codegen.py:8462-8560: symbolic derivatives, difference quotients
+of rates that call fitted functions, the aggregates' coupling U W^T).
+With either Jacobian the oracle equals the reference's build bit for bit,
+and the kernels match the oracle.
 
 earlyUniverse (networks/earlyUniverse.knet, default thermal options, 16
 species, fixed Tgas) adds the RECFAST recombination rates (csrc/
@@ -64,16 +63,26 @@ def test_oracle_equals_the_reference(key):
     np.testing.assert_array_equal(out["T"], ref["T"])
 
 
-def test_oracle_refuses_the_analytic_jacobian_with_rate_terms():
-    info = netinfo.load(KEY)
-    n, T, dt, par = workloads.GENERATORS[KEY](4, info, seed=62)
-    o = dict(workloads.OPTIONS[KEY], jac=1)
-    out = Oracle(KEY).solve(n, T, dt, par, **o)
-    assert (out["flags"] == -104).all()
-    # the default resolves to the difference quotients: the same solve
-    a = Oracle(KEY).solve(n, T, dt, par, **dict(o, jac=0))
-    b = Oracle(KEY).solve(n, T, dt, par, **dict(o, jac=2))
-    np.testing.assert_array_equal(a["n"], b["n"])
+# the analytic Jacobian on networks whose rates depend on the densities
+# (explicit, and JAC_AUTO at fixed Tgas: solve_cell.hpp:2141-2142)
+ANALYTIC = [("primordial3", {"jac": 1}), ("galaxy_ism", {"jac": 1}),
+            (KEY, {"jac": 1}), (KEY, {"jac": 0}), ("earlyUniverse", {"jac": 0})]
+
+
+@pytest.mark.parametrize("key,extra", ANALYTIC,
+                         ids=["%s-jac%d" % (k, e["jac"]) for k, e in ANALYTIC])
+def test_analytic_jacobian_with_rate_terms_equals_the_reference(key, extra):
+    if not (ROOT / "oracle" / "_ref" / ("libkrome_%s_strict.so" % key)).exists():
+        pytest.skip("oracle/_ref not built here (oracle/build_ref.py)")
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](24, info, seed=91)
+    o = dict(workloads.OPTIONS[key], **extra)
+    ref = reference_solve(key, n, T, dt, par, strict=True, **o)
+    out = Oracle(key).solve(n, T, dt, par, **o)
+    assert (ref["flags"] == 0).all()
+    np.testing.assert_array_equal(out["flags"], ref["flags"])
+    np.testing.assert_array_equal(out["n"], ref["n"])
+    np.testing.assert_array_equal(out["T"], ref["T"])
 
 
 def _frozen_case(ncell, seed):
@@ -174,13 +183,22 @@ def test_gpu_matches_the_oracle(key, extra, layout):
 
 
 @pytest.mark.gpu
-def test_gpu_refuses_the_analytic_jacobian_with_rate_terms():
-    info = netinfo.load(KEY)
-    n, T, dt, par = workloads.GENERATORS[KEY](8, info, seed=65)
-    net = krome.load(KEY)
-    opts = net.options(**dict(workloads.OPTIONS[KEY], jac=1))
-    r = net.solve_batch(n, T, dt, par, opts=opts, check=False)
-    assert r.ierr == -104 and (r.flags == -104).all()
+@pytest.mark.parametrize("key,extra", ANALYTIC,
+                         ids=["%s-jac%d" % (k, e["jac"]) for k, e in ANALYTIC])
+@pytest.mark.parametrize("layout", ["lane", "warp"])
+def test_gpu_analytic_jacobian_with_rate_terms_matches_the_oracle(key, extra,
+                                                                  layout):
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](256, info, seed=65)
+    o = dict(workloads.OPTIONS[key], **extra)
+    ref = Oracle(key).solve(n, T, dt, par, **o)
+    net = krome.load(key)
+    opts = net.options(**dict(o, layout=0 if layout == "warp" else 1))
+    r = net.solve_batch(n, T, dt, par, opts=opts, check=False, stats=True)
+    m = parity(r.n, r.Tgas, r.flags, ref["n"], ref["T"], ref["flags"], o["rtol"])
+    assert m["flags_equal"] == 1.0 and m["frac"] >= 0.85, m
+    g, c = r.stats[:, 0].mean(), ref["stats"][:, 0].mean()
+    assert abs(g - c) <= 0.03 * c + 0.5, (g, c)
 
 
 @pytest.mark.gpu
