@@ -405,12 +405,35 @@ def adjoint_form(torch, dev, reps=3, cpu=True):
         if best is None or r[1] + r[2] < best[1] + best[2]:
             best = r
     plain, rec, rev, failed = best
+    # the memory-bounded form: tapes of 4 GB at most (chunks of cells
+    # recorded through one buffer, recomputed in the backward)
+    budget = 4 * 2 ** 30
+    n0, T0 = t(n).requires_grad_(), t(T).requires_grad_()
+    m = torch.zeros(net.nrea, dtype=torch.float64, device=dev,
+                    requires_grad=True)
+    torch.cuda.synchronize()
+    e0 = _events(torch)
+    nout, Tout, flags = autograd.solve(net, n0, T0, m, t(dt), t(par), opts,
+                                       max_tape_bytes=budget)
+    e1 = _events(torch)
+    loss = (nout[:, sp.index("H2")] / nH).sum() + Tout.sum()
+    e2 = _events(torch)
+    loss.backward()
+    e3 = _events(torch)
+    torch.cuda.synchronize()
+    bounded = {"tape_bytes_max": budget,
+               "forward_ms": e0.elapsed_time(e1),
+               "backward_ms": e2.elapsed_time(e3),
+               "gradient_over_forward":
+                   (e0.elapsed_time(e1) + e2.elapsed_time(e3)) / plain}
     out = {"workload": "primordial, 65,536 cells, rtol 1e-6, outputs x_H2 "
                        "and Tgas, inputs n0, T0 and all %d ln k" % net.nrea,
            "plain_forward_ms": plain, "recording_forward_ms": rec,
            "reverse_sweep_ms": rev, "reverse_over_forward": rev / plain,
            "gradient_over_forward": (rec + rev) / plain,
-           "failed_cells": failed, "reps": reps}
+           "failed_cells": failed, "reps": reps,
+           "memory_bounded": bounded,
+           "full_tape_bytes": N * autograd.DEFAULT_TAPE_CAP * 8}
     if cpu:
         # the reference has no adjoint: its gradient is central differences,
         # 2 (nspec + 1 + nrea) forward solves per cell

@@ -16,6 +16,15 @@ current torch stream. A cell that fails (flags != 0, including -120 when
 its tape outgrows tape_cap doubles) gets zero gradients and keeps its
 inputs. The gradients are those of the discrete solution: the step sizes,
 orders and Newton decisions of the forward solve are held fixed.
+
+Memory. The tapes take N x tape_cap doubles (256 KB per cell by default:
+17 GB for 65,536 cells). With max_tape_bytes set below that, the solve
+keeps no tape: the forward records cell chunks of max_tape_bytes / (8
+tape_cap) cells through one reused buffer and keeps only the results, and
+the backward recomputes each chunk's tape from the stored initial state --
+the one checkpoint a cell needs, as every cell is independent -- before its
+reverse sweep. The results and gradients are the same bit for bit; the
+cost is one more recording solve (~3.4 forward solves against ~2.5).
 """
 import torch
 
@@ -85,10 +94,111 @@ class _Solve(torch.autograd.Function):
         return dn0, dT0, dlnm, None, None, None, None, None
 
 
-def solve(net, n0, T0, lnm, dt, par, opts=None, tape_cap=DEFAULT_TAPE_CAP):
-    """(n, Tgas, flags) after dt, differentiable in n0, T0 and lnm"""
+def _record(net, opts, n, T, dtv, P, pstride, mult, mstride, flags, cursor,
+            tape, cap, tlen, yfin, c0, c1):
+    """the recording solve of cells [c0, c1) (rows of the per-cell arrays;
+    broadcast par / mult rows stay whole), in place in n and T"""
+    stream = torch.cuda.current_stream(n.device).cuda_stream
+    neq = yfin.numel() // max(int(n.shape[0]), 1) if c1 > c0 else 0
+    r = net._lib.krome_b200_adjoint_record_device(
+        c1 - c0, n[c0:c1].data_ptr(), T[c0:c1].data_ptr(),
+        dtv[c0:c1].data_ptr(), P[c0:c1].data_ptr() if pstride else P.data_ptr(),
+        pstride, mult[c0:c1].data_ptr() if mstride else mult.data_ptr(),
+        mstride, flags[c0:c1].data_ptr(), None, cursor.data_ptr(),
+        tape.data_ptr(), cap, tlen[c0:c1].data_ptr(),
+        yfin[c0 * neq:c1 * neq].data_ptr(), opts._h, stream)
+    if r != 0:
+        raise krome.KromeError("adjoint forward: %d (%s)"
+                               % (r, net.flag_message(r)))
+
+
+class _SolveChunked(torch.autograd.Function):
+    """the same solve and gradients without keeping the tapes: chunks of
+    `chunk` cells recorded through one buffer, recomputed in the backward"""
+
+    @staticmethod
+    def forward(ctx, n0, T0, lnm, dt, par, net, opts, tape_cap, chunk):
+        N = int(n0.shape[0])
+        neq = net.nspec + (1 if opts["evolve_T"] else 0)
+        dev = n0.device
+        n = n0.detach().to(torch.float64).contiguous().clone()
+        T = T0.detach().to(torch.float64).contiguous().clone()
+        n0c, T0c = n.clone(), T.clone()
+        dtv = dt.detach().to(torch.float64).contiguous()
+        P = par.detach().to(torch.float64).contiguous()
+        pstride = 0 if P.numel() == net.npar else net.npar
+        if pstride:
+            P = P.reshape(N, net.npar)
+        mult = lnm.detach().to(torch.float64).exp().contiguous()
+        mstride = 0 if mult.dim() == 1 else net.nrea
+        flags = torch.zeros(N, dtype=torch.int32, device=dev)
+        cursor = torch.zeros(1, dtype=torch.int32, device=dev)
+        tape = torch.empty(min(chunk, N) * tape_cap, dtype=torch.float64,
+                           device=dev)
+        tlen = torch.zeros(N, dtype=torch.int64, device=dev)
+        yfin = torch.empty(N * neq, dtype=torch.float64, device=dev)
+        for c0 in range(0, N, chunk):
+            _record(net, opts, n, T, dtv, P, pstride, mult, mstride, flags,
+                    cursor, tape, tape_cap, tlen, yfin, c0, min(N, c0 + chunk))
+        ctx.save_for_backward(n0c, T0c, dtv, P, mult, flags)
+        ctx.net, ctx.opts, ctx.cap, ctx.chunk = net, opts, tape_cap, chunk
+        ctx.pstride, ctx.mstride, ctx.neq = pstride, mstride, neq
+        ctx.mark_non_differentiable(flags)
+        return n, T, flags
+
+    @staticmethod
+    def backward(ctx, gn, gT, _gflags):
+        n0c, T0c, dtv, P, mult, flags = ctx.saved_tensors
+        net, cap, chunk, neq = ctx.net, ctx.cap, ctx.chunk, ctx.neq
+        N = int(T0c.shape[0])
+        dev = T0c.device
+        gn = (torch.zeros(N, net.nspec, dtype=torch.float64, device=dev)
+              if gn is None else gn.to(torch.float64).contiguous())
+        gT = (torch.zeros(N, dtype=torch.float64, device=dev)
+              if gT is None else gT.to(torch.float64).contiguous())
+        dn0 = torch.empty(N, net.nspec, dtype=torch.float64, device=dev)
+        dT0 = torch.empty(N, dtype=torch.float64, device=dev)
+        dm = torch.empty(N, net.nrea, dtype=torch.float64, device=dev)
+        n, T = n0c.clone(), T0c.clone()
+        fl = torch.zeros(N, dtype=torch.int32, device=dev)
+        cursor = torch.zeros(1, dtype=torch.int32, device=dev)
+        tape = torch.empty(min(chunk, N) * cap, dtype=torch.float64, device=dev)
+        tlen = torch.zeros(N, dtype=torch.int64, device=dev)
+        yfin = torch.empty(N * neq, dtype=torch.float64, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        ps, ms = ctx.pstride, ctx.mstride
+        for c0 in range(0, N, chunk):
+            c1 = min(N, c0 + chunk)
+            # the chunk's tapes again, from its initial state
+            _record(net, ctx.opts, n, T, dtv, P, ps, mult, ms, fl, cursor,
+                    tape, cap, tlen, yfin, c0, c1)
+            r = net._lib.krome_b200_adjoint_device(
+                c1 - c0, T0c[c0:c1].data_ptr(),
+                P[c0:c1].data_ptr() if ps else P.data_ptr(), ps,
+                mult[c0:c1].data_ptr() if ms else mult.data_ptr(), ms,
+                gn[c0:c1].data_ptr(), gT[c0:c1].data_ptr(),
+                fl[c0:c1].data_ptr(), tape.data_ptr(), cap,
+                tlen[c0:c1].data_ptr(), yfin[c0 * neq:c1 * neq].data_ptr(),
+                dn0[c0:c1].data_ptr(), dT0[c0:c1].data_ptr(),
+                dm[c0:c1].data_ptr(), cursor.data_ptr(), ctx.opts._h, stream)
+            if r != 0:
+                raise krome.KromeError("adjoint backward: %d" % r)
+        dlnm = dm if ms else dm.sum(0)
+        return dn0, dT0, dlnm, None, None, None, None, None, None
+
+
+def solve(net, n0, T0, lnm, dt, par, opts=None, tape_cap=DEFAULT_TAPE_CAP,
+          max_tape_bytes=None):
+    """(n, Tgas, flags) after dt, differentiable in n0, T0 and lnm;
+    max_tape_bytes bounds the device memory of the tapes (the backward then
+    recomputes them chunk by chunk)"""
     opts = net._options(opts)
     # the required-parameter rule, checked before any work
     row = par.detach().cpu().numpy().reshape(-1, net.npar)
     net._params(row if row.shape[0] > 1 else row[0], int(n0.shape[0]))
-    return _Solve.apply(n0, T0, lnm, dt, par, net, opts, int(tape_cap))
+    N = int(n0.shape[0])
+    cap = int(tape_cap)
+    if max_tape_bytes is not None and N * cap * 8 > max_tape_bytes:
+        chunk = max(1, int(max_tape_bytes) // (cap * 8))
+        return _SolveChunked.apply(n0, T0, lnm, dt, par, net, opts, cap, chunk)
+    return _Solve.apply(n0, T0, lnm, dt, par, net, opts, cap)

@@ -741,6 +741,65 @@ struct Slot {
   DevBuf buf;
   cudaStream_t stream = nullptr;
   int dev = -1;
+  // pinned staging for the caller's pageable host arrays: a copy from or to
+  // pageable memory goes through the driver's shared staging and blocks
+  // other threads' copies (and with them their kernels); from pinned memory
+  // each slot's copies run on its own stream
+  void* pin = nullptr;
+  size_t pin_cap = 0;
+  cudaError_t ensure_pin(size_t bytes) {
+    if (pin != nullptr && pin_cap >= bytes) return cudaSuccess;
+    if (pin != nullptr) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_cap = 0;
+    const cudaError_t e = cudaHostAlloc(&pin, bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) pin_cap = bytes;
+    return e;
+  }
+};
+
+// whether a host pointer is page-locked (pinned or registered) memory
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the error of an unknown pointer
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// a call's host<->device copies on its slot's stream: arrays in pinned
+// memory directly, pageable ones through the slot's pinned staging (in on
+// the way, out after the stream's synchronization: finish())
+struct Xfer {
+  Slot* slot;
+  cudaStream_t s;
+  size_t off = 0;
+  struct Out { void* dst; size_t at, bytes; };
+  std::vector<Out> outs;
+  char* pin(size_t at) { return static_cast<char*>(slot->pin) + at; }
+  size_t take(size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return at;
+  }
+  cudaError_t in(void* d, const void* h, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    if (host_pinned(h)) return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
+    const size_t at = take(bytes);
+    std::memcpy(pin(at), h, bytes);
+    return cudaMemcpyAsync(d, pin(at), bytes, cudaMemcpyHostToDevice, s);
+  }
+  cudaError_t out(void* h, const void* d, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    if (host_pinned(h)) return cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s);
+    const size_t at = take(bytes);
+    outs.push_back(Out{h, at, bytes});
+    return cudaMemcpyAsync(pin(at), d, bytes, cudaMemcpyDeviceToHost, s);
+  }
+  void finish() {  // after the stream's synchronization succeeded
+    for (const Out& o : outs) std::memcpy(o.dst, pin(o.at), o.bytes);
+  }
 };
 std::mutex g_slot_mu;
 std::vector<Slot*> g_idle;
@@ -1507,7 +1566,12 @@ int solve_host(int ncell, double* n, double* Tgas, const double* dt,
   const size_t total = al(nb) + 2 * al(tb) + al(pb) + al(fb) + al(sb)
                        + al(xb) + al(hb) + 256;
   SlotLease lease;
-  if (lease.s == nullptr || lease.s->buf.ensure(total) != cudaSuccess) {
+  // the staging the pageable arrays may need: in (n, Tgas, dt, par, Phi),
+  // out (n, Tgas, flags, stats)
+  const size_t stage = al(nb) + 2 * al(tb) + al(pb) + al(xb) + al(hb)
+                       + al(nb) + al(tb) + al(fb) + al(sb);
+  if (lease.s == nullptr || lease.s->buf.ensure(total) != cudaSuccess
+      || lease.s->ensure_pin(stage) != cudaSuccess) {
     if (flags != nullptr)
       for (int c = 0; c < ncell; ++c) flags[c] = -111;
     return -111;
@@ -1523,30 +1587,30 @@ int solve_host(int ncell, double* n, double* Tgas, const double* dt,
   double* dphi = reinterpret_cast<double*>(b); b += al(hb);
   unsigned* dcur = reinterpret_cast<unsigned*>(b);
   cudaStream_t s = lease.s->stream;
-  cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, Tgas, tb, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ddt, dt, tb, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, P, pb, cudaMemcpyHostToDevice, s);
+  Xfer x{lease.s, s};
+  cudaError_t e = x.in(dn, n, nb);
+  if (e == cudaSuccess) e = x.in(dT, Tgas, tb);
+  if (e == cudaSuccess) e = x.in(ddt, dt, tb);
+  if (e == cudaSuccess) e = x.in(dp, P, pb);
   PhotoArgs pa;
   if (B > 0) {
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(dxs, h->photo.sigma.data(), xb, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dphi, phi, hb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = x.in(dxs, h->photo.sigma.data(), xb);
+    if (e == cudaSuccess) e = x.in(dphi, phi, hb);
     pa = PhotoArgs{dxs, dphi, B};
   }
   if (e == cudaSuccess)
     e = launch_any(*h, ncell, dn, dT, ddt, dp, ps, dfl, dst, dcur, s, pa);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(n, dn, nb, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(Tgas, dT, tb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = x.out(n, dn, nb);
+  if (e == cudaSuccess) e = x.out(Tgas, dT, tb);
   int* hfl = flags != nullptr ? flags : fl.data();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(hfl, dfl, fb, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && sb)
-    e = cudaMemcpyAsync(stats, dst, sb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = x.out(hfl, dfl, fb);
+  if (e == cudaSuccess && sb) e = x.out(stats, dst, sb);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     std::fprintf(stderr, "krome_b200: CUDA error %s\n", cudaGetErrorString(e));
     return -104;
   }
+  x.finish();
   for (int c = 0; c < ncell; ++c)
     if (hfl[c] != 0) return hfl[c];
   return 0;

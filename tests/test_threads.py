@@ -109,3 +109,28 @@ def test_concurrent_callers_overlap():
     for got, want in zip(out, serial):
         np.testing.assert_array_equal(got[2], want[2])
     assert t_conc < 0.75 * t_serial, (t_conc, t_serial)
+
+
+@pytest.mark.gpu
+def test_pageable_and_pinned_host_arrays_solve_alike():
+    """krome_solve_cells on pageable arrays (staged through the call's
+    pinned buffer) and on pinned ones (copied directly): the same results"""
+    import torch
+    key = "primordial3"
+    net = krome.load(key)
+    opts = net.options(**workloads.OPTIONS[key])
+    case = _cases(key, 1, 1000)[0]
+    a = _raw_solve(net, opts, case)
+    pin = lambda v: torch.from_numpy(np.ascontiguousarray(v, dtype=float)) \
+        .pin_memory().numpy()
+    n, T, dt = (pin(v) for v in case[:3])
+    P, stride = net._params(case[3], n.shape[0])
+    P = pin(P)
+    flags = pin(np.zeros(n.shape[0])).astype(np.intc)
+    ierr = net._lib.krome_solve_cells(n.shape[0], _dp(n), _dp(T), _dp(dt),
+                                      _dp(P), stride, None,
+                                      flags.ctypes.data_as(_I), opts._h)
+    assert a[0] == ierr
+    np.testing.assert_array_equal(a[1], flags)
+    np.testing.assert_array_equal(a[2], n)
+    np.testing.assert_array_equal(a[3], T)
