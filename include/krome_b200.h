@@ -426,7 +426,8 @@ int krome_b200_adjoint(int ncell, double* n, double* Tgas, const double* dt,
  * the recording forward solve (mult = exp(lnm), rows [ncell][nrea] with
  * mult_stride nrea or one row with 0, NULL for none; tape[ncell][tape_cap];
  * tape_len[ncell] and yfin[ncell][neq] written for the reverse sweep;
- * n, Tgas updated in place as by krome_b200_solve_device) ... */
+ * n, Tgas updated in place as by krome_b200_solve_device; tape NULL: a
+ * counting solve, tape_len[c] the doubles cell c's tape needs) ... */
 int krome_b200_adjoint_record_device(int ncell, double* n, double* Tgas,
                                      const double* dt, const double* par,
                                      int par_stride, const double* mult,

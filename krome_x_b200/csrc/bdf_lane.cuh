@@ -311,14 +311,19 @@ struct Machine {
   __device__ Machine(LaneCell<N>& s_, const SolveOpts& o_) : s(s_), o(o_) {}
 
   // one tape record (REC only): [op, a (na >= 1), b (na == 2), l[] (with_l),
-  // v[N] (v non-null), length]
+  // v[N] (v non-null), length]; with no tape (tp null) only its length is
+  // counted
   __device__ void rec_(int op, int na, double a, double b, bool with_l,
                        const double* v) {
     if constexpr (REC) {
-      if (s.tp == nullptr || s.tlen < 0) return;
+      if (s.tlen < 0) return;
       const long len = 2 + na + (with_l ? L_MAX : 0) + (v != nullptr ? N : 0);
       if (s.tlen + len > s.tcap) {
         s.tlen = -1;
+        return;
+      }
+      if (s.tp == nullptr) {
+        s.tlen += len;
         return;
       }
       double* t = s.tp + s.tlen;
@@ -335,10 +340,14 @@ struct Machine {
   // the accepted step's corrector record
   __device__ void rec_correct_(int q) {
     if constexpr (REC) {
-      if (s.tp == nullptr || s.tlen < 0) return;
+      if (s.tlen < 0) return;
       const long len = 6 + L_MAX + N;
       if (s.tlen + len > s.tcap) {
         s.tlen = -1;
+        return;
+      }
+      if (s.tp == nullptr) {
+        s.tlen += len;
         return;
       }
       double* t = s.tp + s.tlen;

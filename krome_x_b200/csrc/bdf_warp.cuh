@@ -175,6 +175,21 @@ KB_HD inline void freeze_rows(const Params& p, double (&f)[N]) {
   (void)p; (void)f;
 #endif
 }
+#ifndef KB_LARGE_NETWORK
+// the analytic Jacobian's rate-derivative part (jac_dk, then the
+// aggregates' coupling U W^T) added to J (element (i, j) at i rs + j cs),
+// at the rate temperature T. Out of line: its scratch (U, the perturbed
+// state of the difference quotients) would otherwise raise the register
+// and stack budget of every kernel that can call it
+__device__ __noinline__ void jac_rate_terms(double T, const double* y,
+                                            const Params& p, const double* k,
+                                            double* J, long rs, long cs) {
+  double U[NSPEC * NAGG];
+  jac_dk(T, y, p, k, J, U, rs, cs);
+  jac_agg_(J, U, rs, cs);
+}
+#endif
+
 // J's element (i, j) at i rs + j cs
 template <int N>
 KB_HD inline void freeze_jac_rows(const Params& p, double* J, int rs, int cs) {
@@ -793,11 +808,8 @@ struct Cell {
       rates_var(T, yf, p, k0);
       jac_stoich(yf, k0, sJ, N, 1);
 #ifndef KB_LARGE_NETWORK
-      if constexpr (KB_RATE_NDEP > 0) {  // the rate-derivative terms
-        double U[NSPEC * NAGG];
-        jac_dk(T, yf, p, k0, sJ, U, N, 1);
-        jac_agg_(sJ, U, N, 1);
-      }
+      if constexpr (KB_RATE_NDEP > 0)  // the rate-derivative terms
+        jac_rate_terms(T, yf, p, k0, sJ, N, 1);
 #endif
     }
     if (!EVT) {

@@ -29,7 +29,7 @@ KB_HD inline double cool_sigmoid_(double x, double x0, double s) {
 
 KB_HD inline double wCool_(double logT, double logTmin, double logTmax) {
   const double x = (logT - logTmin) / (logTmax - logTmin);
-  const double w = kb_pow(10.0, 200.0 * (cool_sigmoid_(x, -0.2, 50.0)
+  const double w = kb_exp10(200.0 * (cool_sigmoid_(x, -0.2, 50.0)
                             * cool_sigmoid_(-x, -1.2, 50.0) - 1.0));
   return (w < 1e-199) ? 0.0 : w;
 }
@@ -88,15 +88,15 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 #ifdef KB_HAS_H
   double fH2H;
   if (temp <= 1e2)
-    fH2H = kb_pow(10.0, -16.818342 + 37.383713 * logt3
+    fH2H = kb_exp10(-16.818342 + 37.383713 * logt3
            + 58.145166 * logt32 + 48.656103 * logt33
            + 20.159831 * logt34 + 3.8479610 * logt35) * n[IDX_H];
   else if (temp <= 1e3)
-    fH2H = kb_pow(10.0, -24.311209 + 3.5692468 * logt3
+    fH2H = kb_exp10(-24.311209 + 3.5692468 * logt3
            - 11.332860 * logt32 - 27.850082 * logt33
            - 21.328264 * logt34 - 4.2519023 * logt35) * n[IDX_H];
   else if (temp <= 6e3)
-    fH2H = kb_pow(10.0, -24.311209 + 4.6450521 * logt3
+    fH2H = kb_exp10(-24.311209 + 4.6450521 * logt3
            - 3.7209846 * logt32 + 5.9369081 * logt33
            - 5.5108049 * logt34 + 1.5538288 * logt35) * n[IDX_H];
   else
@@ -107,26 +107,26 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 #ifdef KB_HAS_Hj
   double fH2Hp;
   if (temp > 1e1 && temp <= 1e4)
-    fH2Hp = kb_pow(10.0, -22.089523 + 1.5714711 * logt3
+    fH2Hp = kb_exp10(-22.089523 + 1.5714711 * logt3
             + 0.015391166 * logt32 - 0.23619985 * logt33
             - 0.51002221 * logt34 + 0.32168730 * logt35) * n[IDX_Hj];
   else
     fH2Hp = 1.182509139382060e-21 * n[IDX_Hj] * w14;
   cool += fH2Hp;
 #endif
-  cool += w24 * kb_pow(10.0, -23.962112 + 2.09433740 * logt3
+  cool += w24 * kb_exp10(-23.962112 + 2.09433740 * logt3
           - 0.77151436 * logt32 + 0.43693353 * logt33
           - 0.14913216 * logt34 - 0.033638326 * logt35) * n[IDX_H2];
 #ifdef KB_HAS_E
   double fH2e;
   if (temp <= 5e2)
-    fH2e = kb_pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+    fH2e = kb_exp10(std::fmin(-21.928796 + 16.815730 * logt3
            + 96.743155 * logt32 + 343.19180 * logt33
            + 734.71651 * logt34 + 983.67576 * logt35
            + 801.81247 * logt36 + 364.14446 * logt37
            + 70.609154 * logt38, 30.0)) * n[IDX_E];
   else
-    fH2e = kb_pow(10.0, -22.921189 + 1.6802758 * logt3
+    fH2e = kb_exp10(-22.921189 + 1.6802758 * logt3
            + 0.93310622 * logt32 + 4.0406627 * logt33
            - 4.7274036 * logt34 - 8.8077017 * logt35
            + 8.9167183 * logt36 + 6.4380698 * logt37
@@ -136,7 +136,7 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
 #ifdef KB_HAS_He
   double fH2He;
   if (temp > 1e1 && temp <= 1e4)
-    fH2He = kb_pow(10.0, -23.689237 + 2.1892372 * logt3
+    fH2He = kb_exp10(-23.689237 + 2.1892372 * logt3
             - 0.81520438 * logt32 + 0.29036281 * logt33
             - 0.16596184 * logt34 + 0.19191375 * logt35) * n[IDX_He];
   else
@@ -154,7 +154,7 @@ KB_HD inline double cooling_H2(double Tgas, const double* n) {
                         + 1.6e-18 * kb_exp(-11.7 / T3);
     HDL = HDLR + HDLV;
   } else if (temp <= 1e4) {
-    HDL = kb_pow(10.0, -20.584225 + 5.0194035 * logt3
+    HDL = kb_exp10(-20.584225 + 5.0194035 * logt3
           - 1.5738805 * logt32 - 4.7155769 * logt33
           + 2.4714161 * logt34 + 5.4710750 * logt35
           - 3.9467356 * logt36 - 2.2148338 * logt37
@@ -254,22 +254,22 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
   const double w24 = wCool_(logt, 2.0, 4.0);
   (void)w14; (void)logt36; (void)logt37; (void)logt38;
   if (temp <= 1e2)
-    q.aH = kb_pow(10.0, -16.818342 + 37.383713 * logt3
+    q.aH = kb_exp10(-16.818342 + 37.383713 * logt3
            + 58.145166 * logt32 + 48.656103 * logt33
            + 20.159831 * logt34 + 3.8479610 * logt35);
   else if (temp <= 1e3)
-    q.aH = kb_pow(10.0, -24.311209 + 3.5692468 * logt3
+    q.aH = kb_exp10(-24.311209 + 3.5692468 * logt3
            - 11.332860 * logt32 - 27.850082 * logt33
            - 21.328264 * logt34 - 4.2519023 * logt35);
   else if (temp <= 6e3)
-    q.aH = kb_pow(10.0, -24.311209 + 4.6450521 * logt3
+    q.aH = kb_exp10(-24.311209 + 4.6450521 * logt3
            - 3.7209846 * logt32 + 5.9369081 * logt33
            - 5.5108049 * logt34 + 1.5538288 * logt35);
   else
     q.aH = 1.862314467912518e-22 * wCool_(logt, 1.0, kb_log10(6e3));
   if (temp > 1e1 && temp <= 1e4) {
     q.fHp = 1;
-    q.aHp = kb_pow(10.0, -22.089523 + 1.5714711 * logt3
+    q.aHp = kb_exp10(-22.089523 + 1.5714711 * logt3
             + 0.015391166 * logt32 - 0.23619985 * logt33
             - 0.51002221 * logt34 + 0.32168730 * logt35);
   } else {
@@ -277,17 +277,17 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
     q.aHp = 1.182509139382060e-21;
     q.bHp = w14;
   }
-  q.aH2 = w24 * kb_pow(10.0, -23.962112 + 2.09433740 * logt3
+  q.aH2 = w24 * kb_exp10(-23.962112 + 2.09433740 * logt3
           - 0.77151436 * logt32 + 0.43693353 * logt33
           - 0.14913216 * logt34 - 0.033638326 * logt35);
   if (temp <= 5e2)
-    q.ae = kb_pow(10.0, std::fmin(-21.928796 + 16.815730 * logt3
+    q.ae = kb_exp10(std::fmin(-21.928796 + 16.815730 * logt3
            + 96.743155 * logt32 + 343.19180 * logt33
            + 734.71651 * logt34 + 983.67576 * logt35
            + 801.81247 * logt36 + 364.14446 * logt37
            + 70.609154 * logt38, 30.0));
   else
-    q.ae = kb_pow(10.0, -22.921189 + 1.6802758 * logt3
+    q.ae = kb_exp10(-22.921189 + 1.6802758 * logt3
            + 0.93310622 * logt32 + 4.0406627 * logt33
            - 4.7274036 * logt34 - 8.8077017 * logt35
            + 8.9167183 * logt36 + 6.4380698 * logt37
@@ -295,7 +295,7 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
   q.be = w24;
   if (temp > 1e1 && temp <= 1e4) {
     q.fHe = 1;
-    q.aHe = kb_pow(10.0, -23.689237 + 2.1892372 * logt3
+    q.aHe = kb_exp10(-23.689237 + 2.1892372 * logt3
             - 0.81520438 * logt32 + 0.29036281 * logt33
             - 0.16596184 * logt34 + 0.19191375 * logt35);
   } else {
@@ -312,7 +312,7 @@ KB_HD inline CoolH2C cooling_H2_coef(double Tgas) {
                         + 1.6e-18 * kb_exp(-11.7 / T3);
     q.HDL = HDLR + HDLV;
   } else if (temp <= 1e4) {
-    q.HDL = kb_pow(10.0, -20.584225 + 5.0194035 * logt3
+    q.HDL = kb_exp10(-20.584225 + 5.0194035 * logt3
           - 1.5738805 * logt32 - 4.7155769 * logt33
           + 2.4714161 * logt34 + 5.4710750 * logt35
           - 3.9467356 * logt36 - 2.2148338 * logt37
@@ -361,7 +361,7 @@ KB_HD inline double kpla_(const double* n) {
   const double rho = rho_(n);
   if (rho < 1e-12) return 0.0;
   const double y = kb_log10(std::fmin(rho, 0.5));
-  return kb_pow(10.0, 1.000042 * y + 2.14989);
+  return kb_exp10(1.000042 * y + 2.14989);
 }
 
 KB_HD inline double cooling_Continuum(double Tgas, const double* n) {
@@ -410,13 +410,13 @@ KB_UNROLL
     const double logn_c2 = c[17] + logn_c1;
     const double pp = c[18] + c[19] * kb_exp(-Tgas / 1.850e3)
         + c[20] * kb_exp(-Tgas / 4.40e2);
-    const double n_c1 = kb_pow(10.0, logn_c1);
-    const double n_c2 = kb_pow(10.0, logn_c2);
+    const double n_c1 = kb_exp10(logn_c1);
+    const double n_c2 = kb_exp10(logn_c2);
     const double logk_CID = logk_h1
         - (logk_h1 - logk_l1) / (1.0 + kb_pow(n_H / n_c1, pp))
         + logk_h2
         - (logk_h2 - logk_l2) / (1.0 + kb_pow(n_H / n_c2, pp));
-    k_CID += kb_pow(10.0, logk_CID);
+    k_CID += kb_exp10(logk_CID);
   }
   return k_CID;
 }
@@ -541,7 +541,7 @@ KB_HD inline double escape(double tau) {
 
 // the He I recombination fits (square-root terms shared by both)
 KB_HD inline double he_alpha(double s0, double s1, double lg, double e) {
-  return kb_pow(10.0, lg) / (s0 * kb_pow(1.0 + s0, 1.0 - e))
+  return kb_exp10(lg) / (s0 * kb_pow(1.0 + s0, 1.0 - e))
       / kb_pow(1.0 + s1, 1.0 + e);
 }
 
@@ -588,8 +588,8 @@ KB_HD inline Rates helium_triplet(const Common& c, double nH0, double nHe0,
 KB_HD inline void helium(double Tgas, double nH0, double nHe0,
                          const Params& p, Rates& s, Rates& t) {
   const Common c = common(Tgas, p);
-  const double s0 = std::sqrt(c.T / kb_pow(10.0, 0.477121));
-  const double s1 = std::sqrt(c.T / kb_pow(10.0, 5.114));
+  const double s0 = std::sqrt(c.T / kb_exp10(0.477121));
+  const double s1 = std::sqrt(c.T / kb_exp10(5.114));
   s = helium_singlet(c, nH0, nHe0, s0, s1);
   t = helium_triplet(c, nH0, nHe0, s0, s1);
 }

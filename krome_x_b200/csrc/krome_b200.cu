@@ -247,8 +247,9 @@ __device__ bool lane_start(kbl::LaneCell<LaneGeo<EVT>::N>& s,
   }
 #endif
   if constexpr (REC) {
-    s.tp = rio.tape + (long)c * rio.cap;
-    s.tcap = rio.cap;
+    // no tape: the lengths only (tape_len gets what the cell would need)
+    s.tp = rio.tape != nullptr ? rio.tape + (long)c * rio.cap : nullptr;
+    s.tcap = rio.tape != nullptr ? rio.cap : (1L << 62);
     s.tlen = 0;
   }
   s.cell = c;
@@ -495,10 +496,8 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
           if constexpr (KB_RATE_NDEP > 0) {
             // the rate-derivative terms at the base state's rate
             // temperature, then the aggregates' coupling U W^T
-            double U[NSPEC * NAGG];
             const double Tr = fmin(fmax(EVT ? yf[N - 1] : Tfix, p.Tcmb), 1e9);
-            jac_dk(Tr, yf, p, k, J, U, 1, N);
-            jac_agg_(J, U, 1, N);
+            kbw::jac_rate_terms(Tr, yf, p, k, J, 1, N);
           }
 #endif
         }
@@ -1347,9 +1346,10 @@ KB_API int krome_b200_adjoint_record_device(
   return -104;  // the adjoint is built for the small (dense) networks
 #else
   if (ncell == 0) return 0;
+  // tape NULL: a counting solve (tape_len the tape each cell needs)
   if (n == nullptr || Tgas == nullptr || dt == nullptr || par == nullptr
-      || flags == nullptr || tape == nullptr || tape_len == nullptr
-      || yfin == nullptr || tape_cap <= 0)
+      || flags == nullptr || tape_len == nullptr || yfin == nullptr
+      || (tape != nullptr && tape_cap <= 0))
     return -1;
   if (par_stride != 0 && par_stride != kbnet::NPAR) return -1;
   if (mult_stride != 0 && mult_stride != kbnet::NREA) return -1;

@@ -1921,7 +1921,8 @@ def outline_math(text):
     """route the special functions of the emitted code through kb_common.h's
     wrappers (out of line on the device: one copy of each math routine
     instead of one per call site)"""
-    return re.sub(r"(?<![\w:])(?:std::)?(exp|log10|log|pow)\(", r"kb_\1(", text)
+    text = re.sub(r"(?<![\w:])(?:std::)?(exp|log10|log|pow)\(", r"kb_\1(", text)
+    return text.replace("kb_pow(10.0, ", "kb_exp10(")
 
 
 def emit(key):

@@ -163,7 +163,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   k[2] = 1.4e-18 * kb_pow(Tgas, 0.928) * kb_exp(-Tgas / 16200.0);  // H + e- -> H-
   k[3] = 0.11 * kb_pow(p.Trad, 2.13) * kb_exp(-8823.0 / p.Trad);  // H- -> H + e-
   k[8] = 5.7e-06 * 1.0/(std::sqrt(Tgas)) + 6.3e-08 - 9.2e-11 * std::sqrt(Tgas) + 4.4e-13 * Tgas;  // H- + H+ -> H + H
-  k[9] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // H + H+ -> H2+
+  k[9] = kb_exp10(-19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // H + H+ -> H2+
   k[10] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // H2+ -> H + H+
   k[11] = 6.4e-10;  // H2+ + H -> H2 + H+
   k[12] = 2e-07 * 1.0/(std::sqrt(Tgas));  // H2+ + e- -> H + H
@@ -190,8 +190,8 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   k[46] = 2.1e-09;  // D+ + H2 -> H+ + HD
   k[48] = 1e-09 * kb_exp(-464.0 * vh_invTgas);  // HD + H+ -> H2 + D+
   k[49] = (2.1 - 0.4 * kb_log10(Tgas)) * 1e-09;  // HD + H3+ -> H2 + H2D+
-  k[50] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D + H+ -> HD+
-  k[51] = kb_pow(10.0, -19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D+ + H -> HD+
+  k[50] = kb_exp10(-19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D + H+ -> HD+
+  k[51] = kb_exp10(-19.38 - 1.523 * kb_log10(Tgas) + 1.118 * kb_log10(Tgas)*kb_log10(Tgas) - 0.1269 * kb_log10(Tgas)*kb_log10(Tgas)*kb_log10(Tgas));  // D+ + H -> HD+
   k[52] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // HD+ -> H + D+
   k[53] = 16300000.0 * kb_exp(-32400.0 / p.Trad);  // HD+ -> H+ + D
   k[54] = 7.2e-08 * 1.0/(std::sqrt(Tgas));  // HD+ + e- -> H + D

@@ -325,7 +325,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
   k[26] = 5.996e-30 * kb_pow(Tgas, 4.1881) * kb_pow(1.0 + 6.761e-06 * Tgas, -5.6881) * kb_exp(-54657.4 * vh_invT);  // H2 + H2 -> H + H + H2
   k[27] = 1.2e-15 * kb_pow(Tgas / 300.0, 0.25);  // He+ + H -> He + H+
   k[30] = 3.7e-14 * kb_exp(-35.0 / Tgas);  // H2 + He+ -> He + H + H+
-  k[31] = kb_pow(10.0, -27.029 + 3.801 * kb_log10(Tgas) - 29487.0 / Tgas);  // H2 + He -> H + H + He
+  k[31] = kb_exp10(-27.029 + 3.801 * kb_log10(Tgas) - 29487.0 / Tgas);  // H2 + He -> H + H + He
   k[32] = 7.2e-15;  // H2 + He+ -> H2+ + He
   k[33] = 1.2e-17 * kb_pow(Tgas, 1.2) * kb_exp(-157800.0 * vh_invT);  // H + H -> H + H+ + e-
   k[34] = 1.75e-17 * kb_pow(Tgas, 1.3) * kb_exp(-157800.0 * vh_invT);  // H + He -> He + H+ + e-
@@ -361,7 +361,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[10] = 2.1e-20 * kb_pow(T / 30.0, -0.15);  // H + H+ -> H2+
     }
     else if (T >= 30.0) {
-      k[11] = kb_pow(10.0, -18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
+      k[11] = kb_exp10(-18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
     }
   }
   {  // group 4: H2 + H+ -> H2+ + H
@@ -404,10 +404,10 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_sumsbv = v_sumsbv(T, n, p);
     (void)vh_sumsbv;
     if (T >= 100.0 && T >= 100.0 && T < 100000.0) {
-      k[13] = kb_pow(10.0, vh_sumsav);  // H2 + H+ -> H2+ + H
+      k[13] = kb_exp10(vh_sumsav);  // H2 + H+ -> H2+ + H
     }
     else if (T >= 100000.0) {
-      k[14] = kb_pow(10.0, vh_sumsbv);  // H2 + H+ -> H2+ + H
+      k[14] = kb_exp10(vh_sumsbv);  // H2 + H+ -> H2+ + H
     }
   }
   {  // group 5: H- + H -> H + H + e-
@@ -1489,7 +1489,7 @@ inline const double photo_Emax_[8] = {INFINITY, INFINITY, INFINITY, 12398.419843
 // ---- host: the photo cross sections (photon-bin setup) ----
 namespace kbxs {
 inline double H2_sigmaLW(double E) {
-  auto band = [](double lg) { return 1e-18 * kb_pow(10.0, lg); };
+  auto band = [](double lg) { return 1e-18 * kb_exp10(lg); };
   double l0 = 0.0, w0 = 0.0, l1 = 0.0, w1 = 0.0;
   if (E > 14.675 && E < 16.820) l0 = band(15.1289 - 1.05139 * E);
   else if (E > 16.820 && E < 17.6)
@@ -2173,7 +2173,7 @@ static inline double photo_xsec_int_5(double a, double b) {
 // xsec of H2+ -> H+ + H+ + e- [cm^2]
 static inline double photo_xsec_6(double E_eV) {
   (void)E_eV;
-  return kb_pow(10.0, -16.926 - 0.04528 * E_eV + 0.0002238 * E_eV*E_eV + 4.245e-07 * E_eV*E_eV*E_eV);
+  return kb_exp10(-16.926 - 0.04528 * E_eV + 0.0002238 * E_eV*E_eV + 4.245e-07 * E_eV*E_eV*E_eV);
 }
 // xsec of H2 -> H + H [cm^2]
 static inline double photo_xsec_7(double E_eV) {

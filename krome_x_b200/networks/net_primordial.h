@@ -293,7 +293,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
     const double vh_invT = v_invT(T, n, p);
     (void)vh_invT;
     if (T < 2000.0) {
-      k[33] = kb_pow(10.0, -56.4737 + 5.88886 * kb_log10(T) + 7.19692 * kb_log10(T)*kb_log10(T) + 2.25069 * kb_log10(T)*kb_log10(T)*kb_log10(T) - 2.16903 * kb_log10(T)*kb_log10(T)*kb_log10(T)*kb_log10(T) + 0.317887 * ipow_<5>(kb_log10(T)));  // H2 + D -> HD + H
+      k[33] = kb_exp10(-56.4737 + 5.88886 * kb_log10(T) + 7.19692 * kb_log10(T)*kb_log10(T) + 2.25069 * kb_log10(T)*kb_log10(T)*kb_log10(T) - 2.16903 * kb_log10(T)*kb_log10(T)*kb_log10(T)*kb_log10(T) + 0.317887 * ipow_<5>(kb_log10(T)));  // H2 + D -> HD + H
     }
     else if (T >= 2000.0) {
       k[34] = 3.17e-10 * kb_exp(-5207.0 * vh_invT);  // H2 + D -> HD + H

@@ -231,7 +231,7 @@ KB_HD inline double v_kh21(double Tgas, const double* n, const Params& p) {
 }
 KB_HD inline double v_ncr21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
-  return kb_pow(10.0, 4.845 - 1.3 * kb_log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * kb_log10(v_T(Tgas, n, p) * 0.0001)*kb_log10(v_T(Tgas, n, p) * 0.0001));
+  return kb_exp10(4.845 - 1.3 * kb_log10(v_T(Tgas, n, p) * 0.0001) + 1.62 * kb_log10(v_T(Tgas, n, p) * 0.0001)*kb_log10(v_T(Tgas, n, p) * 0.0001));
 }
 KB_HD inline double v_a21(double Tgas, const double* n, const Params& p) {
   (void)Tgas; (void)n; (void)p;
@@ -315,7 +315,7 @@ KB_HD inline void rates_fixed(double Tgas, const double* n, const Params& p, dou
       k[10] = 2.1e-20 * kb_pow(T / 30.0, -0.15);  // H + H+ -> H2+
     }
     else if (T >= 30.0) {
-      k[11] = kb_pow(10.0, -18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
+      k[11] = kb_exp10(-18.2 - 3.194 * kb_log10(T) + 1.786 * kb_log10(T)*kb_log10(T) - 0.2072 * kb_log10(T)*kb_log10(T)*kb_log10(T));  // H + H+ -> H2+
     }
   }
   {  // group 4: H2 + H+ -> H2+ + H

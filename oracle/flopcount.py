@@ -62,6 +62,7 @@ inline cd log(cd a) { ++cnt().flops; ++cnt().special; return cd(std::log(a.v)); 
 inline cd log10(cd a) { ++cnt().flops; ++cnt().special; return cd(std::log10(a.v)); }
 inline cd tanh(cd a) { ++cnt().flops; ++cnt().special; return cd(std::tanh(a.v)); }
 inline cd pow(cd a, cd b) { ++cnt().flops; ++cnt().special; return cd(std::pow(a.v, b.v)); }
+inline cd exp10(cd a) { ++cnt().flops; ++cnt().special; return cd(std::pow(10.0, a.v)); }
 inline cd sqrt(cd a) { ++cnt().flops; return cd(std::sqrt(a.v)); }
 inline cd fabs(cd a) { return cd(std::fabs(a.v)); }
 inline cd fmin(cd a, cd b) { return cd(std::fmin(a.v, b.v)); }
@@ -110,9 +111,14 @@ def counting_source(key):
     def conv(text):
         text = re.sub(r"#include \"../csrc/kb_common.h\"", "", text)
         text = re.sub(r"#include \"../csrc/kb_conserve.h\"", "", text)
+        text = re.sub(r"#include \"../csrc/kb_jacdk.h\"",
+                      lambda m: conv((ROOT / "krome_x_b200/csrc/kb_jacdk.h")
+                                     .read_text().replace("#pragma once", "")),
+                      text)
         text = re.sub(r"#include \"../csrc/kb_physics.h\"",
                       lambda m: conv((ROOT / "krome_x_b200/csrc/kb_physics.h")
                                      .read_text()), text)
+        text = re.sub(r"\bkb_exp10\(", "kbfc::exp10(", text)
         text = re.sub(r"\bkb_(exp|log10|log|pow)\(", r"kbfc::\1(", text)
         text = re.sub(r"\bdouble\b", "kbfc::cd", text)
         text = text.replace("std::", "kbfc::")

@@ -79,12 +79,12 @@ def test_concurrent_callers_equal_serial_calls(key):
 
 @pytest.mark.gpu
 def test_concurrent_callers_overlap():
-    """four threads' calls (2,048 cells each: a batch that leaves most SMs
-    idle) finish in well under the time of the same four calls in a row"""
+    """four threads' calls (256 cells each: a batch that occupies a few SMs)
+    finish in well under the time of the same four calls in a row"""
     key = "primordial3"
     net = krome.load(key)
     opts = net.options(**workloads.OPTIONS[key])
-    cases = _cases(key, 4, 2048)
+    cases = _cases(key, 4, 256)
     out = [None] * len(cases)
 
     def work(t):
