@@ -75,9 +75,9 @@ RTOL = 1e-6
 # DRAM bytes (read + write) the solve kernel moves per cell-solve in a
 # hydro-loop call: one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum) of the third call of a 3-call primordial3 collapse
-# loop on 65,536 cells, 10.24 + 9.09 GB in one launch; the traffic grows
+# loop on 65,536 cells, 10.31 + 9.53 GB in one launch; the traffic grows
 # with the cells solved, so a launch of this benchmark moves this x its cells
-TRAFFIC_PER_CELL_SOLVE = 19.33e9 / 65536
+TRAFFIC_PER_CELL_SOLVE = 19.84e9 / 65536
 from krome_x_b200.krome import STAT_NAMES  # the per-cell counters' columns
 
 

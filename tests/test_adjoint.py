@@ -10,13 +10,15 @@ the initial n and Tgas and the per-reaction ln-multipliers as inputs):
   over the same tape (a dot-product test to 1e-9);
 * the oracle's gradient against central finite differences of
   tight-tolerance (rtol 1e-11) solves, step 1e-3 in ln k and relative 1e-4
-  in the state, per cell as the largest difference over the gradient
-  relative to its largest component: median below 1e-5 and at least 75 %
-  of the cells within 1e-4. The rest, up to a few 1e-3, is the error of
-  differentiating the discrete solution with its step sequence held fixed,
-  which the state's error control does not bound: it shows on sensitivities
-  that cancel over the interval (dT_end / dT0 relaxing from 1 to -0.02),
-  reaches ~2e-2 on a few cells and does not shrink with rtol;
+  in the state, on 64 cells, every ln k, every species and Tgas, per cell
+  as the largest difference over the gradient relative to its largest
+  component: every cell whose temperature stays on one side of the
+  network's piecewise rate breakpoints within 1e-4. A cell that crosses
+  one (primordial's H+ + e- -> H fit jumps at 5500 K) differs by up to a
+  few 1e-2: the finite differences see the jump move with the crossing
+  time, which the adjoint of the smooth pieces leaves out (the same cells
+  at rtol 1e-10 still differ by that much, while the others agree to
+  ~1e-10);
 * the GPU adjoint against the oracle's on the same seeded cells (the
   parity of the forward solves carries over to the gradients), and against
   the same finite differences;
@@ -24,11 +26,12 @@ the initial n and Tgas and the per-reaction ln-multipliers as inputs):
   (a full tape: -120, the cell untouched, zero gradients).
 """
 import ctypes
+import re
 
 import numpy as np
 import pytest
 
-from conftest import NETWORKS
+from conftest import NETWORKS, ROOT
 from krome_x_b200 import krome, netinfo, workloads
 from oracle import Oracle
 
@@ -97,10 +100,31 @@ def fd_gradients(n, T, dt, par, objs, reactions, species, eps=1e-3):
     return out
 
 
-def check_against_fd(res_for_seed, n, T, fd, reactions, species):
+def breakpoints(key):
+    """the temperatures at which the network's piecewise rate fits switch
+    (the emitted groups' range tests)"""
+    h = (ROOT / "krome_x_b200" / "networks" / ("net_%s.h" % key)).read_text()
+    return sorted({float(v) for v in
+                   re.findall(r"\bT (?:<|>=|>|<=) ([0-9][0-9.e+]*)", h)})
+
+
+def crossing(T0, Tend, key=KEY):
+    """per cell: whether its temperature passes a rate breakpoint between
+    the initial and the final state"""
+    lo, hi = np.minimum(T0, Tend), np.maximum(T0, Tend)
+    bp = np.array(breakpoints(key))
+    return ((lo[:, None] < bp[None, :]) & (bp[None, :] < hi[:, None])).any(1)
+
+
+def check_against_fd(res_for_seed, n, T, Tend, fd, reactions, species,
+                     frac=1.0):
     """res_for_seed(i) -> (dm, dn0, dT0) of objective i; the per-cell
-    normalised errors: median <= 1e-5, >= 75 % of cells <= 1e-4, and all
-    <= 0.1 (a wrong sign or a missing term is an O(1) error)"""
+    normalised errors: within 1e-4 on (a fraction frac of) the cells whose
+    temperature stays between two rate breakpoints, those within 1e-3 all,
+    and at most 0.1 on the others (a wrong sign or a missing term is an
+    O(1) error)"""
+    cross = crossing(T, Tend)
+    assert (~cross).sum() >= len(T) // 2, cross
     for i, f in enumerate(fd):
         dm, dn0, dT0 = res_for_seed(i)
         ref = np.stack([f["k"][r] for r in reactions]
@@ -109,23 +133,31 @@ def check_against_fd(res_for_seed, n, T, fd, reactions, species):
                        + [dn0[:, j] * n[:, j] for j in species]
                        + [dT0 * T], axis=1)
         err = normalised_error(got, ref)
-        assert np.median(err) <= 1e-5, (i, err)
-        assert (err <= 1e-4).mean() >= 0.75, (i, err)
+        assert (err[~cross] <= 1e-4).mean() >= frac, (i, err[~cross], err)
+        assert (err[~cross] <= 1e-3).all(), (i, err[~cross].max(), err)
         assert (err <= 0.1).all(), (i, err)
 
 
-REACTIONS = [1, 8, 9, 15, 16, 27]
-SPECIES = ("H", "H2", "e-")
+REACTIONS = list(range(38))
+SPECIES = ("D", "D+", "E", "H", "H+", "H-", "H2", "H2+", "HD", "He", "He+",
+           "He++")
+
+
+_FD = {}
 
 
 def fd_case():
-    info, n, T, dt, par = cells(48, seed=5, pick=16)
-    sp = info["species"]
-    species = [sp.index(s) for s in SPECIES]
-    gx, gxT, gT0n, gT = seeds(info, n, T)
-    objs = [lambda a, b: (a * gx).sum(1), lambda a, b: b * gT]
-    fd = fd_gradients(n, T, dt, par, objs, REACTIONS, species)
-    return (n, T, dt, par), species, ((gx, gxT), (gT0n, gT)), fd
+    """64 seeded cells (the densest of 192), every reaction, species and
+    Tgas; computed once per process"""
+    if "case" not in _FD:
+        info, n, T, dt, par = cells(192, seed=5, pick=64)
+        sp = info["species"]
+        species = [sp.index(s if s in sp else "e-") for s in SPECIES]
+        gx, gxT, gT0n, gT = seeds(info, n, T)
+        objs = [lambda a, b: (a * gx).sum(1), lambda a, b: b * gT]
+        fd = fd_gradients(n, T, dt, par, objs, REACTIONS, species)
+        _FD["case"] = ((n, T, dt, par), species, ((gx, gxT), (gT0n, gT)), fd)
+    return _FD["case"]
 
 
 def test_oracle_adjoint_is_the_transpose_of_its_tangent():
@@ -164,7 +196,7 @@ def test_oracle_adjoint_matches_tight_finite_differences():
     o = workloads.OPTIONS[KEY]
     res = [orc.adjoint(n, T, dt, par, g, gt, **o) for g, gt in sd]
     check_against_fd(lambda i: (res[i]["dm"], res[i]["dn0"], res[i]["dT0"]),
-                     n, T, fd, REACTIONS, species)
+                     n, T, res[0]["T"], fd, REACTIONS, species)
 
 
 @pytest.mark.parametrize("key", NETWORKS)
@@ -263,8 +295,10 @@ def test_gpu_adjoint_matches_tight_finite_differences():
     net = krome.load(KEY)
     res = [net.adjoint(n, T, dt, par, gn=g, gT=gt, opts=gpu_opts(net))
            for g, gt in sd]
+    # the GPU's forward differs from the oracle's in the last bits, which
+    # the solve's step decisions amplify to the rtol level
     check_against_fd(lambda i: (res[i].dm, res[i].dn0, res[i].dT0),
-                     n, T, fd, REACTIONS, species)
+                     n, T, res[0].Tgas, fd, REACTIONS, species, frac=0.98)
 
 
 @pytest.mark.gpu
