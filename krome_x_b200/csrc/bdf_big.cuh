@@ -410,54 +410,36 @@ __device__ double elim_warp(int i, double* A, const double* rpiv, double* w) {
   return piv;
 }
 
-// the dense rows' sparse columns (the Schur complement into S), right-
-// looking: at step s, with pivot row k = bk_sk[s] final, the dense rows' L
-// entries (i, k) are final too; each gets l = a(i, k) / a(k, k) (into lb, a
-// scratch of BK_D doubles), then every pair (i, U entry (k, j)) applies
-// a(i, j) -= l a(k, j) -- distinct targets within a step, so all pairs run
-// in parallel. Per element the operations and their order are those of the
-// row-wise (IKJ) elimination. Two barriers per step; what a step reads that
-// no step writes (its L entries' places, its first pairs' targets and U
-// values) is loaded during the step before.
-__device__ void schur(double* A, double* S, const double* rpiv, double* lb) {
+// the dense rows' sparse columns (the Schur complement into S), by levels
+// of the right-looking pivot steps: a level's steps need no result of each
+// other (a step follows every step that writes one of its L entries), so
+// level L first turns all its L entries into multipliers l = a(i, k) /
+// a(k, k) (a thread per entry), then updates all its targets (a thread per
+// target, a(i, j) -= l a(k, j) over the target's contributions in step
+// order): two barriers per level instead of two per pivot step. Per target
+// the operations are the row-wise (IKJ) elimination's, in its order except
+// where two levels' steps write the same target
+__device__ void schur(double* A, double* S, const double* rpiv) {
   const int tid = threadIdx.x;
-  int pp = -1;  // this thread's L entry of the next step (a place in A)
-  int pt[2];    // the next step's pairs tid and tid + NT: targets, U values
-  double pu[2];
-  auto prefetch = [&](int s) {
-    const int k = d_bk_sk[s], c0 = d_bk_sp[s], nc = d_bk_sp[s + 1] - c0;
-    const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
-    const int* st = d_bk_st + d_bk_so[s];
-    pp = tid < nc ? d_bk_sl[c0 + tid] : -1;
-#pragma unroll
-    for (int y = 0; y < 2; ++y) {
-      const int x = tid + y * NT;
-      const bool in = x < nc * nq;
-      pt[y] = in ? st[x] : 0;
-      pu[y] = in ? A[q0 + x % nq] : 0.0;
+  for (int L = 0; L < BK_NSL; ++L) {
+    const int e1 = d_bkl_lp[L + 1];
+    for (int e = d_bkl_lp[L] + tid; e < e1; e += NT) {
+      const int p = d_bkl_lpl[e];
+      A[p] = A[p] * rpiv[d_bkl_lk[e]];
     }
-  };
-  if (BK_NSCHUR > 0) prefetch(0);
-  for (int s = 0; s < BK_NSCHUR; ++s) {
-    const int k = d_bk_sk[s];
-    const int nc = d_bk_sp[s + 1] - d_bk_sp[s];
-    const int q0 = d_sp_di[k] + 1, nq = d_sp_rp[k + 1] - q0;
-    const int* st = d_bk_st + d_bk_so[s];
-    const int myp = pp;
-    if (myp >= 0) lb[tid] = A[myp] * rpiv[k];
-    const int t0 = pt[0], t1 = pt[1];
-    const double u0 = pu[0], u1 = pu[1];
     __syncthreads();
-    if (s + 1 < BK_NSCHUR) prefetch(s + 1);
-    for (int x = tid, y = 0; x < nc * nq; x += NT, ++y) {
-      const int c = x / nq;
-      const int t = y == 0 ? t0 : (y == 1 ? t1 : st[x]);
-      const double u = y == 0 ? u0 : (y == 1 ? u1 : A[q0 + (x - c * nq)]);
-      const double v = lb[c] * u;
-      if (t >= 0) A[t] -= v;
-      else S[-1 - t] -= v;
+    const int t1 = d_bkl_tp[L + 1];
+    for (int t = d_bkl_tp[L] + tid; t < t1; t += NT) {
+      const int code = d_bkl_tgt[t];
+      double v = code >= 0 ? A[code] : S[-1 - code];
+      const int c1 = d_bkl_cp[t + 1];
+      for (int c = d_bkl_cp[t]; c < c1; ++c) {
+        const double w = A[d_bkl_cl[c]] * A[d_bkl_cu[c]];
+        v -= w;
+      }
+      if (code >= 0) A[code] = v;
+      else S[-1 - code] = v;
     }
-    if (myp >= 0) A[myp] = lb[tid];
     __syncthreads();
   }
 }
@@ -580,7 +562,7 @@ __device__ int block_lu(double* A) {
     }
     __syncthreads();
   }
-  schur(A, S, rpiv, smem() + SM::T);
+  schur(A, S, rpiv);
   bad = dense_lu(S, rpiv + BK_M) || bad;
   return __syncthreads_or(bad) ? 1 : 0;
 }

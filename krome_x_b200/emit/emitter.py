@@ -1570,6 +1570,16 @@ class Emitter:
                              [bk_so[s] .. bk_so[s+1]) the step's update
                              targets, entry by entry then U entry by U
                              entry (bk_tgt in step order)
+          bkl_*              the same Schur complement by levels: a step
+                             joins the level above every earlier step that
+                             writes one of its L entries. Level L divides
+                             its L entries bkl_lpl[bkl_lp[L] .. bkl_lp[L+1])
+                             by their pivots (rows bkl_lk), then updates its
+                             targets bkl_tgt[bkl_tp[L] .. bkl_tp[L+1]), each
+                             target t by its contributions bkl_cl / bkl_cu
+                             [bkl_cp[t] .. bkl_cp[t+1]) (the places of l
+                             and u) in step order: per target the
+                             operations and their order are the steps'
           d_bk_hnuc          H nuclei per species (the terms of Hnuclei_)"""
         w = self.w
         D = min(self.BK_DMAX, n)
@@ -1628,6 +1638,52 @@ class Emitter:
             for p in cols[k]:
                 st += tgt[uoff[p]:uoff[p] + nq]
             so.append(len(st))
+        # the Schur steps by levels (a step reads its L entries; it must
+        # follow every earlier step that writes one of them)
+        nsk = len(sk)
+        reads = [set(sl[sp_[t]:sp_[t + 1]]) for t in range(nsk)]
+        writer = {}
+        lvl = [0] * nsk
+        for t in range(nsk):
+            lv = 0
+            for pl in reads[t]:
+                if pl in writer:
+                    lv = max(lv, writer[pl] + 1)
+            lvl[t] = lv
+            for x in st[so[t]:so[t + 1]]:
+                if x >= 0:
+                    writer[x] = max(writer.get(x, -1), lv)
+        nsl = (max(lvl) + 1) if nsk else 0
+        lpl, lk, lp = [], [], [0]
+        tgt_l, tp, cp, cl, cu = [], [0], [0], [], []
+        for L in range(nsl):
+            contrib = {}
+            order = []
+            for t in range(nsk):
+                if lvl[t] != L:
+                    continue
+                k = sk[t]
+                q0 = di[k] + 1
+                nq = rp[k + 1] - q0
+                ents = sl[sp_[t]:sp_[t + 1]]
+                for pl in ents:
+                    lpl.append(pl)
+                    lk.append(k)
+                for c, pl in enumerate(ents):
+                    for x in range(nq):
+                        tg = st[so[t] + c * nq + x]
+                        if tg not in contrib:
+                            contrib[tg] = []
+                            order.append(tg)
+                        contrib[tg].append((pl, q0 + x))
+            lp.append(len(lpl))
+            for tg in order:
+                tgt_l.append(tg)
+                for pl, q in contrib[tg]:
+                    cl.append(pl)
+                    cu.append(q)
+                cp.append(len(cl))
+            tp.append(len(tgt_l))
         inv = {v: key for key, v in pos.items()}
         jt = [code(*inv[q]) for q in jpos]
         self.meta["bk_m"] = m
@@ -1654,6 +1710,15 @@ class Emitter:
         self._table("bk_sl", sl or [0])
         self._table("bk_so", so)
         self._table("bk_st", st or [0])
+        w("constexpr int BK_NSL = %d;  // Schur levels" % nsl)
+        self._table("bkl_lp", lp)
+        self._table("bkl_lpl", lpl or [0])
+        self._table("bkl_lk", lk or [0])
+        self._table("bkl_tp", tp)
+        self._table("bkl_tgt", tgt_l or [0])
+        self._table("bkl_cp", cp)
+        self._table("bkl_cl", cl or [0])
+        self._table("bkl_cu", cu or [0])
         w("#ifdef __CUDACC__")
         w("__device__ const double d_bk_hnuc[NSPEC] = {%s};"
           % ",".join(repr(float(v)) for v in self.natoms_H))

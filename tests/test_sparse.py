@@ -20,7 +20,9 @@ from oracle import Oracle
 KEY = "semenov"
 TABLES = ("sp_rp", "sp_ci", "sp_di", "sp_perm", "sp_jpos", "bk_frow",
           "bk_flp", "bk_brow", "bk_blp", "bk_uoff", "bk_tgt", "bk_jt",
-          "bk_l21e", "bk_sk", "bk_sp", "bk_sl", "bk_so", "bk_st")
+          "bk_l21e", "bk_sk", "bk_sp", "bk_sl", "bk_so", "bk_st", "bkl_lp",
+          "bkl_lpl", "bkl_lk", "bkl_tp", "bkl_tgt", "bkl_cp", "bkl_cl",
+          "bkl_cu")
 
 
 @pytest.fixture(scope="module")
@@ -41,8 +43,9 @@ def sched():
 def _block_lu(t, A, S):
     """the kernel's factorization (bdf_big.cuh block_lu), phase by phase:
     the sparse rows level by level (each level's rows in reverse order: the
-    rows of a level are independent), the dense rows' sparse columns pivot
-    by pivot (bk_sk / bk_sp / bk_sl), the dense block in panels of 16.
+    rows of a level are independent), the dense rows' sparse columns level
+    by level of the pivot steps (bkl_*: the level's multipliers, then its
+    targets' contributions in order), the dense block in panels of 16.
     Returns 1 / the pivots."""
     rp, ci, di = t["sp_rp"], t["sp_ci"], t["sp_di"]
     m, D, LD, n = t["BK_M"], t["BK_D"], t["BK_LD"], t["NSPEC"]
@@ -64,19 +67,20 @@ def _block_lu(t, A, S):
         for i in frow[flp[L]:flp[L + 1]][::-1]:
             elim(rp[i], di[i])
             rpiv[i] = 1.0 / A[di[i]]
-    sk, sp, sl = t["bk_sk"], t["bk_sp"], t["bk_sl"]
-    for s in range(t["BK_NSCHUR"]):  # the dense rows' columns, pivot by pivot
-        k = sk[s]
-        ps = sl[sp[s]:sp[s + 1]]
-        lb = A[ps] * rpiv[k]
-        q0, q1 = di[k] + 1, rp[k + 1]
-        steps = t["bk_st"][t["bk_so"][s]:t["bk_so"][s + 1]].reshape(len(ps), q1 - q0)
-        for p, l, tg in zip(ps, lb, steps):
-            a = tg >= 0
-            u = A[q0:q1]
-            A[tg[a]] -= l * u[a]
-            S[-1 - tg[~a]] -= l * u[~a]
-        A[ps] = lb
+    cp = t["bkl_cp"]
+    for L in range(t["BK_NSL"]):  # the dense rows' columns, level by level
+        e0, e1 = t["bkl_lp"][L], t["bkl_lp"][L + 1]
+        pl = t["bkl_lpl"][e0:e1]
+        A[pl] = A[pl] * rpiv[t["bkl_lk"][e0:e1]]
+        t0, t1 = t["bkl_tp"][L], t["bkl_tp"][L + 1]
+        c0, c1 = cp[t0], cp[t1]
+        w = A[t["bkl_cl"][c0:c1]] * A[t["bkl_cu"][c0:c1]]
+        # each contribution's target, in the targets' order (ufunc.at
+        # subtracts repeated targets one after another)
+        tg = np.repeat(t["bkl_tgt"][t0:t1], np.diff(cp[t0:t1 + 1]))
+        a = tg >= 0
+        np.subtract.at(A, tg[a], w[a])
+        np.subtract.at(S, -1 - tg[~a], w[~a])
     Sm = S.reshape(D, LD)[:, :D]
     for c0 in range(0, D, 16):
         pe = min(c0 + 16, D)
@@ -172,6 +176,29 @@ def test_block_schedule_is_consistent(sched):
     for s in range(t["BK_NSCHUR"]):
         ps = sl[sp[s]:sp[s + 1]]
         assert (ci[ps] == sk[s]).all() and (np.diff(row_of[ps]) > 0).all()
+    # the Schur levels: every L entry divided once, by its pivot; a level's
+    # targets distinct; what a level reads (multipliers, U values) is
+    # written by no later level and by no target of its own
+    lpl = t["bkl_lpl"]
+    assert sorted(lpl.tolist()) == sorted(sl.tolist())
+    assert (ci[lpl] == t["bkl_lk"]).all()
+    lvl_of = {}
+    for L in range(t["BK_NSL"]):
+        for pl in lpl[t["bkl_lp"][L]:t["bkl_lp"][L + 1]]:
+            lvl_of[int(pl)] = L
+    last_write = {}
+    for L in range(t["BK_NSL"]):
+        tg = t["bkl_tgt"][t["bkl_tp"][L]:t["bkl_tp"][L + 1]]
+        assert len(set(tg.tolist())) == len(tg)
+        for g in tg[tg >= 0]:
+            last_write[int(g)] = L
+    for L in range(t["BK_NSL"]):
+        t0, t1 = t["bkl_tp"][L], t["bkl_tp"][L + 1]
+        c0, c1 = t["bkl_cp"][t0], t["bkl_cp"][t1]
+        for pl in t["bkl_cl"][c0:c1]:
+            assert lvl_of[int(pl)] <= L and last_write.get(int(pl), -1) < lvl_of[int(pl)]
+        for q in t["bkl_cu"][c0:c1]:
+            assert row_of[q] < m and int(q) not in last_write
     for q, g in zip(t["sp_jpos"], t["bk_jt"]):
         i, j = row_of[q], ci[q]
         if i < m or j < m:
