@@ -358,43 +358,61 @@ __device__ __forceinline__ void elim_thread(int p0, int p1, double* A,
 }
 // sparse row i's elimination by a warp through a dense work row w (shared
 // memory, zero on entry and on exit): the row scattered into w by column,
-// each L entry's update applied to w over the lanes -- the U row of the next
-// L entry loaded into registers while the current one is applied, so the
-// chain of L entries runs at shared-memory latency -- then the row gathered
-// back; returns the pivot
+// each L entry's update applied to w over the lanes, then the row gathered
+// back; returns the pivot. The L entries run as a software pipeline: while
+// entry p is applied, the U row of entry p + 1 is loaded into registers and
+// the place of entry p + 2's U row (two dependent table loads: its pivot
+// row, then the row's range) is looked up, so the chain of L entries waits
+// for one L2 round trip per entry at most, not three
 __device__ double elim_warp(int i, double* A, const double* rpiv, double* w) {
   const int lane = threadIdx.x & 31;
   const int p0 = d_sp_rp[i], pd = d_sp_di[i], p1 = d_sp_rp[i + 1];
   for (int p = p0 + lane; p < p1; p += 32) w[d_sp_ci[p]] = A[p];
   __syncwarp();
-  double u[4];
-  int c[4];
-  auto fetch = [&](int p) {
-    const int k = d_sp_ci[p], q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
+  constexpr int UW = 6;  // U-row entries in registers per lane
+  double u[UW];
+  int c[UW];
+  auto where = [&](int p, int& k, int& q0, int& q1) {
+    k = d_sp_ci[p];
+    q0 = d_sp_di[k] + 1;
+    q1 = d_sp_rp[k + 1];
+  };
+  auto fetch = [&](int q0, int q1) {
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < UW; ++s) {
       const int q = q0 + lane + 32 * s;
       c[s] = q < q1 ? d_sp_ci[q] : -1;
       u[s] = q < q1 ? A[q] : 0.0;
     }
   };
-  if (p0 < pd) fetch(p0);
+  int kc = 0, qc0 = 0, qc1 = 0;  // the current entry's pivot row, U range
+  int kn = 0, qn0 = 0, qn1 = 0;  // the next entry's
+  if (p0 < pd) {
+    where(p0, kc, qc0, qc1);
+    fetch(qc0, qc1);
+  }
+  if (p0 + 1 < pd) where(p0 + 1, kn, qn0, qn1);
   for (int p = p0; p < pd; ++p) {
-    const int k = d_sp_ci[p];
+    const int k = kc, q0 = qc0, q1 = qc1;
     const double l = w[k] * rpiv[k];
-    double uc[4];
-    int cc[4];
+    double uc[UW];
+    int cc[UW];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < UW; ++s) {
       uc[s] = u[s];
       cc[s] = c[s];
     }
-    if (p + 1 < pd) fetch(p + 1);
+    if (p + 1 < pd) {
+      fetch(qn0, qn1);
+      kc = kn;
+      qc0 = qn0;
+      qc1 = qn1;
+    }
+    if (p + 2 < pd) where(p + 2, kn, qn0, qn1);
 #pragma unroll
-    for (int s = 0; s < 4; ++s)
+    for (int s = 0; s < UW; ++s)
       if (cc[s] >= 0) w[cc[s]] -= l * uc[s];
-    const int q0 = d_sp_di[k] + 1, q1 = d_sp_rp[k + 1];
-    for (int q = q0 + 128 + lane; q < q1; q += 32) w[d_sp_ci[q]] -= l * A[q];
+    for (int q = q0 + 32 * UW + lane; q < q1; q += 32) w[d_sp_ci[q]] -= l * A[q];
     __syncwarp();
     if (lane == 0) w[k] = l;
     __syncwarp();
