@@ -51,8 +51,12 @@
 // linear solver (bdf_cell.hpp:1163-1264): the sequence of operations of the
 // CPU restatement (oracle/bdf_oracle.cpp, sparse path), whose IKJ row LU
 // this factorization equals up to the order of its roundings (same pivots,
-// same pattern, static pivoting). Fixed Tgas only (the large networks'
-// benchmark configuration). Every loop is bounded (max_steps, the per-step
+// same pattern, static pivoting). Tgas fixed (the large networks'
+// benchmark configuration) or evolved: then the state's last component
+// (the vectors' lengths from neq()), the Newton matrix bordered by its
+// Tgas row and column (bdf_cell.hpp:1192-1264 with one border equation),
+// on networks without thermal processes, whose dT/dt, Tgas row and corner
+// are identically zero. Every loop is bounded (max_steps, the per-step
 // failure limits, max_restarts, the work queue by the number of cells).
 #pragma once
 
@@ -90,7 +94,12 @@ struct WS {
   static constexpr long CP = SJ + rnd4(NNZ_J);        // rhs chunk sums
   static constexpr long VE = CP + rnd4(NCHUNK);       // e0, e1, eh [BK_NVAR]
   static constexpr long A = VE + 3 * rnd4(BK_NVAR);   // LU values
-  static constexpr long SIZE = A + rnd4(NNZ_LU);
+  // an evolved Tgas: the Jacobian's Tgas column over the species (B), and
+  // the full rhs at Tgas +- h for its central differences
+  static constexpr long BT = A + rnd4(NNZ_LU);
+  static constexpr long FP = BT + NV;
+  static constexpr long FM = FP + NV;
+  static constexpr long SIZE = FM + NV;
 };
 
 // the block's shared memory (doubles)
@@ -100,7 +109,8 @@ struct SM {
   static constexpr int RPIV = T + (int)NV;            // 1 / pivot, per row
   static constexpr int YR = RPIV + (int)NV;           // the rhs input (+1)
   static constexpr int RED = YR + (int)NV;            // reductions
-  static constexpr int MISC = RED + NWARP;            // the work queue's cell
+  static constexpr int MISC = RED + NWARP;            // the work queue's cell,
+                                                      // the state's length
   static constexpr int SIZE = MISC + 2;
 };
 constexpr size_t SMEM_BYTES = SM::SIZE * sizeof(double);
@@ -134,24 +144,33 @@ __device__ __forceinline__ double blk_max(double v) {
   return s;
 }
 
+// the integrator's state length: the species, and Tgas (component N) when
+// it is evolved (set by the cell's first thread, then a barrier)
+__device__ __forceinline__ int neq() { return (int)smem()[SM::MISC + 1]; }
+__device__ __forceinline__ void set_neq(int n) {
+  if (threadIdx.x == 0) smem()[SM::MISC + 1] = (double)n;
+}
+
 // ---- element-wise vector operations (component i on thread i mod NT) ----
+// KBG_FOR: the species; KBG_VFOR: the integrator's state
 #define KBG_FOR(i) for (int i = threadIdx.x; i < N; i += NT)
+#define KBG_VFOR(i) for (int i = threadIdx.x, kbg_n_ = neq(); i < kbg_n_; i += NT)
 __device__ __forceinline__ void v_copy(const double* x, double* z) {
-  KBG_FOR(i) z[i] = x[i];
+  KBG_VFOR(i) z[i] = x[i];
 }
 __device__ __forceinline__ void v_scale(double c, const double* x, double* z) {
-  KBG_FOR(i) z[i] = c * x[i];
+  KBG_VFOR(i) z[i] = c * x[i];
 }
 __device__ __forceinline__ void v_const(double c, double* z) {
-  KBG_FOR(i) z[i] = c;
+  KBG_VFOR(i) z[i] = c;
 }
 __device__ __forceinline__ void v_axpy(double a, const double* x, double* y) {
   if (a == 1.0) {
-    KBG_FOR(i) y[i] += x[i];
+    KBG_VFOR(i) y[i] += x[i];
   } else if (a == -1.0) {
-    KBG_FOR(i) y[i] -= x[i];
+    KBG_VFOR(i) y[i] -= x[i];
   } else {
-    KBG_FOR(i) y[i] += a * x[i];
+    KBG_VFOR(i) y[i] += a * x[i];
   }
 }
 // N_VLinearSum with its special cases (bdf_cell.hpp:296-400)
@@ -160,43 +179,43 @@ __device__ void v_lin_sum(double a, const double* x, double b, const double* y,
   if (b == 1.0 && z == y) { v_axpy(a, x, z); return; }
   if (a == 1.0 && z == x) { v_axpy(b, y, z); return; }
   if (a == 1.0 && b == 1.0) {
-    KBG_FOR(i) z[i] = x[i] + y[i];
+    KBG_VFOR(i) z[i] = x[i] + y[i];
   } else if ((a == 1.0 && b == -1.0) || (a == -1.0 && b == 1.0)) {
     const bool test = a == 1.0 && b == -1.0;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBG_FOR(i) z[i] = v2[i] - v1[i];
+    KBG_VFOR(i) z[i] = v2[i] - v1[i];
   } else if (a == 1.0 || b == 1.0) {
     const bool test = a == 1.0;
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBG_FOR(i) z[i] = (c * v1[i]) + v2[i];
+    KBG_VFOR(i) z[i] = (c * v1[i]) + v2[i];
   } else if (a == -1.0 || b == -1.0) {
     const bool test = a == -1.0;
     const double c = test ? b : a;
     const double* v1 = test ? y : x;
     const double* v2 = test ? x : y;
-    KBG_FOR(i) z[i] = (c * v1[i]) - v2[i];
+    KBG_VFOR(i) z[i] = (c * v1[i]) - v2[i];
   } else if (a == b) {
-    KBG_FOR(i) z[i] = a * (x[i] + y[i]);
+    KBG_VFOR(i) z[i] = a * (x[i] + y[i]);
   } else if (a == -b) {
-    KBG_FOR(i) z[i] = a * (x[i] - y[i]);
+    KBG_VFOR(i) z[i] = a * (x[i] - y[i]);
   } else {
-    KBG_FOR(i) z[i] = (a * x[i]) + (b * y[i]);
+    KBG_VFOR(i) z[i] = (a * x[i]) + (b * y[i]);
   }
 }
 __device__ __forceinline__ double v_wrms(const double* x, const double* w) {
   double s = 0.0;
-  KBG_FOR(i) {
+  KBG_VFOR(i) {
     const double pv = x[i] * w[i];
     s += pv * pv;
   }
-  return ssqrt_(blk_sum(s) / N);
+  return ssqrt_(blk_sum(s) / neq());
 }
 __device__ __forceinline__ double v_max_norm(const double* x) {
   double m = 0.0;
-  KBG_FOR(i) m = fmax(m, fabs(x[i]));
+  KBG_VFOR(i) m = fmax(m, fabs(x[i]));
   return blk_max(m);
 }
 
@@ -271,10 +290,17 @@ struct Net {
   // 794-813). Starts and ends with a block barrier.
   __device__ int rhs(const double* yv, double* f) {
     __syncthreads();
+    rates_at(load_state(yv));
+    return sums(f);
+  }
+  // f over the species from the rates in k and the state in yr, and, with
+  // an evolved Tgas, f[N] = dT/dt: identically zero on the networks whose
+  // large path evolves Tgas (no thermal processes: the generated
+  // thermal_dTdt is (gamma - 1) (0 - 0) / (k_B n_tot)). Ends with a barrier.
+  __device__ int sums(double* f) {
     const double* yr = smem() + SM::YR;
     const double* k = ws + WS::K;
     double* fl = ws + WS::FL;
-    rates_at(load_state(yv));
     for (int r = threadIdx.x; r < NREA; r += NT)
       fl[r] = k[r] * yr[d_fx_a[r]] * yr[d_fx_b[r]] * yr[d_fx_c[r]];
     __syncthreads();
@@ -301,7 +327,39 @@ struct Net {
       f[i] = a;
       ok = ok && isfinite(a);
     }
+    if (neq() > N && threadIdx.x == N % NT) f[N] = 0.0;
     return __syncthreads_and(ok) ? 0 : 1;
+  }
+  // the Tgas column of the evolved-Tgas Jacobian over the species
+  // (jac_assemble_, solve_cell.hpp:1053-1066): central differences of the
+  // full rhs at Tgas +- h, h = max(1e-6 |Tgas|, 1e-8), every rate
+  // re-evaluated there (the generated parts; the affine forms of the
+  // density-dependent rates hold at this solve's Tgas only), into B. The
+  // Tgas row and corner are the difference quotients of a dT/dt that is
+  // identically zero: zero. The rates at this solve's Tgas are restored.
+  // Starts and ends with a block barrier.
+  __device__ void jac_tgas(const double* yv, double* B) {
+    double* fp = ws + WS::FP;
+    double* fm = ws + WS::FM;
+    double* k = ws + WS::K;
+    __syncthreads();
+    const double Ty = yv[N];
+    const double h = fmax(1e-6 * fabs(Ty), 1e-8);
+    for (int side = 0; side < 2; ++side) {
+      const double Ts = fmin(fmax(side == 0 ? Ty + h : Ty - h, p.Tcmb), 1e9);
+      const double hn = load_state(yv);
+      if (threadIdx.x < RPART) {
+        rates_fixed_part(threadIdx.x, Ts, smem() + SM::YR, p, hn, k);
+        rates_var_part(threadIdx.x, Ts, smem() + SM::YR, p, hn, k);
+      }
+      __syncthreads();
+      sums(side == 0 ? fp : fm);
+    }
+    KBG_FOR(i) B[i] = (fp[i] - fm[i]) / (2.0 * h);
+    const double hn = load_state(yv);
+    if (threadIdx.x < RPART)
+      rates_fixed_part(threadIdx.x, T, smem() + SM::YR, p, hn, k);
+    __syncthreads();
   }
   // the saved Jacobian's entries at yv (the rates at yv)
   __device__ void jac(const double* yv, double* Jc) {
@@ -741,7 +799,8 @@ struct BigCvode {
   Net& P;
   const SolveOpts& o;
   double* zn[L_MAX];
-  double *ewt, *y, *acor, *tempv, *ftemp, *delta, *A, *savedJ;
+  double *ewt, *y, *acor, *tempv, *ftemp, *delta, *A, *savedJ, *bcol;
+  double zb;  // an evolved Tgas: the 1 x 1 Schur complement of the border
   Stats9 st;
   long mxstep;
   double tn, h, hin, hprime, hscale, next_h, hu, eta, etamax, etaq;
@@ -764,6 +823,8 @@ struct BigCvode {
     delta = w + WS::DELTA;
     savedJ = w + WS::SJ;
     A = w + WS::A;
+    bcol = w + WS::BT;
+    zb = 1.0;
     mxstep = o.max_steps == 0 ? 500
              : (o.max_steps < 0 ? KB_MAX_STEPS_CAP : o.max_steps);
   }
@@ -784,11 +845,12 @@ struct BigCvode {
     eta = 1.0;
   }
 
-  // cvEwtSetSV with one atol for the species (bdf_cell.hpp:689-713)
+  // cvEwtSetSV with one atol for the species and atol_T for an evolved
+  // Tgas (bdf_cell.hpp:689-713)
   __device__ int ewt_set(const double* ycur, double* wt) {
-    const double at = o.atol_n;
     bool bad = false;
-    KBG_FOR(i) {
+    KBG_VFOR(i) {
+      const double at = i < N ? o.atol_n : o.atol_T;
       const double v = (o.rtol * fabs(ycur[i])) + at;
       bad = bad || !(v > 0.0);
       wt[i] = 1.0 / v;
@@ -899,12 +961,12 @@ struct BigCvode {
   __device__ double upper_bound_h0_(double tdist) {
     double* temp1 = tempv;
     double* temp2 = acor;
-    KBG_FOR(i) temp2[i] = fabs(zn[0][i]);
+    KBG_VFOR(i) temp2[i] = fabs(zn[0][i]);
     ewt_set(zn[0], temp1);
-    KBG_FOR(i) temp1[i] = 1.0 / temp1[i];
+    KBG_VFOR(i) temp1[i] = 1.0 / temp1[i];
     v_lin_sum(HUB_FACTOR, temp2, 1.0, temp1, temp1);
-    KBG_FOR(i) temp2[i] = fabs(zn[1][i]);
-    KBG_FOR(i) temp1[i] = temp2[i] / temp1[i];
+    KBG_VFOR(i) temp2[i] = fabs(zn[1][i]);
+    KBG_VFOR(i) temp1[i] = temp2[i] / temp1[i];
     const double hub_inv = v_max_norm(temp1);
     double hub = HUB_FACTOR * tdist;
     if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
@@ -1087,7 +1149,7 @@ struct BigCvode {
       for (;;) {
         niters++;
         v_scale(-1.0, delta, delta);
-        block_solve(A, delta, delta);
+        lsolve_(delta);
         if (gamrat != 1.0) v_scale(2.0 / (1.0 + gamrat), delta, delta);
         v_lin_sum(1.0, acor, 1.0, delta, acor);
         retval = conv_test_(curiter, tol);
@@ -1161,7 +1223,11 @@ struct BigCvode {
                          || ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
                          || (convfail == FAIL_OTHER);
     jcur = jbad_ls;
-    if (jbad_ls) P.jac(y, savedJ);
+    const bool evt = neq() > N;
+    if (jbad_ls) {
+      P.jac(y, savedJ);
+      if (evt) P.jac_tgas(y, bcol);
+    }
     const double c = -gamma;
     double* S = smem() + SM::S;
     for (int k = threadIdx.x; k < NNZ_LU; k += NT) A[k] = 0.0;
@@ -1182,7 +1248,34 @@ struct BigCvode {
       st.nje++;
       nstlj = st.nst;
     }
-    return block_lu(A) > 0 ? LS_LUFACT_FAIL : 0;
+    if (block_lu(A) > 0) return LS_LUFACT_FAIL;
+    if (evt) {
+      // the border (bdf_cell.hpp:1192-1219, m = 1) with a zero Tgas row:
+      // C' = 0, so Z = c D + 1 - C' B' = 1 with D = 0, unless a non-finite
+      // entry of B' makes the products C' B' NaN (then Z is NaN, as there)
+      bool bad = false;
+      KBG_FOR(i) bad = bad || !isfinite(bcol[i] * c);
+      const double dc = 0.0 * c;
+      zb = __syncthreads_or(bad) ? NAN : dc + 1.0;
+      if (zb == 0.0) return LS_LUFACT_FAIL;
+    }
+    return 0;
+  }
+  // x = M^-1 x for the Newton matrix M (the species' block factors, and an
+  // evolved Tgas's border as the reference's solve, bdf_cell.hpp:1233-
+  // 1264: with a zero Tgas row the Tgas component is its right-hand side
+  // over Z, and the species' part takes c B times it off before the
+  // species solve, which the reference skips when it is zero)
+  __device__ void lsolve_(double* x) {
+    if (neq() == N) { block_solve(A, x, x); return; }
+    __syncthreads();
+    const double v = x[N] / zb;
+    if (v != 0.0) {
+      const double c = -gamma;
+      KBG_FOR(i) x[i] -= (bcol[i] * c) * v;
+    }
+    block_solve(A, x, x);
+    if (threadIdx.x == N % NT) x[N] = v;
   }
   __device__ int handle_nflag_(int* nflagPtr, double saved_t, int* ncfPtr) {
     const int nflag = *nflagPtr;

@@ -573,7 +573,8 @@ kb_lane_cells(int ncell, double* n, double* T, const double* dt,
 
 // cell c on this block: the pre-solve rules, the restart wrapper
 // (bdf_cell.hpp:1513-1547) and the post-solve rules (solve_cell.hpp:
-// 2094-2203) around the sparse-path CVODE, fixed Tgas. Every thread runs
+// 2094-2203) around the sparse-path CVODE, fixed or evolved Tgas (the
+// latter on networks without thermal processes). Every thread runs
 // the same control flow (the CVODE scalars are the same in every thread).
 __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
                              const double* par, int pstride, int* flags,
@@ -588,11 +589,17 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
   if (flag == 1 && params_missing(P.p) >= 0) flag = kbw::FLAG_PARAM_UNSET;
   long tot[kbw::NSTAT];
   for (int i = 0; i < kbw::NSTAT; ++i) tot[i] = 0;
+  // an evolved Tgas is the state's last component (rhs_cb_: the rhs
+  // refuses Tgas <= 0, which the large path's Tgas, constant without
+  // thermal processes, fails at its first evaluation)
+  const bool evt = so.evolve_T != 0;
+  if (flag == 1 && evt && !(T[c] > 0.0)) flag = kbw::FLAG_NONPOSITIVE_T;
   if (flag == 1) {
     P.T = fmin(fmax(T[c], P.p.Tcmb), 1e9);
     double* nrow = n + (long)c * NSPEC;
     double* k = ws + kbg::WS::K;
     for (int r = threadIdx.x; r <= NREA; r += kbg::NT) k[r] = 0.0;
+    kbg::set_neq(evt ? NSPEC + 1 : NSPEC);
     __syncthreads();
     // the Tgas/parameter-only rates once per solve, and the three points
     // of the density-dependent ones
@@ -601,8 +608,11 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
       rates_fixed_part(threadIdx.x, P.T, kbg::smem() + kbg::SM::YR, P.p, hnuc, k);
     P.prepare_var(nrow);
     kbg::BigCvode cv(P, so);
-    double* yout = ws + kbg::WS::YOUT;
-    cv.reinit(0.0, nrow, 0.0);
+    double* yout = ws + kbg::WS::YOUT;  // the initial state, then the result
+    for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) yout[i] = nrow[i];
+    if (evt && threadIdx.x == NSPEC % kbg::NT) yout[NSPEC] = T[c];
+    __syncthreads();
+    cv.reinit(0.0, yout, 0.0);
     double t = 0.0;
     int restarts = 0;
     for (;;) {  // bounded by max_restarts
@@ -623,7 +633,12 @@ __device__ void big_one_cell(int c, double* n, double* T, const double* dt,
       cv.reinit(t, yout, hcur > 0.0 ? 0.1 * hcur : 0.0);
     }
     tot[kbw::ST_RESTARTS] = restarts;
+    __syncthreads();
+    const double Tend = evt ? yout[NSPEC] : 1.0;
+    if (flag == 0 && !(Tend > 0.0 && isfinite(Tend)))
+      flag = kbw::FLAG_NONPOSITIVE_T;
     if (flag == 0) {
+      if (evt && threadIdx.x == 0) T[c] = Tend;
       for (int i = threadIdx.x; i < NSPEC; i += kbg::NT) {
         double v = yout[i];
         if (so.clip_negative && v < 0.0) v = 0.0;
@@ -923,7 +938,6 @@ cudaError_t launch(const krome_opts& h, int ncell, double* n, double* T,
   // its workspace slot (the library's device buffer, grown before a launch
   // when needed; never during a graph capture: big_workspace)
   (void)rio;
-  if (EVT) return cudaErrorNotSupported;
   if (cursor == nullptr) return cudaErrorInvalidValue;  // always the queue
   {
     static bool attr[64] = {};
@@ -1292,11 +1306,16 @@ namespace {
 // bins; the FP32 Newton-matrix form exists in the lane layout only
 int unsupported(const krome_opts& h) {
 #ifdef KB_LARGE_NETWORK
-  // the large networks: the sparse LU (linsol auto or sparse), fixed Tgas,
-  // FP64, the scalar tolerances
+  // the large networks: the sparse LU (linsol auto or sparse), FP64, the
+  // scalar tolerances; an evolved Tgas (the Newton matrix's Tgas border)
+  // with the analytic (hybrid) Jacobian on networks without thermal
+  // processes (dT/dt identically zero): the difference quotients over every
+  // column (JAC_AUTO's choice with evolve_T) are not built for them
   if (h.linsol == 1 || h.linsol == 2) return -104;
   if (!h.atol_sp.empty() || !h.rtol_sp.empty()) return -104;
-  if (h.evolve_T != 0 || h.lu32 != 0) return -104;
+  if (h.lu32 != 0) return -104;
+  if (h.evolve_T != 0 && (kbnet::HAS_THERMAL_TERMS || resolved_jac(h) != 1))
+    return -104;
 #else
   if (h.linsol == 2 || h.linsol == 3) return -104;
   if (h.lu32 != 0 && h.layout != 1) return -104;

@@ -224,6 +224,61 @@ void sp_getrs_(const double* a, const double* b, double* t, double* x) {
   }
   for (int i = 0; i < NSPEC; i++) x[sp_perm[i]] = t[i];
 }
+// The Tgas border of an evolved-Tgas solve (bdf_cell.hpp:1192-1219 with
+// m = 1, the reference's layout of one border equation): with the species
+// factors of sp_getrf_, B' = L^-1 (c B), C' = (c C) U^-1 and the Schur
+// complement Z = c D + 1 - C' B' (its 1 x 1 LU: a zero Z fails). B, C:
+// the saved Tgas column and row over the species (species order), D the
+// saved corner.
+struct SpBorder {
+  double *B = nullptr, *C = nullptr, D = 0.0;  // saved Jacobian
+  double *Bt = nullptr, *Ct = nullptr, Z = 0.0;  // factors (pivot order)
+};
+int sp_border_factor_(const double* a, double c, SpBorder& br) {
+  double* x = br.Bt;
+  for (int k = 0; k < NSPEC; k++) x[k] = br.B[sp_perm[k]] * c;
+  for (int i = 0; i < NSPEC; i++) {  // x = L^-1 x (unit lower)
+    double s = x[i];
+    for (int p = sp_rp[i]; p < sp_di[i]; p++) s -= a[p] * x[sp_ci[p]];
+    x[i] = s;
+  }
+  x = br.Ct;  // x U = the row: a forward sweep over U's rows
+  for (int k = 0; k < NSPEC; k++) x[k] = br.C[sp_perm[k]] * c;
+  for (int k = 0; k < NSPEC; k++) {
+    const double xk = x[k] / a[sp_di[k]];
+    x[k] = xk;
+    if (xk != 0.0)
+      for (int q = sp_di[k] + 1; q < sp_rp[k + 1]; q++) x[sp_ci[q]] -= xk * a[q];
+  }
+  double z = br.D * c;
+  z += 1.0;
+  for (int k = 0; k < NSPEC; k++) z -= br.Ct[k] * br.Bt[k];
+  br.Z = z;
+  return z == 0.0 ? 1 : 0;
+}
+// x = A^-1 b for the bordered matrix (bdf_cell.hpp:1233-1264): b, x of
+// NSPEC + 1 entries (Tgas last), may alias; t: NSPEC doubles of scratch
+void sp_getrs_border_(const double* a, const SpBorder& br, const double* b,
+                      double* t, double* x) {
+  for (int i = 0; i < NSPEC; i++) t[i] = b[sp_perm[i]];
+  for (int i = 0; i < NSPEC; i++) {
+    double s = t[i];
+    for (int p = sp_rp[i]; p < sp_di[i]; p++) s -= a[p] * t[sp_ci[p]];
+    t[i] = s;
+  }
+  double v = b[NSPEC];
+  for (int k = 0; k < NSPEC; k++) v -= br.Ct[k] * t[k];
+  v /= br.Z;
+  if (v != 0.0)
+    for (int k = 0; k < NSPEC; k++) t[k] -= br.Bt[k] * v;
+  for (int i = NSPEC - 1; i >= 0; i--) {
+    double s = t[i];
+    for (int p = sp_di[i] + 1; p < sp_rp[i + 1]; p++) s -= a[p] * t[sp_ci[p]];
+    t[i] = s / a[sp_di[i]];
+  }
+  for (int i = 0; i < NSPEC; i++) x[sp_perm[i]] = t[i];
+  x[NSPEC] = v;
+}
 #endif
 
 // ---- the per-cell problem (solve_cell.hpp:438-813, 883-1132) ------------
@@ -278,6 +333,34 @@ struct Problem {
     eval_rates(state_T(y), y, k0);
     for (int part = 0; part < NPART; ++part) jac_gather_part(part, y, k0, Jc);
     return 0;
+  }
+  // the Tgas border of the evolved-Tgas Jacobian (jac_assemble_,
+  // solve_cell.hpp:1053-1090): the Tgas column by central differences of
+  // the full rhs (B over the species, D its Tgas entry), the Tgas row by
+  // difference quotients over the densities with the rates re-evaluated (C)
+  void jac_border(const double* y, double* B, double* C, double* D,
+                  double* yp, double* fp) {
+    const int N = NEQ;
+    const double T = state_T(y);
+    for (int i = 0; i < N; ++i) yp[i] = y[i];
+    const double h = std::fmax(1e-6 * std::fabs(y[iT]), 1e-8);
+    yp[iT] = y[iT] + h;
+    full_rhs(yp, fp);
+    yp[iT] = y[iT] - h;
+    full_rhs(yp, fm);
+    yp[iT] = y[iT];
+    for (int i = 0; i < NSPEC; ++i) B[i] = (fp[i] - fm[i]) / (2.0 * h);
+    *D = (fp[iT] - fm[iT]) / (2.0 * h);
+    eval_rates(T, y, k0);
+    const double f0 = aux(y, k0);
+    for (int j = 0; j < NSPEC; ++j) {
+      const double hj = fd_step_n(y, j);
+      yp[j] = y[j] + hj;
+      eval_rates(T, yp, kp);
+      const double f1 = aux(yp, kp);
+      yp[j] = y[j];
+      C[j] = (f1 - f0) / hj;
+    }
   }
 #endif
   // g[r] += sum_i mu_i d f_i / d ln k_r at y (the emitted lnk_vjp)
@@ -426,7 +509,7 @@ class Cvode {
   Cvode(Problem& prob, int n, const BdfOpts& opts)
       : P(prob), N(n), o(opts),
 #ifdef KB_LARGE_NETWORK
-        work((L_MAX + 10) * n + NNZ_LU + NNZ_J),
+        work((L_MAX + 10) * n + NNZ_LU + NNZ_J + 4 * NSPEC),
 #else
         work((L_MAX + 9) * n + 2 * n * n),
 #endif
@@ -447,6 +530,11 @@ class Cvode {
     savedJ = w; w += NNZ_J;   // the Jacobian's entries
     spw = w;                  // the LU's dense work row (kept zeroed)
     for (int i = 0; i < N; i++) spw[i] = 0.0;
+    w += N;
+    border.B = w; w += NSPEC;  // the Tgas border (evolved Tgas)
+    border.C = w; w += NSPEC;
+    border.Bt = w; w += NSPEC;
+    border.Ct = w;
 #else
     A = w; w += (long)N * N;
     savedJ = w;
@@ -552,6 +640,9 @@ class Cvode {
   double *ewt, *y, *acor, *tempv, *ftemp, *delta, *vtemp1, *vtemp2, *vtemp3;
   double *A, *savedJ;
   double* spw = nullptr;
+#ifdef KB_LARGE_NETWORK
+  SpBorder border;
+#endif
   double tn = 0.0, h = 0.0, hin = 0.0, hprime = 0.0, hscale = 0.0, h0u = 0.0;
   double next_h = 0.0, hu = 0.0, eta = 1.0, etamax = 0.0, etaq = 0.0;
   double etaqm1 = 0.0, etaqp1 = 0.0, tolsf = 1.0, saved_tq5 = 0.0;
@@ -963,17 +1054,24 @@ class Cvode {
                            || ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_JBAD))
                            || (convfail == FAIL_OTHER);
       jcur = jbad_ls;
-      if (jbad_ls) P.jac_sparse_cb(y, savedJ);
+      if (jbad_ls) {
+        P.jac_sparse_cb(y, savedJ);
+        if (N > NSPEC)
+          P.jac_border(y, border.B, border.C, &border.D, vtemp1, vtemp2);
+      }
       const double c = -gamma;
       for (int k = 0; k < NNZ_LU; k++) A[k] = 0.0;
       for (int e = 0; e < NNZ_J; e++) A[sp_jpos[e]] = savedJ[e] * c;
-      for (int i = 0; i < N; i++) A[sp_di[i]] += 1.0;
+      for (int i = 0; i < NSPEC; i++) A[sp_di[i]] += 1.0;
       if (jcur) {
         st.nje++;
         nstlj = st.nst;
       }
       fact32 = false;
-      return sp_getrf_(A, spw) > 0 ? LS_LUFACT_FAIL : 0;
+      if (sp_getrf_(A, spw) > 0) return LS_LUFACT_FAIL;
+      if (N > NSPEC && sp_border_factor_(A, c, border) > 0)
+        return LS_LUFACT_FAIL;
+      return 0;
     }
 #endif
     const long NN = (long)N * N;
@@ -1018,7 +1116,8 @@ class Cvode {
   }
   int lsolve_(double* b) {
 #ifdef KB_LARGE_NETWORK
-    sp_getrs_(A, b, vtemp3, b);
+    if (N > NSPEC) sp_getrs_border_(A, border, b, vtemp3, b);
+    else sp_getrs_(A, b, vtemp3, b);
 #else
     if (fact32) getrs_(A32.data(), N, piv.data(), b);
     else getrs_(A, N, piv.data(), b);
@@ -1378,6 +1477,11 @@ int solve_one_(double* n, double* Tgas, const double* par, double dt,
   // JAC_AUTO (solve_cell.hpp:2141-2142): analytic at fixed Tgas, the
   // difference quotients when Tgas evolves
   const int jac = so->jac != 0 ? so->jac : (so->evolve_T ? 2 : 1);
+#ifdef KB_LARGE_NETWORK
+  // the large path's Jacobian is the analytic one (the difference
+  // quotients over every column are not restated there)
+  if (jac == 2) return -104;
+#endif
   BdfOpts bo;
   bo.rtol = so->rtol;
   bo.atol = avec.data();

@@ -15,6 +15,11 @@ Run where the reference tree and oracle/_ref (oracle/build_ref.py) exist:
   (oracle/_ref/libkrome_<net>_strict.so, krome_solve_cells) with the
   workload's options, each network in its own process (the generated
   libraries must not share one).
+
+and ``tests/golden/semenov_evt.npz``: 8 seeded Semenov cells solved by the
+reference's strict build with Tgas evolved and the analytic (hybrid)
+Jacobian (``evolve_T=1, jac=1``): the sparse LU with its Tgas border
+(``python tests/golden/make_golden.py semenov_evt``).
 """
 import re
 import sys
@@ -40,7 +45,29 @@ def _array(text, name):
     return np.array(eval(body), dtype=float)
 
 
+# fixtures of other solve options: name -> (network, cells, options added)
+VARIANTS = {"semenov_evt": ("semenov", 8, dict(evolve_T=1, jac=1))}
+
+
+def variant(name):
+    key, ncell, extra = VARIANTS[name]
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.GENERATORS[key](ncell, info, seed=11)
+    opts = dict(workloads.OPTIONS[key])
+    opts.update(extra)
+    out = reference_solve(key, n, T, dt, par, strict=True, **opts)
+    np.savez_compressed(HERE / ("%s.npz" % name), n=n, T=T, dt=dt, par=par,
+                        n_out=out["n"], T_out=out["T"], flags=out["flags"],
+                        ret=out["ret"])
+    print(name, "flags", np.unique(out["flags"]), "->", HERE / ("%s.npz" % name))
+
+
 def main(keys=None):
+    for name in [k for k in keys or () if k in VARIANTS]:
+        variant(name)
+    keys = [k for k in keys or () if k not in VARIANTS] if keys else None
+    if keys == []:
+        return
     for key in keys or ("primordial", "primordial3", "galaxy_ism", "semenov"):
         info = netinfo.load(key)
         chk = (ROOT / "oracle" / "_ref" / "gen" / key / "krome_check.cpp").read_text()

@@ -1,5 +1,6 @@
 """The large-network (sparse-LU) path: the Semenov surface-chemistry network,
-655 species and 5639 reactions, fixed Tgas.
+655 species and 5639 reactions, fixed Tgas, and evolved Tgas through the
+Newton matrix's Tgas border.
 
 Its GPU solve runs the same CVODE as the oracle with the same static-pivot
 sparse LU (a minimum-degree order fixed at generation); the bar is the
@@ -361,10 +362,93 @@ def test_sparse_edge_cases():
     assert not np.array_equal(r.n[0], n[0])
 
 
+EVT = dict(evolve_T=1, jac=1)
+
+
+def test_oracle_evolved_tgas_matches_reference_fixture_at_noise_level():
+    """8 reference-solved cells with Tgas evolved and the hybrid Jacobian
+    (the sparse LU bordered by the Tgas row and column): the oracle's
+    bordered factorization and solve at the same noise level as the
+    fixed-Tgas pin; Tgas (no thermal processes) comes back unchanged"""
+    g = golden("semenov_evt")
+    opts = dict(workloads.OPTIONS[KEY])
+    opts.update(EVT)
+    out = Oracle(KEY).solve(g["n"], g["T"], g["dt"], g["par"], **opts)
+    assert out["ret"] == g["ret"]
+    m = parity_major(out["n"], out["flags"], g["n_out"], g["flags"], g["n"],
+                     opts["rtol"])
+    assert m["flags_equal"] == 1.0 and m["cells"] == len(g["n"]), m
+    assert m["max_rel"] < 1e-4 and m["frac"] >= 0.75, m
+    np.testing.assert_array_equal(out["T"], g["T_out"])
+    np.testing.assert_array_equal(g["T_out"], g["T"])
+    # a different solve from the fixed-Tgas one: the norms run over the
+    # Tgas component too, so the step sequence differs
+    fixed = Oracle(KEY).solve(g["n"][:2], g["T"][:2], g["dt"][:2],
+                              g["par"][:2], **workloads.OPTIONS[KEY])
+    assert (fixed["stats"][:, 0] != out["stats"][:2, 0]).any()
+
+
+def test_oracle_evolved_tgas_edge_rules():
+    """evolved Tgas on the large path: Tgas <= 0 fails with -110 and the
+    cell untouched; JAC_AUTO's difference quotients are refused (-104)"""
+    info = netinfo.load(KEY)
+    n, T, dt, par = workloads.semenov(2, info, seed=6)
+    T = T.copy()
+    T[1] = -5.0
+    opts = dict(workloads.OPTIONS[KEY])
+    opts.update(EVT)
+    out = Oracle(KEY).solve(n[1:], T[1:], dt[1:], par[1:], **opts)
+    assert list(out["flags"]) == [-110]
+    np.testing.assert_array_equal(out["n"], n[1:])
+    opts.update(jac=0)
+    out = Oracle(KEY).solve(n[:1], T[:1], dt[:1], par[:1], **opts)
+    assert list(out["flags"]) == [-104]
+
+
+@pytest.mark.gpu
+def test_sparse_evolved_tgas_parity():
+    """the GPU's bordered solve against the reference fixture and the
+    oracle: the large-network metric, flags equal, Tgas returned, the
+    oracle's step counts within the chaotic spread, mass conserved; the
+    edge rules (-110, -104) as the oracle's"""
+    g = golden("semenov_evt")
+    opts = dict(workloads.OPTIONS[KEY])
+    opts.update(EVT)
+    net = krome.load(KEY)
+    r = net.solve_batch(g["n"], g["T"], g["dt"], g["par"],
+                        opts=net.options(**opts), check=False, stats=True)
+    m = parity_major(r.n, r.flags, g["n_out"], g["flags"], g["n"],
+                     opts["rtol"])
+    assert m["flags_equal"] == 1.0 and m["cells"] == len(g["n"]), m
+    assert m["max_rel"] < 2e-4 and m["frac"] >= 0.7, m
+    np.testing.assert_array_equal(r.Tgas, g["T_out"])
+    ref = Oracle(KEY).solve(g["n"], g["T"], g["dt"], g["par"], **opts)
+    m = parity_major(r.n, r.flags, ref["n"], ref["flags"], g["n"],
+                     opts["rtol"])
+    assert m["max_rel"] < 2e-4 and m["frac"] >= 0.7, m
+    a, b = r.stats[:, 0].mean(), ref["stats"][:, 0].mean()
+    assert abs(a - b) <= 0.05 * b, (a, b)
+    mass = np.asarray(netinfo.load(KEY)["mass_g"])
+    np.testing.assert_allclose(r.n @ mass, g["n"] @ mass, rtol=1e-10)
+    info = netinfo.load(KEY)
+    n, T, dt, par = workloads.semenov(2, info, seed=6)
+    T = T.copy()
+    T[1] = -5.0
+    r = net.solve_batch(n[1:], T[1:], dt[1:], par[1:],
+                        opts=net.options(**opts), check=False)
+    assert list(r.flags) == [-110]
+    np.testing.assert_array_equal(r.n, n[1:])
+    opts.update(jac=0)
+    r = net.solve_batch(n[:1], T[:1], dt[:1], par[:1],
+                        opts=net.options(**opts), check=False)
+    assert r.ierr == -104
+
+
 @pytest.mark.gpu
 def test_sparse_unsupported_forms_return_minus_104():
-    """the large path runs fixed Tgas and FP64 sparse (or auto) LU; the
-    dense LU, evolve_T, the FP32 Newton matrix and the adjoint are the small
+    """the large path runs the FP64 sparse (or auto) LU, Tgas fixed or
+    evolved with the analytic Jacobian; the dense LU, the difference-
+    quotient Jacobian, the FP32 Newton matrix and the adjoint are the small
     networks' forms"""
     info = netinfo.load(KEY)
     n, T, dt, par = workloads.semenov(2, info, seed=6)
