@@ -65,6 +65,10 @@ NETWORKS = {
     # required by Semenov.knet (its binding energies)
     "semenov": dict(options_toml="examples/tests/cloudSurface/options.toml",
                     network_file="networks/Semenov.knet"),
+    # a second large network on the sparse path: the reference's gas-phase
+    # dark-cloud chemistry (networks/cloud.knet, 452 species), default
+    # thermal options
+    "cloud": dict(network="cloud", cooling=[], heating=[]),
 }
 # networks above this many species take the sparse path (one warp per cell,
 # the state in HBM, the static-pivot sparse LU)

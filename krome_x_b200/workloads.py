@@ -25,6 +25,11 @@ the network's code-point order, ``Tgas[ncell]``, ``dt[ncell]``,
   crflux 1.3e-17, grains of 0.1 micron: gsize 1e-5, gsize2 1e-10, xdust =
   0.01 rho / (4/3 pi 3 a^3 1.43) grains per cm^3, also GRAIN0's density,
   Tdust = Tgas); dt = 3.15e13 s (examples/tests/cloudSurface/test.cpp).
+* ``cloud``        the reference's gas-phase dark-cloud network (452
+  species), a second network on the sparse path: Semenov's n_H, Tgas and
+  initial abundances (the species both networks have), every other species
+  1e-20 n_H, electrons for neutrality, grains GRAIN0 = 1.3e-12 n_H; Av 10,
+  crate 1.3e-17, gas_dust_ratio 1; dt = 3.15e13 s.
 * ``galaxy_ism``   (config 4) n_H log-uniform in [1e-2, 1e4], Tgas in
   [10, 1e6] K, crate in [1e-17, 1e-16], G0 in [0.3, 3], d2g in
   [0.003, 0.03] (log-uniform, one decade around the typical values);
@@ -229,6 +234,26 @@ def semenov(ncell, info, seed=0):
     return n, T, dt, par
 
 
+def cloud(ncell, info, seed=0):
+    species, param_names = info["species"], info["params"]
+    rng = np.random.default_rng(seed)
+    ix = _index(species)
+    nH = loguniform(rng, 1e2, 1e7, ncell)
+    T = loguniform(rng, 10.0, 300.0, ncell)
+    n = np.repeat((1e-20 * nH)[:, None], len(species), axis=1)
+    for s, x in SEMENOV_INITIAL:
+        n[:, ix[s]] = x * nH * loguniform(rng, 0.5, 2.0, ncell)
+    n[:, ix["GRAIN0"]] = 1.3e-12 * nH
+    charge = np.asarray(info["charge"], dtype=float)
+    ions = [i for i, s in enumerate(species) if s != "e-"]
+    n[:, ix["e-"]] = np.maximum((n[:, ions] * charge[ions]).sum(axis=1), 0.0)
+    par = _default_rows(ncell, info)
+    for name, v in (("Av", 10.0), ("crate", 1.3e-17), ("gas_dust_ratio", 1.0)):
+        par[:, param_names.index(name)] = v
+    dt = np.full(ncell, 3.15e13)
+    return n, T, dt, par
+
+
 def _default_rows(ncell, info):
     """every cell's parameter row at the network defaults (NaN: required)"""
     return np.repeat(np.asarray(info["defaults"], dtype=float)[None, :],
@@ -240,7 +265,7 @@ def hydro_step_info(n, par, info):
 
 
 GENERATORS = {"primordial": primordial, "primordial3": primordial3,
-              "galaxy_ism": galaxy_ism, "semenov": semenov,
+              "galaxy_ism": galaxy_ism, "semenov": semenov, "cloud": cloud,
               "primordialZ": primordialZ, "earlyUniverse": earlyUniverse}
 
 # the solve options of each workload (krome_opts keys)
@@ -257,4 +282,6 @@ OPTIONS = {
                           atol_n=1e-20, atol_T=1e-6),
     "semenov": dict(evolve_T=0, jac=0, linsol=3, rtol=1e-6, atol_n=1e-20,
                     atol_T=1e-6, max_steps=1000000),
+    "cloud": dict(evolve_T=0, jac=0, linsol=3, rtol=1e-6, atol_n=1e-20,
+                  atol_T=1e-6, max_steps=1000000),
 }

@@ -60,7 +60,7 @@ def _configure(key):
         kp.thermal.heating = ["COMPRESS", "CHEM"]
         kp.thermal.h2_opacity = "RIPAMONTI"
         kp.thermal.gamma = "EXACT"
-    elif key in ("galaxy_ism", "primordialZ", "earlyUniverse"):
+    elif key in ("galaxy_ism", "primordialZ", "earlyUniverse", "cloud"):
         kp = Preprocessor(network=key)
     elif key == "semenov":
         kp = Preprocessor.from_file(
@@ -98,7 +98,7 @@ def main(argv):
     sys.path.insert(0, str(REF / "kromex"))
     OUT.mkdir(parents=True, exist_ok=True)
     keys = argv or ["primordial", "primordial3", "galaxy_ism", "primordialZ",
-                    "earlyUniverse", "semenov"]
+                    "earlyUniverse", "semenov", "cloud"]
     for k in keys:
         build(k)
 

@@ -16,7 +16,7 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 NETWORKS = ("primordial", "primordial3", "galaxy_ism")
 # networks past the dense kernels' size, solved by the sparse path
-LARGE = ("semenov",)
+LARGE = ("semenov", "cloud")
 ALL_NETWORKS = NETWORKS + LARGE
 
 

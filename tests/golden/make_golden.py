@@ -10,7 +10,7 @@ Run where the reference tree and oracle/_ref (oracle/build_ref.py) exist:
   independent network interpreter, kromex/netcheck.py), with the probe
   parameters of that check (every parameter 1.3e-17, Tdust 10 K);
 * ``n, T, dt, par`` / ``n_out, T_out, flags``: 64 seeded cells (16 for
-  Semenov) of the
+  the large networks, Semenov and cloud) of the
   benchmark workload solved by the reference's strict build
   (oracle/_ref/libkrome_<net>_strict.so, krome_solve_cells) with the
   workload's options, each network in its own process (the generated
@@ -75,8 +75,8 @@ def main(keys=None):
         k_n = _array(chk, "N_REF")
         k_idx = _array(chk, "I_REF").astype(np.int32)
         k_ref = _array(chk, "K_REF")
-        # the large network's cells take ~1 s each in the reference
-        ncell = 16 if key == "semenov" else NCELL
+        # the large networks' cells take ~1 s each in the reference
+        ncell = 16 if key in ("semenov", "cloud") else NCELL
         n, T, dt, par = workloads.GENERATORS[key](ncell, info, seed=11)
         opts = dict(workloads.OPTIONS[key])
         out = reference_solve(key, n, T, dt, par, strict=True, **opts)

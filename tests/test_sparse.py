@@ -26,11 +26,12 @@ TABLES = ("sp_rp", "sp_ci", "sp_di", "sp_perm", "sp_jpos", "bk_frow",
           "bkl_cu")
 
 
-@pytest.fixture(scope="module")
-def sched():
+@pytest.fixture(scope="module", params=("semenov", "cloud"))
+def sched(request):
     """the sparse LU's generation-time tables and constants, read from the
-    generated network header"""
-    text = (ROOT / "krome_x_b200" / "networks" / ("net_%s.h" % KEY)).read_text()
+    generated network header (each large network's)"""
+    text = (ROOT / "krome_x_b200" / "networks"
+            / ("net_%s.h" % request.param)).read_text()
     t = {}
     for name in TABLES:
         m = re.search(r"#define KB_T_%s ([0-9,\-]+)" % name, text)
