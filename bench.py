@@ -53,6 +53,9 @@ exists for this path). A step is 262,144 cell-solves.
                        the sparse-LU block-per-cell kernel on the first cells
                        of the seeded 16,384-cell batch: cell-solves/s, its
                        algorithmic bytes and DRAM traffic against the HBM peak
+            large_network_cloud  the second large network on the same
+                       kernel: the reference's dark-cloud chemistry (452
+                       species, 4,429 reactions), 2,048 seeded cells
 
 ``python bench.py --gpus N --steps K --warmup W [--impl reference]``; with
 N > 1 each rank (torchrun) solves its own 262,144 cells (weak scaling: no
@@ -583,6 +586,55 @@ def large_network_form(torch, dev, ncell=SEMENOV_CELLS, cpu_cells=512):
             if cpu_cells > 0 else None}
 
 
+def cloud_form(torch, dev, ncell=2048, cpu_cells=512):
+    """the sparse path on the second large network: the reference's
+    gas-phase dark-cloud chemistry (452 species, 4,429 reactions), fixed
+    Tgas, one launch over the seeded 2,048-cell batch"""
+    from krome_x_b200 import krome, netinfo, workloads
+    key = "cloud"
+    info = netinfo.load(key)
+    n, T, dt, par = workloads.cloud(ncell, info, seed=0)
+    net = krome.load(key)
+    opts = net.options(**workloads.OPTIONS[key])
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    nd, Td = t(n), t(T)
+    fl = torch.zeros(ncell, dtype=torch.int32, device=dev)
+    st = torch.zeros((ncell, len(STAT_NAMES)), dtype=torch.int64, device=dev)
+    cur = torch.zeros(1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    e0 = _events(torch)
+    net.solve_device(nd, Td, t(dt), t(par), fl, opts=opts, stats=st,
+                     cursor=cur)
+    e1 = _events(torch)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    tot = dict(zip(STAT_NAMES, st.cpu().numpy().sum(axis=0).astype(float)))
+    nnz_j, nnz_lu = info["nnz_j"], info["nnz_lu"]
+    alg = 8.0 * (tot["nsetups"] * (nnz_j + 2 * nnz_lu) + tot["nni"] * nnz_lu
+                 + (tot["nfe"] + tot["nfeDQ"]) * (net.nrea + 2 * net.nspec))
+    peak, peak_source = _hbm_peak()
+    mass = np.asarray(info["mass_g"])
+    out = nd.cpu().numpy()
+    return {"workload": "cloud (452 species, 4,429 reactions), fixed Tgas, "
+                        "rtol 1e-6, dt 3.15e13 s, sparse LU; %d seeded cells"
+                        % ncell,
+            "cell_solves_per_s": ncell / (ms * 1e-3), "ms": ms,
+            "failed_cells": int((fl != 0).sum().item()),
+            "mean_steps_per_cell": tot["nst"] / ncell,
+            "mass_conservation_max_rel": float(
+                np.abs(out @ mass / (n @ mass) - 1).max()),
+            "hbm": {"algorithmic_bytes": alg,
+                    "algorithmic_gbs": alg / (ms * 1e-3) / 1e9,
+                    "peak_gbs": peak, "peak_source": peak_source,
+                    "algorithmic_frac": alg / (ms * 1e-3) / 1e9 / peak,
+                    "algorithmic_bytes_formula":
+                        "nsetups 8 (nnzJ + 2 nnzLU) + nni 8 nnzLU + nfe 8 "
+                        "(nrea + 2 nspec), nnzJ %d, nnzLU %d" % (nnz_j, nnz_lu)},
+            "cpu_baseline": cpu_form(key, ncell, cpu_cells, 0,
+                                     workloads.OPTIONS[key])
+            if cpu_cells > 0 else None}
+
+
 def batching_form(torch, dev, ncell=262144, calls=3):
     """the batching workload itself (262,144 primordial3 cells of rank 0's
     seeded batch, the captured hydro loop's first `calls` calls: the first,
@@ -806,7 +858,9 @@ def run_ours(args, rank, world, local):
                  "precision": precision_form(torch, dev, cpu=cpu_forms),
                  "large_network": large_network_form(
                      torch, dev, args.large_cells,
-                     args.large_cpu_cells if cpu_forms else 0)}
+                     args.large_cpu_cells if cpu_forms else 0),
+                 "large_network_cloud": cloud_form(
+                     torch, dev, cpu_cells=512 if cpu_forms else 0)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_leg(args.cpu_cells, args.cells, args.warmup, args.steps)
