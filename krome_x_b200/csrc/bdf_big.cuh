@@ -705,45 +705,60 @@ enum { RW_FWD, RW_BWD, RW_L21 };
 // the next row's entries loaded while the current one is summed. MODE:
 // RW_FWD the L entries (sc = 1, unit diagonal), RW_BWD the U entries (sc =
 // 1 / the pivot), RW_L21 a dense row's sparse-column L entries (sc = 1).
+// a row's range of entries in MODE's part of the factors
 template <int MODE>
-__device__ void rows_by_warp(const int* rows, int r0, int r1, int rs,
-                             const double* A, const double* rpiv, double* t) {
-  const int lane = threadIdx.x & 31;
-  auto range = [&](int i, int& p0, int& p1) {
-    if (MODE == RW_FWD) { p0 = d_sp_rp[i]; p1 = d_sp_di[i]; }
-    else if (MODE == RW_BWD) { p0 = d_sp_di[i] + 1; p1 = d_sp_rp[i + 1]; }
-    else { p0 = d_sp_rp[i]; p1 = d_bk_l21e[i - BK_M]; }
-  };
-  auto row = [&](int r) { return rows != nullptr ? rows[r] : r; };
+__device__ __forceinline__ void row_range(int i, int& p0, int& p1) {
+  if (MODE == RW_FWD) { p0 = d_sp_rp[i]; p1 = d_sp_di[i]; }
+  else if (MODE == RW_BWD) { p0 = d_sp_di[i] + 1; p1 = d_sp_rp[i + 1]; }
+  else { p0 = d_sp_rp[i]; p1 = d_bk_l21e[i - BK_M]; }
+}
+// the first 128 entries of a warp's row (4 a lane): values and columns.
+// The factors and the tables do not change during a solve, so a warp loads
+// the row of its next call before the barrier that ends the current one
+// (only t, read after it, does).
+struct RowAhead {
   double a[4];
   int c[4];
-  auto fetch = [&](int r) {
-    int p0, p1;
-    range(row(r), p0, p1);
+  bool ok;
+};
+template <int MODE>
+__device__ __forceinline__ void row_ahead(const int* rows, int r, int r1,
+                                          const double* A, RowAhead& q) {
+  q.ok = r < r1;
+  if (!q.ok) return;
+  const int lane = threadIdx.x & 31;
+  int p0, p1;
+  row_range<MODE>(rows != nullptr ? rows[r] : r, p0, p1);
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int p = p0 + lane + 32 * s;
-      c[s] = p < p1 ? d_sp_ci[p] : -1;
-      a[s] = p < p1 ? A[p] : 0.0;
-    }
-  };
-  if (r0 < r1) fetch(r0);
+  for (int s = 0; s < 4; ++s) {
+    const int p = p0 + lane + 32 * s;
+    q.c[s] = p < p1 ? d_sp_ci[p] : -1;
+    q.a[s] = p < p1 ? A[p] : 0.0;
+  }
+}
+
+// rows r0, r0 + rs, ... < r1 of `rows` (nullptr: the rows themselves), a
+// warp per row, each row's first 128 entries loaded while the previous
+// row is summed (the first row's from q when it holds them)
+template <int MODE>
+__device__ void rows_by_warp(const int* rows, int r0, int r1, int rs,
+                             const double* A, const double* rpiv, double* t,
+                             const RowAhead* q = nullptr) {
+  const int lane = threadIdx.x & 31;
+  auto row = [&](int r) { return rows != nullptr ? rows[r] : r; };
+  RowAhead cur;
+  if (q != nullptr && q->ok) cur = *q;
+  else row_ahead<MODE>(rows, r0, r1, A, cur);
   for (int r = r0; r < r1; r += rs) {
     const int i = row(r);
-    double ac[4];
-    int cc[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      ac[s] = a[s];
-      cc[s] = c[s];
-    }
-    if (r + rs < r1) fetch(r + rs);
+    const RowAhead now = cur;
+    if (r + rs < r1) row_ahead<MODE>(rows, r + rs, r1, A, cur);
     double sum = 0.0;
 #pragma unroll
     for (int s = 0; s < 4; ++s)
-      if (cc[s] >= 0) sum += ac[s] * t[cc[s]];
+      if (now.c[s] >= 0) sum += now.a[s] * t[now.c[s]];
     int p0, p1;
-    range(i, p0, p1);
+    row_range<MODE>(i, p0, p1);
     for (int p = p0 + 128 + lane; p < p1; p += 32) sum += A[p] * t[d_sp_ci[p]];
     sum = warp_sum(sum);
     if (lane == 0) t[i] = MODE == RW_BWD ? (t[i] - sum) * rpiv[i] : t[i] - sum;
@@ -761,6 +776,9 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   __syncthreads();
   KBG_FOR(i) t[i] = b[d_sp_perm[i]];
   __syncthreads();
+  // q: this warp's first row of the next narrow level, loaded ahead
+  RowAhead q;
+  q.ok = false;
   for (int L = 1; L < BK_NLF; ++L) {  // level 0 rows have no L entries
     const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
     if (r1 - r0 >= 16) {  // wide levels' rows have a few L entries each
@@ -771,19 +789,29 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
         t[i] -= s;
       }
     } else {
-      rows_by_warp<RW_FWD>(d_bk_frow, r0 + warp, r1, NWARP, A, rpiv, t);
+      rows_by_warp<RW_FWD>(d_bk_frow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
+    }
+    if (L + 1 < BK_NLF) {
+      const int n0 = d_bk_flp[L + 1], n1 = d_bk_flp[L + 2];
+      if (n1 - n0 < 16) row_ahead<RW_FWD>(d_bk_frow, n0 + warp, n1, A, q);
+      else q.ok = false;
+    } else {
+      row_ahead<RW_L21>(nullptr, BK_M + warp, N, A, q);
     }
     __syncthreads();
   }
   // the dense rows' sparse columns: a warp per row (a hub row has hundreds)
-  rows_by_warp<RW_L21>(nullptr, BK_M + warp, N, NWARP, A, rpiv, t);
+  rows_by_warp<RW_L21>(nullptr, BK_M + warp, N, NWARP, A, rpiv, t, &q);
+  row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[0] + warp, d_bk_blp[1], A, q);
   __syncthreads();
   dense_fwd(S, t + BK_M);
   dense_bwd(S, rpiv + BK_M, t + BK_M);
   for (int L = 0; L < BK_NLB; ++L) {  // a warp per row (U rows reach into
                                       // the dense columns)
     const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
-    rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t);
+    rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
+    if (L + 1 < BK_NLB)
+      row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[L + 1] + warp, d_bk_blp[L + 2], A, q);
     __syncthreads();
   }
   KBG_FOR(i) x[d_sp_perm[i]] = t[i];
