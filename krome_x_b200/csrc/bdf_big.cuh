@@ -766,6 +766,36 @@ __device__ void rows_by_warp(const int* rows, int r0, int r1, int rs,
   }
 }
 
+// the rows r0.. < r1 of a level wider than the block's warps, G lanes a
+// row (32 / G rows a warp at a time): a level of many short rows (the
+// backward sweep's first levels: 50-80 rows of ~12 entries) would leave a
+// warp per row mostly idle and its rows one after another
+template <int MODE, int G>
+__device__ void rows_by_group(const int* rows, int r0, int r1,
+                              const double* A, const double* rpiv, double* t) {
+  constexpr int PW = 32 / G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane % G;
+  // bounded: each pass advances every lane's row by NWARP * PW
+  for (int r = r0 + warp * PW + lane / G;; r += NWARP * PW) {
+    const bool has = r < r1;
+    if (!__any_sync(FULLM, has)) break;
+    double sum = 0.0;
+    int i = 0;
+    if (has) {
+      i = rows != nullptr ? rows[r] : r;
+      int p0, p1;
+      row_range<MODE>(i, p0, p1);
+      for (int p = p0 + sub; p < p1; p += G) sum += A[p] * t[d_sp_ci[p]];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(FULLM, sum, o);
+    if (has && sub == 0)
+      t[i] = MODE == RW_BWD ? (t[i] - sum) * rpiv[i] : t[i] - sum;
+    __syncwarp();
+  }
+}
+
 // x = A^-1 b with the factors (b and x in the species order; x may be b).
 // Starts and ends with a block barrier; one barrier per level.
 __device__ void block_solve(const double* A, const double* b, double* x) {
@@ -788,12 +818,14 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
         for (int p = d_sp_rp[i]; p < d_sp_di[i]; ++p) s += A[p] * t[d_sp_ci[p]];
         t[i] -= s;
       }
+    } else if (r1 - r0 > NWARP) {
+      rows_by_group<RW_FWD, 8>(d_bk_frow, r0, r1, A, rpiv, t);
     } else {
       rows_by_warp<RW_FWD>(d_bk_frow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
     }
     if (L + 1 < BK_NLF) {
       const int n0 = d_bk_flp[L + 1], n1 = d_bk_flp[L + 2];
-      if (n1 - n0 < 16) row_ahead<RW_FWD>(d_bk_frow, n0 + warp, n1, A, q);
+      if (n1 - n0 <= NWARP) row_ahead<RW_FWD>(d_bk_frow, n0 + warp, n1, A, q);
       else q.ok = false;
     } else {
       row_ahead<RW_L21>(nullptr, BK_M + warp, N, A, q);
@@ -802,15 +834,22 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   }
   // the dense rows' sparse columns: a warp per row (a hub row has hundreds)
   rows_by_warp<RW_L21>(nullptr, BK_M + warp, N, NWARP, A, rpiv, t, &q);
-  row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[0] + warp, d_bk_blp[1], A, q);
+  if (d_bk_blp[1] - d_bk_blp[0] <= NWARP)
+    row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[0] + warp, d_bk_blp[1], A, q);
+  else
+    q.ok = false;
   __syncthreads();
   dense_fwd(S, t + BK_M);
   dense_bwd(S, rpiv + BK_M, t + BK_M);
   for (int L = 0; L < BK_NLB; ++L) {  // a warp per row (U rows reach into
                                       // the dense columns)
     const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
-    rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
-    if (L + 1 < BK_NLB)
+    if (r1 - r0 > NWARP)
+      rows_by_group<RW_BWD, 8>(d_bk_brow, r0, r1, A, rpiv, t);
+    else
+      rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
+    q.ok = false;
+    if (L + 1 < BK_NLB && d_bk_blp[L + 2] - d_bk_blp[L + 1] <= NWARP)
       row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[L + 1] + warp, d_bk_blp[L + 2], A, q);
     __syncthreads();
   }
