@@ -809,9 +809,17 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   // q: this warp's first row of the next narrow level, loaded ahead
   RowAhead q;
   q.ok = false;
-  for (int L = 1; L < BK_NLF; ++L) {  // level 0 rows have no L entries
+  // (a run of single-row levels -- the chain before the dense block --
+  // goes to warp 0 in one call: its rows in order, no block barrier
+  // between them, each row's factors loaded while the previous is summed)
+  for (int L = 1, Ln; L < BK_NLF; L = Ln) {  // level 0 rows have no L entries
     const int r0 = d_bk_flp[L], r1 = d_bk_flp[L + 1];
-    if (r1 - r0 >= 16) {  // wide levels' rows have a few L entries each
+    Ln = L + 1;
+    if (r1 - r0 == 1) {
+      while (Ln < BK_NLF && d_bk_flp[Ln + 1] - d_bk_flp[Ln] == 1) ++Ln;
+      if (warp == 0)
+        rows_by_warp<RW_FWD>(d_bk_frow, r0, d_bk_flp[Ln], 1, A, rpiv, t, &q);
+    } else if (r1 - r0 >= 16) {  // wide levels' rows have a few L entries each
       for (int r = r0 + tid; r < r1; r += NT) {
         const int i = d_bk_frow[r];
         double s = 0.0;
@@ -823,8 +831,8 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
     } else {
       rows_by_warp<RW_FWD>(d_bk_frow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
     }
-    if (L + 1 < BK_NLF) {
-      const int n0 = d_bk_flp[L + 1], n1 = d_bk_flp[L + 2];
+    if (Ln < BK_NLF) {
+      const int n0 = d_bk_flp[Ln], n1 = d_bk_flp[Ln + 1];
       if (n1 - n0 <= NWARP) row_ahead<RW_FWD>(d_bk_frow, n0 + warp, n1, A, q);
       else q.ok = false;
     } else {
@@ -841,16 +849,22 @@ __device__ void block_solve(const double* A, const double* b, double* x) {
   __syncthreads();
   dense_fwd(S, t + BK_M);
   dense_bwd(S, rpiv + BK_M, t + BK_M);
-  for (int L = 0; L < BK_NLB; ++L) {  // a warp per row (U rows reach into
-                                      // the dense columns)
+  for (int L = 0, Ln; L < BK_NLB; L = Ln) {  // a warp per row (U rows reach
+                                             // into the dense columns)
     const int r0 = d_bk_blp[L], r1 = d_bk_blp[L + 1];
-    if (r1 - r0 > NWARP)
+    Ln = L + 1;
+    if (r1 - r0 == 1) {  // a run of single-row levels: warp 0, in order
+      while (Ln < BK_NLB && d_bk_blp[Ln + 1] - d_bk_blp[Ln] == 1) ++Ln;
+      if (warp == 0)
+        rows_by_warp<RW_BWD>(d_bk_brow, r0, d_bk_blp[Ln], 1, A, rpiv, t, &q);
+    } else if (r1 - r0 > NWARP) {
       rows_by_group<RW_BWD, 8>(d_bk_brow, r0, r1, A, rpiv, t);
-    else
+    } else {
       rows_by_warp<RW_BWD>(d_bk_brow, r0 + warp, r1, NWARP, A, rpiv, t, &q);
+    }
     q.ok = false;
-    if (L + 1 < BK_NLB && d_bk_blp[L + 2] - d_bk_blp[L + 1] <= NWARP)
-      row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[L + 1] + warp, d_bk_blp[L + 2], A, q);
+    if (Ln < BK_NLB && d_bk_blp[Ln + 1] - d_bk_blp[Ln] <= NWARP)
+      row_ahead<RW_BWD>(d_bk_brow, d_bk_blp[Ln] + warp, d_bk_blp[Ln + 1], A, q);
     __syncthreads();
   }
   KBG_FOR(i) x[d_sp_perm[i]] = t[i];
