@@ -16,10 +16,11 @@ Run where the reference tree and oracle/_ref (oracle/build_ref.py) exist:
   workload's options, each network in its own process (the generated
   libraries must not share one).
 
-and ``tests/golden/semenov_evt.npz``: 8 seeded Semenov cells solved by the
-reference's strict build with Tgas evolved and the analytic (hybrid)
-Jacobian (``evolve_T=1, jac=1``): the sparse LU with its Tgas border
-(``python tests/golden/make_golden.py semenov_evt``).
+and ``tests/golden/semenov_evt.npz`` / ``cloud_evt.npz``: 8 seeded cells of
+each large network solved by the reference's strict build with Tgas evolved
+and the analytic (hybrid) Jacobian (``evolve_T=1, jac=1``): the sparse LU
+with its Tgas border (``python tests/golden/make_golden.py semenov_evt
+cloud_evt``).
 """
 import re
 import sys
@@ -46,7 +47,8 @@ def _array(text, name):
 
 
 # fixtures of other solve options: name -> (network, cells, options added)
-VARIANTS = {"semenov_evt": ("semenov", 8, dict(evolve_T=1, jac=1))}
+VARIANTS = {"semenov_evt": ("semenov", 8, dict(evolve_T=1, jac=1)),
+            "cloud_evt": ("cloud", 8, dict(evolve_T=1, jac=1))}
 
 
 def variant(name):

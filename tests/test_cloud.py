@@ -61,3 +61,39 @@ def test_cloud_gpu_parity_with_reference_fixture_and_oracle():
     np.testing.assert_allclose(r.n @ mass, n @ mass, rtol=1e-10)
     a, b = r.stats[:, 0].mean(), ref["stats"][:, 0].mean()
     assert abs(a - b) <= 0.05 * b, (a, b)
+
+
+EVT = dict(evolve_T=1, jac=1)
+
+
+def test_cloud_evolved_tgas_oracle_equals_reference_bitwise():
+    """8 reference-solved cells with Tgas evolved and the hybrid Jacobian:
+    the oracle's bordered sparse LU (B' = L^-1 cB, C' = cC U^-1, the Schur
+    complement Z and the bordered solve) equals the reference's strict
+    build bit for bit; Tgas (no thermal processes) comes back unchanged"""
+    g = golden("cloud_evt")
+    opts = dict(workloads.OPTIONS[KEY])
+    opts.update(EVT)
+    out = Oracle(KEY).solve(g["n"], g["T"], g["dt"], g["par"], **opts)
+    np.testing.assert_array_equal(out["flags"], g["flags"])
+    np.testing.assert_array_equal(out["n"], g["n_out"])
+    np.testing.assert_array_equal(out["T"], g["T_out"])
+    np.testing.assert_array_equal(g["T_out"], g["T"])
+
+
+@pytest.mark.gpu
+def test_cloud_gpu_evolved_tgas_parity():
+    """the GPU's bordered solve on this network against the reference's
+    evolved-Tgas fixture: the large networks' bar, flags equal, Tgas
+    returned"""
+    g = golden("cloud_evt")
+    opts = dict(workloads.OPTIONS[KEY])
+    opts.update(EVT)
+    net = krome.load(KEY)
+    r = net.solve_batch(g["n"], g["T"], g["dt"], g["par"],
+                        opts=net.options(**opts), check=False)
+    m = parity_major(r.n, r.flags, g["n_out"], g["flags"], g["n"],
+                     opts["rtol"])
+    assert m["flags_equal"] == 1.0 and m["cells"] == len(g["n"]), m
+    assert m["max_rel"] < 2e-4 and m["frac"] >= 0.7, m
+    np.testing.assert_array_equal(r.Tgas, g["T_out"])
